@@ -1,0 +1,286 @@
+"""Assembled multilevel systems: the data that crosses the drop-in boundary.
+
+A ``Problem`` holds exactly what the reference hands its GPU backend for the
+linear-solve path (Gascoigne ``cuda/cudasolver.cc:115-128, 161-298``,
+``cuda/cudamgintepolatornested.cc:21-25``):
+
+* per level (0 = coarsest, the reference's solver indexing,
+  ``Solver/stdmultilevelsolver.cc:224-231``) the block-CSR matrix of
+  ``SparseBlockMatrix<FMatrixBlock<B>>`` with its ``ColumnDiagStencil``
+  (``LinAlg/columnstencil.h:57-60``, ``LinAlg/columndiagstencil.h:54-57``),
+  blocks row-major (``LinAlg/nodematrix.h:44-48``);
+* per level the strong-Dirichlet node list (``DofHandler/cgdisc.h:1162-1179``);
+* per level pair the mesh-transfer maps ``c2f``/``zweier``/``vierer``/``achter``
+  (``Mesh/gascoignemeshtransfer.h:48-51``);
+* the finest-level right-hand side.
+
+Two producers exist: ``load_reference_dump`` reads what the reference's own
+solver assembled (written by the oracle harness), and ``structured_problem``
+assembles the same operator on a lexicographically numbered uniform Q1 mesh
+(the synthetic workload generator used where the reference is not present).
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+
+@dataclass
+class Level:
+    n: int                      # block rows (nodes)
+    B: int                      # block size (components per node)
+    rowptr: np.ndarray          # int64 [n+1]
+    col: np.ndarray             # int64 [nnzb]
+    diag: np.ndarray            # int64 [n]   position of the diagonal block
+    val: np.ndarray             # float64 [nnzb*B*B]
+    dirichlet: np.ndarray       # int64 [ndir] Dirichlet nodes
+    dircomp_mask: int = 1       # bit c: component c is Dirichlet
+    coord: Optional[np.ndarray] = None  # float64 [n, dim]
+
+    @property
+    def nnzb(self) -> int:
+        return int(self.col.shape[0])
+
+    @property
+    def ndof(self) -> int:
+        return self.n * self.B
+
+
+@dataclass
+class Transfer:
+    """Transfer between level l (coarse) and l+1 (fine)."""
+    c2f: np.ndarray             # int64 [ncoarse]
+    zweier: np.ndarray          # int64 [nz, 3]  fine, 2 coarse parents
+    vierer: np.ndarray          # int64 [nv, 5]
+    achter: np.ndarray          # int64 [na, 9]
+
+    @property
+    def ncoarse(self) -> int:
+        return int(self.c2f.shape[0])
+
+
+@dataclass
+class Problem:
+    dim: int
+    levels: List[Level]
+    transfers: List[Transfer]
+    rhs: np.ndarray
+    info: dict = field(default_factory=dict)
+
+    @property
+    def nlevels(self) -> int:
+        return len(self.levels)
+
+    @property
+    def finest(self) -> Level:
+        return self.levels[-1]
+
+
+def _i64(path):
+    return np.fromfile(path, dtype=np.int64)
+
+
+def load_reference_dump(d: str) -> Problem:
+    """Reads the arrays the oracle harness wrote for the reference's solver."""
+    summ = {}
+    with open(os.path.join(d, "summary.txt")) as f:
+        for line in f:
+            k, *v = line.split()
+            summ[k] = v
+    nl = int(summ["nlevels"][0])
+    levels, transfers = [], []
+    dim = None
+    for l in range(nl):
+        p = os.path.join(d, f"L{l}_")
+        rowptr = _i64(p + "rowptr.i64")
+        n = rowptr.shape[0] - 1
+        coord = np.fromfile(p + "coord.f64")
+        dim = coord.shape[0] // n
+        levels.append(Level(n=n, B=1, rowptr=rowptr, col=_i64(p + "col.i64"),
+                            diag=_i64(p + "diag.i64"),
+                            val=np.fromfile(p + "val.f64"),
+                            dirichlet=_i64(p + "dirichlet.i64"),
+                            coord=coord.reshape(n, dim)))
+    for l in range(nl - 1):
+        p = os.path.join(d, f"T{l}_")
+        transfers.append(Transfer(c2f=_i64(p + "c2f.i64"),
+                                  zweier=_i64(p + "zweier.i64").reshape(-1, 3),
+                                  vierer=_i64(p + "vierer.i64").reshape(-1, 5),
+                                  achter=_i64(p + "achter.i64").reshape(-1, 9)))
+    info = {k: v for k, v in summ.items()}
+    return Problem(dim=dim, levels=levels, transfers=transfers,
+                   rhs=np.fromfile(os.path.join(d, "rhs.f64")), info=info)
+
+
+# ---------------------------------------------------------------- generator
+
+def _q1_local_stiffness(dim: int, h: float) -> np.ndarray:
+    """Q1 element stiffness of a cube of width h, unit coefficient, local node
+    order lexicographic (x fastest): tensor products of the 1D mass
+    [[1/3,1/6],[1/6,1/3]]*h and stiffness [[1,-1],[-1,1]]/h."""
+    m = np.array([[1.0 / 3.0, 1.0 / 6.0], [1.0 / 6.0, 1.0 / 3.0]]) * h
+    s = np.array([[1.0, -1.0], [-1.0, 1.0]]) / h
+    if dim == 2:
+        # local index = ey*2 + ex  -> kron(y, x)
+        return np.kron(m, s) + np.kron(s, m)
+    return (np.kron(np.kron(m, m), s) + np.kron(np.kron(m, s), m)
+            + np.kron(np.kron(s, m), m))
+
+
+def kappa_pyramid(dim: int, fine: np.ndarray, levels: int) -> List[np.ndarray]:
+    """Per-level cell coefficients, finest last; a coarse cell takes the mean of
+    its 2^dim children summed in lexicographic child order (z, y, x)."""
+    out = [fine]
+    cur = fine
+    for _ in range(levels - 1):
+        if dim == 3:
+            s = np.zeros(tuple(d // 2 for d in cur.shape))
+            for a in range(2):
+                for b in range(2):
+                    for e in range(2):
+                        s = s + cur[a::2, b::2, e::2]
+            cur = s / 8.0
+        else:
+            s = np.zeros(tuple(d // 2 for d in cur.shape))
+            for b in range(2):
+                for e in range(2):
+                    s = s + cur[b::2, e::2]
+            cur = s / 4.0
+        out.append(cur)
+    return out[::-1]
+
+
+def _assemble_level(dim: int, N: int, kappa: np.ndarray) -> Level:
+    """Assembles -div(kappa grad u) with Q1 on N^dim uniform cells of the unit
+    square/cube, lexicographic node numbering, full neighbour stencil with
+    columns sorted ascending, strong zero Dirichlet on the whole boundary
+    (SparseBlockMatrix::dirichlet: row and column zeroed, diagonal 1,
+    LinAlg/sparseblockmatrix.xx:205-218)."""
+    import scipy.sparse as sp
+    h = 1.0 / N
+    n1 = N + 1
+    K = _q1_local_stiffness(dim, h)
+    nloc = 2 ** dim
+    if dim == 3:
+        k, j, i = np.meshgrid(np.arange(N), np.arange(N), np.arange(N), indexing="ij")
+        base = ((k * n1 + j) * n1 + i).ravel()
+        offs = np.array([(a * n1 + b) * n1 + e for a in range(2) for b in range(2)
+                         for e in range(2)])
+    else:
+        j, i = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+        base = (j * n1 + i).ravel()
+        offs = np.array([b * n1 + e for b in range(2) for e in range(2)])
+    nodes = base[:, None] + offs[None, :]                 # [ncell, nloc]
+    kap = kappa.ravel()
+    rows = np.repeat(nodes, nloc, axis=1).ravel()
+    cols = np.tile(nodes, (1, nloc)).ravel()
+    vals = (kap[:, None] * K.ravel()[None, :]).ravel()
+    n = n1 ** dim
+    A = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+    A.sum_duplicates()
+    A.sort_indices()
+    # Dirichlet: boundary nodes
+    idx = np.arange(n)
+    coords = [(idx // n1 ** d) % n1 for d in range(dim)]
+    onb = np.zeros(n, dtype=bool)
+    for c in coords:
+        onb |= (c == 0) | (c == N)
+    rowptr = A.indptr.astype(np.int64)
+    col = A.indices.astype(np.int64)
+    val = A.data.astype(np.float64).copy()
+    rowidx = np.repeat(np.arange(n), np.diff(rowptr))
+    zero = onb[rowidx] | onb[col]
+    val[zero] = 0.0
+    isdiag = rowidx == col
+    val[isdiag & onb[rowidx]] = 1.0
+    diag = np.nonzero(isdiag)[0].astype(np.int64)
+    coord = np.stack([c * h for c in coords], axis=1).astype(np.float64)
+    return Level(n=n, B=1, rowptr=rowptr, col=col, diag=diag, val=val,
+                 dirichlet=np.nonzero(onb)[0].astype(np.int64), coord=coord)
+
+
+def _structured_transfer(dim: int, Nc: int) -> Transfer:
+    """Nested Q1 transfer maps between Nc and 2*Nc cells per dimension in
+    lexicographic numbering: a fine node with m odd coordinates has 2^m coarse
+    parents (c2f for m = 0, zweier/vierer/achter for m = 1, 2, 3)."""
+    nf1, nc1 = 2 * Nc + 1, Nc + 1
+    fidx = np.arange(nf1 ** dim)
+    fc = [(fidx // nf1 ** d) % nf1 for d in range(dim)]
+    odd = np.stack([c % 2 for c in fc], axis=1)
+    nodd = odd.sum(axis=1)
+
+    def cid(cs):
+        r = np.zeros_like(cs[0])
+        for d in reversed(range(dim)):
+            r = r * nc1 + cs[d]
+        return r
+
+    c2f = np.empty(nc1 ** dim, dtype=np.int64)
+    m0 = nodd == 0
+    c2f[cid([c[m0] // 2 for c in fc])] = fidx[m0]
+    maps = []
+    for m in (1, 2, 3):
+        sel = nodd == m
+        f = fidx[sel]
+        parents = []
+        if f.size:
+            lo = [c[sel] // 2 for c in fc]
+            od = [o for o in odd[sel].T]
+            # enumerate 2^m parent combinations over the odd coordinates
+            for bits in range(2 ** dim):
+                take = np.ones(f.size, dtype=bool)
+                cs = []
+                for d in range(dim):
+                    bd = (bits >> d) & 1
+                    take &= (bd == 0) | (od[d] == 1)
+                    cs.append(lo[d] + bd * od[d])
+                parents.append((take, cid(cs)))
+            par = np.stack([p for t, p in parents if True], axis=1)
+            tk = np.stack([t for t, p in parents], axis=1)
+            par = par[tk].reshape(f.size, 2 ** m)
+            maps.append(np.concatenate([f[:, None], par], axis=1).astype(np.int64))
+        else:
+            maps.append(np.zeros((0, 1 + 2 ** m), dtype=np.int64))
+    return Transfer(c2f=c2f, zweier=maps[0], vierer=maps[1], achter=maps[2])
+
+
+def structured_problem(dim: int, coarse: int, refine: int,
+                       kappa: Optional[np.ndarray] = None,
+                       rhs: Optional[np.ndarray] = None) -> Problem:
+    """The reference's multilevel system for -div(kappa grad u) = f on the unit
+    square/cube built from coarse^dim cells refined `refine` times, with the
+    reference's default patchdepth 1: `refine` multigrid levels, the coarsest
+    having 2*coarse cells per dimension (Mesh/hierarchicalmesh.cc:126-148,
+    Mesh/meshagent.cc:83). kappa: per finest cell (lexicographic, x fastest),
+    default 1. rhs: per finest node (lexicographic), default 1; zeroed at
+    Dirichlet nodes."""
+    Nf = coarse << refine
+    if kappa is None:
+        kappa = np.ones((Nf,) * dim)
+    kappa = np.asarray(kappa, dtype=np.float64).reshape((Nf,) * dim)
+    nlev = refine
+    kap = kappa_pyramid(dim, kappa, nlev)
+    levels = []
+    for l in range(nlev):
+        N = (2 * coarse) << l
+        levels.append(_assemble_level(dim, N, kap[l]))
+    transfers = [_structured_transfer(dim, (2 * coarse) << l) for l in range(nlev - 1)]
+    nfin = levels[-1].n
+    b = np.ones(nfin) if rhs is None else np.asarray(rhs, dtype=np.float64).copy()
+    b[levels[-1].dirichlet] = 0.0
+    return Problem(dim=dim, levels=levels, transfers=transfers, rhs=b,
+                   info={"generator": "structured", "coarse": coarse,
+                         "refine": refine})
+
+
+def seeded_inputs(dim: int, coarse: int, refine: int, kappa_seed: int = 1001,
+                  rhs_seed: int = 1002, sigma: float = 1.0):
+    """Seeded synthetic coefficient and load: kappa = exp(N(0, sigma)) per finest
+    cell, f ~ U[-1, 1] per finest node (numpy PCG64 default_rng)."""
+    Nf = coarse << refine
+    kappa = np.exp(np.random.default_rng(kappa_seed).normal(0.0, sigma, size=Nf ** dim))
+    rhs = np.random.default_rng(rhs_seed).uniform(-1.0, 1.0, size=(Nf + 1) ** dim)
+    return kappa, rhs

@@ -1,0 +1,676 @@
+/*
+ * ORACLE - TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C, FP64, single-threaded restatement of the reference's CPU linear-solve
+ * path (Gascoigne: StdMultiLevelSolver::Gmres + LinearMg/mgstep, damped-Jacobi
+ * smoothing, MgInterpolatorMatrix transfers, strong Dirichlet zeroing, CGInfo).
+ * Only the tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
+ * it, and only as the checker. The product path never calls it.
+ *
+ * Parity is pinned against the reference itself: tests run this restatement and
+ * the compiled reference (oracle/_ref/ref_harness, built from the reference's own
+ * sources by oracle/ref/Makefile) on identical per-level matrices and transfer
+ * maps dumped by that harness, and compare iteration counts and solutions.
+ *
+ * Every function cites the reference file:line it restates. Arithmetic order
+ * follows the reference where it matters for rounding (sequential per-row
+ * accumulation of FMatrixBlock::cadd, sequential dot products).
+ *
+ * Conventions: level 0 is the coarsest, as in the reference's solver indexing
+ * (Solver/stdmultilevelsolver.cc:224-231). Vectors are node-major interleaved
+ * (CompVector, Common/compvector.h:98-113): entry (node i, comp c) at i*B+c.
+ * Matrix blocks are row-major B x B (NodeMatrix::value, LinAlg/nodematrix.h:44-48).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OR_MAXB 8
+
+typedef struct
+{
+  int64_t n;              /* block rows */
+  int B;                  /* block size (ncomp) */
+  const int64_t* rowptr;  /* n+1 */
+  const int64_t* col;     /* nnzb */
+  const int64_t* diag;    /* n, position of the diagonal block in row i */
+  const double* val;      /* nnzb*B*B, row-major blocks */
+  int64_t ndir;           /* Dirichlet nodes */
+  const int64_t* dir;     /* node indices */
+  int dircomp_mask;       /* bit c set: component c is Dirichlet (all colours) */
+} or_level;
+
+/* Transfer level l (coarse) <-> l+1 (fine) in the form MgInterpolatorMatrix
+ * builds it (Discretization/Q1/mginterpolatormatrix.cc:34-121): both directions
+ * as CSR with columns sorted ascending (SparseStructure keeps std::set rows). */
+typedef struct
+{
+  int64_t ncoarse, nfine;
+  int64_t *r_ptr, *r_col; /* restriction: coarse row -> fine columns */
+  double* r_w;
+  int64_t *p_ptr, *p_col; /* prolongation: fine row -> coarse columns */
+  double* p_w;
+} or_transfer;
+
+typedef struct
+{
+  int nlevels;
+  or_level* L;            /* nlevels */
+  or_transfer* T;         /* nlevels-1 */
+  /* StdSolver / SolverData keys (Solver/solverdata.cc:41-55) */
+  int iterpre, iterpost, iterexact;
+  double omega;
+  /* StdMultiLevelSolverData keys (Solver/stdmultilevelsolverdata.cc:88-100) */
+  double mgomega;
+  char mgtype;            /* 'V', 'W' or 'F' */
+  /* work vectors per level: u, b, v of mgstep and the smoother's h */
+  double **u, **b, **v;
+} or_mg;
+
+/* ---------------------------------------------------------------- vectors */
+
+/* nvector::operator* (Common/nvector.h:332-343): sequential sum */
+double
+or_dot(int64_t n, const double* x, const double* y)
+{
+  double d = 0.0;
+  for (int64_t i = 0; i < n; ++i)
+    d += x[i] * y[i];
+  return d;
+}
+
+/* nvector::norm: sqrt of the sequential sum of squares */
+double
+or_norm(int64_t n, const double* x)
+{
+  return sqrt(or_dot(n, x, x));
+}
+
+/* ------------------------------------------------------------- block ops */
+
+/* SparseBlockMatrix<B>::vmult (LinAlg/sparseblockmatrix.xx:378-392) with
+ * FMatrixBlock::cadd (LinAlg/fmatrixblock.h:110-122): y(i) += s * (A_ij x(j)),
+ * blocks visited in stencil order, each block row sum formed first. */
+void
+or_bsr_vmult(const or_level* A, double* y, const double* x, double s)
+{
+  const int B = A->B;
+  for (int64_t i = 0; i < A->n; ++i) {
+    double* yi = y + i * B;
+    for (int64_t pos = A->rowptr[i]; pos < A->rowptr[i + 1]; ++pos) {
+      const double* m = A->val + pos * B * B;
+      const double* xj = x + A->col[pos] * B;
+      for (int r = 0; r < B; ++r) {
+        double sum = 0.0;
+        for (int c = 0; c < B; ++c)
+          sum += m[r * B + c] * xj[c];
+        yi[r] += s * sum;
+      }
+    }
+  }
+}
+
+/* Transposed product y += s * A^T x, the operator SparseBlockMatrix::transpose
+ * (LinAlg/sparseblockmatrix.xx:478-491) followed by vmult applies. */
+void
+or_bsr_vmult_transpose(const or_level* A, double* y, const double* x, double s)
+{
+  const int B = A->B;
+  for (int64_t i = 0; i < A->n; ++i) {
+    const double* xi = x + i * B;
+    for (int64_t pos = A->rowptr[i]; pos < A->rowptr[i + 1]; ++pos) {
+      const double* m = A->val + pos * B * B;
+      double* yj = y + A->col[pos] * B;
+      for (int c = 0; c < B; ++c) {
+        double sum = 0.0;
+        for (int r = 0; r < B; ++r)
+          sum += m[r * B + c] * xi[r];
+        yj[c] += s * sum;
+      }
+    }
+  }
+}
+
+/* NodeMatrix::gauss_jordan (LinAlg/nodematrix.h:159-213), in place on a
+ * row-major N x N block. */
+void
+or_gauss_jordan(int N, double* a)
+{
+  int p[OR_MAXB];
+  double hv[OR_MAXB];
+  int i, j, k, r;
+  double max, hr;
+#define A_(i, j) a[(i) * N + (j)]
+  for (i = 0; i < N; i++)
+    p[i] = i;
+  for (j = 0; j < N; j++) {
+    max = fabs(A_(j, j));
+    r = j;
+    for (i = j + 1; i < N; i++) {
+      if (fabs(A_(i, j)) > max) {
+        max = fabs(A_(i, j));
+        r = i;
+      }
+    }
+    if (r > j) {
+      for (k = 0; k < N; k++) {
+        hr = A_(j, k);
+        A_(j, k) = A_(r, k);
+        A_(r, k) = hr;
+      }
+      i = p[j];
+      p[j] = p[r];
+      p[r] = i;
+    }
+    hr = 1. / A_(j, j);
+    A_(j, j) = hr;
+    for (k = 0; k < N; k++) {
+      if (k == j)
+        continue;
+      for (i = 0; i < N; i++) {
+        if (i == j)
+          continue;
+        A_(i, k) -= A_(i, j) * A_(j, k) * hr;
+      }
+    }
+    for (i = 0; i < N; i++) {
+      A_(i, j) *= hr;
+      A_(j, i) *= -hr;
+    }
+    A_(j, j) = hr;
+  }
+  for (i = 0; i < N; i++) {
+    for (k = 0; k < N; k++)
+      hv[p[k]] = A_(i, k);
+    for (k = 0; k < N; k++)
+      A_(i, k) = hv[k];
+  }
+#undef A_
+}
+
+/* SparseBlockMatrix::Jacobi (LinAlg/sparseblockmatrix.xx:47-56): each node's
+ * diagonal block is inverted (gauss_jordan) and applied in place with
+ * FMatrixBlock::vmult (LinAlg/fmatrixblock.h:192-218). */
+void
+or_jacobi(const or_level* A, double* h)
+{
+  const int B = A->B;
+  double d[OR_MAXB * OR_MAXB], t[OR_MAXB];
+  for (int64_t i = 0; i < A->n; ++i) {
+    memcpy(d, A->val + A->diag[i] * B * B, sizeof(double) * B * B);
+    or_gauss_jordan(B, d);
+    double* hi = h + i * B;
+    for (int c = 0; c < B; ++c)
+      t[c] = hi[c];
+    for (int r = 0; r < B; ++r) {
+      hi[r] = 0.0;
+      for (int c = 0; c < B; ++c)
+        hi[r] += d[r * B + c] * t[c];
+    }
+  }
+}
+
+/* Inverse diagonal blocks for all nodes (the per-assembly form of the above). */
+void
+or_blockdiag_inverse(const or_level* A, double* out)
+{
+  const int B = A->B;
+  for (int64_t i = 0; i < A->n; ++i) {
+    memcpy(out + i * B * B, A->val + A->diag[i] * B * B, sizeof(double) * B * B);
+    or_gauss_jordan(B, out + i * B * B);
+  }
+}
+
+/* CGDisc::StrongDirichletVectorZero (DofHandler/cgdisc.h:1162-1179) */
+void
+or_dirichlet_zero(const or_level* A, double* u)
+{
+  for (int64_t k = 0; k < A->ndir; ++k)
+    for (int c = 0; c < A->B; ++c)
+      if (A->dircomp_mask & (1 << c))
+        u[A->dir[k] * A->B + c] = 0.0;
+}
+
+/* ---------------------------------------------------------- transfers */
+
+static int
+cmp_i64(const void* a, const void* b)
+{
+  int64_t x = *(const int64_t*)a, y = *(const int64_t*)b;
+  return (x > y) - (x < y);
+}
+
+/* MgInterpolatorMatrix::BasicInit (Discretization/Q1/mginterpolatormatrix.cc:
+ * 34-121) from the GascoigneMeshTransfer maps: c2f[coarse] = fine; zweier rows
+ * [fine, 2 coarse], vierer [fine, 4 coarse], achter [fine, 8 coarse]. A fine
+ * node's weight is 1/2, 1/4, 1/8 by the map it is in, else 1. */
+int
+or_transfer_build(or_transfer* T, int64_t ncoarse, const int64_t* c2f,
+                  int64_t nz, const int64_t* zweier, int64_t nv,
+                  const int64_t* vierer, int64_t na, const int64_t* achter)
+{
+  int64_t nfine = -1;
+  for (int64_t i = 0; i < ncoarse; ++i)
+    nfine = c2f[i] > nfine ? c2f[i] : nfine;
+  for (int64_t i = 0; i < nz; ++i)
+    nfine = zweier[3 * i] > nfine ? zweier[3 * i] : nfine;
+  for (int64_t i = 0; i < nv; ++i)
+    nfine = vierer[5 * i] > nfine ? vierer[5 * i] : nfine;
+  for (int64_t i = 0; i < na; ++i)
+    nfine = achter[9 * i] > nfine ? achter[9 * i] : nfine;
+  nfine++;
+  T->ncoarse = ncoarse;
+  T->nfine = nfine;
+  int64_t nent = ncoarse + 2 * nz + 4 * nv + 8 * na;
+  double* wfine = (double*)calloc(nfine, sizeof(double));
+  int64_t* cntf = (int64_t*)calloc(nfine + 1, sizeof(int64_t));
+  int64_t* cntc = (int64_t*)calloc(ncoarse + 1, sizeof(int64_t));
+  int64_t* pairs_f = (int64_t*)malloc(sizeof(int64_t) * nent); /* fine */
+  int64_t* pairs_c = (int64_t*)malloc(sizeof(int64_t) * nent); /* coarse */
+  if (!wfine || !cntf || !cntc || !pairs_f || !pairs_c)
+    return -1;
+  int64_t e = 0;
+  for (int64_t i = 0; i < ncoarse; ++i) {
+    pairs_f[e] = c2f[i];
+    pairs_c[e++] = i;
+    wfine[c2f[i]] = 1.0;
+  }
+  for (int64_t i = 0; i < nz; ++i)
+    for (int q = 0; q < 2; ++q) {
+      pairs_f[e] = zweier[3 * i];
+      pairs_c[e++] = zweier[3 * i + 1 + q];
+      wfine[zweier[3 * i]] = 0.5;
+    }
+  for (int64_t i = 0; i < nv; ++i)
+    for (int q = 0; q < 4; ++q) {
+      pairs_f[e] = vierer[5 * i];
+      pairs_c[e++] = vierer[5 * i + 1 + q];
+      wfine[vierer[5 * i]] = 0.25;
+    }
+  for (int64_t i = 0; i < na; ++i)
+    for (int q = 0; q < 8; ++q) {
+      pairs_f[e] = achter[9 * i];
+      pairs_c[e++] = achter[9 * i + 1 + q];
+      wfine[achter[9 * i]] = 0.125;
+    }
+  for (int64_t k = 0; k < nent; ++k) {
+    cntf[pairs_f[k] + 1]++;
+    cntc[pairs_c[k] + 1]++;
+  }
+  for (int64_t i = 0; i < nfine; ++i)
+    cntf[i + 1] += cntf[i];
+  for (int64_t i = 0; i < ncoarse; ++i)
+    cntc[i + 1] += cntc[i];
+  T->p_ptr = (int64_t*)malloc(sizeof(int64_t) * (nfine + 1));
+  T->r_ptr = (int64_t*)malloc(sizeof(int64_t) * (ncoarse + 1));
+  T->p_col = (int64_t*)malloc(sizeof(int64_t) * nent);
+  T->r_col = (int64_t*)malloc(sizeof(int64_t) * nent);
+  T->p_w = (double*)malloc(sizeof(double) * nent);
+  T->r_w = (double*)malloc(sizeof(double) * nent);
+  memcpy(T->p_ptr, cntf, sizeof(int64_t) * (nfine + 1));
+  memcpy(T->r_ptr, cntc, sizeof(int64_t) * (ncoarse + 1));
+  for (int64_t k = 0; k < nent; ++k) {
+    T->p_col[cntf[pairs_f[k]]++] = pairs_c[k];
+    T->r_col[cntc[pairs_c[k]]++] = pairs_f[k];
+  }
+  for (int64_t i = 0; i < nfine; ++i) {
+    qsort(T->p_col + T->p_ptr[i], T->p_ptr[i + 1] - T->p_ptr[i],
+          sizeof(int64_t), cmp_i64);
+    for (int64_t k = T->p_ptr[i]; k < T->p_ptr[i + 1]; ++k)
+      T->p_w[k] = wfine[i];
+  }
+  for (int64_t i = 0; i < ncoarse; ++i) {
+    qsort(T->r_col + T->r_ptr[i], T->r_ptr[i + 1] - T->r_ptr[i],
+          sizeof(int64_t), cmp_i64);
+    for (int64_t k = T->r_ptr[i]; k < T->r_ptr[i + 1]; ++k)
+      T->r_w[k] = wfine[T->r_col[k]];
+  }
+  free(wfine);
+  free(cntf);
+  free(cntc);
+  free(pairs_f);
+  free(pairs_c);
+  return 0;
+}
+
+void
+or_transfer_free(or_transfer* T)
+{
+  free(T->p_ptr);
+  free(T->p_col);
+  free(T->p_w);
+  free(T->r_ptr);
+  free(T->r_col);
+  free(T->r_w);
+  memset(T, 0, sizeof(*T));
+}
+
+/* MgInterpolatorMatrix::restrict_zero (mginterpolatormatrix.cc:123-133) */
+void
+or_restrict_zero(const or_transfer* T, int B, double* uL, const double* ul)
+{
+  for (int64_t i = 0; i < T->ncoarse; ++i) {
+    for (int c = 0; c < B; ++c)
+      uL[i * B + c] = 0.0;
+    for (int64_t k = T->r_ptr[i]; k < T->r_ptr[i + 1]; ++k)
+      for (int c = 0; c < B; ++c)
+        uL[i * B + c] += T->r_w[k] * ul[T->r_col[k] * B + c];
+  }
+}
+
+/* MgInterpolatorMatrix::prolongate_add (mginterpolatormatrix.cc:137-147) */
+void
+or_prolongate_add(const or_transfer* T, int B, double* ul, const double* uL)
+{
+  for (int64_t i = 0; i < T->nfine; ++i)
+    for (int64_t k = T->p_ptr[i]; k < T->p_ptr[i + 1]; ++k)
+      for (int c = 0; c < B; ++c)
+        ul[i * B + c] += T->p_w[k] * uL[T->p_col[k] * B + c];
+}
+
+/* ---------------------------------------------------------- multigrid */
+
+static int64_t
+ndof(const or_mg* M, int l)
+{
+  return M->L[l].n * M->L[l].B;
+}
+
+or_mg*
+or_mg_create(int nlevels, or_level* L, or_transfer* T, int iterpre,
+             int iterpost, int iterexact, double omega, double mgomega,
+             char mgtype)
+{
+  or_mg* M = (or_mg*)calloc(1, sizeof(or_mg));
+  M->nlevels = nlevels;
+  M->L = L;
+  M->T = T;
+  M->iterpre = iterpre;
+  M->iterpost = iterpost;
+  M->iterexact = iterexact;
+  M->omega = omega;
+  M->mgomega = mgomega;
+  M->mgtype = mgtype;
+  M->u = (double**)calloc(nlevels, sizeof(double*));
+  M->b = (double**)calloc(nlevels, sizeof(double*));
+  M->v = (double**)calloc(nlevels, sizeof(double*));
+  for (int l = 0; l < nlevels; ++l) {
+    M->u[l] = (double*)calloc(ndof(M, l), sizeof(double));
+    M->b[l] = (double*)calloc(ndof(M, l), sizeof(double));
+    M->v[l] = (double*)calloc(ndof(M, l), sizeof(double));
+  }
+  return M;
+}
+
+void
+or_mg_free(or_mg* M)
+{
+  for (int l = 0; l < M->nlevels; ++l) {
+    free(M->u[l]);
+    free(M->b[l]);
+    free(M->v[l]);
+  }
+  free(M->u);
+  free(M->b);
+  free(M->v);
+  free(M);
+}
+
+/* StdSolver::MatrixResidual (Solver/stdsolver.cc:783-791): y = b - A x */
+void
+or_matrix_residual(const or_level* A, double* y, const double* x,
+                   const double* b)
+{
+  memcpy(y, b, sizeof(double) * A->n * A->B);
+  or_bsr_vmult(A, y, x, -1.0);
+}
+
+/* StdSolver::smooth with linear_smooth = jacobi (Solver/stdsolver.cc:951-986):
+ * h = y - A x; h = D^-1 h; x += omega h. No pressure filter. */
+void
+or_smooth(const or_mg* M, int l, int niter, double* x, const double* y,
+          double* h)
+{
+  const or_level* A = &M->L[l];
+  const int64_t n = ndof(M, l);
+  for (int it = 0; it < niter; ++it) {
+    or_matrix_residual(A, h, x, y);
+    or_jacobi(A, h);
+    for (int64_t i = 0; i < n; ++i)
+      x[i] += M->omega * h[i];
+  }
+}
+
+/* StdMultiLevelSolver::mgstep (Solver/stdmultilevelsolver.cc:462-531), the
+ * smoothing, residual and transfer steps in the reference's order. The final
+ * residual and norms only feed CGInfo and are kept for completeness. */
+static void
+or_mgstep(or_mg* M, double* res, double* rw, int l, int finelevel,
+          int coarselevel, char* p0, char p)
+{
+  double** u = M->u;
+  double** b = M->b;
+  double** v = M->v;
+  if (l == coarselevel) {
+    if (p == 'F')
+      *p0 = 'V';
+    or_smooth(M, l, M->iterexact, u[l], b[l], v[l]); /* smooth_exact */
+    if (l == finelevel) {
+      or_matrix_residual(&M->L[l], v[l], u[l], b[l]);
+      res[l] = or_norm(ndof(M, l), v[l]);
+    }
+  } else {
+    or_smooth(M, l, M->iterpre, u[l], b[l], v[l]);
+    or_matrix_residual(&M->L[l], v[l], u[l], b[l]);
+    or_restrict_zero(&M->T[l - 1], M->L[l].B, b[l - 1], v[l]);
+    /* HNDistribute: no hanging nodes on these meshes */
+    or_dirichlet_zero(&M->L[l - 1], b[l - 1]);
+    memset(u[l - 1], 0, sizeof(double) * ndof(M, l - 1));
+    int j = (*p0 == 'V') ? 1 : (*p0 == 'W') ? 2 : (*p0 == 'F') ? 3 : 0;
+    for (int i = 0; i < j; ++i)
+      or_mgstep(M, res, rw, l - 1, finelevel, coarselevel, p0, p);
+    if ((l == 0) && (p == 'F'))
+      *p0 = 'W';
+    rw[l] = or_norm(ndof(M, l - 1), u[l - 1]);
+    memset(v[l], 0, sizeof(double) * ndof(M, l));
+    /* HNAverage: none */
+    or_prolongate_add(&M->T[l - 1], M->L[l].B, v[l], u[l - 1]);
+    /* HNZero (coarse, fine): none */
+    or_dirichlet_zero(&M->L[l], v[l]);
+    for (int64_t i = 0; i < ndof(M, l); ++i)
+      u[l][i] += M->mgomega * v[l][i];
+    or_smooth(M, l, M->iterpost, u[l], b[l], v[l]);
+    or_matrix_residual(&M->L[l], v[l], u[l], b[l]);
+    res[l] = or_norm(ndof(M, l), v[l]);
+  }
+}
+
+/* StdMultiLevelSolver::precondition -> LinearMg (Solver/stdmultilevelsolver.cc:
+ * 940-952, 411-458) with prec_maxiter = 1: exactly one cycle, started from the
+ * current content of x, on right-hand side y. */
+void
+or_precondition(or_mg* M, double* x, const double* y)
+{
+  const int fl = M->nlevels - 1;
+  const int64_t n = ndof(M, fl);
+  double res[64], rw[64];
+  memcpy(M->b[fl], y, sizeof(double) * n);
+  memcpy(M->u[fl], x, sizeof(double) * n);
+  or_matrix_residual(&M->L[fl], M->v[fl], M->u[fl], M->b[fl]);
+  res[fl] = or_norm(n, M->v[fl]);
+  char p = M->mgtype;
+  char p0 = (p == 'F') ? 'W' : p;
+  or_mgstep(M, res, rw, fl, fl, 0, &p0, p);
+  memcpy(x, M->u[fl], sizeof(double) * n);
+}
+
+/* -------------------------------------------------------------- CGInfo */
+
+typedef struct
+{
+  double tol, globaltol, breaktol;
+  int miniter, maxiter;
+  int status; /* 0 waiting, 1 running, 2 converged, 3 too many, 4 exploded, 5 diverging */
+  double firstresidual, previousresidual, residual, aimedresidual;
+  int iteration;
+} or_cginfo;
+
+/* CGInfo::check (Common/cginfo.cc:201-255) */
+int
+or_cginfo_check(or_cginfo* I, double resi)
+{
+  double res = fabs(resi);
+  I->residual = res;
+  if (I->status != 1) {
+    I->firstresidual = res;
+    I->previousresidual = res;
+    I->aimedresidual = res * I->tol;
+    I->status = 1;
+  } else {
+    I->previousresidual = res;
+  }
+  double aim = I->aimedresidual > I->globaltol ? I->aimedresidual : I->globaltol;
+  if (I->residual < aim)
+    I->status = 2;
+  else if (I->iteration >= I->maxiter)
+    I->status = 3;
+  else if (I->residual > I->breaktol)
+    I->status = 4;
+  /* "diverging" compares against previousresidual after it was overwritten
+   * with res in the running branch, so it can only fire on the first call,
+   * where the two are equal: it never fires. */
+  I->iteration++;
+  if (I->status == 1)
+    return 0;
+  if (I->iteration < I->miniter)
+    return 0;
+  return 1;
+}
+
+/* ---------------------------------------------------------------- GMRES */
+
+/* GMRES::solve with left preconditioning (LinAlg/gmres.cc:159-230),
+ * orthogonalization/reortho_test (:108-135), givens_rotation (:88-104),
+ * solution + backward (:234-259, Common/mult.h:130-141), as called by
+ * StdMultiLevelSolver::NewtonLinearSolve/Gmres (Solver/stdmultilevelsolver.cc:
+ * 646-689): x is zeroed first. Returns `reached` (1 when CGInfo stopped).
+ * hist (may be NULL) receives |gamma| per Arnoldi step, at most vmax entries. */
+int
+or_gmres_solve(or_mg* M, const double* b, double* x, int vmax, double tol,
+               double globaltol, int maxiter, int* out_iters, int* out_status,
+               double* out_first, double* out_last, double* hist)
+{
+  const int fl = M->nlevels - 1;
+  const or_level* A = &M->L[fl];
+  const int64_t n = ndof(M, fl);
+  double** mem = (double**)calloc(vmax + 1, sizeof(double*));
+  for (int i = 0; i <= vmax; ++i)
+    mem[i] = (double*)calloc(n, sizeof(double));
+  double* p = (double*)calloc(n, sizeof(double));
+  double* H = (double*)calloc((size_t)vmax * (vmax + 1), sizeof(double));
+  double* gamma = (double*)calloc(vmax + 1, sizeof(double));
+  double* ci = (double*)calloc(vmax, sizeof(double));
+  double* si = (double*)calloc(vmax, sizeof(double));
+#define Hc(j, i) H[(size_t)(j) * (vmax + 1) + (i)] /* column j = H[j][i] */
+  or_cginfo info = { tol, globaltol, 1e15, 0, maxiter, 0, 0, 1, 0, 0, 0 };
+  int reached = 0, dim = 0;
+
+  memset(x, 0, sizeof(double) * n);
+  /* residualgmres (Solver/stdsolver.cc:742-754): p = b - A x, Dirichlet zero */
+  memset(p, 0, sizeof(double) * n);
+  or_bsr_vmult(A, p, x, 1.0);
+  for (int64_t i = 0; i < n; ++i)
+    p[i] = -1.0 * p[i] + 1.0 * b[i];
+  or_dirichlet_zero(A, p);
+  or_precondition(M, mem[0], p);
+  double rho = sqrt(or_dot(n, mem[0], mem[0]));
+  if (rho == 0.0) {
+    reached = 1;
+    goto done;
+  }
+  gamma[0] = rho;
+  {
+    double s = 1.0 / rho;
+    for (int64_t i = 0; i < n; ++i)
+      mem[0][i] = s * mem[0][i];
+  }
+  while ((dim < vmax - 1) && !reached) {
+    dim++;
+    int last = dim - 1;
+    double* vv = mem[dim];
+    memset(p, 0, sizeof(double) * n); /* vmulteq */
+    or_bsr_vmult(A, p, mem[last], 1.0);
+    or_precondition(M, vv, p);
+    double* h = &Hc(last, 0);
+    double s;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int i = 0; i < dim; ++i) {
+        double d = or_dot(n, vv, mem[i]);
+        h[i] += d;
+        for (int64_t k = 0; k < n; ++k)
+          vv[k] += -d * mem[i][k];
+      }
+      h[dim] = sqrt(or_dot(n, vv, vv));
+      s = h[dim];
+      double oldnorm = sqrt(or_dot(n, vv, vv));
+      double newnorm = oldnorm + 1.e-3 * s;
+      if (pass == 1 || oldnorm != newnorm)
+        break;
+    }
+    {
+      double inv = 1.0 / s;
+      for (int64_t k = 0; k < n; ++k)
+        vv[k] = inv * vv[k];
+    }
+    /* givens_rotation(H[last], last) */
+    for (int i = 0; i < last; i++) {
+      double dummy = h[i];
+      h[i] = ci[i] * dummy + si[i] * h[i + 1];
+      h[i + 1] = -si[i] * dummy + ci[i] * h[i + 1];
+    }
+    double r = 1. / sqrt(h[last] * h[last] + h[last + 1] * h[last + 1]);
+    si[last] = h[last + 1] * r;
+    ci[last] = h[last] * r;
+    h[last] = ci[last] * h[last] + si[last] * h[last + 1];
+    gamma[last + 1] = -si[last] * gamma[last];
+    gamma[last] *= ci[last];
+    rho = fabs(gamma[dim]);
+    if (hist)
+      hist[dim - 1] = rho;
+    reached = or_cginfo_check(&info, rho);
+  }
+  /* solution: backward substitution on H1 (dim+1 x dim), x += sum h_i v_i */
+  {
+    double* hs = (double*)calloc(dim > 0 ? dim : 1, sizeof(double));
+    for (int i = dim - 1; i >= 0; i--) {
+      double s = gamma[i];
+      for (int j = i + 1; j < dim; j++)
+        s -= hs[j] * Hc(j, i);
+      hs[i] = s / Hc(i, i);
+    }
+    for (int i = 0; i < dim; i++)
+      for (int64_t k = 0; k < n; ++k)
+        x[k] += hs[i] * mem[i][k];
+    free(hs);
+  }
+done:
+  if (out_iters)
+    *out_iters = info.iteration;
+  if (out_status)
+    *out_status = info.status;
+  if (out_first)
+    *out_first = info.firstresidual;
+  if (out_last)
+    *out_last = info.residual;
+  for (int i = 0; i <= vmax; ++i)
+    free(mem[i]);
+  free(mem);
+  free(p);
+  free(H);
+  free(gamma);
+  free(ci);
+  free(si);
+#undef Hc
+  return reached;
+}

@@ -1,0 +1,231 @@
+"""ORACLE - TEST INFRASTRUCTURE ONLY.
+
+ctypes binding of the C restatement in ``gascoigne_oracle.c`` (built by
+``oracle/Makefile`` into ``oracle/_lib``) and a runner for the compiled reference
+harness (``oracle/_ref/ref_harness``, built from the reference's own sources by
+``oracle/ref/Makefile``). Only the tests, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg use this module, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libgascoigne_oracle.so")
+REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
+
+_P64 = C.POINTER(C.c_int64)
+_PD = C.POINTER(C.c_double)
+
+
+class _Level(C.Structure):
+    _fields_ = [("n", C.c_int64), ("B", C.c_int), ("rowptr", _P64), ("col", _P64),
+                ("diag", _P64), ("val", _PD), ("ndir", C.c_int64), ("dir", _P64),
+                ("dircomp_mask", C.c_int)]
+
+
+class _Transfer(C.Structure):
+    _fields_ = [("ncoarse", C.c_int64), ("nfine", C.c_int64),
+                ("r_ptr", _P64), ("r_col", _P64), ("r_w", _PD),
+                ("p_ptr", _P64), ("p_col", _P64), ("p_w", _PD)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-C", HERE, "_lib/libgascoigne_oracle.so"],
+                           check=True, capture_output=True)
+        L = C.CDLL(LIB_PATH)
+        L.or_mg_create.restype = C.c_void_p
+        L.or_mg_create.argtypes = [C.c_int, C.POINTER(_Level), C.POINTER(_Transfer),
+                                   C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                   C.c_char]
+        L.or_mg_free.argtypes = [C.c_void_p]
+        L.or_transfer_build.argtypes = [C.POINTER(_Transfer), C.c_int64, _P64,
+                                        C.c_int64, _P64, C.c_int64, _P64, C.c_int64,
+                                        _P64]
+        L.or_transfer_free.argtypes = [C.POINTER(_Transfer)]
+        L.or_gmres_solve.argtypes = [C.c_void_p, _PD, _PD, C.c_int, C.c_double,
+                                     C.c_double, C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), _PD, _PD, _PD]
+        L.or_precondition.argtypes = [C.c_void_p, _PD, _PD]
+        L.or_bsr_vmult.argtypes = [C.POINTER(_Level), _PD, _PD, C.c_double]
+        L.or_bsr_vmult_transpose.argtypes = [C.POINTER(_Level), _PD, _PD, C.c_double]
+        L.or_jacobi.argtypes = [C.POINTER(_Level), _PD]
+        L.or_blockdiag_inverse.argtypes = [C.POINTER(_Level), _PD]
+        L.or_smooth.argtypes = [C.c_void_p, C.c_int, C.c_int, _PD, _PD, _PD]
+        L.or_restrict_zero.argtypes = [C.POINTER(_Transfer), C.c_int, _PD, _PD]
+        L.or_prolongate_add.argtypes = [C.POINTER(_Transfer), C.c_int, _PD, _PD]
+        L.or_dirichlet_zero.argtypes = [C.POINTER(_Level), _PD]
+        L.or_matrix_residual.argtypes = [C.POINTER(_Level), _PD, _PD, _PD]
+        L.or_dot.restype = C.c_double
+        L.or_dot.argtypes = [C.c_int64, _PD, _PD]
+        _lib = L
+    return _lib
+
+
+def _p64(a):
+    return a.ctypes.data_as(_P64)
+
+
+def _pd(a):
+    return a.ctypes.data_as(_PD)
+
+
+class Oracle:
+    """FP64 CPU restatement of the reference's multilevel GMRES on a Problem."""
+
+    def __init__(self, prob, iterpre=2, iterpost=2, iterexact=10, omega=0.8,
+                 mgomega=1.0, mgtype="V"):
+        L = lib()
+        self.prob = prob
+        self._keep = []
+        nl = prob.nlevels
+        self.levels = (_Level * nl)()
+        for l, lv in enumerate(prob.levels):
+            arrs = [np.ascontiguousarray(a) for a in
+                    (lv.rowptr, lv.col, lv.diag, lv.val, lv.dirichlet)]
+            self._keep += arrs
+            rp, cl, dg, vl, dr = arrs
+            self.levels[l] = _Level(lv.n, lv.B, _p64(rp), _p64(cl), _p64(dg), _pd(vl),
+                                    dr.shape[0], _p64(dr), lv.dircomp_mask)
+        self.transfers = (_Transfer * max(nl - 1, 1))()
+        for l, t in enumerate(prob.transfers):
+            arrs = [np.ascontiguousarray(a, dtype=np.int64) for a in
+                    (t.c2f, t.zweier, t.vierer, t.achter)]
+            self._keep += arrs
+            c2f, z, v, a = arrs
+            rc = L.or_transfer_build(C.byref(self.transfers[l]), c2f.shape[0],
+                                     _p64(c2f), z.shape[0], _p64(z), v.shape[0],
+                                     _p64(v), a.shape[0], _p64(a))
+            if rc != 0:
+                raise MemoryError("or_transfer_build")
+        self.mg = L.or_mg_create(nl, self.levels, self.transfers, iterpre, iterpost,
+                                 iterexact, omega, mgomega, mgtype.encode()[:1])
+
+    def close(self):
+        if getattr(self, "mg", None):
+            L = lib()
+            L.or_mg_free(self.mg)
+            for l in range(self.prob.nlevels - 1):
+                L.or_transfer_free(C.byref(self.transfers[l]))
+            self.mg = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # single operations -----------------------------------------------------
+    def vmult(self, level, y, x, s=1.0):
+        y = np.array(y, dtype=np.float64)
+        lib().or_bsr_vmult(C.byref(self.levels[level]), _pd(y),
+                           _pd(np.ascontiguousarray(x, dtype=np.float64)), s)
+        return y
+
+    def vmult_transpose(self, level, y, x, s=1.0):
+        y = np.array(y, dtype=np.float64)
+        lib().or_bsr_vmult_transpose(C.byref(self.levels[level]), _pd(y),
+                                     _pd(np.ascontiguousarray(x, dtype=np.float64)), s)
+        return y
+
+    def blockdiag_inverse(self, level):
+        lv = self.prob.levels[level]
+        out = np.zeros(lv.n * lv.B * lv.B)
+        lib().or_blockdiag_inverse(C.byref(self.levels[level]), _pd(out))
+        return out
+
+    def smooth(self, level, niter, x, y):
+        x = np.array(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        h = np.zeros_like(x)
+        lib().or_smooth(self.mg, level, niter, _pd(x), _pd(y), _pd(h))
+        return x
+
+    def restrict_zero(self, level, fine):
+        B = self.prob.levels[level].B
+        out = np.zeros(self.prob.levels[level].n * B)
+        lib().or_restrict_zero(C.byref(self.transfers[level]), B, _pd(out),
+                               _pd(np.ascontiguousarray(fine, dtype=np.float64)))
+        return out
+
+    def prolongate_add(self, level, fine, coarse):
+        B = self.prob.levels[level].B
+        fine = np.array(fine, dtype=np.float64)
+        lib().or_prolongate_add(C.byref(self.transfers[level]), B, _pd(fine),
+                                _pd(np.ascontiguousarray(coarse, dtype=np.float64)))
+        return fine
+
+    def dirichlet_zero(self, level, u):
+        u = np.array(u, dtype=np.float64)
+        lib().or_dirichlet_zero(C.byref(self.levels[level]), _pd(u))
+        return u
+
+    def matrix_residual(self, level, x, b):
+        y = np.zeros_like(np.asarray(b, dtype=np.float64))
+        lib().or_matrix_residual(C.byref(self.levels[level]), _pd(y),
+                                 _pd(np.ascontiguousarray(x, dtype=np.float64)),
+                                 _pd(np.ascontiguousarray(b, dtype=np.float64)))
+        return y
+
+    def precondition(self, x, y):
+        x = np.array(x, dtype=np.float64)
+        lib().or_precondition(self.mg, _pd(x),
+                              _pd(np.ascontiguousarray(y, dtype=np.float64)))
+        return x
+
+    def gmres(self, b=None, vmax=21, tol=1e-8, globaltol=1e-16, maxiter=100):
+        b = np.ascontiguousarray(self.prob.rhs if b is None else b, dtype=np.float64)
+        x = np.zeros_like(b)
+        it, st = C.c_int(), C.c_int()
+        f, r = C.c_double(), C.c_double()
+        hist = np.zeros(vmax)
+        reached = lib().or_gmres_solve(self.mg, _pd(b), _pd(x), vmax, tol, globaltol,
+                                       maxiter, C.byref(it), C.byref(st), C.byref(f),
+                                       C.byref(r), _pd(hist))
+        status = {0: "waiting", 1: "running", 2: "converged", 3: "too many iterations",
+                  4: "exploded", 5: "diverging"}[st.value]
+        return x, {"reached": reached, "iterations": it.value, "status": status,
+                   "firstresidual": f.value, "residual": r.value,
+                   "history": hist[:max(it.value, 0)]}
+
+
+def run_reference(out_dir=None, **kw):
+    """Runs the compiled reference harness; returns (out_dir, summary dict)."""
+    if not os.path.exists(REF_HARNESS):
+        raise FileNotFoundError(REF_HARNESS)
+    if out_dir is None:
+        out_dir = tempfile.mkdtemp(prefix="gb_ref_")
+    args = [REF_HARNESS, f"out={out_dir}"] + [f"{k}={v}" for k, v in kw.items()]
+    env = dict(os.environ)
+    subprocess.run(args, check=True, capture_output=True, env=env)
+    summ = {}
+    with open(os.path.join(out_dir, "summary.txt")) as f:
+        for line in f:
+            k, *v = line.split()
+            summ[k] = v
+    return out_dir, summ
+
+
+def write_inputs(d, kappa=None, rhs=None):
+    """Writes kappa/rhs arrays for the harness; returns harness keyword args."""
+    kw = {}
+    if kappa is not None:
+        p = os.path.join(d, "kappa_in.f64")
+        np.ascontiguousarray(kappa, dtype=np.float64).tofile(p)
+        kw["kappa"] = p
+    if rhs is not None:
+        p = os.path.join(d, "rhs_in.f64")
+        np.ascontiguousarray(rhs, dtype=np.float64).tofile(p)
+        kw["rhs"] = p
+    return kw

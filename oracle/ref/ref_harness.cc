@@ -1,0 +1,527 @@
+// Oracle harness (test infrastructure, never shipped): drives the reference's own
+// FP64 CPU multilevel solver on a seeded synthetic problem and writes what it did.
+//
+// It builds the problem through the reference's public classes only:
+//   MeshAgent (Mesh/meshagent.cc:361-404) on a generated unit square/cube .inp,
+//   StdMultiLevelSolver::ReInit/SetProblem/ReInitMatrix/AssembleMatrix/ComputeIlu
+//   (Solver/stdmultilevelsolver.cc:152-309,762-790), and
+//   StdMultiLevelSolver::NewtonLinearSolve -> Gmres -> GMRES::solve + LinearMg
+//   (Solver/stdmultilevelsolver.cc:646-689, LinAlg/gmres.cc:159-230).
+// The equation is -div(kappa grad u) = f with kappa piecewise constant per cell
+// (per finest cell from a file; a coarse cell takes the mean of its 2^dim
+// children, summed in lexicographic child order), assembled by the reference's
+// CGDisc with its own Q1 element integrator (HexGauss8 / QuadGauss4,
+// DofHandler/elementintegrator.h:215-222). Dirichlet data: u = 0 on the whole
+// boundary (colour 1). The right-hand side is a nodal vector read from a file
+// (lexicographic node order) and copied into the finest-level vector f, then
+// zeroed at Dirichlet nodes (StdSolver::SetBoundaryVectorZero).
+//
+// Usage: ref_harness key=value ...   (see parse() for the keys)
+// Output (directory out=): summary.txt, and with dump=1 raw little-endian arrays
+//   L<l>_rowptr.i64 L<l>_col.i64 L<l>_diag.i64 L<l>_val.f64 L<l>_coord.f64
+//   L<l>_dirichlet.i64   (level l = 0 coarsest, as the reference indexes solvers)
+//   T<l>_c2f.i64 T<l>_zweier.i64 T<l>_vierer.i64 T<l>_achter.i64
+//     (transfer between level l (coarse) and l+1 (fine); zweier rows are
+//      [fine, coarse0, coarse1], vierer [fine, 4 coarse], achter [fine, 8 coarse])
+//   rhs.f64 solution.f64 (finest level, reference node numbering)
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "cginfo.h"
+#include "columndiagstencil.h"
+#include "equation.h"
+#include "fmatrixblock.h"
+#include "functionalcontainer.h"
+#include "gascoignemeshtransfer.h"
+#include "meshagent.h"
+#include "paramfile.h"
+#include "problemcontainer.h"
+#include "problemdescriptorbase.h"
+#include "sparseblockmatrix.h"
+#include "stdmultilevelsolver.h"
+#include "stdsolver.h"
+#include "zerodirichletdata.h"
+
+using namespace Gascoigne;
+
+namespace {
+
+struct Config
+{
+  int dim = 3;
+  int coarse = 1; // coarse mesh cells per dimension (1 or 2)
+  int refine = 3; // global refinements
+  std::string kappa, rhs, out = ".";
+  int gmressize = 21, iterpre = 2, iterpost = 2, iterexact = 10;
+  double omega = 0.8, tol = 1e-8, globaltol = 1e-16, mgomega = 1.0;
+  int maxiter = 100, ndirect = 1, dump = 0, repeat = 1, patchdepth = 1;
+  std::string mgtype = "V";
+};
+
+// kappa per cell, one array per resolution N = coarse * 2^l (cells per dim),
+// lexicographic (x fastest).
+struct KappaPyramid
+{
+  int dim = 3;
+  std::map<int, std::vector<double>> byN;
+  double at(int N, double x, double y, double z) const
+  {
+    auto it = byN.find(N);
+    if (it == byN.end()) {
+      fprintf(stderr, "ref_harness: no kappa for resolution %d\n", N);
+      abort();
+    }
+    auto clampi = [N](double t) {
+      int i = static_cast<int>(std::floor(t * N));
+      return i < 0 ? 0 : (i >= N ? N - 1 : i);
+    };
+    long i = clampi(x), j = clampi(y), k = dim == 3 ? clampi(z) : 0;
+    return it->second[(k * N + j) * N + i];
+  }
+};
+KappaPyramid g_kappa;
+
+class DiffusionEquation : public virtual Equation
+{
+  mutable double kappa_ = 1.0;
+  int dim_;
+
+public:
+  explicit DiffusionEquation(int dim)
+    : dim_(dim)
+  {}
+  DiffusionEquation* createNew() const override
+  {
+    return new DiffusionEquation(dim_);
+  }
+  std::string GetName() const override { return "OracleDiffusion"; }
+  int GetNcomp() const override { return 1; }
+  // h = vol^(1/dim) is the cell width on these uniform meshes
+  // (ElementIntegrator::Matrix, DofHandler/elementintegrator.xx:369-379).
+  void point(double h, const FemFunction&, const Vertex2d& v) const override
+  {
+    int N = static_cast<int>(std::lround(1.0 / h));
+    kappa_ = g_kappa.at(N, v.x(), v.y(), 0.0);
+  }
+  void point(double h, const FemFunction&, const Vertex3d& v) const override
+  {
+    int N = static_cast<int>(std::lround(1.0 / h));
+    kappa_ = g_kappa.at(N, v.x(), v.y(), v.z());
+  }
+  void Form(VectorIterator b,
+            const FemFunction& U,
+            const TestFunction& N) const override
+  {
+    for (int i = 0; i < dim_; ++i)
+      b[0] += kappa_ * U[0][i + 1] * N[i + 1];
+  }
+  void Matrix(EntryMatrix& A,
+              const FemFunction&,
+              const TestFunction& M,
+              const TestFunction& N) const override
+  {
+    for (int i = 0; i < dim_; ++i)
+      A(0, 0) += kappa_ * M[i + 1] * N[i + 1];
+  }
+};
+
+class DiffusionProblem : public ProblemDescriptorBase
+{
+public:
+  void BasicInit(const ParamFile& pf, int dim)
+  {
+    GetParamFile() = pf;
+    GetEquationPointer() = new DiffusionEquation(dim);
+    GetDirichletDataPointer() = new ZeroDirichletData(pf);
+    ProblemDescriptorBase::BasicInit(pf);
+  }
+};
+
+Config
+parse(int argc, char** argv)
+{
+  Config c;
+  for (int a = 1; a < argc; ++a) {
+    std::string s = argv[a];
+    auto eq = s.find('=');
+    if (eq == std::string::npos) {
+      fprintf(stderr, "ref_harness: bad argument %s\n", s.c_str());
+      exit(2);
+    }
+    std::string k = s.substr(0, eq), v = s.substr(eq + 1);
+    if (k == "dim") c.dim = atoi(v.c_str());
+    else if (k == "coarse") c.coarse = atoi(v.c_str());
+    else if (k == "refine") c.refine = atoi(v.c_str());
+    else if (k == "kappa") c.kappa = v;
+    else if (k == "rhs") c.rhs = v;
+    else if (k == "out") c.out = v;
+    else if (k == "gmressize") c.gmressize = atoi(v.c_str());
+    else if (k == "iterpre") c.iterpre = atoi(v.c_str());
+    else if (k == "iterpost") c.iterpost = atoi(v.c_str());
+    else if (k == "iterexact") c.iterexact = atoi(v.c_str());
+    else if (k == "omega") c.omega = atof(v.c_str());
+    else if (k == "tol") c.tol = atof(v.c_str());
+    else if (k == "globaltol") c.globaltol = atof(v.c_str());
+    else if (k == "mgomega") c.mgomega = atof(v.c_str());
+    else if (k == "maxiter") c.maxiter = atoi(v.c_str());
+    else if (k == "ndirect") c.ndirect = atoi(v.c_str());
+    else if (k == "mgtype") c.mgtype = v;
+    else if (k == "dump") c.dump = atoi(v.c_str());
+    else if (k == "repeat") c.repeat = atoi(v.c_str());
+    else if (k == "patchdepth") c.patchdepth = atoi(v.c_str());
+    else {
+      fprintf(stderr, "ref_harness: unknown key %s\n", k.c_str());
+      exit(2);
+    }
+  }
+  return c;
+}
+
+std::vector<double>
+read_f64(const std::string& path, size_t n)
+{
+  std::vector<double> v(n);
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f || fread(v.data(), sizeof(double), n, f) != n) {
+    fprintf(stderr, "ref_harness: cannot read %zu doubles from %s\n", n,
+            path.c_str());
+    exit(2);
+  }
+  fclose(f);
+  return v;
+}
+
+template<class T>
+void
+write_raw(const std::string& path, const std::vector<T>& v)
+{
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) {
+    fprintf(stderr, "ref_harness: cannot write %s\n", path.c_str());
+    exit(2);
+  }
+  if (!v.empty())
+    fwrite(v.data(), sizeof(T), v.size(), f);
+  fclose(f);
+}
+
+void
+write_mesh(const Config& c, const std::string& path)
+{
+  // Unit square / cube split into coarse^dim cells, every boundary face colour 1,
+  // in the reference's .inp format (evaluation/examples/Elasticity3d/box.inp).
+  int m = c.coarse, np = m + 1;
+  std::ofstream o(path);
+  o.precision(17);
+  if (c.dim == 2) {
+    int nn = np * np, nc = m * m, nb = 4 * m;
+    o << nn << " " << nc + nb << " 0 0 0\n";
+    for (int j = 0; j < np; ++j)
+      for (int i = 0; i < np; ++i)
+        o << j * np + i << " " << double(i) / m << " " << double(j) / m
+          << " 0\n"; // 2D vertices are read as Vertex3d
+    int id = 0;
+    auto N = [np](int i, int j) { return j * np + i; };
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i)
+        o << id++ << " 0 quad " << N(i, j) << " " << N(i + 1, j) << " "
+          << N(i + 1, j + 1) << " " << N(i, j + 1) << "\n";
+    for (int i = 0; i < m; ++i) {
+      o << id++ << " 1 line " << N(i, 0) << " " << N(i + 1, 0) << "\n";
+      o << id++ << " 1 line " << N(i + 1, m) << " " << N(i, m) << "\n";
+      o << id++ << " 1 line " << N(0, i + 1) << " " << N(0, i) << "\n";
+      o << id++ << " 1 line " << N(m, i) << " " << N(m, i + 1) << "\n";
+    }
+  } else {
+    int nn = np * np * np, nc = m * m * m, nb = 6 * m * m;
+    o << nn << " " << nc + nb << " 0 0 0\n";
+    auto N = [np](int i, int j, int k) { return (k * np + j) * np + i; };
+    for (int k = 0; k < np; ++k)
+      for (int j = 0; j < np; ++j)
+        for (int i = 0; i < np; ++i)
+          o << N(i, j, k) << " " << double(i) / m << " " << double(j) / m << " "
+            << double(k) / m << "\n";
+    int id = 0;
+    for (int k = 0; k < m; ++k)
+      for (int j = 0; j < m; ++j)
+        for (int i = 0; i < m; ++i)
+          o << id++ << " 0 hex " << N(i, j, k) << " " << N(i + 1, j, k) << " "
+            << N(i + 1, j + 1, k) << " " << N(i, j + 1, k) << " "
+            << N(i, j, k + 1) << " " << N(i + 1, j, k + 1) << " "
+            << N(i + 1, j + 1, k + 1) << " " << N(i, j + 1, k + 1) << "\n";
+    for (int a = 0; a < m; ++a)
+      for (int b = 0; b < m; ++b) {
+        // z = 0, z = 1, y = 0, y = 1, x = 0, x = 1
+        o << id++ << " 1 quad " << N(a, b, 0) << " " << N(a, b + 1, 0) << " "
+          << N(a + 1, b + 1, 0) << " " << N(a + 1, b, 0) << "\n";
+        o << id++ << " 1 quad " << N(a, b, m) << " " << N(a + 1, b, m) << " "
+          << N(a + 1, b + 1, m) << " " << N(a, b + 1, m) << "\n";
+        o << id++ << " 1 quad " << N(a, 0, b) << " " << N(a + 1, 0, b) << " "
+          << N(a + 1, 0, b + 1) << " " << N(a, 0, b + 1) << "\n";
+        o << id++ << " 1 quad " << N(a, m, b) << " " << N(a, m, b + 1) << " "
+          << N(a + 1, m, b + 1) << " " << N(a + 1, m, b) << "\n";
+        o << id++ << " 1 quad " << N(0, a, b) << " " << N(0, a, b + 1) << " "
+          << N(0, a + 1, b + 1) << " " << N(0, a + 1, b) << "\n";
+        o << id++ << " 1 quad " << N(m, a, b) << " " << N(m, a + 1, b) << " "
+          << N(m, a + 1, b + 1) << " " << N(m, a, b + 1) << "\n";
+      }
+  }
+}
+
+void
+write_param(const Config& c, const std::string& path, const std::string& grid)
+{
+  std::ofstream o(path);
+  o.precision(17);
+  o << "//Block Mesh\n"
+    << "dimension " << c.dim << "\n"
+    << "prerefine " << c.refine << "\n"
+    << "patchdepth " << c.patchdepth << "\n"
+    << "gridname " << grid << "\n\n"
+    << "//Block BoundaryManager\n"
+    << "dirichlet 1 1\n"
+    << "dirichletcomp 1 1 0\n\n"
+    << "//Block MultiLevelSolver\n"
+    << "linearsolve gmres\n"
+    << "gmressize " << c.gmressize << "\n"
+    << "mgtype " << c.mgtype << "\n"
+    << "mgomega " << c.mgomega << "\n"
+    << "coarselevel 0\n\n"
+    << "//Block Solver\n"
+    << "matrixtype block\n"
+    << "discname CGQ1\n"
+    << "ndirect " << c.ndirect << "\n"
+    << "iterpre " << c.iterpre << "\n"
+    << "iterpost " << c.iterpost << "\n"
+    << "iterexact " << c.iterexact << "\n"
+    << "linear_smooth jacobi\n"
+    << "omega " << c.omega << "\n";
+}
+
+void
+build_kappa(const Config& c)
+{
+  g_kappa.dim = c.dim;
+  int Nf = c.coarse << c.refine;
+  size_t ncell = 1;
+  for (int d = 0; d < c.dim; ++d)
+    ncell *= Nf;
+  std::vector<double> fine = c.kappa.empty() ? std::vector<double>(ncell, 1.0)
+                                             : read_f64(c.kappa, ncell);
+  g_kappa.byN[Nf] = fine;
+  for (int N = Nf / 2; N >= c.coarse; N /= 2) {
+    const std::vector<double>& f = g_kappa.byN[2 * N];
+    int M = 2 * N;
+    std::vector<double> k(c.dim == 3 ? size_t(N) * N * N : size_t(N) * N);
+    int nz = c.dim == 3 ? N : 1;
+    for (int kk = 0; kk < nz; ++kk)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          double s = 0.0;
+          int dz = c.dim == 3 ? 2 : 1;
+          for (int a = 0; a < dz; ++a)
+            for (int b = 0; b < 2; ++b)
+              for (int e = 0; e < 2; ++e) {
+                size_t idx = c.dim == 3
+                               ? (size_t(2 * kk + a) * M + 2 * j + b) * M + 2 * i + e
+                               : size_t(2 * j + b) * M + 2 * i + e;
+                s += f[idx];
+              }
+          k[(size_t(kk) * N + j) * N + i] = s / (c.dim == 3 ? 8.0 : 4.0);
+        }
+    g_kappa.byN[N] = k;
+  }
+}
+
+} // namespace
+
+int
+main(int argc, char** argv)
+{
+  Config c = parse(argc, argv);
+  std::string grid = c.out + "/oracle_mesh.inp";
+  std::string pfile = c.out + "/oracle.param";
+  write_mesh(c, grid);
+  write_param(c, pfile, grid);
+  build_kappa(c);
+
+  ParamFile pf(pfile);
+  DiffusionProblem PD;
+  PD.BasicInit(pf, c.dim);
+  ProblemContainer PC;
+  PC.AddProblem("diffusion", &PD);
+  FunctionalContainer FC;
+
+  MeshAgent MA;
+  MA.BasicInit(pf);
+  StdMultiLevelSolver MLS;
+  MLS.BasicInit(&MA, pf, &PC, &FC);
+  MLS.ReInit();
+  MLS.SetProblem("diffusion");
+
+  Matrix A("A");
+  Vector u("u"), f("f");
+  MLS.ReInitMatrix(A);
+  MLS.ReInitVector(u);
+  MLS.ReInitVector(f);
+
+  auto t_as0 = std::chrono::steady_clock::now();
+  MLS.AssembleMatrix(A, u);
+  MLS.ComputeIlu(A, u);
+  auto t_as1 = std::chrono::steady_clock::now();
+
+  const int nl = MLS.nlevels();
+  const int Nf = c.coarse << c.refine;
+  StdSolver* S = MLS.GetSolver();
+  const GascoigneMesh* Mf = S->GetMesh();
+  const int nf = Mf->nnodes();
+  GlobalVector& F = S->GetGV(f);
+  {
+    size_t nlex = 1;
+    for (int d = 0; d < c.dim; ++d)
+      nlex *= Nf + 1;
+    std::vector<double> r = c.rhs.empty() ? std::vector<double>(nlex, 1.0)
+                                          : read_f64(c.rhs, nlex);
+    for (int i = 0; i < nf; ++i) {
+      long ix, iy, iz = 0;
+      if (c.dim == 3) {
+        const Vertex3d& v = Mf->vertex3d(i);
+        ix = std::lround(v.x() * Nf);
+        iy = std::lround(v.y() * Nf);
+        iz = std::lround(v.z() * Nf);
+      } else {
+        const Vertex2d& v = Mf->vertex2d(i);
+        ix = std::lround(v.x() * Nf);
+        iy = std::lround(v.y() * Nf);
+      }
+      F(i, 0) = r[(iz * (Nf + 1) + iy) * (Nf + 1) + ix];
+    }
+  }
+  S->SetBoundaryVectorZero(f);
+
+  std::vector<double> times;
+  CGInfo info(c.tol, c.globaltol, 0, c.maxiter, "Lin");
+  for (int rep = 0; rep < std::max(1, c.repeat); ++rep) {
+    info.reset();
+    auto t0 = std::chrono::steady_clock::now();
+    MLS.NewtonLinearSolve(A, u, f, info);
+    auto t1 = std::chrono::steady_clock::now();
+    times.push_back(std::chrono::duration<double>(t1 - t0).count());
+  }
+
+  // true relative residual ||f - A u|| / ||f|| with the reference's own vmult
+  Vector r("r");
+  MLS.ReInitVector(r);
+  S->residualgmres(A, r, u, f);
+  double rnorm = S->Norm(r), fnorm = S->Norm(f);
+
+  {
+    std::ofstream o(c.out + "/summary.txt");
+    o.precision(17);
+    o << "nlevels " << nl << "\n";
+    for (int l = 0; l < nl; ++l)
+      o << "nnodes_L" << l << " " << MLS.GetSolver(l)->GetMesh()->nnodes()
+        << "\n";
+    o << "iterations " << info.control().iteration() << "\n";
+    o << "status " << info.control().status() << "\n";
+    o << "firstresidual " << info.control().firstresidual() << "\n";
+    o << "residual " << info.control().residual() << "\n";
+    o << "true_rel_residual " << rnorm / fnorm << "\n";
+    o << "assemble_s "
+      << std::chrono::duration<double>(t_as1 - t_as0).count() << "\n";
+    o << "solve_s";
+    for (double t : times)
+      o << " " << t;
+    o << "\n";
+  }
+
+  if (c.dump) {
+    for (int l = 0; l < nl; ++l) {
+      StdSolver* SL = MLS.GetSolver(l);
+      const auto* M =
+        dynamic_cast<const SparseBlockMatrix<FMatrixBlock<1>>*>(&SL->GetMatrix(A));
+      if (!M) {
+        fprintf(stderr, "ref_harness: level %d is not a block matrix\n", l);
+        return 3;
+      }
+      const auto* ST = dynamic_cast<const ColumnDiagStencil*>(M->GetStencil());
+      const int n = ST->n();
+      std::vector<long> rowptr(n + 1), col(ST->nentries()), diag(n);
+      std::vector<double> val(ST->nentries());
+      for (int i = 0; i <= n; ++i)
+        rowptr[i] = ST->start(i);
+      for (size_t p = 0; p < ST->nentries(); ++p) {
+        col[p] = ST->col(p);
+        val[p] = (*M->mat(p))(0, 0);
+      }
+      for (int i = 0; i < n; ++i)
+        diag[i] = ST->diag(i);
+      std::string L = c.out + "/L" + std::to_string(l) + "_";
+      write_raw(L + "rowptr.i64", rowptr);
+      write_raw(L + "col.i64", col);
+      write_raw(L + "diag.i64", diag);
+      write_raw(L + "val.f64", val);
+      const GascoigneMesh* ML = SL->GetMesh();
+      std::vector<double> xyz;
+      for (int i = 0; i < ML->nnodes(); ++i) {
+        if (c.dim == 3) {
+          const Vertex3d& v = ML->vertex3d(i);
+          xyz.push_back(v.x());
+          xyz.push_back(v.y());
+          xyz.push_back(v.z());
+        } else {
+          const Vertex2d& v = ML->vertex2d(i);
+          xyz.push_back(v.x());
+          xyz.push_back(v.y());
+        }
+      }
+      write_raw(L + "coord.f64", xyz);
+      std::vector<long> dn;
+      const IntVector* bv = ML->VertexOnBoundary(1);
+      if (bv)
+        for (int i : *bv)
+          dn.push_back(i);
+      write_raw(L + "dirichlet.i64", dn);
+    }
+    for (int l = 0; l + 1 < nl; ++l) {
+      // interpolator l maps level l+1 (fine) to level l (coarse); it is built
+      // from mesh transfer nlevels-l-2 (Solver/stdmultilevelsolver.cc:290-296)
+      const GascoigneMeshTransfer* GT = MA.GetTransfer(nl - l - 2);
+      std::string T = c.out + "/T" + std::to_string(l) + "_";
+      std::vector<long> c2f(GT->GetC2f().begin(), GT->GetC2f().end());
+      write_raw(T + "c2f.i64", c2f);
+      std::vector<long> z, v4, a8;
+      for (const auto& p : GT->GetZweier()) {
+        z.push_back(p.first);
+        for (int q : p.second)
+          z.push_back(q);
+      }
+      for (const auto& p : GT->GetVierer()) {
+        v4.push_back(p.first);
+        for (int q : p.second)
+          v4.push_back(q);
+      }
+      for (const auto& p : GT->GetAchter()) {
+        a8.push_back(p.first);
+        for (int q : p.second)
+          a8.push_back(q);
+      }
+      write_raw(T + "zweier.i64", z);
+      write_raw(T + "vierer.i64", v4);
+      write_raw(T + "achter.i64", a8);
+    }
+    std::vector<double> rhs(F.begin(), F.end());
+    write_raw(c.out + "/rhs.f64", rhs);
+    const GlobalVector& U = S->GetGV(u);
+    std::vector<double> sol(U.begin(), U.end());
+    write_raw(c.out + "/solution.f64", sol);
+  }
+  return 0;
+}
