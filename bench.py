@@ -1,0 +1,327 @@
+"""Benchmark: multigrid-preconditioned GMRES solve of the 3D 64^3 Q1
+variable-coefficient diffusion problem (274,625 DoFs) to a true relative
+residual of 1e-8, on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one complete solve from x = 0 (mixed precision: FP32 V(2,2)-Jacobi
+multigrid cycle inside FP64 flexible GMRES with refinement). The FP64 variant
+(same kernels, FP64 cycle) and the reference-semantics left-preconditioned FP64
+GMRES are timed beside it and reported as extra keys. Inputs are synthetic and
+seeded: kappa = exp(N(0,1)) per cell (seed 1001), f ~ U[-1,1] per node (seed
+1002), assembled like the reference's CGDisc Q1 (checked by the tests).
+
+Multi-GPU: the path does not shard on one problem in this build (replicas
+only): each rank solves its own copy; value = DoFs solved by all ranks / max
+over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solve DoF/s to 1e-8 rel. residual, mixed vs FP64 on GPU; SpMV % of HBM peak"
+WORKLOAD = ("3D scalar diffusion -div(kappa grad u)=f, unit cube, Q1 hex 64^3 cells "
+            "(274,625 DoFs), kappa log-normal per cell (mu 0, sigma 1, seed 1001), "
+            "f~U[-1,1] per node (seed 1002); 6-level V(2,2) damped Jacobi (omega 0.8) "
+            "multigrid preconditioning GMRES(20), tol 1e-8")
+DIM, COARSE, REFINE = 3, 1, 6
+PARAMS = dict(iterpre=2, iterpost=2, iterexact=10, omega=0.8, mgomega=1.0, mgtype="V",
+              gmressize=21, tol=1e-8, globaltol=1e-300, maxiter=200)
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                r = subprocess.run(["nvidia-smi", "-i", str(self.index),
+                                    f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
+                                   capture_output=True, text=True, timeout=5)
+                if r.returncode == 0 and r.stdout.strip():
+                    self.samples.append([x.strip() for x in r.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def cpu_baseline(kappa_rhs, ndof, threads):
+    """The reference's own FP64 CPU solver (compiled from its sources into
+    oracle/_ref) on the same workload; one bounded sample (one mesh build +
+    assembly, then `repeat` solves). Falls back to the C restatement."""
+    from oracle.oracle import REF_HARNESS, Oracle, run_reference, write_inputs
+    kappa, rhs = kappa_rhs
+    if os.path.exists(REF_HARNESS):
+        d = tempfile.mkdtemp(prefix="gb_cpu_")
+        env_threads = os.environ.get("OMP_NUM_THREADS")
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        try:
+            t0 = time.time()
+            out, s = run_reference(d, dim=DIM, coarse=COARSE, refine=REFINE, repeat=3,
+                                   tol=1e-8, globaltol=1e-16, gmressize=21, iterpre=2,
+                                   iterpost=2, omega=0.8, **write_inputs(d, kappa, rhs))
+            wall = time.time() - t0
+        finally:
+            if env_threads is None:
+                os.environ.pop("OMP_NUM_THREADS", None)
+            else:
+                os.environ["OMP_NUM_THREADS"] = env_threads
+        times = [float(t) for t in s["solve_s"]]
+        med = statistics.median(times)
+        return {"value": ndof / med, "unit": "DoF/s", "cores": threads, "kind": "reference",
+                "sample": (f"reference CPU StdMultiLevelSolver GMRES+V-cycle on the same "
+                           f"64^3 problem, median of {len(times)} solves after assembly "
+                           f"({med:.3f} s/solve, {s['iterations'][0]} iterations, true rel "
+                           f"residual {float(s['true_rel_residual'][0]):.2e}; "
+                           f"harness wall {wall:.1f} s incl. mesh+assembly)"),
+                "solve_s": med, "iterations": int(s["iterations"][0])}
+    from gascoignelib_b200.problem import structured_problem
+    P = structured_problem(DIM, COARSE, REFINE, kappa, rhs)
+    O = Oracle(P)
+    t0 = time.time()
+    x, info = O.gmres(vmax=21, tol=1e-8)
+    dt = time.time() - t0
+    return {"value": ndof / dt, "unit": "DoF/s", "cores": 1, "kind": "port",
+            "sample": f"oracle C restatement, one solve ({dt:.2f} s, {info['iterations']} it)",
+            "solve_s": dt, "iterations": info["iterations"]}
+
+
+def run_reference_arm(args, world, rank):
+    from gascoignelib_b200.problem import seeded_inputs
+    if rank != 0:
+        return
+    kappa, rhs = seeded_inputs(DIM, COARSE, REFINE)
+    ndof = (((COARSE << REFINE) + 1) ** DIM)
+    threads = os.cpu_count() or 1
+    from oracle.oracle import REF_HARNESS, run_reference, write_inputs
+    line = {"metric": METRIC, "impl": "reference", "unit": "DoF/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp64 (reference CPU)"}}
+    if not os.path.exists(REF_HARNESS):
+        # oracle port: the C restatement, single thread
+        cb = cpu_baseline((kappa, rhs), ndof, threads)
+        line.update(value=cb["value"], ms_per_step=1e3 * cb["solve_s"], cpu_baseline=cb,
+                    e2e={"value": cb["value"], "unit": "DoF/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0})
+        print(json.dumps(line))
+        return
+    d = tempfile.mkdtemp(prefix="gb_refarm_")
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    out, s = run_reference(d, dim=DIM, coarse=COARSE, refine=REFINE,
+                           repeat=args.warmup + args.steps, tol=1e-8, globaltol=1e-16,
+                           gmressize=21, iterpre=2, iterpost=2, omega=0.8,
+                           **write_inputs(d, kappa, rhs))
+    times = [float(t) for t in s["solve_s"]][args.warmup:]
+    tot = sum(times)
+    value = ndof * len(times) / tot
+    line.update(value=value, ms_per_step=1e3 * tot / len(times),
+                cpu_baseline={"value": value, "unit": "DoF/s", "cores": threads,
+                              "kind": "reference",
+                              "sample": f"{len(times)} timed solves after {args.warmup} "
+                                        f"warm-up, {s['iterations'][0]} iterations, true "
+                                        f"rel residual {float(s['true_rel_residual'][0]):.2e}"},
+                e2e={"value": value, "unit": "DoF/s", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0})
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from gascoignelib_b200.build import build_library
+    from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
+    from gascoignelib_b200.problem import seeded_inputs, structured_problem
+
+    if rank == 0:
+        build_library()
+    if dist:
+        dist.barrier()
+    kappa, rhs = seeded_inputs(DIM, COARSE, REFINE)
+    P = structured_problem(DIM, COARSE, REFINE, kappa, rhs)
+    ndof = P.finest.ndof
+    ctx = Context(local)
+    ctx.load_problem(P)
+    ctx.set_params(**PARAMS)
+    fl = P.nlevels - 1
+    xv, bv = ctx.vec(), ctx.vec()
+    ctx.upload(fl, bv, P.rhs)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def run_steps(prec, k, timed):
+        ms, infos = [], []
+        for _ in range(k):
+            flush.random_(0, 255)            # L2 (126 MB) flush between steps
+            torch.cuda.synchronize()
+            info = ctx.fgmres(xv, bv, prec) if prec is not None else ctx.gmres(xv, bv)
+            ms.append(info["device_ms"])
+            infos.append(info)
+        return ms, infos
+
+    # warm-up
+    run_steps(GB_FP32, args.warmup, False)
+    run_steps(GB_FP64, max(1, args.warmup // 2), False)
+    run_steps(None, 1, False)
+
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    k0 = ctx.kernel_count()
+    with ClockSampler(local) as clk:
+        ms32, info32 = run_steps(GB_FP32, args.steps, True)
+    launches = ctx.kernel_count() - k0
+    ms64, info64 = run_steps(GB_FP64, args.steps, True)
+    msleft, infoleft = run_steps(None, args.steps, True)
+    torch.cuda.synchronize()
+
+    t32 = sum(ms32)
+    tmax = t32
+    if dist:
+        t = torch.tensor([t32], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tmax = float(t.item())
+    value = ndof * args.steps * world / (tmax / 1e3)
+    v64 = ndof * args.steps / (sum(ms64) / 1e3)
+    vleft = ndof * args.steps / (sum(msleft) / 1e3)
+
+    # e2e: the C-ABI call with host buffers (pinned), H2D + solve + D2H timed
+    b_host = torch.from_numpy(P.rhs.copy()).pin_memory()
+    x_host = torch.empty_like(b_host).pin_memory()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.random_(0, 255)
+        torch.cuda.synchronize()
+        bn = b_host.numpy()
+        xn = x_host.numpy()
+        _, info = ctx.solve_host(bn, method=2, out=xn)
+        e2e_ms.append(info["device_ms"])
+    e2e_val = ndof * args.steps * world / (sum(e2e_ms) / 1e3)
+
+    # roofline: finest-level SpMV, timed alone with the L2 flushed before each launch
+    peak, peak_kind = _peaks()
+    spmv_ms64, spmv_b64 = ctx.bench_spmv(fl, GB_FP64, reps=20, flush_l2=True)
+    spmv_ms32, spmv_b32 = ctx.bench_spmv(fl, GB_FP32, reps=20, flush_l2=True)
+    ach64 = spmv_b64 / (spmv_ms64 * 1e-3) / 1e9
+    ach32 = spmv_b32 / (spmv_ms32 * 1e-3) / 1e9
+
+    if rank == 0:
+        cb = None
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline((kappa, rhs), ndof, os.cpu_count() or 1)
+        i32 = info32[-1]
+        line = {
+            "metric": METRIC, "value": value, "unit": "DoF/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tmax / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 cycle / f64 outer",
+            "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "dofs": ndof, "levels": P.nlevels,
+                       "nnz_finest": int(P.finest.nnzb), "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MB write) before every step",
+                       "precision": "FP32 V-cycle in FP64 flexible GMRES + refinement"},
+            "fp64": {"value": v64, "unit": "DoF/s", "ms_per_step": sum(ms64) / args.steps,
+                     "iterations": info64[-1]["iterations"],
+                     "true_rel_residual": info64[-1]["true_rel_residual"]},
+            "mixed_over_fp64": value / world / v64,
+            "reference_semantics_fp64_left_gmres": {
+                "value": vleft, "unit": "DoF/s", "ms_per_step": sum(msleft) / args.steps,
+                "iterations": infoleft[-1]["iterations"],
+                "true_rel_residual": infoleft[-1]["true_rel_residual"]},
+            "iterations": i32["iterations"], "restarts": i32["restarts"],
+            "true_rel_residual": i32["true_rel_residual"],
+            "e2e": {"value": e2e_val, "unit": "DoF/s",
+                    "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8},
+            "roofline": {"bound": "hbm", "kernel": "k_sell_spmv<kAx,double> finest level",
+                         "achieved": ach64, "peak": peak, "unit": "GB/s",
+                         "frac": ach64 / peak, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "ms_per_launch": spmv_ms64, "algorithmic_bytes": spmv_b64,
+                         "fp32": {"achieved": ach32, "frac": ach32 / peak,
+                                  "ms_per_launch": spmv_ms32,
+                                  "algorithmic_bytes": spmv_b32}},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "cpu_baseline": cb,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,58 @@
+"""Builds the in-tree CUDA library for sm_100a (and the oracle for the tests).
+
+    python -m gascoignelib_b200.build
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+SRC = [os.path.join(HERE, "csrc", "gb_solver.cu")]
+DEPS = SRC + [os.path.join(HERE, "csrc", "gb_kernels.cuh"),
+              os.path.join(ROOT, "include", "gascoigne_b200.h")]
+OUT = os.path.join(HERE, "_lib", "libgascoigne_b200.so")
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
+              "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
+
+
+def _nvcc():
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def build_library(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    if not force and os.path.exists(OUT):
+        t = os.path.getmtime(OUT)
+        if all(os.path.getmtime(d) <= t for d in DEPS):
+            return OUT
+    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", OUT] + SRC
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    if verbose:
+        print(" ".join(cmd))
+    return OUT
+
+
+def build_oracle() -> None:
+    """Compiles the oracle's C restatement and, when the reference sources are
+    present, the reference CPU solver (test infrastructure only)."""
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True,
+                   capture_output=True)
+
+
+def build(force: bool = False) -> None:
+    build_library(force=force)
+    build_oracle()
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)
+    print(OUT)

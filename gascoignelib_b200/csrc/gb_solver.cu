@@ -1,0 +1,1485 @@
+// Host orchestration of the B200 linear-solve path and its C-ABI.
+//
+// The classes here mirror the reference's call surface for this path:
+//   Level      ~ StdSolver / CudaSolver per level (vmult, MatrixResidual, smooth,
+//                SetBoundaryVectorZero, vector ops)   Solver/stdsolver.cc,
+//                cuda/cudasolver.cc
+//   Transfer   ~ MgInterpolatorMatrix / CudaMgInterpolatorNested
+//                (restrict_zero, prolongate_add)      Discretization/Q1/
+//                mginterpolatormatrix.cc, cuda/cudamgintepolatornested.cc
+//   Context    ~ StdMultiLevelSolver / CudaMultiLevelSolver (LinearMg, mgstep,
+//                precondition, Gmres)                 Solver/stdmultilevelsolver.cc
+// Device vectors stay resident for the whole solve; nothing is copied between
+// host and device inside a solve except 8-byte status words.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/gascoigne_b200.h"
+#include "gb_kernels.cuh"
+
+namespace gb {
+
+// ------------------------------------------------------------------ memory
+
+template<class T>
+struct DeviceArray
+{
+  T* p = nullptr;
+  size_t n = 0;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  DeviceArray(DeviceArray&& o) noexcept
+    : p(o.p)
+    , n(o.n)
+  {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DeviceArray& operator=(DeviceArray&& o) noexcept
+  {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DeviceArray() { release(); }
+  void release()
+  {
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count)
+  {
+    if (count == n && p)
+      return cudaSuccess;
+    release();
+    if (count == 0)
+      return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess)
+      n = count;
+    else
+      p = nullptr;
+    return e;
+  }
+};
+
+struct Error
+{
+  int code;
+  std::string msg;
+};
+
+#define GB_CUDA(call)                                                          \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      throw ::gb::Error{ (e_ == cudaErrorMemoryAllocation) ? GB_ENOMEM         \
+                                                           : GB_ECUDA,         \
+                         std::string(#call) + ": " + cudaGetErrorString(e_) }; \
+  } while (0)
+
+#define GB_REQUIRE(cond, code, msg)                                            \
+  do {                                                                         \
+    if (!(cond))                                                               \
+      throw ::gb::Error{ code, msg };                                          \
+  } while (0)
+
+// --------------------------------------------------------------- matrices
+
+// SELL-32: slice s holds rows 32s..32s+31, column-major (entry j of lane l at
+// sptr[s] + 32 j + l); slice width = longest row of the slice; padding uses
+// column = own row (or 0 past n) and value 0.
+struct Sell
+{
+  int n = 0, nslices = 0;
+  int64_t entries = 0, nnz = 0;
+  DeviceArray<int> sptr, col;
+  DeviceArray<double> v64;
+  DeviceArray<float> v32;
+};
+
+static void
+build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
+           const double* val, cudaStream_t st)
+{
+  S.n = static_cast<int>(n);
+  S.nslices = static_cast<int>((n + kSlice - 1) / kSlice);
+  S.nnz = rowptr[n];
+  std::vector<int> sptr(S.nslices + 1, 0);
+  for (int s = 0; s < S.nslices; ++s) {
+    int64_t w = 0;
+    for (int l = 0; l < kSlice; ++l) {
+      int64_t r = int64_t(s) * kSlice + l;
+      if (r < n)
+        w = std::max<int64_t>(w, rowptr[r + 1] - rowptr[r]);
+    }
+    int64_t next = int64_t(sptr[s]) + w * kSlice;
+    GB_REQUIRE(next < (int64_t(1) << 31), GB_EINVAL,
+               "matrix too large for 32-bit SELL offsets");
+    sptr[s + 1] = static_cast<int>(next);
+  }
+  S.entries = sptr[S.nslices];
+  std::vector<int> c(S.entries);
+  std::vector<double> v(S.entries, 0.0);
+  std::vector<float> v32(S.entries, 0.0f);
+  for (int s = 0; s < S.nslices; ++s) {
+    int w = (sptr[s + 1] - sptr[s]) / kSlice;
+    for (int l = 0; l < kSlice; ++l) {
+      int64_t r = int64_t(s) * kSlice + l;
+      int64_t len = r < n ? rowptr[r + 1] - rowptr[r] : 0;
+      for (int j = 0; j < w; ++j) {
+        int64_t e = sptr[s] + int64_t(j) * kSlice + l;
+        if (j < len) {
+          int64_t cc = col[rowptr[r] + j];
+          GB_REQUIRE(cc >= 0 && cc < n, GB_EINVAL, "column index out of range");
+          c[e] = static_cast<int>(cc);
+          v[e] = val[rowptr[r] + j];
+          v32[e] = static_cast<float>(v[e]);
+        } else {
+          c[e] = r < n ? static_cast<int>(r) : 0;
+        }
+      }
+    }
+  }
+  GB_CUDA(S.sptr.alloc(sptr.size()));
+  GB_CUDA(S.col.alloc(std::max<size_t>(c.size(), 1)));
+  GB_CUDA(S.v64.alloc(std::max<size_t>(v.size(), 1)));
+  GB_CUDA(S.v32.alloc(std::max<size_t>(v32.size(), 1)));
+  GB_CUDA(cudaMemcpyAsync(S.sptr.p, sptr.data(), sptr.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, st));
+  if (S.entries) {
+    GB_CUDA(cudaMemcpyAsync(S.col.p, c.data(), c.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(S.v64.p, v.data(), v.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(S.v32.p, v32.data(), v32.size() * sizeof(float),
+                            cudaMemcpyHostToDevice, st));
+  }
+  // host vectors must outlive the async copies
+  GB_CUDA(cudaStreamSynchronize(st));
+}
+
+template<class T>
+static const T* sell_vals(const Sell& S);
+template<>
+const double* sell_vals<double>(const Sell& S)
+{
+  return S.v64.p;
+}
+template<>
+const float* sell_vals<float>(const Sell& S)
+{
+  return S.v32.p;
+}
+
+struct Level
+{
+  int64_t n = 0;
+  int B = 1;
+  bool has_matrix = false;
+  std::vector<int64_t> h_rowptr, h_col, h_diag;
+  std::vector<double> h_val;
+  Sell A, AT;
+  bool has_AT = false;
+  DeviceArray<double> dinv64;
+  DeviceArray<float> dinv32;
+  DeviceArray<uint8_t> dirmask;
+  DeviceArray<int> dirlist;
+  int ndir = 0;
+  int64_t ndof() const { return n * B; }
+};
+
+struct Transfer
+{
+  bool set = false;
+  int nc = 0, nf = 0;
+  int64_t nent = 0;
+  DeviceArray<int> rptr, pptr;
+  DeviceArray<uint32_t> rent, pent;
+};
+
+template<class T>
+struct MgWork
+{
+  std::vector<DeviceArray<T>> u, b, v; // per level (finest: v only used)
+};
+
+} // namespace gb
+
+struct gb_ctx
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  gb_params params{ 4, 4, 10, 1.0, 1.0, 'V', 10, 1e-2, 1e-12, 10 };
+  int nlevels = 0;
+  std::vector<gb::Level> L;
+  std::vector<gb::Transfer> T;
+  std::map<int, std::vector<gb::DeviceArray<double>>> vecs;
+  int next_id = 1;
+  gb::MgWork<double> w64;
+  gb::MgWork<float> w32;
+  bool work_ready = false;
+  gb::DeviceArray<double> partials;
+  gb::DeviceArray<unsigned> ticket;
+  gb::DeviceArray<double> scal; // general device scalars
+  gb::DeviceArray<gb::GmresDev> G;
+  gb::DeviceArray<double> krylov, zb64, pbuf, fine32_rhs_dummy;
+  gb::DeviceArray<float> zb32, fine_rhs32;
+  int* h_flags = nullptr; // pinned
+  int64_t launches = 0;
+  gb::DeviceArray<unsigned char> flush;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace gb {
+using Context = gb_ctx;
+
+static void
+check_launch(Context& c)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw Error{ GB_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e) };
+}
+
+template<class K, class... Args>
+static void
+launch(Context& c, K kern, int grid, int block, Args... args)
+{
+  if (grid <= 0)
+    return;
+  kern<<<grid, block, 0, c.stream>>>(args...);
+  c.launches++;
+  check_launch(c);
+}
+
+static int
+blocks_for(int64_t n, int threads)
+{
+  return static_cast<int>((n + threads - 1) / threads);
+}
+
+static int
+red_blocks(int64_t n)
+{
+  int64_t b = (n + kRedThreads * 8 - 1) / (kRedThreads * 8);
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, kMaxRedBlocks)));
+}
+
+static int
+stream_blocks(int64_t n)
+{
+  int64_t b = (n + 255) / 256;
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16)));
+}
+
+static Level&
+level(Context& c, int l)
+{
+  GB_REQUIRE(l >= 0 && l < c.nlevels, GB_EINVAL, "level out of range");
+  return c.L[l];
+}
+
+static Level&
+level_with_matrix(Context& c, int l)
+{
+  Level& L = level(c, l);
+  GB_REQUIRE(L.has_matrix, GB_ESTATE, "no matrix on this level");
+  return L;
+}
+
+static double*
+vec(Context& c, int l, int id)
+{
+  auto it = c.vecs.find(id);
+  GB_REQUIRE(it != c.vecs.end(), GB_EINVAL, "unknown vector id");
+  Level& L = level_with_matrix(c, l);
+  auto& lv = it->second;
+  if (lv.size() < static_cast<size_t>(c.nlevels))
+    lv.resize(c.nlevels);
+  if (lv[l].n != static_cast<size_t>(L.ndof())) {
+    GB_CUDA(lv[l].alloc(L.ndof()));
+    GB_CUDA(cudaMemsetAsync(lv[l].p, 0, L.ndof() * sizeof(double), c.stream));
+  }
+  return lv[l].p;
+}
+
+// --------------------------------------------------------------- reductions
+
+static void
+dot_dev(Context& c, int64_t n, const double* a, const double* b, RedOut ro)
+{
+  launch(c, k_dot<double, double>, red_blocks(n), kRedThreads, n, a, b,
+         c.partials.p, c.ticket.p, ro);
+}
+
+static double
+read_scalar(Context& c, const double* dptr)
+{
+  double h = 0;
+  GB_CUDA(cudaMemcpyAsync(&h, dptr, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  return h;
+}
+
+// ----------------------------------------------------------------- SpMV
+
+template<int MODE, class TV, class TX, class TO>
+static void
+spmv(Context& c, const Level& L, const Sell& S, const TX* x, TO* y, const TO* b,
+     const TV* dinv, double alpha)
+{
+  launch(c, k_sell_spmv<MODE, TV, TX, TO>, blocks_for(S.n, kSpmvThreads),
+         kSpmvThreads, S.n, S.sptr.p, S.col.p, sell_vals<TV>(S), x, y, b, dinv,
+         L.dirmask.p, alpha);
+}
+
+template<class T>
+static const T* dinv_of(const Level& L);
+template<>
+const double* dinv_of<double>(const Level& L)
+{
+  return L.dinv64.p;
+}
+template<>
+const float* dinv_of<float>(const Level& L)
+{
+  return L.dinv32.p;
+}
+
+// ---------------------------------------------------------- level set-up
+
+static void
+ensure_work(Context& c)
+{
+  if (c.work_ready)
+    return;
+  for (int l = 0; l < c.nlevels; ++l) {
+    GB_REQUIRE(c.L[l].has_matrix, GB_ESTATE, "every level needs a matrix");
+    if (l + 1 < c.nlevels) {
+      GB_REQUIRE(c.T[l].set, GB_ESTATE, "every level pair needs a transfer");
+      GB_REQUIRE(c.T[l].nc == c.L[l].n && c.T[l].nf == c.L[l + 1].n, GB_ESTATE,
+                 "transfer sizes differ from the level sizes");
+    }
+  }
+  c.w64.u.resize(c.nlevels);
+  c.w64.b.resize(c.nlevels);
+  c.w64.v.resize(c.nlevels);
+  c.w32.u.resize(c.nlevels);
+  c.w32.b.resize(c.nlevels);
+  c.w32.v.resize(c.nlevels);
+  for (int l = 0; l < c.nlevels; ++l) {
+    size_t nd = c.L[l].ndof();
+    GB_CUDA(c.w64.u[l].alloc(nd));
+    GB_CUDA(c.w64.b[l].alloc(nd));
+    GB_CUDA(c.w64.v[l].alloc(nd));
+    GB_CUDA(c.w32.u[l].alloc(nd));
+    GB_CUDA(c.w32.b[l].alloc(nd));
+    GB_CUDA(c.w32.v[l].alloc(nd));
+  }
+  c.work_ready = true;
+}
+
+// ------------------------------------------------------------ smoothing
+
+// StdSolver::smooth, linear_smooth jacobi (Solver/stdsolver.cc:951-986): each
+// sweep computes h = y - A x, h = D^-1 h, x += omega h; fused into one pass that
+// writes the new iterate to the other buffer (u and tmp swap roles). A sweep
+// from x = 0 needs no product (y - A 0 == y).
+template<class T>
+static void
+smooth(Context& c, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
+{
+  const Level& L = c.L[l];
+  for (int it = 0; it < niter; ++it) {
+    if (u_zero) {
+      launch(c, k_jacobi_from_zero<T, T>, blocks_for(L.n, 256), 256, (int)L.n,
+             dinv_of<T>(L), b, u, c.params.omega);
+      u_zero = false;
+    } else {
+      spmv<kJacobi, T, T, T>(c, L, L.A, u, tmp, b, dinv_of<T>(L), c.params.omega);
+      std::swap(u, tmp);
+    }
+  }
+}
+
+// StdMultiLevelSolver::mgstep (Solver/stdmultilevelsolver.cc:462-531). Steps
+// that only feed CGInfo (the norms and the final residual) are not computed:
+// they do not change u. HNDistribute/HNAverage/HNZero are identities on meshes
+// without hanging nodes.
+// Returns true when u is still implicitly zero (no sweep has written it).
+template<class T>
+static bool
+mgstep(Context& c, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
+       char p, T*& u, T*& tmp, const T* b, bool u_zero)
+{
+  const gb_params& P = c.params;
+  if (l == coarselevel) {
+    if (p == 'F')
+      p0 = 'V';
+    smooth<T>(c, l, P.iterexact, u, tmp, b, u_zero); // smooth_exact
+    return u_zero;
+  }
+  const Level& L = c.L[l];
+  const Level& Lc = c.L[l - 1];
+  const Transfer& Tr = c.T[l - 1];
+  smooth<T>(c, l, P.iterpre, u, tmp, b, u_zero);
+  // MatrixResidual into tmp, restrict_zero + SetBoundaryVectorZero on l-1
+  if (u_zero) {
+    // u is still 0 (iterpre == 0): the residual is b itself
+    launch(c, k_restrict<T>, blocks_for(Tr.nc, 256), 256, Tr.nc, Tr.rptr.p,
+           Tr.rent.p, b, W.b[l - 1].p, Lc.dirmask.p);
+  } else {
+    spmv<kResid, T, T, T>(c, L, L.A, u, tmp, b, nullptr, 0.0);
+    launch(c, k_restrict<T>, blocks_for(Tr.nc, 256), 256, Tr.nc, Tr.rptr.p,
+           Tr.rent.p, (const T*)tmp, W.b[l - 1].p, Lc.dirmask.p);
+  }
+  int j = (p0 == 'V') ? 1 : (p0 == 'W') ? 2 : (p0 == 'F') ? 3 : 0;
+  T* uc = W.u[l - 1].p;
+  T* tc = W.v[l - 1].p;
+  bool czero = true; // Zero(u) on l-1
+  for (int i = 0; i < j; ++i)
+    czero = mgstep<T>(c, W, l - 1, finelevel, coarselevel, p0, p, uc, tc,
+                      W.b[l - 1].p, czero);
+  if (czero) // no sweep ran on l-1: its u is the zero of Zero(u)
+    launch(c, k_fill<T>, stream_blocks(Lc.ndof()), 256, (int64_t)Lc.ndof(), uc, T(0));
+  if ((l == 0) && (p == 'F'))
+    p0 = 'W';
+  if (u_zero) {
+    launch(c, k_fill<T>, stream_blocks(L.ndof()), 256, (int64_t)L.ndof(), u, T(0));
+  }
+  // Zero(v); prolongate_add; HNZero; SetBoundaryVectorZero(v); Add(u, mgomega, v)
+  launch(c, k_prolong<1, T>, blocks_for(Tr.nf, 256), 256, Tr.nf, Tr.pptr.p,
+         Tr.pent.p, (const T*)uc, u, L.dirmask.p, P.mgomega);
+  bool post_zero = false;
+  smooth<T>(c, l, P.iterpost, u, tmp, b, post_zero);
+  return false;
+}
+
+// One cycle on the finest level into x (T), rhs y (T), from x's content or 0.
+template<class T>
+static void
+precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero)
+{
+  ensure_work(c);
+  const int fl = c.nlevels - 1;
+  T* u = x;
+  T* tmp = W.v[fl].p;
+  // Pick the buffer of the first sweep so that the last write lands in x.
+  const gb_params& P = c.params;
+  int pingpong = (x_zero ? std::max(P.iterpre - 1, 0) : P.iterpre) + P.iterpost;
+  if (fl == 0)
+    pingpong = x_zero ? std::max(P.iterexact - 1, 0) : P.iterexact;
+  if (x_zero && (pingpong & 1))
+    std::swap(u, tmp);
+  char p = P.mgtype;
+  char p0 = (p == 'F') ? 'W' : p;
+  if (mgstep<T>(c, W, fl, fl, 0, p0, p, u, tmp, y, x_zero))
+    launch(c, k_fill<T>, stream_blocks(c.L[fl].ndof()), 256,
+           (int64_t)c.L[fl].ndof(), u, T(0));
+  if (u != x) {
+    GB_CUDA(cudaMemcpyAsync(x, u, c.L[fl].ndof() * sizeof(T),
+                            cudaMemcpyDeviceToDevice, c.stream));
+  }
+}
+
+// ------------------------------------------------------------------ GMRES
+
+static void
+ensure_gmres(Context& c, int vmax, bool flexible, int prec)
+{
+  GB_REQUIRE(vmax >= 2 && vmax <= kMaxV, GB_EINVAL, "gmressize out of range [2, 128]");
+  const size_t n = c.L[c.nlevels - 1].ndof();
+  GB_CUDA(c.krylov.alloc((vmax + 1) * n));
+  GB_CUDA(c.pbuf.alloc(n));
+  if (!c.G.p)
+    GB_CUDA(c.G.alloc(1));
+  if (flexible) {
+    if (prec == GB_FP32) {
+      GB_CUDA(c.zb32.alloc(vmax * n));
+      GB_CUDA(c.fine_rhs32.alloc(n));
+    } else {
+      GB_CUDA(c.zb64.alloc(vmax * n));
+    }
+  }
+}
+
+__global__ void
+k_gmres_setup(GmresDev* G, double tol, double globaltol, int maxiter)
+{
+  G->info.tol = tol;
+  G->info.globaltol = globaltol;
+  G->info.breaktol = 1e15;
+  G->info.miniter = 0;
+  G->info.maxiter = maxiter;
+  G->info.status = 0;
+  G->info.iteration = 0;
+  G->info.firstresidual = 0;
+  G->info.previousresidual = 1;
+  G->info.residual = 0;
+  G->info.aimedresidual = 0;
+  G->reached = 0;
+  G->need_reortho = 0;
+  G->zero_rho = 0;
+}
+
+__global__ void
+k_scale_gmres(int64_t n, double* __restrict__ y, const GmresDev* G)
+{
+  if (G->need_reortho)
+    return;
+  const double s = G->inv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = s * y[i];
+}
+
+// MGS of vv against V_0..V_{dim-1} into column H[last] (GMRES::orthogonalization)
+static void
+mgs(Context& c, int64_t n, double* vv, double* V, int dim, int last)
+{
+  GmresDev* G = c.G.p;
+  const int grid = red_blocks(n);
+  // d_0 = <vv, V_0>; H[last][0] += d_0
+  {
+    RedOut ro{ &G->d[0], &G->H[last][0], nullptr, 0 };
+    launch(c, k_mgs, grid, kRedThreads, n, vv, (const double*)nullptr,
+           (const double*)nullptr, (const double*)V, c.partials.p, c.ticket.p, ro);
+  }
+  for (int i = 0; i < dim; ++i) {
+    const double* vi = V + int64_t(i) * n;
+    if (i + 1 < dim) {
+      RedOut ro{ &G->d[i + 1], &G->H[last][i + 1], nullptr, 0 };
+      launch(c, k_mgs, grid, kRedThreads, n, vv, vi, (const double*)&G->d[i],
+             (const double*)(V + int64_t(i + 1) * n), c.partials.p, c.ticket.p, ro);
+    } else {
+      RedOut ro{ &G->H[last][dim], nullptr, nullptr, 1 };
+      launch(c, k_mgs, grid, kRedThreads, n, vv, vi, (const double*)&G->d[i],
+             (const double*)vv, c.partials.p, c.ticket.p, ro);
+    }
+  }
+}
+
+static void
+read_flags(Context& c)
+{
+  GB_CUDA(cudaMemcpyAsync(c.h_flags, &c.G.p->reached, 3 * sizeof(int),
+                          cudaMemcpyDeviceToHost, c.stream));
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+static void
+fill_info(Context& c, gb_solve_info* info, double* x_for_residual, const double* b)
+{
+  CGInfoDev I;
+  GB_CUDA(cudaMemcpyAsync(&I, &c.G.p->info, sizeof(I), cudaMemcpyDeviceToHost,
+                          c.stream));
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  info->iterations = I.iteration;
+  info->status = I.status;
+  info->firstresidual = I.firstresidual;
+  info->residual = I.residual;
+  // true residual ||b - A x|| and ||b|| (FP64)
+  const int fl = c.nlevels - 1;
+  Level& L = c.L[fl];
+  spmv<kResid, double, double, double>(c, L, L.A, x_for_residual, c.pbuf.p, b,
+                                       nullptr, 0.0);
+  dot_dev(c, L.ndof(), c.pbuf.p, c.pbuf.p, RedOut{ c.scal.p + 4, nullptr, nullptr, 1 });
+  dot_dev(c, L.ndof(), b, b, RedOut{ c.scal.p + 5, nullptr, nullptr, 1 });
+  double two[2];
+  GB_CUDA(cudaMemcpyAsync(two, c.scal.p + 4, 2 * sizeof(double),
+                          cudaMemcpyDeviceToHost, c.stream));
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  info->true_residual = two[0];
+  info->rhs_norm = two[1];
+}
+
+// StdMultiLevelSolver::Gmres -> GMRES::solve (left preconditioning)
+static int
+gmres_left(Context& c, double* x, const double* b, gb_solve_info* info)
+{
+  ensure_work(c);
+  const int vmax = c.params.gmressize;
+  ensure_gmres(c, vmax, false, GB_FP64);
+  const int fl = c.nlevels - 1;
+  Level& L = c.L[fl];
+  const int64_t n = L.ndof();
+  GmresDev* G = c.G.p;
+  double* V = c.krylov.p;
+  const int64_t l0 = c.launches;
+  GB_CUDA(cudaEventRecord(c.ev0, c.stream));
+
+  GB_CUDA(cudaMemsetAsync(G, 0, sizeof(GmresDev), c.stream));
+  launch(c, k_gmres_setup, 1, 1, G, c.params.tol, c.params.globaltol,
+         c.params.maxiter);
+  GB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), c.stream)); // NewtonLinearSolve
+  // residualgmres: p = b - A x, Dirichlet zero
+  spmv<kResidDir, double, double, double>(c, L, L.A, x, c.pbuf.p, b, nullptr, 0.0);
+  precondition_T<double>(c, c.w64, V, c.pbuf.p, true);
+  dot_dev(c, n, V, V, RedOut{ c.scal.p, nullptr, nullptr, 1 });
+  launch(c, k_gmres_init, 1, 1, G, (const double*)c.scal.p);
+  read_flags(c);
+  int dim = 0;
+  if (!c.h_flags[2]) { // rho != 0
+    launch(c, k_scale_dev, stream_blocks(n), 256, n, V, (const double*)&G->inv);
+    int reached = 0;
+    while (dim < vmax - 1 && !reached) {
+      dim++;
+      const int last = dim - 1;
+      double* vv = V + int64_t(dim) * n;
+      spmv<kAx, double, double, double>(c, L, L.A, V + int64_t(last) * n, c.pbuf.p,
+                                        nullptr, nullptr, 1.0);
+      precondition_T<double>(c, c.w64, vv, c.pbuf.p, true);
+      mgs(c, n, vv, V, dim, last);
+      launch(c, k_gmres_step, 1, 1, G, dim, 0, 1, 0);
+      launch(c, k_scale_gmres, stream_blocks(n), 256, n, vv, (const GmresDev*)G);
+      read_flags(c);
+      if (c.h_flags[1]) { // REORTHO: second orthogonalization pass
+        mgs(c, n, vv, V, dim, last);
+        launch(c, k_gmres_step, 1, 1, G, dim, 1, 1, 0);
+        launch(c, k_scale_gmres, stream_blocks(n), 256, n, vv, (const GmresDev*)G);
+        read_flags(c);
+      }
+      reached = c.h_flags[0];
+    }
+    launch(c, k_gmres_backward, 1, 1, G, dim);
+    launch(c, k_multi_axpy<double>, stream_blocks(n), 256, n, x, (const double*)V, n,
+           (const double*)G->hs, dim);
+  }
+  GB_CUDA(cudaEventRecord(c.ev1, c.stream));
+  GB_CUDA(cudaEventSynchronize(c.ev1));
+  float ms = 0;
+  GB_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+  if (info) {
+    fill_info(c, info, x, b);
+    info->restarts = 0;
+    info->kernel_launches = static_cast<int>(c.launches - l0);
+    info->device_ms = ms;
+    if (c.h_flags[2]) {
+      info->iterations = 0;
+      info->status = 2;
+    }
+  }
+  return GB_OK;
+}
+
+// Flexible GMRES (FP64 Arnoldi, cycle in `prec`), restarted as iterative
+// refinement on the true FP64 residual.
+static int
+gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* info)
+{
+  ensure_work(c);
+  const int vmax = c.params.gmressize;
+  ensure_gmres(c, vmax, true, prec);
+  const int fl = c.nlevels - 1;
+  Level& L = c.L[fl];
+  const int64_t n = L.ndof();
+  const int m = vmax - 1;
+  GmresDev* G = c.G.p;
+  double* V = c.krylov.p;
+  const int64_t l0 = c.launches;
+  GB_CUDA(cudaEventRecord(c.ev0, c.stream));
+
+  GB_CUDA(cudaMemsetAsync(G, 0, sizeof(GmresDev), c.stream));
+  launch(c, k_gmres_setup, 1, 1, G, c.params.tol, c.params.globaltol,
+         c.params.maxiter);
+  dot_dev(c, n, b, b, RedOut{ &G->bnorm, nullptr, nullptr, 1 });
+  GB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), c.stream));
+  int total = 0, restarts = 0, converged = 0;
+  double bnorm = -1.0;
+  for (;;) {
+    // r = b - A x (Dirichlet zero) into V_0, beta = ||r||
+    spmv<kResidDir, double, double, double>(c, L, L.A, x, V, b, nullptr, 0.0);
+    dot_dev(c, n, V, V, RedOut{ c.scal.p, nullptr, nullptr, 1 });
+    launch(c, k_fgmres_restart, 1, 1, G, (const double*)c.scal.p, vmax);
+    double hv[2];
+    GB_CUDA(cudaMemcpyAsync(&hv[0], c.scal.p, sizeof(double), cudaMemcpyDeviceToHost,
+                            c.stream));
+    GB_CUDA(cudaMemcpyAsync(&hv[1], &G->bnorm, sizeof(double), cudaMemcpyDeviceToHost,
+                            c.stream));
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+    const double beta = hv[0];
+    bnorm = hv[1];
+    if (beta <= c.params.tol * bnorm || beta < c.params.globaltol || beta == 0.0) {
+      converged = 1;
+      break;
+    }
+    if (total >= c.params.maxiter || restarts > 50)
+      break;
+    launch(c, k_scale_dev, stream_blocks(n), 256, n, V, (const double*)&G->inv);
+    int steps = 0;
+    const int maxsteps = std::min(m, c.params.maxiter - total);
+    for (int j = 0; j < maxsteps; ++j) {
+      double* vj = V + int64_t(j) * n;
+      double* w = V + int64_t(j + 1) * n;
+      if (prec == GB_FP32) {
+        float* z = c.zb32.p + int64_t(j) * n;
+        launch(c, k_convert<double, float>, stream_blocks(n), 256, n, c.fine_rhs32.p,
+               (const double*)vj);
+        precondition_T<float>(c, c.w32, z, c.fine_rhs32.p, true);
+        spmv<kAx, double, float, double>(c, L, L.A, (const float*)z, w, nullptr,
+                                         nullptr, 1.0);
+      } else {
+        double* z = c.zb64.p + int64_t(j) * n;
+        precondition_T<double>(c, c.w64, z, vj, true);
+        spmv<kAx, double, double, double>(c, L, L.A, (const double*)z, w, nullptr,
+                                          nullptr, 1.0);
+      }
+      mgs(c, n, w, V, j + 1, j);
+      launch(c, k_gmres_step, 1, 1, G, j + 1, 1, 2, maxsteps);
+      launch(c, k_scale_gmres, stream_blocks(n), 256, n, w, (const GmresDev*)G);
+      steps = j + 1;
+      read_flags(c);
+      if (c.h_flags[0])
+        break;
+    }
+    launch(c, k_gmres_backward, 1, 1, G, steps);
+    if (prec == GB_FP32)
+      launch(c, k_multi_axpy<float>, stream_blocks(n), 256, n, x,
+             (const float*)c.zb32.p, n, (const double*)G->hs, steps);
+    else
+      launch(c, k_multi_axpy<double>, stream_blocks(n), 256, n, x,
+             (const double*)c.zb64.p, n, (const double*)G->hs, steps);
+    total += steps;
+    restarts++;
+  }
+  GB_CUDA(cudaEventRecord(c.ev1, c.stream));
+  GB_CUDA(cudaEventSynchronize(c.ev1));
+  float ms = 0;
+  GB_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+  if (info) {
+    fill_info(c, info, x, b);
+    info->iterations = total;
+    info->status = converged ? 2 : 3;
+    info->restarts = restarts;
+    info->kernel_launches = static_cast<int>(c.launches - l0);
+    info->device_ms = ms;
+  }
+  return converged ? GB_OK : GB_ENOTCONV;
+}
+
+} // namespace gb
+
+// ==================================================================== C-ABI
+
+using namespace gb;
+
+#define GB_API_BEGIN                                                           \
+  if (!ctx)                                                                    \
+    return GB_EINVAL;                                                          \
+  try {
+#define GB_API_END                                                             \
+  }                                                                            \
+  catch (const gb::Error& e)                                                   \
+  {                                                                            \
+    ctx->err = e.msg;                                                          \
+    return e.code;                                                             \
+  }                                                                            \
+  catch (const std::bad_alloc&)                                                \
+  {                                                                            \
+    ctx->err = "host allocation failed";                                       \
+    return GB_ENOMEM;                                                          \
+  }                                                                            \
+  return GB_OK;
+
+extern "C" {
+
+int
+gb_ctx_create(gb_ctx** out, int device)
+{
+  if (!out)
+    return GB_EINVAL;
+  *out = nullptr;
+  gb_ctx* ctx = new (std::nothrow) gb_ctx;
+  if (!ctx)
+    return GB_ENOMEM;
+  try {
+    ctx->device = device;
+    GB_CUDA(cudaSetDevice(device));
+    GB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    GB_CUDA(cudaEventCreate(&ctx->ev0));
+    GB_CUDA(cudaEventCreate(&ctx->ev1));
+    GB_CUDA(ctx->partials.alloc(kMaxRedBlocks));
+    GB_CUDA(ctx->ticket.alloc(1));
+    GB_CUDA(cudaMemset(ctx->ticket.p, 0, sizeof(unsigned)));
+    GB_CUDA(ctx->scal.alloc(16));
+    GB_CUDA(cudaMallocHost(&ctx->h_flags, 16 * sizeof(int)));
+  } catch (const gb::Error& e) {
+    fprintf(stderr, "gb_ctx_create: %s\n", e.msg.c_str());
+    int code = e.code;
+    gb_ctx_destroy(ctx);
+    return code;
+  }
+  *out = ctx;
+  return GB_OK;
+}
+
+int
+gb_ctx_destroy(gb_ctx* ctx)
+{
+  if (!ctx)
+    return GB_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream)
+    cudaStreamSynchronize(ctx->stream);
+  if (ctx->h_flags)
+    cudaFreeHost(ctx->h_flags);
+  if (ctx->ev0)
+    cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1)
+    cudaEventDestroy(ctx->ev1);
+  cudaStream_t st = ctx->stream;
+  delete ctx; // releases device arrays
+  if (st)
+    cudaStreamDestroy(st);
+  return GB_OK;
+}
+
+const char*
+gb_last_error_string(const gb_ctx* ctx)
+{
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+int
+gb_ctx_synchronize(gb_ctx* ctx)
+{
+  GB_API_BEGIN
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_API_END
+}
+
+int
+gb_set_params(gb_ctx* ctx, const gb_params* p)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(p, GB_EINVAL, "null params");
+  GB_REQUIRE(p->iterpre >= 0 && p->iterpost >= 0 && p->iterexact >= 0, GB_EINVAL,
+             "negative sweep count");
+  GB_REQUIRE(p->mgtype == 'V' || p->mgtype == 'W' || p->mgtype == 'F', GB_EINVAL,
+             "mgtype must be V, W or F");
+  GB_REQUIRE(p->gmressize >= 2 && p->gmressize <= kMaxV, GB_EINVAL,
+             "gmressize out of range [2, 128]");
+  GB_REQUIRE(p->maxiter >= 1, GB_EINVAL, "maxiter must be >= 1");
+  ctx->params = *p;
+  GB_API_END
+}
+
+int
+gb_get_params(const gb_ctx* ctx, gb_params* p)
+{
+  if (!ctx || !p)
+    return GB_EINVAL;
+  *p = ctx->params;
+  return GB_OK;
+}
+
+int
+gb_set_nlevels(gb_ctx* ctx, int nlevels)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(nlevels >= 1 && nlevels <= 32, GB_EINVAL, "nlevels out of range [1, 32]");
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->nlevels = nlevels;
+  ctx->L.clear();
+  ctx->L.resize(nlevels);
+  ctx->T.clear();
+  ctx->T.resize(nlevels > 1 ? nlevels - 1 : 0);
+  ctx->work_ready = false;
+  for (auto& kv : ctx->vecs)
+    kv.second.clear();
+  GB_API_END
+}
+
+int
+gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowptr,
+                    const int64_t* col, const int64_t* diag, const double* val)
+{
+  GB_API_BEGIN
+  Level& L = level(*ctx, lvl);
+  GB_REQUIRE(B == 1, GB_EINVAL, "only block size 1 is supported by this build");
+  GB_REQUIRE(n >= 1 && n < (int64_t(1) << 29), GB_EINVAL, "n out of range");
+  GB_REQUIRE(rowptr && col && diag && val, GB_EINVAL, "null array");
+  GB_REQUIRE(rowptr[0] == 0, GB_EINVAL, "rowptr[0] != 0");
+  for (int64_t i = 0; i < n; ++i) {
+    GB_REQUIRE(rowptr[i + 1] >= rowptr[i], GB_EINVAL, "rowptr not monotone");
+    GB_REQUIRE(diag[i] >= rowptr[i] && diag[i] < rowptr[i + 1] && col[diag[i]] == i,
+               GB_EINVAL, "diag does not point at the diagonal block");
+  }
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  const int64_t nnzb = rowptr[n];
+  L.n = n;
+  L.B = B;
+  L.h_rowptr.assign(rowptr, rowptr + n + 1);
+  L.h_col.assign(col, col + nnzb);
+  L.h_diag.assign(diag, diag + n);
+  L.h_val.assign(val, val + nnzb * B * B);
+  build_sell(L.A, n, rowptr, col, val, ctx->stream);
+  L.has_AT = false;
+  // block-diagonal inverse on the device (get_inverse_diagonal / K1)
+  std::vector<double> dblk(n * B * B);
+  for (int64_t i = 0; i < n; ++i)
+    for (int q = 0; q < B * B; ++q)
+      dblk[i * B * B + q] = val[diag[i] * B * B + q];
+  DeviceArray<double> dd;
+  GB_CUDA(dd.alloc(dblk.size()));
+  GB_CUDA(cudaMemcpyAsync(dd.p, dblk.data(), dblk.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(L.dinv64.alloc(n * B * B));
+  GB_CUDA(L.dinv32.alloc(n * B * B));
+  launch(*ctx, k_blockdiag_inverse<1>, blocks_for(n, 128), 128, (int)n,
+         (const double*)dd.p, L.dinv64.p, L.dinv32.p);
+  if (L.dirmask.n != static_cast<size_t>(n * B)) {
+    GB_CUDA(L.dirmask.alloc(n * B));
+    GB_CUDA(cudaMemsetAsync(L.dirmask.p, 0, n * B, ctx->stream));
+    L.dirlist.release();
+    L.ndir = 0;
+  }
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  L.has_matrix = true;
+  ctx->work_ready = false;
+  GB_API_END
+}
+
+int
+gb_level_set_dirichlet(gb_ctx* ctx, int lvl, int64_t nnodes, const int64_t* nodes,
+                       int comp_mask)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(nnodes >= 0 && (nnodes == 0 || nodes), GB_EINVAL, "bad node list");
+  std::vector<uint8_t> mask(L.ndof(), 0);
+  std::vector<int> dofs;
+  for (int64_t k = 0; k < nnodes; ++k) {
+    GB_REQUIRE(nodes[k] >= 0 && nodes[k] < L.n, GB_EINVAL, "Dirichlet node out of range");
+    for (int c = 0; c < L.B; ++c)
+      if (comp_mask & (1 << c)) {
+        int64_t d = nodes[k] * L.B + c;
+        if (!mask[d])
+          dofs.push_back(static_cast<int>(d));
+        mask[d] = 1;
+      }
+  }
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_CUDA(L.dirmask.alloc(mask.size()));
+  GB_CUDA(cudaMemcpy(L.dirmask.p, mask.data(), mask.size(), cudaMemcpyHostToDevice));
+  GB_CUDA(L.dirlist.alloc(std::max<size_t>(dofs.size(), 1)));
+  if (!dofs.empty())
+    GB_CUDA(cudaMemcpy(L.dirlist.p, dofs.data(), dofs.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+  L.ndir = static_cast<int>(dofs.size());
+  GB_API_END
+}
+
+int
+gb_level_set_transfer(gb_ctx* ctx, int lvl, int64_t ncoarse, const int64_t* c2f,
+                      int64_t nz, const int64_t* zweier, int64_t nv,
+                      const int64_t* vierer, int64_t na, const int64_t* achter)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(lvl >= 0 && lvl + 1 < ctx->nlevels, GB_EINVAL, "transfer level out of range");
+  Level& Lc = level_with_matrix(*ctx, lvl);
+  Level& Lf = level_with_matrix(*ctx, lvl + 1);
+  GB_REQUIRE(ncoarse == Lc.n, GB_EINVAL, "c2f size differs from the coarse level size");
+  GB_REQUIRE(Lc.B == 1 && Lf.B == 1, GB_EINVAL, "only block size 1");
+  const int64_t nf = Lf.n;
+  // (fine, coarse, weight code) pairs as MgInterpolatorMatrix::BasicInit forms them
+  std::vector<int> wcode(nf, -1);
+  std::vector<std::pair<int64_t, int64_t>> pairs;
+  pairs.reserve(ncoarse + 2 * nz + 4 * nv + 8 * na);
+  auto add = [&](int64_t f, int64_t cc, int code) {
+    GB_REQUIRE(f >= 0 && f < nf, GB_EINVAL, "fine index out of range");
+    GB_REQUIRE(cc >= 0 && cc < ncoarse, GB_EINVAL, "coarse index out of range");
+    pairs.emplace_back(f, cc);
+    wcode[f] = code;
+  };
+  for (int64_t i = 0; i < ncoarse; ++i)
+    add(c2f[i], i, 0);
+  for (int64_t i = 0; i < nz; ++i)
+    for (int q = 0; q < 2; ++q)
+      add(zweier[3 * i], zweier[3 * i + 1 + q], 1);
+  for (int64_t i = 0; i < nv; ++i)
+    for (int q = 0; q < 4; ++q)
+      add(vierer[5 * i], vierer[5 * i + 1 + q], 2);
+  for (int64_t i = 0; i < na; ++i)
+    for (int q = 0; q < 8; ++q)
+      add(achter[9 * i], achter[9 * i + 1 + q], 3);
+  // fine rows (prolongation) and coarse rows (restriction), columns ascending
+  std::vector<std::vector<int64_t>> prow(nf), rrow(ncoarse);
+  for (auto& pr : pairs) {
+    prow[pr.first].push_back(pr.second);
+    rrow[pr.second].push_back(pr.first);
+  }
+  std::vector<int> pptr(nf + 1, 0), rptr(ncoarse + 1, 0);
+  std::vector<uint32_t> pent, rent;
+  pent.reserve(pairs.size());
+  rent.reserve(pairs.size());
+  for (int64_t f = 0; f < nf; ++f) {
+    auto& r = prow[f];
+    std::sort(r.begin(), r.end());
+    for (int64_t cc : r)
+      pent.push_back(static_cast<uint32_t>(cc) | (uint32_t(wcode[f]) << kWShift));
+    pptr[f + 1] = static_cast<int>(pent.size());
+  }
+  for (int64_t cc = 0; cc < ncoarse; ++cc) {
+    auto& r = rrow[cc];
+    std::sort(r.begin(), r.end());
+    for (int64_t f : r)
+      rent.push_back(static_cast<uint32_t>(f) | (uint32_t(wcode[f]) << kWShift));
+    rptr[cc + 1] = static_cast<int>(rent.size());
+  }
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  Transfer& T = ctx->T[lvl];
+  T.nc = static_cast<int>(ncoarse);
+  T.nf = static_cast<int>(nf);
+  T.nent = static_cast<int64_t>(pairs.size());
+  GB_CUDA(T.pptr.alloc(pptr.size()));
+  GB_CUDA(T.rptr.alloc(rptr.size()));
+  GB_CUDA(T.pent.alloc(std::max<size_t>(pent.size(), 1)));
+  GB_CUDA(T.rent.alloc(std::max<size_t>(rent.size(), 1)));
+  GB_CUDA(cudaMemcpy(T.pptr.p, pptr.data(), pptr.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(T.rptr.p, rptr.data(), rptr.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  if (!pent.empty())
+    GB_CUDA(cudaMemcpy(T.pent.p, pent.data(), pent.size() * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice));
+  if (!rent.empty())
+    GB_CUDA(cudaMemcpy(T.rent.p, rent.data(), rent.size() * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice));
+  T.set = true;
+  ctx->work_ready = false;
+  GB_API_END
+}
+
+int
+gb_level_size(const gb_ctx* cctx, int lvl, int64_t* n, int* B, int64_t* nnzb)
+{
+  if (!cctx || lvl < 0 || lvl >= cctx->nlevels)
+    return GB_EINVAL;
+  const Level& L = cctx->L[lvl];
+  if (n)
+    *n = L.n;
+  if (B)
+    *B = L.B;
+  if (nnzb)
+    *nnzb = L.has_matrix ? L.A.nnz : 0;
+  return GB_OK;
+}
+
+int
+gb_vec_create(gb_ctx* ctx, int* id)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(id, GB_EINVAL, "null id");
+  *id = ctx->next_id++;
+  ctx->vecs[*id] = std::vector<DeviceArray<double>>();
+  GB_API_END
+}
+
+int
+gb_vec_free(gb_ctx* ctx, int id)
+{
+  GB_API_BEGIN
+  auto it = ctx->vecs.find(id);
+  GB_REQUIRE(it != ctx->vecs.end(), GB_EINVAL, "unknown vector id");
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->vecs.erase(it);
+  GB_API_END
+}
+
+int
+gb_vec_upload(gb_ctx* ctx, int lvl, int id, const double* host, int64_t len)
+{
+  GB_API_BEGIN
+  double* d = vec(*ctx, lvl, id);
+  GB_REQUIRE(host && len == ctx->L[lvl].ndof(), GB_EINVAL, "length differs from level size");
+  GB_CUDA(cudaMemcpyAsync(d, host, len * sizeof(double), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_API_END
+}
+
+int
+gb_vec_download(gb_ctx* ctx, int lvl, int id, double* host, int64_t len)
+{
+  GB_API_BEGIN
+  double* d = vec(*ctx, lvl, id);
+  GB_REQUIRE(host && len == ctx->L[lvl].ndof(), GB_EINVAL, "length differs from level size");
+  GB_CUDA(cudaMemcpyAsync(host, d, len * sizeof(double), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_API_END
+}
+
+int
+gb_vec_zero(gb_ctx* ctx, int lvl, int id)
+{
+  GB_API_BEGIN
+  double* d = vec(*ctx, lvl, id);
+  GB_CUDA(cudaMemsetAsync(d, 0, ctx->L[lvl].ndof() * sizeof(double), ctx->stream));
+  GB_API_END
+}
+
+int
+gb_vec_equ(gb_ctx* ctx, int lvl, int dst, double s, int src)
+{
+  GB_API_BEGIN
+  double* y = vec(*ctx, lvl, dst);
+  double* x = vec(*ctx, lvl, src);
+  int64_t n = ctx->L[lvl].ndof();
+  launch(*ctx, k_equ<double, double>, stream_blocks(n), 256, n, y, s, (const double*)x);
+  GB_API_END
+}
+
+int
+gb_vec_add(gb_ctx* ctx, int lvl, int dst, double s, int src)
+{
+  GB_API_BEGIN
+  double* y = vec(*ctx, lvl, dst);
+  double* x = vec(*ctx, lvl, src);
+  int64_t n = ctx->L[lvl].ndof();
+  launch(*ctx, k_add, stream_blocks(n), 256, n, y, s, (const double*)x);
+  GB_API_END
+}
+
+int
+gb_vec_dot(gb_ctx* ctx, int lvl, int a, int b, double* out)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(out, GB_EINVAL, "null output");
+  double* x = vec(*ctx, lvl, a);
+  double* y = vec(*ctx, lvl, b);
+  dot_dev(*ctx, ctx->L[lvl].ndof(), x, y, RedOut{ ctx->scal.p, nullptr, nullptr, 0 });
+  *out = read_scalar(*ctx, ctx->scal.p);
+  GB_API_END
+}
+
+int
+gb_vec_norm(gb_ctx* ctx, int lvl, int id, double* out)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(out, GB_EINVAL, "null output");
+  double* x = vec(*ctx, lvl, id);
+  dot_dev(*ctx, ctx->L[lvl].ndof(), x, x, RedOut{ ctx->scal.p, nullptr, nullptr, 1 });
+  *out = read_scalar(*ctx, ctx->scal.p);
+  GB_API_END
+}
+
+int
+gb_vmult(gb_ctx* ctx, int lvl, int y, int x, double d)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(y != x, GB_EINVAL, "y and x must differ");
+  Level& L = level_with_matrix(*ctx, lvl);
+  spmv<kAddAx, double, double, double>(*ctx, L, L.A, (const double*)vec(*ctx, lvl, x),
+                                       vec(*ctx, lvl, y), nullptr, nullptr, d);
+  GB_API_END
+}
+
+int
+gb_vmulteq(gb_ctx* ctx, int lvl, int y, int x, double d)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(y != x, GB_EINVAL, "y and x must differ");
+  Level& L = level_with_matrix(*ctx, lvl);
+  spmv<kAx, double, double, double>(*ctx, L, L.A, (const double*)vec(*ctx, lvl, x),
+                                    vec(*ctx, lvl, y), nullptr, nullptr, d);
+  GB_API_END
+}
+
+int
+gb_vmult_transpose(gb_ctx* ctx, int lvl, int y, int x, double d)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(y != x, GB_EINVAL, "y and x must differ");
+  Level& L = level_with_matrix(*ctx, lvl);
+  if (!L.has_AT) {
+    // transposed block-CSR, rows of A^T = columns of A, ascending
+    const int64_t n = L.n, nnz = L.h_rowptr[n];
+    std::vector<int64_t> tp(n + 1, 0), tc(nnz);
+    std::vector<double> tv(nnz);
+    for (int64_t k = 0; k < nnz; ++k)
+      tp[L.h_col[k] + 1]++;
+    for (int64_t i = 0; i < n; ++i)
+      tp[i + 1] += tp[i];
+    std::vector<int64_t> pos(tp.begin(), tp.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k) {
+        int64_t q = pos[L.h_col[k]]++;
+        tc[q] = i;
+        tv[q] = L.h_val[k];
+      }
+    GB_CUDA(cudaStreamSynchronize(ctx->stream));
+    build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), ctx->stream);
+    L.has_AT = true;
+  }
+  spmv<kAddAx, double, double, double>(*ctx, L, L.AT, (const double*)vec(*ctx, lvl, x),
+                                       vec(*ctx, lvl, y), nullptr, nullptr, d);
+  GB_API_END
+}
+
+int
+gb_matrix_residual(gb_ctx* ctx, int lvl, int y, int x, int b)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(y != x && y != b, GB_EINVAL, "y must differ from x and b");
+  Level& L = level_with_matrix(*ctx, lvl);
+  spmv<kResid, double, double, double>(*ctx, L, L.A, (const double*)vec(*ctx, lvl, x),
+                                       vec(*ctx, lvl, y),
+                                       (const double*)vec(*ctx, lvl, b), nullptr, 0.0);
+  GB_API_END
+}
+
+int
+gb_residualgmres(gb_ctx* ctx, int lvl, int y, int x, int b)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(y != x && y != b, GB_EINVAL, "y must differ from x and b");
+  Level& L = level_with_matrix(*ctx, lvl);
+  spmv<kResidDir, double, double, double>(*ctx, L, L.A,
+                                          (const double*)vec(*ctx, lvl, x),
+                                          vec(*ctx, lvl, y),
+                                          (const double*)vec(*ctx, lvl, b), nullptr, 0.0);
+  GB_API_END
+}
+
+int
+gb_smooth_jacobi(gb_ctx* ctx, int lvl, int niter, int x, int y, int h)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(niter >= 0, GB_EINVAL, "niter < 0");
+  GB_REQUIRE(x != y && x != h && y != h, GB_EINVAL, "x, y, h must differ");
+  level_with_matrix(*ctx, lvl);
+  double* xd = vec(*ctx, lvl, x);
+  double* hd = vec(*ctx, lvl, h);
+  const double* yd = vec(*ctx, lvl, y);
+  double* u = xd;
+  double* t = hd;
+  bool zero = false;
+  smooth<double>(*ctx, lvl, niter, u, t, yd, zero);
+  if (u != xd)
+    GB_CUDA(cudaMemcpyAsync(xd, u, ctx->L[lvl].ndof() * sizeof(double),
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+  GB_API_END
+}
+
+int
+gb_dirichlet_zero(gb_ctx* ctx, int lvl, int id)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  launch(*ctx, k_dirichlet_zero<double>, blocks_for(L.ndir, 256), 256, L.ndir,
+         (const int*)L.dirlist.p, vec(*ctx, lvl, id));
+  GB_API_END
+}
+
+int
+gb_level_get_inverse_diagonal(gb_ctx* ctx, int lvl, double* host, int64_t len)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(host && len == L.n * L.B * L.B, GB_EINVAL, "length must be n*B*B");
+  GB_CUDA(cudaMemcpyAsync(host, L.dinv64.p, len * sizeof(double), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_API_END
+}
+
+int
+gb_restrict_zero(gb_ctx* ctx, int lvl, int coarse_id, int fine_id)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(lvl >= 0 && lvl + 1 < ctx->nlevels && ctx->T[lvl].set, GB_ESTATE,
+             "no transfer on this level");
+  Transfer& T = ctx->T[lvl];
+  launch(*ctx, k_restrict<double>, blocks_for(T.nc, 256), 256, T.nc, (const int*)T.rptr.p,
+         (const uint32_t*)T.rent.p, (const double*)vec(*ctx, lvl + 1, fine_id),
+         vec(*ctx, lvl, coarse_id), (const uint8_t*)nullptr);
+  GB_API_END
+}
+
+int
+gb_prolongate_add(gb_ctx* ctx, int lvl, int fine_id, int coarse_id)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(lvl >= 0 && lvl + 1 < ctx->nlevels && ctx->T[lvl].set, GB_ESTATE,
+             "no transfer on this level");
+  Transfer& T = ctx->T[lvl];
+  launch(*ctx, k_prolong<0, double>, blocks_for(T.nf, 256), 256, T.nf,
+         (const int*)T.pptr.p, (const uint32_t*)T.pent.p,
+         (const double*)vec(*ctx, lvl, coarse_id), vec(*ctx, lvl + 1, fine_id),
+         (const uint8_t*)nullptr, 1.0);
+  GB_API_END
+}
+
+int
+gb_precondition(gb_ctx* ctx, int x, int y, int precision)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(x != y, GB_EINVAL, "x and y must differ");
+  const int fl = ctx->nlevels - 1;
+  GB_REQUIRE(fl >= 0, GB_ESTATE, "no levels");
+  ensure_work(*ctx);
+  double* xd = vec(*ctx, fl, x);
+  const double* yd = vec(*ctx, fl, y);
+  const int64_t n = ctx->L[fl].ndof();
+  if (precision == GB_FP32) {
+    float* x32 = ctx->w32.u[fl].p;
+    float* y32 = ctx->w32.b[fl].p;
+    launch(*ctx, k_convert<double, float>, stream_blocks(n), 256, n, y32, yd);
+    launch(*ctx, k_convert<double, float>, stream_blocks(n), 256, n, x32,
+           (const double*)xd);
+    precondition_T<float>(*ctx, ctx->w32, x32, y32, false);
+    launch(*ctx, k_convert<float, double>, stream_blocks(n), 256, n, xd,
+           (const float*)x32);
+  } else {
+    GB_REQUIRE(precision == GB_FP64, GB_EINVAL, "precision must be GB_FP64 or GB_FP32");
+    precondition_T<double>(*ctx, ctx->w64, xd, yd, false);
+  }
+  GB_API_END
+}
+
+int
+gb_gmres(gb_ctx* ctx, int x, int b, gb_solve_info* info)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(x != b, GB_EINVAL, "x and b must differ");
+  const int fl = ctx->nlevels - 1;
+  GB_REQUIRE(fl >= 0, GB_ESTATE, "no levels");
+  ensure_work(*ctx);
+  return gmres_left(*ctx, vec(*ctx, fl, x), vec(*ctx, fl, b), info);
+  GB_API_END
+}
+
+int
+gb_fgmres(gb_ctx* ctx, int x, int b, int precision, gb_solve_info* info)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(x != b, GB_EINVAL, "x and b must differ");
+  GB_REQUIRE(precision == GB_FP64 || precision == GB_FP32, GB_EINVAL, "bad precision");
+  const int fl = ctx->nlevels - 1;
+  GB_REQUIRE(fl >= 0, GB_ESTATE, "no levels");
+  ensure_work(*ctx);
+  return gmres_flexible(*ctx, vec(*ctx, fl, x), vec(*ctx, fl, b), precision, info);
+  GB_API_END
+}
+
+int
+gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x, int64_t len,
+              gb_solve_info* info)
+{
+  GB_API_BEGIN
+  const int fl = ctx->nlevels - 1;
+  GB_REQUIRE(fl >= 0, GB_ESTATE, "no levels");
+  GB_REQUIRE(b && x && len == ctx->L[fl].ndof(), GB_EINVAL, "length differs from level size");
+  GB_REQUIRE(method >= 0 && method <= 2, GB_EINVAL, "method must be 0, 1 or 2");
+  ensure_work(*ctx);
+  // resident work vectors for the host-buffer call
+  static const int kB = -1, kX = -2;
+  auto& bv = ctx->vecs[kB];
+  auto& xv = ctx->vecs[kX];
+  (void)bv;
+  (void)xv;
+  double* bd = vec(*ctx, fl, kB);
+  double* xd = vec(*ctx, fl, kX);
+  cudaEvent_t e0, e1;
+  GB_CUDA(cudaEventCreate(&e0));
+  GB_CUDA(cudaEventCreate(&e1));
+  GB_CUDA(cudaEventRecord(e0, ctx->stream));
+  GB_CUDA(cudaMemcpyAsync(bd, b, len * sizeof(double), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  int rc;
+  if (method == 0)
+    rc = gmres_left(*ctx, xd, bd, info);
+  else
+    rc = gmres_flexible(*ctx, xd, bd, method == 1 ? GB_FP64 : GB_FP32, info);
+  GB_CUDA(cudaMemcpyAsync(x, xd, len * sizeof(double), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  GB_CUDA(cudaEventRecord(e1, ctx->stream));
+  GB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  GB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (info)
+    info->device_ms = ms;
+  return rc;
+  GB_API_END
+}
+
+int
+gb_set_timing(gb_ctx* ctx, int on)
+{
+  (void)on;
+  return ctx ? GB_OK : GB_EINVAL;
+}
+
+int
+gb_get_kernel_count(const gb_ctx* ctx, int64_t* launches)
+{
+  if (!ctx || !launches)
+    return GB_EINVAL;
+  *launches = ctx->launches;
+  return GB_OK;
+}
+
+int
+gb_bench_spmv(gb_ctx* ctx, int lvl, int precision, int reps, int flush_l2,
+              double* ms_per_launch, double* bytes_per_launch)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(reps >= 1, GB_EINVAL, "reps < 1");
+  Level& L = level_with_matrix(*ctx, lvl);
+  ensure_work(*ctx);
+  const size_t flush_bytes = size_t(256) << 20; // > 126 MB L2
+  if (flush_l2 && ctx->flush.n < flush_bytes)
+    GB_CUDA(ctx->flush.alloc(flush_bytes));
+  cudaEvent_t a, bq;
+  GB_CUDA(cudaEventCreate(&a));
+  GB_CUDA(cudaEventCreate(&bq));
+  double total = 0;
+  for (int r = 0; r < reps; ++r) {
+    if (flush_l2)
+      GB_CUDA(cudaMemsetAsync(ctx->flush.p, r & 0xff, flush_bytes, ctx->stream));
+    GB_CUDA(cudaEventRecord(a, ctx->stream));
+    if (precision == GB_FP32)
+      spmv<kAx, float, float, float>(*ctx, L, L.A, (const float*)ctx->w32.b[lvl].p,
+                                     ctx->w32.u[lvl].p, nullptr, nullptr, 1.0);
+    else
+      spmv<kAx, double, double, double>(*ctx, L, L.A,
+                                        (const double*)ctx->w64.b[lvl].p,
+                                        ctx->w64.u[lvl].p, nullptr, nullptr, 1.0);
+    GB_CUDA(cudaEventRecord(bq, ctx->stream));
+    GB_CUDA(cudaEventSynchronize(bq));
+    float ms = 0;
+    GB_CUDA(cudaEventElapsedTime(&ms, a, bq));
+    total += ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(bq);
+  const double sv = precision == GB_FP32 ? 4.0 : 8.0;
+  const double nnz = static_cast<double>(L.A.nnz), n = static_cast<double>(L.n);
+  if (ms_per_launch)
+    *ms_per_launch = total / reps;
+  if (bytes_per_launch) // SpMV algorithmic bytes: values + indices + rowptr + x + y
+    *bytes_per_launch = nnz * sv + 4.0 * nnz + 4.0 * (n + 1) + 2.0 * n * sv;
+  GB_API_END
+}
+
+} // extern "C"

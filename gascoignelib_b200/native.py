@@ -1,0 +1,308 @@
+"""ctypes binding of the C-ABI in include/gascoigne_b200.h.
+
+The shared library is built in-tree (gascoignelib_b200/_lib/libgascoigne_b200.so,
+see build.py). There is no fallback: if the library cannot be loaded, or no GPU
+is visible, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libgascoigne_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "gascoigne_b200.h")
+
+GB_OK, GB_EINVAL, GB_ENOMEM, GB_ECUDA, GB_ENOTCONV, GB_ESTATE, GB_ETIMEOUT = range(7)
+GB_FP64, GB_FP32 = 0, 1
+STATUS = {0: "waiting", 1: "running", 2: "converged", 3: "too many iterations",
+          4: "exploded"}
+
+_P64 = C.POINTER(C.c_int64)
+_PD = C.POINTER(C.c_double)
+
+
+class GbParams(C.Structure):
+    _fields_ = [("iterpre", C.c_int), ("iterpost", C.c_int), ("iterexact", C.c_int),
+                ("omega", C.c_double), ("mgomega", C.c_double), ("mgtype", C.c_char),
+                ("gmressize", C.c_int), ("tol", C.c_double), ("globaltol", C.c_double),
+                ("maxiter", C.c_int)]
+
+
+class GbSolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("restarts", C.c_int),
+                ("firstresidual", C.c_double), ("residual", C.c_double),
+                ("true_residual", C.c_double), ("rhs_norm", C.c_double),
+                ("kernel_launches", C.c_int), ("device_ms", C.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["status_name"] = STATUS.get(self.status, str(self.status))
+        d["true_rel_residual"] = (self.true_residual / self.rhs_norm
+                                  if self.rhs_norm else 0.0)
+        return d
+
+
+class GBError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gascoigne_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+_SIGS = {
+    "gb_ctx_create": [C.POINTER(C.c_void_p), C.c_int],
+    "gb_ctx_destroy": [C.c_void_p],
+    "gb_ctx_synchronize": [C.c_void_p],
+    "gb_set_params": [C.c_void_p, C.POINTER(GbParams)],
+    "gb_get_params": [C.c_void_p, C.POINTER(GbParams)],
+    "gb_set_nlevels": [C.c_void_p, C.c_int],
+    "gb_level_set_matrix": [C.c_void_p, C.c_int, C.c_int64, C.c_int, _P64, _P64, _P64, _PD],
+    "gb_level_set_dirichlet": [C.c_void_p, C.c_int, C.c_int64, _P64, C.c_int],
+    "gb_level_set_transfer": [C.c_void_p, C.c_int, C.c_int64, _P64, C.c_int64, _P64,
+                              C.c_int64, _P64, C.c_int64, _P64],
+    "gb_level_size": [C.c_void_p, C.c_int, _P64, C.POINTER(C.c_int), _P64],
+    "gb_vec_create": [C.c_void_p, C.POINTER(C.c_int)],
+    "gb_vec_free": [C.c_void_p, C.c_int],
+    "gb_vec_upload": [C.c_void_p, C.c_int, C.c_int, _PD, C.c_int64],
+    "gb_vec_download": [C.c_void_p, C.c_int, C.c_int, _PD, C.c_int64],
+    "gb_vec_zero": [C.c_void_p, C.c_int, C.c_int],
+    "gb_vec_equ": [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int],
+    "gb_vec_add": [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int],
+    "gb_vec_norm": [C.c_void_p, C.c_int, C.c_int, _PD],
+    "gb_vec_dot": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD],
+    "gb_vmult": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double],
+    "gb_vmulteq": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double],
+    "gb_vmult_transpose": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double],
+    "gb_matrix_residual": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int],
+    "gb_residualgmres": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int],
+    "gb_smooth_jacobi": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
+    "gb_dirichlet_zero": [C.c_void_p, C.c_int, C.c_int],
+    "gb_level_get_inverse_diagonal": [C.c_void_p, C.c_int, _PD, C.c_int64],
+    "gb_restrict_zero": [C.c_void_p, C.c_int, C.c_int, C.c_int],
+    "gb_prolongate_add": [C.c_void_p, C.c_int, C.c_int, C.c_int],
+    "gb_precondition": [C.c_void_p, C.c_int, C.c_int, C.c_int],
+    "gb_gmres": [C.c_void_p, C.c_int, C.c_int, C.POINTER(GbSolveInfo)],
+    "gb_fgmres": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(GbSolveInfo)],
+    "gb_solve_host": [C.c_void_p, C.c_int, _PD, _PD, C.c_int64, C.POINTER(GbSolveInfo)],
+    "gb_set_timing": [C.c_void_p, C.c_int],
+    "gb_get_kernel_count": [C.c_void_p, _P64],
+    "gb_bench_spmv": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
+}
+
+
+def lib():
+    """Loads the in-tree CUDA library; raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with gascoignelib_b200.build.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.gb_last_error_string.argtypes = [C.c_void_p]
+        L.gb_last_error_string.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _p64(a):
+    return a.ctypes.data_as(_P64)
+
+
+def _pd(a):
+    return a.ctypes.data_as(_PD)
+
+
+class Context:
+    """One device context: levels, transfers, named vectors, solver keys."""
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.gb_ctx_create(C.byref(h), device)
+        if rc != GB_OK:
+            raise GBError(rc, "gb_ctx_create failed (no usable CUDA device?)")
+        self.h = h
+        self.nlevels = 0
+        self.sizes = []
+
+    # ------------------------------------------------------------ plumbing
+    def _chk(self, rc):
+        if rc != GB_OK:
+            msg = self._L.gb_last_error_string(self.h)
+            raise GBError(rc, msg.decode() if msg else "")
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.gb_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------- set-up
+    def set_params(self, iterpre=2, iterpost=2, iterexact=10, omega=0.8, mgomega=1.0,
+                   mgtype="V", gmressize=21, tol=1e-8, globaltol=1e-16, maxiter=100):
+        p = GbParams(iterpre, iterpost, iterexact, omega, mgomega, mgtype.encode()[:1],
+                     gmressize, tol, globaltol, maxiter)
+        self._chk(self._L.gb_set_params(self.h, C.byref(p)))
+
+    def get_params(self):
+        p = GbParams()
+        self._chk(self._L.gb_get_params(self.h, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in p._fields_}
+
+    def load_problem(self, prob):
+        """Uploads every level's matrix, Dirichlet list and transfer maps."""
+        nl = prob.nlevels
+        self._chk(self._L.gb_set_nlevels(self.h, nl))
+        self.nlevels = nl
+        self.sizes = []
+        for l, lv in enumerate(prob.levels):
+            rp, cl, dg = (np.ascontiguousarray(a, dtype=np.int64)
+                          for a in (lv.rowptr, lv.col, lv.diag))
+            vl = np.ascontiguousarray(lv.val, dtype=np.float64)
+            self._chk(self._L.gb_level_set_matrix(self.h, l, lv.n, lv.B, _p64(rp),
+                                                  _p64(cl), _p64(dg), _pd(vl)))
+            dr = np.ascontiguousarray(lv.dirichlet, dtype=np.int64)
+            self._chk(self._L.gb_level_set_dirichlet(self.h, l, dr.shape[0], _p64(dr),
+                                                     lv.dircomp_mask))
+            self.sizes.append(lv.n * lv.B)
+        for l, t in enumerate(prob.transfers):
+            c2f, z, v, a = (np.ascontiguousarray(x, dtype=np.int64)
+                            for x in (t.c2f, t.zweier, t.vierer, t.achter))
+            self._chk(self._L.gb_level_set_transfer(
+                self.h, l, c2f.shape[0], _p64(c2f), z.shape[0], _p64(z), v.shape[0],
+                _p64(v), a.shape[0], _p64(a)))
+
+    # ------------------------------------------------------------ vectors
+    def vec(self):
+        i = C.c_int()
+        self._chk(self._L.gb_vec_create(self.h, C.byref(i)))
+        return i.value
+
+    def free(self, vid):
+        self._chk(self._L.gb_vec_free(self.h, vid))
+
+    def upload(self, level, vid, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self._chk(self._L.gb_vec_upload(self.h, level, vid, _pd(a), a.shape[0]))
+
+    def download(self, level, vid):
+        out = np.empty(self.sizes[level])
+        self._chk(self._L.gb_vec_download(self.h, level, vid, _pd(out), out.shape[0]))
+        return out
+
+    def zero(self, level, vid):
+        self._chk(self._L.gb_vec_zero(self.h, level, vid))
+
+    def equ(self, level, dst, s, src):
+        self._chk(self._L.gb_vec_equ(self.h, level, dst, s, src))
+
+    def add(self, level, dst, s, src):
+        self._chk(self._L.gb_vec_add(self.h, level, dst, s, src))
+
+    def norm(self, level, vid):
+        out = C.c_double()
+        self._chk(self._L.gb_vec_norm(self.h, level, vid, C.byref(out)))
+        return out.value
+
+    def dot(self, level, a, b):
+        out = C.c_double()
+        self._chk(self._L.gb_vec_dot(self.h, level, a, b, C.byref(out)))
+        return out.value
+
+    # ----------------------------------------------------------- operators
+    def vmult(self, level, y, x, d=1.0):
+        self._chk(self._L.gb_vmult(self.h, level, y, x, d))
+
+    def vmulteq(self, level, y, x, d=1.0):
+        self._chk(self._L.gb_vmulteq(self.h, level, y, x, d))
+
+    def vmult_transpose(self, level, y, x, d=1.0):
+        self._chk(self._L.gb_vmult_transpose(self.h, level, y, x, d))
+
+    def matrix_residual(self, level, y, x, b):
+        self._chk(self._L.gb_matrix_residual(self.h, level, y, x, b))
+
+    def residualgmres(self, level, y, x, b):
+        self._chk(self._L.gb_residualgmres(self.h, level, y, x, b))
+
+    def smooth_jacobi(self, level, niter, x, y, h):
+        self._chk(self._L.gb_smooth_jacobi(self.h, level, niter, x, y, h))
+
+    def dirichlet_zero(self, level, vid):
+        self._chk(self._L.gb_dirichlet_zero(self.h, level, vid))
+
+    def inverse_diagonal(self, level):
+        out = np.empty(self.sizes[level])
+        self._chk(self._L.gb_level_get_inverse_diagonal(self.h, level, _pd(out),
+                                                        out.shape[0]))
+        return out
+
+    def restrict_zero(self, level, coarse, fine):
+        self._chk(self._L.gb_restrict_zero(self.h, level, coarse, fine))
+
+    def prolongate_add(self, level, fine, coarse):
+        self._chk(self._L.gb_prolongate_add(self.h, level, fine, coarse))
+
+    def precondition(self, x, y, precision=GB_FP64):
+        self._chk(self._L.gb_precondition(self.h, x, y, precision))
+
+    def gmres(self, x, b):
+        info = GbSolveInfo()
+        self._chk(self._L.gb_gmres(self.h, x, b, C.byref(info)))
+        return info.as_dict()
+
+    def fgmres(self, x, b, precision=GB_FP32, check=True):
+        info = GbSolveInfo()
+        rc = self._L.gb_fgmres(self.h, x, b, precision, C.byref(info))
+        if check or rc not in (GB_OK, GB_ENOTCONV):
+            self._chk(rc)
+        return info.as_dict()
+
+    def solve_host(self, b, method=2, out=None, check=True):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty_like(b) if out is None else out
+        info = GbSolveInfo()
+        rc = self._L.gb_solve_host(self.h, method, _pd(b), _pd(x), b.shape[0],
+                                   C.byref(info))
+        if check or rc not in (GB_OK, GB_ENOTCONV):
+            self._chk(rc)
+        return x, info.as_dict()
+
+    def kernel_count(self):
+        v = C.c_int64()
+        self._chk(self._L.gb_get_kernel_count(self.h, C.byref(v)))
+        return v.value
+
+    def bench_spmv(self, level, precision=GB_FP64, reps=10, flush_l2=True):
+        ms, by = C.c_double(), C.c_double()
+        self._chk(self._L.gb_bench_spmv(self.h, level, precision, reps, int(flush_l2),
+                                        C.byref(ms), C.byref(by)))
+        return ms.value, by.value
+
+
+def declared_symbols(header: str = HEADER):
+    """Function names declared in the public header."""
+    import re
+    txt = open(header).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(gb_\w+)\s*\(", txt,
+                                 flags=re.M)))

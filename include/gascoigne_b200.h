@@ -1,0 +1,212 @@
+/*
+ * gascoigne_b200.h - C-ABI of the B200 (sm_100a) linear-solve path for Gascoigne.
+ *
+ * This is the boundary a Gascoigne host build binds in place of its cuSPARSE
+ * backend (cuda/): the drop-in subclasses B200Solver : StdSolver,
+ * B200MultiLevelSolver : StdMultiLevelSolver and B200MgInterpolatorNested :
+ * MgInterpolatorNested forward their virtual overrides to these functions
+ * (see INTEGRATION.md). Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Every function returns int status: GB_OK (0) or a GB_E* code; the message
+ *    of the last failure is gb_last_error_string(ctx). Nothing calls exit().
+ *  - Levels are indexed as the reference indexes its solvers: 0 = coarsest,
+ *    nlevels-1 = finest (Solver/stdmultilevelsolver.cc:224-231).
+ *  - Vectors are node-major interleaved like CompVector (Common/compvector.h:
+ *    98-113); matrix blocks are row-major B x B (LinAlg/nodematrix.h:44-48).
+ *  - A vector id names one vector on every level, like Gascoigne's Vector name
+ *    (Interface/vectorinterface.h:40-81) with per-level GlobalVectors.
+ *  - All work is enqueued on the context's CUDA stream; functions that return
+ *    a host scalar or copy to host synchronise that stream.
+ *  - A context is used by one host thread at a time.
+ */
+#ifndef GASCOIGNE_B200_H
+#define GASCOIGNE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum gb_status
+{
+  GB_OK = 0,
+  GB_EINVAL = 1,    /* bad argument or size */
+  GB_ENOMEM = 2,    /* device or host allocation failed */
+  GB_ECUDA = 3,     /* CUDA runtime error */
+  GB_ENOTCONV = 4,  /* solver stopped without reaching the tolerance */
+  GB_ESTATE = 5,    /* call out of order (e.g. no matrix on a level) */
+  GB_ETIMEOUT = 6   /* a bounded device wait ran out */
+};
+
+enum gb_precision
+{
+  GB_FP64 = 0,      /* V-cycle values and vectors in FP64 */
+  GB_FP32 = 1       /* V-cycle values and vectors in FP32, FP32 accumulation */
+};
+
+/* Solver keys, with the reference's defaults where it has them:
+ * SolverData (Solver/solverdata.cc:41-55): iterpre 4, iterpost 4, iterexact 10,
+ * omega 1; StdMultiLevelSolverData (Solver/stdmultilevelsolverdata.cc:88-100):
+ * mgomega 1, mgtype V, gmressize 10; SolverInfos (Solver/solverinfos.cc:89-94):
+ * linear_tol 1e-2, linear_globaltol 1e-12, linear_maxiter 10. */
+typedef struct gb_params
+{
+  int iterpre, iterpost, iterexact;
+  double omega;      /* Jacobi damping */
+  double mgomega;    /* coarse-grid correction weight */
+  char mgtype;       /* 'V', 'W' or 'F' */
+  int gmressize;     /* Krylov memory: at most gmressize-1 Arnoldi steps */
+  double tol;        /* linear_tol (relative) */
+  double globaltol;  /* linear_globaltol (absolute) */
+  int maxiter;       /* linear_maxiter */
+} gb_params;
+
+typedef struct gb_solve_info
+{
+  int iterations;        /* Arnoldi steps (CGInfo iteration count) */
+  int status;            /* 0 waiting 1 running 2 converged 3 too many iterations
+                            4 exploded */
+  int restarts;          /* refinement cycles (flexible solver), 0 otherwise */
+  double firstresidual;  /* CGInfo first residual */
+  double residual;       /* last residual estimate */
+  double true_residual;  /* ||b - A x||_2 in FP64 after the solve */
+  double rhs_norm;       /* ||b||_2 */
+  int kernel_launches;   /* kernels this call launched */
+  double device_ms;      /* CUDA-event time of the call on the context stream */
+} gb_solve_info;
+
+typedef struct gb_ctx gb_ctx;
+
+/* ---- context -------------------------------------------------------------
+ * Replaces the handle set-up of CudaSolver::CudaSolver (cuda/cudasolver.cc:
+ * 25-33) and check_cuda.h's abort-on-error (cuda/check_cuda.h:28-67). */
+int gb_ctx_create(gb_ctx** ctx, int device);
+int gb_ctx_destroy(gb_ctx* ctx);
+const char* gb_last_error_string(const gb_ctx* ctx);
+int gb_ctx_synchronize(gb_ctx* ctx);
+/* Solver keys; replaces the ParamFile reads listed at gb_params. */
+int gb_set_params(gb_ctx* ctx, const gb_params* p);
+int gb_get_params(const gb_ctx* ctx, gb_params* p);
+/* Number of multigrid levels; replaces StdMultiLevelSolver::NewSolvers
+ * (Solver/stdmultilevelsolver.cc:210-234). Drops all level data. */
+int gb_set_nlevels(gb_ctx* ctx, int nlevels);
+
+/* ---- level data ----------------------------------------------------------
+ * Uploads the assembled block-CSR matrix of one level: SparseBlockMatrix
+ * <FMatrixBlock<B>>::mat() with its ColumnDiagStencil start/col/diag
+ * (LinAlg/sparseblockmatrix.h:84, LinAlg/columnstencil.h:57-60,
+ * LinAlg/columndiagstencil.h:54-57). Replaces CudaSolver::AssembleMatrix's
+ * CudaCSRMatrixInterface upload and get_inverse_diagonal (cuda/cudasolver.cc:
+ * 115-128, cuda/cudacsrmatrixinterface.cc:119-141,176-230). B = 1 on this
+ * build. Rows keep their column order; FP64 and FP32 copies are kept. */
+int gb_level_set_matrix(gb_ctx* ctx, int level, int64_t n, int B,
+                        const int64_t* rowptr, const int64_t* col,
+                        const int64_t* diag, const double* val);
+/* Strong-Dirichlet node list of a level with its component mask (bit c set:
+ * component c). Replaces CudaSolver::SetProblem's Dirichlet matrix
+ * (cuda/cudasolver.cc:271-297) and CGDisc::StrongDirichletVectorZero
+ * (DofHandler/cgdisc.h:1162-1179). */
+int gb_level_set_dirichlet(gb_ctx* ctx, int level, int64_t nnodes,
+                           const int64_t* nodes, int comp_mask);
+/* Mesh-transfer maps between coarse level `level` and level+1, as
+ * GascoigneMeshTransfer holds them (Mesh/gascoignemeshtransfer.h:48-51):
+ * c2f[ncoarse]; zweier rows [fine, c0, c1]; vierer [fine, c0..c3]; achter
+ * [fine, c0..c7]. Replaces CudaMgInterpolatorNested::BasicInit
+ * (cuda/cudamgintepolatornested.cc:21-25) and its R/P SimpleMatrix build. */
+int gb_level_set_transfer(gb_ctx* ctx, int level, int64_t ncoarse,
+                          const int64_t* c2f, int64_t nz, const int64_t* zweier,
+                          int64_t nv, const int64_t* vierer, int64_t na,
+                          const int64_t* achter);
+int gb_level_size(const gb_ctx* ctx, int level, int64_t* n, int* B,
+                  int64_t* nnzb);
+
+/* ---- vectors -------------------------------------------------------------
+ * Replaces CudaVectorInterface (cuda/cudavectorinterface.h:33-83) and
+ * StdSolver's vector ops (Solver/stdsolver.cc:685-688,1775-1810). */
+int gb_vec_create(gb_ctx* ctx, int* id);
+int gb_vec_free(gb_ctx* ctx, int id);
+int gb_vec_upload(gb_ctx* ctx, int level, int id, const double* host,
+                  int64_t len);
+int gb_vec_download(gb_ctx* ctx, int level, int id, double* host, int64_t len);
+int gb_vec_zero(gb_ctx* ctx, int level, int id);                   /* Zero */
+int gb_vec_equ(gb_ctx* ctx, int level, int dst, double s, int src); /* Equ */
+int gb_vec_add(gb_ctx* ctx, int level, int dst, double s, int src); /* Add */
+int gb_vec_norm(gb_ctx* ctx, int level, int id, double* out);       /* Norm */
+int gb_vec_dot(gb_ctx* ctx, int level, int a, int b, double* out); /* ScalarProduct */
+
+/* ---- level operators (StdSolver / CudaSolver overrides) ------------------ */
+/* y += d A x: StdSolver::vmult (Solver/stdsolver.cc:757-764),
+ * CudaSolver::vmult (cuda/cudasolver.cc:301-320). */
+int gb_vmult(gb_ctx* ctx, int level, int y, int x, double d);
+/* y = d A x: StdSolver::vmulteq (Solver/stdsolver.cc:768-778). */
+int gb_vmulteq(gb_ctx* ctx, int level, int y, int x, double d);
+/* y += d A^T x: the transposed operator SparseBlockMatrix::transpose builds
+ * (LinAlg/sparseblockmatrix.xx:478-491), applied without transposing. */
+int gb_vmult_transpose(gb_ctx* ctx, int level, int y, int x, double d);
+/* y = b - A x: StdSolver::MatrixResidual (Solver/stdsolver.cc:783-791). */
+int gb_matrix_residual(gb_ctx* ctx, int level, int y, int x, int b);
+/* y = b - A x, Dirichlet-zeroed: StdSolver::residualgmres
+ * (Solver/stdsolver.cc:742-754). */
+int gb_residualgmres(gb_ctx* ctx, int level, int y, int x, int b);
+/* niter damped-Jacobi sweeps x += omega D^-1 (y - A x): StdSolver::smooth with
+ * linear_smooth jacobi (Solver/stdsolver.cc:951-986), CudaSolver::smooth
+ * (cuda/cudasolver.cc:345-374). h is work space, as in the reference. */
+int gb_smooth_jacobi(gb_ctx* ctx, int level, int niter, int x, int y, int h);
+/* u = 0 on Dirichlet dofs: StdSolver::SetBoundaryVectorZero
+ * (Solver/stdsolver.cc:795-812). */
+int gb_dirichlet_zero(gb_ctx* ctx, int level, int id);
+/* Per-node inverse diagonal blocks (row-major B x B, FP64) as
+ * SparseBlockMatrix::Jacobi forms them (LinAlg/sparseblockmatrix.xx:47-56,
+ * NodeMatrix::gauss_jordan LinAlg/nodematrix.h:159-213). */
+int gb_level_get_inverse_diagonal(gb_ctx* ctx, int level, double* host,
+                                  int64_t len);
+
+/* ---- transfers (MgInterpolatorInterface overrides) ------------------------
+ * coarse = R fine: MgInterpolatorMatrix/Nested::restrict_zero
+ * (Discretization/Q1/mginterpolatormatrix.cc:123-133,
+ *  cuda/cudamgintepolatornested.cc:131-139). */
+int gb_restrict_zero(gb_ctx* ctx, int level, int coarse_id, int fine_id);
+/* fine += P coarse: prolongate_add (mginterpolatormatrix.cc:137-147,
+ * cuda/cudamgintepolatornested.cc:160-167). */
+int gb_prolongate_add(gb_ctx* ctx, int level, int fine_id, int coarse_id);
+
+/* ---- multilevel solver (StdMultiLevelSolver / CudaMultiLevelSolver) ------- */
+/* One multigrid cycle on the finest level, started from the current content
+ * of x, right-hand side y: StdMultiLevelSolver::precondition -> LinearMg ->
+ * mgstep with prec_maxiter 1 (Solver/stdmultilevelsolver.cc:411-531,940-952;
+ * cuda/cudamultilevelsolver.cc:107-246). */
+int gb_precondition(gb_ctx* ctx, int x, int y, int precision);
+/* StdMultiLevelSolver::Gmres -> GMRES::solve (Solver/stdmultilevelsolver.cc:
+ * 677-689, LinAlg/gmres.cc:159-230): x zeroed, left-preconditioned MGS-GMRES,
+ * one cycle of at most gmressize-1 steps, CGInfo stopping rule
+ * (Common/cginfo.cc:201-255). FP64 throughout (the parity variant). */
+int gb_gmres(gb_ctx* ctx, int x, int b, gb_solve_info* info);
+/* Flexible (right-preconditioned) GMRES in FP64 with the multigrid cycle run
+ * in `precision`, restarted as iterative refinement until the true relative
+ * residual ||b - A x|| / ||b|| <= tol (or maxiter Arnoldi steps). No
+ * counterpart in the reference; it replaces the same Gmres call. */
+int gb_fgmres(gb_ctx* ctx, int x, int b, int precision, gb_solve_info* info);
+/* End-to-end call with host buffers: uploads b, solves (method 0: gb_gmres,
+ * 1: gb_fgmres FP64 cycle, 2: gb_fgmres FP32 cycle), downloads x. */
+int gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x,
+                  int64_t len, gb_solve_info* info);
+
+/* ---- instrumentation ------------------------------------------------------
+ * Per-kernel-class device time of the last gb_* solve call when timing is on
+ * (CUDA events on the context stream); replaces GlobalTimer's vmult/smooth
+ * labels (Common/stopwatch.h:143-270) for the device path. */
+int gb_set_timing(gb_ctx* ctx, int on);
+int gb_get_kernel_count(const gb_ctx* ctx, int64_t* launches);
+/* Times `reps` launches of the finest-level SpMV y = A x in `precision`,
+ * writing the L2 (126 MB) flush buffer between launches when flush_l2 != 0.
+ * Returns the average launch time (ms) and the algorithmic bytes per launch. */
+int gb_bench_spmv(gb_ctx* ctx, int level, int precision, int reps,
+                  int flush_l2, double* ms_per_launch, double* bytes_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

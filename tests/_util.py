@@ -1,0 +1,63 @@
+"""Shared helpers of the test suite (fixture loading, tolerances)."""
+import glob
+import os
+
+import numpy as np
+
+from gascoignelib_b200.problem import Level, Problem, Transfer
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden_cases():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_golden(name):
+    """Returns (Problem in the reference's numbering, reference results dict)."""
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    nl = int(z["nlevels"])
+    levels, transfers = [], []
+    for l in range(nl):
+        rp = z[f"L{l}_rowptr"].astype(np.int64)
+        levels.append(Level(n=rp.shape[0] - 1, B=1, rowptr=rp,
+                            col=z[f"L{l}_col"].astype(np.int64),
+                            diag=z[f"L{l}_diag"].astype(np.int64),
+                            val=z[f"L{l}_val"],
+                            dirichlet=z[f"L{l}_dirichlet"].astype(np.int64),
+                            coord=z[f"L{l}_coord"]))
+    for l in range(nl - 1):
+        transfers.append(Transfer(c2f=z[f"T{l}_c2f"].astype(np.int64),
+                                  zweier=z[f"T{l}_zweier"].astype(np.int64),
+                                  vierer=z[f"T{l}_vierer"].astype(np.int64),
+                                  achter=z[f"T{l}_achter"].astype(np.int64)))
+    P = Problem(dim=int(z["dim"]), levels=levels, transfers=transfers,
+                rhs=z["rhs"].copy())
+    keys = {k[4:]: z[k].item() for k in z.files if k.startswith("key_")}
+    ref = {"solution": z["solution"], "iterations": int(z["iterations"]),
+           "firstresidual": float(z["firstresidual"]), "residual": float(z["residual"]),
+           "status": str(z["status"]), "keys": keys}
+    return P, ref
+
+
+def solver_keys(keys):
+    """Harness keys -> Oracle / Context.set_params keyword arguments."""
+    return dict(iterpre=int(keys.get("iterpre", 2)), iterpost=int(keys.get("iterpost", 2)),
+                iterexact=int(keys.get("iterexact", 10)),
+                omega=float(keys.get("omega", 0.8)),
+                mgomega=float(keys.get("mgomega", 1.0)),
+                mgtype=str(keys.get("mgtype", "V")))
+
+
+def rel(a, b):
+    """max |a - b| / max |b| (0 when both are zero)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    s = np.abs(b).max() if b.size else 0.0
+    d = np.abs(a - b).max() if a.size else 0.0
+    return d / s if s > 0 else d
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)

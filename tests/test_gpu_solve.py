@@ -1,0 +1,137 @@
+"""Solve-level parity of the CUDA path with the oracle and the reference.
+
+FP64 left-preconditioned GMRES (the reference's GMRES::solve semantics):
+iteration count within +-1 of the reference's and solution within 1e-8
+relative L2 of it. Flexible GMRES (FP64 or FP32 cycle, FP64 Arnoldi with
+refinement): true relative residual <= tol and solution within
+cond-scaled tolerance of the FP64 oracle solution.
+"""
+import numpy as np
+import pytest
+
+from _util import golden_cases, load_golden, rel_l2, solver_keys
+from gascoignelib_b200.native import GB_FP32, GB_FP64
+from gascoignelib_b200.problem import seeded_inputs, structured_problem
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_gmres_matches_reference_golden(ctx, name):
+    P, ref = load_golden(name)
+    keys = ref["keys"]
+    ctx.load_problem(P)
+    ctx.set_params(**solver_keys(keys), gmressize=int(keys["gmressize"]),
+                   tol=float(keys["tol"]), globaltol=1e-16, maxiter=100)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    info = ctx.gmres(x, b)
+    u = ctx.download(l, x)
+    assert abs(info["iterations"] - ref["iterations"]) <= 1
+    assert info["status_name"] == "converged"
+    assert rel_l2(u, ref["solution"]) < 1e-8
+    assert abs(info["firstresidual"] - ref["firstresidual"]) <= 1e-10 * ref["firstresidual"]
+    ctx.free(x)
+    ctx.free(b)
+
+
+@pytest.mark.parametrize("dim,coarse,refine", [(2, 2, 6), (3, 1, 5), (3, 1, 6)])
+def test_gmres_matches_oracle_structured(ctx, dim, coarse, refine):
+    """C1 (2D 128^2 Poisson-like) and C2 (3D 64^3 log-normal kappa) shapes."""
+    kappa, rhs = seeded_inputs(dim, coarse, refine)
+    if dim == 2:
+        kappa, rhs = None, None  # C1: -Laplace u = 1
+    P = structured_problem(dim, coarse, refine, kappa, rhs)
+    tol = 1e-10 if dim == 2 else 1e-8
+    O = Oracle(P)
+    xo, io = O.gmres(vmax=21, tol=tol)
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=21, tol=tol, globaltol=1e-16, maxiter=100)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    info = ctx.gmres(x, b)
+    u = ctx.download(l, x)
+    assert abs(info["iterations"] - io["iterations"]) <= 1
+    assert rel_l2(u, xo) < 1e-8
+    ctx.free(x)
+    ctx.free(b)
+
+
+@pytest.mark.parametrize("prec", [GB_FP64, GB_FP32])
+def test_flexible_gmres_reaches_true_residual(ctx, prec):
+    kappa, rhs = seeded_inputs(3, 1, 5)
+    P = structured_problem(3, 1, 5, kappa, rhs)
+    O = Oracle(P)
+    xo, io = O.gmres(vmax=21, tol=1e-12)
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=21, tol=1e-8, globaltol=1e-300, maxiter=200)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    info = ctx.fgmres(x, b, prec)
+    u = ctx.download(l, x)
+    assert info["status_name"] == "converged"
+    assert info["true_rel_residual"] <= 1e-8
+    # independent check of the residual with the oracle's FP64 product
+    r = O.matrix_residual(l, u, P.rhs)
+    assert np.linalg.norm(r) / np.linalg.norm(P.rhs) <= 1.0001e-8
+    assert rel_l2(u, xo) < 1e-6
+    ctx.free(x)
+    ctx.free(b)
+
+
+def test_solve_host_end_to_end(ctx):
+    kappa, rhs = seeded_inputs(3, 1, 4)
+    P = structured_problem(3, 1, 4, kappa, rhs)
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=21, tol=1e-8, globaltol=1e-16, maxiter=100)
+    xo, io = Oracle(P).gmres(vmax=21, tol=1e-8)
+    for method in (0, 1, 2):
+        u, info = ctx.solve_host(P.rhs, method=method)
+        assert info["status_name"] == "converged"
+        assert rel_l2(u, xo) < 1e-6
+        assert info["device_ms"] > 0
+
+
+def test_zero_rhs_and_maxiter(ctx):
+    P = structured_problem(2, 2, 3)
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=21, tol=1e-8, globaltol=1e-16, maxiter=100)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, np.zeros(P.finest.ndof))
+    info = ctx.gmres(x, b)
+    assert info["iterations"] == 0 and not ctx.download(l, x).any()
+    # maxiter: status "too many iterations" after maxiter+1 checks, as CGInfo
+    kappa, rhs = seeded_inputs(2, 2, 4)
+    P = structured_problem(2, 2, 4, kappa, rhs)
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=21, tol=1e-14, globaltol=1e-16, maxiter=3)
+    l = P.nlevels - 1
+    ctx.upload(l, b, P.rhs)
+    info = ctx.gmres(x, b)
+    xo, io = Oracle(P).gmres(vmax=21, tol=1e-14, maxiter=3)
+    assert info["status_name"] == "too many iterations"
+    assert info["iterations"] == io["iterations"]
+    assert rel_l2(ctx.download(l, x), xo) < 1e-10
+    ctx.free(x)
+    ctx.free(b)
+
+
+def test_single_level_and_small_gmres(ctx):
+    """One level (coarse smoother only) and gmressize 2 (one Arnoldi step)."""
+    P = structured_problem(2, 1, 1)
+    assert P.nlevels == 1
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=2, tol=1e-8, globaltol=1e-16, maxiter=100)
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(0, b, P.rhs)
+    info = ctx.gmres(x, b)
+    xo, io = Oracle(P).gmres(vmax=2, tol=1e-8)
+    assert info["iterations"] == io["iterations"] == 1
+    assert rel_l2(ctx.download(0, x), xo) < 1e-12
+    ctx.free(x)
+    ctx.free(b)

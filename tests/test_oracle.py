@@ -1,0 +1,134 @@
+"""The oracle (C restatement) against the reference's own results.
+
+Golden fixtures were produced by the reference's CPU solver (tests/golden/
+make_golden.py); where the compiled reference is present (oracle/_ref), more
+cases are run against it directly.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from _util import golden_cases, load_golden, rel, rel_l2, solver_keys
+from gascoignelib_b200.problem import (load_reference_dump, seeded_inputs,
+                                       structured_problem)
+from oracle.oracle import REF_HARNESS, Oracle, run_reference, write_inputs
+
+HAVE_REF = os.path.exists(REF_HARNESS)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_oracle_matches_reference_golden(name):
+    P, ref = load_golden(name)
+    O = Oracle(P, **solver_keys(ref["keys"]))
+    x, info = O.gmres(vmax=int(ref["keys"]["gmressize"]), tol=float(ref["keys"]["tol"]))
+    assert info["iterations"] == ref["iterations"]
+    assert info["status"] == ref["status"]
+    # same operations in the same order as the reference: bit-identical
+    assert np.array_equal(x, ref["solution"]), rel_l2(x, ref["solution"])
+    assert info["firstresidual"] == ref["firstresidual"]
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="compiled reference not present")
+@pytest.mark.parametrize("dim,coarse,refine", [(2, 1, 5), (3, 1, 4), (3, 2, 2)])
+def test_oracle_matches_reference_live(dim, coarse, refine):
+    kappa, rhs = seeded_inputs(dim, coarse, refine, kappa_seed=7, rhs_seed=8)
+    d = tempfile.mkdtemp()
+    out, summ = run_reference(d, dim=dim, coarse=coarse, refine=refine, dump=1,
+                              tol=1e-9, **write_inputs(d, kappa, rhs))
+    P = load_reference_dump(out)
+    x, info = Oracle(P).gmres(vmax=21, tol=1e-9)
+    assert info["iterations"] == int(summ["iterations"][0])
+    assert np.array_equal(x, np.fromfile(os.path.join(out, "solution.f64")))
+
+
+def _lex_permutation(level, N, dim):
+    idx = np.rint(level.coord * N).astype(np.int64)
+    lex = np.zeros(level.n, np.int64)
+    for d in reversed(range(dim)):
+        lex = lex * (N + 1) + idx[:, d]
+    return lex
+
+
+@pytest.mark.parametrize("name", ["q1_2d_c2_r3_seeded", "q1_3d_c1_r3_seeded",
+                                  "q1_2d_c2_r4_poisson"])
+def test_structured_generator_matches_reference_assembly(name):
+    """The synthetic generator assembles the reference's operators (same values
+    up to rounding, same sparsity, same Dirichlet and transfer maps) in
+    lexicographic numbering."""
+    import scipy.sparse as sp
+    P, ref = load_golden(name)
+    dim = P.dim
+    coarse = 2 if dim == 2 else 1
+    refine = P.nlevels
+    seeded = "seeded" in name
+    kappa, rhs = seeded_inputs(dim, coarse, refine) if seeded else (None, None)
+    G = structured_problem(dim, coarse, refine, kappa, rhs)
+    assert G.nlevels == P.nlevels
+    perms = []
+    for l in range(P.nlevels):
+        N = (2 * coarse) << l
+        lex = _lex_permutation(P.levels[l], N, dim)
+        perms.append(lex)
+        lr, lg = P.levels[l], G.levels[l]
+        rows = np.repeat(np.arange(lr.n), np.diff(lr.rowptr))
+        # permute by index arithmetic (keeps the explicit zeros of the stencil)
+        Arl = sp.coo_matrix((lr.val, (lex[rows], lex[lr.col])), shape=(lr.n, lr.n)).tocsr()
+        Arl.sort_indices()
+        assert lr.nnzb == lg.nnzb
+        assert np.array_equal(Arl.indptr, lg.rowptr) and np.array_equal(Arl.indices, lg.col)
+        assert rel(Arl.data, lg.val) < 1e-13
+        assert np.array_equal(np.sort(lex[lr.dirichlet]), np.sort(lg.dirichlet))
+    # transfers: the same (fine, coarse) couplings
+    for l, (tr, tg) in enumerate(zip(P.transfers, G.transfers)):
+        pc, pf = perms[l], perms[l + 1]
+
+        def pairs(t, mc, mf):
+            s = {(int(mf[f]), int(mc[c])) for c, f in enumerate(t.c2f)}
+            for arr in (t.zweier, t.vierer, t.achter):
+                for row in arr:
+                    s |= {(int(mf[row[0]]), int(mc[q])) for q in row[1:]}
+            return s
+        ident_c = np.arange(G.levels[l].n)
+        ident_f = np.arange(G.levels[l + 1].n)
+        assert pairs(tr, pc, pf) == pairs(tg, ident_c, ident_f)
+    # rhs and solution: same problem => same solution after permutation
+    x, info = Oracle(G).gmres(vmax=21, tol=float(ref["keys"]["tol"]))
+    xr = np.empty_like(ref["solution"])
+    xr[perms[-1]] = ref["solution"]
+    assert abs(info["iterations"] - ref["iterations"]) <= 1
+    assert rel_l2(x, xr) < 1e-8
+
+
+def test_oracle_operator_identities():
+    """Adjoint identity of the transposed product and of R = P^T."""
+    kappa, rhs = seeded_inputs(3, 1, 3)
+    P = structured_problem(3, 1, 3, kappa, rhs)
+    O = Oracle(P)
+    rng = np.random.default_rng(3)
+    fl = P.nlevels - 1
+    n = P.finest.n
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    Ax = O.vmult(fl, np.zeros(n), x)
+    ATy = O.vmult_transpose(fl, np.zeros(n), y)
+    assert abs(y @ Ax - x @ ATy) < 1e-12 * np.linalg.norm(Ax) * np.linalg.norm(y)
+    nc = P.levels[fl - 1].n
+    xc = rng.standard_normal(nc)
+    Rx = O.restrict_zero(fl - 1, x)
+    Pxc = O.prolongate_add(fl - 1, np.zeros(n), xc)
+    assert abs(xc @ Rx - x @ Pxc) < 1e-12 * np.linalg.norm(Rx) * np.linalg.norm(xc)
+
+
+def test_oracle_zero_rhs_returns_immediately():
+    P = structured_problem(2, 2, 3)
+    x, info = Oracle(P).gmres(b=np.zeros(P.finest.n))
+    assert info["reached"] == 1 and info["iterations"] == 0
+    assert not x.any()
+
+
+def test_oracle_maxiter_stops():
+    kappa, rhs = seeded_inputs(2, 2, 4)
+    P = structured_problem(2, 2, 4, kappa, rhs)
+    x, info = Oracle(P).gmres(vmax=21, tol=1e-14, maxiter=3)
+    assert info["status"] == "too many iterations" and info["iterations"] == 4
