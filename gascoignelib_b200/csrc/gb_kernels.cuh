@@ -43,66 +43,71 @@ __device__ __forceinline__ T ldg(const T* p)
   return __ldg(p);
 }
 
-// One SELL-32 row: lane `lane` of slice `s`, width w. Columns in the order
-// the reference stores them, accumulated one by one.
-template<int MODE, class TV, class TX, class TO>
+// Device view of one SELL-32 matrix. Slice s holds rows 32s..32s+31,
+// column-major: entry j of lane l at sptr[s] + 32 j + l. Column indices are
+// either explicit (col) or, when the rows of the level share few column-offset
+// patterns, implicit: row + ptab[pid[row] * W + j] (pattern-compressed SELL).
+template<class TV>
+struct SellView
+{
+  int n;
+  const int* sptr;
+  const int* col;      // explicit columns, or null
+  const uint8_t* pid;  // pattern id per row, or null
+  const int* ptab;     // [npatterns][W] offsets col - row (0-padded)
+  int W;
+  const TV* val;
+};
+
+// y = f(A x) for one row per thread, columns in the reference's stored order.
+// Loads are issued in predicated chunks of kChunk entries so that a thread keeps
+// kChunk value loads and kChunk gathers of x in flight.
+// Optional device-indexed output (flexible GMRES, graph-resident): when yidx is
+// set, y += (*yidx + 1) * ystride and x[row] is also copied to
+// xcopy + (*yidx) * ystride.
+constexpr int kChunk = 16;
+
+template<int MODE, class TV, class TX, class TO, bool PAT>
 __global__ void __launch_bounds__(kSpmvThreads)
-k_sell_spmv(int n, const int* __restrict__ sptr, const int* __restrict__ col,
-            const TV* __restrict__ val, const TX* __restrict__ x,
-            TO* __restrict__ y, const TO* __restrict__ b,
-            const TV* __restrict__ dinv, const uint8_t* __restrict__ dirmask,
-            double alpha_)
+k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
+       const TO* __restrict__ b, const TV* __restrict__ dinv,
+       const uint8_t* __restrict__ dirmask, double alpha_,
+       const int* __restrict__ yidx, int64_t ystride, TX* __restrict__ xcopy)
 {
   using TA = typename Acc<TV, TO>::type;
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n)
+  if (row >= A.n)
     return;
   const int s = row >> 5, lane = row & 31;
-  const int beg = sptr[s];
-  const int w = (sptr[s + 1] - beg) >> 5;
-  const int* cp = col + beg + lane;
-  const TV* vp = val + beg + lane;
+  const int beg = A.sptr[s];
+  const int w = (A.sptr[s + 1] - beg) >> 5;
+  const TV* vp = A.val + beg + lane;
+  const int* cp = PAT ? (A.ptab + int(A.pid[row]) * A.W) : (A.col + beg + lane);
   const TA alpha = static_cast<TA>(alpha_);
-  TA acc;
-  if (MODE == kResid || MODE == kResidDir || MODE == kJacobi)
-    acc = static_cast<TA>(b[row]);
-  else
-    acc = TA(0);
-  int j = 0;
-#pragma unroll 1
-  for (; j + 4 <= w; j += 4) {
-    const int c0 = ldg(cp + 0 * kSlice), c1 = ldg(cp + 1 * kSlice);
-    const int c2 = ldg(cp + 2 * kSlice), c3 = ldg(cp + 3 * kSlice);
-    const TA a0 = static_cast<TA>(ldg(vp + 0 * kSlice));
-    const TA a1 = static_cast<TA>(ldg(vp + 1 * kSlice));
-    const TA a2 = static_cast<TA>(ldg(vp + 2 * kSlice));
-    const TA a3 = static_cast<TA>(ldg(vp + 3 * kSlice));
-    const TA x0 = static_cast<TA>(ldg(x + c0)), x1 = static_cast<TA>(ldg(x + c1));
-    const TA x2 = static_cast<TA>(ldg(x + c2)), x3 = static_cast<TA>(ldg(x + c3));
-    if (MODE == kResid || MODE == kResidDir || MODE == kJacobi) {
-      acc = fma(-a0, x0, acc);
-      acc = fma(-a1, x1, acc);
-      acc = fma(-a2, x2, acc);
-      acc = fma(-a3, x3, acc);
-    } else {
-      acc = fma(a0, x0, acc);
-      acc = fma(a1, x1, acc);
-      acc = fma(a2, x2, acc);
-      acc = fma(a3, x3, acc);
+  constexpr bool NEG = (MODE == kResid || MODE == kResidDir || MODE == kJacobi);
+  TA acc = NEG ? static_cast<TA>(b[row]) : TA(0);
+  for (int j0 = 0; j0 < w; j0 += kChunk) {
+    TA av[kChunk], xv[kChunk];
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) {
+      const int j = j0 + q;
+      if (j < w) {
+        const int c = PAT ? row + ldg(cp + j) : ldg(cp + j * kSlice);
+        av[q] = static_cast<TA>(ldg(vp + j * kSlice));
+        xv[q] = static_cast<TA>(ldg(x + c));
+      } else {
+        av[q] = TA(0);
+        xv[q] = TA(0);
+      }
     }
-    cp += 4 * kSlice;
-    vp += 4 * kSlice;
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q)
+      acc = NEG ? fma(-av[q], xv[q], acc) : fma(av[q], xv[q], acc);
   }
-  for (; j < w; ++j) {
-    const int c0 = ldg(cp);
-    const TA a0 = static_cast<TA>(ldg(vp));
-    const TA x0 = static_cast<TA>(ldg(x + c0));
-    if (MODE == kResid || MODE == kResidDir || MODE == kJacobi)
-      acc = fma(-a0, x0, acc);
-    else
-      acc = fma(a0, x0, acc);
-    cp += kSlice;
-    vp += kSlice;
+  if (yidx) {
+    const int64_t jj = *yidx;
+    xcopy[jj * ystride + row] = x[row];
+    y += (jj + 1) * ystride;
   }
   if (MODE == kAx) {
     y[row] = static_cast<TO>(alpha * acc);
@@ -139,7 +144,8 @@ constexpr uint32_t kIdxMask = (1u << kWShift) - 1u;
 template<class T>
 __device__ __forceinline__ T wcode(uint32_t e)
 {
-  return static_cast<T>(1.0) / static_cast<T>(1u << (e >> kWShift));
+  const uint32_t c = e >> kWShift;
+  return c == 0 ? T(1) : c == 1 ? T(0.5) : c == 2 ? T(0.25) : T(0.125);
 }
 
 // coarse = R fine (gather over the coarse row, ascending fine index, as
@@ -459,6 +465,13 @@ struct GmresDev
   double bnorm, beta, xnorm;
   CGInfoDev info;
   int reached, need_reortho, zero_rho, pad;
+  // graph-resident flexible GMRES
+  double d2[kMaxV + 1];       // second CGS pass coefficients
+  double beta_tmp;            // ||r|| of the current restart
+  int j;                      // Arnoldi step of the current cycle
+  int total;                  // Arnoldi steps over all cycles
+  int restarts;               // refinement cycles started
+  int stop, converged, pad2;
 };
 
 // CGInfo::check (Common/cginfo.cc:201-255); "diverging" cannot fire there.
@@ -575,6 +588,250 @@ k_fgmres_restart(GmresDev* G, const double* beta_p, int vmax)
   G->inv = 1.0 / beta;
   G->zero_rho = (beta == 0.0);
   G->reached = 0;
+}
+
+// ------------------------------------------- graph-resident flexible GMRES
+//
+// The whole flexible GMRES solve is one CUDA graph: a conditional WHILE node runs
+// the refinement cycles, a nested one the Arnoldi steps. Loop indices live in
+// GmresDev; kernels read them, so the graph needs no host round trip.
+
+constexpr int kCgsMaxJ = 32; // graph path: gmressize <= 33
+
+__global__ void
+k_fg_setup(GmresDev* G, double tol, double globaltol, int maxiter)
+{
+  G->info.tol = tol;
+  G->info.globaltol = globaltol;
+  G->info.maxiter = maxiter;
+  G->info.status = 1;
+  G->info.iteration = 0;
+  G->info.residual = 0;
+  G->total = 0;
+  G->restarts = 0;
+  G->j = 0;
+  G->stop = 0;
+  G->converged = 0;
+}
+
+// Refinement cycle start: beta = ||b - A x|| (in beta_tmp). Stops both loops
+// when converged, out of iterations or non-finite; otherwise resets the
+// Hessenberg system of the cycle.
+__global__ void
+k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
+             cudaGraphConditionalHandle inner, int m, int maxrestarts)
+{
+  const double beta = G->beta_tmp;
+  const double aim = fmax(G->info.tol * G->bnorm, G->info.globaltol);
+  const int conv = (beta <= aim) || beta == 0.0;
+  const int stop = conv || G->total >= G->info.maxiter ||
+                   G->restarts >= maxrestarts || !(beta == beta);
+  G->converged = conv;
+  G->j = 0;
+  if (G->restarts == 0)
+    G->info.firstresidual = beta;
+  G->info.residual = beta;
+  if (stop) {
+    G->stop = 1;
+    G->inv = 0.0;
+    G->info.status = conv ? 2 : 3;
+    cudaGraphSetConditional(outer, 0);
+    cudaGraphSetConditional(inner, 0);
+    return;
+  }
+  for (int c = 0; c < m; ++c) {
+    for (int r = 0; r <= m; ++r)
+      G->H[c][r] = 0.0;
+    G->ci[c] = 0.0;
+    G->si[c] = 0.0;
+  }
+  for (int r = 0; r <= m; ++r)
+    G->gamma[r] = 0.0;
+  G->gamma[0] = beta;
+  G->beta = beta;
+  G->inv = 1.0 / beta;
+  G->restarts += 1;
+  cudaGraphSetConditional(inner, 1);
+}
+
+// y = (TO) V[(*jp) * n + i]   (Arnoldi vector j into the cycle's right-hand side)
+template<class TO>
+__global__ void
+k_load_idx(int64_t n, TO* __restrict__ y, const double* __restrict__ V,
+           const int* __restrict__ jp)
+{
+  const double* v = V + int64_t(*jp) * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = static_cast<TO>(v[i]);
+}
+
+// V[(*jp) * n + i] *= *s
+__global__ void
+k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
+            const double* __restrict__ sp)
+{
+  double* v = V + int64_t(*jp) * n;
+  const double s = *sp;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = s * v[i];
+}
+
+// Classical Gram-Schmidt, twice (CGS2), on w = V_{j+1} against V_0..V_j, j = G->j:
+//  MODE 0: c1[i] = <w, V_i>;                         H[j][i]  = c1[i]
+//  MODE 1: w -= sum_i c1[i] V_i; c2[i] = <w, V_i>;   H[j][i] += c2[i]
+//  MODE 2: w -= sum_i c2[i] V_i; s = ||w||;          H[j][j+1] = s
+// Each pass reads the j+1 basis vectors once; accumulators stay in registers;
+// reductions are deterministic (fixed grid, fixed order).
+template<int MODE>
+__global__ void __launch_bounds__(kRedThreads)
+k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
+      unsigned* ticket)
+{
+  __shared__ double s_coef[kCgsMaxJ];
+  __shared__ double s_red[kRedThreads / 32][kCgsMaxJ];
+  __shared__ bool am_last;
+  const int j = G->j;
+  const int nv = j + 1;
+  double* w = V + int64_t(j + 1) * n;
+  if (MODE >= 1 && threadIdx.x < kCgsMaxJ)
+    s_coef[threadIdx.x] = (threadIdx.x < nv) ? (MODE == 1 ? G->d[threadIdx.x]
+                                                          : G->d2[threadIdx.x])
+                                             : 0.0;
+  __syncthreads();
+  double acc[kCgsMaxJ];
+#pragma unroll
+  for (int i = 0; i < kCgsMaxJ; ++i)
+    acc[i] = 0.0;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    double t = w[r];
+    if (MODE >= 1) {
+#pragma unroll
+      for (int i = 0; i < kCgsMaxJ; ++i)
+        if (i < nv)
+          t = fma(-s_coef[i], V[int64_t(i) * n + r], t);
+      w[r] = t;
+    }
+    if (MODE <= 1) {
+#pragma unroll
+      for (int i = 0; i < kCgsMaxJ; ++i)
+        if (i < nv)
+          acc[i] = fma(t, V[int64_t(i) * n + r], acc[i]);
+    } else {
+      acc[0] = fma(t, t, acc[0]);
+    }
+  }
+  const int nred = (MODE == 2) ? 1 : nv;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < kCgsMaxJ; ++i) {
+    if (i < nred) {
+      double v = acc[i];
+      for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0)
+        s_red[wid][i] = v;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < nred) {
+    double v = 0.0;
+    for (int q = 0; q < kRedThreads / 32; ++q)
+      v += s_red[q][threadIdx.x];
+    partials[int64_t(threadIdx.x) * gridDim.x + blockIdx.x] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0)
+    am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!am_last)
+    return;
+  __threadfence();
+  if (threadIdx.x < nred) {
+    double v = 0.0;
+    for (int q = 0; q < (int)gridDim.x; ++q)
+      v += __ldcg(partials + int64_t(threadIdx.x) * gridDim.x + q);
+    const int i = threadIdx.x;
+    if (MODE == 0) {
+      G->d[i] = v;
+      G->H[j][i] = v;
+    } else if (MODE == 1) {
+      G->d2[i] = v;
+      G->H[j][i] += v;
+    } else {
+      const double sv = sqrt(v);
+      G->H[j][j + 1] = sv;
+      G->s = sv;
+    }
+  }
+  if (threadIdx.x == 0)
+    *ticket = 0u;
+}
+
+// Givens update of column j (LinAlg/gmres.cc:88-104 applied to the flexible
+// Hessenberg), residual estimate |gamma[j+1]| = ||b - A x_j|| in exact
+// arithmetic, then j += 1 and the inner loop condition.
+__global__ void
+k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m)
+{
+  const int last = G->j, dim = last + 1;
+  double* h = G->H[last];
+  const double s = h[dim];
+  G->inv = 1.0 / s;
+  for (int i = 0; i < last; i++) {
+    double dummy = h[i];
+    h[i] = G->ci[i] * dummy + G->si[i] * h[i + 1];
+    h[i + 1] = -G->si[i] * dummy + G->ci[i] * h[i + 1];
+  }
+  double r = 1. / sqrt(h[last] * h[last] + h[last + 1] * h[last + 1]);
+  G->si[last] = h[last + 1] * r;
+  G->ci[last] = h[last] * r;
+  h[last] = G->ci[last] * h[last] + G->si[last] * h[last + 1];
+  G->gamma[last + 1] = -G->si[last] * G->gamma[last];
+  G->gamma[last] *= G->ci[last];
+  const double rho = fabs(G->gamma[dim]);
+  if (G->total < kMaxV)
+    G->hist[G->total] = rho;
+  G->info.residual = rho;
+  G->info.iteration += 1;
+  G->total += 1;
+  G->j = dim;
+  const double aim = fmax(G->info.tol * G->bnorm, G->info.globaltol);
+  const int reached = (rho <= aim) || dim >= m || G->total >= G->info.maxiter ||
+                      !(rho == rho);
+  cudaGraphSetConditional(inner, reached ? 0 : 1);
+}
+
+// hs = H^-1 gamma on the first G->j columns (Common/mult.h:130-141)
+__global__ void
+k_fg_backward(GmresDev* G)
+{
+  const int dim = G->j;
+  for (int i = dim - 1; i >= 0; i--) {
+    double s = G->gamma[i];
+    for (int jj = i + 1; jj < dim; jj++)
+      s -= G->hs[jj] * G->H[jj][i];
+    G->hs[i] = s / G->H[i][i];
+  }
+}
+
+// x += sum_{q < G->j} hs[q] Z_q
+template<class TZ>
+__global__ void
+k_fg_update(int64_t n, double* __restrict__ x, const TZ* __restrict__ Z,
+            const GmresDev* __restrict__ G)
+{
+  const int k = G->j;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double acc = x[i];
+    for (int q = 0; q < k; ++q)
+      acc = fma(G->hs[q], static_cast<double>(Z[int64_t(q) * n + i]), acc);
+    x[i] = acc;
+  }
 }
 
 } // namespace gb

@@ -110,7 +110,65 @@ struct Sell
   DeviceArray<int> sptr, col;
   DeviceArray<double> v64;
   DeviceArray<float> v32;
+  // pattern-compressed form: row r's columns are r + ptab[pid[r]*W + j]
+  bool pat = false;
+  int npat = 0, W = 0;
+  DeviceArray<uint8_t> pid;
+  DeviceArray<int> ptab;
 };
+
+template<class TV>
+static SellView<TV>
+view(const Sell& S, const TV* val)
+{
+  return SellView<TV>{ S.n, S.sptr.p, S.pat ? nullptr : S.col.p,
+                       S.pat ? S.pid.p : nullptr, S.pat ? S.ptab.p : nullptr,
+                       S.W, val };
+}
+
+// Rows whose column lists, relative to the row, coincide share one pattern. A
+// level uses the compressed form when it has at most 256 patterns.
+static void
+build_patterns(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
+               cudaStream_t st)
+{
+  S.pat = false;
+  int64_t W = 0;
+  for (int64_t r = 0; r < n; ++r)
+    W = std::max<int64_t>(W, rowptr[r + 1] - rowptr[r]);
+  std::map<std::vector<int>, int> dict;
+  std::vector<uint8_t> pid(n);
+  std::vector<int> key;
+  for (int64_t r = 0; r < n; ++r) {
+    key.clear();
+    for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+      int64_t d = col[k] - r;
+      if (d < INT32_MIN || d > INT32_MAX)
+        return;
+      key.push_back(static_cast<int>(d));
+    }
+    auto it = dict.find(key);
+    if (it == dict.end()) {
+      if (dict.size() >= 256)
+        return;
+      it = dict.emplace(key, static_cast<int>(dict.size())).first;
+    }
+    pid[r] = static_cast<uint8_t>(it->second);
+  }
+  std::vector<int> tab(dict.size() * W, 0);
+  for (auto& kv : dict)
+    for (size_t j = 0; j < kv.first.size(); ++j)
+      tab[kv.second * W + j] = kv.first[j];
+  GB_CUDA(S.pid.alloc(n));
+  GB_CUDA(S.ptab.alloc(std::max<size_t>(tab.size(), 1)));
+  GB_CUDA(cudaMemcpyAsync(S.pid.p, pid.data(), n, cudaMemcpyHostToDevice, st));
+  GB_CUDA(cudaMemcpyAsync(S.ptab.p, tab.data(), tab.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, st));
+  GB_CUDA(cudaStreamSynchronize(st));
+  S.npat = static_cast<int>(dict.size());
+  S.W = static_cast<int>(W);
+  S.pat = true;
+}
 
 static void
 build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
@@ -171,6 +229,7 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
   }
   // host vectors must outlive the async copies
   GB_CUDA(cudaStreamSynchronize(st));
+  build_patterns(S, n, rowptr, col, st);
 }
 
 template<class T>
@@ -244,6 +303,26 @@ struct gb_ctx
   int64_t launches = 0;
   gb::DeviceArray<unsigned char> flush;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // graph-resident flexible GMRES, one per cycle precision
+  int64_t version = 0; // bumped by every change of levels, transfers or keys
+  struct FGraph
+  {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t version = -1;
+    int setup_k = 0, outer_k = 0, inner_k = 0;
+  } fg[2];
+  gb::DeviceArray<double> xg, bg, rhs64, zfix64;
+  gb::DeviceArray<float> rhs32, zfix32;
+  ~gb_ctx()
+  {
+    for (auto& g : fg) {
+      if (g.exec)
+        cudaGraphExecDestroy(g.exec);
+      if (g.graph)
+        cudaGraphDestroy(g.graph);
+    }
+  }
 };
 
 namespace gb {
@@ -342,11 +421,18 @@ read_scalar(Context& c, const double* dptr)
 template<int MODE, class TV, class TX, class TO>
 static void
 spmv(Context& c, const Level& L, const Sell& S, const TX* x, TO* y, const TO* b,
-     const TV* dinv, double alpha)
+     const TV* dinv, double alpha, const int* yidx = nullptr, int64_t ystride = 0,
+     TX* xcopy = nullptr)
 {
-  launch(c, k_sell_spmv<MODE, TV, TX, TO>, blocks_for(S.n, kSpmvThreads),
-         kSpmvThreads, S.n, S.sptr.p, S.col.p, sell_vals<TV>(S), x, y, b, dinv,
-         L.dirmask.p, alpha);
+  const SellView<TV> A = view<TV>(S, sell_vals<TV>(S));
+  if (S.pat)
+    launch(c, k_spmv<MODE, TV, TX, TO, true>, blocks_for(S.n, kSpmvThreads),
+           kSpmvThreads, A, x, y, b, dinv, (const uint8_t*)L.dirmask.p, alpha, yidx,
+           ystride, xcopy);
+  else
+    launch(c, k_spmv<MODE, TV, TX, TO, false>, blocks_for(S.n, kSpmvThreads),
+           kSpmvThreads, A, x, y, b, dinv, (const uint8_t*)L.dirmask.p, alpha, yidx,
+           ystride, xcopy);
 }
 
 template<class T>
@@ -773,6 +859,214 @@ gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* 
   return converged ? GB_OK : GB_ENOTCONV;
 }
 
+
+// ------------------------------------------------ graph-resident flexible GMRES
+
+template<class T>
+static MgWork<T>& work(Context& c);
+template<>
+MgWork<double>& work<double>(Context& c)
+{
+  return c.w64;
+}
+template<>
+MgWork<float>& work<float>(Context& c)
+{
+  return c.w32;
+}
+
+static std::vector<cudaGraphNode_t>
+leaf_nodes(cudaGraph_t g)
+{
+  size_t nn = 0, ne = 0;
+  GB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn)
+    GB_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  GB_CUDA(cudaGraphGetEdges(g, nullptr, nullptr, &ne));
+  std::vector<cudaGraphNode_t> from(ne), to(ne);
+  if (ne)
+    GB_CUDA(cudaGraphGetEdges(g, from.data(), to.data(), &ne));
+  std::vector<cudaGraphNode_t> leaves;
+  for (auto nd : nodes)
+    if (std::find(from.begin(), from.end(), nd) == from.end())
+      leaves.push_back(nd);
+  return leaves;
+}
+
+static cudaGraph_t
+add_while(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
+          cudaGraphConditionalHandle h, cudaGraphNode_t* node)
+{
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  GB_CUDA(cudaGraphAddNode(node, g, deps.empty() ? nullptr : deps.data(), deps.size(),
+                           &cp));
+  return cp.conditional.phGraph_out[0];
+}
+
+// Builds the one-graph solve: setup; WHILE(refine) { r = b - A x; beta; restart;
+// v0 = r / beta; WHILE(arnoldi) { z = M v_j (cycle in T); v_{j+1} = A z; CGS2;
+// Givens } ; y = H^-1 gamma; x += Z y }. Operates on the context's xg/bg.
+template<class T>
+static void
+build_fgraph(Context& c, int prec)
+{
+  ensure_work(c);
+  const int vmax = c.params.gmressize;
+  const int m = vmax - 1;
+  GB_REQUIRE(m + 1 <= kCgsMaxJ, GB_EINVAL, "graph solver needs gmressize <= 33");
+  const int fl = c.nlevels - 1;
+  Level& L = c.L[fl];
+  const int64_t n = L.ndof();
+  GB_CUDA(c.krylov.alloc((vmax + 1) * n));
+  GB_CUDA(c.pbuf.alloc(n));
+  if (!c.G.p)
+    GB_CUDA(c.G.alloc(1));
+  GB_CUDA(c.xg.alloc(n));
+  GB_CUDA(c.bg.alloc(n));
+  T* Z;
+  T* zfix;
+  T* rhs;
+  if (prec == GB_FP32) {
+    GB_CUDA(c.zb32.alloc(vmax * n));
+    GB_CUDA(c.zfix32.alloc(n));
+    GB_CUDA(c.rhs32.alloc(n));
+    Z = reinterpret_cast<T*>(c.zb32.p);
+    zfix = reinterpret_cast<T*>(c.zfix32.p);
+    rhs = reinterpret_cast<T*>(c.rhs32.p);
+  } else {
+    GB_CUDA(c.zb64.alloc(vmax * n));
+    GB_CUDA(c.zfix64.alloc(n));
+    GB_CUDA(c.rhs64.alloc(n));
+    Z = reinterpret_cast<T*>(c.zb64.p);
+    zfix = reinterpret_cast<T*>(c.zfix64.p);
+    rhs = reinterpret_cast<T*>(c.rhs64.p);
+  }
+  MgWork<T>& W = work<T>(c);
+  auto& F = c.fg[prec];
+  if (F.exec) {
+    cudaGraphExecDestroy(F.exec);
+    F.exec = nullptr;
+  }
+  if (F.graph) {
+    cudaGraphDestroy(F.graph);
+    F.graph = nullptr;
+  }
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  GmresDev* G = c.G.p;
+  double* V = c.krylov.p;
+  double* x = c.xg.p;
+  const double* b = c.bg.p;
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+  cudaGraph_t top;
+  GB_CUDA(cudaGraphCreate(&top, 0));
+  F.graph = top;
+  // each conditional handle belongs to the graph that holds its node
+  cudaGraphConditionalHandle hOuter, hInner;
+  GB_CUDA(cudaGraphConditionalHandleCreate(&hOuter, top, 1, cudaGraphCondAssignDefault));
+  const int maxrestarts = 50;
+  const int64_t k_start = c.launches;
+  int64_t k0 = c.launches;
+  // setup
+  GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, top, nullptr, nullptr, 0, mode));
+  launch(c, k_fg_setup, 1, 1, G, c.params.tol, c.params.globaltol, c.params.maxiter);
+  dot_dev(c, n, b, b, RedOut{ &G->bnorm, nullptr, nullptr, 1 });
+  launch(c, k_fill<double>, stream_blocks(n), 256, n, x, 0.0);
+  GB_CUDA(cudaStreamEndCapture(c.stream, &top));
+  F.setup_k = static_cast<int>(c.launches - k0);
+  cudaGraphNode_t outerNode, innerNode;
+  cudaGraph_t outerBody = add_while(top, leaf_nodes(top), hOuter, &outerNode);
+  GB_CUDA(cudaGraphConditionalHandleCreate(&hInner, outerBody, 0,
+                                           cudaGraphCondAssignDefault));
+  // refinement cycle start
+  k0 = c.launches;
+  GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, outerBody, nullptr, nullptr, 0, mode));
+  spmv<kResidDir, double, double, double>(c, L, L.A, (const double*)x, V, b, nullptr,
+                                          0.0);
+  dot_dev(c, n, V, V, RedOut{ &G->beta_tmp, nullptr, nullptr, 1 });
+  launch(c, k_fg_restart, 1, 1, G, hOuter, hInner, m, maxrestarts);
+  launch(c, k_scale_dev, stream_blocks(n), 256, n, V, (const double*)&G->inv);
+  GB_CUDA(cudaStreamEndCapture(c.stream, &outerBody));
+  cudaGraph_t innerBody = add_while(outerBody, leaf_nodes(outerBody), hInner, &innerNode);
+  // Arnoldi step
+  int64_t k1 = c.launches;
+  GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, innerBody, nullptr, nullptr, 0, mode));
+  launch(c, k_load_idx<T>, stream_blocks(n), 256, n, rhs, (const double*)V,
+         (const int*)&G->j);
+  precondition_T<T>(c, W, zfix, rhs, true);
+  spmv<kAx, double, T, double>(c, L, L.A, (const T*)zfix, V, nullptr, nullptr, 1.0,
+                               (const int*)&G->j, n, Z);
+  const int rg = red_blocks(n);
+  launch(c, k_cgs<0>, rg, kRedThreads, n, V, G, c.partials.p, c.ticket.p);
+  launch(c, k_cgs<1>, rg, kRedThreads, n, V, G, c.partials.p, c.ticket.p);
+  launch(c, k_cgs<2>, rg, kRedThreads, n, V, G, c.partials.p, c.ticket.p);
+  launch(c, k_fg_step, 1, 1, G, hInner, m);
+  launch(c, k_scale_idx, stream_blocks(n), 256, n, V, (const int*)&G->j,
+         (const double*)&G->inv);
+  GB_CUDA(cudaStreamEndCapture(c.stream, &innerBody));
+  F.inner_k = static_cast<int>(c.launches - k1);
+  // cycle end: x += Z H^-1 gamma
+  int64_t k2 = c.launches;
+  GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, outerBody, &innerNode, nullptr, 1, mode));
+  launch(c, k_fg_backward, 1, 1, G);
+  launch(c, k_fg_update<T>, stream_blocks(n), 256, n, x, (const T*)Z, (const GmresDev*)G);
+  GB_CUDA(cudaStreamEndCapture(c.stream, &outerBody));
+  F.outer_k = static_cast<int>(k1 - k0) + static_cast<int>(c.launches - k2);
+  c.launches = k_start; // capture executes nothing; executions are counted per solve
+  GB_CUDA(cudaGraphInstantiate(&F.exec, top, 0));
+  F.version = c.version;
+}
+
+// Runs the graph on b (device), result into x (device); info as gb_fgmres.
+static int
+fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* info,
+             bool copy_in = true, bool copy_out = true)
+{
+  auto& F = c.fg[prec];
+  if (!F.exec || F.version != c.version) {
+    if (prec == GB_FP32)
+      build_fgraph<float>(c, prec);
+    else
+      build_fgraph<double>(c, prec);
+  }
+  const int64_t n = c.L[c.nlevels - 1].ndof();
+  if (copy_in && b != c.bg.p)
+    GB_CUDA(cudaMemcpyAsync(c.bg.p, b, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c.stream));
+  GB_CUDA(cudaEventRecord(c.ev0, c.stream));
+  GB_CUDA(cudaGraphLaunch(F.exec, c.stream));
+  GB_CUDA(cudaEventRecord(c.ev1, c.stream));
+  if (copy_out && x != c.xg.p)
+    GB_CUDA(cudaMemcpyAsync(x, c.xg.p, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c.stream));
+  int cnt[3];
+  GB_CUDA(cudaMemcpyAsync(cnt, &c.G.p->total, 3 * sizeof(int), cudaMemcpyDeviceToHost,
+                          c.stream));
+  int conv = 0;
+  GB_CUDA(cudaMemcpyAsync(&conv, &c.G.p->converged, sizeof(int), cudaMemcpyDeviceToHost,
+                          c.stream));
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  float ms = 0;
+  GB_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+  const int total = cnt[0], restarts = cnt[1];
+  const int64_t kernels = F.setup_k + int64_t(restarts + 1) * F.outer_k +
+                          int64_t(total) * F.inner_k;
+  c.launches += kernels;
+  if (info) {
+    fill_info(c, info, c.xg.p, c.bg.p);
+    info->iterations = total;
+    info->restarts = restarts;
+    info->status = conv ? 2 : 3;
+    info->kernel_launches = static_cast<int>(kernels);
+    info->device_ms = ms;
+  }
+  return conv ? GB_OK : GB_ENOTCONV;
+}
+
 } // namespace gb
 
 // ==================================================================== C-ABI
@@ -814,7 +1108,7 @@ gb_ctx_create(gb_ctx** out, int device)
     GB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     GB_CUDA(cudaEventCreate(&ctx->ev0));
     GB_CUDA(cudaEventCreate(&ctx->ev1));
-    GB_CUDA(ctx->partials.alloc(kMaxRedBlocks));
+    GB_CUDA(ctx->partials.alloc(size_t(kCgsMaxJ + 1) * kMaxRedBlocks));
     GB_CUDA(ctx->ticket.alloc(1));
     GB_CUDA(cudaMemset(ctx->ticket.p, 0, sizeof(unsigned)));
     GB_CUDA(ctx->scal.alloc(16));
@@ -868,6 +1162,7 @@ int
 gb_set_params(gb_ctx* ctx, const gb_params* p)
 {
   GB_API_BEGIN
+  ctx->version++;
   GB_REQUIRE(p, GB_EINVAL, "null params");
   GB_REQUIRE(p->iterpre >= 0 && p->iterpost >= 0 && p->iterexact >= 0, GB_EINVAL,
              "negative sweep count");
@@ -893,6 +1188,7 @@ int
 gb_set_nlevels(gb_ctx* ctx, int nlevels)
 {
   GB_API_BEGIN
+  ctx->version++;
   GB_REQUIRE(nlevels >= 1 && nlevels <= 32, GB_EINVAL, "nlevels out of range [1, 32]");
   GB_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->nlevels = nlevels;
@@ -911,6 +1207,7 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
                     const int64_t* col, const int64_t* diag, const double* val)
 {
   GB_API_BEGIN
+  ctx->version++;
   Level& L = level(*ctx, lvl);
   GB_REQUIRE(B == 1, GB_EINVAL, "only block size 1 is supported by this build");
   GB_REQUIRE(n >= 1 && n < (int64_t(1) << 29), GB_EINVAL, "n out of range");
@@ -961,6 +1258,7 @@ gb_level_set_dirichlet(gb_ctx* ctx, int lvl, int64_t nnodes, const int64_t* node
                        int comp_mask)
 {
   GB_API_BEGIN
+  ctx->version++;
   Level& L = level_with_matrix(*ctx, lvl);
   GB_REQUIRE(nnodes >= 0 && (nnodes == 0 || nodes), GB_EINVAL, "bad node list");
   std::vector<uint8_t> mask(L.ndof(), 0);
@@ -992,6 +1290,7 @@ gb_level_set_transfer(gb_ctx* ctx, int lvl, int64_t ncoarse, const int64_t* c2f,
                       const int64_t* vierer, int64_t na, const int64_t* achter)
 {
   GB_API_BEGIN
+  ctx->version++;
   GB_REQUIRE(lvl >= 0 && lvl + 1 < ctx->nlevels, GB_EINVAL, "transfer level out of range");
   Level& Lc = level_with_matrix(*ctx, lvl);
   Level& Lf = level_with_matrix(*ctx, lvl + 1);
@@ -1376,6 +1675,8 @@ gb_fgmres(gb_ctx* ctx, int x, int b, int precision, gb_solve_info* info)
   const int fl = ctx->nlevels - 1;
   GB_REQUIRE(fl >= 0, GB_ESTATE, "no levels");
   ensure_work(*ctx);
+  if (ctx->params.gmressize <= kCgsMaxJ)
+    return fgmres_graph(*ctx, vec(*ctx, fl, x), vec(*ctx, fl, b), precision, info);
   return gmres_flexible(*ctx, vec(*ctx, fl, x), vec(*ctx, fl, b), precision, info);
   GB_API_END
 }
@@ -1407,6 +1708,8 @@ gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x, int64_t len,
   int rc;
   if (method == 0)
     rc = gmres_left(*ctx, xd, bd, info);
+  else if (ctx->params.gmressize <= kCgsMaxJ)
+    rc = fgmres_graph(*ctx, xd, bd, method == 1 ? GB_FP64 : GB_FP32, info);
   else
     rc = gmres_flexible(*ctx, xd, bd, method == 1 ? GB_FP64 : GB_FP32, info);
   GB_CUDA(cudaMemcpyAsync(x, xd, len * sizeof(double), cudaMemcpyDeviceToHost,

@@ -1,0 +1,59 @@
+"""Fixed workloads for profiling runs (ncu launch lists and kernel captures).
+
+    python -m gascoignelib_b200.workload --method mixed --solves 2 [--refine 6]
+    python -m gascoignelib_b200.workload --spmv 3 [--precision fp64]
+
+--method: mixed (FP32 cycle, flexible FP64 GMRES), fp64 (FP64 cycle, flexible),
+left (reference-semantics left-preconditioned FP64 GMRES). --spmv K runs only K
+finest-level SpMV launches (L2 flushed before each) after the set-up.
+The problem is the seeded 3D Q1 diffusion problem (refine 6: 64^3 cells).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--method", default="mixed", choices=["mixed", "fp64", "left"])
+    ap.add_argument("--solves", type=int, default=2)
+    ap.add_argument("--refine", type=int, default=6)
+    ap.add_argument("--spmv", type=int, default=0)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    a = ap.parse_args(argv)
+
+    from gascoignelib_b200.build import build_library
+    from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
+    from gascoignelib_b200.problem import seeded_inputs, structured_problem
+
+    build_library()
+    kappa, rhs = seeded_inputs(3, 1, a.refine)
+    P = structured_problem(3, 1, a.refine, kappa, rhs)
+    with Context(0) as ctx:
+        ctx.load_problem(P)
+        ctx.set_params(gmressize=21, tol=1e-8, globaltol=1e-300, maxiter=200,
+                       iterpre=2, iterpost=2, omega=0.8)
+        fl = P.nlevels - 1
+        if a.spmv:
+            prec = GB_FP32 if a.precision == "fp32" else GB_FP64
+            ms, by = ctx.bench_spmv(fl, prec, reps=a.spmv, flush_l2=True)
+            print(json.dumps({"spmv_ms": ms, "bytes": by, "GBps": by / ms / 1e6}))
+            return
+        x, b = ctx.vec(), ctx.vec()
+        ctx.upload(fl, b, P.rhs)
+        for _ in range(a.solves):
+            if a.method == "left":
+                info = ctx.gmres(x, b)
+            else:
+                info = ctx.fgmres(x, b, GB_FP32 if a.method == "mixed" else GB_FP64)
+            print(json.dumps({k: info[k] for k in ("iterations", "restarts", "device_ms",
+                                                   "true_rel_residual", "kernel_launches")}))
+
+
+if __name__ == "__main__":
+    main()
