@@ -91,6 +91,7 @@ _SIGS = {
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
     "gb_bench_spmv": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
+    "gb_dot_noalloc": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
 }
 
 

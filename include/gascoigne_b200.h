@@ -205,6 +205,25 @@ int gb_get_kernel_count(const gb_ctx* ctx, int64_t* launches);
 int gb_bench_spmv(gb_ctx* ctx, int level, int precision, int reps,
                   int flush_l2, double* ms_per_launch, double* bytes_per_launch);
 
+/* ---- allocation-free dot product -----------------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory: code running while a CUDA stream is being captured into a graph
+ * (cudaMalloc is not capturable), applications that hand all device memory
+ * to their own pool up front, and host callbacks that must not allocate.
+ * Computes *out = <a, b> over n doubles; a, b and out are device pointers
+ * the caller owns; work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * default stream). It allocates nothing: its reduction scratch is a
+ * file-scope device array of 4096 partial sums (32 KiB) that every GPU which
+ * loads this library keeps until the process exits, so n is limited to
+ * 4096 * 2048 = 8,388,608; larger n returns GB_EINVAL. The first call on a
+ * device looks up that array's device address and should come before any
+ * stream capture. Calls share the array: two calls that overlap on the GPU
+ * (other streams, other host threads) race and give wrong sums. Same
+ * deterministic reduction as gb_vec_dot; for n <= 606,208 the two use the
+ * same partition and return the same bits. */
+int gb_dot_noalloc(const double* a, const double* b, int64_t n, double* out,
+                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif
