@@ -43,6 +43,48 @@ __device__ __forceinline__ T ldg(const T* p)
   return __ldg(p);
 }
 
+// Eight independent read-only loads issued back to back from one asm block, so
+// that a thread keeps all eight in flight (kernels with few threads per SM,
+// where a serial chain of loads would set the time).
+__device__ __forceinline__ void
+ld8(double (&v)[8], const double* const (&p)[8])
+{
+  asm volatile("{\n\t"
+               "ld.global.nc.f64 %0, [%8];\n\tld.global.nc.f64 %1, [%9];\n\t"
+               "ld.global.nc.f64 %2, [%10];\n\tld.global.nc.f64 %3, [%11];\n\t"
+               "ld.global.nc.f64 %4, [%12];\n\tld.global.nc.f64 %5, [%13];\n\t"
+               "ld.global.nc.f64 %6, [%14];\n\tld.global.nc.f64 %7, [%15];\n\t}"
+               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]), "=d"(v[4]), "=d"(v[5]),
+                 "=d"(v[6]), "=d"(v[7])
+               : "l"(p[0]), "l"(p[1]), "l"(p[2]), "l"(p[3]), "l"(p[4]), "l"(p[5]),
+                 "l"(p[6]), "l"(p[7]));
+}
+__device__ __forceinline__ void
+ld8(float (&v)[8], const float* const (&p)[8])
+{
+  asm volatile("{\n\t"
+               "ld.global.nc.f32 %0, [%8];\n\tld.global.nc.f32 %1, [%9];\n\t"
+               "ld.global.nc.f32 %2, [%10];\n\tld.global.nc.f32 %3, [%11];\n\t"
+               "ld.global.nc.f32 %4, [%12];\n\tld.global.nc.f32 %5, [%13];\n\t"
+               "ld.global.nc.f32 %6, [%14];\n\tld.global.nc.f32 %7, [%15];\n\t}"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+                 "=f"(v[6]), "=f"(v[7])
+               : "l"(p[0]), "l"(p[1]), "l"(p[2]), "l"(p[3]), "l"(p[4]), "l"(p[5]),
+                 "l"(p[6]), "l"(p[7]));
+}
+__device__ __forceinline__ void
+ld8(uint32_t (&v)[8], const uint32_t* const (&p)[8])
+{
+  asm volatile("{\n\t"
+               "ld.global.nc.u32 %0, [%8];\n\tld.global.nc.u32 %1, [%9];\n\t"
+               "ld.global.nc.u32 %2, [%10];\n\tld.global.nc.u32 %3, [%11];\n\t"
+               "ld.global.nc.u32 %4, [%12];\n\tld.global.nc.u32 %5, [%13];\n\t"
+               "ld.global.nc.u32 %6, [%14];\n\tld.global.nc.u32 %7, [%15];\n\t}"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                 "=r"(v[6]), "=r"(v[7])
+               : "l"(p[0]), "l"(p[1]), "l"(p[2]), "l"(p[3]), "l"(p[4]), "l"(p[5]),
+                 "l"(p[6]), "l"(p[7]));
+}
 // Device view of one SELL-32 matrix. Slice s holds rows 32s..32s+31,
 // column-major: entry j of lane l at sptr[s] + 32 j + l. Column indices are
 // either explicit (col) or, when the rows of the level share few column-offset
@@ -137,7 +179,8 @@ k_jacobi_from_zero(int n, const TV* __restrict__ dinv, const T* __restrict__ b,
 }
 
 // Transfer weights are exact powers of two: packed entry = index | code << 29,
-// weight = 2^-code (1, 1/2, 1/4, 1/8).
+// weight = 2^-code (1, 1/2, 1/4, 1/8); code 7 marks SELL padding (weight 0).
+constexpr uint32_t kPadEntry = 7u << 29;
 constexpr int kWShift = 29;
 constexpr uint32_t kIdxMask = (1u << kWShift) - 1u;
 
@@ -145,46 +188,70 @@ template<class T>
 __device__ __forceinline__ T wcode(uint32_t e)
 {
   const uint32_t c = e >> kWShift;
-  return c == 0 ? T(1) : c == 1 ? T(0.5) : c == 2 ? T(0.25) : T(0.125);
+  return c == 0 ? T(1) : c == 1 ? T(0.5) : c == 2 ? T(0.25) : c == 3 ? T(0.125) : T(0);
 }
 
-// coarse = R fine (gather over the coarse row, ascending fine index, as
-// MgInterpolatorMatrix::restrict_zero), then 0 on coarse Dirichlet dofs.
+// Transfer tables use the SELL-32 layout of the matrices: row i's entries at
+// tsp[i >> 5] + 32 j + (i & 31), padded with kPadEntry. The gathers of a chunk
+// are issued together; the sum runs over the entries in ascending order.
+template<class T>
+__device__ __forceinline__ T
+transfer_row(const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
+             const T* __restrict__ src, int i)
+{
+  const int beg = __ldg(tsp + (i >> 5));
+  const int w = (__ldg(tsp + (i >> 5) + 1) - beg) >> 5;
+  const uint32_t* ep = tent + beg + (i & 31);
+  T acc = T(0);
+  for (int j0 = 0; j0 < w; j0 += 8) {
+    const uint32_t* pe[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      pe[q] = ep + min(j0 + q, w - 1) * kSlice;
+    uint32_t e[8];
+    ld8(e, pe);
+    const T* ps[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      ps[q] = src + (e[q] & kIdxMask);
+    T f[8];
+    ld8(f, ps);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (j0 + q < w)
+        acc = fma(wcode<T>(e[q]), f[q], acc);
+  }
+  return acc;
+}
+
+// coarse = R fine (MgInterpolatorMatrix::restrict_zero order), then 0 on the
+// coarse Dirichlet dofs.
 template<class T>
 __global__ void
-k_restrict(int nc, const int* __restrict__ rptr, const uint32_t* __restrict__ rent,
+k_restrict(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
            const T* __restrict__ fine, T* __restrict__ coarse,
            const uint8_t* __restrict__ cdir)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nc)
     return;
-  T acc = T(0);
-  for (int k = rptr[i]; k < rptr[i + 1]; ++k) {
-    uint32_t e = rent[k];
-    acc = fma(wcode<T>(e), ldg(fine + (e & kIdxMask)), acc);
-  }
+  const T acc = transfer_row<T>(tsp, tent, fine, i);
   coarse[i] = (cdir && cdir[i]) ? T(0) : acc;
 }
 
-// Plain restriction without the Dirichlet step (gb_restrict_zero).
-// fine += P coarse (gather over the fine row's parents, ascending), optionally
-// masked by the fine Dirichlet dofs and scaled: MODE 0: fine += P c;
-// MODE 1 (coarse-grid correction): u += mgomega * (dir ? 0 : P c).
+// fine += P coarse (prolongate_add order), optionally masked by the fine
+// Dirichlet dofs and scaled: MODE 0: fine += P c; MODE 1 (coarse-grid
+// correction): u += mgomega * (dir ? 0 : P c).
 template<int MODE, class T>
 __global__ void
-k_prolong(int nf, const int* __restrict__ pptr, const uint32_t* __restrict__ pent,
+k_prolong(int nf, const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
           const T* __restrict__ coarse, T* __restrict__ fine,
           const uint8_t* __restrict__ fdir, double mgomega)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf)
     return;
-  T acc = T(0);
-  for (int k = pptr[i]; k < pptr[i + 1]; ++k) {
-    uint32_t e = pent[k];
-    acc = fma(wcode<T>(e), ldg(coarse + (e & kIdxMask)), acc);
-  }
+  T acc = transfer_row<T>(tsp, tent, coarse, i);
   if (MODE == 0) {
     fine[i] = fine[i] + acc;
   } else {
@@ -619,7 +686,7 @@ k_fg_setup(GmresDev* G, double tol, double globaltol, int maxiter)
 // Hessenberg system of the cycle.
 __global__ void
 k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
-             cudaGraphConditionalHandle inner, int m, int maxrestarts)
+             cudaGraphConditionalHandle inner, int m, int maxrestarts, int use_cond)
 {
   const double beta = G->beta_tmp;
   const double aim = fmax(G->info.tol * G->bnorm, G->info.globaltol);
@@ -635,8 +702,10 @@ k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
     G->stop = 1;
     G->inv = 0.0;
     G->info.status = conv ? 2 : 3;
-    cudaGraphSetConditional(outer, 0);
-    cudaGraphSetConditional(inner, 0);
+    if (use_cond) {
+      cudaGraphSetConditional(outer, 0);
+      cudaGraphSetConditional(inner, 0);
+    }
     return;
   }
   for (int c = 0; c < m; ++c) {
@@ -651,7 +720,9 @@ k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
   G->beta = beta;
   G->inv = 1.0 / beta;
   G->restarts += 1;
-  cudaGraphSetConditional(inner, 1);
+  G->stop = 0;
+  if (use_cond)
+    cudaGraphSetConditional(inner, 1);
 }
 
 // y = (TO) V[(*jp) * n + i]   (Arnoldi vector j into the cycle's right-hand side)
@@ -682,92 +753,93 @@ k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
 //  MODE 0: c1[i] = <w, V_i>;                         H[j][i]  = c1[i]
 //  MODE 1: w -= sum_i c1[i] V_i; c2[i] = <w, V_i>;   H[j][i] += c2[i]
 //  MODE 2: w -= sum_i c2[i] V_i; s = ||w||;          H[j][j+1] = s
-// Each pass reads the j+1 basis vectors once; accumulators stay in registers;
-// reductions are deterministic (fixed grid, fixed order).
+// One pass over the j+1 basis vectors; per-thread dot accumulators live in
+// shared memory (column per thread); block and grid reductions are warp-parallel
+// and deterministic (fixed grid, fixed order).
+constexpr int kCgsThreads = 1024;
+
 template<int MODE>
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kCgsThreads)
 k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
       unsigned* ticket)
 {
+  constexpr int kWarps = kCgsThreads / 32;
   __shared__ double s_coef[kCgsMaxJ];
-  __shared__ double s_red[kRedThreads / 32][kCgsMaxJ];
+  __shared__ double s_warp[kWarps][kCgsMaxJ];
   __shared__ bool am_last;
   const int j = G->j;
   const int nv = j + 1;
+  const int nred = (MODE == 2) ? 1 : nv;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   double* w = V + int64_t(j + 1) * n;
-  if (MODE >= 1 && threadIdx.x < kCgsMaxJ)
-    s_coef[threadIdx.x] = (threadIdx.x < nv) ? (MODE == 1 ? G->d[threadIdx.x]
-                                                          : G->d2[threadIdx.x])
-                                             : 0.0;
+  if (MODE >= 1 && tid < kCgsMaxJ)
+    s_coef[tid] = (tid < nv) ? (MODE == 1 ? G->d[tid] : G->d2[tid]) : 0.0;
+  s_warp[wid][lane] = 0.0;
   __syncthreads();
-  double acc[kCgsMaxJ];
-#pragma unroll
-  for (int i = 0; i < kCgsMaxJ; ++i)
-    acc[i] = 0.0;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    double t = w[r];
+  // warp-uniform loop: every lane takes part in the shuffles
+  for (int64_t base = int64_t(blockIdx.x) * kCgsThreads + wid * 32; base < n;
+       base += int64_t(gridDim.x) * kCgsThreads) {
+    const int64_t r = base + lane;
+    const bool ok = r < n;
+    double t = ok ? w[r] : 0.0;
     if (MODE >= 1) {
-#pragma unroll
-      for (int i = 0; i < kCgsMaxJ; ++i)
-        if (i < nv)
-          t = fma(-s_coef[i], V[int64_t(i) * n + r], t);
-      w[r] = t;
+      for (int i = 0; i < nv; ++i)
+        t = fma(-s_coef[i], ok ? V[int64_t(i) * n + r] : 0.0, t);
+      if (ok)
+        w[r] = t;
     }
     if (MODE <= 1) {
-#pragma unroll
-      for (int i = 0; i < kCgsMaxJ; ++i)
-        if (i < nv)
-          acc[i] = fma(t, V[int64_t(i) * n + r], acc[i]);
+      for (int i = 0; i < nv; ++i) {
+        double p = ok ? t * V[int64_t(i) * n + r] : 0.0;
+        for (int o = 16; o > 0; o >>= 1)
+          p += __shfl_down_sync(0xffffffffu, p, o);
+        if (lane == 0)
+          s_warp[wid][i] += p;
+      }
     } else {
-      acc[0] = fma(t, t, acc[0]);
-    }
-  }
-  const int nred = (MODE == 2) ? 1 : nv;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < kCgsMaxJ; ++i) {
-    if (i < nred) {
-      double v = acc[i];
+      double p = t * t;
       for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_down_sync(0xffffffffu, v, o);
+        p += __shfl_down_sync(0xffffffffu, p, o);
       if (lane == 0)
-        s_red[wid][i] = v;
+        s_warp[wid][0] += p;
     }
   }
   __syncthreads();
-  if (threadIdx.x < nred) {
+  if (tid < nred) {
     double v = 0.0;
-    for (int q = 0; q < kRedThreads / 32; ++q)
-      v += s_red[q][threadIdx.x];
-    partials[int64_t(threadIdx.x) * gridDim.x + blockIdx.x] = v;
+    for (int q = 0; q < kWarps; ++q)
+      v += s_warp[q][tid];
+    partials[int64_t(tid) * gridDim.x + blockIdx.x] = v;
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0)
+  if (tid == 0)
     am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
   __syncthreads();
   if (!am_last)
     return;
   __threadfence();
-  if (threadIdx.x < nred) {
+  for (int i = wid; i < nred; i += kWarps) {
     double v = 0.0;
-    for (int q = 0; q < (int)gridDim.x; ++q)
-      v += __ldcg(partials + int64_t(threadIdx.x) * gridDim.x + q);
-    const int i = threadIdx.x;
-    if (MODE == 0) {
-      G->d[i] = v;
-      G->H[j][i] = v;
-    } else if (MODE == 1) {
-      G->d2[i] = v;
-      G->H[j][i] += v;
-    } else {
-      const double sv = sqrt(v);
-      G->H[j][j + 1] = sv;
-      G->s = sv;
+    for (int q = lane; q < (int)gridDim.x; q += 32)
+      v += __ldcg(partials + int64_t(i) * gridDim.x + q);
+    for (int o = 16; o > 0; o >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) {
+      if (MODE == 0) {
+        G->d[i] = v;
+        G->H[j][i] = v;
+      } else if (MODE == 1) {
+        G->d2[i] = v;
+        G->H[j][i] += v;
+      } else {
+        const double sv = sqrt(v);
+        G->H[j][j + 1] = sv;
+        G->s = sv;
+      }
     }
   }
-  if (threadIdx.x == 0)
+  if (tid == 0)
     *ticket = 0u;
 }
 
@@ -775,7 +847,7 @@ k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
 // Hessenberg), residual estimate |gamma[j+1]| = ||b - A x_j|| in exact
 // arithmetic, then j += 1 and the inner loop condition.
 __global__ void
-k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m)
+k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
 {
   const int last = G->j, dim = last + 1;
   double* h = G->H[last];
@@ -802,7 +874,9 @@ k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m)
   const double aim = fmax(G->info.tol * G->bnorm, G->info.globaltol);
   const int reached = (rho <= aim) || dim >= m || G->total >= G->info.maxiter ||
                       !(rho == rho);
-  cudaGraphSetConditional(inner, reached ? 0 : 1);
+  G->reached = reached;
+  if (use_cond)
+    cudaGraphSetConditional(inner, reached ? 0 : 1);
 }
 
 // hs = H^-1 gamma on the first G->j columns (Common/mult.h:130-141)
@@ -832,6 +906,265 @@ k_fg_update(int64_t n, double* __restrict__ x, const TZ* __restrict__ Z,
       acc = fma(G->hs[q], static_cast<double>(Z[int64_t(q) * n + i]), acc);
     x[i] = acc;
   }
+}
+
+// -------------------------------------------------- coarse-level CTA kernel
+//
+// Levels with at most kCoarseMaxRows rows are latency-bound: one kernel per
+// smoothing sweep costs more in launch and drain time than the sweep itself.
+// One CTA of kCoarseThreads threads runs the whole sub-cycle of those levels
+// from a recorded program of ops, with a block barrier between ops. Each op does
+// per row exactly what the corresponding standalone kernel does (same operation
+// order). All of its data traffic stays on one SM, so its vector loads go
+// through L1 (coherent within the SM) and the small levels' matrices stay in L1
+// after the first sweep.
+
+constexpr int kCoarseThreads = 1024;
+constexpr int kCoarseMaxRows = 1024;
+
+// A vector the sub-cycle stages in shared memory: loaded at the start when
+// read before written, stored back at the end when written.
+struct CoarseBuf
+{
+  void* gptr;
+  int bytes, off, load, store;
+};
+// A read-only range (matrix, inverse diagonal, masks, transfer tables) that the
+// kernel prefetches into L1 at its start.
+struct CoarsePrefetch
+{
+  const void* p;
+  int bytes;
+};
+
+enum CoarseOpKind
+{
+  kOpJacobiZero = 0, // out = omega * (dinv * b)
+  kOpJacobi = 1,     // out = in + omega * dinv * (b - A in)
+  kOpResid = 2,      // out = b - A in
+  kOpRestrict = 3,   // out = R in, 0 on mask
+  kOpFill0 = 4,      // out = 0
+  kOpProlong = 5     // out += omega * (mask ? 0 : P in)
+};
+
+struct CoarseOp
+{
+  int kind, n;
+  void* out;       // global vectors as recorded (host bookkeeping)
+  const void* in;
+  const void* b;
+  int in_n, b_n;   // lengths of in and b (out has n)
+  int out_off, in_off, b_off; // byte offsets of the staged vectors in shared memory
+  const int* sptr;
+  const int* col;
+  const uint8_t* pid;
+  const int* ptab;
+  int W;
+  const void* val;
+  const void* dinv;
+  const uint8_t* mask;
+  const int* tptr;
+  const uint32_t* tent;
+  double alpha;
+};
+
+
+// b - A x (or A x when NEG is false) for row r of a SELL-32 level; the loads
+// of a chunk are issued together (one row per thread: the latency of a serial
+// chain of loads would dominate), the sum runs in stored order.
+template<class T, bool NEG>
+__device__ __forceinline__ T
+coarse_row_spmv(const CoarseOp& op, const T* __restrict__ x, int r, T acc)
+{
+  const int s = r >> 5, lane = r & 31;
+  const int beg = __ldg(op.sptr + s);
+  const int w = (__ldg(op.sptr + s + 1) - beg) >> 5;
+  const T* val = static_cast<const T*>(op.val) + beg + lane;
+  const int* prow = op.pid ? op.ptab + int(__ldg(op.pid + r)) * op.W : nullptr;
+  const int* crow = op.col + beg + lane;
+  for (int j0 = 0; j0 < w; j0 += 8) {
+    const T* pa[8];
+    int c[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int j = min(j0 + q, w - 1);
+      pa[q] = val + j * kSlice;
+      c[q] = prow ? r + __ldg(prow + j) : __ldg(crow + j * kSlice);
+    }
+    T av[8];
+    ld8(av, pa);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (j0 + q < w)
+        acc = NEG ? fma(-av[q], x[c[q]], acc) : fma(av[q], x[c[q]], acc);
+  }
+  return acc;
+}
+
+// R or P row in the SELL transfer layout, source vector in shared memory
+template<class T>
+__device__ __forceinline__ T
+coarse_row_transfer(const CoarseOp& op, const T* __restrict__ src, int i)
+{
+  const int beg = __ldg(op.tptr + (i >> 5));
+  const int w = (__ldg(op.tptr + (i >> 5) + 1) - beg) >> 5;
+  const uint32_t* ep = op.tent + beg + (i & 31);
+  T acc = T(0);
+  for (int j0 = 0; j0 < w; j0 += 8) {
+    const uint32_t* pe[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      pe[q] = ep + min(j0 + q, w - 1) * kSlice;
+    uint32_t e[8];
+    ld8(e, pe);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (j0 + q < w)
+        acc = fma(wcode<T>(e[q]), src[e[q] & kIdxMask], acc);
+  }
+  return acc;
+}
+
+// Batch mode (K != null): CTA j applies the program to the j-th unit input
+// (unit entry j of the root right-hand side b, or, for j >= nb, unit entry
+// j - nb of the starting root u) and writes the resulting root u as column j of
+// K (row-major, K[i * ncols + j]); every vector starts from zero in shared
+// memory and nothing else is stored. This forms the sub-cycle's linear map
+// u = K [b; u_start] once per assembly.
+struct CoarseBatch
+{
+  void* K;
+  int ncols, nb, b_off, u_in_off, u_out_off, n_root;
+};
+
+template<class T>
+__global__ void __launch_bounds__(kCoarseThreads)
+k_coarse_cycle(const CoarseOp* __restrict__ ops, int nops,
+               const CoarseBuf* __restrict__ bufs, int nbufs,
+               const CoarsePrefetch* __restrict__ pre, int npre, int vec_bytes,
+               CoarseBatch batch)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  CoarseOp* s_ops = reinterpret_cast<CoarseOp*>(smem + vec_bytes);
+  const int t = threadIdx.x;
+  const bool bm = batch.K != nullptr;
+  if (bm) {
+    for (int q = t; q < vec_bytes / int(sizeof(T)); q += kCoarseThreads)
+      reinterpret_cast<T*>(smem)[q] = T(0);
+    __syncthreads();
+    if (t == 0) {
+      const int j = blockIdx.x;
+      if (j < batch.nb)
+        reinterpret_cast<T*>(smem + batch.b_off)[j] = T(1);
+      else
+        reinterpret_cast<T*>(smem + batch.u_in_off)[j - batch.nb] = T(1);
+    }
+  }
+  // stage: program, vectors read before written, L1 prefetch of read-only data
+  {
+    const int* src = reinterpret_cast<const int*>(ops);
+    int* dst = reinterpret_cast<int*>(s_ops);
+    const int words = nops * int(sizeof(CoarseOp) / sizeof(int));
+    for (int q = t; q < words; q += kCoarseThreads)
+      dst[q] = src[q];
+  }
+  for (int bi = 0; bi < nbufs; ++bi) {
+    const CoarseBuf cb = bufs[bi];
+    if (!cb.load || bm)
+      continue;
+    const T* g = static_cast<const T*>(cb.gptr);
+    T* sv = reinterpret_cast<T*>(smem + cb.off);
+    for (int q = t; q < cb.bytes / int(sizeof(T)); q += kCoarseThreads)
+      sv[q] = g[q];
+  }
+  for (int pi = 0; pi < npre; ++pi) {
+    const char* p = static_cast<const char*>(pre[pi].p);
+    for (int off = t * 128; off < pre[pi].bytes; off += kCoarseThreads * 128)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(p + off));
+  }
+  __syncthreads();
+  for (int k = 0; k < nops; ++k) {
+    const CoarseOp& op = s_ops[k];
+    T* out = reinterpret_cast<T*>(smem + op.out_off);
+    const T* in = reinterpret_cast<const T*>(smem + op.in_off);
+    const T* b = reinterpret_cast<const T*>(smem + op.b_off);
+    for (int r = t; r < op.n; r += kCoarseThreads) {
+      switch (op.kind) {
+        case kOpJacobiZero: {
+          const T d = __ldg(static_cast<const T*>(op.dinv) + r);
+          out[r] = static_cast<T>(op.alpha) * (d * b[r]);
+          break;
+        }
+        case kOpJacobi: {
+          const T acc = coarse_row_spmv<T, true>(op, in, r, b[r]);
+          const T h = __ldg(static_cast<const T*>(op.dinv) + r) * acc;
+          out[r] = in[r] + static_cast<T>(op.alpha) * h;
+          break;
+        }
+        case kOpResid:
+          out[r] = coarse_row_spmv<T, true>(op, in, r, b[r]);
+          break;
+        case kOpRestrict: {
+          const T acc = coarse_row_transfer<T>(op, in, r);
+          out[r] = (op.mask && __ldg(op.mask + r)) ? T(0) : acc;
+          break;
+        }
+        case kOpFill0:
+          out[r] = T(0);
+          break;
+        case kOpProlong: {
+          T acc = coarse_row_transfer<T>(op, in, r);
+          if (op.mask && __ldg(op.mask + r))
+            acc = T(0);
+          out[r] = out[r] + static_cast<T>(op.alpha) * acc;
+          break;
+        }
+        default:
+          break;
+      }
+    }
+    // every thread reaches every barrier (no early exit)
+    __syncthreads();
+  }
+  if (bm) {
+    const T* u = reinterpret_cast<const T*>(smem + batch.u_out_off);
+    T* K = static_cast<T*>(batch.K);
+    for (int i = t; i < batch.n_root; i += kCoarseThreads)
+      K[int64_t(i) * batch.ncols + blockIdx.x] = u[i];
+    return;
+  }
+  for (int bi = 0; bi < nbufs; ++bi) {
+    const CoarseBuf cb = bufs[bi];
+    if (!cb.store)
+      continue;
+    T* g = static_cast<T*>(cb.gptr);
+    const T* sv = reinterpret_cast<const T*>(smem + cb.off);
+    for (int q = t; q < cb.bytes / int(sizeof(T)); q += kCoarseThreads)
+      g[q] = sv[q];
+  }
+}
+
+// u_out = K [b; u_in] for the coarse sub-cycle's precomputed linear map: one
+// warp per row, FP64 accumulation, fixed lane order (deterministic).
+template<class T>
+__global__ void
+k_coarse_apply(int n_root, int ncols, int nb, const T* __restrict__ K,
+               const T* __restrict__ b, const T* __restrict__ u_in, T* __restrict__ u_out)
+{
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n_root) // whole warps exit together
+    return;
+  const T* row = K + int64_t(warp) * ncols;
+  double acc = 0.0;
+  for (int j = lane; j < ncols; j += 32) {
+    const double x = j < nb ? double(b[j]) : double(u_in[j - nb]);
+    acc = fma(double(__ldg(row + j)), x, acc);
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0)
+    u_out[warp] = static_cast<T>(acc);
 }
 
 } // namespace gb

@@ -14,10 +14,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -272,6 +274,37 @@ struct Transfer
   DeviceArray<uint32_t> rent, pent;
 };
 
+struct CoarseKey
+{
+  int tsize, level;
+  const void *u, *tmp, *b;
+  bool zero;
+  char p0, p;
+  bool operator<(const CoarseKey& o) const
+  {
+    return std::tie(tsize, level, u, tmp, b, zero, p0, p) <
+           std::tie(o.tsize, o.level, o.u, o.tmp, o.b, o.zero, o.p0, o.p);
+  }
+};
+
+struct CoarseProgram
+{
+  DeviceArray<CoarseOp> ops;
+  DeviceArray<CoarseBuf> bufs;
+  DeviceArray<CoarsePrefetch> pre;
+  int nops = 0, nbufs = 0, npre = 0, vec_bytes = 0, smem_bytes = 0;
+  // precomputed linear map u_out = K [b; u_start] (dense mode)
+  DeviceArray<double> K64;
+  DeviceArray<float> K32;
+  int ncols = 0, nb = 0, n_root = 0;
+  const void* b_root = nullptr;
+  const void* u_in = nullptr;
+  const void* u_out = nullptr;
+  const void* tmp_out = nullptr;
+  char p0_out = 'V';
+  bool zero_out = false;
+};
+
 template<class T>
 struct MgWork
 {
@@ -313,10 +346,32 @@ struct gb_ctx
     int64_t version = -1;
     int setup_k = 0, outer_k = 0, inner_k = 0;
   } fg[2];
+  // coarse-level kernel: levels 0..coarse_root, programs per entry state
+  bool coarse_on = true;
+  bool coarse_dense = true; // apply the coarse sub-cycle as its precomputed map
+  bool use_graph = true; // flexible solver as one CUDA graph (GB_GRAPH=0: host loops)
+  // per-kernel timing
+  bool ktime = false;
+  struct KtPending
+  {
+    const void* func;
+    cudaEvent_t e0, e1;
+  };
+  std::vector<cudaEvent_t> kt_pool;
+  std::vector<KtPending> kt_pending;
+  std::map<std::string, std::pair<int64_t, double>> kt_acc;
+  int coarse_root = -1;
+  std::map<gb::CoarseKey, gb::CoarseProgram> coarse_progs;
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
   gb::DeviceArray<float> rhs32, zfix32;
   ~gb_ctx()
   {
+    for (auto e : kt_pool)
+      cudaEventDestroy(e);
+    for (auto& p : kt_pending) {
+      cudaEventDestroy(p.e0);
+      cudaEventDestroy(p.e1);
+    }
     for (auto& g : fg) {
       if (g.exec)
         cudaGraphExecDestroy(g.exec);
@@ -337,15 +392,90 @@ check_launch(Context& c)
     throw Error{ GB_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e) };
 }
 
+// Per-kernel device timing (gb_set_timing): an event pair around each launch
+// outside graph capture, resolved by kt_flush.
+static void
+kt_begin(Context& c, cudaEvent_t* e0)
+{
+  *e0 = nullptr;
+  if (!c.ktime)
+    return;
+  cudaStreamCaptureStatus cs;
+  if (cudaStreamIsCapturing(c.stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return;
+  if (c.kt_pool.empty()) {
+    cudaEvent_t e;
+    GB_CUDA(cudaEventCreate(&e));
+    c.kt_pool.push_back(e);
+  }
+  *e0 = c.kt_pool.back();
+  c.kt_pool.pop_back();
+  GB_CUDA(cudaEventRecord(*e0, c.stream));
+}
+
+static void
+kt_end(Context& c, cudaEvent_t e0, const void* func)
+{
+  if (!e0)
+    return;
+  if (c.kt_pool.empty()) {
+    cudaEvent_t e;
+    GB_CUDA(cudaEventCreate(&e));
+    c.kt_pool.push_back(e);
+  }
+  cudaEvent_t e1 = c.kt_pool.back();
+  c.kt_pool.pop_back();
+  GB_CUDA(cudaEventRecord(e1, c.stream));
+  c.kt_pending.push_back({ func, e0, e1 });
+}
+
+static void
+kt_flush(Context& c)
+{
+  if (c.kt_pending.empty())
+    return;
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  for (auto& p : c.kt_pending) {
+    float ms = 0;
+    GB_CUDA(cudaEventElapsedTime(&ms, p.e0, p.e1));
+    const char* name = nullptr;
+    if (cudaFuncGetName(&name, p.func) != cudaSuccess || !name)
+      name = "?";
+    auto& a = c.kt_acc[name];
+    a.first += 1;
+    a.second += ms;
+    c.kt_pool.push_back(p.e0);
+    c.kt_pool.push_back(p.e1);
+  }
+  c.kt_pending.clear();
+}
+
+template<class K, class... Args>
+static void
+launch_smem(Context& c, K kern, int grid, int block, int smem, Args... args)
+{
+  if (grid <= 0)
+    return;
+  cudaEvent_t e0;
+  kt_begin(c, &e0);
+  kern<<<grid, block, smem, c.stream>>>(args...);
+  c.launches++;
+  check_launch(c);
+  kt_end(c, e0, reinterpret_cast<const void*>(kern));
+}
+
 template<class K, class... Args>
 static void
 launch(Context& c, K kern, int grid, int block, Args... args)
 {
   if (grid <= 0)
     return;
+  cudaEvent_t e0;
+  kt_begin(c, &e0);
   kern<<<grid, block, 0, c.stream>>>(args...);
   c.launches++;
   check_launch(c);
+  kt_end(c, e0, reinterpret_cast<const void*>(kern));
 }
 
 static int
@@ -479,10 +609,125 @@ ensure_work(Context& c)
     GB_CUDA(c.w32.b[l].alloc(nd));
     GB_CUDA(c.w32.v[l].alloc(nd));
   }
+  c.coarse_root = -1;
+  for (int l = 0; l < c.nlevels; ++l) {
+    if (c.L[l].ndof() > kCoarseMaxRows)
+      break;
+    c.coarse_root = l;
+  }
+  c.coarse_progs.clear();
   c.work_ready = true;
 }
 
 // ------------------------------------------------------------ smoothing
+
+// ------------------------------------------------------------ cycle steps
+//
+// Every step of the cycle goes through Emit: it either launches the step's
+// kernel on the context stream, or (rec set) appends it to the program of the
+// coarse-level kernel.
+template<class T>
+struct Emit
+{
+  Context& c;
+  std::vector<CoarseOp>* rec = nullptr;
+
+  CoarseOp level_op(int kind, const Level& L, void* out, const void* in,
+                    const void* b, double alpha) const
+  {
+    CoarseOp o{};
+    o.kind = kind;
+    o.n = static_cast<int>(L.ndof());
+    o.out = out;
+    o.in = in;
+    o.b = b;
+    o.in_n = in ? o.n : 0;
+    o.b_n = b ? o.n : 0;
+    o.sptr = L.A.sptr.p;
+    o.col = L.A.pat ? nullptr : L.A.col.p;
+    o.pid = L.A.pat ? L.A.pid.p : nullptr;
+    o.ptab = L.A.pat ? L.A.ptab.p : nullptr;
+    o.W = L.A.W;
+    o.val = sell_vals<T>(L.A);
+    o.dinv = dinv_of<T>(L);
+    o.mask = L.dirmask.p;
+    o.alpha = alpha;
+    return o;
+  }
+  void jacobi_zero(int l, T* u, const T* b)
+  {
+    const Level& L = c.L[l];
+    if (rec)
+      return rec->push_back(level_op(kOpJacobiZero, L, u, nullptr, b, c.params.omega));
+    launch(c, k_jacobi_from_zero<T, T>, blocks_for(L.n, 256), 256, (int)L.n,
+           dinv_of<T>(L), b, u, c.params.omega);
+  }
+  void jacobi(int l, const T* u, T* out, const T* b)
+  {
+    const Level& L = c.L[l];
+    if (rec)
+      return rec->push_back(level_op(kOpJacobi, L, out, u, b, c.params.omega));
+    spmv<kJacobi, T, T, T>(c, L, L.A, u, out, b, dinv_of<T>(L), c.params.omega);
+  }
+  void resid(int l, const T* u, T* out, const T* b)
+  {
+    const Level& L = c.L[l];
+    if (rec)
+      return rec->push_back(level_op(kOpResid, L, out, u, b, 0.0));
+    spmv<kResid, T, T, T>(c, L, L.A, u, out, b, nullptr, 0.0);
+  }
+  // coarse (level l) = R fine, 0 on the coarse Dirichlet dofs
+  void restrict_to(int l, const T* fine, T* coarse)
+  {
+    const Transfer& Tr = c.T[l];
+    if (rec) {
+      CoarseOp o{};
+      o.kind = kOpRestrict;
+      o.n = Tr.nc;
+      o.out = coarse;
+      o.in = fine;
+      o.in_n = Tr.nf;
+      o.mask = c.L[l].dirmask.p;
+      o.tptr = Tr.rptr.p;
+      o.tent = Tr.rent.p;
+      return rec->push_back(o);
+    }
+    launch(c, k_restrict<T>, blocks_for(Tr.nc, 256), 256, Tr.nc, Tr.rptr.p, Tr.rent.p,
+           fine, coarse, (const uint8_t*)c.L[l].dirmask.p);
+  }
+  void fill0(int l, T* u)
+  {
+    const Level& L = c.L[l];
+    if (rec) {
+      CoarseOp o{};
+      o.kind = kOpFill0;
+      o.n = static_cast<int>(L.ndof());
+      o.out = u;
+      return rec->push_back(o);
+    }
+    launch(c, k_fill<T>, stream_blocks(L.ndof()), 256, (int64_t)L.ndof(), u, T(0));
+  }
+  // fine (level l+1) += mgomega * (dir ? 0 : P coarse)
+  void prolong(int l, const T* coarse, T* fine)
+  {
+    const Transfer& Tr = c.T[l];
+    if (rec) {
+      CoarseOp o{};
+      o.kind = kOpProlong;
+      o.n = Tr.nf;
+      o.out = fine;
+      o.in = coarse;
+      o.in_n = Tr.nc;
+      o.mask = c.L[l + 1].dirmask.p;
+      o.tptr = Tr.pptr.p;
+      o.tent = Tr.pent.p;
+      o.alpha = c.params.mgomega;
+      return rec->push_back(o);
+    }
+    launch(c, k_prolong<1, T>, blocks_for(Tr.nf, 256), 256, Tr.nf, Tr.pptr.p, Tr.pent.p,
+           coarse, fine, (const uint8_t*)c.L[l + 1].dirmask.p, c.params.mgomega);
+  }
+};
 
 // StdSolver::smooth, linear_smooth jacobi (Solver/stdsolver.cc:951-986): each
 // sweep computes h = y - A x, h = D^-1 h, x += omega h; fused into one pass that
@@ -490,19 +735,181 @@ ensure_work(Context& c)
 // from x = 0 needs no product (y - A 0 == y).
 template<class T>
 static void
-smooth(Context& c, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
+smooth(Emit<T>& E, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
 {
-  const Level& L = c.L[l];
   for (int it = 0; it < niter; ++it) {
     if (u_zero) {
-      launch(c, k_jacobi_from_zero<T, T>, blocks_for(L.n, 256), 256, (int)L.n,
-             dinv_of<T>(L), b, u, c.params.omega);
+      E.jacobi_zero(l, u, b);
       u_zero = false;
     } else {
-      spmv<kJacobi, T, T, T>(c, L, L.A, u, tmp, b, dinv_of<T>(L), c.params.omega);
+      E.jacobi(l, u, tmp, b);
       std::swap(u, tmp);
     }
   }
+}
+
+template<class T>
+static bool mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel,
+                   char& p0, char p, T*& u, T*& tmp, const T* b, bool u_zero);
+
+// Runs mgstep(l) for a level handled by the coarse-level kernel: the step is
+// recorded once per entry state (cached) and launched as one single-CTA kernel.
+template<class T>
+static bool
+run_coarse(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
+           char p, T*& u, T*& tmp, const T* b, bool u_zero)
+{
+  Context& c = E.c;
+  CoarseKey key{ int(sizeof(T)), l, (const void*)u, (const void*)tmp, (const void*)b,
+                 u_zero, p0, p };
+  auto it = c.coarse_progs.find(key);
+  if (it == c.coarse_progs.end()) {
+    std::vector<CoarseOp> ops;
+    Emit<T> R{ c, &ops };
+    T* u2 = u;
+    T* t2 = tmp;
+    char p02 = p0;
+    const bool z = mgstep<T>(R, W, l, finelevel, coarselevel, p02, p, u2, t2, b, u_zero);
+    CoarseProgram prog;
+    prog.nops = static_cast<int>(ops.size());
+    // stage every vector in shared memory: offsets in first-use order; load
+    // those read before written, store back those written
+    std::vector<CoarseBuf> bufs;
+    std::map<const void*, int> bidx;
+    auto buf_of = [&](const void* p, int n) {
+      auto it2 = bidx.find(p);
+      if (it2 != bidx.end())
+        return it2->second;
+      CoarseBuf cb{ const_cast<void*>(p), n * int(sizeof(T)), prog.vec_bytes, 0, 0 };
+      prog.vec_bytes += (cb.bytes + 15) / 16 * 16;
+      bufs.push_back(cb);
+      return bidx[p] = static_cast<int>(bufs.size()) - 1;
+    };
+    std::vector<char> written;
+    auto read = [&](int bi) {
+      if (bi >= static_cast<int>(written.size()))
+        written.resize(bi + 1, 0);
+      if (!written[bi])
+        bufs[bi].load = 1;
+    };
+    auto write = [&](int bi) {
+      if (bi >= static_cast<int>(written.size()))
+        written.resize(bi + 1, 0);
+      written[bi] = 1;
+      bufs[bi].store = 1;
+    };
+    for (auto& o : ops) {
+      int bi_in = o.in ? buf_of(o.in, o.in_n) : -1;
+      int bi_b = o.b ? buf_of(o.b, o.b_n) : -1;
+      int bi_out = buf_of(o.out, o.n);
+      if (bi_in >= 0)
+        read(bi_in);
+      if (bi_b >= 0)
+        read(bi_b);
+      if (o.kind == kOpProlong)
+        read(bi_out); // out += ...
+      write(bi_out);
+      o.in_off = bi_in >= 0 ? bufs[bi_in].off : 0;
+      o.b_off = bi_b >= 0 ? bufs[bi_b].off : 0;
+      o.out_off = bufs[bi_out].off;
+    }
+    // read-only data of the levels and transfers the program touches
+    std::vector<CoarsePrefetch> pre;
+    for (int lv = 0; lv <= l; ++lv) {
+      const Level& L = c.L[lv];
+      pre.push_back({ sell_vals<T>(L.A), int(L.A.entries * sizeof(T)) });
+      pre.push_back({ L.A.sptr.p, int((L.A.nslices + 1) * sizeof(int)) });
+      if (L.A.pat) {
+        pre.push_back({ L.A.pid.p, int(L.n) });
+        pre.push_back({ L.A.ptab.p, int(L.A.npat * L.A.W * sizeof(int)) });
+      } else {
+        pre.push_back({ L.A.col.p, int(L.A.entries * sizeof(int)) });
+      }
+      pre.push_back({ dinv_of<T>(L), int(L.ndof() * sizeof(T)) });
+      pre.push_back({ L.dirmask.p, int(L.ndof()) });
+      if (lv + 1 <= l) {
+        const Transfer& Tr = c.T[lv];
+        pre.push_back({ Tr.rptr.p, int(Tr.rptr.n * sizeof(int)) });
+        pre.push_back({ Tr.rent.p, int(Tr.rent.n * sizeof(uint32_t)) });
+        pre.push_back({ Tr.pptr.p, int(Tr.pptr.n * sizeof(int)) });
+        pre.push_back({ Tr.pent.p, int(Tr.pent.n * sizeof(uint32_t)) });
+      }
+    }
+    prog.nbufs = static_cast<int>(bufs.size());
+    prog.npre = static_cast<int>(pre.size());
+    prog.smem_bytes = prog.vec_bytes + prog.nops * int(sizeof(CoarseOp));
+    GB_REQUIRE(prog.smem_bytes <= 200 * 1024, GB_EINVAL,
+               "coarse-level program does not fit in shared memory");
+    GB_CUDA(prog.ops.alloc(std::max<size_t>(ops.size(), 1)));
+    GB_CUDA(prog.bufs.alloc(std::max<size_t>(bufs.size(), 1)));
+    GB_CUDA(prog.pre.alloc(std::max<size_t>(pre.size(), 1)));
+    if (!ops.empty())
+      GB_CUDA(cudaMemcpy(prog.ops.p, ops.data(), ops.size() * sizeof(CoarseOp),
+                         cudaMemcpyHostToDevice));
+    if (!bufs.empty())
+      GB_CUDA(cudaMemcpy(prog.bufs.p, bufs.data(), bufs.size() * sizeof(CoarseBuf),
+                         cudaMemcpyHostToDevice));
+    if (!pre.empty())
+      GB_CUDA(cudaMemcpy(prog.pre.p, pre.data(), pre.size() * sizeof(CoarsePrefetch),
+                         cudaMemcpyHostToDevice));
+    if (prog.smem_bytes > 48 * 1024)
+      GB_CUDA(cudaFuncSetAttribute(k_coarse_cycle<T>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   prog.smem_bytes));
+    if (c.coarse_dense && u_zero && prog.nops > 0) {
+      // columns: unit entries of the root b (the sub-cycle starts from u = 0, so
+      // it is linear in b alone; a non-zero start runs the op program instead)
+      prog.n_root = static_cast<int>(c.L[l].ndof());
+      prog.nb = prog.n_root;
+      prog.ncols = prog.nb;
+      prog.b_root = b;
+      prog.u_in = u;
+      CoarseBatch bt{};
+      bt.ncols = prog.ncols;
+      bt.nb = prog.nb;
+      bt.n_root = prog.n_root;
+      bt.b_off = bufs[bidx.at((const void*)b)].off;
+      bt.u_in_off = 0;
+      bt.u_out_off = bufs[bidx.at((const void*)u2)].off;
+      const size_t kn = size_t(prog.n_root) * prog.ncols;
+      if (sizeof(T) == 8) {
+        GB_CUDA(prog.K64.alloc(kn));
+        bt.K = prog.K64.p;
+      } else {
+        GB_CUDA(prog.K32.alloc(kn));
+        bt.K = prog.K32.p;
+      }
+      launch_smem(c, k_coarse_cycle<T>, prog.ncols, kCoarseThreads, prog.smem_bytes,
+                  (const CoarseOp*)prog.ops.p, prog.nops, (const CoarseBuf*)prog.bufs.p,
+                  prog.nbufs, (const CoarsePrefetch*)prog.pre.p, prog.npre,
+                  prog.vec_bytes, bt);
+      GB_CUDA(cudaStreamSynchronize(c.stream));
+      c.launches--; // set-up, not part of a solve
+    }
+    prog.u_out = u2;
+    prog.tmp_out = t2;
+    prog.p0_out = p02;
+    prog.zero_out = z;
+    it = c.coarse_progs.emplace(key, std::move(prog)).first;
+  }
+  const CoarseProgram& prog = it->second;
+  if (prog.nops > 0 && prog.ncols > 0) {
+    const T* K = sizeof(T) == 8 ? reinterpret_cast<const T*>(prog.K64.p)
+                                : reinterpret_cast<const T*>(prog.K32.p);
+    launch(c, k_coarse_apply<T>, blocks_for(int64_t(prog.n_root) * 32, 256), 256,
+           prog.n_root, prog.ncols, prog.nb, K, static_cast<const T*>(prog.b_root),
+           static_cast<const T*>(prog.u_in),
+           static_cast<T*>(const_cast<void*>(prog.u_out)));
+  } else if (prog.nops > 0) {
+    launch_smem(c, k_coarse_cycle<T>, 1, kCoarseThreads, prog.smem_bytes,
+                (const CoarseOp*)prog.ops.p, prog.nops, (const CoarseBuf*)prog.bufs.p,
+                prog.nbufs, (const CoarsePrefetch*)prog.pre.p, prog.npre,
+                prog.vec_bytes, CoarseBatch{});
+  }
+  u = static_cast<T*>(const_cast<void*>(prog.u_out));
+  tmp = static_cast<T*>(const_cast<void*>(prog.tmp_out));
+  p0 = prog.p0_out;
+  return prog.zero_out;
 }
 
 // StdMultiLevelSolver::mgstep (Solver/stdmultilevelsolver.cc:462-531). Steps
@@ -512,49 +919,44 @@ smooth(Context& c, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
 // Returns true when u is still implicitly zero (no sweep has written it).
 template<class T>
 static bool
-mgstep(Context& c, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
+mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
        char p, T*& u, T*& tmp, const T* b, bool u_zero)
 {
+  Context& c = E.c;
+  if (!E.rec && c.coarse_on && l <= c.coarse_root)
+    return run_coarse<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b, u_zero);
   const gb_params& P = c.params;
   if (l == coarselevel) {
     if (p == 'F')
       p0 = 'V';
-    smooth<T>(c, l, P.iterexact, u, tmp, b, u_zero); // smooth_exact
+    smooth<T>(E, l, P.iterexact, u, tmp, b, u_zero); // smooth_exact
     return u_zero;
   }
-  const Level& L = c.L[l];
-  const Level& Lc = c.L[l - 1];
-  const Transfer& Tr = c.T[l - 1];
-  smooth<T>(c, l, P.iterpre, u, tmp, b, u_zero);
+  smooth<T>(E, l, P.iterpre, u, tmp, b, u_zero);
   // MatrixResidual into tmp, restrict_zero + SetBoundaryVectorZero on l-1
   if (u_zero) {
-    // u is still 0 (iterpre == 0): the residual is b itself
-    launch(c, k_restrict<T>, blocks_for(Tr.nc, 256), 256, Tr.nc, Tr.rptr.p,
-           Tr.rent.p, b, W.b[l - 1].p, Lc.dirmask.p);
+    E.restrict_to(l - 1, b, W.b[l - 1].p); // u == 0: the residual is b
   } else {
-    spmv<kResid, T, T, T>(c, L, L.A, u, tmp, b, nullptr, 0.0);
-    launch(c, k_restrict<T>, blocks_for(Tr.nc, 256), 256, Tr.nc, Tr.rptr.p,
-           Tr.rent.p, (const T*)tmp, W.b[l - 1].p, Lc.dirmask.p);
+    E.resid(l, u, tmp, b);
+    E.restrict_to(l - 1, tmp, W.b[l - 1].p);
   }
   int j = (p0 == 'V') ? 1 : (p0 == 'W') ? 2 : (p0 == 'F') ? 3 : 0;
   T* uc = W.u[l - 1].p;
   T* tc = W.v[l - 1].p;
   bool czero = true; // Zero(u) on l-1
   for (int i = 0; i < j; ++i)
-    czero = mgstep<T>(c, W, l - 1, finelevel, coarselevel, p0, p, uc, tc,
+    czero = mgstep<T>(E, W, l - 1, finelevel, coarselevel, p0, p, uc, tc,
                       W.b[l - 1].p, czero);
   if (czero) // no sweep ran on l-1: its u is the zero of Zero(u)
-    launch(c, k_fill<T>, stream_blocks(Lc.ndof()), 256, (int64_t)Lc.ndof(), uc, T(0));
+    E.fill0(l - 1, uc);
   if ((l == 0) && (p == 'F'))
     p0 = 'W';
-  if (u_zero) {
-    launch(c, k_fill<T>, stream_blocks(L.ndof()), 256, (int64_t)L.ndof(), u, T(0));
-  }
+  if (u_zero)
+    E.fill0(l, u);
   // Zero(v); prolongate_add; HNZero; SetBoundaryVectorZero(v); Add(u, mgomega, v)
-  launch(c, k_prolong<1, T>, blocks_for(Tr.nf, 256), 256, Tr.nf, Tr.pptr.p,
-         Tr.pent.p, (const T*)uc, u, L.dirmask.p, P.mgomega);
+  E.prolong(l - 1, uc, u);
   bool post_zero = false;
-  smooth<T>(c, l, P.iterpost, u, tmp, b, post_zero);
+  smooth<T>(E, l, P.iterpost, u, tmp, b, post_zero);
   return false;
 }
 
@@ -576,9 +978,9 @@ precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero)
     std::swap(u, tmp);
   char p = P.mgtype;
   char p0 = (p == 'F') ? 'W' : p;
-  if (mgstep<T>(c, W, fl, fl, 0, p0, p, u, tmp, y, x_zero))
-    launch(c, k_fill<T>, stream_blocks(c.L[fl].ndof()), 256,
-           (int64_t)c.L[fl].ndof(), u, T(0));
+  Emit<T> E{ c, nullptr };
+  if (mgstep<T>(E, W, fl, fl, 0, p0, p, u, tmp, y, x_zero))
+    E.fill0(fl, u);
   if (u != x) {
     GB_CUDA(cudaMemcpyAsync(x, u, c.L[fl].ndof() * sizeof(T),
                             cudaMemcpyDeviceToDevice, c.stream));
@@ -909,6 +1311,109 @@ add_while(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
   return cp.conditional.phGraph_out[0];
 }
 
+// Buffers of the flexible solver for cycle precision T.
+template<class T>
+struct FBufs
+{
+  T* Z;
+  T* zfix;
+  T* rhs;
+};
+
+template<class T>
+static FBufs<T>
+fg_buffers(Context& c, int prec)
+{
+  ensure_work(c);
+  const int vmax = c.params.gmressize;
+  GB_REQUIRE(vmax <= kCgsMaxJ, GB_EINVAL, "flexible solver needs gmressize <= 32");
+  const int64_t n = c.L[c.nlevels - 1].ndof();
+  GB_CUDA(c.krylov.alloc((vmax + 1) * n));
+  GB_CUDA(c.pbuf.alloc(n));
+  if (!c.G.p)
+    GB_CUDA(c.G.alloc(1));
+  GB_CUDA(c.xg.alloc(n));
+  GB_CUDA(c.bg.alloc(n));
+  if (prec == GB_FP32) {
+    GB_CUDA(c.zb32.alloc(vmax * n));
+    GB_CUDA(c.zfix32.alloc(n));
+    GB_CUDA(c.rhs32.alloc(n));
+    return FBufs<T>{ reinterpret_cast<T*>(c.zb32.p), reinterpret_cast<T*>(c.zfix32.p),
+                     reinterpret_cast<T*>(c.rhs32.p) };
+  }
+  GB_CUDA(c.zb64.alloc(vmax * n));
+  GB_CUDA(c.zfix64.alloc(n));
+  GB_CUDA(c.rhs64.alloc(n));
+  return FBufs<T>{ reinterpret_cast<T*>(c.zb64.p), reinterpret_cast<T*>(c.zfix64.p),
+                   reinterpret_cast<T*>(c.rhs64.p) };
+}
+
+// Segments of the flexible solve; the graph captures them, the eager driver
+// (profiling) launches them from host loops. hOuter/hInner == 0: no graph.
+template<class T>
+static void
+fg_setup(Context& c)
+{
+  const int64_t n = c.L[c.nlevels - 1].ndof();
+  GmresDev* G = c.G.p;
+  launch(c, k_fg_setup, 1, 1, G, c.params.tol, c.params.globaltol, c.params.maxiter);
+  dot_dev(c, n, c.bg.p, c.bg.p, RedOut{ &G->bnorm, nullptr, nullptr, 1 });
+  launch(c, k_fill<double>, stream_blocks(n), 256, n, c.xg.p, 0.0);
+}
+
+template<class T>
+static void
+fg_outer_pre(Context& c, cudaGraphConditionalHandle hOuter,
+             cudaGraphConditionalHandle hInner, int use_cond)
+{
+  const int fl = c.nlevels - 1;
+  Level& L = c.L[fl];
+  const int64_t n = L.ndof();
+  GmresDev* G = c.G.p;
+  double* V = c.krylov.p;
+  spmv<kResidDir, double, double, double>(c, L, L.A, (const double*)c.xg.p, V, c.bg.p,
+                                          nullptr, 0.0);
+  dot_dev(c, n, V, V, RedOut{ &G->beta_tmp, nullptr, nullptr, 1 });
+  launch(c, k_fg_restart, 1, 1, G, hOuter, hInner, c.params.gmressize - 1, 50,
+         use_cond);
+  launch(c, k_scale_dev, stream_blocks(n), 256, n, V, (const double*)&G->inv);
+}
+
+template<class T>
+static void
+fg_inner(Context& c, const FBufs<T>& F, cudaGraphConditionalHandle hInner, int use_cond)
+{
+  const int fl = c.nlevels - 1;
+  Level& L = c.L[fl];
+  const int64_t n = L.ndof();
+  GmresDev* G = c.G.p;
+  double* V = c.krylov.p;
+  launch(c, k_load_idx<T>, stream_blocks(n), 256, n, F.rhs, (const double*)V,
+         (const int*)&G->j);
+  precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true);
+  spmv<kAx, double, T, double>(c, L, L.A, (const T*)F.zfix, V, nullptr, nullptr, 1.0,
+                               (const int*)&G->j, n, F.Z);
+  const int rg = static_cast<int>(std::max<int64_t>(
+    1, std::min<int64_t>((n + kCgsThreads - 1) / kCgsThreads, kMaxRedBlocks)));
+  launch(c, k_cgs<0>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p);
+  launch(c, k_cgs<1>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p);
+  launch(c, k_cgs<2>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p);
+  launch(c, k_fg_step, 1, 1, G, hInner, c.params.gmressize - 1, use_cond);
+  launch(c, k_scale_idx, stream_blocks(n), 256, n, V, (const int*)&G->j,
+         (const double*)&G->inv);
+}
+
+template<class T>
+static void
+fg_outer_post(Context& c, const FBufs<T>& F)
+{
+  const int64_t n = c.L[c.nlevels - 1].ndof();
+  GmresDev* G = c.G.p;
+  launch(c, k_fg_backward, 1, 1, G);
+  launch(c, k_fg_update<T>, stream_blocks(n), 256, n, c.xg.p, (const T*)F.Z,
+         (const GmresDev*)G);
+}
+
 // Builds the one-graph solve: setup; WHILE(refine) { r = b - A x; beta; restart;
 // v0 = r / beta; WHILE(arnoldi) { z = M v_j (cycle in T); v_{j+1} = A z; CGS2;
 // Givens } ; y = H^-1 gamma; x += Z y }. Operates on the context's xg/bg.
@@ -916,110 +1421,88 @@ template<class T>
 static void
 build_fgraph(Context& c, int prec)
 {
-  ensure_work(c);
-  const int vmax = c.params.gmressize;
-  const int m = vmax - 1;
-  GB_REQUIRE(m + 1 <= kCgsMaxJ, GB_EINVAL, "graph solver needs gmressize <= 33");
-  const int fl = c.nlevels - 1;
-  Level& L = c.L[fl];
-  const int64_t n = L.ndof();
-  GB_CUDA(c.krylov.alloc((vmax + 1) * n));
-  GB_CUDA(c.pbuf.alloc(n));
-  if (!c.G.p)
-    GB_CUDA(c.G.alloc(1));
-  GB_CUDA(c.xg.alloc(n));
-  GB_CUDA(c.bg.alloc(n));
-  T* Z;
-  T* zfix;
-  T* rhs;
-  if (prec == GB_FP32) {
-    GB_CUDA(c.zb32.alloc(vmax * n));
-    GB_CUDA(c.zfix32.alloc(n));
-    GB_CUDA(c.rhs32.alloc(n));
-    Z = reinterpret_cast<T*>(c.zb32.p);
-    zfix = reinterpret_cast<T*>(c.zfix32.p);
-    rhs = reinterpret_cast<T*>(c.rhs32.p);
-  } else {
-    GB_CUDA(c.zb64.alloc(vmax * n));
-    GB_CUDA(c.zfix64.alloc(n));
-    GB_CUDA(c.rhs64.alloc(n));
-    Z = reinterpret_cast<T*>(c.zb64.p);
-    zfix = reinterpret_cast<T*>(c.zfix64.p);
-    rhs = reinterpret_cast<T*>(c.rhs64.p);
+  const FBufs<T> F = fg_buffers<T>(c, prec);
+  const int64_t n = c.L[c.nlevels - 1].ndof();
+  auto& FG = c.fg[prec];
+  if (FG.exec) {
+    cudaGraphExecDestroy(FG.exec);
+    FG.exec = nullptr;
   }
-  MgWork<T>& W = work<T>(c);
-  auto& F = c.fg[prec];
-  if (F.exec) {
-    cudaGraphExecDestroy(F.exec);
-    F.exec = nullptr;
+  if (FG.graph) {
+    cudaGraphDestroy(FG.graph);
+    FG.graph = nullptr;
   }
-  if (F.graph) {
-    cudaGraphDestroy(F.graph);
-    F.graph = nullptr;
-  }
+  // Record the coarse-kernel programs outside the capture (one eager cycle on
+  // zeros), so that nothing is allocated or copied while capturing.
+  GB_CUDA(cudaMemsetAsync(F.rhs, 0, n * sizeof(T), c.stream));
+  precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true);
   GB_CUDA(cudaStreamSynchronize(c.stream));
-  GmresDev* G = c.G.p;
-  double* V = c.krylov.p;
-  double* x = c.xg.p;
-  const double* b = c.bg.p;
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
   cudaGraph_t top;
   GB_CUDA(cudaGraphCreate(&top, 0));
-  F.graph = top;
+  FG.graph = top;
   // each conditional handle belongs to the graph that holds its node
   cudaGraphConditionalHandle hOuter, hInner;
   GB_CUDA(cudaGraphConditionalHandleCreate(&hOuter, top, 1, cudaGraphCondAssignDefault));
-  const int maxrestarts = 50;
   const int64_t k_start = c.launches;
-  int64_t k0 = c.launches;
-  // setup
   GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, top, nullptr, nullptr, 0, mode));
-  launch(c, k_fg_setup, 1, 1, G, c.params.tol, c.params.globaltol, c.params.maxiter);
-  dot_dev(c, n, b, b, RedOut{ &G->bnorm, nullptr, nullptr, 1 });
-  launch(c, k_fill<double>, stream_blocks(n), 256, n, x, 0.0);
+  fg_setup<T>(c);
   GB_CUDA(cudaStreamEndCapture(c.stream, &top));
-  F.setup_k = static_cast<int>(c.launches - k0);
+  FG.setup_k = static_cast<int>(c.launches - k_start);
   cudaGraphNode_t outerNode, innerNode;
   cudaGraph_t outerBody = add_while(top, leaf_nodes(top), hOuter, &outerNode);
   GB_CUDA(cudaGraphConditionalHandleCreate(&hInner, outerBody, 0,
                                            cudaGraphCondAssignDefault));
-  // refinement cycle start
-  k0 = c.launches;
+  const int64_t k0 = c.launches;
   GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, outerBody, nullptr, nullptr, 0, mode));
-  spmv<kResidDir, double, double, double>(c, L, L.A, (const double*)x, V, b, nullptr,
-                                          0.0);
-  dot_dev(c, n, V, V, RedOut{ &G->beta_tmp, nullptr, nullptr, 1 });
-  launch(c, k_fg_restart, 1, 1, G, hOuter, hInner, m, maxrestarts);
-  launch(c, k_scale_dev, stream_blocks(n), 256, n, V, (const double*)&G->inv);
+  fg_outer_pre<T>(c, hOuter, hInner, 1);
   GB_CUDA(cudaStreamEndCapture(c.stream, &outerBody));
   cudaGraph_t innerBody = add_while(outerBody, leaf_nodes(outerBody), hInner, &innerNode);
-  // Arnoldi step
-  int64_t k1 = c.launches;
+  const int64_t k1 = c.launches;
   GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, innerBody, nullptr, nullptr, 0, mode));
-  launch(c, k_load_idx<T>, stream_blocks(n), 256, n, rhs, (const double*)V,
-         (const int*)&G->j);
-  precondition_T<T>(c, W, zfix, rhs, true);
-  spmv<kAx, double, T, double>(c, L, L.A, (const T*)zfix, V, nullptr, nullptr, 1.0,
-                               (const int*)&G->j, n, Z);
-  const int rg = red_blocks(n);
-  launch(c, k_cgs<0>, rg, kRedThreads, n, V, G, c.partials.p, c.ticket.p);
-  launch(c, k_cgs<1>, rg, kRedThreads, n, V, G, c.partials.p, c.ticket.p);
-  launch(c, k_cgs<2>, rg, kRedThreads, n, V, G, c.partials.p, c.ticket.p);
-  launch(c, k_fg_step, 1, 1, G, hInner, m);
-  launch(c, k_scale_idx, stream_blocks(n), 256, n, V, (const int*)&G->j,
-         (const double*)&G->inv);
+  fg_inner<T>(c, F, hInner, 1);
   GB_CUDA(cudaStreamEndCapture(c.stream, &innerBody));
-  F.inner_k = static_cast<int>(c.launches - k1);
-  // cycle end: x += Z H^-1 gamma
-  int64_t k2 = c.launches;
+  FG.inner_k = static_cast<int>(c.launches - k1);
+  const int64_t k2 = c.launches;
   GB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, outerBody, &innerNode, nullptr, 1, mode));
-  launch(c, k_fg_backward, 1, 1, G);
-  launch(c, k_fg_update<T>, stream_blocks(n), 256, n, x, (const T*)Z, (const GmresDev*)G);
+  fg_outer_post<T>(c, F);
   GB_CUDA(cudaStreamEndCapture(c.stream, &outerBody));
-  F.outer_k = static_cast<int>(k1 - k0) + static_cast<int>(c.launches - k2);
+  FG.outer_k = static_cast<int>(k1 - k0) + static_cast<int>(c.launches - k2);
   c.launches = k_start; // capture executes nothing; executions are counted per solve
-  GB_CUDA(cudaGraphInstantiate(&F.exec, top, 0));
-  F.version = c.version;
+  GB_CUDA(cudaGraphInstantiate(&FG.exec, top, 0));
+  FG.version = c.version;
+}
+
+// The same solve driven from the host (no graph, no conditional nodes): used
+// when GB_GRAPH=0, e.g. for per-kernel profiling, which cannot see inside
+// conditional graph nodes.
+template<class T>
+static void
+fgmres_eager(Context& c, int prec)
+{
+  const FBufs<T> F = fg_buffers<T>(c, prec);
+  GmresDev* G = c.G.p;
+  fg_setup<T>(c);
+  for (;;) {
+    fg_outer_pre<T>(c, 0, 0, 0);
+    int st = 0;
+    GB_CUDA(cudaMemcpyAsync(&st, &G->stop, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+    if (!st) {
+      for (;;) {
+        fg_inner<T>(c, F, 0, 0);
+        int reached = 0;
+        GB_CUDA(cudaMemcpyAsync(&reached, &G->reached, sizeof(int),
+                                cudaMemcpyDeviceToHost, c.stream));
+        GB_CUDA(cudaStreamSynchronize(c.stream));
+        if (reached)
+          break;
+      }
+    }
+    fg_outer_post<T>(c, F);
+    if (st)
+      break;
+  }
 }
 
 // Runs the graph on b (device), result into x (device); info as gb_fgmres.
@@ -1028,18 +1511,31 @@ fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* in
              bool copy_in = true, bool copy_out = true)
 {
   auto& F = c.fg[prec];
-  if (!F.exec || F.version != c.version) {
+  if (c.use_graph && (!F.exec || F.version != c.version)) {
     if (prec == GB_FP32)
       build_fgraph<float>(c, prec);
     else
       build_fgraph<double>(c, prec);
   }
+  if (!c.use_graph) {
+    if (prec == GB_FP32)
+      fg_buffers<float>(c, prec);
+    else
+      fg_buffers<double>(c, prec);
+  }
   const int64_t n = c.L[c.nlevels - 1].ndof();
   if (copy_in && b != c.bg.p)
     GB_CUDA(cudaMemcpyAsync(c.bg.p, b, n * sizeof(double), cudaMemcpyDeviceToDevice,
                             c.stream));
+  const int64_t l_before = c.launches;
   GB_CUDA(cudaEventRecord(c.ev0, c.stream));
-  GB_CUDA(cudaGraphLaunch(F.exec, c.stream));
+  if (c.use_graph) {
+    GB_CUDA(cudaGraphLaunch(F.exec, c.stream));
+  } else if (prec == GB_FP32) {
+    fgmres_eager<float>(c, prec);
+  } else {
+    fgmres_eager<double>(c, prec);
+  }
   GB_CUDA(cudaEventRecord(c.ev1, c.stream));
   if (copy_out && x != c.xg.p)
     GB_CUDA(cudaMemcpyAsync(x, c.xg.p, n * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -1054,9 +1550,11 @@ fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* in
   float ms = 0;
   GB_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
   const int total = cnt[0], restarts = cnt[1];
-  const int64_t kernels = F.setup_k + int64_t(restarts + 1) * F.outer_k +
-                          int64_t(total) * F.inner_k;
-  c.launches += kernels;
+  int64_t kernels = c.launches - l_before;
+  if (c.use_graph) {
+    kernels = F.setup_k + int64_t(restarts + 1) * F.outer_k + int64_t(total) * F.inner_k;
+    c.launches += kernels;
+  }
   if (info) {
     fill_info(c, info, c.xg.p, c.bg.p);
     info->iterations = total;
@@ -1105,6 +1603,12 @@ gb_ctx_create(gb_ctx** out, int device)
     return GB_ENOMEM;
   try {
     ctx->device = device;
+    if (const char* e = getenv("GB_COARSE_KERNEL"))
+      ctx->coarse_on = atoi(e) != 0;
+    if (const char* e = getenv("GB_GRAPH"))
+      ctx->use_graph = atoi(e) != 0;
+    if (const char* e = getenv("GB_COARSE_DENSE"))
+      ctx->coarse_dense = atoi(e) != 0;
     GB_CUDA(cudaSetDevice(device));
     GB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     GB_CUDA(cudaEventCreate(&ctx->ev0));
@@ -1173,6 +1677,7 @@ gb_set_params(gb_ctx* ctx, const gb_params* p)
              "gmressize out of range [2, 128]");
   GB_REQUIRE(p->maxiter >= 1, GB_EINVAL, "maxiter must be >= 1");
   ctx->params = *p;
+  ctx->work_ready = false; // recorded coarse programs depend on the keys
   GB_API_END
 }
 
@@ -1325,24 +1830,33 @@ gb_level_set_transfer(gb_ctx* ctx, int lvl, int64_t ncoarse, const int64_t* c2f,
     prow[pr.first].push_back(pr.second);
     rrow[pr.second].push_back(pr.first);
   }
-  std::vector<int> pptr(nf + 1, 0), rptr(ncoarse + 1, 0);
+  // SELL-32 layout of both tables (see transfer_row), columns ascending
+  auto sell = [&](std::vector<std::vector<int64_t>>& rows, bool fine_rows,
+                  std::vector<int>& tsp, std::vector<uint32_t>& tent) {
+    const int64_t nr = static_cast<int64_t>(rows.size());
+    const int64_t ns = (nr + kSlice - 1) / kSlice;
+    tsp.assign(ns + 1, 0);
+    for (auto& r : rows)
+      std::sort(r.begin(), r.end());
+    for (int64_t sl = 0; sl < ns; ++sl) {
+      size_t w = 0;
+      for (int64_t q = sl * kSlice; q < std::min(nr, (sl + 1) * kSlice); ++q)
+        w = std::max(w, rows[q].size());
+      tsp[sl + 1] = tsp[sl] + static_cast<int>(w) * kSlice;
+    }
+    tent.assign(tsp[ns], kPadEntry);
+    for (int64_t q = 0; q < nr; ++q)
+      for (size_t j = 0; j < rows[q].size(); ++j) {
+        const int64_t other = rows[q][j];
+        const int code = fine_rows ? wcode[q] : wcode[other];
+        tent[tsp[q / kSlice] + j * kSlice + (q % kSlice)] =
+          static_cast<uint32_t>(other) | (uint32_t(code) << kWShift);
+      }
+  };
+  std::vector<int> pptr, rptr;
   std::vector<uint32_t> pent, rent;
-  pent.reserve(pairs.size());
-  rent.reserve(pairs.size());
-  for (int64_t f = 0; f < nf; ++f) {
-    auto& r = prow[f];
-    std::sort(r.begin(), r.end());
-    for (int64_t cc : r)
-      pent.push_back(static_cast<uint32_t>(cc) | (uint32_t(wcode[f]) << kWShift));
-    pptr[f + 1] = static_cast<int>(pent.size());
-  }
-  for (int64_t cc = 0; cc < ncoarse; ++cc) {
-    auto& r = rrow[cc];
-    std::sort(r.begin(), r.end());
-    for (int64_t f : r)
-      rent.push_back(static_cast<uint32_t>(f) | (uint32_t(wcode[f]) << kWShift));
-    rptr[cc + 1] = static_cast<int>(rent.size());
-  }
+  sell(prow, true, pptr, pent);
+  sell(rrow, false, rptr, rent);
   GB_CUDA(cudaStreamSynchronize(ctx->stream));
   Transfer& T = ctx->T[lvl];
   T.nc = static_cast<int>(ncoarse);
@@ -1572,7 +2086,8 @@ gb_smooth_jacobi(gb_ctx* ctx, int lvl, int niter, int x, int y, int h)
   double* u = xd;
   double* t = hd;
   bool zero = false;
-  smooth<double>(*ctx, lvl, niter, u, t, yd, zero);
+  Emit<double> E{ *ctx, nullptr };
+  smooth<double>(E, lvl, niter, u, t, yd, zero);
   if (u != xd)
     GB_CUDA(cudaMemcpyAsync(xd, u, ctx->L[lvl].ndof() * sizeof(double),
                             cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1730,8 +2245,32 @@ gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x, int64_t len,
 int
 gb_set_timing(gb_ctx* ctx, int on)
 {
-  (void)on;
-  return ctx ? GB_OK : GB_EINVAL;
+  GB_API_BEGIN
+  kt_flush(*ctx);
+  ctx->ktime = on != 0;
+  ctx->kt_acc.clear();
+  GB_API_END
+}
+
+int
+gb_get_kernel_times(gb_ctx* ctx, char* buf, int64_t len)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(buf && len > 0, GB_EINVAL, "null buffer");
+  kt_flush(*ctx);
+  std::string js = "{";
+  bool first = true;
+  for (auto& kv : ctx->kt_acc) {
+    char item[512];
+    snprintf(item, sizeof(item), "%s\"%s\": [%lld, %.6f]", first ? "" : ", ",
+             kv.first.c_str(), (long long)kv.second.first, kv.second.second);
+    js += item;
+    first = false;
+  }
+  js += "}";
+  GB_REQUIRE(int64_t(js.size()) < len, GB_EINVAL, "buffer too small");
+  memcpy(buf, js.c_str(), js.size() + 1);
+  GB_API_END
 }
 
 int

@@ -92,6 +92,7 @@ _SIGS = {
     "gb_get_kernel_count": [C.c_void_p, _P64],
     "gb_bench_spmv": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
     "gb_dot_noalloc": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
+    "gb_get_kernel_times": [C.c_void_p, C.c_char_p, C.c_int64],
 }
 
 
@@ -293,6 +294,16 @@ class Context:
         v = C.c_int64()
         self._chk(self._L.gb_get_kernel_count(self.h, C.byref(v)))
         return v.value
+
+    def set_timing(self, on=True):
+        self._chk(self._L.gb_set_timing(self.h, int(on)))
+
+    def kernel_times(self):
+        """{kernel name: (launches, total ms)} since set_timing(True)."""
+        import json
+        buf = C.create_string_buffer(1 << 20)
+        self._chk(self._L.gb_get_kernel_times(self.h, buf, len(buf)))
+        return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
 
     def bench_spmv(self, level, precision=GB_FP64, reps=10, flush_l2=True):
         ms, by = C.c_double(), C.c_double()

@@ -25,6 +25,8 @@ def main(argv=None):
     ap.add_argument("--refine", type=int, default=6)
     ap.add_argument("--spmv", type=int, default=0)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--ktime", action="store_true",
+                    help="per-kernel CUDA-event times of the last solve (GB_GRAPH=0)")
     a = ap.parse_args(argv)
 
     from gascoignelib_b200.build import build_library
@@ -46,13 +48,22 @@ def main(argv=None):
             return
         x, b = ctx.vec(), ctx.vec()
         ctx.upload(fl, b, P.rhs)
-        for _ in range(a.solves):
+        for it in range(a.solves):
+            if a.ktime and it == a.solves - 1:
+                ctx.set_timing(True)
             if a.method == "left":
                 info = ctx.gmres(x, b)
             else:
                 info = ctx.fgmres(x, b, GB_FP32 if a.method == "mixed" else GB_FP64)
             print(json.dumps({k: info[k] for k in ("iterations", "restarts", "device_ms",
                                                    "true_rel_residual", "kernel_launches")}))
+        if a.ktime:
+            kt = ctx.kernel_times()
+            tot = sum(v[1] for v in kt.values())
+            for name, (cnt, ms) in sorted(kt.items(), key=lambda kv: -kv[1][1]):
+                print(f"{cnt:6d} {1e3 * ms:10.1f} us {1e3 * ms / cnt:8.2f} us/launch "
+                      f"{100 * ms / tot:5.1f}%  {name[:90]}")
+            print(f"kernel time total {1e3 * tot:.1f} us")
 
 
 if __name__ == "__main__":

@@ -198,6 +198,10 @@ int gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x,
  * (CUDA events on the context stream); replaces GlobalTimer's vmult/smooth
  * labels (Common/stopwatch.h:143-270) for the device path. */
 int gb_set_timing(gb_ctx* ctx, int on);
+/* Per-kernel device times accumulated since gb_set_timing(ctx, 1), as JSON
+ * {"kernel name": [launches, total ms], ...}; kernels inside a CUDA graph are
+ * not timed individually (run the flexible solver with GB_GRAPH=0 for that). */
+int gb_get_kernel_times(gb_ctx* ctx, char* buf, int64_t len);
 int gb_get_kernel_count(const gb_ctx* ctx, int64_t* launches);
 /* Times `reps` launches of the finest-level SpMV y = A x in `precision`,
  * writing the L2 (126 MB) flush buffer between launches when flush_l2 != 0.

@@ -135,3 +135,66 @@ def test_single_level_and_small_gmres(ctx):
     assert rel_l2(ctx.download(0, x), xo) < 1e-12
     ctx.free(x)
     ctx.free(b)
+
+
+def _solve_with_env(env, P, method, prec=GB_FP32):
+    import os
+
+    from gascoignelib_b200.native import Context
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        with Context(0) as c:
+            c.load_problem(P)
+            c.set_params(gmressize=21, tol=1e-8, globaltol=1e-300, maxiter=200)
+            l = P.nlevels - 1
+            x, b = c.vec(), c.vec()
+            c.upload(l, b, P.rhs)
+            info = c.gmres(x, b) if method == "left" else c.fgmres(x, b, prec)
+            return c.download(l, x), info
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("method,prec", [("left", GB_FP64), ("flex", GB_FP32),
+                                         ("flex", GB_FP64)])
+def test_coarse_level_kernel_matches_per_level_kernels(method, prec):
+    """Levels with <= 1024 rows run in one single-CTA kernel; it does per row
+    what the per-level kernels do, so the solves agree bit for bit (up to the
+    sign of zeros)."""
+    kappa, rhs = seeded_inputs(3, 1, 5)
+    P = structured_problem(3, 1, 5, kappa, rhs)
+    u1, i1 = _solve_with_env({"GB_COARSE_KERNEL": "1", "GB_COARSE_DENSE": "0"}, P,
+                             method, prec)
+    u0, i0 = _solve_with_env({"GB_COARSE_KERNEL": "0"}, P, method, prec)
+    assert i1["iterations"] == i0["iterations"]
+    assert np.array_equal(u1, u0)
+    assert i1["kernel_launches"] < i0["kernel_launches"]
+
+
+@pytest.mark.parametrize("prec", [GB_FP32, GB_FP64])
+def test_graph_and_host_driven_flexible_solver_agree(prec):
+    kappa, rhs = seeded_inputs(3, 1, 4)
+    P = structured_problem(3, 1, 4, kappa, rhs)
+    ug, ig = _solve_with_env({"GB_GRAPH": "1"}, P, "flex", prec)
+    ue, ie = _solve_with_env({"GB_GRAPH": "0"}, P, "flex", prec)
+    assert ig["iterations"] == ie["iterations"] and ig["restarts"] == ie["restarts"]
+    assert np.array_equal(ug, ue)
+    assert ig["kernel_launches"] == ie["kernel_launches"]
+
+
+@pytest.mark.parametrize("prec", [GB_FP32, GB_FP64])
+def test_coarse_dense_map_matches_op_program(prec):
+    """The coarse sub-cycle applied as its precomputed dense map agrees with
+    running its ops (rounding-level differences only)."""
+    kappa, rhs = seeded_inputs(3, 1, 5)
+    P = structured_problem(3, 1, 5, kappa, rhs)
+    ud, idn = _solve_with_env({"GB_COARSE_DENSE": "1"}, P, "flex", prec)
+    uo, io = _solve_with_env({"GB_COARSE_DENSE": "0"}, P, "flex", prec)
+    assert abs(idn["iterations"] - io["iterations"]) <= 1
+    assert idn["true_rel_residual"] <= 1e-8 and io["true_rel_residual"] <= 1e-8
+    assert rel_l2(ud, uo) < (1e-6 if prec == GB_FP32 else 1e-9)
