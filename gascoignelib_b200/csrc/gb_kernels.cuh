@@ -1167,4 +1167,19 @@ k_coarse_apply(int n_root, int ncols, int nb, const T* __restrict__ K,
     u_out[warp] = static_cast<T>(acc);
 }
 
+// Reads n 16-byte words (an L2 eviction that leaves only clean lines behind);
+// the sink write never happens for real data.
+__global__ void
+k_read_flush(const uint4* __restrict__ p, int64_t n, unsigned* sink)
+{
+  unsigned acc = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 v = __ldcs(p + i);
+    acc ^= v.x ^ v.y ^ v.z ^ v.w;
+  }
+  if (acc == 0x9e3779b9u && sink)
+    *sink = acc;
+}
+
 } // namespace gb

@@ -2297,9 +2297,14 @@ gb_bench_spmv(gb_ctx* ctx, int lvl, int precision, int reps, int flush_l2,
   GB_CUDA(cudaEventCreate(&a));
   GB_CUDA(cudaEventCreate(&bq));
   double total = 0;
+  if (flush_l2 == 2) // first touch, so that the read flush finds mapped pages
+    GB_CUDA(cudaMemsetAsync(ctx->flush.p, 0, flush_bytes, ctx->stream));
   for (int r = 0; r < reps; ++r) {
-    if (flush_l2)
+    if (flush_l2 == 1)
       GB_CUDA(cudaMemsetAsync(ctx->flush.p, r & 0xff, flush_bytes, ctx->stream));
+    else if (flush_l2 == 2)
+      k_read_flush<<<4 * 148, 512, 0, ctx->stream>>>(
+        reinterpret_cast<const uint4*>(ctx->flush.p), int64_t(flush_bytes / 16), nullptr);
     GB_CUDA(cudaEventRecord(a, ctx->stream));
     if (precision == GB_FP32)
       spmv<kAx, float, float, float>(*ctx, L, L.A, (const float*)ctx->w32.b[lvl].p,

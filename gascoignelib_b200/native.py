@@ -305,7 +305,8 @@ class Context:
         self._chk(self._L.gb_get_kernel_times(self.h, buf, len(buf)))
         return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
 
-    def bench_spmv(self, level, precision=GB_FP64, reps=10, flush_l2=True):
+    def bench_spmv(self, level, precision=GB_FP64, reps=10, flush_l2=2):
+        """flush_l2: 0 none, 1 write-flush, 2 read-flush (clean lines)."""
         ms, by = C.c_double(), C.c_double()
         self._chk(self._L.gb_bench_spmv(self.h, level, precision, reps, int(flush_l2),
                                         C.byref(ms), C.byref(by)))

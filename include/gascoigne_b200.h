@@ -203,9 +203,11 @@ int gb_set_timing(gb_ctx* ctx, int on);
  * not timed individually (run the flexible solver with GB_GRAPH=0 for that). */
 int gb_get_kernel_times(gb_ctx* ctx, char* buf, int64_t len);
 int gb_get_kernel_count(const gb_ctx* ctx, int64_t* launches);
-/* Times `reps` launches of the finest-level SpMV y = A x in `precision`,
- * writing the L2 (126 MB) flush buffer between launches when flush_l2 != 0.
- * Returns the average launch time (ms) and the algorithmic bytes per launch. */
+/* Times `reps` launches of the SpMV y = A x of `level` in `precision` with
+ * CUDA events around each launch. flush_l2 between launches: 0 none, 1 write
+ * a 256 MB buffer (leaves the L2 full of dirty lines), 2 read a 256 MB buffer
+ * (leaves clean lines). Returns the average launch time (ms) and the
+ * algorithmic bytes per launch. */
 int gb_bench_spmv(gb_ctx* ctx, int level, int precision, int reps,
                   int flush_l2, double* ms_per_launch, double* bytes_per_launch);
 
