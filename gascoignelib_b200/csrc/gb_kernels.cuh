@@ -8,6 +8,13 @@
 
 namespace gb {
 
+// Programmatic dependent launch (sm_90 and later): every kernel first waits
+// until the kernel before it in the stream has completed and its memory is
+// visible. The next kernel may start launching when this one's blocks exit (the
+// implicit trigger), so its launch overlaps this kernel's drain without parking
+// its CTAs on SMs that this kernel still needs. A no-op for ordinary launches.
+#define GB_PDL_ENTRY() asm volatile("griddepcontrol.wait;" ::: "memory")
+
 constexpr int kSlice = 32;          // SELL slice height = warp size
 constexpr int kSpmvThreads = 256;   // 8 warps = 8 slices per CTA
 constexpr int kRedThreads = 256;
@@ -116,6 +123,7 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
        const uint8_t* __restrict__ dirmask, double alpha_,
        const int* __restrict__ yidx, int64_t ystride, TX* __restrict__ xcopy)
 {
+  GB_PDL_ENTRY();
   using TA = typename Acc<TV, TO>::type;
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= A.n)
@@ -171,6 +179,7 @@ __global__ void
 k_jacobi_from_zero(int n, const TV* __restrict__ dinv, const T* __restrict__ b,
                    T* __restrict__ x, double omega)
 {
+  GB_PDL_ENTRY();
   using TA = typename Acc<TV, T>::type;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n)
@@ -232,6 +241,7 @@ k_restrict(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ ten
            const T* __restrict__ fine, T* __restrict__ coarse,
            const uint8_t* __restrict__ cdir)
 {
+  GB_PDL_ENTRY();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nc)
     return;
@@ -248,6 +258,7 @@ k_prolong(int nf, const int* __restrict__ tsp, const uint32_t* __restrict__ tent
           const T* __restrict__ coarse, T* __restrict__ fine,
           const uint8_t* __restrict__ fdir, double mgomega)
 {
+  GB_PDL_ENTRY();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf)
     return;
@@ -267,6 +278,7 @@ template<class T>
 __global__ void
 k_fill(int64_t n, T* __restrict__ y, T v)
 {
+  GB_PDL_ENTRY();
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   for (; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = v;
@@ -277,6 +289,7 @@ template<class TI, class TO>
 __global__ void
 k_equ(int64_t n, TO* __restrict__ y, double s, const TI* __restrict__ x)
 {
+  GB_PDL_ENTRY();
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   for (; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = static_cast<TO>(s * static_cast<double>(x[i]));
@@ -287,6 +300,7 @@ template<class TI, class TO>
 __global__ void
 k_convert(int64_t n, TO* __restrict__ y, const TI* __restrict__ x)
 {
+  GB_PDL_ENTRY();
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   for (; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = static_cast<TO>(x[i]);
@@ -296,6 +310,7 @@ k_convert(int64_t n, TO* __restrict__ y, const TI* __restrict__ x)
 __global__ void
 k_add(int64_t n, double* __restrict__ y, double s, const double* __restrict__ x)
 {
+  GB_PDL_ENTRY();
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   for (; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = fma(s, x[i], y[i]);
@@ -305,6 +320,7 @@ k_add(int64_t n, double* __restrict__ y, double s, const double* __restrict__ x)
 __global__ void
 k_scale_dev(int64_t n, double* __restrict__ y, const double* __restrict__ scale)
 {
+  GB_PDL_ENTRY();
   const double s = *scale;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   for (; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -316,6 +332,7 @@ template<class T>
 __global__ void
 k_dirichlet_zero(int nd, const int* __restrict__ dofs, T* __restrict__ y)
 {
+  GB_PDL_ENTRY();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nd)
     y[dofs[i]] = T(0);
@@ -328,6 +345,7 @@ __global__ void
 k_multi_axpy(int64_t n, double* __restrict__ x, const TV* __restrict__ base,
              int64_t stride, const double* __restrict__ coef, int k)
 {
+  GB_PDL_ENTRY();
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   for (; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double acc = x[i];
@@ -406,6 +424,7 @@ __global__ void __launch_bounds__(kRedThreads)
 k_dot(int64_t n, const TA* __restrict__ a, const TB* __restrict__ b,
       double* partials, unsigned* ticket, RedOut ro)
 {
+  GB_PDL_ENTRY();
   __shared__ double sh[32];
   double v = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -422,6 +441,7 @@ k_mgs(int64_t n, double* __restrict__ vv, const double* __restrict__ vi,
       const double* __restrict__ dcoef, const double* __restrict__ vnext,
       double* partials, unsigned* ticket, RedOut ro)
 {
+  GB_PDL_ENTRY();
   __shared__ double sh[32];
   const double d = vi ? *dcoef : 0.0;
   double v = 0.0;
@@ -448,6 +468,7 @@ __global__ void
 k_blockdiag_inverse(int n, const double* __restrict__ dblocks, double* __restrict__ dinv64,
                     float* __restrict__ dinv32)
 {
+  GB_PDL_ENTRY();
   int node = blockIdx.x * blockDim.x + threadIdx.x;
   if (node >= n)
     return;
@@ -574,6 +595,7 @@ cginfo_check(CGInfoDev& I, double resi)
 __global__ void
 k_gmres_init(GmresDev* G, const double* rho_p)
 {
+  GB_PDL_ENTRY();
   double rho = *rho_p;
   G->gamma[0] = rho;
   G->zero_rho = (rho == 0.0);
@@ -588,6 +610,7 @@ k_gmres_init(GmresDev* G, const double* rho_p)
 __global__ void
 k_gmres_step(GmresDev* G, int dim, int second_pass, int mode, int maxsteps)
 {
+  GB_PDL_ENTRY();
   const int last = dim - 1;
   double* h = G->H[last];
   const double s = h[dim];
@@ -629,6 +652,7 @@ k_gmres_step(GmresDev* G, int dim, int second_pass, int mode, int maxsteps)
 __global__ void
 k_gmres_backward(GmresDev* G, int dim)
 {
+  GB_PDL_ENTRY();
   for (int i = dim - 1; i >= 0; i--) {
     double s = G->gamma[i];
     for (int j = i + 1; j < dim; j++)
@@ -641,6 +665,7 @@ k_gmres_backward(GmresDev* G, int dim)
 __global__ void
 k_fgmres_restart(GmresDev* G, const double* beta_p, int vmax)
 {
+  GB_PDL_ENTRY();
   double beta = *beta_p;
   G->beta = beta;
   for (int j = 0; j < vmax && j < kMaxV; ++j) {
@@ -668,6 +693,7 @@ constexpr int kCgsMaxJ = 32; // graph path: gmressize <= 33
 __global__ void
 k_fg_setup(GmresDev* G, double tol, double globaltol, int maxiter)
 {
+  GB_PDL_ENTRY();
   G->info.tol = tol;
   G->info.globaltol = globaltol;
   G->info.maxiter = maxiter;
@@ -688,6 +714,7 @@ __global__ void
 k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
              cudaGraphConditionalHandle inner, int m, int maxrestarts, int use_cond)
 {
+  GB_PDL_ENTRY();
   const double beta = G->beta_tmp;
   const double aim = fmax(G->info.tol * G->bnorm, G->info.globaltol);
   const int conv = (beta <= aim) || beta == 0.0;
@@ -726,15 +753,27 @@ k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
 }
 
 // y = (TO) V[(*jp) * n + i]   (Arnoldi vector j into the cycle's right-hand side)
+// y = (TO) v_j with v_j = V[(*jp) * n + i]; for j > 0 the pending
+// normalisation v_j *= 1/h[j][j-1] (G->inv) is applied first and stored back
+// (v_0 was normalised at the restart).
 template<class TO>
 __global__ void
-k_load_idx(int64_t n, TO* __restrict__ y, const double* __restrict__ V,
-           const int* __restrict__ jp)
+k_load_idx(int64_t n, TO* __restrict__ y, double* __restrict__ V,
+           const GmresDev* __restrict__ G)
 {
-  const double* v = V + int64_t(*jp) * n;
+  GB_PDL_ENTRY();
+  const int j = G->j;
+  double* v = V + int64_t(j) * n;
+  const double s = G->inv;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    y[i] = static_cast<TO>(v[i]);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double t = v[i];
+    if (j > 0) {
+      t = s * t;
+      v[i] = t;
+    }
+    y[i] = static_cast<TO>(t);
+  }
 }
 
 // V[(*jp) * n + i] *= *s
@@ -742,6 +781,7 @@ __global__ void
 k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
             const double* __restrict__ sp)
 {
+  GB_PDL_ENTRY();
   double* v = V + int64_t(*jp) * n;
   const double s = *sp;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -758,11 +798,17 @@ k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
 // and deterministic (fixed grid, fixed order).
 constexpr int kCgsThreads = 1024;
 
+__device__ void fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m,
+                        int use_cond);
+
+// MODE 2 also performs the Givens update and the loop test (fg_step) in its
+// last block, after the norm is known.
 template<int MODE>
 __global__ void __launch_bounds__(kCgsThreads)
 k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
-      unsigned* ticket)
+      unsigned* ticket, cudaGraphConditionalHandle inner, int m, int use_cond)
 {
+  GB_PDL_ENTRY();
   constexpr int kWarps = kCgsThreads / 32;
   __shared__ double s_coef[kCgsMaxJ];
   __shared__ double s_warp[kWarps][kCgsMaxJ];
@@ -839,15 +885,20 @@ k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
       }
     }
   }
-  if (tid == 0)
+  if (tid == 0) {
     *ticket = 0u;
+    if (MODE == 2) {
+      __threadfence_block();
+      fg_step(G, inner, m, use_cond);
+    }
+  }
 }
 
 // Givens update of column j (LinAlg/gmres.cc:88-104 applied to the flexible
 // Hessenberg), residual estimate |gamma[j+1]| = ||b - A x_j|| in exact
 // arithmetic, then j += 1 and the inner loop condition.
-__global__ void
-k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
+__device__ void
+fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
 {
   const int last = G->j, dim = last + 1;
   double* h = G->H[last];
@@ -879,10 +930,18 @@ k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
     cudaGraphSetConditional(inner, reached ? 0 : 1);
 }
 
+__global__ void
+k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
+{
+  GB_PDL_ENTRY();
+  fg_step(G, inner, m, use_cond);
+}
+
 // hs = H^-1 gamma on the first G->j columns (Common/mult.h:130-141)
 __global__ void
 k_fg_backward(GmresDev* G)
 {
+  GB_PDL_ENTRY();
   const int dim = G->j;
   for (int i = dim - 1; i >= 0; i--) {
     double s = G->gamma[i];
@@ -898,6 +957,7 @@ __global__ void
 k_fg_update(int64_t n, double* __restrict__ x, const TZ* __restrict__ Z,
             const GmresDev* __restrict__ G)
 {
+  GB_PDL_ENTRY();
   const int k = G->j;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -1044,6 +1104,7 @@ k_coarse_cycle(const CoarseOp* __restrict__ ops, int nops,
                const CoarsePrefetch* __restrict__ pre, int npre, int vec_bytes,
                CoarseBatch batch)
 {
+  GB_PDL_ENTRY();
   extern __shared__ __align__(16) unsigned char smem[];
   CoarseOp* s_ops = reinterpret_cast<CoarseOp*>(smem + vec_bytes);
   const int t = threadIdx.x;
@@ -1151,6 +1212,7 @@ __global__ void
 k_coarse_apply(int n_root, int ncols, int nb, const T* __restrict__ K,
                const T* __restrict__ b, const T* __restrict__ u_in, T* __restrict__ u_out)
 {
+  GB_PDL_ENTRY();
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n_root) // whole warps exit together
@@ -1172,6 +1234,7 @@ k_coarse_apply(int n_root, int ncols, int nb, const T* __restrict__ K,
 __global__ void
 k_read_flush(const uint4* __restrict__ p, int64_t n, unsigned* sink)
 {
+  GB_PDL_ENTRY();
   unsigned acc = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {

@@ -350,6 +350,7 @@ struct gb_ctx
   bool coarse_on = true;
   bool coarse_dense = true; // apply the coarse sub-cycle as its precomputed map
   bool use_graph = true; // flexible solver as one CUDA graph (GB_GRAPH=0: host loops)
+  bool pdl = true;       // programmatic dependent launch between kernels
   // per-kernel timing
   bool ktime = false;
   struct KtPending
@@ -450,32 +451,38 @@ kt_flush(Context& c)
   c.kt_pending.clear();
 }
 
-template<class K, class... Args>
+// Launches on the context stream; with programmatic dependent launch unless
+// GB_PDL=0 (every kernel begins with GB_PDL_ENTRY).
+template<class... KArgs, class... Args>
 static void
-launch_smem(Context& c, K kern, int grid, int block, int smem, Args... args)
+launch_smem(Context& c, void (*kern)(KArgs...), int grid, int block, int smem,
+            Args... args)
 {
   if (grid <= 0)
     return;
   cudaEvent_t e0;
   kt_begin(c, &e0);
-  kern<<<grid, block, smem, c.stream>>>(args...);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = c.pdl ? 1 : 0;
+  GB_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
   c.launches++;
   check_launch(c);
   kt_end(c, e0, reinterpret_cast<const void*>(kern));
 }
 
-template<class K, class... Args>
+template<class... KArgs, class... Args>
 static void
-launch(Context& c, K kern, int grid, int block, Args... args)
+launch(Context& c, void (*kern)(KArgs...), int grid, int block, Args... args)
 {
-  if (grid <= 0)
-    return;
-  cudaEvent_t e0;
-  kt_begin(c, &e0);
-  kern<<<grid, block, 0, c.stream>>>(args...);
-  c.launches++;
-  check_launch(c);
-  kt_end(c, e0, reinterpret_cast<const void*>(kern));
+  launch_smem(c, kern, grid, block, 0, args...);
 }
 
 static int
@@ -1011,6 +1018,7 @@ ensure_gmres(Context& c, int vmax, bool flexible, int prec)
 __global__ void
 k_gmres_setup(GmresDev* G, double tol, double globaltol, int maxiter)
 {
+  GB_PDL_ENTRY();
   G->info.tol = tol;
   G->info.globaltol = globaltol;
   G->info.breaktol = 1e15;
@@ -1030,6 +1038,7 @@ k_gmres_setup(GmresDev* G, double tol, double globaltol, int maxiter)
 __global__ void
 k_scale_gmres(int64_t n, double* __restrict__ y, const GmresDev* G)
 {
+  GB_PDL_ENTRY();
   if (G->need_reortho)
     return;
   const double s = G->inv;
@@ -1286,10 +1295,12 @@ leaf_nodes(cudaGraph_t g)
   std::vector<cudaGraphNode_t> nodes(nn);
   if (nn)
     GB_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
-  GB_CUDA(cudaGraphGetEdges(g, nullptr, nullptr, &ne));
+  // _v2: the graph may hold programmatic (PDL) edges
+  GB_CUDA(cudaGraphGetEdges_v2(g, nullptr, nullptr, nullptr, &ne));
   std::vector<cudaGraphNode_t> from(ne), to(ne);
+  std::vector<cudaGraphEdgeData> ed(ne);
   if (ne)
-    GB_CUDA(cudaGraphGetEdges(g, from.data(), to.data(), &ne));
+    GB_CUDA(cudaGraphGetEdges_v2(g, from.data(), to.data(), ed.data(), &ne));
   std::vector<cudaGraphNode_t> leaves;
   for (auto nd : nodes)
     if (std::find(from.begin(), from.end(), nd) == from.end())
@@ -1388,19 +1399,18 @@ fg_inner(Context& c, const FBufs<T>& F, cudaGraphConditionalHandle hInner, int u
   const int64_t n = L.ndof();
   GmresDev* G = c.G.p;
   double* V = c.krylov.p;
-  launch(c, k_load_idx<T>, stream_blocks(n), 256, n, F.rhs, (const double*)V,
-         (const int*)&G->j);
+  launch(c, k_load_idx<T>, stream_blocks(n), 256, n, F.rhs, V, (const GmresDev*)G);
   precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true);
   spmv<kAx, double, T, double>(c, L, L.A, (const T*)F.zfix, V, nullptr, nullptr, 1.0,
                                (const int*)&G->j, n, F.Z);
   const int rg = static_cast<int>(std::max<int64_t>(
     1, std::min<int64_t>((n + kCgsThreads - 1) / kCgsThreads, kMaxRedBlocks)));
-  launch(c, k_cgs<0>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p);
-  launch(c, k_cgs<1>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p);
-  launch(c, k_cgs<2>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p);
-  launch(c, k_fg_step, 1, 1, G, hInner, c.params.gmressize - 1, use_cond);
-  launch(c, k_scale_idx, stream_blocks(n), 256, n, V, (const int*)&G->j,
-         (const double*)&G->inv);
+  const int m = c.params.gmressize - 1;
+  launch(c, k_cgs<0>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m, 0);
+  launch(c, k_cgs<1>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m, 0);
+  // norm, Givens update, loop test; v_{j+1} is normalised by the next k_load_idx
+  launch(c, k_cgs<2>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m,
+         use_cond);
 }
 
 template<class T>
@@ -1609,6 +1619,8 @@ gb_ctx_create(gb_ctx** out, int device)
       ctx->use_graph = atoi(e) != 0;
     if (const char* e = getenv("GB_COARSE_DENSE"))
       ctx->coarse_dense = atoi(e) != 0;
+    if (const char* e = getenv("GB_PDL"))
+      ctx->pdl = atoi(e) != 0;
     GB_CUDA(cudaSetDevice(device));
     GB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     GB_CUDA(cudaEventCreate(&ctx->ev0));
