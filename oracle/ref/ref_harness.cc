@@ -58,7 +58,7 @@ struct Config
   int dim = 3;
   int coarse = 1; // coarse mesh cells per dimension (1 or 2)
   int refine = 3; // global refinements
-  std::string kappa, rhs, out = ".";
+  std::string kappa, rhs, dualrhs, out = ".";
   int gmressize = 21, iterpre = 2, iterpost = 2, iterexact = 10;
   double omega = 0.8, tol = 1e-8, globaltol = 1e-16, mgomega = 1.0;
   int maxiter = 100, ndirect = 1, dump = 0, repeat = 1, patchdepth = 1;
@@ -161,6 +161,7 @@ parse(int argc, char** argv)
     else if (k == "refine") c.refine = atoi(v.c_str());
     else if (k == "kappa") c.kappa = v;
     else if (k == "rhs") c.rhs = v;
+    else if (k == "dualrhs") c.dualrhs = v;
     else if (k == "out") c.out = v;
     else if (k == "gmressize") c.gmressize = atoi(v.c_str());
     else if (k == "iterpre") c.iterpre = atoi(v.c_str());
@@ -424,6 +425,7 @@ main(int argc, char** argv)
 
   {
     std::ofstream o(c.out + "/summary.txt");
+
     o.precision(17);
     o << "nlevels " << nl << "\n";
     for (int l = 0; l < nl; ++l)
@@ -523,5 +525,67 @@ main(int argc, char** argv)
     std::vector<double> sol(U.begin(), U.end());
     write_raw(c.out + "/solution.f64", sol);
   }
+  // Dual problem (optional): StdMultiLevelSolver::AssembleDualMatrix
+  // (Solver/stdmultilevelsolver.cc:920-926, Solver/stdsolver.cc:1815-1834:
+  // transpose, Dirichlet rows) and the same Gmres on it, right-hand side read
+  // like rhs and zeroed at Dirichlet nodes.
+  int dual_iterations = -1;
+  std::string dual_status = "none";
+  double dual_first = 0, dual_last = 0;
+  std::vector<double> dual_times;
+  Vector z("z"), g("g");
+  if (!c.dualrhs.empty()) {
+    MLS.ReInitVector(z);
+    MLS.ReInitVector(g);
+    GlobalVector& Gv = S->GetGV(g);
+    size_t nlex = 1;
+    for (int d = 0; d < c.dim; ++d)
+      nlex *= Nf + 1;
+    std::vector<double> r = read_f64(c.dualrhs, nlex);
+    for (int i = 0; i < nf; ++i) {
+      long ix, iy, iz = 0;
+      if (c.dim == 3) {
+        const Vertex3d& v = Mf->vertex3d(i);
+        ix = std::lround(v.x() * Nf);
+        iy = std::lround(v.y() * Nf);
+        iz = std::lround(v.z() * Nf);
+      } else {
+        const Vertex2d& v = Mf->vertex2d(i);
+        ix = std::lround(v.x() * Nf);
+        iy = std::lround(v.y() * Nf);
+      }
+      Gv(i, 0) = r[(iz * (Nf + 1) + iy) * (Nf + 1) + ix];
+    }
+    S->SetBoundaryVectorZero(g);
+    MLS.AssembleDualMatrix(A, u);
+    CGInfo dinfo(c.tol, c.globaltol, 0, c.maxiter, "Dual");
+    for (int rep = 0; rep < std::max(1, c.repeat); ++rep) {
+      dinfo.reset();
+      auto t0 = std::chrono::steady_clock::now();
+      MLS.NewtonLinearSolve(A, z, g, dinfo);
+      auto t1 = std::chrono::steady_clock::now();
+      dual_times.push_back(std::chrono::duration<double>(t1 - t0).count());
+    }
+    dual_iterations = dinfo.control().iteration();
+    dual_status = dinfo.control().status();
+    dual_first = dinfo.control().firstresidual();
+    dual_last = dinfo.control().residual();
+    const GlobalVector& Z = S->GetGV(z);
+    std::vector<double> zz(Z.begin(), Z.end());
+    write_raw(c.out + "/dual_solution.f64", zz);
+    std::vector<double> gg(Gv.begin(), Gv.end());
+    write_raw(c.out + "/dual_rhs.f64", gg);
+    std::ofstream o(c.out + "/dual_summary.txt");
+    o.precision(17);
+    o << "dual_iterations " << dual_iterations << "\n";
+    o << "dual_status " << dual_status << "\n";
+    o << "dual_firstresidual " << dual_first << "\n";
+    o << "dual_residual " << dual_last << "\n";
+    o << "dual_solve_s";
+    for (double t : dual_times)
+      o << " " << t;
+    o << "\n";
+  }
+
   return 0;
 }
