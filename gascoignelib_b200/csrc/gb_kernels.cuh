@@ -530,6 +530,57 @@ k_blockdiag_inverse(int n, const double* __restrict__ dblocks, double* __restric
   }
 }
 
+// ------------------------------------------------- coefficient gradient
+
+// grad[c] = -scale[c] * lam_c^T K u_c, one thread per cell. cn holds the cell
+// nodes node-major (entry i of cell c at cn[i * ncells + c]) so that a warp's
+// loads of one local node are contiguous; K (nloc x nloc, row = test
+// function) is staged in shared memory. Dirichlet dofs read as 0. NL is the
+// local node count (0: runtime nloc <= 32).
+template<int NL>
+__global__ void __launch_bounds__(256)
+k_coeff_gradient(int ncells, int nloc_rt, const int* __restrict__ cn,
+                 const double* __restrict__ kloc, const double* __restrict__ scale,
+                 const double* __restrict__ u, const double* __restrict__ lam,
+                 const uint8_t* __restrict__ mask, double* __restrict__ grad)
+{
+  GB_PDL_ENTRY();
+  constexpr int NMAX = NL > 0 ? NL : 32;
+  const int nloc = NL > 0 ? NL : nloc_rt;
+  __shared__ double K[NMAX * NMAX];
+  for (int i = threadIdx.x; i < nloc * nloc; i += blockDim.x)
+    K[i] = kloc[i];
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells)
+    return;
+  double uu[NMAX], ll[NMAX];
+#pragma unroll
+  for (int i = 0; i < NMAX; ++i) {
+    if (NL == 0 && i >= nloc)
+      break;
+    const int node = __ldg(cn + int64_t(i) * ncells + c);
+    const bool d = mask[node] != 0;
+    uu[i] = d ? 0.0 : __ldg(u + node);
+    ll[i] = d ? 0.0 : __ldg(lam + node);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < NMAX; ++i) {
+    if (NL == 0 && i >= nloc)
+      break;
+    double t = 0.0;
+#pragma unroll
+    for (int j = 0; j < NMAX; ++j) {
+      if (NL == 0 && j >= nloc)
+        break;
+      t = fma(K[i * nloc + j], uu[j], t);
+    }
+    s = fma(ll[i], t, s);
+  }
+  grad[c] = -(scale ? scale[c] : 1.0) * s;
+}
+
 // ---------------------------------------------------------- GMRES scalars
 
 struct CGInfoDev

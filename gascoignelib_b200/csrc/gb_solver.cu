@@ -262,6 +262,12 @@ struct Level
   DeviceArray<uint8_t> dirmask;
   DeviceArray<int> dirlist;
   int ndir = 0;
+  // cells for the coefficient gradient (gb_level_set_cells)
+  int ncells = 0, nloc = 0;
+  int64_t cells_n = -1; // level size the cell node indices were checked against
+  DeviceArray<int> cells; // node-major: entry i of cell c at i * ncells + c
+  DeviceArray<double> kloc, cscale, grad;
+  bool has_scale = false;
   int64_t ndof() const { return n * B; }
 };
 
@@ -280,10 +286,11 @@ struct CoarseKey
   const void *u, *tmp, *b;
   bool zero;
   char p0, p;
+  bool tr;
   bool operator<(const CoarseKey& o) const
   {
-    return std::tie(tsize, level, u, tmp, b, zero, p0, p) <
-           std::tie(o.tsize, o.level, o.u, o.tmp, o.b, o.zero, o.p0, o.p);
+    return std::tie(tsize, level, u, tmp, b, zero, p0, p, tr) <
+           std::tie(o.tsize, o.level, o.u, o.tmp, o.b, o.zero, o.p0, o.p, o.tr);
   }
 };
 
@@ -345,7 +352,9 @@ struct gb_ctx
     cudaGraphExec_t exec = nullptr;
     int64_t version = -1;
     int setup_k = 0, outer_k = 0, inner_k = 0;
-  } fg[2];
+  } fg[2][2]; // [operator transposed][cycle precision]
+  // level operators: A (0) or A^T (1) for every solver step (gb_set_operator)
+  int transposed = 0;
   // coarse-level kernel: levels 0..coarse_root, programs per entry state
   bool coarse_on = true;
   bool coarse_dense = true; // apply the coarse sub-cycle as its precomputed map
@@ -373,12 +382,13 @@ struct gb_ctx
       cudaEventDestroy(p.e0);
       cudaEventDestroy(p.e1);
     }
-    for (auto& g : fg) {
-      if (g.exec)
-        cudaGraphExecDestroy(g.exec);
-      if (g.graph)
-        cudaGraphDestroy(g.graph);
-    }
+    for (auto& row : fg)
+      for (auto& g : row) {
+        if (g.exec)
+          cudaGraphExecDestroy(g.exec);
+        if (g.graph)
+          cudaGraphDestroy(g.graph);
+      }
   }
 };
 
@@ -586,6 +596,65 @@ const float* dinv_of<float>(const Level& L)
   return L.dinv32.p;
 }
 
+// The operator of every solver step on level L: A, or A^T after
+// gb_set_operator(ctx, 1) (the dual matrix of StdSolver::AssembleDualMatrix,
+// Solver/stdsolver.cc:1815-1834).
+static const Sell&
+opA(const Context& c, const Level& L)
+{
+  return c.transposed ? L.AT : L.A;
+}
+
+// A^T of the uploaded (Dirichlet-modified) level matrix. A structurally
+// symmetric matrix keeps its own sparsity pattern and row order, with the
+// values swapped in place as SparseBlockMatrix::transpose does
+// (LinAlg/sparseblockmatrix.xx:478-491); otherwise rows of A^T list the
+// columns of A in ascending order. Strong Dirichlet rows and columns of the
+// uploaded matrix are both identity, so A^T is the reference's dual matrix
+// (transpose, then DirichletMatrixOnlyRow) wherever it meets a vector that is
+// zero on the Dirichlet dofs, which every vector of the dual solve is.
+static void
+ensure_AT(Context& c, Level& L)
+{
+  if (L.has_AT)
+    return;
+  const int64_t n = L.n, nnz = L.h_rowptr[n];
+  std::vector<int64_t> tp(n + 1, 0), tc(nnz);
+  std::vector<double> tv(nnz);
+  bool symmetric = true;
+  for (int64_t i = 0; i < n && symmetric; ++i)
+    for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k) {
+      const int64_t j = L.h_col[k];
+      const int64_t* b = L.h_col.data() + L.h_rowptr[j];
+      const int64_t* e = L.h_col.data() + L.h_rowptr[j + 1];
+      const int64_t* f = std::find(b, e, i);
+      if (f == e) {
+        symmetric = false;
+        break;
+      }
+      tv[k] = L.h_val[L.h_rowptr[j] + (f - b)];
+    }
+  if (symmetric) {
+    tp = L.h_rowptr;
+    tc = L.h_col;
+  } else {
+    for (int64_t k = 0; k < nnz; ++k)
+      tp[L.h_col[k] + 1]++;
+    for (int64_t i = 0; i < n; ++i)
+      tp[i + 1] += tp[i];
+    std::vector<int64_t> pos(tp.begin(), tp.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k) {
+        int64_t q = pos[L.h_col[k]]++;
+        tc[q] = i;
+        tv[q] = L.h_val[k];
+      }
+  }
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), c.stream);
+  L.has_AT = true;
+}
+
 // ---------------------------------------------------------- level set-up
 
 static void
@@ -616,6 +685,9 @@ ensure_work(Context& c)
     GB_CUDA(c.w32.b[l].alloc(nd));
     GB_CUDA(c.w32.v[l].alloc(nd));
   }
+  if (c.transposed)
+    for (int l = 0; l < c.nlevels; ++l)
+      ensure_AT(c, c.L[l]);
   c.coarse_root = -1;
   for (int l = 0; l < c.nlevels; ++l) {
     if (c.L[l].ndof() > kCoarseMaxRows)
@@ -650,12 +722,13 @@ struct Emit
     o.b = b;
     o.in_n = in ? o.n : 0;
     o.b_n = b ? o.n : 0;
-    o.sptr = L.A.sptr.p;
-    o.col = L.A.pat ? nullptr : L.A.col.p;
-    o.pid = L.A.pat ? L.A.pid.p : nullptr;
-    o.ptab = L.A.pat ? L.A.ptab.p : nullptr;
-    o.W = L.A.W;
-    o.val = sell_vals<T>(L.A);
+    const Sell& A = opA(c, L);
+    o.sptr = A.sptr.p;
+    o.col = A.pat ? nullptr : A.col.p;
+    o.pid = A.pat ? A.pid.p : nullptr;
+    o.ptab = A.pat ? A.ptab.p : nullptr;
+    o.W = A.W;
+    o.val = sell_vals<T>(A);
     o.dinv = dinv_of<T>(L);
     o.mask = L.dirmask.p;
     o.alpha = alpha;
@@ -674,14 +747,14 @@ struct Emit
     const Level& L = c.L[l];
     if (rec)
       return rec->push_back(level_op(kOpJacobi, L, out, u, b, c.params.omega));
-    spmv<kJacobi, T, T, T>(c, L, L.A, u, out, b, dinv_of<T>(L), c.params.omega);
+    spmv<kJacobi, T, T, T>(c, L, opA(c, L), u, out, b, dinv_of<T>(L), c.params.omega);
   }
   void resid(int l, const T* u, T* out, const T* b)
   {
     const Level& L = c.L[l];
     if (rec)
       return rec->push_back(level_op(kOpResid, L, out, u, b, 0.0));
-    spmv<kResid, T, T, T>(c, L, L.A, u, out, b, nullptr, 0.0);
+    spmv<kResid, T, T, T>(c, L, opA(c, L), u, out, b, nullptr, 0.0);
   }
   // coarse (level l) = R fine, 0 on the coarse Dirichlet dofs
   void restrict_to(int l, const T* fine, T* coarse)
@@ -768,7 +841,7 @@ run_coarse(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char
 {
   Context& c = E.c;
   CoarseKey key{ int(sizeof(T)), l, (const void*)u, (const void*)tmp, (const void*)b,
-                 u_zero, p0, p };
+                 u_zero, p0, p, c.transposed != 0 };
   auto it = c.coarse_progs.find(key);
   if (it == c.coarse_progs.end()) {
     std::vector<CoarseOp> ops;
@@ -824,13 +897,14 @@ run_coarse(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char
     std::vector<CoarsePrefetch> pre;
     for (int lv = 0; lv <= l; ++lv) {
       const Level& L = c.L[lv];
-      pre.push_back({ sell_vals<T>(L.A), int(L.A.entries * sizeof(T)) });
-      pre.push_back({ L.A.sptr.p, int((L.A.nslices + 1) * sizeof(int)) });
-      if (L.A.pat) {
-        pre.push_back({ L.A.pid.p, int(L.n) });
-        pre.push_back({ L.A.ptab.p, int(L.A.npat * L.A.W * sizeof(int)) });
+      const Sell& A = opA(c, L);
+      pre.push_back({ sell_vals<T>(A), int(A.entries * sizeof(T)) });
+      pre.push_back({ A.sptr.p, int((A.nslices + 1) * sizeof(int)) });
+      if (A.pat) {
+        pre.push_back({ A.pid.p, int(L.n) });
+        pre.push_back({ A.ptab.p, int(A.npat * A.W * sizeof(int)) });
       } else {
-        pre.push_back({ L.A.col.p, int(L.A.entries * sizeof(int)) });
+        pre.push_back({ A.col.p, int(A.entries * sizeof(int)) });
       }
       pre.push_back({ dinv_of<T>(L), int(L.ndof() * sizeof(T)) });
       pre.push_back({ L.dirmask.p, int(L.ndof()) });
@@ -1095,7 +1169,7 @@ fill_info(Context& c, gb_solve_info* info, double* x_for_residual, const double*
   // true residual ||b - A x|| and ||b|| (FP64)
   const int fl = c.nlevels - 1;
   Level& L = c.L[fl];
-  spmv<kResid, double, double, double>(c, L, L.A, x_for_residual, c.pbuf.p, b,
+  spmv<kResid, double, double, double>(c, L, opA(c, L), x_for_residual, c.pbuf.p, b,
                                        nullptr, 0.0);
   dot_dev(c, L.ndof(), c.pbuf.p, c.pbuf.p, RedOut{ c.scal.p + 4, nullptr, nullptr, 1 });
   dot_dev(c, L.ndof(), b, b, RedOut{ c.scal.p + 5, nullptr, nullptr, 1 });
@@ -1127,7 +1201,7 @@ gmres_left(Context& c, double* x, const double* b, gb_solve_info* info)
          c.params.maxiter);
   GB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), c.stream)); // NewtonLinearSolve
   // residualgmres: p = b - A x, Dirichlet zero
-  spmv<kResidDir, double, double, double>(c, L, L.A, x, c.pbuf.p, b, nullptr, 0.0);
+  spmv<kResidDir, double, double, double>(c, L, opA(c, L), x, c.pbuf.p, b, nullptr, 0.0);
   precondition_T<double>(c, c.w64, V, c.pbuf.p, true);
   dot_dev(c, n, V, V, RedOut{ c.scal.p, nullptr, nullptr, 1 });
   launch(c, k_gmres_init, 1, 1, G, (const double*)c.scal.p);
@@ -1140,7 +1214,7 @@ gmres_left(Context& c, double* x, const double* b, gb_solve_info* info)
       dim++;
       const int last = dim - 1;
       double* vv = V + int64_t(dim) * n;
-      spmv<kAx, double, double, double>(c, L, L.A, V + int64_t(last) * n, c.pbuf.p,
+      spmv<kAx, double, double, double>(c, L, opA(c, L), V + int64_t(last) * n, c.pbuf.p,
                                         nullptr, nullptr, 1.0);
       precondition_T<double>(c, c.w64, vv, c.pbuf.p, true);
       mgs(c, n, vv, V, dim, last);
@@ -1202,7 +1276,7 @@ gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* 
   double bnorm = -1.0;
   for (;;) {
     // r = b - A x (Dirichlet zero) into V_0, beta = ||r||
-    spmv<kResidDir, double, double, double>(c, L, L.A, x, V, b, nullptr, 0.0);
+    spmv<kResidDir, double, double, double>(c, L, opA(c, L), x, V, b, nullptr, 0.0);
     dot_dev(c, n, V, V, RedOut{ c.scal.p, nullptr, nullptr, 1 });
     launch(c, k_fgmres_restart, 1, 1, G, (const double*)c.scal.p, vmax);
     double hv[2];
@@ -1230,12 +1304,12 @@ gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* 
         launch(c, k_convert<double, float>, stream_blocks(n), 256, n, c.fine_rhs32.p,
                (const double*)vj);
         precondition_T<float>(c, c.w32, z, c.fine_rhs32.p, true);
-        spmv<kAx, double, float, double>(c, L, L.A, (const float*)z, w, nullptr,
+        spmv<kAx, double, float, double>(c, L, opA(c, L), (const float*)z, w, nullptr,
                                          nullptr, 1.0);
       } else {
         double* z = c.zb64.p + int64_t(j) * n;
         precondition_T<double>(c, c.w64, z, vj, true);
-        spmv<kAx, double, double, double>(c, L, L.A, (const double*)z, w, nullptr,
+        spmv<kAx, double, double, double>(c, L, opA(c, L), (const double*)z, w, nullptr,
                                           nullptr, 1.0);
       }
       mgs(c, n, w, V, j + 1, j);
@@ -1382,7 +1456,7 @@ fg_outer_pre(Context& c, cudaGraphConditionalHandle hOuter,
   const int64_t n = L.ndof();
   GmresDev* G = c.G.p;
   double* V = c.krylov.p;
-  spmv<kResidDir, double, double, double>(c, L, L.A, (const double*)c.xg.p, V, c.bg.p,
+  spmv<kResidDir, double, double, double>(c, L, opA(c, L), (const double*)c.xg.p, V, c.bg.p,
                                           nullptr, 0.0);
   dot_dev(c, n, V, V, RedOut{ &G->beta_tmp, nullptr, nullptr, 1 });
   launch(c, k_fg_restart, 1, 1, G, hOuter, hInner, c.params.gmressize - 1, 50,
@@ -1401,7 +1475,7 @@ fg_inner(Context& c, const FBufs<T>& F, cudaGraphConditionalHandle hInner, int u
   double* V = c.krylov.p;
   launch(c, k_load_idx<T>, stream_blocks(n), 256, n, F.rhs, V, (const GmresDev*)G);
   precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true);
-  spmv<kAx, double, T, double>(c, L, L.A, (const T*)F.zfix, V, nullptr, nullptr, 1.0,
+  spmv<kAx, double, T, double>(c, L, opA(c, L), (const T*)F.zfix, V, nullptr, nullptr, 1.0,
                                (const int*)&G->j, n, F.Z);
   const int rg = static_cast<int>(std::max<int64_t>(
     1, std::min<int64_t>((n + kCgsThreads - 1) / kCgsThreads, kMaxRedBlocks)));
@@ -1433,7 +1507,7 @@ build_fgraph(Context& c, int prec)
 {
   const FBufs<T> F = fg_buffers<T>(c, prec);
   const int64_t n = c.L[c.nlevels - 1].ndof();
-  auto& FG = c.fg[prec];
+  auto& FG = c.fg[c.transposed][prec];
   if (FG.exec) {
     cudaGraphExecDestroy(FG.exec);
     FG.exec = nullptr;
@@ -1520,7 +1594,7 @@ static int
 fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* info,
              bool copy_in = true, bool copy_out = true)
 {
-  auto& F = c.fg[prec];
+  auto& F = c.fg[c.transposed][prec];
   if (c.use_graph && (!F.exec || F.version != c.version)) {
     if (prec == GB_FP32)
       build_fgraph<float>(c, prec);
@@ -1581,6 +1655,27 @@ fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* in
 // ==================================================================== C-ABI
 
 using namespace gb;
+
+// Runs f with the transposed level operators, restoring the setting after.
+template<class F>
+static int
+with_transposed(gb_ctx* ctx, F f)
+{
+  const int saved = ctx->transposed;
+  if (!saved) {
+    for (auto& L : ctx->L)
+      if (L.has_matrix)
+        gb::ensure_AT(*ctx, L);
+    ctx->transposed = 1;
+  }
+  struct Restore
+  {
+    gb_ctx* c;
+    int v;
+    ~Restore() { c->transposed = v; }
+  } restore{ ctx, saved };
+  return f();
+}
 
 #define GB_API_BEGIN                                                           \
   if (!ctx)                                                                    \
@@ -1746,6 +1841,8 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   L.h_val.assign(val, val + nnzb * B * B);
   build_sell(L.A, n, rowptr, col, val, ctx->stream);
   L.has_AT = false;
+  if (ctx->transposed)
+    ensure_AT(*ctx, L);
   // block-diagonal inverse on the device (get_inverse_diagonal / K1)
   std::vector<double> dblk(n * B * B);
   for (int64_t i = 0; i < n; ++i)
@@ -2013,7 +2110,7 @@ gb_vmult(gb_ctx* ctx, int lvl, int y, int x, double d)
   GB_API_BEGIN
   GB_REQUIRE(y != x, GB_EINVAL, "y and x must differ");
   Level& L = level_with_matrix(*ctx, lvl);
-  spmv<kAddAx, double, double, double>(*ctx, L, L.A, (const double*)vec(*ctx, lvl, x),
+  spmv<kAddAx, double, double, double>(*ctx, L, opA(*ctx, L), (const double*)vec(*ctx, lvl, x),
                                        vec(*ctx, lvl, y), nullptr, nullptr, d);
   GB_API_END
 }
@@ -2024,7 +2121,7 @@ gb_vmulteq(gb_ctx* ctx, int lvl, int y, int x, double d)
   GB_API_BEGIN
   GB_REQUIRE(y != x, GB_EINVAL, "y and x must differ");
   Level& L = level_with_matrix(*ctx, lvl);
-  spmv<kAx, double, double, double>(*ctx, L, L.A, (const double*)vec(*ctx, lvl, x),
+  spmv<kAx, double, double, double>(*ctx, L, opA(*ctx, L), (const double*)vec(*ctx, lvl, x),
                                     vec(*ctx, lvl, y), nullptr, nullptr, d);
   GB_API_END
 }
@@ -2035,27 +2132,10 @@ gb_vmult_transpose(gb_ctx* ctx, int lvl, int y, int x, double d)
   GB_API_BEGIN
   GB_REQUIRE(y != x, GB_EINVAL, "y and x must differ");
   Level& L = level_with_matrix(*ctx, lvl);
-  if (!L.has_AT) {
-    // transposed block-CSR, rows of A^T = columns of A, ascending
-    const int64_t n = L.n, nnz = L.h_rowptr[n];
-    std::vector<int64_t> tp(n + 1, 0), tc(nnz);
-    std::vector<double> tv(nnz);
-    for (int64_t k = 0; k < nnz; ++k)
-      tp[L.h_col[k] + 1]++;
-    for (int64_t i = 0; i < n; ++i)
-      tp[i + 1] += tp[i];
-    std::vector<int64_t> pos(tp.begin(), tp.end() - 1);
-    for (int64_t i = 0; i < n; ++i)
-      for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k) {
-        int64_t q = pos[L.h_col[k]]++;
-        tc[q] = i;
-        tv[q] = L.h_val[k];
-      }
-    GB_CUDA(cudaStreamSynchronize(ctx->stream));
-    build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), ctx->stream);
-    L.has_AT = true;
-  }
-  spmv<kAddAx, double, double, double>(*ctx, L, L.AT, (const double*)vec(*ctx, lvl, x),
+  ensure_AT(*ctx, L);
+  // the transpose of the current level operator
+  spmv<kAddAx, double, double, double>(*ctx, L, ctx->transposed ? L.A : L.AT,
+                                       (const double*)vec(*ctx, lvl, x),
                                        vec(*ctx, lvl, y), nullptr, nullptr, d);
   GB_API_END
 }
@@ -2066,7 +2146,7 @@ gb_matrix_residual(gb_ctx* ctx, int lvl, int y, int x, int b)
   GB_API_BEGIN
   GB_REQUIRE(y != x && y != b, GB_EINVAL, "y must differ from x and b");
   Level& L = level_with_matrix(*ctx, lvl);
-  spmv<kResid, double, double, double>(*ctx, L, L.A, (const double*)vec(*ctx, lvl, x),
+  spmv<kResid, double, double, double>(*ctx, L, opA(*ctx, L), (const double*)vec(*ctx, lvl, x),
                                        vec(*ctx, lvl, y),
                                        (const double*)vec(*ctx, lvl, b), nullptr, 0.0);
   GB_API_END
@@ -2078,7 +2158,7 @@ gb_residualgmres(gb_ctx* ctx, int lvl, int y, int x, int b)
   GB_API_BEGIN
   GB_REQUIRE(y != x && y != b, GB_EINVAL, "y must differ from x and b");
   Level& L = level_with_matrix(*ctx, lvl);
-  spmv<kResidDir, double, double, double>(*ctx, L, L.A,
+  spmv<kResidDir, double, double, double>(*ctx, L, opA(*ctx, L),
                                           (const double*)vec(*ctx, lvl, x),
                                           vec(*ctx, lvl, y),
                                           (const double*)vec(*ctx, lvl, b), nullptr, 0.0);
@@ -2255,6 +2335,123 @@ gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x, int64_t len,
 }
 
 int
+gb_set_operator(gb_ctx* ctx, int transposed)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(transposed == 0 || transposed == 1, GB_EINVAL, "transposed must be 0 or 1");
+  if (transposed)
+    for (auto& L : ctx->L)
+      if (L.has_matrix)
+        ensure_AT(*ctx, L);
+  ctx->transposed = transposed;
+  GB_API_END
+}
+
+int
+gb_get_operator(const gb_ctx* ctx, int* transposed)
+{
+  if (!ctx || !transposed)
+    return GB_EINVAL;
+  *transposed = ctx->transposed;
+  return GB_OK;
+}
+
+int
+gb_adjoint_gmres(gb_ctx* ctx, int x, int b, gb_solve_info* info)
+{
+  GB_API_BEGIN
+  return with_transposed(ctx, [&] { return gb_gmres(ctx, x, b, info); });
+  GB_API_END
+}
+
+int
+gb_adjoint_fgmres(gb_ctx* ctx, int x, int b, int precision, gb_solve_info* info)
+{
+  GB_API_BEGIN
+  return with_transposed(ctx, [&] { return gb_fgmres(ctx, x, b, precision, info); });
+  GB_API_END
+}
+
+int
+gb_level_set_cells(gb_ctx* ctx, int lvl, int64_t ncells, int nloc,
+                   const int64_t* cell_nodes, const double* kloc, const double* cell_scale)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(ncells >= 1 && ncells < (int64_t(1) << 31) / 32, GB_EINVAL,
+             "ncells out of range");
+  GB_REQUIRE(nloc >= 1 && nloc <= 32, GB_EINVAL, "nloc must be in 1..32");
+  GB_REQUIRE(cell_nodes && kloc, GB_EINVAL, "null array");
+  std::vector<int> cn(size_t(ncells) * nloc);
+  for (int64_t c = 0; c < ncells; ++c)
+    for (int i = 0; i < nloc; ++i) {
+      const int64_t v = cell_nodes[c * nloc + i];
+      GB_REQUIRE(v >= 0 && v < L.n, GB_EINVAL, "cell node out of range");
+      cn[size_t(i) * ncells + c] = static_cast<int>(v);
+    }
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_CUDA(L.cells.alloc(cn.size()));
+  GB_CUDA(L.kloc.alloc(size_t(nloc) * nloc));
+  GB_CUDA(L.grad.alloc(ncells));
+  GB_CUDA(cudaMemcpyAsync(L.cells.p, cn.data(), cn.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(cudaMemcpyAsync(L.kloc.p, kloc, size_t(nloc) * nloc * sizeof(double),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  L.has_scale = cell_scale != nullptr;
+  if (cell_scale) {
+    GB_CUDA(L.cscale.alloc(ncells));
+    GB_CUDA(cudaMemcpyAsync(L.cscale.p, cell_scale, ncells * sizeof(double),
+                            cudaMemcpyHostToDevice, ctx->stream));
+  }
+  GB_CUDA(cudaStreamSynchronize(ctx->stream)); // host arrays end with the call
+  L.ncells = static_cast<int>(ncells);
+  L.nloc = nloc;
+  L.cells_n = L.n;
+  GB_API_END
+}
+
+int
+gb_coeff_gradient(gb_ctx* ctx, int lvl, int u, int lam, double* grad, int64_t ncells)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(L.ncells > 0 && L.cells_n == L.n, GB_ESTATE,
+             "no cells for this level's matrix (gb_level_set_cells)");
+  GB_REQUIRE(L.B == 1, GB_EINVAL, "coefficient gradient needs block size 1");
+  GB_REQUIRE(grad && ncells == L.ncells, GB_EINVAL, "grad length differs from ncells");
+  const double* ud = vec(*ctx, lvl, u);
+  const double* ld = vec(*ctx, lvl, lam);
+  const int nb = blocks_for(L.ncells, 256);
+  const double* sc = L.has_scale ? L.cscale.p : nullptr;
+  const uint8_t* mk = L.dirmask.p;
+  switch (L.nloc) {
+    case 4:
+      launch(*ctx, k_coeff_gradient<4>, nb, 256, L.ncells, 4, (const int*)L.cells.p,
+             (const double*)L.kloc.p, sc, ud, ld, mk, L.grad.p);
+      break;
+    case 8:
+      launch(*ctx, k_coeff_gradient<8>, nb, 256, L.ncells, 8, (const int*)L.cells.p,
+             (const double*)L.kloc.p, sc, ud, ld, mk, L.grad.p);
+      break;
+    case 9:
+      launch(*ctx, k_coeff_gradient<9>, nb, 256, L.ncells, 9, (const int*)L.cells.p,
+             (const double*)L.kloc.p, sc, ud, ld, mk, L.grad.p);
+      break;
+    case 27:
+      launch(*ctx, k_coeff_gradient<27>, nb, 256, L.ncells, 27, (const int*)L.cells.p,
+             (const double*)L.kloc.p, sc, ud, ld, mk, L.grad.p);
+      break;
+    default:
+      launch(*ctx, k_coeff_gradient<0>, nb, 256, L.ncells, L.nloc, (const int*)L.cells.p,
+             (const double*)L.kloc.p, sc, ud, ld, mk, L.grad.p);
+  }
+  GB_CUDA(cudaMemcpyAsync(grad, L.grad.p, ncells * sizeof(double),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_API_END
+}
+
+int
 gb_set_timing(gb_ctx* ctx, int on)
 {
   GB_API_BEGIN
@@ -2319,10 +2516,10 @@ gb_bench_spmv(gb_ctx* ctx, int lvl, int precision, int reps, int flush_l2,
         reinterpret_cast<const uint4*>(ctx->flush.p), int64_t(flush_bytes / 16), nullptr);
     GB_CUDA(cudaEventRecord(a, ctx->stream));
     if (precision == GB_FP32)
-      spmv<kAx, float, float, float>(*ctx, L, L.A, (const float*)ctx->w32.b[lvl].p,
+      spmv<kAx, float, float, float>(*ctx, L, opA(*ctx, L), (const float*)ctx->w32.b[lvl].p,
                                      ctx->w32.u[lvl].p, nullptr, nullptr, 1.0);
     else
-      spmv<kAx, double, double, double>(*ctx, L, L.A,
+      spmv<kAx, double, double, double>(*ctx, L, opA(*ctx, L),
                                         (const double*)ctx->w64.b[lvl].p,
                                         ctx->w64.u[lvl].p, nullptr, nullptr, 1.0);
     GB_CUDA(cudaEventRecord(bq, ctx->stream));

@@ -88,6 +88,12 @@ _SIGS = {
     "gb_gmres": [C.c_void_p, C.c_int, C.c_int, C.POINTER(GbSolveInfo)],
     "gb_fgmres": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(GbSolveInfo)],
     "gb_solve_host": [C.c_void_p, C.c_int, _PD, _PD, C.c_int64, C.POINTER(GbSolveInfo)],
+    "gb_set_operator": [C.c_void_p, C.c_int],
+    "gb_get_operator": [C.c_void_p, C.POINTER(C.c_int)],
+    "gb_adjoint_gmres": [C.c_void_p, C.c_int, C.c_int, C.POINTER(GbSolveInfo)],
+    "gb_adjoint_fgmres": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(GbSolveInfo)],
+    "gb_level_set_cells": [C.c_void_p, C.c_int, C.c_int64, C.c_int, _P64, _PD, _PD],
+    "gb_coeff_gradient": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD, C.c_int64],
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
     "gb_bench_spmv": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
@@ -193,6 +199,20 @@ class Context:
             self._chk(self._L.gb_level_set_transfer(
                 self.h, l, c2f.shape[0], _p64(c2f), z.shape[0], _p64(z), v.shape[0],
                 _p64(v), a.shape[0], _p64(a)))
+        cells = getattr(prob, "cells", None)
+        if cells is not None:
+            self.set_cells(nl - 1, cells)
+
+    def set_cells(self, level, cells):
+        """Cells of `level` for gb_coeff_gradient (a problem.Cells)."""
+        nd = np.ascontiguousarray(cells.nodes, dtype=np.int64)
+        kl = np.ascontiguousarray(cells.kloc, dtype=np.float64)
+        sc = (None if cells.scale is None
+              else np.ascontiguousarray(cells.scale, dtype=np.float64))
+        self._chk(self._L.gb_level_set_cells(
+            self.h, level, nd.shape[0], nd.shape[1], _p64(nd), _pd(kl),
+            _pd(sc) if sc is not None else None))
+        self.ncells = nd.shape[0]
 
     # ------------------------------------------------------------ vectors
     def vec(self):
@@ -279,6 +299,32 @@ class Context:
         if check or rc not in (GB_OK, GB_ENOTCONV):
             self._chk(rc)
         return info.as_dict()
+
+    # ------------------------------------------------------------ adjoint
+    def set_operator(self, transposed):
+        self._chk(self._L.gb_set_operator(self.h, int(transposed)))
+
+    def get_operator(self):
+        v = C.c_int()
+        self._chk(self._L.gb_get_operator(self.h, C.byref(v)))
+        return v.value
+
+    def adjoint_gmres(self, x, b):
+        info = GbSolveInfo()
+        self._chk(self._L.gb_adjoint_gmres(self.h, x, b, C.byref(info)))
+        return info.as_dict()
+
+    def adjoint_fgmres(self, x, b, precision=GB_FP32, check=True):
+        info = GbSolveInfo()
+        rc = self._L.gb_adjoint_fgmres(self.h, x, b, precision, C.byref(info))
+        if check or rc not in (GB_OK, GB_ENOTCONV):
+            self._chk(rc)
+        return info.as_dict()
+
+    def coeff_gradient(self, level, u, lam):
+        g = np.empty(self.ncells, dtype=np.float64)
+        self._chk(self._L.gb_coeff_gradient(self.h, level, u, lam, _pd(g), g.shape[0]))
+        return g
 
     def solve_host(self, b, method=2, out=None, check=True):
         b = np.ascontiguousarray(b, dtype=np.float64)

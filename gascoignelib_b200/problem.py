@@ -63,12 +63,44 @@ class Transfer:
 
 
 @dataclass
+class Cells:
+    """Finest-level cells for the coefficient gradient: the per-cell element
+    matrix of the equation is kappa_c * scale_c * kloc (the reference's
+    element assembly with a per-cell coefficient, DofHandler/cgdisc.h:599-635,
+    Interface/equation.h:104), so dA/dkappa_c = scale_c * kloc on the cell's
+    nodes."""
+    nodes: np.ndarray                   # int64 [ncells, nloc] local node order
+    kloc: np.ndarray                    # float64 [nloc, nloc] unit-coefficient matrix
+    mloc: Optional[np.ndarray] = None   # float64 [nloc, nloc] element mass matrix
+    scale: Optional[np.ndarray] = None  # float64 [ncells], default 1
+
+    @property
+    def ncells(self) -> int:
+        return int(self.nodes.shape[0])
+
+    @property
+    def nloc(self) -> int:
+        return int(self.nodes.shape[1])
+
+    def assemble(self, local: np.ndarray, n: int):
+        """Sum of local[.,.] over the cells as a scipy CSR matrix of size n."""
+        import scipy.sparse as sp
+        nl = self.nloc
+        w = np.ones(self.ncells) if self.scale is None else self.scale
+        rows = np.repeat(self.nodes, nl, axis=1).ravel()
+        cols = np.tile(self.nodes, (1, nl)).ravel()
+        vals = (w[:, None] * local.ravel()[None, :]).ravel()
+        return sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+
+
+@dataclass
 class Problem:
     dim: int
     levels: List[Level]
     transfers: List[Transfer]
     rhs: np.ndarray
     info: dict = field(default_factory=dict)
+    cells: Optional[Cells] = None
 
     @property
     def nlevels(self) -> int:
@@ -130,6 +162,40 @@ def _q1_local_stiffness(dim: int, h: float) -> np.ndarray:
             + np.kron(np.kron(s, m), m))
 
 
+def _q1_local_mass(dim: int, h: float) -> np.ndarray:
+    """Q1 element mass matrix of a cube of width h (local order as above)."""
+    m = np.array([[1.0 / 3.0, 1.0 / 6.0], [1.0 / 6.0, 1.0 / 3.0]]) * h
+    return np.kron(m, m) if dim == 2 else np.kron(np.kron(m, m), m)
+
+
+def _q1_local_convection(dim: int, h: float, beta) -> np.ndarray:
+    """Q1 element matrix of (beta . grad u) v: entry [i, j] = integral of
+    (beta . grad phi_j) phi_i, from the 1D mass m and d[i, j] = integral of
+    phi_j' phi_i = [[-1/2, 1/2], [-1/2, 1/2]]."""
+    m = np.array([[1.0 / 3.0, 1.0 / 6.0], [1.0 / 6.0, 1.0 / 3.0]]) * h
+    d = np.array([[-0.5, 0.5], [-0.5, 0.5]])
+    if dim == 2:
+        return beta[0] * np.kron(m, d) + beta[1] * np.kron(d, m)
+    return (beta[0] * np.kron(np.kron(m, m), d) + beta[1] * np.kron(np.kron(m, d), m)
+            + beta[2] * np.kron(np.kron(d, m), m))
+
+
+def cell_nodes(dim: int, N: int) -> np.ndarray:
+    """Node indices of the N^dim cells (lexicographic cells and nodes, x
+    fastest), local node order lexicographic: int64 [N^dim, 2^dim]."""
+    n1 = N + 1
+    if dim == 3:
+        k, j, i = np.meshgrid(np.arange(N), np.arange(N), np.arange(N), indexing="ij")
+        base = ((k * n1 + j) * n1 + i).ravel()
+        offs = np.array([(a * n1 + b) * n1 + e for a in range(2) for b in range(2)
+                         for e in range(2)])
+    else:
+        j, i = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+        base = (j * n1 + i).ravel()
+        offs = np.array([b * n1 + e for b in range(2) for e in range(2)])
+    return (base[:, None] + offs[None, :]).astype(np.int64)
+
+
 def kappa_pyramid(dim: int, fine: np.ndarray, levels: int) -> List[np.ndarray]:
     """Per-level cell coefficients, finest last; a coarse cell takes the mean of
     its 2^dim children summed in lexicographic child order (z, y, x)."""
@@ -153,8 +219,8 @@ def kappa_pyramid(dim: int, fine: np.ndarray, levels: int) -> List[np.ndarray]:
     return out[::-1]
 
 
-def _assemble_level(dim: int, N: int, kappa: np.ndarray) -> Level:
-    """Assembles -div(kappa grad u) with Q1 on N^dim uniform cells of the unit
+def _assemble_level(dim: int, N: int, kappa: np.ndarray, beta=None) -> Level:
+    """Assembles -div(kappa grad u) [+ beta . grad u] with Q1 on N^dim uniform cells of the unit
     square/cube, lexicographic node numbering, full neighbour stencil with
     columns sorted ascending, strong zero Dirichlet on the whole boundary
     (SparseBlockMatrix::dirichlet: row and column zeroed, diagonal 1,
@@ -164,20 +230,14 @@ def _assemble_level(dim: int, N: int, kappa: np.ndarray) -> Level:
     n1 = N + 1
     K = _q1_local_stiffness(dim, h)
     nloc = 2 ** dim
-    if dim == 3:
-        k, j, i = np.meshgrid(np.arange(N), np.arange(N), np.arange(N), indexing="ij")
-        base = ((k * n1 + j) * n1 + i).ravel()
-        offs = np.array([(a * n1 + b) * n1 + e for a in range(2) for b in range(2)
-                         for e in range(2)])
-    else:
-        j, i = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
-        base = (j * n1 + i).ravel()
-        offs = np.array([b * n1 + e for b in range(2) for e in range(2)])
-    nodes = base[:, None] + offs[None, :]                 # [ncell, nloc]
+    nodes = cell_nodes(dim, N)                            # [ncell, nloc]
     kap = kappa.ravel()
     rows = np.repeat(nodes, nloc, axis=1).ravel()
     cols = np.tile(nodes, (1, nloc)).ravel()
-    vals = (kap[:, None] * K.ravel()[None, :]).ravel()
+    vals = (kap[:, None] * K.ravel()[None, :])
+    if beta is not None and any(beta):
+        vals = vals + _q1_local_convection(dim, h, beta).ravel()[None, :]
+    vals = vals.ravel()
     n = n1 ** dim
     A = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
     A.sum_duplicates()
@@ -249,14 +309,16 @@ def _structured_transfer(dim: int, Nc: int) -> Transfer:
 
 def structured_problem(dim: int, coarse: int, refine: int,
                        kappa: Optional[np.ndarray] = None,
-                       rhs: Optional[np.ndarray] = None) -> Problem:
+                       rhs: Optional[np.ndarray] = None, beta=None) -> Problem:
     """The reference's multilevel system for -div(kappa grad u) = f on the unit
     square/cube built from coarse^dim cells refined `refine` times, with the
     reference's default patchdepth 1: `refine` multigrid levels, the coarsest
     having 2*coarse cells per dimension (Mesh/hierarchicalmesh.cc:126-148,
     Mesh/meshagent.cc:83). kappa: per finest cell (lexicographic, x fastest),
     default 1. rhs: per finest node (lexicographic), default 1; zeroed at
-    Dirichlet nodes."""
+    Dirichlet nodes. beta: constant convection vector (default none; the
+    operator is then symmetric). The finest level's cells (for the
+    coefficient gradient and the L2 functional) come with the problem."""
     Nf = coarse << refine
     if kappa is None:
         kappa = np.ones((Nf,) * dim)
@@ -266,14 +328,19 @@ def structured_problem(dim: int, coarse: int, refine: int,
     levels = []
     for l in range(nlev):
         N = (2 * coarse) << l
-        levels.append(_assemble_level(dim, N, kap[l]))
+        levels.append(_assemble_level(dim, N, kap[l], beta))
     transfers = [_structured_transfer(dim, (2 * coarse) << l) for l in range(nlev - 1)]
     nfin = levels[-1].n
     b = np.ones(nfin) if rhs is None else np.asarray(rhs, dtype=np.float64).copy()
     b[levels[-1].dirichlet] = 0.0
+    hf = 1.0 / ((2 * coarse) << (nlev - 1))
+    cells = Cells(nodes=cell_nodes(dim, (2 * coarse) << (nlev - 1)),
+                  kloc=_q1_local_stiffness(dim, hf), mloc=_q1_local_mass(dim, hf))
     return Problem(dim=dim, levels=levels, transfers=transfers, rhs=b,
                    info={"generator": "structured", "coarse": coarse,
-                         "refine": refine})
+                         "refine": refine,
+                         "beta": None if beta is None else list(beta)},
+                   cells=cells)
 
 
 def seeded_inputs(dim: int, coarse: int, refine: int, kappa_seed: int = 1001,

@@ -193,6 +193,45 @@ int gb_fgmres(gb_ctx* ctx, int x, int b, int precision, gb_solve_info* info);
 int gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x,
                   int64_t len, gb_solve_info* info);
 
+/* ---- adjoint (dual) path ---------------------------------------------------
+ * gb_set_operator(ctx, 1) makes every level operator A^T for all following
+ * calls (vmult, residuals, smoothers, the cycle, both GMRES forms;
+ * gb_vmult_transpose then applies A), 0 switches back to A. It stands in for
+ * StdMultiLevelSolver::AssembleDualMatrix (Solver/stdmultilevelsolver.cc:
+ * 920-926 -> Solver/stdsolver.cc:1815-1834: assemble, transpose, Dirichlet
+ * rows only) without re-uploading: A^T is built once per level from the
+ * uploaded matrix, keeping its sparsity pattern when that is structurally
+ * symmetric (values swapped as SparseBlockMatrix::transpose,
+ * LinAlg/sparseblockmatrix.xx:478-491). The transfers stay those of the
+ * forward hierarchy (restriction R = P^T, prolongation P), as the reference's
+ * dual solve uses them. Solutions equal the reference's dual solutions for
+ * right-hand sides that are zero on Dirichlet dofs (the reference zeroes them,
+ * StdSolver::SetBoundaryVectorZero). */
+int gb_set_operator(gb_ctx* ctx, int transposed);
+int gb_get_operator(const gb_ctx* ctx, int* transposed);
+/* A^T x = b with the reference-semantics solver (as gb_gmres) or the
+ * flexible solver (as gb_fgmres); the operator setting is restored after. */
+int gb_adjoint_gmres(gb_ctx* ctx, int x, int b, gb_solve_info* info);
+int gb_adjoint_fgmres(gb_ctx* ctx, int x, int b, int precision, gb_solve_info* info);
+/* Cells of `level` for the coefficient gradient: cell c has nodes
+ * cell_nodes[c*nloc .. c*nloc+nloc-1] (int64) and element matrix
+ * kappa_c * cell_scale[c] * kloc (kloc: nloc x nloc doubles, row-major, row =
+ * test function, column = trial function; cell_scale NULL means 1), the
+ * element assembly of an equation with a per-cell coefficient
+ * (DofHandler/cgdisc.h:599-635, Interface/equation.h:104,
+ * Interface/application.h:69). nloc <= 32. */
+int gb_level_set_cells(gb_ctx* ctx, int level, int64_t ncells, int nloc,
+                       const int64_t* cell_nodes, const double* kloc,
+                       const double* cell_scale);
+/* grad[c] = -cell_scale[c] * lam_c^T kloc u_c over the cells of `level`, with
+ * u and lam (vector ids) read as 0 on Dirichlet dofs: dJ/dkappa_c for
+ * J(u(kappa)) when lam solves A^T lam = dJ/du (gb_adjoint_*), since
+ * dA/dkappa_c is the cell matrix restricted to the non-Dirichlet dofs.
+ * grad: host array of ncells doubles. No counterpart in the reference
+ * (StdSolver::AdjointForm aborts, Solver/stdsolver.cc:1080). */
+int gb_coeff_gradient(gb_ctx* ctx, int level, int u, int lam, double* grad,
+                      int64_t ncells);
+
 /* ---- instrumentation ------------------------------------------------------
  * Per-kernel-class device time of the last gb_* solve call when timing is on
  * (CUDA events on the context stream); replaces GlobalTimer's vmult/smooth

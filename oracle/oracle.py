@@ -229,3 +229,55 @@ def write_inputs(d, kappa=None, rhs=None):
         np.ascontiguousarray(rhs, dtype=np.float64).tofile(p)
         kw["rhs"] = p
     return kw
+
+
+# ------------------------------------------------------------------ adjoint
+
+def transposed_problem(prob):
+    """The dual system of ``StdSolver::AssembleDualMatrix``
+    (Solver/stdsolver.cc:1815-1834) on every level: each level matrix
+    transposed inside its own stencil, entry (i, j) taking the value of (j, i)
+    as ``SparseBlockMatrix::transpose`` swaps them
+    (LinAlg/sparseblockmatrix.xx:478-491), so row i keeps its column order.
+    The uploaded matrices have Dirichlet rows and columns both set to identity,
+    so their transposes are the reference's transpose-then-Dirichlet-rows
+    matrices on every vector that is zero on the Dirichlet dofs. Transfers and
+    the right-hand side are shared with ``prob``."""
+    import copy
+    out = copy.copy(prob)
+    out.levels = []
+    for L in prob.levels:
+        assert L.B == 1
+        n = L.n
+        rowidx = np.repeat(np.arange(n), np.diff(L.rowptr))
+        # position of (j, i) for every entry (i, j): sort the entries by key
+        key = rowidx * n + L.col
+        tkey = L.col * n + rowidx
+        order = np.argsort(key)
+        pos = np.searchsorted(key[order], tkey)
+        if np.any(pos >= key.size) or np.any(key[order][np.minimum(pos, key.size - 1)] != tkey):
+            raise ValueError("level matrix is not structurally symmetric")
+        Lt = copy.copy(L)
+        Lt.val = L.val[order[pos]].copy()
+        out.levels.append(Lt)
+    return out
+
+
+def coeff_gradient(cells, u, lam, dirichlet):
+    """dJ/dkappa_c = -scale_c * lam_c^T kloc u_c with u, lam zero on the
+    Dirichlet nodes: the derivative of the per-cell element assembly
+    (DofHandler/cgdisc.h:599-635 with a per-cell coefficient) restricted to the
+    non-Dirichlet rows and columns of the strongly constrained matrix
+    (LinAlg/sparseblockmatrix.xx:205-218), contracted with the dual and primal
+    solutions. Plain numpy; the reference has no such gradient
+    (Solver/stdsolver.cc:1080)."""
+    u = np.array(u, dtype=np.float64)
+    lam = np.array(lam, dtype=np.float64)
+    u[dirichlet] = 0.0
+    lam[dirichlet] = 0.0
+    uc = u[cells.nodes]
+    lc = lam[cells.nodes]
+    g = -np.einsum("ci,ij,cj->c", lc, cells.kloc, uc)
+    if cells.scale is not None:
+        g = g * cells.scale
+    return g

@@ -7,9 +7,12 @@
 //   (Solver/stdmultilevelsolver.cc:152-309,762-790), and
 //   StdMultiLevelSolver::NewtonLinearSolve -> Gmres -> GMRES::solve + LinearMg
 //   (Solver/stdmultilevelsolver.cc:646-689, LinAlg/gmres.cc:159-230).
-// The equation is -div(kappa grad u) = f with kappa piecewise constant per cell
+// The equation is -div(kappa grad u) + beta . grad u = f with kappa piecewise
+// constant per cell
 // (per finest cell from a file; a coarse cell takes the mean of its 2^dim
-// children, summed in lexicographic child order), assembled by the reference's
+// children, summed in lexicographic child order) and a constant convection
+// vector beta (key conv=bx,by[,bz]; default 0, which leaves the operator
+// symmetric), assembled by the reference's
 // CGDisc with its own Q1 element integrator (HexGauss8 / QuadGauss4,
 // DofHandler/elementintegrator.h:215-222). Dirichlet data: u = 0 on the whole
 // boundary (colour 1). The right-hand side is a nodal vector read from a file
@@ -24,6 +27,9 @@
 //     (transfer between level l (coarse) and l+1 (fine); zweier rows are
 //      [fine, coarse0, coarse1], vierer [fine, 4 coarse], achter [fine, 8 coarse])
 //   rhs.f64 solution.f64 (finest level, reference node numbering)
+// and with dualrhs= (a nodal vector like rhs): dual_summary.txt,
+//   dual_rhs.f64 dual_solution.f64, and with dump=1 L<l>_dualval.f64 (the
+//   dual matrices' values in the stencil of L<l>_col.i64)
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -63,6 +69,7 @@ struct Config
   double omega = 0.8, tol = 1e-8, globaltol = 1e-16, mgomega = 1.0;
   int maxiter = 100, ndirect = 1, dump = 0, repeat = 1, patchdepth = 1;
   std::string mgtype = "V";
+  double conv[3] = { 0.0, 0.0, 0.0 };
 };
 
 // kappa per cell, one array per resolution N = coarse * 2^l (cells per dim),
@@ -92,14 +99,18 @@ class DiffusionEquation : public virtual Equation
 {
   mutable double kappa_ = 1.0;
   int dim_;
+  double beta_[3];
 
 public:
-  explicit DiffusionEquation(int dim)
+  DiffusionEquation(int dim, const double* beta)
     : dim_(dim)
-  {}
+  {
+    for (int i = 0; i < 3; ++i)
+      beta_[i] = beta[i];
+  }
   DiffusionEquation* createNew() const override
   {
-    return new DiffusionEquation(dim_);
+    return new DiffusionEquation(dim_, beta_);
   }
   std::string GetName() const override { return "OracleDiffusion"; }
   int GetNcomp() const override { return 1; }
@@ -120,25 +131,26 @@ public:
             const TestFunction& N) const override
   {
     for (int i = 0; i < dim_; ++i)
-      b[0] += kappa_ * U[0][i + 1] * N[i + 1];
+      b[0] += kappa_ * U[0][i + 1] * N[i + 1] + beta_[i] * U[0][i + 1] * N.m();
   }
   void Matrix(EntryMatrix& A,
               const FemFunction&,
               const TestFunction& M,
               const TestFunction& N) const override
   {
+    // M: trial function, N: test function (as Problems/navierstokes.h:164)
     for (int i = 0; i < dim_; ++i)
-      A(0, 0) += kappa_ * M[i + 1] * N[i + 1];
+      A(0, 0) += kappa_ * M[i + 1] * N[i + 1] + beta_[i] * M[i + 1] * N.m();
   }
 };
 
 class DiffusionProblem : public ProblemDescriptorBase
 {
 public:
-  void BasicInit(const ParamFile& pf, int dim)
+  void BasicInit(const ParamFile& pf, int dim, const double* beta)
   {
     GetParamFile() = pf;
-    GetEquationPointer() = new DiffusionEquation(dim);
+    GetEquationPointer() = new DiffusionEquation(dim, beta);
     GetDirichletDataPointer() = new ZeroDirichletData(pf);
     ProblemDescriptorBase::BasicInit(pf);
   }
@@ -177,6 +189,12 @@ parse(int argc, char** argv)
     else if (k == "dump") c.dump = atoi(v.c_str());
     else if (k == "repeat") c.repeat = atoi(v.c_str());
     else if (k == "patchdepth") c.patchdepth = atoi(v.c_str());
+    else if (k == "conv") {
+      std::stringstream ss(v);
+      std::string t;
+      for (int i = 0; i < 3 && std::getline(ss, t, ','); ++i)
+        c.conv[i] = atof(t.c_str());
+    }
     else {
       fprintf(stderr, "ref_harness: unknown key %s\n", k.c_str());
       exit(2);
@@ -355,7 +373,7 @@ main(int argc, char** argv)
 
   ParamFile pf(pfile);
   DiffusionProblem PD;
-  PD.BasicInit(pf, c.dim);
+  PD.BasicInit(pf, c.dim, c.conv);
   ProblemContainer PC;
   PC.AddProblem("diffusion", &PD);
   FunctionalContainer FC;
@@ -558,6 +576,16 @@ main(int argc, char** argv)
     }
     S->SetBoundaryVectorZero(g);
     MLS.AssembleDualMatrix(A, u);
+    if (c.dump)
+      for (int l = 0; l < nl; ++l) {
+        const auto* M = dynamic_cast<const SparseBlockMatrix<FMatrixBlock<1>>*>(
+          &MLS.GetSolver(l)->GetMatrix(A));
+        const auto* ST = dynamic_cast<const ColumnDiagStencil*>(M->GetStencil());
+        std::vector<double> val(ST->nentries());
+        for (size_t p = 0; p < ST->nentries(); ++p)
+          val[p] = (*M->mat(p))(0, 0);
+        write_raw(c.out + "/L" + std::to_string(l) + "_dualval.f64", val);
+      }
     CGInfo dinfo(c.tol, c.globaltol, 0, c.maxiter, "Dual");
     for (int rep = 0; rep < std::max(1, c.repeat); ++rep) {
       dinfo.reset();

@@ -4,7 +4,8 @@ import os
 
 import numpy as np
 
-from gascoignelib_b200.problem import Level, Problem, Transfer
+from gascoignelib_b200.problem import (Cells, Level, Problem, Transfer, _q1_local_mass,
+                                       _q1_local_stiffness, cell_nodes)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -37,7 +38,45 @@ def load_golden(name):
     ref = {"solution": z["solution"], "iterations": int(z["iterations"]),
            "firstresidual": float(z["firstresidual"]), "residual": float(z["residual"]),
            "status": str(z["status"]), "keys": keys}
+    if "dual_solution" in z.files:
+        ref.update(dual_rhs=z["dual_rhs"], dual_solution=z["dual_solution"],
+                   dual_iterations=int(z["dual_iterations"]),
+                   dual_firstresidual=float(z["dual_firstresidual"]),
+                   dual_residual=float(z["dual_residual"]),
+                   dual_status=str(z["dual_status"]),
+                   dualval=[z[f"L{l}_dualval"] for l in range(nl)])
     return P, ref
+
+
+def golden_dual_cases():
+    return [n for n in golden_cases() if n.endswith("_dual")]
+
+
+def dual_problem(P, ref):
+    """P with the reference's own dual matrices (transpose, Dirichlet rows)."""
+    import copy
+    D = copy.copy(P)
+    D.levels = []
+    for L, dv in zip(P.levels, ref["dualval"]):
+        Lt = copy.copy(L)
+        Lt.val = dv
+        D.levels.append(Lt)
+    return D
+
+
+def reference_cells(P):
+    """Finest-level cells of a uniform unit square/cube mesh in the
+    reference's node numbering (mapped through the node coordinates)."""
+    dim = P.dim
+    N = round(P.finest.n ** (1.0 / dim)) - 1
+    c = np.rint(P.finest.coord * N).astype(np.int64)
+    lex = np.zeros(c.shape[0], dtype=np.int64)
+    for d in reversed(range(dim)):
+        lex = lex * (N + 1) + c[:, d]
+    inv = np.empty_like(lex)
+    inv[lex] = np.arange(lex.size)
+    return Cells(nodes=inv[cell_nodes(dim, N)], kloc=_q1_local_stiffness(dim, 1.0 / N),
+                 mloc=_q1_local_mass(dim, 1.0 / N))
 
 
 def solver_keys(keys):

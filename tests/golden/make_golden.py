@@ -3,7 +3,11 @@ CPU solver (oracle/_ref/ref_harness, compiled from the reference's sources by
 oracle/ref/Makefile) on small seeded problems and saving what it assembled and
 solved: per-level matrices, Dirichlet lists and transfer maps in the
 reference's node numbering, the right-hand side, the solution, the iteration
-count and its CGInfo residuals.
+count and its CGInfo residuals. The "_dual" cases add a convection term (a
+nonsymmetric operator) and the reference's dual solve
+(StdMultiLevelSolver::AssembleDualMatrix + the same Gmres): the dual matrices'
+values, the dual right-hand side dJ/du = 2 M u of J(u) = integral of u^2 (M the
+Q1 mass matrix, u the forward solution of a first run) and the dual solution.
 
     python tests/golden/make_golden.py
 """
@@ -16,7 +20,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-from gascoignelib_b200.problem import load_reference_dump, seeded_inputs  # noqa: E402
+from gascoignelib_b200.problem import (cell_nodes, load_reference_dump,  # noqa: E402
+                                       seeded_inputs, _q1_local_mass)
 from oracle.oracle import run_reference, write_inputs  # noqa: E402
 
 # name: (dim, coarse, refine, seeded, tol, extra harness keys)
@@ -27,7 +32,37 @@ CASES = {
     "q1_3d_c1_r3_wcycle": (3, 1, 3, True, 1e-8, {"mgtype": "W", "iterpre": 1,
                                                   "iterpost": 3, "omega": 0.7}),
     "q1_2d_c2_r3_fcycle": (2, 2, 3, True, 1e-10, {"mgtype": "F", "mgomega": 0.9}),
+    "q1_3d_c1_r3_conv_dual": (3, 1, 3, True, 1e-8, {"conv": "1,0.5,0.25"}),
+    "q1_2d_c2_r4_conv_dual": (2, 2, 4, True, 1e-10, {"conv": "4,2"}),
 }
+
+
+def lex_permutation(coord, N):
+    """Reference node -> lexicographic node index (x fastest) on N cells per
+    dimension."""
+    c = np.rint(coord * N).astype(np.int64)
+    idx = np.zeros(c.shape[0], dtype=np.int64)
+    for d in reversed(range(c.shape[1])):
+        idx = idx * (N + 1) + c[:, d]
+    return idx
+
+
+def l2_dual_rhs(P, u_ref):
+    """2 M u on the lexicographic node order (what the harness reads)."""
+    import scipy.sparse as sp
+    dim = P.dim
+    N = round(P.finest.n ** (1.0 / dim)) - 1
+    perm = lex_permutation(P.finest.coord, N)
+    u = np.empty_like(u_ref)
+    u[perm] = u_ref
+    nodes = cell_nodes(dim, N)
+    ml = _q1_local_mass(dim, 1.0 / N)
+    nl = nodes.shape[1]
+    M = sp.coo_matrix((np.tile(ml.ravel(), nodes.shape[0]),
+                       (np.repeat(nodes, nl, axis=1).ravel(),
+                        np.tile(nodes, (1, nl)).ravel())),
+                      shape=(u.size, u.size)).tocsr()
+    return 2.0 * (M @ u)
 
 
 def make(name, dim, coarse, refine, seeded, tol, extra):
@@ -39,6 +74,14 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
     keys = dict(dim=dim, coarse=coarse, refine=refine, dump=1, tol=tol,
                 gmressize=21, iterpre=2, iterpost=2, iterexact=10, omega=0.8)
     keys.update(extra)
+    dual = name.endswith("_dual")
+    if dual:
+        out0, _ = run_reference(d, **keys, **kw)
+        P0 = load_reference_dump(out0)
+        g = l2_dual_rhs(P0, np.fromfile(os.path.join(out0, "solution.f64")))
+        gp = os.path.join(d, "dual_in.f64")
+        g.tofile(gp)
+        kw["dualrhs"] = gp
     out, summ = run_reference(d, **keys, **kw)
     P = load_reference_dump(out)
     arrs = {"dim": P.dim, "nlevels": P.nlevels, "rhs": P.rhs,
@@ -50,6 +93,20 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
             else " ".join(summ["status"])}
     for k, v in keys.items():
         arrs["key_" + k] = v
+    if dual:
+        ds = {}
+        with open(os.path.join(out, "dual_summary.txt")) as f:
+            for line in f:
+                k, *v = line.split()
+                ds[k] = v
+        arrs["dual_rhs"] = np.fromfile(os.path.join(out, "dual_rhs.f64"))
+        arrs["dual_solution"] = np.fromfile(os.path.join(out, "dual_solution.f64"))
+        arrs["dual_iterations"] = int(ds["dual_iterations"][0])
+        arrs["dual_firstresidual"] = float(ds["dual_firstresidual"][0])
+        arrs["dual_residual"] = float(ds["dual_residual"][0])
+        arrs["dual_status"] = " ".join(ds["dual_status"])
+        for l in range(P.nlevels):
+            arrs[f"L{l}_dualval"] = np.fromfile(os.path.join(out, f"L{l}_dualval.f64"))
     for l, lv in enumerate(P.levels):
         arrs[f"L{l}_rowptr"] = lv.rowptr.astype(np.int32)
         arrs[f"L{l}_col"] = lv.col.astype(np.int32)
@@ -67,5 +124,7 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
 
 
 if __name__ == "__main__":
+    only = sys.argv[1:]
     for name, spec in CASES.items():
-        make(name, *spec)
+        if not only or name in only:
+            make(name, *spec)
