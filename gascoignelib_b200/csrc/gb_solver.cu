@@ -268,6 +268,9 @@ struct Level
   DeviceArray<int> cells; // node-major: entry i of cell c at i * ncells + c
   DeviceArray<double> kloc, cscale, grad;
   bool has_scale = false;
+  // quadratic functional J(u) = u^T M u over the cells (gb_level_set_functional)
+  Sell M;
+  int64_t func_n = -1;
   int64_t ndof() const { return n * B; }
 };
 
@@ -2411,6 +2414,80 @@ gb_level_set_cells(gb_ctx* ctx, int lvl, int64_t ncells, int nloc,
 }
 
 int
+gb_level_set_functional(gb_ctx* ctx, int lvl, const double* mloc, const double* cell_scale)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(L.ncells > 0 && L.cells_n == L.n, GB_ESTATE,
+             "no cells for this level's matrix (gb_level_set_cells)");
+  GB_REQUIRE(L.B == 1, GB_EINVAL, "functional needs block size 1");
+  GB_REQUIRE(mloc, GB_EINVAL, "null array");
+  const int64_t n = L.n, nc = L.ncells;
+  const int nl = L.nloc;
+  // cell nodes back from the device layout
+  std::vector<int> cn(size_t(nc) * nl);
+  GB_CUDA(cudaMemcpyAsync(cn.data(), L.cells.p, cn.size() * sizeof(int),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  // per row: columns sorted with their stencil positions, for the lookups
+  std::vector<std::pair<int64_t, int64_t>> sc(L.h_col.size());
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k)
+      sc[k] = { L.h_col[k], k };
+    std::sort(sc.begin() + L.h_rowptr[i], sc.begin() + L.h_rowptr[i + 1]);
+  }
+  std::vector<double> mv(L.h_col.size(), 0.0);
+  for (int64_t c = 0; c < nc; ++c) {
+    const double w = cell_scale ? cell_scale[c] : 1.0;
+    for (int a = 0; a < nl; ++a) {
+      const int64_t r = cn[size_t(a) * nc + c];
+      auto b = sc.begin() + L.h_rowptr[r], e = sc.begin() + L.h_rowptr[r + 1];
+      for (int q = 0; q < nl; ++q) {
+        const int64_t col = cn[size_t(q) * nc + c];
+        auto f = std::lower_bound(b, e, std::make_pair(col, int64_t(-1)));
+        GB_REQUIRE(f != e && f->first == col, GB_EINVAL,
+                   "cell matrix entry outside the level's sparsity pattern");
+        mv[f->second] += w * mloc[a * nl + q];
+      }
+    }
+  }
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  build_sell(L.M, n, L.h_rowptr.data(), L.h_col.data(), mv.data(), ctx->stream);
+  L.func_n = n;
+  GB_API_END
+}
+
+int
+gb_functional(gb_ctx* ctx, int lvl, int u, int g, double* J)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(L.func_n == L.n, GB_ESTATE,
+             "no functional for this level's matrix (gb_level_set_functional)");
+  GB_REQUIRE(u != g, GB_EINVAL, "u and g must differ");
+  const double* ud = vec(*ctx, lvl, u);
+  double* gd = vec(*ctx, lvl, g);
+  // g = 2 M u, J = u . (M u) = (u . g) / 2, then g = 0 on Dirichlet dofs
+  spmv<kAx, double, double, double>(*ctx, L, L.M, ud, gd, nullptr, nullptr, 2.0);
+  if (J)
+    dot_dev(*ctx, L.ndof(), ud, gd, RedOut{ ctx->scal.p + 6, nullptr, nullptr, 0 });
+  launch(*ctx, k_dirichlet_zero<double>, blocks_for(L.ndir, 256), 256, L.ndir,
+         (const int*)L.dirlist.p, gd);
+  if (J)
+    *J = 0.5 * read_scalar(*ctx, ctx->scal.p + 6);
+  GB_API_END
+}
+
+int
+gb_ctx_get_stream(const gb_ctx* ctx, void** stream)
+{
+  if (!ctx || !stream)
+    return GB_EINVAL;
+  *stream = ctx->stream;
+  return GB_OK;
+}
+
+int
 gb_coeff_gradient(gb_ctx* ctx, int lvl, int u, int lam, double* grad, int64_t ncells)
 {
   GB_API_BEGIN
@@ -2418,7 +2495,7 @@ gb_coeff_gradient(gb_ctx* ctx, int lvl, int u, int lam, double* grad, int64_t nc
   GB_REQUIRE(L.ncells > 0 && L.cells_n == L.n, GB_ESTATE,
              "no cells for this level's matrix (gb_level_set_cells)");
   GB_REQUIRE(L.B == 1, GB_EINVAL, "coefficient gradient needs block size 1");
-  GB_REQUIRE(grad && ncells == L.ncells, GB_EINVAL, "grad length differs from ncells");
+  GB_REQUIRE(ncells == L.ncells, GB_EINVAL, "ncells differs from the level's cells");
   const double* ud = vec(*ctx, lvl, u);
   const double* ld = vec(*ctx, lvl, lam);
   const int nb = blocks_for(L.ncells, 256);
@@ -2445,9 +2522,11 @@ gb_coeff_gradient(gb_ctx* ctx, int lvl, int u, int lam, double* grad, int64_t nc
       launch(*ctx, k_coeff_gradient<0>, nb, 256, L.ncells, L.nloc, (const int*)L.cells.p,
              (const double*)L.kloc.p, sc, ud, ld, mk, L.grad.p);
   }
-  GB_CUDA(cudaMemcpyAsync(grad, L.grad.p, ncells * sizeof(double),
-                          cudaMemcpyDeviceToHost, ctx->stream));
-  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (grad) {
+    GB_CUDA(cudaMemcpyAsync(grad, L.grad.p, ncells * sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
   GB_API_END
 }
 

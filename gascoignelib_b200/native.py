@@ -94,6 +94,9 @@ _SIGS = {
     "gb_adjoint_fgmres": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(GbSolveInfo)],
     "gb_level_set_cells": [C.c_void_p, C.c_int, C.c_int64, C.c_int, _P64, _PD, _PD],
     "gb_coeff_gradient": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD, C.c_int64],
+    "gb_level_set_functional": [C.c_void_p, C.c_int, _PD, _PD],
+    "gb_functional": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD],
+    "gb_ctx_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
     "gb_bench_spmv": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
@@ -213,6 +216,9 @@ class Context:
             self.h, level, nd.shape[0], nd.shape[1], _p64(nd), _pd(kl),
             _pd(sc) if sc is not None else None))
         self.ncells = nd.shape[0]
+        if cells.mloc is not None:
+            ml = np.ascontiguousarray(cells.mloc, dtype=np.float64)
+            self._chk(self._L.gb_level_set_functional(self.h, level, _pd(ml), None))
 
     # ------------------------------------------------------------ vectors
     def vec(self):
@@ -321,10 +327,25 @@ class Context:
             self._chk(rc)
         return info.as_dict()
 
-    def coeff_gradient(self, level, u, lam):
+    def coeff_gradient(self, level, u, lam, download=True):
+        if not download:  # computed and kept on the device
+            self._chk(self._L.gb_coeff_gradient(self.h, level, u, lam, None, self.ncells))
+            return None
         g = np.empty(self.ncells, dtype=np.float64)
         self._chk(self._L.gb_coeff_gradient(self.h, level, u, lam, _pd(g), g.shape[0]))
         return g
+
+    def functional(self, level, u, g, read=True):
+        """J = u^T M u and g = 2 M u (0 on Dirichlet dofs) on the device."""
+        J = C.c_double()
+        self._chk(self._L.gb_functional(self.h, level, u, g, C.byref(J) if read else None))
+        return J.value if read else None
+
+    def stream(self):
+        """The context's CUDA stream handle (cudaStream_t as an int)."""
+        s = C.c_void_p()
+        self._chk(self._L.gb_ctx_get_stream(self.h, C.byref(s)))
+        return s.value or 0
 
     def solve_host(self, b, method=2, out=None, check=True):
         b = np.ascontiguousarray(b, dtype=np.float64)

@@ -227,10 +227,26 @@ int gb_level_set_cells(gb_ctx* ctx, int level, int64_t ncells, int nloc,
  * u and lam (vector ids) read as 0 on Dirichlet dofs: dJ/dkappa_c for
  * J(u(kappa)) when lam solves A^T lam = dJ/du (gb_adjoint_*), since
  * dA/dkappa_c is the cell matrix restricted to the non-Dirichlet dofs.
- * grad: host array of ncells doubles. No counterpart in the reference
+ * grad: host array of ncells doubles or NULL. No counterpart in the reference
  * (StdSolver::AdjointForm aborts, Solver/stdsolver.cc:1080). */
 int gb_coeff_gradient(gb_ctx* ctx, int level, int u, int lam, double* grad,
                       int64_t ncells);
+/* (grad may be NULL: the gradient is computed and kept on the device, nothing
+ * is copied and the call does not wait for the GPU.)
+ * A quadratic functional J(u) = u^T M u over the cells of gb_level_set_cells,
+ * M = sum over cells of cell_scale[c] * mloc (nloc x nloc, row-major; NULL
+ * scale means 1), assembled into the level matrix's sparsity pattern; with
+ * the Q1 element mass matrix this is J = integral of u^2, the reference's
+ * DomainFunctional for it (Interface/domainfunctional.h:42-64).
+ * gb_functional computes J (J may be NULL: not read back) and g = dJ/du =
+ * 2 M u with g = 0 on Dirichlet dofs, the dual right-hand side of
+ * gb_adjoint_*. No counterpart in the reference's GPU backend. */
+int gb_level_set_functional(gb_ctx* ctx, int level, const double* mloc,
+                            const double* cell_scale);
+int gb_functional(gb_ctx* ctx, int level, int u, int g, double* J);
+/* The context's CUDA stream (a cudaStream_t): every gb_* call enqueues its
+ * work there, so callers can order their own work or record events on it. */
+int gb_ctx_get_stream(const gb_ctx* ctx, void** stream);
 
 /* ---- instrumentation ------------------------------------------------------
  * Per-kernel-class device time of the last gb_* solve call when timing is on

@@ -259,3 +259,57 @@ def test_autograd_gradient_matches_central_fd(ctx, dim, coarse, refine, beta):
     k2 = torch.tensor(kappa0, dtype=torch.float64, requires_grad=True)
     _functional(k2, (ctx, dim, coarse, refine, rhs, beta, GB_FP32), M).backward()
     assert np.linalg.norm(k2.grad.numpy() - grad) <= 1e-7 * np.linalg.norm(grad)
+
+
+def test_c5_adjoint_gradient_full_size(ctx):
+    """96^3 cells (912,673 dofs), kappa = exp(N(0,1)), J = int u^2: GPU
+    forward and adjoint solves with the FP32 cycle in FP64 flexible GMRES and
+    the gradient kernel, against the oracle's FP64 reference-semantics forward
+    and dual solves (1e-6 relative in the gradient)."""
+    kappa, rhs = seeded_inputs(3, 3, 5)
+    P = structured_problem(3, 3, 5, kappa, rhs)
+    assert P.finest.n == 912673 and P.cells.ncells == 884736
+    O = Oracle(P)
+    uo, io = O.gmres(vmax=21, tol=1e-10)
+    M = P.cells.assemble(P.cells.mloc, P.finest.n)
+    g = 2.0 * (M @ uo)
+    g[P.finest.dirichlet] = 0.0
+    # the diffusion operator is symmetric: its dual system is the forward one
+    A = _csr(P.finest)
+    assert abs(A - A.T).max() == 0.0
+    lo, _ = O.gmres(g, vmax=21, tol=1e-10)
+    go = coeff_gradient(P.cells, uo, lo, P.finest.dirichlet)
+    O.close()
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=21, tol=1e-10, globaltol=1e-300, maxiter=200)
+    l = P.nlevels - 1
+    u, b, lam, gv = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    assert ctx.fgmres(u, b, GB_FP32)["true_rel_residual"] <= 1e-10
+    Jg = ctx.functional(l, u, gv)  # J = u^T M u and the dual rhs 2 M u on the device
+    assert ctx.adjoint_fgmres(lam, gv, GB_FP32)["true_rel_residual"] <= 1e-10
+    grad = ctx.coeff_gradient(l, u, lam)
+    assert np.linalg.norm(grad - go) <= 1e-6 * np.linalg.norm(go)
+    Jo = uo @ (M @ uo)
+    assert abs(Jg - Jo) <= 1e-8 * abs(Jo)
+    for v in (u, b, lam, gv):
+        ctx.free(v)
+
+
+def test_device_functional_and_stream(ctx):
+    kappa, rhs = seeded_inputs(3, 1, 4)
+    P = structured_problem(3, 1, 4, kappa, rhs)
+    ctx.load_problem(P)
+    l = P.nlevels - 1
+    M = P.cells.assemble(P.cells.mloc, P.finest.n)
+    uv = np.random.default_rng(9).normal(size=P.finest.n)
+    u, g = ctx.vec(), ctx.vec()
+    ctx.upload(l, u, uv)
+    J = ctx.functional(l, u, g)
+    assert abs(J - uv @ (M @ uv)) <= 1e-13 * abs(J)
+    gr = 2.0 * (M @ uv)
+    gr[P.finest.dirichlet] = 0.0
+    assert rel(ctx.download(l, g), gr) < 1e-14
+    assert ctx.stream() != 0
+    ctx.free(u)
+    ctx.free(g)
