@@ -39,6 +39,14 @@ class Level:
     dirichlet: np.ndarray       # int64 [ndir] Dirichlet nodes
     dircomp_mask: int = 1       # bit c: component c is Dirichlet
     coord: Optional[np.ndarray] = None  # float64 [n, dim]
+    # pressure filter (PressureFilter): filtered components, per-node weights
+    # (integrals of the basis functions) and the domain size; mask 0: inactive
+    pf_mask: int = 0
+    pf_weights: Optional[np.ndarray] = None
+    pf_domain: float = 0.0
+    # Vanka patches: [npatch, nodes per patch] node indices (DofHandler::
+    # GetElement(2, p)); None when the level has none
+    patches: Optional[np.ndarray] = None
 
     @property
     def nnzb(self) -> int:
@@ -125,17 +133,27 @@ def load_reference_dump(d: str) -> Problem:
     nl = int(summ["nlevels"][0])
     levels, transfers = [], []
     dim = None
+    B = int(summ.get("ncomp", ["1"])[0])
+    dmask = sum(1 << int(c) for c in summ.get("dircomps", ["0"]))
     for l in range(nl):
         p = os.path.join(d, f"L{l}_")
         rowptr = _i64(p + "rowptr.i64")
         n = rowptr.shape[0] - 1
         coord = np.fromfile(p + "coord.f64")
         dim = coord.shape[0] // n
-        levels.append(Level(n=n, B=1, rowptr=rowptr, col=_i64(p + "col.i64"),
-                            diag=_i64(p + "diag.i64"),
-                            val=np.fromfile(p + "val.f64"),
-                            dirichlet=_i64(p + "dirichlet.i64"),
-                            coord=coord.reshape(n, dim)))
+        lv = Level(n=n, B=B, rowptr=rowptr, col=_i64(p + "col.i64"),
+                   diag=_i64(p + "diag.i64"), val=np.fromfile(p + "val.f64"),
+                   dirichlet=_i64(p + "dirichlet.i64"), dircomp_mask=dmask,
+                   coord=coord.reshape(n, dim))
+        if os.path.exists(p + "pfw.f64") and f"pfdomain_L{l}" in summ:
+            lv.pf_mask = 1
+            lv.pf_weights = np.fromfile(p + "pfw.f64")
+            lv.pf_domain = float(summ[f"pfdomain_L{l}"][0])
+        if os.path.exists(p + "patches.i64"):
+            pt = _i64(p + "patches.i64")
+            npp = 3 ** dim
+            lv.patches = pt.reshape(-1, npp)
+        levels.append(lv)
     for l in range(nl - 1):
         p = os.path.join(d, f"T{l}_")
         transfers.append(Transfer(c2f=_i64(p + "c2f.i64"),

@@ -39,6 +39,16 @@ typedef struct
   int64_t ndir;           /* Dirichlet nodes */
   const int64_t* dir;     /* node indices */
   int dircomp_mask;       /* bit c set: component c is Dirichlet (all colours) */
+  /* pressure filter (PressureFilter, Discretization/Q1/pressurefilter.cc:56-100,
+   * weights from CGDisc::InitFilter, DofHandler/cgdisc.h:1061-1090) */
+  int pf_mask;            /* bit c set: component c is filtered; 0: inactive */
+  const double* pf_w;     /* n weights: integral of each basis function */
+  double pf_domain;       /* domain size */
+  int64_t nhanging;       /* hanging nodes (excluded from the algebraic mean) */
+  /* Vanka patches: DofHandler::GetElement(2, p) (DofHandler/dofhandler.h:389-396) */
+  int64_t npatch;
+  int npp;                /* nodes per patch */
+  const int64_t* patches; /* npatch * npp node indices */
 } or_level;
 
 /* Transfer level l (coarse) <-> l+1 (fine) in the form MgInterpolatorMatrix
@@ -66,6 +76,12 @@ typedef struct
   char mgtype;            /* 'V', 'W' or 'F' */
   /* work vectors per level: u, b, v of mgstep and the smoother's h */
   double **u, **b, **v;
+  /* linear_smooth: 0 jacobi, 1 ilu with matrixtype vanka (VankaSmoother) */
+  int smoother;
+  double** vlu;           /* per level: npatch LU factors, (npp*B)^2 each */
+  int** vperm;            /* per level: npatch row permutations, npp*B each */
+  double* vtmp;           /* finest-size scratch for the Vanka solve */
+  int* vcount;
 } or_mg;
 
 /* ---------------------------------------------------------------- vectors */
@@ -232,6 +248,149 @@ or_dirichlet_zero(const or_level* A, double* u)
         u[A->dir[k] * A->B + c] = 0.0;
 }
 
+/* PressureFilter::SubtractMean (Discretization/Q1/pressurefilter.cc:56-84)
+ * via StdSolver::SubtractMean (Solver/stdsolver.cc:1736-1747): per filtered
+ * component, mean = sum_j u(j,c) w_j (sequential), u(., c) -= mean / domain. */
+void
+or_subtract_mean(const or_level* A, double* u)
+{
+  const int B = A->B;
+  for (int c = 0; c < B; ++c) {
+    if (!(A->pf_mask & (1 << c)))
+      continue;
+    double mean = 0.0;
+    for (int64_t j = 0; j < A->n; ++j)
+      mean += u[j * B + c] * A->pf_w[j];
+    const double sub = mean / A->pf_domain;
+    for (int64_t j = 0; j < A->n; ++j)
+      u[j * B + c] += -sub;
+  }
+}
+
+/* PressureFilter::SubtractMeanAlgebraic (pressurefilter.cc:88-100) via
+ * StdSolver::SubtractMeanAlgebraic (Solver/stdsolver.cc:1752-1762). */
+void
+or_subtract_mean_algebraic(const or_level* A, double* u)
+{
+  const int B = A->B;
+  for (int c = 0; c < B; ++c) {
+    if (!(A->pf_mask & (1 << c)))
+      continue;
+    double d = 0.0;
+    for (int64_t j = 0; j < A->n; ++j)
+      d += u[j * B + c];
+    d /= (double)(A->n - A->nhanging);
+    for (int64_t j = 0; j < A->n; ++j)
+      u[j * B + c] += -d;
+  }
+}
+
+/* VankaSmoother::copy_entries_sparseblockmatrix (LinAlg/vankasmoother.cc:
+ * 65-113): the patch matrix (entries of the level matrix whose row and column
+ * nodes both lie in the patch, node-major with the components inside), then
+ * its LU factorisation with row partial pivoting (Eigen::PartialPivLU as the
+ * oracle's Eigen shim restates it: the first row of largest |a_ik| is the
+ * pivot; the column below the pivot is divided by it; the trailing block is
+ * updated entry by entry, k ascending). lu is row-major m x m, m = npp*B. */
+void
+or_vanka_factor(const or_level* A, int64_t p, double* lu, int* perm)
+{
+  const int B = A->B, npp = A->npp, m = npp * B;
+  const int64_t* pn = A->patches + p * npp;
+  memset(lu, 0, sizeof(double) * m * m);
+  for (int r = 0; r < npp; ++r) {
+    const int64_t row = pn[r];
+    for (int64_t pos = A->rowptr[row]; pos < A->rowptr[row + 1]; ++pos) {
+      int c = -1;
+      for (int q = 0; q < npp; ++q)
+        if (pn[q] == A->col[pos]) {
+          c = q;
+          break;
+        }
+      if (c < 0)
+        continue;
+      const double* blk = A->val + pos * B * B;
+      for (int cr = 0; cr < B; ++cr)
+        for (int cc = 0; cc < B; ++cc)
+          lu[(B * r + cr) * m + B * c + cc] = blk[cr * B + cc];
+    }
+  }
+  for (int i = 0; i < m; ++i)
+    perm[i] = i;
+  for (int k = 0; k < m; ++k) {
+    int piv = k;
+    double best = fabs(lu[k * m + k]);
+    for (int i = k + 1; i < m; ++i)
+      if (fabs(lu[i * m + k]) > best) {
+        best = fabs(lu[i * m + k]);
+        piv = i;
+      }
+    if (piv != k) {
+      for (int j = 0; j < m; ++j) {
+        double t = lu[k * m + j];
+        lu[k * m + j] = lu[piv * m + j];
+        lu[piv * m + j] = t;
+      }
+      int t = perm[k];
+      perm[k] = perm[piv];
+      perm[piv] = t;
+    }
+    if (lu[k * m + k] != 0)
+      for (int i = k + 1; i < m; ++i)
+        lu[i * m + k] /= lu[k * m + k];
+    for (int j = k + 1; j < m; ++j)
+      for (int i = k + 1; i < m; ++i)
+        lu[i * m + j] -= lu[i * m + k] * lu[k * m + j];
+  }
+}
+
+/* VankaSmoother::solve (LinAlg/vankasmoother.cc:192-237) with one thread:
+ * x = average over the patches containing each node of the patch solutions
+ * of the local systems with right-hand side x (the residual); contributions
+ * are summed in patch order. tmp: ndof scratch, count: n scratch. */
+void
+or_vanka_solve(const or_level* A, const double* lu, const int* perm, double* x,
+               double* tmp, int* count)
+{
+  const int B = A->B, npp = A->npp, m = npp * B;
+  double H[8 * 27], G[8 * 27];
+  memcpy(tmp, x, sizeof(double) * A->n * B);
+  memset(x, 0, sizeof(double) * A->n * B);
+  memset(count, 0, sizeof(int) * A->n);
+  for (int64_t p = 0; p < A->npatch; ++p) {
+    const int64_t* pn = A->patches + p * npp;
+    const double* L = lu + p * m * m;
+    const int* P = perm + p * m;
+    for (int r = 0; r < npp; ++r)
+      for (int c = 0; c < B; ++c)
+        G[B * r + c] = tmp[pn[r] * B + c];
+    for (int i = 0; i < m; ++i)
+      H[i] = G[P[i]];
+    for (int i = 0; i < m; ++i) { /* unit lower */
+      double s = H[i];
+      for (int j = 0; j < i; ++j)
+        s -= L[i * m + j] * H[j];
+      H[i] = s;
+    }
+    for (int i = m - 1; i >= 0; --i) { /* upper */
+      double s = H[i];
+      for (int j = i + 1; j < m; ++j)
+        s -= L[i * m + j] * H[j];
+      H[i] = s / L[i * m + i];
+    }
+    for (int r = 0; r < npp; ++r) {
+      count[pn[r]]++;
+      for (int c = 0; c < B; ++c)
+        x[pn[r] * B + c] += H[B * r + c];
+    }
+  }
+  for (int64_t i = 0; i < A->n; ++i) {
+    const double s = 1.0 / count[i];
+    for (int c = 0; c < B; ++c)
+      x[i * B + c] *= s;
+  }
+}
+
 /* ---------------------------------------------------------- transfers */
 
 static int
@@ -380,7 +539,7 @@ ndof(const or_mg* M, int l)
 or_mg*
 or_mg_create(int nlevels, or_level* L, or_transfer* T, int iterpre,
              int iterpost, int iterexact, double omega, double mgomega,
-             char mgtype)
+             char mgtype, int smoother)
 {
   or_mg* M = (or_mg*)calloc(1, sizeof(or_mg));
   M->nlevels = nlevels;
@@ -400,6 +559,27 @@ or_mg_create(int nlevels, or_level* L, or_transfer* T, int iterpre,
     M->b[l] = (double*)calloc(ndof(M, l), sizeof(double));
     M->v[l] = (double*)calloc(ndof(M, l), sizeof(double));
   }
+  M->smoother = smoother;
+  if (smoother == 1) {
+    /* VankaSmoother::ConstructStructure + copy_entries (ComputeIlu,
+     * Solver/stdsolver.cc:1547-1573) on every level */
+    M->vlu = (double**)calloc(nlevels, sizeof(double*));
+    M->vperm = (int**)calloc(nlevels, sizeof(int*));
+    int64_t nmax = 0;
+    for (int l = 0; l < nlevels; ++l) {
+      const or_level* A = &L[l];
+      const int64_t m = (int64_t)A->npp * A->B;
+      if (A->npatch <= 0 || m > 8 * 27)
+        return NULL;
+      M->vlu[l] = (double*)malloc(sizeof(double) * A->npatch * m * m);
+      M->vperm[l] = (int*)malloc(sizeof(int) * A->npatch * m);
+      for (int64_t p = 0; p < A->npatch; ++p)
+        or_vanka_factor(A, p, M->vlu[l] + p * m * m, M->vperm[l] + p * m);
+      nmax = ndof(M, l) > nmax ? ndof(M, l) : nmax;
+    }
+    M->vtmp = (double*)malloc(sizeof(double) * nmax);
+    M->vcount = (int*)malloc(sizeof(int) * nmax);
+  }
   return M;
 }
 
@@ -414,20 +594,33 @@ or_mg_free(or_mg* M)
   free(M->u);
   free(M->b);
   free(M->v);
+  if (M->vlu) {
+    for (int l = 0; l < M->nlevels; ++l) {
+      free(M->vlu[l]);
+      free(M->vperm[l]);
+    }
+    free(M->vlu);
+    free(M->vperm);
+    free(M->vtmp);
+    free(M->vcount);
+  }
   free(M);
 }
 
-/* StdSolver::MatrixResidual (Solver/stdsolver.cc:783-791): y = b - A x */
+/* StdSolver::MatrixResidual (Solver/stdsolver.cc:783-791): y = b - A x,
+ * then SubtractMeanAlgebraic (a no-op without a pressure filter) */
 void
 or_matrix_residual(const or_level* A, double* y, const double* x,
                    const double* b)
 {
   memcpy(y, b, sizeof(double) * A->n * A->B);
   or_bsr_vmult(A, y, x, -1.0);
+  or_subtract_mean_algebraic(A, y);
 }
 
-/* StdSolver::smooth with linear_smooth = jacobi (Solver/stdsolver.cc:951-986):
- * h = y - A x; h = D^-1 h; x += omega h. No pressure filter. */
+/* StdSolver::smooth (Solver/stdsolver.cc:951-986): h = y - A x (filtered);
+ * h = D^-1 h (jacobi) or the Vanka solve (ilu with matrixtype vanka);
+ * x += omega h; SubtractMean(x). */
 void
 or_smooth(const or_mg* M, int l, int niter, double* x, const double* y,
           double* h)
@@ -436,9 +629,13 @@ or_smooth(const or_mg* M, int l, int niter, double* x, const double* y,
   const int64_t n = ndof(M, l);
   for (int it = 0; it < niter; ++it) {
     or_matrix_residual(A, h, x, y);
-    or_jacobi(A, h);
+    if (M->smoother == 1)
+      or_vanka_solve(A, M->vlu[l], M->vperm[l], h, M->vtmp, M->vcount);
+    else
+      or_jacobi(A, h);
     for (int64_t i = 0; i < n; ++i)
       x[i] += M->omega * h[i];
+    or_subtract_mean(A, x);
   }
 }
 
@@ -655,6 +852,7 @@ or_gmres_solve(or_mg* M, const double* b, double* x, int vmax, double tol,
     free(hs);
   }
 done:
+  or_subtract_mean(A, x); /* NewtonLinearSolve, Solver/stdmultilevelsolver.cc:671 */
   if (out_iters)
     *out_iters = info.iteration;
   if (out_status)

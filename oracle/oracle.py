@@ -26,7 +26,9 @@ _PD = C.POINTER(C.c_double)
 class _Level(C.Structure):
     _fields_ = [("n", C.c_int64), ("B", C.c_int), ("rowptr", _P64), ("col", _P64),
                 ("diag", _P64), ("val", _PD), ("ndir", C.c_int64), ("dir", _P64),
-                ("dircomp_mask", C.c_int)]
+                ("dircomp_mask", C.c_int), ("pf_mask", C.c_int), ("pf_w", _PD),
+                ("pf_domain", C.c_double), ("nhanging", C.c_int64),
+                ("npatch", C.c_int64), ("npp", C.c_int), ("patches", _P64)]
 
 
 class _Transfer(C.Structure):
@@ -48,7 +50,7 @@ def lib():
         L.or_mg_create.restype = C.c_void_p
         L.or_mg_create.argtypes = [C.c_int, C.POINTER(_Level), C.POINTER(_Transfer),
                                    C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                   C.c_char]
+                                   C.c_char, C.c_int]
         L.or_mg_free.argtypes = [C.c_void_p]
         L.or_transfer_build.argtypes = [C.POINTER(_Transfer), C.c_int64, _P64,
                                         C.c_int64, _P64, C.c_int64, _P64, C.c_int64,
@@ -67,6 +69,12 @@ def lib():
         L.or_prolongate_add.argtypes = [C.POINTER(_Transfer), C.c_int, _PD, _PD]
         L.or_dirichlet_zero.argtypes = [C.POINTER(_Level), _PD]
         L.or_matrix_residual.argtypes = [C.POINTER(_Level), _PD, _PD, _PD]
+        L.or_subtract_mean.argtypes = [C.POINTER(_Level), _PD]
+        L.or_subtract_mean_algebraic.argtypes = [C.POINTER(_Level), _PD]
+        L.or_vanka_factor.argtypes = [C.POINTER(_Level), C.c_int64, _PD,
+                                      C.POINTER(C.c_int)]
+        L.or_vanka_solve.argtypes = [C.POINTER(_Level), _PD, C.POINTER(C.c_int), _PD,
+                                     _PD, C.POINTER(C.c_int)]
         L.or_dot.restype = C.c_double
         L.or_dot.argtypes = [C.c_int64, _PD, _PD]
         _lib = L
@@ -85,7 +93,7 @@ class Oracle:
     """FP64 CPU restatement of the reference's multilevel GMRES on a Problem."""
 
     def __init__(self, prob, iterpre=2, iterpost=2, iterexact=10, omega=0.8,
-                 mgomega=1.0, mgtype="V"):
+                 mgomega=1.0, mgtype="V", smoother=None):
         L = lib()
         self.prob = prob
         self._keep = []
@@ -96,8 +104,17 @@ class Oracle:
                     (lv.rowptr, lv.col, lv.diag, lv.val, lv.dirichlet)]
             self._keep += arrs
             rp, cl, dg, vl, dr = arrs
-            self.levels[l] = _Level(lv.n, lv.B, _p64(rp), _p64(cl), _p64(dg), _pd(vl),
-                                    dr.shape[0], _p64(dr), lv.dircomp_mask)
+            lev = _Level(lv.n, lv.B, _p64(rp), _p64(cl), _p64(dg), _pd(vl),
+                         dr.shape[0], _p64(dr), lv.dircomp_mask)
+            if lv.pf_mask:
+                w = np.ascontiguousarray(lv.pf_weights, dtype=np.float64)
+                self._keep.append(w)
+                lev.pf_mask, lev.pf_w, lev.pf_domain = lv.pf_mask, _pd(w), lv.pf_domain
+            if lv.patches is not None:
+                pt = np.ascontiguousarray(lv.patches, dtype=np.int64)
+                self._keep.append(pt)
+                lev.npatch, lev.npp, lev.patches = pt.shape[0], pt.shape[1], _p64(pt)
+            self.levels[l] = lev
         self.transfers = (_Transfer * max(nl - 1, 1))()
         for l, t in enumerate(prob.transfers):
             arrs = [np.ascontiguousarray(a, dtype=np.int64) for a in
@@ -109,8 +126,14 @@ class Oracle:
                                      _p64(v), a.shape[0], _p64(a))
             if rc != 0:
                 raise MemoryError("or_transfer_build")
+        if smoother is None:
+            smoother = prob.info.get("smoother", "jacobi")
+        self.smoother = smoother
         self.mg = L.or_mg_create(nl, self.levels, self.transfers, iterpre, iterpost,
-                                 iterexact, omega, mgomega, mgtype.encode()[:1])
+                                 iterexact, omega, mgomega, mgtype.encode()[:1],
+                                 1 if smoother == "vanka" else 0)
+        if not self.mg:
+            raise ValueError("or_mg_create failed (Vanka needs patches on every level)")
 
     def close(self):
         if getattr(self, "mg", None):
@@ -200,14 +223,17 @@ class Oracle:
                    "history": hist[:max(it.value, 0)]}
 
 
-def run_reference(out_dir=None, **kw):
-    """Runs the compiled reference harness; returns (out_dir, summary dict)."""
+def run_reference(out_dir=None, threads=None, **kw):
+    """Runs the compiled reference harness; returns (out_dir, summary dict).
+    threads: OpenMP threads (1 makes Vanka's patch sums ordered)."""
     if not os.path.exists(REF_HARNESS):
         raise FileNotFoundError(REF_HARNESS)
     if out_dir is None:
         out_dir = tempfile.mkdtemp(prefix="gb_ref_")
     args = [REF_HARNESS, f"out={out_dir}"] + [f"{k}={v}" for k, v in kw.items()]
     env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
     subprocess.run(args, check=True, capture_output=True, env=env)
     summ = {}
     with open(os.path.join(out_dir, "summary.txt")) as f:

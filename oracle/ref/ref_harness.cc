@@ -19,6 +19,15 @@
 // (lexicographic node order) and copied into the finest-level vector f, then
 // zeroed at Dirichlet nodes (StdSolver::SetBoundaryVectorZero).
 //
+// With problem=stokes the equation is instead the Stokes system in the
+// reference's NavierStokes component order (0 = p, 1..dim = velocity):
+// -visc Laplace v + grad p = f, div v + stab h^2 (-Laplace p) = g (equal-order
+// Q1/Q1 with Brezzi-Pitkaranta pressure stabilisation, h the cell width),
+// velocity Dirichlet on the whole boundary, the pressure filter on component 0
+// (pfilter=1), and the smoother smoother=vanka (matrixtype vanka, linear_smooth
+// ilu: VankaSmoother, LinAlg/vankasmoother.cc) or smoother=jacobi (block
+// Jacobi). The right-hand side file then holds ncomp values per node.
+//
 // Usage: ref_harness key=value ...   (see parse() for the keys)
 // Output (directory out=): summary.txt, and with dump=1 raw little-endian arrays
 //   L<l>_rowptr.i64 L<l>_col.i64 L<l>_diag.i64 L<l>_val.f64 L<l>_coord.f64
@@ -27,6 +36,10 @@
 //     (transfer between level l (coarse) and l+1 (fine); zweier rows are
 //      [fine, coarse0, coarse1], vierer [fine, 4 coarse], achter [fine, 8 coarse])
 //   rhs.f64 solution.f64 (finest level, reference node numbering)
+//   L<l>_val.f64 holds nnzb*ncomp^2 values (row-major blocks); for
+//   problem=stokes also L<l>_pfw.f64 (pressure-filter weights) and
+//   L<l>_patches.i64 (Vanka patches, npatches x nodes_per_patch), with
+//   pfdomain_L<l>, ncomp and dircomps in summary.txt
 // and with dualrhs= (a nodal vector like rhs): dual_summary.txt,
 //   dual_rhs.f64 dual_solution.f64, and with dump=1 L<l>_dualval.f64 (the
 //   dual matrices' values in the stencil of L<l>_col.i64)
@@ -53,6 +66,7 @@
 #include "sparseblockmatrix.h"
 #include "stdmultilevelsolver.h"
 #include "stdsolver.h"
+#include "pressurefilter.h"
 #include "zerodirichletdata.h"
 
 using namespace Gascoigne;
@@ -70,6 +84,9 @@ struct Config
   int maxiter = 100, ndirect = 1, dump = 0, repeat = 1, patchdepth = 1;
   std::string mgtype = "V";
   double conv[3] = { 0.0, 0.0, 0.0 };
+  std::string problem = "diffusion", smoother = "jacobi";
+  double visc = 1.0, stab = 0.1;
+  int pfilter = 1;
 };
 
 // kappa per cell, one array per resolution N = coarse * 2^l (cells per dim),
@@ -144,6 +161,77 @@ public:
   }
 };
 
+// Stokes, components (p, v_1, .., v_dim) as Problems/navierstokes.h:144-168
+// orders them (M trial, N test function).
+class StokesEquation : public virtual Equation
+{
+  int dim_;
+  double visc_, stab_;
+  mutable double h_ = 1.0;
+
+public:
+  StokesEquation(int dim, double visc, double stab)
+    : dim_(dim)
+    , visc_(visc)
+    , stab_(stab)
+  {}
+  StokesEquation* createNew() const override
+  {
+    return new StokesEquation(dim_, visc_, stab_);
+  }
+  std::string GetName() const override { return "OracleStokes"; }
+  int GetNcomp() const override { return dim_ + 1; }
+  void point(double h, const FemFunction&, const Vertex2d&) const override { h_ = h; }
+  void point(double h, const FemFunction&, const Vertex3d&) const override { h_ = h; }
+  void Form(VectorIterator b, const FemFunction& U, const TestFunction& N) const override
+  {
+    for (int i = 0; i < dim_; ++i) {
+      b[0] += U[i + 1][i + 1] * N.m() + stab_ * h_ * h_ * U[0][i + 1] * N[i + 1];
+      for (int j = 0; j < dim_; ++j)
+        b[i + 1] += visc_ * U[i + 1][j + 1] * N[j + 1];
+      b[i + 1] -= U[0].m() * N[i + 1];
+    }
+  }
+  void Matrix(EntryMatrix& A, const FemFunction&, const TestFunction& M,
+              const TestFunction& N) const override
+  {
+    for (int i = 0; i < dim_; ++i) {
+      A(0, i + 1) += M[i + 1] * N.m();
+      A(0, 0) += stab_ * h_ * h_ * M[i + 1] * N[i + 1];
+      for (int j = 0; j < dim_; ++j)
+        A(i + 1, i + 1) += visc_ * M[j + 1] * N[j + 1];
+      A(i + 1, 0) -= M.m() * N[i + 1];
+    }
+  }
+};
+
+class StokesProblem : public ProblemDescriptorBase
+{
+public:
+  void BasicInit(const ParamFile& pf, int dim, double visc, double stab)
+  {
+    GetParamFile() = pf;
+    GetEquationPointer() = new StokesEquation(dim, visc, stab);
+    GetDirichletDataPointer() = new ZeroDirichletData(pf);
+    ProblemDescriptorBase::BasicInit(pf);
+  }
+};
+
+// the pressure filter's domain size is not exposed by PressureFilter, and
+// StdSolver::GetPfilter is protected: read both through derived-class access
+struct PressureFilterView : public PressureFilter
+{
+  double domain() const { return domainsize; }
+};
+struct SolverView : public StdSolver
+{
+  static const PressureFilter& pfilter(const StdSolver* s)
+  {
+    const PressureFilter& (StdSolver::*get)() const = &SolverView::GetPfilter;
+    return (s->*get)();
+  }
+};
+
 class DiffusionProblem : public ProblemDescriptorBase
 {
 public:
@@ -189,6 +277,11 @@ parse(int argc, char** argv)
     else if (k == "dump") c.dump = atoi(v.c_str());
     else if (k == "repeat") c.repeat = atoi(v.c_str());
     else if (k == "patchdepth") c.patchdepth = atoi(v.c_str());
+    else if (k == "problem") c.problem = v;
+    else if (k == "smoother") c.smoother = v;
+    else if (k == "visc") c.visc = atof(v.c_str());
+    else if (k == "stab") c.stab = atof(v.c_str());
+    else if (k == "pfilter") c.pfilter = atoi(v.c_str());
     else if (k == "conv") {
       std::stringstream ss(v);
       std::string t;
@@ -305,8 +398,16 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "patchdepth " << c.patchdepth << "\n"
     << "gridname " << grid << "\n\n"
     << "//Block BoundaryManager\n"
-    << "dirichlet 1 1\n"
-    << "dirichletcomp 1 1 0\n\n"
+    << "dirichlet 1 1\n";
+  if (c.problem == "stokes") {
+    o << "dirichletcomp 1 " << c.dim;
+    for (int d = 1; d <= c.dim; ++d)
+      o << " " << d;
+    o << "\n\n";
+  } else {
+    o << "dirichletcomp 1 1 0\n\n";
+  }
+  o
     << "//Block MultiLevelSolver\n"
     << "linearsolve gmres\n"
     << "gmressize " << c.gmressize << "\n"
@@ -314,14 +415,16 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "mgomega " << c.mgomega << "\n"
     << "coarselevel 0\n\n"
     << "//Block Solver\n"
-    << "matrixtype block\n"
+    << "matrixtype " << (c.smoother == "vanka" ? "vanka" : "block") << "\n"
     << "discname CGQ1\n"
     << "ndirect " << c.ndirect << "\n"
     << "iterpre " << c.iterpre << "\n"
     << "iterpost " << c.iterpost << "\n"
     << "iterexact " << c.iterexact << "\n"
-    << "linear_smooth jacobi\n"
+    << "linear_smooth " << (c.smoother == "vanka" ? "ilu" : "jacobi") << "\n"
     << "omega " << c.omega << "\n";
+  if (c.problem == "stokes" && c.pfilter)
+    o << "pfilter 1 0\n";
 }
 
 void
@@ -359,6 +462,26 @@ build_kappa(const Config& c)
   }
 }
 
+// Values of a SparseBlockMatrix<FMatrixBlock<NCOMP>> in stencil order,
+// row-major blocks (NodeMatrix::value, LinAlg/nodematrix.h:44-48).
+template<int NCOMP>
+bool
+block_values(const MatrixInterface& MI, std::vector<double>& val,
+             const StencilInterface*& st)
+{
+  const auto* M = dynamic_cast<const SparseBlockMatrix<FMatrixBlock<NCOMP>>*>(&MI);
+  if (!M)
+    return false;
+  const auto* ST = dynamic_cast<const ColumnDiagStencil*>(M->GetStencil());
+  st = ST;
+  val.resize(ST->nentries() * NCOMP * NCOMP);
+  for (size_t p = 0; p < ST->nentries(); ++p)
+    for (int r = 0; r < NCOMP; ++r)
+      for (int q = 0; q < NCOMP; ++q)
+        val[(p * NCOMP + r) * NCOMP + q] = (*M->mat(p))(r, q);
+  return true;
+}
+
 } // namespace
 
 int
@@ -373,9 +496,16 @@ main(int argc, char** argv)
 
   ParamFile pf(pfile);
   DiffusionProblem PD;
-  PD.BasicInit(pf, c.dim, c.conv);
+  StokesProblem PS;
+  const bool stokes = c.problem == "stokes";
+  if (stokes)
+    PS.BasicInit(pf, c.dim, c.visc, c.stab);
+  else
+    PD.BasicInit(pf, c.dim, c.conv);
+  const int ncomp = stokes ? c.dim + 1 : 1;
   ProblemContainer PC;
-  PC.AddProblem("diffusion", &PD);
+  PC.AddProblem("diffusion", stokes ? static_cast<ProblemDescriptorInterface*>(&PS)
+                                    : static_cast<ProblemDescriptorInterface*>(&PD));
   FunctionalContainer FC;
 
   MeshAgent MA;
@@ -406,8 +536,8 @@ main(int argc, char** argv)
     size_t nlex = 1;
     for (int d = 0; d < c.dim; ++d)
       nlex *= Nf + 1;
-    std::vector<double> r = c.rhs.empty() ? std::vector<double>(nlex, 1.0)
-                                          : read_f64(c.rhs, nlex);
+    std::vector<double> r = c.rhs.empty() ? std::vector<double>(nlex * ncomp, 1.0)
+                                          : read_f64(c.rhs, nlex * ncomp);
     for (int i = 0; i < nf; ++i) {
       long ix, iy, iz = 0;
       if (c.dim == 3) {
@@ -420,7 +550,8 @@ main(int argc, char** argv)
         ix = std::lround(v.x() * Nf);
         iy = std::lround(v.y() * Nf);
       }
-      F(i, 0) = r[(iz * (Nf + 1) + iy) * (Nf + 1) + ix];
+      for (int cc = 0; cc < ncomp; ++cc)
+        F(i, cc) = r[((iz * (Nf + 1) + iy) * (Nf + 1) + ix) * ncomp + cc];
     }
   }
   S->SetBoundaryVectorZero(f);
@@ -454,6 +585,20 @@ main(int argc, char** argv)
     o << "firstresidual " << info.control().firstresidual() << "\n";
     o << "residual " << info.control().residual() << "\n";
     o << "true_rel_residual " << rnorm / fnorm << "\n";
+    o << "ncomp " << ncomp << "\n";
+    o << "dircomps";
+    if (stokes)
+      for (int d = 1; d <= c.dim; ++d)
+        o << " " << d;
+    else
+      o << " 0";
+    o << "\n";
+    if (stokes)
+      for (int l = 0; l < nl; ++l)
+        o << "pfdomain_L" << l << " "
+          << static_cast<const PressureFilterView&>(SolverView::pfilter(MLS.GetSolver(l)))
+               .domain()
+          << "\n";
     o << "assemble_s "
       << std::chrono::duration<double>(t_as1 - t_as0).count() << "\n";
     o << "solve_s";
@@ -465,22 +610,21 @@ main(int argc, char** argv)
   if (c.dump) {
     for (int l = 0; l < nl; ++l) {
       StdSolver* SL = MLS.GetSolver(l);
-      const auto* M =
-        dynamic_cast<const SparseBlockMatrix<FMatrixBlock<1>>*>(&SL->GetMatrix(A));
-      if (!M) {
+      const MatrixInterface& MI = SL->GetMatrix(A);
+      const StencilInterface* STI = nullptr;
+      std::vector<double> val;
+      if (!block_values<1>(MI, val, STI) && !block_values<2>(MI, val, STI) &&
+          !block_values<3>(MI, val, STI) && !block_values<4>(MI, val, STI)) {
         fprintf(stderr, "ref_harness: level %d is not a block matrix\n", l);
         return 3;
       }
-      const auto* ST = dynamic_cast<const ColumnDiagStencil*>(M->GetStencil());
+      const auto* ST = dynamic_cast<const ColumnDiagStencil*>(STI);
       const int n = ST->n();
       std::vector<long> rowptr(n + 1), col(ST->nentries()), diag(n);
-      std::vector<double> val(ST->nentries());
       for (int i = 0; i <= n; ++i)
         rowptr[i] = ST->start(i);
-      for (size_t p = 0; p < ST->nentries(); ++p) {
+      for (size_t p = 0; p < ST->nentries(); ++p)
         col[p] = ST->col(p);
-        val[p] = (*M->mat(p))(0, 0);
-      }
       for (int i = 0; i < n; ++i)
         diag[i] = ST->diag(i);
       std::string L = c.out + "/L" + std::to_string(l) + "_";
@@ -509,6 +653,16 @@ main(int argc, char** argv)
         for (int i : *bv)
           dn.push_back(i);
       write_raw(L + "dirichlet.i64", dn);
+      if (stokes) {
+        const PressureFilter& PF = SolverView::pfilter(SL);
+        std::vector<double> w(PF.begin(), PF.end());
+        write_raw(L + "pfw.f64", w);
+        std::vector<long> pl;
+        for (int p = 0; p < ML->npatches(); ++p)
+          for (int i : *ML->IndicesOfPatch(p))
+            pl.push_back(i);
+        write_raw(L + "patches.i64", pl);
+      }
     }
     for (int l = 0; l + 1 < nl; ++l) {
       // interpolator l maps level l+1 (fine) to level l (coarse); it is built

@@ -18,23 +18,32 @@ def load_golden(name):
     """Returns (Problem in the reference's numbering, reference results dict)."""
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     nl = int(z["nlevels"])
+    B = int(z["B"]) if "B" in z.files else 1
+    dmask = int(z["dircomp_mask"]) if "dircomp_mask" in z.files else 1
     levels, transfers = [], []
     for l in range(nl):
         rp = z[f"L{l}_rowptr"].astype(np.int64)
-        levels.append(Level(n=rp.shape[0] - 1, B=1, rowptr=rp,
-                            col=z[f"L{l}_col"].astype(np.int64),
-                            diag=z[f"L{l}_diag"].astype(np.int64),
-                            val=z[f"L{l}_val"],
-                            dirichlet=z[f"L{l}_dirichlet"].astype(np.int64),
-                            coord=z[f"L{l}_coord"]))
+        lv = Level(n=rp.shape[0] - 1, B=B, rowptr=rp,
+                   col=z[f"L{l}_col"].astype(np.int64),
+                   diag=z[f"L{l}_diag"].astype(np.int64),
+                   val=z[f"L{l}_val"],
+                   dirichlet=z[f"L{l}_dirichlet"].astype(np.int64),
+                   dircomp_mask=dmask, coord=z[f"L{l}_coord"])
+        if f"L{l}_pfw" in z.files:
+            lv.pf_mask = 1
+            lv.pf_weights = z[f"L{l}_pfw"]
+            lv.pf_domain = float(z[f"L{l}_pfdomain"])
+        if f"L{l}_patches" in z.files:
+            lv.patches = z[f"L{l}_patches"].astype(np.int64)
+        levels.append(lv)
     for l in range(nl - 1):
         transfers.append(Transfer(c2f=z[f"T{l}_c2f"].astype(np.int64),
                                   zweier=z[f"T{l}_zweier"].astype(np.int64),
                                   vierer=z[f"T{l}_vierer"].astype(np.int64),
                                   achter=z[f"T{l}_achter"].astype(np.int64)))
-    P = Problem(dim=int(z["dim"]), levels=levels, transfers=transfers,
-                rhs=z["rhs"].copy())
     keys = {k[4:]: z[k].item() for k in z.files if k.startswith("key_")}
+    P = Problem(dim=int(z["dim"]), levels=levels, transfers=transfers,
+                rhs=z["rhs"].copy(), info={"smoother": keys.get("smoother", "jacobi")})
     ref = {"solution": z["solution"], "iterations": int(z["iterations"]),
            "firstresidual": float(z["firstresidual"]), "residual": float(z["residual"]),
            "status": str(z["status"]), "keys": keys}
@@ -46,6 +55,10 @@ def load_golden(name):
                    dual_status=str(z["dual_status"]),
                    dualval=[z[f"L{l}_dualval"] for l in range(nl)])
     return P, ref
+
+
+def golden_stokes_cases():
+    return [n for n in golden_cases() if n.startswith("stokes_")]
 
 
 def golden_dual_cases():

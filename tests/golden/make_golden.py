@@ -8,6 +8,10 @@ nonsymmetric operator) and the reference's dual solve
 (StdMultiLevelSolver::AssembleDualMatrix + the same Gmres): the dual matrices'
 values, the dual right-hand side dJ/du = 2 M u of J(u) = integral of u^2 (M the
 Q1 mass matrix, u the forward solution of a first run) and the dual solution.
+The "stokes_" cases are the Q1/Q1 Stokes system (ncomp = dim+1, block
+matrices) with the pressure filter and the Vanka or block-Jacobi smoother; the
+harness runs them on one OpenMP thread, so Vanka's patch contributions are
+summed in patch order.
 
     python tests/golden/make_golden.py
 """
@@ -34,7 +38,26 @@ CASES = {
     "q1_2d_c2_r3_fcycle": (2, 2, 3, True, 1e-10, {"mgtype": "F", "mgomega": 0.9}),
     "q1_3d_c1_r3_conv_dual": (3, 1, 3, True, 1e-8, {"conv": "1,0.5,0.25"}),
     "q1_2d_c2_r4_conv_dual": (2, 2, 4, True, 1e-10, {"conv": "4,2"}),
+    "stokes_2d_c2_r4_vanka": (2, 2, 4, True, 1e-8,
+                              {"problem": "stokes", "smoother": "vanka", "omega": 1.0,
+                               "gmressize": 31}),
+    "stokes_2d_c2_r3_jacobi": (2, 2, 3, True, 1e-8,
+                               {"problem": "stokes", "smoother": "jacobi", "omega": 0.5,
+                                "gmressize": 31}),
+    "stokes_3d_c1_r3_vanka": (3, 1, 3, True, 1e-8,
+                              {"problem": "stokes", "smoother": "vanka", "omega": 1.0,
+                               "gmressize": 31}),
 }
+
+
+def stokes_rhs(dim, coarse, refine, seed=1002):
+    """f ~ U[-1, 1] per node and component (p, v_1..v_dim), the pressure part
+    made algebraically mean-free so that the system with its constant-pressure
+    null space is consistent."""
+    n1 = (coarse << refine) + 1
+    r = np.random.default_rng(seed).uniform(-1.0, 1.0, size=(n1 ** dim, dim + 1))
+    r[:, 0] -= r[:, 0].mean()
+    return r.ravel()
 
 
 def lex_permutation(coord, N):
@@ -68,7 +91,10 @@ def l2_dual_rhs(P, u_ref):
 def make(name, dim, coarse, refine, seeded, tol, extra):
     d = tempfile.mkdtemp(prefix="gb_golden_")
     kw = {}
-    if seeded:
+    stokes = extra.get("problem") == "stokes"
+    if stokes:
+        kw = write_inputs(d, None, stokes_rhs(dim, coarse, refine))
+    elif seeded:
         kappa, rhs = seeded_inputs(dim, coarse, refine)
         kw = write_inputs(d, kappa, rhs)
     keys = dict(dim=dim, coarse=coarse, refine=refine, dump=1, tol=tol,
@@ -82,7 +108,7 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
         gp = os.path.join(d, "dual_in.f64")
         g.tofile(gp)
         kw["dualrhs"] = gp
-    out, summ = run_reference(d, **keys, **kw)
+    out, summ = run_reference(d, threads=1, **keys, **kw)
     P = load_reference_dump(out)
     arrs = {"dim": P.dim, "nlevels": P.nlevels, "rhs": P.rhs,
             "solution": np.fromfile(os.path.join(out, "solution.f64")),
@@ -107,7 +133,14 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
         arrs["dual_status"] = " ".join(ds["dual_status"])
         for l in range(P.nlevels):
             arrs[f"L{l}_dualval"] = np.fromfile(os.path.join(out, f"L{l}_dualval.f64"))
+    arrs["B"] = P.finest.B
+    arrs["dircomp_mask"] = P.finest.dircomp_mask
     for l, lv in enumerate(P.levels):
+        if lv.pf_mask:
+            arrs[f"L{l}_pfw"] = lv.pf_weights
+            arrs[f"L{l}_pfdomain"] = lv.pf_domain
+        if lv.patches is not None:
+            arrs[f"L{l}_patches"] = lv.patches.astype(np.int32)
         arrs[f"L{l}_rowptr"] = lv.rowptr.astype(np.int32)
         arrs[f"L{l}_col"] = lv.col.astype(np.int32)
         arrs[f"L{l}_diag"] = lv.diag.astype(np.int32)

@@ -43,6 +43,27 @@ def test_oracle_matches_reference_live(dim, coarse, refine):
     assert np.array_equal(x, np.fromfile(os.path.join(out, "solution.f64")))
 
 
+@pytest.mark.skipif(not HAVE_REF, reason="compiled reference not present")
+@pytest.mark.parametrize("dim,smoother,omega", [(2, "vanka", 1.0), (2, "jacobi", 0.5),
+                                                (3, "jacobi", 0.5)])
+def test_oracle_matches_reference_live_stokes(dim, smoother, omega):
+    """Block systems (ncomp = dim+1), pressure filter, Vanka / block Jacobi."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import stokes_rhs
+    coarse, refine = (2, 3) if dim == 2 else (1, 3)
+    d = tempfile.mkdtemp()
+    out, summ = run_reference(d, threads=1, dim=dim, coarse=coarse, refine=refine,
+                              dump=1, tol=1e-9, problem="stokes", smoother=smoother,
+                              omega=omega, gmressize=31, maxiter=200,
+                              **write_inputs(d, None, stokes_rhs(dim, coarse, refine, 9)))
+    P = load_reference_dump(out)
+    P.info["smoother"] = smoother
+    x, info = Oracle(P, omega=omega).gmres(vmax=31, tol=1e-9, maxiter=200)
+    assert info["iterations"] == int(summ["iterations"][0])
+    assert np.array_equal(x, np.fromfile(os.path.join(out, "solution.f64")))
+
+
 def _lex_permutation(level, N, dim):
     idx = np.rint(level.coord * N).astype(np.int64)
     lex = np.zeros(level.n, np.int64)
