@@ -206,12 +206,11 @@ __device__ __forceinline__ T wcode(uint32_t e)
 template<class T>
 __device__ __forceinline__ T
 transfer_row(const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
-             const T* __restrict__ src, int i)
+             const T* __restrict__ src, int i, T acc = T(0))
 {
   const int beg = __ldg(tsp + (i >> 5));
   const int w = (__ldg(tsp + (i >> 5) + 1) - beg) >> 5;
   const uint32_t* ep = tent + beg + (i & 31);
-  T acc = T(0);
   for (int j0 = 0; j0 < w; j0 += 8) {
     const uint32_t* pe[8];
 #pragma unroll
@@ -262,10 +261,12 @@ k_prolong(int nf, const int* __restrict__ tsp, const uint32_t* __restrict__ tent
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf)
     return;
+  if (MODE == 0) { // in place, entry by entry (powers-of-two weights)
+    fine[i] = transfer_row<T>(tsp, tent, coarse, i, fine[i]);
+    return;
+  }
   T acc = transfer_row<T>(tsp, tent, coarse, i);
-  if (MODE == 0) {
-    fine[i] = fine[i] + acc;
-  } else {
+  {
     if (fdir && fdir[i])
       acc = T(0);
     fine[i] = fine[i] + static_cast<T>(mgomega) * acc;
@@ -506,7 +507,9 @@ k_blockdiag_inverse(int n, const double* __restrict__ dblocks, double* __restric
       for (int i = 0; i < B; i++) {
         if (i == j)
           continue;
-        A_(i, k) -= A_(i, j) * A_(j, k) * hr;
+        // (a_ij * a_jk) * hr, then the subtraction: no contraction, so the
+        // rounding is the reference's
+        A_(i, k) = __dsub_rn(A_(i, k), __dmul_rn(__dmul_rn(A_(i, j), A_(j, k)), hr));
       }
     }
     for (int i = 0; i < B; i++) {

@@ -25,6 +25,7 @@
 
 #include "../../include/gascoigne_b200.h"
 #include "gb_kernels.cuh"
+#include "gb_block.cuh"
 
 namespace gb {
 
@@ -105,10 +106,11 @@ struct Error
 
 // SELL-32: slice s holds rows 32s..32s+31, column-major (entry j of lane l at
 // sptr[s] + 32 j + l); slice width = longest row of the slice; padding uses
-// column = own row (or 0 past n) and value 0.
+// column = own row (or 0 past n) and value 0. Block rows (B > 1) keep one
+// column per block; value q of the block is at (sptr[s] + 32 j) * B*B + 32 q + l.
 struct Sell
 {
-  int n = 0, nslices = 0;
+  int n = 0, nslices = 0, B = 1; // n block rows of B x B blocks
   int64_t entries = 0, nnz = 0;
   DeviceArray<int> sptr, col;
   DeviceArray<double> v64;
@@ -175,8 +177,10 @@ build_patterns(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
 
 static void
 build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
-           const double* val, cudaStream_t st)
+           const double* val, cudaStream_t st, int B = 1)
 {
+  const int B2 = B * B;
+  S.B = B;
   S.n = static_cast<int>(n);
   S.nslices = static_cast<int>((n + kSlice - 1) / kSlice);
   S.nnz = rowptr[n];
@@ -195,8 +199,8 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
   }
   S.entries = sptr[S.nslices];
   std::vector<int> c(S.entries);
-  std::vector<double> v(S.entries, 0.0);
-  std::vector<float> v32(S.entries, 0.0f);
+  std::vector<double> v(S.entries * B2, 0.0);
+  std::vector<float> v32(S.entries * B2, 0.0f);
   for (int s = 0; s < S.nslices; ++s) {
     int w = (sptr[s + 1] - sptr[s]) / kSlice;
     for (int l = 0; l < kSlice; ++l) {
@@ -208,8 +212,11 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
           int64_t cc = col[rowptr[r] + j];
           GB_REQUIRE(cc >= 0 && cc < n, GB_EINVAL, "column index out of range");
           c[e] = static_cast<int>(cc);
-          v[e] = val[rowptr[r] + j];
-          v32[e] = static_cast<float>(v[e]);
+          for (int q = 0; q < B2; ++q) {
+            const int64_t ev = (sptr[s] + int64_t(j) * kSlice) * B2 + int64_t(q) * kSlice + l;
+            v[ev] = val[(rowptr[r] + j) * B2 + q];
+            v32[ev] = static_cast<float>(v[ev]);
+          }
         } else {
           c[e] = r < n ? static_cast<int>(r) : 0;
         }
@@ -271,6 +278,19 @@ struct Level
   // quadratic functional J(u) = u^T M u over the cells (gb_level_set_functional)
   Sell M;
   int64_t func_n = -1;
+  // pressure filter (gb_level_set_pfilter): filtered components, weights
+  int pf_mask = 0;
+  DeviceArray<double> pf_w;
+  double pf_domain = 0.0;
+  int64_t nhanging = 0;
+  // Vanka patches (gb_level_set_patches) and their factorisations
+  std::vector<int64_t> h_patches;
+  int npatch = 0, npp = 0, vk_M = 0;
+  bool vk_ready = false, vk_warp = false;
+  DeviceArray<int> vk_pn, vk_nptr, vk_ent;
+  DeviceArray<double> vk_lu64, vk_out64;
+  DeviceArray<float> vk_lu32, vk_out32;
+  DeviceArray<uint8_t> vk_perm;
   int64_t ndof() const { return n * B; }
 };
 
@@ -569,12 +589,40 @@ read_scalar(Context& c, const double* dptr)
 
 // ----------------------------------------------------------------- SpMV
 
+template<int MODE, int B, class TV, class TX, class TO>
+static void
+bspmv(Context& c, const Level& L, const Sell& S, const TX* x, TO* y, const TO* b,
+      const TV* dinv, double alpha, const int* yidx, int64_t ystride, TX* xcopy)
+{
+  const SellView<TV> A = view<TV>(S, sell_vals<TV>(S));
+  if (S.pat)
+    launch(c, k_bspmv<MODE, B, TV, TX, TO, true>, blocks_for(S.n, kSpmvThreads),
+           kSpmvThreads, A, x, y, b, dinv, (const uint8_t*)L.dirmask.p, alpha, yidx,
+           ystride, xcopy);
+  else
+    launch(c, k_bspmv<MODE, B, TV, TX, TO, false>, blocks_for(S.n, kSpmvThreads),
+           kSpmvThreads, A, x, y, b, dinv, (const uint8_t*)L.dirmask.p, alpha, yidx,
+           ystride, xcopy);
+}
+
 template<int MODE, class TV, class TX, class TO>
 static void
 spmv(Context& c, const Level& L, const Sell& S, const TX* x, TO* y, const TO* b,
      const TV* dinv, double alpha, const int* yidx = nullptr, int64_t ystride = 0,
      TX* xcopy = nullptr)
 {
+  switch (S.B) {
+    case 1:
+      break;
+    case 2:
+      return bspmv<MODE, 2>(c, L, S, x, y, b, dinv, alpha, yidx, ystride, xcopy);
+    case 3:
+      return bspmv<MODE, 3>(c, L, S, x, y, b, dinv, alpha, yidx, ystride, xcopy);
+    case 4:
+      return bspmv<MODE, 4>(c, L, S, x, y, b, dinv, alpha, yidx, ystride, xcopy);
+    default:
+      throw Error{ GB_EINVAL, "block size must be 1..4" };
+  }
   const SellView<TV> A = view<TV>(S, sell_vals<TV>(S));
   if (S.pat)
     launch(c, k_spmv<MODE, TV, TX, TO, true>, blocks_for(S.n, kSpmvThreads),
@@ -621,6 +669,8 @@ ensure_AT(Context& c, Level& L)
 {
   if (L.has_AT)
     return;
+  GB_REQUIRE(L.B == 1, GB_EINVAL,
+             "the transposed operator is available for block size 1 only");
   const int64_t n = L.n, nnz = L.h_rowptr[n];
   std::vector<int64_t> tp(n + 1, 0), tc(nnz);
   std::vector<double> tv(nnz);
@@ -660,6 +710,116 @@ ensure_AT(Context& c, Level& L)
 
 // ---------------------------------------------------------- level set-up
 
+// VankaSmoother::ConstructStructure + copy_entries (LinAlg/vankasmoother.cc:
+// 7-113) for one level: each patch's matrix (the level matrix's entries whose
+// row and column nodes both lie in the patch; node-major, components inside)
+// factorised on the host with row partial pivoting in the reference's
+// operation order (first row of largest |a_ik| as pivot, column divided by the
+// pivot, trailing entries updated k by k), uploaded in FP64 and FP32 with the
+// pivots, the patch node lists and, per node, the (patch, local node) pairs in
+// ascending patch order for the averaging gather.
+static void
+ensure_vanka(Context& c, Level& L)
+{
+  if (L.vk_ready)
+    return;
+  GB_REQUIRE(L.npatch > 0, GB_ESTATE, "Vanka needs the patches of every level "
+                                      "(gb_level_set_patches)");
+  const int B = L.B, npp = L.npp, M = npp * B, B2 = B * B;
+  GB_REQUIRE(M <= kVankaMaxM && npp <= 32, GB_EINVAL, "Vanka patch too large");
+  const int64_t np = L.npatch;
+  const bool warp = M > 32;
+  std::vector<double> lu(size_t(np) * M * M);
+  std::vector<uint8_t> perm(size_t(np) * M);
+  std::vector<int> pn(size_t(np) * npp);
+  std::vector<double> a(size_t(M) * M);
+  std::vector<int> pv(M);
+  for (int64_t p = 0; p < np; ++p) {
+    const int64_t* nodes = L.h_patches.data() + p * npp;
+    std::fill(a.begin(), a.end(), 0.0);
+    for (int r = 0; r < npp; ++r) {
+      const int64_t row = nodes[r];
+      for (int64_t pos = L.h_rowptr[row]; pos < L.h_rowptr[row + 1]; ++pos) {
+        int cl = -1;
+        for (int q = 0; q < npp; ++q)
+          if (nodes[q] == L.h_col[pos]) {
+            cl = q;
+            break;
+          }
+        if (cl < 0)
+          continue;
+        for (int cr = 0; cr < B; ++cr)
+          for (int cc = 0; cc < B; ++cc)
+            a[size_t(B * r + cr) * M + B * cl + cc] = L.h_val[pos * B2 + cr * B + cc];
+      }
+    }
+    for (int i = 0; i < M; ++i)
+      pv[i] = i;
+    for (int k = 0; k < M; ++k) {
+      int piv = k;
+      double best = std::fabs(a[size_t(k) * M + k]);
+      for (int i = k + 1; i < M; ++i)
+        if (std::fabs(a[size_t(i) * M + k]) > best) {
+          best = std::fabs(a[size_t(i) * M + k]);
+          piv = i;
+        }
+      if (piv != k) {
+        for (int j = 0; j < M; ++j)
+          std::swap(a[size_t(k) * M + j], a[size_t(piv) * M + j]);
+        std::swap(pv[k], pv[piv]);
+      }
+      if (a[size_t(k) * M + k] != 0)
+        for (int i = k + 1; i < M; ++i)
+          a[size_t(i) * M + k] /= a[size_t(k) * M + k];
+      for (int j = k + 1; j < M; ++j)
+        for (int i = k + 1; i < M; ++i)
+          a[size_t(i) * M + j] -= a[size_t(i) * M + k] * a[size_t(k) * M + j];
+    }
+    for (int e = 0; e < M * M; ++e)
+      lu[warp ? size_t(p) * M * M + e : size_t(e) * np + p] = a[e];
+    for (int i = 0; i < M; ++i)
+      perm[warp ? size_t(p) * M + i : size_t(i) * np + p] = static_cast<uint8_t>(pv[i]);
+    for (int r = 0; r < npp; ++r)
+      pn[size_t(r) * np + p] = static_cast<int>(nodes[r]);
+  }
+  // node -> (patch, local node), patches ascending
+  std::vector<int> nptr(L.n + 1, 0), ent(size_t(np) * npp);
+  for (size_t k = 0; k < L.h_patches.size(); ++k)
+    nptr[L.h_patches[k] + 1]++;
+  for (int64_t i = 0; i < L.n; ++i) {
+    GB_REQUIRE(nptr[i + 1] > 0, GB_EINVAL, "a node lies in no Vanka patch");
+    nptr[i + 1] += nptr[i];
+  }
+  std::vector<int> fill(nptr.begin(), nptr.end() - 1);
+  for (int64_t p = 0; p < np; ++p)
+    for (int r = 0; r < npp; ++r)
+      ent[fill[L.h_patches[p * npp + r]]++] = static_cast<int>(p * 32 + r);
+  std::vector<float> lu32(lu.begin(), lu.end());
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  GB_CUDA(L.vk_lu64.alloc(lu.size()));
+  GB_CUDA(L.vk_lu32.alloc(lu.size()));
+  GB_CUDA(L.vk_perm.alloc(perm.size()));
+  GB_CUDA(L.vk_pn.alloc(pn.size()));
+  GB_CUDA(L.vk_nptr.alloc(nptr.size()));
+  GB_CUDA(L.vk_ent.alloc(ent.size()));
+  GB_CUDA(L.vk_out64.alloc(size_t(np) * M));
+  GB_CUDA(L.vk_out32.alloc(size_t(np) * M));
+  GB_CUDA(cudaMemcpy(L.vk_lu64.p, lu.data(), lu.size() * sizeof(double),
+                     cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(L.vk_lu32.p, lu32.data(), lu32.size() * sizeof(float),
+                     cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(L.vk_perm.p, perm.data(), perm.size(), cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(L.vk_pn.p, pn.data(), pn.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(L.vk_nptr.p, nptr.data(), nptr.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(L.vk_ent.p, ent.data(), ent.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  L.vk_M = M;
+  L.vk_warp = warp;
+  L.vk_ready = true;
+}
+
 static void
 ensure_work(Context& c)
 {
@@ -691,8 +851,19 @@ ensure_work(Context& c)
   if (c.transposed)
     for (int l = 0; l < c.nlevels; ++l)
       ensure_AT(c, c.L[l]);
+  GB_REQUIRE(c.params.smoother == 0 || c.params.smoother == 1, GB_EINVAL,
+             "smoother must be 0 (jacobi) or 1 (vanka)");
+  if (c.params.smoother == 1) {
+    GB_REQUIRE(!c.transposed, GB_EINVAL, "Vanka with the transposed operator");
+    for (int l = 0; l < c.nlevels; ++l)
+      ensure_vanka(c, c.L[l]);
+  }
+  // the single-CTA coarse-level program covers scalar Jacobi cycles
+  bool simple = c.params.smoother == 0;
+  for (int l = 0; l < c.nlevels; ++l)
+    simple = simple && c.L[l].B == 1 && !c.L[l].pf_mask;
   c.coarse_root = -1;
-  for (int l = 0; l < c.nlevels; ++l) {
+  for (int l = 0; l < c.nlevels && simple; ++l) {
     if (c.L[l].ndof() > kCoarseMaxRows)
       break;
     c.coarse_root = l;
@@ -742,9 +913,124 @@ struct Emit
     const Level& L = c.L[l];
     if (rec)
       return rec->push_back(level_op(kOpJacobiZero, L, u, nullptr, b, c.params.omega));
-    launch(c, k_jacobi_from_zero<T, T>, blocks_for(L.n, 256), 256, (int)L.n,
-           dinv_of<T>(L), b, u, c.params.omega);
+    if (L.B == 1)
+      launch(c, k_jacobi_from_zero<T, T>, blocks_for(L.n, 256), 256, (int)L.n,
+             dinv_of<T>(L), b, u, c.params.omega);
+    else
+      jacobi_apply(l, b, u, true);
   }
+  // u = (u_zero ? 0 : u) + omega D^-1 h (block Jacobi update, h given)
+  void jacobi_apply(int l, const T* h, T* u, bool u_zero)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    const int nb = blocks_for(L.n, 256);
+    switch (L.B) {
+      case 1:
+        launch(c, k_block_jacobi_apply<1, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
+               c.params.omega, int(u_zero));
+        break;
+      case 2:
+        launch(c, k_block_jacobi_apply<2, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
+               c.params.omega, int(u_zero));
+        break;
+      case 3:
+        launch(c, k_block_jacobi_apply<3, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
+               c.params.omega, int(u_zero));
+        break;
+      default:
+        launch(c, k_block_jacobi_apply<4, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
+               c.params.omega, int(u_zero));
+    }
+  }
+  // u = (u_zero ? 0 : u) + omega * Vanka(h) (VankaSmoother::solve + Add)
+  void vanka(int l, const T* h, T* u, bool u_zero)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    const TV_of* lu = vk_lu(L);
+    T* out = vk_out(L);
+    if (!L.vk_warp) {
+      const int nb = blocks_for(L.npatch, 128);
+      switch (L.vk_M * 8 + L.B) {
+#define GB_VK(MM, BB)                                                          \
+  case MM * 8 + BB:                                                            \
+    launch(c, k_vanka_local<MM, BB, T, T>, nb, 128, L.npatch, (const int*)L.vk_pn.p, \
+           lu, (const uint8_t*)L.vk_perm.p, h, out);                           \
+    break;
+        GB_VK(9, 1)
+        GB_VK(27, 1)
+        GB_VK(18, 2)
+        GB_VK(27, 3)
+        GB_VK(8, 2)
+        GB_VK(12, 3)
+        GB_VK(16, 4)
+        GB_VK(4, 1)
+        GB_VK(8, 1)
+#undef GB_VK
+        default:
+          throw Error{ GB_EINVAL, "no Vanka kernel for this patch size" };
+      }
+    } else {
+      launch(c, k_vanka_local_warp<T, T>, blocks_for(L.npatch, kVankaWarps),
+             32 * kVankaWarps, L.npatch, L.vk_M, L.B, (const int*)L.vk_pn.p, lu,
+             (const uint8_t*)L.vk_perm.p, h, out);
+    }
+    const int64_t s1 = L.vk_warp ? 1 : L.npatch, s2 = L.vk_warp ? L.vk_M : 1;
+    const int nb = blocks_for(L.n, 256);
+    switch (L.B) {
+      case 1:
+        launch(c, k_vanka_gather<1, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
+               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
+               int(u_zero));
+        break;
+      case 2:
+        launch(c, k_vanka_gather<2, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
+               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
+               int(u_zero));
+        break;
+      case 3:
+        launch(c, k_vanka_gather<3, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
+               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
+               int(u_zero));
+        break;
+      default:
+        launch(c, k_vanka_gather<4, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
+               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
+               int(u_zero));
+    }
+  }
+  // pressure filter on x: weighted (SubtractMean) or algebraic
+  // (SubtractMeanAlgebraic) mean of every filtered component removed
+  void pf_sub(int l, T* x, bool weighted)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    for (int comp = 0; comp < L.B; ++comp) {
+      if (!(L.pf_mask & (1 << comp)))
+        continue;
+      launch(c, k_comp_sum<T>, red_blocks(L.n), kRedThreads, (int)L.n, L.B, comp,
+             (const T*)x, weighted ? (const double*)L.pf_w.p : nullptr, c.partials.p,
+             c.ticket.p, RedOut{ c.scal.p + 8, nullptr, nullptr, 0 });
+      const double denom = weighted ? L.pf_domain : double(L.n - L.nhanging);
+      launch(c, k_comp_sub<T>, stream_blocks(L.n), 256, (int)L.n, L.B, comp, x,
+             (const double*)(c.scal.p + 8), denom);
+    }
+  }
+  void copy(int l, T* dst, const T* src)
+  {
+    no_rec();
+    launch(c, k_equ<T, T>, stream_blocks(c.L[l].ndof()), 256, (int64_t)c.L[l].ndof(), dst,
+           1.0, src);
+  }
+  void no_rec() const
+  {
+    if (rec)
+      throw Error{ GB_EINVAL, "step not available in the coarse-level program" };
+  }
+  using TV_of = T;
+  static const T* vk_lu(const Level& L);
+  static T* vk_out(const Level& L);
   void jacobi(int l, const T* u, T* out, const T* b)
   {
     const Level& L = c.L[l];
@@ -775,8 +1061,21 @@ struct Emit
       o.tent = Tr.rent.p;
       return rec->push_back(o);
     }
-    launch(c, k_restrict<T>, blocks_for(Tr.nc, 256), 256, Tr.nc, Tr.rptr.p, Tr.rent.p,
-           fine, coarse, (const uint8_t*)c.L[l].dirmask.p);
+    const uint8_t* cm = c.L[l].dirmask.p;
+    const int nb = blocks_for(Tr.nc, 256);
+    switch (c.L[l].B) {
+      case 1:
+        launch(c, k_restrict<T>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        break;
+      case 2:
+        launch(c, k_restrict_b<T, 2>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        break;
+      case 3:
+        launch(c, k_restrict_b<T, 3>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        break;
+      default:
+        launch(c, k_restrict_b<T, 4>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+    }
   }
   void fill0(int l, T* u)
   {
@@ -807,27 +1106,98 @@ struct Emit
       o.alpha = c.params.mgomega;
       return rec->push_back(o);
     }
-    launch(c, k_prolong<1, T>, blocks_for(Tr.nf, 256), 256, Tr.nf, Tr.pptr.p, Tr.pent.p,
-           coarse, fine, (const uint8_t*)c.L[l + 1].dirmask.p, c.params.mgomega);
+    const uint8_t* fm = c.L[l + 1].dirmask.p;
+    const double mw = c.params.mgomega;
+    const int nb = blocks_for(Tr.nf, 256);
+    switch (c.L[l + 1].B) {
+      case 1:
+        launch(c, k_prolong<1, T>, nb, 256, Tr.nf, Tr.pptr.p, Tr.pent.p, coarse, fine, fm, mw);
+        break;
+      case 2:
+        launch(c, k_prolong_b<1, T, 2>, nb, 256, Tr.nf, Tr.pptr.p, Tr.pent.p, coarse, fine,
+               fm, mw);
+        break;
+      case 3:
+        launch(c, k_prolong_b<1, T, 3>, nb, 256, Tr.nf, Tr.pptr.p, Tr.pent.p, coarse, fine,
+               fm, mw);
+        break;
+      default:
+        launch(c, k_prolong_b<1, T, 4>, nb, 256, Tr.nf, Tr.pptr.p, Tr.pent.p, coarse, fine,
+               fm, mw);
+    }
   }
 };
+
+template<>
+const double* Emit<double>::vk_lu(const Level& L)
+{
+  return L.vk_lu64.p;
+}
+template<>
+const float* Emit<float>::vk_lu(const Level& L)
+{
+  return L.vk_lu32.p;
+}
+template<>
+double* Emit<double>::vk_out(const Level& L)
+{
+  return L.vk_out64.p;
+}
+template<>
+float* Emit<float>::vk_out(const Level& L)
+{
+  return L.vk_out32.p;
+}
 
 // StdSolver::smooth, linear_smooth jacobi (Solver/stdsolver.cc:951-986): each
 // sweep computes h = y - A x, h = D^-1 h, x += omega h; fused into one pass that
 // writes the new iterate to the other buffer (u and tmp swap roles). A sweep
 // from x = 0 needs no product (y - A 0 == y).
+//
+// With the Vanka smoother or a pressure filter a sweep is done in place:
+// h = y - A x (tmp), SubtractMeanAlgebraic(h), h = Vanka(h) or D^-1 h,
+// x += omega h, SubtractMean(x).
+static bool
+fused_smoother(const Context& c, const Level& L)
+{
+  return c.params.smoother == 0 && !L.pf_mask;
+}
+
 template<class T>
 static void
 smooth(Emit<T>& E, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
 {
+  Context& c = E.c;
+  const Level& L = c.L[l];
+  const bool fused = fused_smoother(c, L);
   for (int it = 0; it < niter; ++it) {
-    if (u_zero) {
-      E.jacobi_zero(l, u, b);
-      u_zero = false;
-    } else {
-      E.jacobi(l, u, tmp, b);
-      std::swap(u, tmp);
+    if (fused) {
+      if (u_zero) {
+        E.jacobi_zero(l, u, b);
+        u_zero = false;
+      } else {
+        E.jacobi(l, u, tmp, b);
+        std::swap(u, tmp);
+      }
+      continue;
     }
+    const T* h = b; // y - A 0
+    if (!u_zero) {
+      E.resid(l, u, tmp, b);
+      h = tmp;
+    } else if (L.pf_mask) {
+      E.copy(l, tmp, b);
+      h = tmp;
+    }
+    if (L.pf_mask)
+      E.pf_sub(l, tmp, false);
+    if (c.params.smoother == 1)
+      E.vanka(l, h, u, u_zero);
+    else
+      E.jacobi_apply(l, h, u, u_zero);
+    u_zero = false;
+    if (L.pf_mask)
+      E.pf_sub(l, u, true);
   }
 }
 
@@ -1017,8 +1387,16 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
     return u_zero;
   }
   smooth<T>(E, l, P.iterpre, u, tmp, b, u_zero);
-  // MatrixResidual into tmp, restrict_zero + SetBoundaryVectorZero on l-1
-  if (u_zero) {
+  // MatrixResidual into tmp (with SubtractMeanAlgebraic), restrict_zero +
+  // SetBoundaryVectorZero on l-1
+  if (c.L[l].pf_mask) {
+    if (u_zero)
+      E.copy(l, tmp, b);
+    else
+      E.resid(l, u, tmp, b);
+    E.pf_sub(l, tmp, false);
+    E.restrict_to(l - 1, tmp, W.b[l - 1].p);
+  } else if (u_zero) {
     E.restrict_to(l - 1, b, W.b[l - 1].p); // u == 0: the residual is b
   } else {
     E.resid(l, u, tmp, b);
@@ -1058,6 +1436,8 @@ precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero)
   int pingpong = (x_zero ? std::max(P.iterpre - 1, 0) : P.iterpre) + P.iterpost;
   if (fl == 0)
     pingpong = x_zero ? std::max(P.iterexact - 1, 0) : P.iterexact;
+  if (!fused_smoother(c, c.L[fl]))
+    pingpong = 0; // sweeps in place
   if (x_zero && (pingpong & 1))
     std::swap(u, tmp);
   char p = P.mgtype;
@@ -1184,6 +1564,18 @@ fill_info(Context& c, gb_solve_info* info, double* x_for_residual, const double*
   info->rhs_norm = two[1];
 }
 
+// NewtonLinearSolve's closing SubtractMean(x) on the finest level
+// (Solver/stdmultilevelsolver.cc:671); a no-op without a pressure filter.
+static void
+final_filter(Context& c, double* x)
+{
+  const int fl = c.nlevels - 1;
+  if (!c.L[fl].pf_mask)
+    return;
+  Emit<double> E{ c, nullptr };
+  E.pf_sub(fl, x, true);
+}
+
 // StdMultiLevelSolver::Gmres -> GMRES::solve (left preconditioning)
 static int
 gmres_left(Context& c, double* x, const double* b, gb_solve_info* info)
@@ -1236,6 +1628,7 @@ gmres_left(Context& c, double* x, const double* b, gb_solve_info* info)
     launch(c, k_multi_axpy<double>, stream_blocks(n), 256, n, x, (const double*)V, n,
            (const double*)G->hs, dim);
   }
+  final_filter(c, x);
   GB_CUDA(cudaEventRecord(c.ev1, c.stream));
   GB_CUDA(cudaEventSynchronize(c.ev1));
   float ms = 0;
@@ -1333,6 +1726,7 @@ gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* 
     total += steps;
     restarts++;
   }
+  final_filter(c, x);
   GB_CUDA(cudaEventRecord(c.ev1, c.stream));
   GB_CUDA(cudaEventSynchronize(c.ev1));
   float ms = 0;
@@ -1623,6 +2017,9 @@ fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* in
   } else {
     fgmres_eager<double>(c, prec);
   }
+  const int64_t l_filter = c.launches;
+  final_filter(c, c.xg.p);
+  const int64_t filter_k = c.launches - l_filter;
   GB_CUDA(cudaEventRecord(c.ev1, c.stream));
   if (copy_out && x != c.xg.p)
     GB_CUDA(cudaMemcpyAsync(x, c.xg.p, n * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -1641,6 +2038,7 @@ fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* in
   if (c.use_graph) {
     kernels = F.setup_k + int64_t(restarts + 1) * F.outer_k + int64_t(total) * F.inner_k;
     c.launches += kernels;
+    kernels += filter_k;
   }
   if (info) {
     fill_info(c, info, c.xg.p, c.bg.p);
@@ -1825,8 +2223,10 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   GB_API_BEGIN
   ctx->version++;
   Level& L = level(*ctx, lvl);
-  GB_REQUIRE(B == 1, GB_EINVAL, "only block size 1 is supported by this build");
-  GB_REQUIRE(n >= 1 && n < (int64_t(1) << 29), GB_EINVAL, "n out of range");
+  GB_REQUIRE(B >= 1 && B <= 4, GB_EINVAL, "block size must be 1..4");
+  GB_REQUIRE(B == 1 || !ctx->transposed, GB_EINVAL,
+             "the transposed operator is available for block size 1 only");
+  GB_REQUIRE(n >= 1 && n * B < (int64_t(1) << 29), GB_EINVAL, "n out of range");
   GB_REQUIRE(rowptr && col && diag && val, GB_EINVAL, "null array");
   GB_REQUIRE(rowptr[0] == 0, GB_EINVAL, "rowptr[0] != 0");
   for (int64_t i = 0; i < n; ++i) {
@@ -1842,8 +2242,9 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   L.h_col.assign(col, col + nnzb);
   L.h_diag.assign(diag, diag + n);
   L.h_val.assign(val, val + nnzb * B * B);
-  build_sell(L.A, n, rowptr, col, val, ctx->stream);
+  build_sell(L.A, n, rowptr, col, val, ctx->stream, B);
   L.has_AT = false;
+  L.vk_ready = false;
   if (ctx->transposed)
     ensure_AT(*ctx, L);
   // block-diagonal inverse on the device (get_inverse_diagonal / K1)
@@ -1857,8 +2258,23 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
                           cudaMemcpyHostToDevice, ctx->stream));
   GB_CUDA(L.dinv64.alloc(n * B * B));
   GB_CUDA(L.dinv32.alloc(n * B * B));
-  launch(*ctx, k_blockdiag_inverse<1>, blocks_for(n, 128), 128, (int)n,
-         (const double*)dd.p, L.dinv64.p, L.dinv32.p);
+  switch (B) {
+    case 1:
+      launch(*ctx, k_blockdiag_inverse<1>, blocks_for(n, 128), 128, (int)n,
+             (const double*)dd.p, L.dinv64.p, L.dinv32.p);
+      break;
+    case 2:
+      launch(*ctx, k_blockdiag_inverse<2>, blocks_for(n, 128), 128, (int)n,
+             (const double*)dd.p, L.dinv64.p, L.dinv32.p);
+      break;
+    case 3:
+      launch(*ctx, k_blockdiag_inverse<3>, blocks_for(n, 128), 128, (int)n,
+             (const double*)dd.p, L.dinv64.p, L.dinv32.p);
+      break;
+    default:
+      launch(*ctx, k_blockdiag_inverse<4>, blocks_for(n, 128), 128, (int)n,
+             (const double*)dd.p, L.dinv64.p, L.dinv32.p);
+  }
   if (L.dirmask.n != static_cast<size_t>(n * B)) {
     GB_CUDA(L.dirmask.alloc(n * B));
     GB_CUDA(cudaMemsetAsync(L.dirmask.p, 0, n * B, ctx->stream));
@@ -1913,7 +2329,7 @@ gb_level_set_transfer(gb_ctx* ctx, int lvl, int64_t ncoarse, const int64_t* c2f,
   Level& Lc = level_with_matrix(*ctx, lvl);
   Level& Lf = level_with_matrix(*ctx, lvl + 1);
   GB_REQUIRE(ncoarse == Lc.n, GB_EINVAL, "c2f size differs from the coarse level size");
-  GB_REQUIRE(Lc.B == 1 && Lf.B == 1, GB_EINVAL, "only block size 1");
+  GB_REQUIRE(Lc.B == Lf.B, GB_EINVAL, "levels of different block size");
   const int64_t nf = Lf.n;
   // (fine, coarse, weight code) pairs as MgInterpolatorMatrix::BasicInit forms them
   std::vector<int> wcode(nf, -1);
@@ -2149,9 +2565,13 @@ gb_matrix_residual(gb_ctx* ctx, int lvl, int y, int x, int b)
   GB_API_BEGIN
   GB_REQUIRE(y != x && y != b, GB_EINVAL, "y must differ from x and b");
   Level& L = level_with_matrix(*ctx, lvl);
+  double* yd = vec(*ctx, lvl, y);
   spmv<kResid, double, double, double>(*ctx, L, opA(*ctx, L), (const double*)vec(*ctx, lvl, x),
-                                       vec(*ctx, lvl, y),
-                                       (const double*)vec(*ctx, lvl, b), nullptr, 0.0);
+                                       yd, (const double*)vec(*ctx, lvl, b), nullptr, 0.0);
+  if (L.pf_mask) { // SubtractMeanAlgebraic
+    Emit<double> E{ *ctx, nullptr };
+    E.pf_sub(lvl, yd, false);
+  }
   GB_API_END
 }
 
@@ -2168,24 +2588,129 @@ gb_residualgmres(gb_ctx* ctx, int lvl, int y, int x, int b)
   GB_API_END
 }
 
-int
-gb_smooth_jacobi(gb_ctx* ctx, int lvl, int niter, int x, int y, int h)
+// StdSolver::smooth with smoother 0 (jacobi) or 1 (Vanka), FP64.
+static void
+smooth_api(gb_ctx* ctx, int lvl, int niter, int x, int y, int h, int smoother)
 {
-  GB_API_BEGIN
   GB_REQUIRE(niter >= 0, GB_EINVAL, "niter < 0");
   GB_REQUIRE(x != y && x != h && y != h, GB_EINVAL, "x, y, h must differ");
-  level_with_matrix(*ctx, lvl);
+  Level& L = level_with_matrix(*ctx, lvl);
+  if (smoother == 1) {
+    GB_REQUIRE(!ctx->transposed, GB_EINVAL, "Vanka with the transposed operator");
+    ensure_vanka(*ctx, L);
+  }
   double* xd = vec(*ctx, lvl, x);
   double* hd = vec(*ctx, lvl, h);
   const double* yd = vec(*ctx, lvl, y);
   double* u = xd;
   double* t = hd;
   bool zero = false;
+  const int saved = ctx->params.smoother;
+  ctx->params.smoother = smoother;
+  struct Restore
+  {
+    gb_ctx* c;
+    int v;
+    ~Restore() { c->params.smoother = v; }
+  } restore{ ctx, saved };
   Emit<double> E{ *ctx, nullptr };
   smooth<double>(E, lvl, niter, u, t, yd, zero);
   if (u != xd)
     GB_CUDA(cudaMemcpyAsync(xd, u, ctx->L[lvl].ndof() * sizeof(double),
                             cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+int
+gb_smooth_jacobi(gb_ctx* ctx, int lvl, int niter, int x, int y, int h)
+{
+  GB_API_BEGIN
+  smooth_api(ctx, lvl, niter, x, y, h, 0);
+  GB_API_END
+}
+
+int
+gb_smooth_vanka(gb_ctx* ctx, int lvl, int niter, int x, int y, int h)
+{
+  GB_API_BEGIN
+  smooth_api(ctx, lvl, niter, x, y, h, 1);
+  GB_API_END
+}
+
+int
+gb_smooth(gb_ctx* ctx, int lvl, int niter, int x, int y, int h)
+{
+  GB_API_BEGIN
+  smooth_api(ctx, lvl, niter, x, y, h, ctx->params.smoother);
+  GB_API_END
+}
+
+int
+gb_level_set_patches(gb_ctx* ctx, int lvl, int64_t npatch, int npp, const int64_t* patches)
+{
+  GB_API_BEGIN
+  ctx->version++;
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(npatch >= 1 && npp >= 1 && npp <= 27 && patches, GB_EINVAL,
+             "bad patch list (npp must be 1..27)");
+  GB_REQUIRE(npatch * npp < (int64_t(1) << 31) && npatch < (int64_t(1) << 26), GB_EINVAL,
+             "too many patches");
+  for (int64_t k = 0; k < npatch * npp; ++k)
+    GB_REQUIRE(patches[k] >= 0 && patches[k] < L.n, GB_EINVAL, "patch node out of range");
+  for (int64_t p = 0; p < npatch; ++p)
+    for (int a = 0; a < npp; ++a)
+      for (int b = a + 1; b < npp; ++b)
+        GB_REQUIRE(patches[p * npp + a] != patches[p * npp + b], GB_EINVAL,
+                   "a node appears twice in a patch");
+  L.h_patches.assign(patches, patches + npatch * npp);
+  L.npatch = static_cast<int>(npatch);
+  L.npp = npp;
+  L.vk_ready = false;
+  ctx->work_ready = false;
+  GB_API_END
+}
+
+int
+gb_level_set_pfilter(gb_ctx* ctx, int lvl, int comp_mask, const double* weights,
+                     double domain, int64_t nhanging)
+{
+  GB_API_BEGIN
+  ctx->version++;
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(comp_mask >= 0 && comp_mask < (1 << L.B), GB_EINVAL, "bad component mask");
+  GB_REQUIRE(comp_mask == 0 || (weights && domain > 0.0), GB_EINVAL,
+             "the filter needs weights and a positive domain size");
+  GB_REQUIRE(nhanging >= 0 && nhanging < L.n, GB_EINVAL, "bad hanging-node count");
+  if (comp_mask) {
+    GB_CUDA(cudaStreamSynchronize(ctx->stream));
+    GB_CUDA(L.pf_w.alloc(L.n));
+    GB_CUDA(cudaMemcpy(L.pf_w.p, weights, L.n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  L.pf_mask = comp_mask;
+  L.pf_domain = domain;
+  L.nhanging = nhanging;
+  ctx->work_ready = false;
+  GB_API_END
+}
+
+int
+gb_subtract_mean(gb_ctx* ctx, int lvl, int id)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  Emit<double> E{ *ctx, nullptr };
+  if (L.pf_mask)
+    E.pf_sub(lvl, vec(*ctx, lvl, id), true);
+  GB_API_END
+}
+
+int
+gb_subtract_mean_algebraic(gb_ctx* ctx, int lvl, int id)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  Emit<double> E{ *ctx, nullptr };
+  if (L.pf_mask)
+    E.pf_sub(lvl, vec(*ctx, lvl, id), false);
   GB_API_END
 }
 
@@ -2218,9 +2743,25 @@ gb_restrict_zero(gb_ctx* ctx, int lvl, int coarse_id, int fine_id)
   GB_REQUIRE(lvl >= 0 && lvl + 1 < ctx->nlevels && ctx->T[lvl].set, GB_ESTATE,
              "no transfer on this level");
   Transfer& T = ctx->T[lvl];
-  launch(*ctx, k_restrict<double>, blocks_for(T.nc, 256), 256, T.nc, (const int*)T.rptr.p,
-         (const uint32_t*)T.rent.p, (const double*)vec(*ctx, lvl + 1, fine_id),
-         vec(*ctx, lvl, coarse_id), (const uint8_t*)nullptr);
+  const int B = ctx->L[lvl].B, nb = blocks_for(T.nc, 256);
+  const int* tp = T.rptr.p;
+  const uint32_t* te = T.rent.p;
+  const double* f = vec(*ctx, lvl + 1, fine_id);
+  double* cc = vec(*ctx, lvl, coarse_id);
+  const uint8_t* nm = nullptr;
+  switch (B) {
+    case 1:
+      launch(*ctx, k_restrict<double>, nb, 256, T.nc, tp, te, f, cc, nm);
+      break;
+    case 2:
+      launch(*ctx, k_restrict_b<double, 2>, nb, 256, T.nc, tp, te, f, cc, nm);
+      break;
+    case 3:
+      launch(*ctx, k_restrict_b<double, 3>, nb, 256, T.nc, tp, te, f, cc, nm);
+      break;
+    default:
+      launch(*ctx, k_restrict_b<double, 4>, nb, 256, T.nc, tp, te, f, cc, nm);
+  }
   GB_API_END
 }
 
@@ -2231,10 +2772,25 @@ gb_prolongate_add(gb_ctx* ctx, int lvl, int fine_id, int coarse_id)
   GB_REQUIRE(lvl >= 0 && lvl + 1 < ctx->nlevels && ctx->T[lvl].set, GB_ESTATE,
              "no transfer on this level");
   Transfer& T = ctx->T[lvl];
-  launch(*ctx, k_prolong<0, double>, blocks_for(T.nf, 256), 256, T.nf,
-         (const int*)T.pptr.p, (const uint32_t*)T.pent.p,
-         (const double*)vec(*ctx, lvl, coarse_id), vec(*ctx, lvl + 1, fine_id),
-         (const uint8_t*)nullptr, 1.0);
+  const int B = ctx->L[lvl].B, nb = blocks_for(T.nf, 256);
+  const int* tp = T.pptr.p;
+  const uint32_t* te = T.pent.p;
+  const double* cc = vec(*ctx, lvl, coarse_id);
+  double* f = vec(*ctx, lvl + 1, fine_id);
+  const uint8_t* nm = nullptr;
+  switch (B) {
+    case 1:
+      launch(*ctx, k_prolong<0, double>, nb, 256, T.nf, tp, te, cc, f, nm, 1.0);
+      break;
+    case 2:
+      launch(*ctx, k_prolong_b<0, double, 2>, nb, 256, T.nf, tp, te, cc, f, nm, 1.0);
+      break;
+    case 3:
+      launch(*ctx, k_prolong_b<0, double, 3>, nb, 256, T.nf, tp, te, cc, f, nm, 1.0);
+      break;
+    default:
+      launch(*ctx, k_prolong_b<0, double, 4>, nb, 256, T.nf, tp, te, cc, f, nm, 1.0);
+  }
   GB_API_END
 }
 

@@ -28,7 +28,7 @@ class GbParams(C.Structure):
     _fields_ = [("iterpre", C.c_int), ("iterpost", C.c_int), ("iterexact", C.c_int),
                 ("omega", C.c_double), ("mgomega", C.c_double), ("mgtype", C.c_char),
                 ("gmressize", C.c_int), ("tol", C.c_double), ("globaltol", C.c_double),
-                ("maxiter", C.c_int)]
+                ("maxiter", C.c_int), ("smoother", C.c_int)]
 
 
 class GbSolveInfo(C.Structure):
@@ -80,6 +80,12 @@ _SIGS = {
     "gb_matrix_residual": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int],
     "gb_residualgmres": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int],
     "gb_smooth_jacobi": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
+    "gb_smooth_vanka": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
+    "gb_smooth": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
+    "gb_subtract_mean": [C.c_void_p, C.c_int, C.c_int],
+    "gb_subtract_mean_algebraic": [C.c_void_p, C.c_int, C.c_int],
+    "gb_level_set_patches": [C.c_void_p, C.c_int, C.c_int64, C.c_int, _P64],
+    "gb_level_set_pfilter": [C.c_void_p, C.c_int, C.c_int, _PD, C.c_double, C.c_int64],
     "gb_dirichlet_zero": [C.c_void_p, C.c_int, C.c_int],
     "gb_level_get_inverse_diagonal": [C.c_void_p, C.c_int, _PD, C.c_int64],
     "gb_restrict_zero": [C.c_void_p, C.c_int, C.c_int, C.c_int],
@@ -143,6 +149,7 @@ class Context:
         self.h = h
         self.nlevels = 0
         self.sizes = []
+        self.blocks = []
 
     # ------------------------------------------------------------ plumbing
     def _chk(self, rc):
@@ -170,9 +177,14 @@ class Context:
 
     # ------------------------------------------------------------- set-up
     def set_params(self, iterpre=2, iterpost=2, iterexact=10, omega=0.8, mgomega=1.0,
-                   mgtype="V", gmressize=21, tol=1e-8, globaltol=1e-16, maxiter=100):
+                   mgtype="V", gmressize=21, tol=1e-8, globaltol=1e-16, maxiter=100,
+                   smoother=None):
+        """smoother: "jacobi", "vanka" (or 0/1); default: the loaded problem's."""
+        if smoother is None:
+            smoother = getattr(self, "smoother", "jacobi")
+        sm = {"jacobi": 0, "vanka": 1}.get(smoother, smoother)
         p = GbParams(iterpre, iterpost, iterexact, omega, mgomega, mgtype.encode()[:1],
-                     gmressize, tol, globaltol, maxiter)
+                     gmressize, tol, globaltol, maxiter, int(sm))
         self._chk(self._L.gb_set_params(self.h, C.byref(p)))
 
     def get_params(self):
@@ -181,11 +193,15 @@ class Context:
         return {k: getattr(p, k) for k, _ in p._fields_}
 
     def load_problem(self, prob):
-        """Uploads every level's matrix, Dirichlet list and transfer maps."""
+        """Uploads every level's matrix, Dirichlet list, Vanka patches, pressure
+        filter and transfer maps; the problem's smoother becomes the default of
+        set_params."""
+        self.smoother = prob.info.get("smoother", "jacobi")
         nl = prob.nlevels
         self._chk(self._L.gb_set_nlevels(self.h, nl))
         self.nlevels = nl
         self.sizes = []
+        self.blocks = []
         for l, lv in enumerate(prob.levels):
             rp, cl, dg = (np.ascontiguousarray(a, dtype=np.int64)
                           for a in (lv.rowptr, lv.col, lv.diag))
@@ -195,7 +211,16 @@ class Context:
             dr = np.ascontiguousarray(lv.dirichlet, dtype=np.int64)
             self._chk(self._L.gb_level_set_dirichlet(self.h, l, dr.shape[0], _p64(dr),
                                                      lv.dircomp_mask))
+            if getattr(lv, "patches", None) is not None:
+                pt = np.ascontiguousarray(lv.patches, dtype=np.int64)
+                self._chk(self._L.gb_level_set_patches(self.h, l, pt.shape[0], pt.shape[1],
+                                                       _p64(pt)))
+            if getattr(lv, "pf_mask", 0):
+                w = np.ascontiguousarray(lv.pf_weights, dtype=np.float64)
+                self._chk(self._L.gb_level_set_pfilter(self.h, l, lv.pf_mask, _pd(w),
+                                                       lv.pf_domain, 0))
             self.sizes.append(lv.n * lv.B)
+            self.blocks.append(lv.B)
         for l, t in enumerate(prob.transfers):
             c2f, z, v, a = (np.ascontiguousarray(x, dtype=np.int64)
                             for x in (t.c2f, t.zweier, t.vierer, t.achter))
@@ -276,11 +301,21 @@ class Context:
     def smooth_jacobi(self, level, niter, x, y, h):
         self._chk(self._L.gb_smooth_jacobi(self.h, level, niter, x, y, h))
 
+    def smooth_vanka(self, level, niter, x, y, h):
+        self._chk(self._L.gb_smooth_vanka(self.h, level, niter, x, y, h))
+
+    def smooth(self, level, niter, x, y, h):
+        self._chk(self._L.gb_smooth(self.h, level, niter, x, y, h))
+
+    def subtract_mean(self, level, vid, algebraic=False):
+        f = self._L.gb_subtract_mean_algebraic if algebraic else self._L.gb_subtract_mean
+        self._chk(f(self.h, level, vid))
+
     def dirichlet_zero(self, level, vid):
         self._chk(self._L.gb_dirichlet_zero(self.h, level, vid))
 
     def inverse_diagonal(self, level):
-        out = np.empty(self.sizes[level])
+        out = np.empty(self.sizes[level] * self.blocks[level])
         self._chk(self._L.gb_level_get_inverse_diagonal(self.h, level, _pd(out),
                                                         out.shape[0]))
         return out

@@ -61,6 +61,8 @@ typedef struct gb_params
   double tol;        /* linear_tol (relative) */
   double globaltol;  /* linear_globaltol (absolute) */
   int maxiter;       /* linear_maxiter */
+  int smoother;      /* 0: linear_smooth jacobi (block Jacobi); 1: linear_smooth
+                        ilu with matrixtype vanka (VankaSmoother) */
 } gb_params;
 
 typedef struct gb_solve_info
@@ -99,8 +101,9 @@ int gb_set_nlevels(gb_ctx* ctx, int nlevels);
  * (LinAlg/sparseblockmatrix.h:84, LinAlg/columnstencil.h:57-60,
  * LinAlg/columndiagstencil.h:54-57). Replaces CudaSolver::AssembleMatrix's
  * CudaCSRMatrixInterface upload and get_inverse_diagonal (cuda/cudasolver.cc:
- * 115-128, cuda/cudacsrmatrixinterface.cc:119-141,176-230). B = 1 on this
- * build. Rows keep their column order; FP64 and FP32 copies are kept. */
+ * 115-128, cuda/cudacsrmatrixinterface.cc:119-141,176-230). B = 1..4
+ * components per node (ncomp; Stokes in 2D is B = 3). Rows keep their column
+ * order; FP64 and FP32 copies are kept. */
 int gb_level_set_matrix(gb_ctx* ctx, int level, int64_t n, int B,
                         const int64_t* rowptr, const int64_t* col,
                         const int64_t* diag, const double* val);
@@ -121,6 +124,22 @@ int gb_level_set_transfer(gb_ctx* ctx, int level, int64_t ncoarse,
                           const int64_t* achter);
 int gb_level_size(const gb_ctx* ctx, int level, int64_t* n, int* B,
                   int64_t* nnzb);
+/* Vanka patches of a level: npatch lists of npp node indices (npp <= 27), as
+ * DofHandler::GetElement(2, p) returns them (DofHandler/dofhandler.h:389-396;
+ * patchlevel 2 in VankaSmoother::ConstructStructure,
+ * LinAlg/vankasmoother.cc:7-63). The patch matrices are copied from the
+ * level matrix and LU-factorised (copy_entries_sparseblockmatrix, :65-113)
+ * when a solve first needs them after a matrix or patch upload. */
+int gb_level_set_patches(gb_ctx* ctx, int level, int64_t npatch, int npp,
+                         const int64_t* patches);
+/* Pressure filter of a level (PressureFilter, Discretization/Q1/
+ * pressurefilter.h:31-54; set up by StdSolver::NewMesh ->
+ * CGDisc::InitFilter, Solver/stdsolver.cc:214-227, DofHandler/cgdisc.h:
+ * 1061-1090): the filtered components (bit mask, 0 = off), the weights (per
+ * node, the integral of its basis function), the domain size and the number of
+ * hanging nodes. */
+int gb_level_set_pfilter(gb_ctx* ctx, int level, int comp_mask,
+                         const double* weights, double domain, int64_t nhanging);
 
 /* ---- vectors -------------------------------------------------------------
  * Replaces CudaVectorInterface (cuda/cudavectorinterface.h:33-83) and
@@ -145,15 +164,29 @@ int gb_vmulteq(gb_ctx* ctx, int level, int y, int x, double d);
 /* y += d A^T x: the transposed operator SparseBlockMatrix::transpose builds
  * (LinAlg/sparseblockmatrix.xx:478-491), applied without transposing. */
 int gb_vmult_transpose(gb_ctx* ctx, int level, int y, int x, double d);
-/* y = b - A x: StdSolver::MatrixResidual (Solver/stdsolver.cc:783-791). */
+/* y = b - A x, then SubtractMeanAlgebraic(y): StdSolver::MatrixResidual
+ * (Solver/stdsolver.cc:783-791). */
 int gb_matrix_residual(gb_ctx* ctx, int level, int y, int x, int b);
 /* y = b - A x, Dirichlet-zeroed: StdSolver::residualgmres
  * (Solver/stdsolver.cc:742-754). */
 int gb_residualgmres(gb_ctx* ctx, int level, int y, int x, int b);
 /* niter damped-Jacobi sweeps x += omega D^-1 (y - A x): StdSolver::smooth with
  * linear_smooth jacobi (Solver/stdsolver.cc:951-986), CudaSolver::smooth
- * (cuda/cudasolver.cc:345-374). h is work space, as in the reference. */
+ * (cuda/cudasolver.cc:345-374). h is work space, as in the reference. With a
+ * pressure filter each sweep filters the residual (SubtractMeanAlgebraic)
+ * and x (SubtractMean), as the reference does. */
 int gb_smooth_jacobi(gb_ctx* ctx, int level, int niter, int x, int y, int h);
+/* The same with linear_smooth ilu on matrixtype vanka: each sweep
+ * h = VankaSmoother::solve(y - A x) (LinAlg/vankasmoother.cc:192-237),
+ * x += omega h. Needs the level's patches. */
+int gb_smooth_vanka(gb_ctx* ctx, int level, int niter, int x, int y, int h);
+/* StdSolver::smooth with the smoother of gb_params.smoother. */
+int gb_smooth(gb_ctx* ctx, int level, int niter, int x, int y, int h);
+/* StdSolver::SubtractMean / SubtractMeanAlgebraic (Solver/stdsolver.cc:
+ * 1736-1762): remove the weighted (integral) or plain mean of every filtered
+ * component; no-ops without a pressure filter. */
+int gb_subtract_mean(gb_ctx* ctx, int level, int id);
+int gb_subtract_mean_algebraic(gb_ctx* ctx, int level, int id);
 /* u = 0 on Dirichlet dofs: StdSolver::SetBoundaryVectorZero
  * (Solver/stdsolver.cc:795-812). */
 int gb_dirichlet_zero(gb_ctx* ctx, int level, int id);

@@ -189,6 +189,12 @@ class Oracle:
                                 _pd(np.ascontiguousarray(coarse, dtype=np.float64)))
         return fine
 
+    def subtract_mean(self, level, u, algebraic=False):
+        u = np.array(u, dtype=np.float64)
+        f = lib().or_subtract_mean_algebraic if algebraic else lib().or_subtract_mean
+        f(C.byref(self.levels[level]), _pd(u))
+        return u
+
     def dirichlet_zero(self, level, u):
         u = np.array(u, dtype=np.float64)
         lib().or_dirichlet_zero(C.byref(self.levels[level]), _pd(u))

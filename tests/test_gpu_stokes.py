@@ -1,0 +1,118 @@
+"""Block systems on the GPU (Stokes, ncomp = dim + 1): block SpMV, block
+Jacobi, Vanka, the pressure filter, block transfers and the solvers, against
+the oracle and the reference's golden Stokes fixtures."""
+import numpy as np
+import pytest
+
+from _util import golden_stokes_cases, load_golden, rel, rel_l2, solver_keys
+from gascoignelib_b200.native import GB_FP32, GB_FP64
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(ctx, name):
+    P, ref = load_golden(name)
+    keys = ref["keys"]
+    ctx.load_problem(P)
+    ctx.set_params(**solver_keys(keys), gmressize=int(keys["gmressize"]),
+                   tol=float(keys["tol"]), globaltol=1e-16, maxiter=200)
+    return P, ref, keys
+
+
+@pytest.mark.parametrize("name", golden_stokes_cases())
+def test_block_operators_match_oracle(ctx, name):
+    P, ref, keys = _setup(ctx, name)
+    O = Oracle(P, **solver_keys(keys))
+    rng = np.random.default_rng(4)
+    for l in range(P.nlevels):
+        lv = P.levels[l]
+        n = lv.ndof
+        xv, bv = rng.normal(size=n), rng.normal(size=n)
+        x, y, b = ctx.vec(), ctx.vec(), ctx.vec()
+        ctx.upload(l, x, xv)
+        ctx.upload(l, b, bv)
+        ctx.zero(l, y)
+        ctx.vmult(l, y, x, 1.0)
+        assert rel(ctx.download(l, y), O.vmult(l, np.zeros(n), xv)) < 1e-13
+        # MatrixResidual with SubtractMeanAlgebraic
+        ctx.matrix_residual(l, y, x, b)
+        assert rel(ctx.download(l, y), O.matrix_residual(l, xv, bv)) < 1e-12
+        # inverse diagonal blocks: NodeMatrix::gauss_jordan, bit for bit
+        assert np.array_equal(ctx.inverse_diagonal(l), O.blockdiag_inverse(l))
+        # pressure filter
+        ctx.upload(l, y, xv)
+        ctx.subtract_mean(l, y)
+        assert rel(ctx.download(l, y), O.subtract_mean(l, xv)) < 1e-13
+        ctx.upload(l, y, xv)
+        ctx.subtract_mean(l, y, algebraic=True)
+        assert rel(ctx.download(l, y), O.subtract_mean(l, xv, algebraic=True)) < 1e-13
+        if l > 0:
+            c = ctx.vec()
+            ctx.restrict_zero(l - 1, c, x)
+            assert np.array_equal(ctx.download(l - 1, c), O.restrict_zero(l - 1, xv))
+            cv = rng.normal(size=P.levels[l - 1].ndof)
+            ctx.upload(l - 1, c, cv)
+            ctx.upload(l, y, xv)
+            ctx.prolongate_add(l - 1, y, c)
+            assert np.array_equal(ctx.download(l, y), O.prolongate_add(l - 1, xv, cv))
+            ctx.free(c)
+        for v in (x, y, b):
+            ctx.free(v)
+
+
+@pytest.mark.parametrize("name", golden_stokes_cases())
+def test_smoother_sweeps_match_oracle(ctx, name):
+    """Vanka or block-Jacobi sweeps with the pressure filter, from a nonzero
+    start, within rounding of the oracle."""
+    P, ref, keys = _setup(ctx, name)
+    O = Oracle(P, **solver_keys(keys))
+    rng = np.random.default_rng(5)
+    for l in range(P.nlevels):
+        n = P.levels[l].ndof
+        xv, yv = rng.normal(size=n), rng.normal(size=n)
+        x, y, h = ctx.vec(), ctx.vec(), ctx.vec()
+        ctx.upload(l, x, xv)
+        ctx.upload(l, y, yv)
+        ctx.smooth(l, 3, x, y, h)
+        assert rel(ctx.download(l, x), O.smooth(l, 3, xv, yv)) < 1e-11
+        for v in (x, y, h):
+            ctx.free(v)
+
+
+@pytest.mark.parametrize("name", golden_stokes_cases())
+def test_stokes_gmres_matches_reference(ctx, name):
+    P, ref, keys = _setup(ctx, name)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    info = ctx.gmres(x, b)
+    u = ctx.download(l, x)
+    assert info["status_name"] == "converged"
+    assert abs(info["iterations"] - ref["iterations"]) <= 1
+    assert rel_l2(u, ref["solution"]) < 1e-8
+    ctx.free(x)
+    ctx.free(b)
+
+
+@pytest.mark.parametrize("prec", [GB_FP64, GB_FP32])
+@pytest.mark.parametrize("name", golden_stokes_cases())
+def test_stokes_flexible_gmres(ctx, name, prec):
+    """Flexible GMRES with an FP64 or FP32 Vanka/Jacobi cycle: true residual
+    at tol and the reference's solution (its pressure mean fixed by the
+    filter) within the solve tolerance."""
+    P, ref, keys = _setup(ctx, name)
+    ctx.set_params(**solver_keys(keys), gmressize=int(keys["gmressize"]), tol=1e-10,
+                   globaltol=1e-300, maxiter=300)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    info = ctx.fgmres(x, b, prec)
+    u = ctx.download(l, x)
+    assert info["status_name"] == "converged"
+    assert info["true_rel_residual"] <= 1e-10
+    O = Oracle(P, **solver_keys(keys))
+    r = O.matrix_residual(l, u, P.rhs)
+    assert rel_l2(u, ref["solution"]) < 1e-6
+    ctx.free(x)
+    ctx.free(b)
