@@ -369,3 +369,129 @@ def seeded_inputs(dim: int, coarse: int, refine: int, kappa_seed: int = 1001,
     kappa = np.exp(np.random.default_rng(kappa_seed).normal(0.0, sigma, size=Nf ** dim))
     rhs = np.random.default_rng(rhs_seed).uniform(-1.0, 1.0, size=(Nf + 1) ** dim)
     return kappa, rhs
+
+
+# ------------------------------------------------------------------ Stokes
+
+def _q1_local_derivative_mass(dim: int, h: float):
+    """D[i][a, b] = integral of (d phi_b / d x_i) phi_a over a cube of width h
+    (local order as _q1_local_stiffness)."""
+    m = np.array([[1.0 / 3.0, 1.0 / 6.0], [1.0 / 6.0, 1.0 / 3.0]]) * h
+    d = np.array([[-0.5, 0.5], [-0.5, 0.5]])
+    if dim == 2:
+        return [np.kron(m, d), np.kron(d, m)]
+    return [np.kron(np.kron(m, m), d), np.kron(np.kron(m, d), m), np.kron(np.kron(d, m), m)]
+
+
+def _stokes_local(dim: int, h: float, visc: float, stab: float) -> np.ndarray:
+    """Element blocks E[a, b] ((dim+1) x (dim+1)) of the Stokes system in the
+    reference's NavierStokes component order (0 = p, 1..dim = velocity):
+    div v tested with q, Brezzi-Pitkaranta stab h^2 grad p . grad q,
+    visc grad v_i . grad w_i and -p div w."""
+    K = _q1_local_stiffness(dim, h)
+    D = _q1_local_derivative_mass(dim, h)
+    nl, B = 2 ** dim, dim + 1
+    E = np.zeros((nl, nl, B, B))
+    E[:, :, 0, 0] = stab * h * h * K
+    for i in range(dim):
+        E[:, :, 0, i + 1] = D[i]
+        E[:, :, i + 1, i + 1] = visc * K
+        E[:, :, i + 1, 0] = -D[i].T
+    return E
+
+
+def _patches(dim: int, N: int) -> np.ndarray:
+    """Patches of 2^dim cells (3^dim nodes, local order lexicographic) of the
+    N^dim lexicographic mesh, patches in lexicographic order."""
+    n1, P = N + 1, N // 2
+    loc = np.array([(a * n1 + b) * n1 + e for a in range(3) for b in range(3)
+                    for e in range(3)]) if dim == 3 else \
+        np.array([b * n1 + e for b in range(3) for e in range(3)])
+    if dim == 3:
+        k, j, i = np.meshgrid(np.arange(P), np.arange(P), np.arange(P), indexing="ij")
+        base = ((2 * k * n1 + 2 * j) * n1 + 2 * i).ravel()
+    else:
+        j, i = np.meshgrid(np.arange(P), np.arange(P), indexing="ij")
+        base = (2 * j * n1 + 2 * i).ravel()
+    return (base[:, None] + loc[None, :]).astype(np.int64)
+
+
+def _assemble_stokes_level(dim: int, N: int, visc: float, stab: float) -> Level:
+    import scipy.sparse as sp
+    h = 1.0 / N
+    n1 = N + 1
+    n = n1 ** dim
+    B = dim + 1
+    E = _stokes_local(dim, h, visc, stab)
+    nodes = cell_nodes(dim, N)
+    nl = nodes.shape[1]
+    rows = np.repeat(nodes, nl, axis=1).ravel()
+    cols = np.tile(nodes, (1, nl)).ravel()
+    comp = []
+    for r in range(B):
+        for c in range(B):
+            vals = np.tile(E[:, :, r, c].ravel(), nodes.shape[0])
+            A = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+            A.sum_duplicates()
+            A.sort_indices()
+            comp.append(A)
+    rowptr = comp[0].indptr.astype(np.int64)
+    col = comp[0].indices.astype(np.int64)
+    for A in comp[1:]:
+        assert np.array_equal(A.indptr, comp[0].indptr)
+        assert np.array_equal(A.indices, comp[0].indices)
+    val = np.stack([A.data for A in comp], axis=1).reshape(-1, B, B).copy()
+    idx = np.arange(n)
+    coords = [(idx // n1 ** d) % n1 for d in range(dim)]
+    onb = np.zeros(n, dtype=bool)
+    for c in coords:
+        onb |= (c == 0) | (c == N)
+    rowidx = np.repeat(np.arange(n), np.diff(rowptr))
+    for c in range(1, B):  # velocity: strong Dirichlet rows and columns
+        val[onb[rowidx], c, :] = 0.0
+        val[onb[col], :, c] = 0.0
+    isdiag = rowidx == col
+    for c in range(1, B):
+        val[isdiag & onb[rowidx], c, c] = 1.0
+    diag = np.nonzero(isdiag)[0].astype(np.int64)
+    # pressure filter weights: integral of each basis function
+    w = np.zeros(n)
+    np.add.at(w, nodes.ravel(), h ** dim / nl)
+    lv = Level(n=n, B=B, rowptr=rowptr, col=col, diag=diag, val=val.ravel(),
+               dirichlet=np.nonzero(onb)[0].astype(np.int64),
+               dircomp_mask=sum(1 << c for c in range(1, B)),
+               coord=np.stack([c * h for c in coords], axis=1).astype(np.float64),
+               pf_mask=1, pf_weights=w, pf_domain=1.0, patches=_patches(dim, N))
+    return lv
+
+
+def stokes_rhs(dim: int, coarse: int, refine: int, seed: int = 1002) -> np.ndarray:
+    """f ~ U[-1, 1] per node and component (p, v_1..v_dim), the pressure part
+    made algebraically mean-free so that the system, whose pressure is fixed
+    only up to a constant, is consistent."""
+    n1 = (coarse << refine) + 1
+    r = np.random.default_rng(seed).uniform(-1.0, 1.0, size=(n1 ** dim, dim + 1))
+    r[:, 0] -= r[:, 0].mean()
+    return r.ravel()
+
+
+def structured_stokes(dim: int, coarse: int, refine: int, visc: float = 1.0,
+                      stab: float = 0.1, rhs: Optional[np.ndarray] = None,
+                      smoother: str = "vanka") -> Problem:
+    """The reference's multilevel Stokes system (Q1/Q1, Brezzi-Pitkaranta
+    pressure stabilisation, velocity Dirichlet on the whole boundary, pressure
+    filter on component 0, Vanka patches of 2^dim cells) on the unit
+    square/cube in lexicographic numbering: what the oracle harness assembles
+    with problem=stokes, in another node order."""
+    nlev = refine
+    levels = [_assemble_stokes_level(dim, (2 * coarse) << l, visc, stab)
+              for l in range(nlev)]
+    transfers = [_structured_transfer(dim, (2 * coarse) << l) for l in range(nlev - 1)]
+    b = stokes_rhs(dim, coarse, refine) if rhs is None else np.array(rhs, dtype=np.float64)
+    fin = levels[-1]
+    bd = b.reshape(fin.n, fin.B)
+    bd[fin.dirichlet, 1:] = 0.0
+    return Problem(dim=dim, levels=levels, transfers=transfers, rhs=bd.ravel(),
+                   info={"generator": "structured-stokes", "coarse": coarse,
+                         "refine": refine, "smoother": smoother, "visc": visc,
+                         "stab": stab})

@@ -116,3 +116,32 @@ def test_stokes_flexible_gmres(ctx, name, prec):
     assert rel_l2(u, ref["solution"]) < 1e-6
     ctx.free(x)
     ctx.free(b)
+
+
+def test_c3_stokes_vanka_full_size(ctx):
+    """C3 shape: 512^2 Q1/Q1 Stokes (789,507 dofs), Vanka V(2,2), GMRES(30):
+    reference-semantics FP64 solve against the oracle (iterations +-1, 1e-8),
+    then the mixed solve (FP32 Vanka cycle) to a true residual of 1e-8."""
+    from gascoignelib_b200.problem import structured_stokes
+    P = structured_stokes(2, 2, 8)
+    assert P.finest.ndof == 789507
+    O = Oracle(P, omega=1.0)
+    xo, io = O.gmres(vmax=31, tol=1e-8, maxiter=200)
+    O.close()
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=31, tol=1e-8, globaltol=1e-16, maxiter=200, omega=1.0)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    info = ctx.gmres(x, b)
+    assert info["status_name"] == "converged"
+    assert abs(info["iterations"] - io["iterations"]) <= 1
+    assert rel_l2(ctx.download(l, x), xo) < 1e-8
+    ctx.set_params(gmressize=31, tol=1e-8, globaltol=1e-300, maxiter=300, omega=1.0)
+    for prec in (GB_FP32, GB_FP64):
+        info = ctx.fgmres(x, b, prec)
+        assert info["status_name"] == "converged"
+        assert info["true_rel_residual"] <= 1e-8
+        assert rel_l2(ctx.download(l, x), xo) < 1e-5
+    ctx.free(x)
+    ctx.free(b)

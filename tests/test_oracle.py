@@ -153,3 +153,39 @@ def test_oracle_maxiter_stops():
     P = structured_problem(2, 2, 4, kappa, rhs)
     x, info = Oracle(P).gmres(vmax=21, tol=1e-14, maxiter=3)
     assert info["status"] == "too many iterations" and info["iterations"] == 4
+
+
+@pytest.mark.parametrize("name", ["stokes_2d_c2_r4_vanka", "stokes_3d_c1_r3_vanka"])
+def test_structured_stokes_matches_reference_assembly(name):
+    """problem.structured_stokes (lexicographic numbering) builds the
+    reference's Stokes matrices, Dirichlet masks, pressure-filter weights and
+    Vanka patches."""
+    from gascoignelib_b200.problem import structured_stokes
+    P, ref = load_golden(name)
+    keys = ref["keys"]
+    S = structured_stokes(P.dim, int(keys["coarse"]), int(keys["refine"]))
+    assert S.nlevels == P.nlevels
+    for Lr, Ls in zip(P.levels, S.levels):
+        N = round(Ls.n ** (1.0 / P.dim)) - 1
+        perm = _lex_permutation(Lr, N, P.dim)
+        B = Ls.B
+        assert Lr.B == B and Lr.dircomp_mask == Ls.dircomp_mask
+        # same blocks at the same (row, col) node pairs
+        kr = perm[np.repeat(np.arange(Lr.n), np.diff(Lr.rowptr))] * Lr.n + perm[Lr.col]
+        ks = np.repeat(np.arange(Ls.n), np.diff(Ls.rowptr)) * Ls.n + Ls.col
+        orr, oss = np.argsort(kr), np.argsort(ks)
+        assert np.array_equal(kr[orr], ks[oss])
+        vr = Lr.val.reshape(-1, B, B)[orr]
+        vs = Ls.val.reshape(-1, B, B)[oss]
+        assert np.abs(vr - vs).max() <= 1e-13 * np.abs(vr).max()
+        w = np.empty(Lr.n)
+        w[perm] = Lr.pf_weights
+        assert np.abs(w - Ls.pf_weights).max() <= 1e-15
+        assert Lr.pf_domain == pytest.approx(Ls.pf_domain, rel=1e-14)
+        assert {tuple(sorted(perm[p])) for p in Lr.patches} == \
+            {tuple(sorted(p)) for p in Ls.patches}
+        dr = np.zeros(Lr.n, bool)
+        dr[perm[Lr.dirichlet]] = True
+        ds = np.zeros(Ls.n, bool)
+        ds[Ls.dirichlet] = True
+        assert np.array_equal(dr, ds)
