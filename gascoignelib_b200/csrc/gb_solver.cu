@@ -669,11 +669,16 @@ ensure_AT(Context& c, Level& L)
 {
   if (L.has_AT)
     return;
-  GB_REQUIRE(L.B == 1, GB_EINVAL,
-             "the transposed operator is available for block size 1 only");
+  const int B = L.B, B2 = B * B;
   const int64_t n = L.n, nnz = L.h_rowptr[n];
   std::vector<int64_t> tp(n + 1, 0), tc(nnz);
-  std::vector<double> tv(nnz);
+  std::vector<double> tv(nnz * B2);
+  // block (j, i) of A, transposed, as block (i, j) of A^T
+  auto put = [&](int64_t dst, int64_t src) {
+    for (int r = 0; r < B; ++r)
+      for (int q = 0; q < B; ++q)
+        tv[dst * B2 + r * B + q] = L.h_val[src * B2 + q * B + r];
+  };
   bool symmetric = true;
   for (int64_t i = 0; i < n && symmetric; ++i)
     for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k) {
@@ -685,7 +690,7 @@ ensure_AT(Context& c, Level& L)
         symmetric = false;
         break;
       }
-      tv[k] = L.h_val[L.h_rowptr[j] + (f - b)];
+      put(k, L.h_rowptr[j] + (f - b));
     }
   if (symmetric) {
     tp = L.h_rowptr;
@@ -700,11 +705,11 @@ ensure_AT(Context& c, Level& L)
       for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k) {
         int64_t q = pos[L.h_col[k]]++;
         tc[q] = i;
-        tv[q] = L.h_val[k];
+        put(q, k);
       }
   }
   GB_CUDA(cudaStreamSynchronize(c.stream));
-  build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), c.stream);
+  build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), c.stream, B);
   L.has_AT = true;
 }
 
@@ -2065,8 +2070,11 @@ with_transposed(gb_ctx* ctx, F f)
   const int saved = ctx->transposed;
   if (!saved) {
     for (auto& L : ctx->L)
-      if (L.has_matrix)
+      if (L.has_matrix) {
+        GB_REQUIRE(L.B == 1, GB_EINVAL,
+                   "the transposed solver operators need block size 1");
         gb::ensure_AT(*ctx, L);
+      }
     ctx->transposed = 1;
   }
   struct Restore
@@ -2900,8 +2908,11 @@ gb_set_operator(gb_ctx* ctx, int transposed)
   GB_REQUIRE(transposed == 0 || transposed == 1, GB_EINVAL, "transposed must be 0 or 1");
   if (transposed)
     for (auto& L : ctx->L)
-      if (L.has_matrix)
+      if (L.has_matrix) {
+        GB_REQUIRE(L.B == 1, GB_EINVAL,
+                   "the transposed solver operators need block size 1");
         ensure_AT(*ctx, L);
+      }
   ctx->transposed = transposed;
   GB_API_END
 }

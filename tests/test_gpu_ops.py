@@ -70,8 +70,9 @@ def test_residuals_and_dirichlet(ctx, loaded):
         ctx.matrix_residual(l, y, x, b)
         r = O.matrix_residual(l, xv, bv)
         assert rel(ctx.download(l, y), r) < 1e-13
+        # residualgmres: b - A x, Dirichlet-zeroed, no pressure filter
         ctx.residualgmres(l, y, x, b)
-        assert rel(ctx.download(l, y), O.dirichlet_zero(l, r)) < 1e-13
+        assert rel(ctx.download(l, y), O.dirichlet_zero(l, O.vmult(l, bv, xv, -1.0))) < 1e-13
         ctx.dirichlet_zero(l, x)
         assert np.array_equal(ctx.download(l, x), O.dirichlet_zero(l, xv))
     for v in (x, b, y):
@@ -84,7 +85,9 @@ def test_inverse_diagonal_bitexact(ctx, loaded):
         assert np.array_equal(ctx.inverse_diagonal(l), O.blockdiag_inverse(l))
 
 
-def test_jacobi_smoothing(ctx, loaded):
+def test_smoothing(ctx, loaded):
+    """StdSolver::smooth with the problem's smoother (Jacobi, block Jacobi or
+    Vanka; with the pressure filter where the problem has one)."""
     P, keys, O = loaded
     rng = np.random.default_rng(7)
     x, y, h = ctx.vec(), ctx.vec(), ctx.vec()
@@ -94,8 +97,8 @@ def test_jacobi_smoothing(ctx, loaded):
         for niter in (1, 2, 3):
             ctx.upload(l, x, xv)
             ctx.upload(l, y, yv)
-            ctx.smooth_jacobi(l, niter, x, y, h)
-            assert rel(ctx.download(l, x), O.smooth(l, niter, xv, yv)) < 1e-12
+            ctx.smooth(l, niter, x, y, h)
+            assert rel(ctx.download(l, x), O.smooth(l, niter, xv, yv)) < 1e-11
     for v in (x, y, h):
         ctx.free(v)
 
@@ -158,7 +161,8 @@ def test_one_cycle_fp64_and_fp32(ctx, loaded):
         assert rel(ctx.download(l, x), ref) < 1e-11
         ctx.upload(l, x, x0)
         ctx.precondition(x, y, GB_FP32)
-        assert rel(ctx.download(l, x), ref) < 2e-5
+        # FP32 cycle: FP32 rounding, amplified by the local LU solves of Vanka
+        assert rel(ctx.download(l, x), ref) < (2e-5 if P.finest.B == 1 else 2e-4)
     ctx.free(x)
     ctx.free(y)
 
