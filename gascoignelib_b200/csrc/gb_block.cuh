@@ -88,31 +88,133 @@ k_bspmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
   }
 }
 
-// u = (u_zero ? 0 : u) + omega * (D^-1 h) per node: SparseBlockMatrix::Jacobi
-// (LinAlg/sparseblockmatrix.xx:47-56) followed by Add(x, omega, h).
-template<int B, class TV, class T>
-__global__ void
-k_block_jacobi_apply(int n, const TV* __restrict__ dinv, const T* __restrict__ h,
-                     T* __restrict__ u, double omega, int u_zero)
+// y = b - A x on block rows with the pressure filter's plain mean of
+// component pc of y (StdSolver::MatrixResidual with SubtractMeanAlgebraic):
+// the last block writes sum / denom to *mean; consumers subtract it on read.
+template<int B, class TV, class T, bool PAT>
+__global__ void __launch_bounds__(kSpmvThreads)
+k_bspmv_resid_mean(SellView<TV> A, const T* __restrict__ x, T* __restrict__ y,
+                   const T* __restrict__ b, int pc, double denom, double* partials,
+                   unsigned* ticket, double* mean)
 {
   GB_PDL_ENTRY();
   using TA = typename Acc<TV, T>::type;
+  constexpr int B2 = B * B;
+  __shared__ double sh[32];
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (row < A.n) {
+    const int s = row >> 5, lane = row & 31;
+    const int beg = A.sptr[s];
+    const int w = (A.sptr[s + 1] - beg) >> 5;
+    const TV* vp = A.val + int64_t(beg) * B2 + lane;
+    const int* cp = PAT ? (A.ptab + int(A.pid[row]) * A.W) : (A.col + beg + lane);
+    TA acc[B];
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+      acc[r] = static_cast<TA>(b[int64_t(row) * B + r]);
+#pragma unroll 2
+    for (int j = 0; j < w; ++j) {
+      const int c = PAT ? row + ldg(cp + j) : ldg(cp + j * kSlice);
+      TA xv[B], m[B2];
+#pragma unroll
+      for (int k = 0; k < B; ++k)
+        xv[k] = static_cast<TA>(ldg(x + int64_t(c) * B + k));
+#pragma unroll
+      for (int q = 0; q < B2; ++q)
+        m[q] = static_cast<TA>(ldg(vp + int64_t(j) * kSlice * B2 + q * kSlice));
+#pragma unroll
+      for (int r = 0; r < B; ++r) {
+        TA sum = TA(0);
+#pragma unroll
+        for (int k = 0; k < B; ++k)
+          sum = fma(m[r * B + k], xv[k], sum);
+        acc[r] = acc[r] - sum;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < B; ++r) {
+      const T o = static_cast<T>(acc[r]);
+      y[int64_t(row) * B + r] = o;
+      if (r == pc)
+        v = static_cast<double>(o);
+    }
+  }
+  v = block_sum(v, sh);
+  red_finish(partials, ticket, v, RedOut{ mean, nullptr, nullptr, 0, denom }, sh);
+}
+
+// Plain or weighted mean of component pc (no subtraction): *mean =
+// (sum_j x(j, pc) [* w_j]) / denom.
+template<class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_comp_mean(int n, int B, int pc, const T* __restrict__ x, const double* __restrict__ w,
+            double denom, double* partials, unsigned* ticket, double* mean)
+{
+  GB_PDL_ENTRY();
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const double xv = static_cast<double>(x[int64_t(j) * B + pc]);
+    v = w ? fma(xv, w[j], v) : v + xv;
+  }
+  v = block_sum(v, sh);
+  red_finish(partials, ticket, v, RedOut{ mean, nullptr, nullptr, 0, denom }, sh);
+}
+
+// u = (u_zero ? 0 : u) + omega * (D^-1 h) per node: SparseBlockMatrix::Jacobi
+// (LinAlg/sparseblockmatrix.xx:47-56) followed by Add(x, omega, h).
+// Pressure filter around it (pc >= 0): h's component pc is read minus *hmean
+// (its algebraic mean, when hmean is set), and the weighted mean of the new
+// u's component pc is reduced into *umean (sum of u(j, pc) w_j / domain) when
+// w is set.
+struct PfArgs
+{
+  int pc;              // filtered component, -1: none
+  const double* hmean; // subtract from h(., pc) on read, or null
+  const double* w;     // weights for the mean of the result, or null
+  double domain;
+  double* partials;
+  unsigned* ticket;
+  double* umean;
+};
+
+template<int B, class TV, class T>
+__global__ void __launch_bounds__(256)
+k_block_jacobi_apply(int n, const TV* __restrict__ dinv, const T* __restrict__ h,
+                     T* __restrict__ u, double omega, int u_zero, PfArgs pf)
+{
+  GB_PDL_ENTRY();
+  using TA = typename Acc<TV, T>::type;
+  __shared__ double sh[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n)
-    return;
-  const int64_t o = int64_t(i) * B;
-  TA t[B];
-#pragma unroll
-  for (int k = 0; k < B; ++k)
-    t[k] = static_cast<TA>(h[o + k]);
-#pragma unroll
-  for (int r = 0; r < B; ++r) {
-    TA v = TA(0);
+  double wv = 0.0;
+  if (i < n) {
+    const int64_t o = int64_t(i) * B;
+    const double hm = pf.hmean ? *pf.hmean : 0.0;
+    TA t[B];
 #pragma unroll
     for (int k = 0; k < B; ++k)
-      v = fma(static_cast<TA>(dinv[o * B + r * B + k]), t[k], v);
-    const TA base = u_zero ? TA(0) : static_cast<TA>(u[o + r]);
-    u[o + r] = static_cast<T>(base + static_cast<TA>(omega) * v);
+      t[k] = (pf.hmean && k == pf.pc)
+               ? static_cast<TA>(static_cast<double>(h[o + k]) - hm)
+               : static_cast<TA>(h[o + k]);
+#pragma unroll
+    for (int r = 0; r < B; ++r) {
+      TA v = TA(0);
+#pragma unroll
+      for (int k = 0; k < B; ++k)
+        v = fma(static_cast<TA>(dinv[o * B + r * B + k]), t[k], v);
+      const TA base = u_zero ? TA(0) : static_cast<TA>(u[o + r]);
+      const T un = static_cast<T>(base + static_cast<TA>(omega) * v);
+      u[o + r] = un;
+      if (pf.w && r == pf.pc)
+        wv = static_cast<double>(un) * pf.w[i];
+    }
+  }
+  if (pf.w) {
+    wv = block_sum(wv, sh);
+    red_finish(pf.partials, pf.ticket, wv, RedOut{ pf.umean, nullptr, nullptr, 0, pf.domain },
+               sh);
   }
 }
 
@@ -123,7 +225,8 @@ k_block_jacobi_apply(int n, const TV* __restrict__ dinv, const T* __restrict__ h
 template<class T, int B>
 __device__ __forceinline__ void
 transfer_row_b(const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
-               const T* __restrict__ src, int i, T (&acc)[B])
+               const T* __restrict__ src, int i, T (&acc)[B], int pc = -1,
+               double smean = 0.0)
 {
   const int beg = __ldg(tsp + (i >> 5));
   const int w = (__ldg(tsp + (i >> 5) + 1) - beg) >> 5;
@@ -133,16 +236,22 @@ transfer_row_b(const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
     const T wgt = wcode<T>(e);
     const T* sp = src + int64_t(e & kIdxMask) * B;
 #pragma unroll
-    for (int c = 0; c < B; ++c)
-      acc[c] = fma(wgt, __ldg(sp + c), acc[c]);
+    for (int c = 0; c < B; ++c) {
+      const T sv = c == pc ? static_cast<T>(static_cast<double>(__ldg(sp + c)) - smean)
+                           : __ldg(sp + c);
+      acc[c] = fma(wgt, sv, acc[c]);
+    }
   }
 }
 
+// fine's component pc is read minus *smean when smean is set (the filtered
+// residual of MatrixResidual, restricted).
 template<class T, int B>
 __global__ void
 k_restrict_b(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
              const T* __restrict__ fine, T* __restrict__ coarse,
-             const uint8_t* __restrict__ cdir)
+             const uint8_t* __restrict__ cdir, int pc = -1,
+             const double* __restrict__ smean = nullptr)
 {
   GB_PDL_ENTRY();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -152,7 +261,7 @@ k_restrict_b(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ t
 #pragma unroll
   for (int c = 0; c < B; ++c)
     acc[c] = T(0);
-  transfer_row_b<T, B>(tsp, tent, fine, i, acc);
+  transfer_row_b<T, B>(tsp, tent, fine, i, acc, smean ? pc : -1, smean ? *smean : 0.0);
 #pragma unroll
   for (int c = 0; c < B; ++c) {
     const int64_t d = int64_t(i) * B + c;
@@ -229,100 +338,55 @@ k_comp_sub(int n, int B, int c, T* __restrict__ x, const double* __restrict__ su
 // patch order (the reference's order on one thread), scales by 1/count and
 // adds omega times it to u (StdSolver::smooth's Add).
 //
-// Thread per patch (M = patch nodes * B <= 32): LU factors, pivots and
-// solutions stored entry-major ([entry][patch]) so that a warp's loads are
-// contiguous. The right-hand side is gathered through the row permutation,
-// then unit-lower forward and upper backward substitution, rows in order and
-// each row's sum in ascending column order (the triangular solves of the LU).
-template<int M, int B, class TL, class T>
-__global__ void __launch_bounds__(128)
-k_vanka_local(int npatch, const int* __restrict__ pn, const TL* __restrict__ lu,
-              const uint8_t* __restrict__ perm, const T* __restrict__ h,
-              T* __restrict__ hout)
-{
-  GB_PDL_ENTRY();
-  using TA = typename Acc<TL, T>::type;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= npatch)
-    return;
-  const int64_t np = npatch;
-  TA H[M];
-#pragma unroll
-  for (int i = 0; i < M; ++i) {
-    const int P = __ldg(perm + i * np + p);
-    const int node = __ldg(pn + (P / B) * np + p);
-    H[i] = static_cast<TA>(__ldg(h + int64_t(node) * B + (P % B)));
-  }
-#pragma unroll
-  for (int i = 1; i < M; ++i) {
-    TA s = H[i];
-#pragma unroll
-    for (int j = 0; j < i; ++j)
-      s -= static_cast<TA>(__ldg(lu + (i * M + j) * np + p)) * H[j];
-    H[i] = s;
-  }
-#pragma unroll
-  for (int i = M - 1; i >= 0; --i) {
-    TA s = H[i];
-#pragma unroll
-    for (int j = i + 1; j < M; ++j)
-      s -= static_cast<TA>(__ldg(lu + (i * M + j) * np + p)) * H[j];
-    H[i] = s / static_cast<TA>(__ldg(lu + (i * M + i) * np + p));
-  }
-#pragma unroll
-  for (int i = 0; i < M; ++i)
-    hout[i * np + p] = static_cast<T>(H[i]);
-}
-
-// Warp per patch (any M <= kVankaMaxM): factors patch-major ([patch][M*M]),
-// solutions patch-major ([patch][M]); each row's sum is split over the lanes
-// and reduced by shuffles.
+// The local solves apply each patch's inverse (formed once per assembly from
+// its LU factors): one warp per patch, lane i computing rows i, i+32, ..;
+// the inverse is stored transposed per patch ([patch][j][i]) so that for each
+// column j the warp's loads are contiguous; the patch's right-hand side
+// (component pc read minus *hmean when set) is staged in shared memory.
 constexpr int kVankaMaxM = 128;
 constexpr int kVankaWarps = 4;
 
-template<class TL, class T>
+template<int R, class TL, class T>
 __global__ void __launch_bounds__(32 * kVankaWarps)
-k_vanka_local_warp(int npatch, int M, int B, const int* __restrict__ pn,
-                   const TL* __restrict__ lu, const uint8_t* __restrict__ perm,
-                   const T* __restrict__ h, T* __restrict__ hout)
+k_vanka_inv(int npatch, int M, int B, const int* __restrict__ pn,
+            const TL* __restrict__ inv, const T* __restrict__ h, int pc,
+            const double* __restrict__ hmean, T* __restrict__ hout)
 {
   GB_PDL_ENTRY();
-  __shared__ double sH[kVankaWarps][kVankaMaxM];
+  using TA = typename Acc<TL, T>::type;
+  __shared__ TA sH[kVankaWarps][kVankaMaxM];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.x * kVankaWarps + wid;
   if (p >= npatch)
-    return;
+    return; // whole warp
   const int64_t np = npatch;
-  double* H = sH[wid];
-  const TL* L = lu + int64_t(p) * M * M;
+  TA* H = sH[wid];
+  const double hm = hmean ? *hmean : 0.0;
   for (int i = lane; i < M; i += 32) {
-    const int P = perm[int64_t(p) * M + i];
-    const int node = pn[(P / B) * np + p];
-    H[i] = static_cast<double>(h[int64_t(node) * B + (P % B)]);
+    const int r = i / B, c = i - r * B;
+    const int node = __ldg(pn + r * np + p);
+    const T hv = __ldg(h + int64_t(node) * B + c);
+    H[i] = (hmean && c == pc) ? static_cast<TA>(static_cast<double>(hv) - hm)
+                              : static_cast<TA>(hv);
   }
   __syncwarp();
-  for (int i = 1; i < M; ++i) {
-    double s = 0.0;
-    for (int j = lane; j < i; j += 32)
-      s = fma(static_cast<double>(L[i * M + j]), H[j], s);
-    for (int o = 16; o > 0; o >>= 1)
-      s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0)
-      H[i] -= s;
-    __syncwarp();
+  const TL* ip = inv + int64_t(p) * M * M + lane;
+  TA acc[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k)
+    acc[k] = TA(0);
+#pragma unroll 3
+  for (int j = 0; j < M; ++j) {
+    const TA hj = H[j];
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+      if (lane + 32 * k < M)
+        acc[k] = fma(static_cast<TA>(__ldg(ip + j * M + 32 * k)), hj, acc[k]);
   }
-  for (int i = M - 1; i >= 0; --i) {
-    double s = 0.0;
-    for (int j = i + 1 + lane; j < M; j += 32)
-      s = fma(static_cast<double>(L[i * M + j]), H[j], s);
-    for (int o = 16; o > 0; o >>= 1)
-      s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0)
-      H[i] = (H[i] - s) / static_cast<double>(L[i * M + i]);
-    __syncwarp();
-  }
-  for (int i = lane; i < M; i += 32)
-    hout[int64_t(p) * M + i] = static_cast<T>(H[i]);
+#pragma unroll
+  for (int k = 0; k < R; ++k)
+    if (lane + 32 * k < M)
+      hout[int64_t(p) * M + lane + 32 * k] = static_cast<T>(acc[k]);
 }
 
 // u(i, c) = (u_zero ? 0 : u(i, c)) + omega * ((sum over the node's patches of
@@ -330,34 +394,44 @@ k_vanka_local_warp(int npatch, int M, int B, const int* __restrict__ pn,
 // patch * 32 + r (npp <= 27). Solution (patch p, local dof q) at
 // hout[q * s1 + p * s2].
 template<int B, class T>
-__global__ void
+__global__ void __launch_bounds__(256)
 k_vanka_gather(int n, const int* __restrict__ nptr, const int* __restrict__ ent,
-               const T* __restrict__ hout, int64_t s1, int64_t s2, T* __restrict__ u,
-               double omega, int u_zero)
+               const T* __restrict__ hout, int M, T* __restrict__ u, double omega,
+               int u_zero, PfArgs pf)
 {
   GB_PDL_ENTRY();
   using TA = typename Acc<T, T>::type;
+  __shared__ double sh[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n)
-    return;
-  const int k0 = __ldg(nptr + i), k1 = __ldg(nptr + i + 1);
-  TA acc[B];
-#pragma unroll
-  for (int c = 0; c < B; ++c)
-    acc[c] = TA(0);
-  for (int k = k0; k < k1; ++k) {
-    const int e = __ldg(ent + k);
-    const int64_t p = e >> 5, r = e & 31;
+  double wv = 0.0;
+  if (i < n) {
+    const int k0 = __ldg(nptr + i), k1 = __ldg(nptr + i + 1);
+    TA acc[B];
 #pragma unroll
     for (int c = 0; c < B; ++c)
-      acc[c] += static_cast<TA>(hout[(r * B + c) * s1 + p * s2]);
-  }
-  const TA sc = TA(1) / static_cast<TA>(k1 - k0);
+      acc[c] = TA(0);
+    for (int k = k0; k < k1; ++k) {
+      const int e = __ldg(ent + k);
+      const int64_t p = e >> 5, r = e & 31;
 #pragma unroll
-  for (int c = 0; c < B; ++c) {
-    const int64_t d = int64_t(i) * B + c;
-    const TA base = u_zero ? TA(0) : static_cast<TA>(u[d]);
-    u[d] = static_cast<T>(base + static_cast<TA>(omega) * (acc[c] * sc));
+      for (int c = 0; c < B; ++c)
+        acc[c] += static_cast<TA>(hout[p * M + r * B + c]);
+    }
+    const TA sc = TA(1) / static_cast<TA>(k1 - k0);
+#pragma unroll
+    for (int c = 0; c < B; ++c) {
+      const int64_t d = int64_t(i) * B + c;
+      const TA base = u_zero ? TA(0) : static_cast<TA>(u[d]);
+      const T un = static_cast<T>(base + static_cast<TA>(omega) * (acc[c] * sc));
+      u[d] = un;
+      if (pf.w && c == pf.pc)
+        wv = static_cast<double>(un) * pf.w[i];
+    }
+  }
+  if (pf.w) {
+    wv = block_sum(wv, sh);
+    red_finish(pf.partials, pf.ticket, wv, RedOut{ pf.umean, nullptr, nullptr, 0, pf.domain },
+               sh);
   }
 }
 

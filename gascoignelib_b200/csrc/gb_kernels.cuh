@@ -387,6 +387,7 @@ struct RedOut
   double* accum;    // accum[0] += op(r)         (may be null)
   double* recip;    // recip[0] = 1 / op(r)      (may be null)
   int sqrt_result;  // op = sqrt when set
+  double div;       // op = r / div when nonzero (a mean)
 };
 
 __device__ __forceinline__ void
@@ -409,6 +410,8 @@ red_finish(double* partials, unsigned* ticket, double bsum, RedOut ro, double* s
   v = block_sum(v, sh);
   if (threadIdx.x == 0) {
     double r = ro.sqrt_result ? sqrt(v) : v;
+    if (ro.div != 0.0)
+      r = r / ro.div;
     if (ro.out)
       ro.out[0] = r;
     if (ro.accum)

@@ -286,11 +286,10 @@ struct Level
   // Vanka patches (gb_level_set_patches) and their factorisations
   std::vector<int64_t> h_patches;
   int npatch = 0, npp = 0, vk_M = 0;
-  bool vk_ready = false, vk_warp = false;
+  bool vk_ready = false;
   DeviceArray<int> vk_pn, vk_nptr, vk_ent;
-  DeviceArray<double> vk_lu64, vk_out64;
-  DeviceArray<float> vk_lu32, vk_out32;
-  DeviceArray<uint8_t> vk_perm;
+  DeviceArray<double> vk_inv64, vk_out64; // inverses [patch][j][i], solutions
+  DeviceArray<float> vk_inv32, vk_out32;
   int64_t ndof() const { return n * B; }
 };
 
@@ -358,6 +357,8 @@ struct gb_ctx
   gb::MgWork<float> w32;
   bool work_ready = false;
   gb::DeviceArray<double> partials;
+  gb::DeviceArray<double> pfpart;    // per-block sums of the fused filter reductions
+  gb::DeviceArray<unsigned> pfticket;
   gb::DeviceArray<unsigned> ticket;
   gb::DeviceArray<double> scal; // general device scalars
   gb::DeviceArray<gb::GmresDev> G;
@@ -715,14 +716,31 @@ ensure_AT(Context& c, Level& L)
 
 // ---------------------------------------------------------- level set-up
 
+// Per-block sums of the filter reductions fused into the residual and update
+// kernels (grid of blocks_for(n, 256) blocks on a level of n nodes).
+static void
+ensure_pf_scratch(Context& c, int64_t n)
+{
+  const size_t need = static_cast<size_t>((n + 255) / 256 + 1);
+  if (c.pfpart.n < need)
+    GB_CUDA(c.pfpart.alloc(need));
+  if (c.pfticket.n < 1) {
+    GB_CUDA(c.pfticket.alloc(1));
+    GB_CUDA(cudaMemsetAsync(c.pfticket.p, 0, sizeof(unsigned), c.stream));
+  }
+}
+
 // VankaSmoother::ConstructStructure + copy_entries (LinAlg/vankasmoother.cc:
 // 7-113) for one level: each patch's matrix (the level matrix's entries whose
 // row and column nodes both lie in the patch; node-major, components inside)
 // factorised on the host with row partial pivoting in the reference's
 // operation order (first row of largest |a_ik| as pivot, column divided by the
-// pivot, trailing entries updated k by k), uploaded in FP64 and FP32 with the
-// pivots, the patch node lists and, per node, the (patch, local node) pairs in
-// ascending patch order for the averaging gather.
+// pivot, trailing entries updated k by k). The device applies the inverse,
+// formed from these factors column by column (the LU solves of the unit
+// vectors), so a local solve is a dense product without dependency chains; it
+// agrees with the reference's LU solves to rounding. Uploaded in FP64 and FP32,
+// transposed per patch, with the patch node lists and, per node, the (patch,
+// local node) pairs in ascending patch order for the averaging gather.
 static void
 ensure_vanka(Context& c, Level& L)
 {
@@ -733,11 +751,9 @@ ensure_vanka(Context& c, Level& L)
   const int B = L.B, npp = L.npp, M = npp * B, B2 = B * B;
   GB_REQUIRE(M <= kVankaMaxM && npp <= 32, GB_EINVAL, "Vanka patch too large");
   const int64_t np = L.npatch;
-  const bool warp = M > 32;
-  std::vector<double> lu(size_t(np) * M * M);
-  std::vector<uint8_t> perm(size_t(np) * M);
+  std::vector<double> inv(size_t(np) * M * M);
   std::vector<int> pn(size_t(np) * npp);
-  std::vector<double> a(size_t(M) * M);
+  std::vector<double> a(size_t(M) * M), x(M);
   std::vector<int> pv(M);
   for (int64_t p = 0; p < np; ++p) {
     const int64_t* nodes = L.h_patches.data() + p * npp;
@@ -780,10 +796,24 @@ ensure_vanka(Context& c, Level& L)
         for (int i = k + 1; i < M; ++i)
           a[size_t(i) * M + j] -= a[size_t(i) * M + k] * a[size_t(k) * M + j];
     }
-    for (int e = 0; e < M * M; ++e)
-      lu[warp ? size_t(p) * M * M + e : size_t(e) * np + p] = a[e];
-    for (int i = 0; i < M; ++i)
-      perm[warp ? size_t(p) * M + i : size_t(i) * np + p] = static_cast<uint8_t>(pv[i]);
+    for (int j = 0; j < M; ++j) { // column j of the inverse: LU x = P e_j
+      for (int i = 0; i < M; ++i)
+        x[i] = pv[i] == j ? 1.0 : 0.0;
+      for (int i = 1; i < M; ++i) {
+        double sacc = x[i];
+        for (int q = 0; q < i; ++q)
+          sacc -= a[size_t(i) * M + q] * x[q];
+        x[i] = sacc;
+      }
+      for (int i = M - 1; i >= 0; --i) {
+        double sacc = x[i];
+        for (int q = i + 1; q < M; ++q)
+          sacc -= a[size_t(i) * M + q] * x[q];
+        x[i] = sacc / a[size_t(i) * M + i];
+      }
+      for (int i = 0; i < M; ++i)
+        inv[size_t(p) * M * M + size_t(j) * M + i] = x[i];
+    }
     for (int r = 0; r < npp; ++r)
       pn[size_t(r) * np + p] = static_cast<int>(nodes[r]);
   }
@@ -799,21 +829,19 @@ ensure_vanka(Context& c, Level& L)
   for (int64_t p = 0; p < np; ++p)
     for (int r = 0; r < npp; ++r)
       ent[fill[L.h_patches[p * npp + r]]++] = static_cast<int>(p * 32 + r);
-  std::vector<float> lu32(lu.begin(), lu.end());
+  std::vector<float> inv32(inv.begin(), inv.end());
   GB_CUDA(cudaStreamSynchronize(c.stream));
-  GB_CUDA(L.vk_lu64.alloc(lu.size()));
-  GB_CUDA(L.vk_lu32.alloc(lu.size()));
-  GB_CUDA(L.vk_perm.alloc(perm.size()));
+  GB_CUDA(L.vk_inv64.alloc(inv.size()));
+  GB_CUDA(L.vk_inv32.alloc(inv.size()));
   GB_CUDA(L.vk_pn.alloc(pn.size()));
   GB_CUDA(L.vk_nptr.alloc(nptr.size()));
   GB_CUDA(L.vk_ent.alloc(ent.size()));
   GB_CUDA(L.vk_out64.alloc(size_t(np) * M));
   GB_CUDA(L.vk_out32.alloc(size_t(np) * M));
-  GB_CUDA(cudaMemcpy(L.vk_lu64.p, lu.data(), lu.size() * sizeof(double),
+  GB_CUDA(cudaMemcpy(L.vk_inv64.p, inv.data(), inv.size() * sizeof(double),
                      cudaMemcpyHostToDevice));
-  GB_CUDA(cudaMemcpy(L.vk_lu32.p, lu32.data(), lu32.size() * sizeof(float),
+  GB_CUDA(cudaMemcpy(L.vk_inv32.p, inv32.data(), inv32.size() * sizeof(float),
                      cudaMemcpyHostToDevice));
-  GB_CUDA(cudaMemcpy(L.vk_perm.p, perm.data(), perm.size(), cudaMemcpyHostToDevice));
   GB_CUDA(cudaMemcpy(L.vk_pn.p, pn.data(), pn.size() * sizeof(int),
                      cudaMemcpyHostToDevice));
   GB_CUDA(cudaMemcpy(L.vk_nptr.p, nptr.data(), nptr.size() * sizeof(int),
@@ -821,7 +849,6 @@ ensure_vanka(Context& c, Level& L)
   GB_CUDA(cudaMemcpy(L.vk_ent.p, ent.data(), ent.size() * sizeof(int),
                      cudaMemcpyHostToDevice));
   L.vk_M = M;
-  L.vk_warp = warp;
   L.vk_ready = true;
 }
 
@@ -863,6 +890,8 @@ ensure_work(Context& c)
     for (int l = 0; l < c.nlevels; ++l)
       ensure_vanka(c, c.L[l]);
   }
+  for (int l = 0; l < c.nlevels; ++l)
+    ensure_pf_scratch(c, c.L[l].n);
   // the single-CTA coarse-level program covers scalar Jacobi cycles
   bool simple = c.params.smoother == 0;
   for (int l = 0; l < c.nlevels; ++l)
@@ -924,86 +953,161 @@ struct Emit
     else
       jacobi_apply(l, b, u, true);
   }
-  // u = (u_zero ? 0 : u) + omega D^-1 h (block Jacobi update, h given)
-  void jacobi_apply(int l, const T* h, T* u, bool u_zero)
+  // u = (u_zero ? 0 : u) + omega D^-1 h (block Jacobi update, h given;
+  // h's filtered component read minus *hmean when set; the weighted mean of
+  // the new u reduced into scal[9] when the level has one filtered component)
+  void jacobi_apply(int l, const T* h, T* u, bool u_zero, const double* hmean = nullptr)
   {
     const Level& L = c.L[l];
     no_rec();
+    PfArgs pf = weighted_mean_args(L);
+    pf.hmean = hmean;
     const int nb = blocks_for(L.n, 256);
     switch (L.B) {
       case 1:
         launch(c, k_block_jacobi_apply<1, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
-               c.params.omega, int(u_zero));
+               c.params.omega, int(u_zero), pf);
         break;
       case 2:
         launch(c, k_block_jacobi_apply<2, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
-               c.params.omega, int(u_zero));
+               c.params.omega, int(u_zero), pf);
         break;
       case 3:
         launch(c, k_block_jacobi_apply<3, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
-               c.params.omega, int(u_zero));
+               c.params.omega, int(u_zero), pf);
         break;
       default:
         launch(c, k_block_jacobi_apply<4, T, T>, nb, 256, (int)L.n, dinv_of<T>(L), h, u,
-               c.params.omega, int(u_zero));
+               c.params.omega, int(u_zero), pf);
     }
   }
   // u = (u_zero ? 0 : u) + omega * Vanka(h) (VankaSmoother::solve + Add)
-  void vanka(int l, const T* h, T* u, bool u_zero)
+  void vanka(int l, const T* h, T* u, bool u_zero, const double* hmean = nullptr)
   {
     const Level& L = c.L[l];
     no_rec();
-    const TV_of* lu = vk_lu(L);
+    const T* inv = vk_lu(L);
     T* out = vk_out(L);
-    if (!L.vk_warp) {
-      const int nb = blocks_for(L.npatch, 128);
-      switch (L.vk_M * 8 + L.B) {
-#define GB_VK(MM, BB)                                                          \
-  case MM * 8 + BB:                                                            \
-    launch(c, k_vanka_local<MM, BB, T, T>, nb, 128, L.npatch, (const int*)L.vk_pn.p, \
-           lu, (const uint8_t*)L.vk_perm.p, h, out);                           \
-    break;
-        GB_VK(9, 1)
-        GB_VK(27, 1)
-        GB_VK(18, 2)
-        GB_VK(27, 3)
-        GB_VK(8, 2)
-        GB_VK(12, 3)
-        GB_VK(16, 4)
-        GB_VK(4, 1)
-        GB_VK(8, 1)
-#undef GB_VK
-        default:
-          throw Error{ GB_EINVAL, "no Vanka kernel for this patch size" };
-      }
-    } else {
-      launch(c, k_vanka_local_warp<T, T>, blocks_for(L.npatch, kVankaWarps),
-             32 * kVankaWarps, L.npatch, L.vk_M, L.B, (const int*)L.vk_pn.p, lu,
-             (const uint8_t*)L.vk_perm.p, h, out);
+    const int pc = pf_comp(L);
+    const int nbp = blocks_for(L.npatch, kVankaWarps);
+    switch ((L.vk_M + 31) / 32) {
+      case 1:
+        launch(c, k_vanka_inv<1, T, T>, nbp, 32 * kVankaWarps, L.npatch, L.vk_M, L.B,
+               (const int*)L.vk_pn.p, inv, h, pc, hmean, out);
+        break;
+      case 2:
+        launch(c, k_vanka_inv<2, T, T>, nbp, 32 * kVankaWarps, L.npatch, L.vk_M, L.B,
+               (const int*)L.vk_pn.p, inv, h, pc, hmean, out);
+        break;
+      case 3:
+        launch(c, k_vanka_inv<3, T, T>, nbp, 32 * kVankaWarps, L.npatch, L.vk_M, L.B,
+               (const int*)L.vk_pn.p, inv, h, pc, hmean, out);
+        break;
+      default:
+        launch(c, k_vanka_inv<4, T, T>, nbp, 32 * kVankaWarps, L.npatch, L.vk_M, L.B,
+               (const int*)L.vk_pn.p, inv, h, pc, hmean, out);
     }
-    const int64_t s1 = L.vk_warp ? 1 : L.npatch, s2 = L.vk_warp ? L.vk_M : 1;
+    const PfArgs pf = weighted_mean_args(L);
     const int nb = blocks_for(L.n, 256);
     switch (L.B) {
       case 1:
         launch(c, k_vanka_gather<1, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
-               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
-               int(u_zero));
+               (const int*)L.vk_ent.p, (const T*)out, L.vk_M, u, c.params.omega,
+               int(u_zero), pf);
         break;
       case 2:
         launch(c, k_vanka_gather<2, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
-               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
-               int(u_zero));
+               (const int*)L.vk_ent.p, (const T*)out, L.vk_M, u, c.params.omega,
+               int(u_zero), pf);
         break;
       case 3:
         launch(c, k_vanka_gather<3, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
-               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
-               int(u_zero));
+               (const int*)L.vk_ent.p, (const T*)out, L.vk_M, u, c.params.omega,
+               int(u_zero), pf);
         break;
       default:
         launch(c, k_vanka_gather<4, T>, nb, 256, (int)L.n, (const int*)L.vk_nptr.p,
-               (const int*)L.vk_ent.p, (const T*)out, s1, s2, u, c.params.omega,
-               int(u_zero));
+               (const int*)L.vk_ent.p, (const T*)out, L.vk_M, u, c.params.omega,
+               int(u_zero), pf);
     }
+  }
+  // The single filtered component of a level (-1: no filter, or several
+  // components, which take the unfused pf_sub path).
+  static int pf_comp(const Level& L)
+  {
+    if (!L.pf_mask || (L.pf_mask & (L.pf_mask - 1)))
+      return -1;
+    return __builtin_ctz(static_cast<unsigned>(L.pf_mask));
+  }
+  // weighted mean of the updated iterate reduced by the update kernel
+  void check_pf_scratch(const Level& L) const
+  {
+    GB_REQUIRE(c.pfpart.p && c.pfpart.n >= static_cast<size_t>((L.n + 255) / 256 + 1) &&
+                 c.pfticket.p,
+               GB_ESTATE, "filter scratch not allocated for this level");
+  }
+  PfArgs weighted_mean_args(const Level& L) const
+  {
+    PfArgs a{};
+    a.pc = pf_comp(L);
+    if (a.pc >= 0) {
+      check_pf_scratch(L);
+      a.w = L.pf_w.p;
+      a.domain = L.pf_domain;
+      a.partials = c.pfpart.p;
+      a.ticket = c.pfticket.p;
+      a.umean = c.scal.p + 9;
+    }
+    return a;
+  }
+  // out = b - A u (MatrixResidual) with the algebraic mean of the filtered
+  // component left in scal[8] for the consumers to subtract on read.
+  const double* resid_mean(int l, const T* u, T* out, const T* b)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    const int pc = pf_comp(L);
+    const double denom = double(L.n - L.nhanging);
+    const Sell& S = opA(c, L);
+    if (L.B > 1) {
+      check_pf_scratch(L);
+      const SellView<T> A = view<T>(S, sell_vals<T>(S));
+      const int nb = blocks_for(S.n, kSpmvThreads);
+#define GB_RM(BB, PP)                                                                 \
+  launch(c, k_bspmv_resid_mean<BB, T, T, PP>, nb, kSpmvThreads, A, u, out, b, pc, denom, \
+         c.pfpart.p, c.pfticket.p, c.scal.p + 8)
+      if (L.B == 2) {
+        if (S.pat) GB_RM(2, true); else GB_RM(2, false);
+      } else if (L.B == 3) {
+        if (S.pat) GB_RM(3, true); else GB_RM(3, false);
+      } else {
+        if (S.pat) GB_RM(4, true); else GB_RM(4, false);
+      }
+#undef GB_RM
+      return c.scal.p + 8;
+    }
+    resid(l, u, out, b);
+    return mean_of(l, out, false);
+  }
+  // scal[8] = algebraic (or, weighted, the integral) mean of the filtered
+  // component of x
+  const double* mean_of(int l, const T* x, bool weighted)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    launch(c, k_comp_mean<T>, red_blocks(L.n), kRedThreads, (int)L.n, L.B, pf_comp(L), x,
+           weighted ? (const double*)L.pf_w.p : nullptr,
+           weighted ? L.pf_domain : double(L.n - L.nhanging), c.partials.p, c.ticket.p,
+           c.scal.p + 8);
+    return c.scal.p + 8;
+  }
+  // x(., pc) -= *mean
+  void sub_mean(int l, T* x, const double* mean)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    launch(c, k_comp_sub<T>, stream_blocks(L.n), 256, (int)L.n, L.B, pf_comp(L), x, mean,
+           1.0);
   }
   // pressure filter on x: weighted (SubtractMean) or algebraic
   // (SubtractMeanAlgebraic) mean of every filtered component removed
@@ -1050,8 +1154,9 @@ struct Emit
       return rec->push_back(level_op(kOpResid, L, out, u, b, 0.0));
     spmv<kResid, T, T, T>(c, L, opA(c, L), u, out, b, nullptr, 0.0);
   }
-  // coarse (level l) = R fine, 0 on the coarse Dirichlet dofs
-  void restrict_to(int l, const T* fine, T* coarse)
+  // coarse (level l) = R fine, 0 on the coarse Dirichlet dofs; with smean
+  // (block levels) the filtered component of fine is read minus *smean
+  void restrict_to(int l, const T* fine, T* coarse, const double* smean = nullptr)
   {
     const Transfer& Tr = c.T[l];
     if (rec) {
@@ -1073,13 +1178,16 @@ struct Emit
         launch(c, k_restrict<T>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
         break;
       case 2:
-        launch(c, k_restrict_b<T, 2>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        launch(c, k_restrict_b<T, 2>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm,
+               pf_comp(c.L[l + 1]), smean);
         break;
       case 3:
-        launch(c, k_restrict_b<T, 3>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        launch(c, k_restrict_b<T, 3>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm,
+               pf_comp(c.L[l + 1]), smean);
         break;
       default:
-        launch(c, k_restrict_b<T, 4>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        launch(c, k_restrict_b<T, 4>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm,
+               pf_comp(c.L[l + 1]), smean);
     }
   }
   void fill0(int l, T* u)
@@ -1136,12 +1244,12 @@ struct Emit
 template<>
 const double* Emit<double>::vk_lu(const Level& L)
 {
-  return L.vk_lu64.p;
+  return L.vk_inv64.p;
 }
 template<>
 const float* Emit<float>::vk_lu(const Level& L)
 {
-  return L.vk_lu32.p;
+  return L.vk_inv32.p;
 }
 template<>
 double* Emit<double>::vk_out(const Level& L)
@@ -1184,6 +1292,26 @@ smooth(Emit<T>& E, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
         E.jacobi(l, u, tmp, b);
         std::swap(u, tmp);
       }
+      continue;
+    }
+    if (L.pf_mask && Emit<T>::pf_comp(L) >= 0) {
+      // one filtered component: the residual kernel reduces its algebraic
+      // mean, the smoother subtracts it on read and reduces the weighted mean
+      // of the new iterate, which one pass then subtracts
+      const T* h = b; // y - A 0
+      const double* hm;
+      if (!u_zero) {
+        hm = E.resid_mean(l, u, tmp, b);
+        h = tmp;
+      } else {
+        hm = E.mean_of(l, b, false);
+      }
+      if (c.params.smoother == 1)
+        E.vanka(l, h, u, u_zero, hm);
+      else
+        E.jacobi_apply(l, h, u, u_zero, hm);
+      u_zero = false;
+      E.sub_mean(l, u, c.scal.p + 9);
       continue;
     }
     const T* h = b; // y - A 0
@@ -1394,7 +1522,15 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
   smooth<T>(E, l, P.iterpre, u, tmp, b, u_zero);
   // MatrixResidual into tmp (with SubtractMeanAlgebraic), restrict_zero +
   // SetBoundaryVectorZero on l-1
-  if (c.L[l].pf_mask) {
+  if (c.L[l].pf_mask && Emit<T>::pf_comp(c.L[l]) >= 0 && c.L[l].B > 1) {
+    // filtered residual: its mean is subtracted as the restriction reads it
+    if (u_zero) {
+      E.restrict_to(l - 1, b, W.b[l - 1].p, E.mean_of(l, b, false));
+    } else {
+      const double* hm = E.resid_mean(l, u, tmp, b);
+      E.restrict_to(l - 1, tmp, W.b[l - 1].p, hm);
+    }
+  } else if (c.L[l].pf_mask) {
     if (u_zero)
       E.copy(l, tmp, b);
     else
@@ -2693,6 +2829,8 @@ gb_level_set_pfilter(gb_ctx* ctx, int lvl, int comp_mask, const double* weights,
     GB_CUDA(L.pf_w.alloc(L.n));
     GB_CUDA(cudaMemcpy(L.pf_w.p, weights, L.n * sizeof(double), cudaMemcpyHostToDevice));
   }
+  if (comp_mask)
+    ensure_pf_scratch(*ctx, L.n);
   L.pf_mask = comp_mask;
   L.pf_domain = domain;
   L.nhanging = nhanging;
@@ -2762,13 +2900,16 @@ gb_restrict_zero(gb_ctx* ctx, int lvl, int coarse_id, int fine_id)
       launch(*ctx, k_restrict<double>, nb, 256, T.nc, tp, te, f, cc, nm);
       break;
     case 2:
-      launch(*ctx, k_restrict_b<double, 2>, nb, 256, T.nc, tp, te, f, cc, nm);
+      launch(*ctx, k_restrict_b<double, 2>, nb, 256, T.nc, tp, te, f, cc, nm, -1,
+             (const double*)nullptr);
       break;
     case 3:
-      launch(*ctx, k_restrict_b<double, 3>, nb, 256, T.nc, tp, te, f, cc, nm);
+      launch(*ctx, k_restrict_b<double, 3>, nb, 256, T.nc, tp, te, f, cc, nm, -1,
+             (const double*)nullptr);
       break;
     default:
-      launch(*ctx, k_restrict_b<double, 4>, nb, 256, T.nc, tp, te, f, cc, nm);
+      launch(*ctx, k_restrict_b<double, 4>, nb, 256, T.nc, tp, te, f, cc, nm, -1,
+             (const double*)nullptr);
   }
   GB_API_END
 }

@@ -25,21 +25,29 @@ def main(argv=None):
     ap.add_argument("--refine", type=int, default=6)
     ap.add_argument("--spmv", type=int, default=0)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--problem", default="diffusion", choices=["diffusion", "stokes"],
+                    help="stokes: 2D Q1/Q1 Stokes with Vanka on (2*2^(refine-1))^2 cells")
     ap.add_argument("--ktime", action="store_true",
                     help="per-kernel CUDA-event times of the last solve (GB_GRAPH=0)")
     a = ap.parse_args(argv)
 
     from gascoignelib_b200.build import build_library
     from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
-    from gascoignelib_b200.problem import seeded_inputs, structured_problem
+    from gascoignelib_b200.problem import (seeded_inputs, structured_problem,
+                                           structured_stokes)
 
     build_library()
-    kappa, rhs = seeded_inputs(3, 1, a.refine)
-    P = structured_problem(3, 1, a.refine, kappa, rhs)
+    if a.problem == "stokes":
+        P = structured_stokes(2, 2, a.refine)
+        keys = dict(gmressize=31, omega=1.0)
+    else:
+        kappa, rhs = seeded_inputs(3, 1, a.refine)
+        P = structured_problem(3, 1, a.refine, kappa, rhs)
+        keys = dict(gmressize=21, omega=0.8)
     with Context(0) as ctx:
         ctx.load_problem(P)
-        ctx.set_params(gmressize=21, tol=1e-8, globaltol=1e-300, maxiter=200,
-                       iterpre=2, iterpost=2, omega=0.8)
+        ctx.set_params(tol=1e-8, globaltol=1e-300, maxiter=200, iterpre=2, iterpost=2,
+                       **keys)
         fl = P.nlevels - 1
         if a.spmv:
             prec = GB_FP32 if a.precision == "fp32" else GB_FP64

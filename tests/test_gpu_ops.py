@@ -93,6 +93,10 @@ def test_smoothing(ctx, loaded):
     x, y, h = ctx.vec(), ctx.vec(), ctx.vec()
     for l in range(P.nlevels):
         n = P.levels[l].ndof
+        lv = P.levels[l]
+        if (P.info.get("smoother") == "vanka" and lv.patches is not None
+                and lv.patches.shape[0] == 1):
+            continue  # one patch = the whole singular level (test_gpu_stokes)
         xv, yv = rng.standard_normal(n), rng.standard_normal(n)
         for niter in (1, 2, 3):
             ctx.upload(l, x, xv)
