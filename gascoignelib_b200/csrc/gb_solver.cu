@@ -396,6 +396,10 @@ struct gb_ctx
   std::map<std::string, std::pair<int64_t, double>> kt_acc;
   int coarse_root = -1;
   std::map<gb::CoarseKey, gb::CoarseProgram> coarse_progs;
+  // dense maps of coarse sub-cycles that the single-CTA program does not cover
+  // (block systems, Vanka, pressure filter): levels 0..dense_root
+  int dense_root = -1;
+  std::map<gb::CoarseKey, gb::CoarseProgram> dense_maps;
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
   gb::DeviceArray<float> rhs32, zfix32;
   ~gb_ctx()
@@ -902,7 +906,14 @@ ensure_work(Context& c)
       break;
     c.coarse_root = l;
   }
+  c.dense_root = -1;
+  for (int l = 0; l < c.nlevels && !simple && c.coarse_dense; ++l) {
+    if (c.L[l].ndof() > kCoarseMaxRows)
+      break;
+    c.dense_root = l;
+  }
   c.coarse_progs.clear();
+  c.dense_maps.clear();
   c.work_ready = true;
 }
 
@@ -918,6 +929,7 @@ struct Emit
 {
   Context& c;
   std::vector<CoarseOp>* rec = nullptr;
+  int no_dense_at = -1; // level whose dense map is being built (run its steps)
 
   CoarseOp level_op(int kind, const Level& L, void* out, const void* in,
                     const void* b, double alpha) const
@@ -1499,6 +1511,81 @@ run_coarse(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char
   return prog.zero_out;
 }
 
+// mgstep(l) from u = 0 for a level whose sub-cycle the single-CTA program does
+// not cover: the sub-cycle is linear in b, so it is applied as its matrix K
+// (u_out = K b, one GEMV), built once per entry state by running the
+// sub-cycle's own kernels on the unit vectors (b is saved and restored).
+template<class T>
+static bool
+run_dense(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
+          char p, T*& u, T*& tmp, const T* b)
+{
+  Context& c = E.c;
+  CoarseKey key{ int(sizeof(T)), l, (const void*)u, (const void*)tmp, (const void*)b,
+                 true, p0, p, c.transposed != 0 };
+  auto it = c.dense_maps.find(key);
+  if (it == c.dense_maps.end()) {
+    const int n = static_cast<int>(c.L[l].ndof());
+    CoarseProgram dm;
+    dm.n_root = n;
+    dm.nb = n;
+    dm.ncols = n;
+    dm.b_root = b;
+    DeviceArray<T> bsave, Kt;
+    GB_CUDA(bsave.alloc(n));
+    GB_CUDA(Kt.alloc(size_t(n) * n));
+    T* bw = const_cast<T*>(b);
+    GB_CUDA(cudaMemcpyAsync(bsave.p, b, n * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
+    const int64_t launches0 = c.launches;
+    const T one = T(1);
+    T* u2 = u;
+    T* t2 = tmp;
+    char p02 = p0;
+    bool z = true;
+    for (int j = 0; j < n; ++j) {
+      GB_CUDA(cudaMemsetAsync(bw, 0, n * sizeof(T), c.stream));
+      GB_CUDA(cudaMemcpyAsync(bw + j, &one, sizeof(T), cudaMemcpyHostToDevice, c.stream));
+      Emit<T> E2{ c, nullptr, l };
+      u2 = u;
+      t2 = tmp;
+      p02 = p0;
+      z = mgstep<T>(E2, W, l, finelevel, coarselevel, p02, p, u2, t2, bw, true);
+      if (z)
+        E2.fill0(l, u2);
+      // column j of K (row-major n x n) = the response to e_j
+      GB_CUDA(cudaMemcpy2DAsync(Kt.p + j, n * sizeof(T), u2, sizeof(T), sizeof(T), n,
+                                cudaMemcpyDeviceToDevice, c.stream));
+      GB_CUDA(cudaStreamSynchronize(c.stream)); // `one` lives on this stack frame
+    }
+    GB_CUDA(cudaMemcpyAsync(bw, bsave.p, n * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+    c.launches = launches0; // set-up, not part of a solve
+    if (sizeof(T) == 8)
+      dm.K64.p = reinterpret_cast<double*>(Kt.p), dm.K64.n = Kt.n;
+    else
+      dm.K32.p = reinterpret_cast<float*>(Kt.p), dm.K32.n = Kt.n;
+    Kt.p = nullptr;
+    Kt.n = 0;
+    dm.u_in = u;
+    dm.u_out = u2;
+    dm.tmp_out = t2;
+    dm.p0_out = p02;
+    dm.zero_out = false;
+    dm.nops = 1;
+    it = c.dense_maps.emplace(key, std::move(dm)).first;
+  }
+  const CoarseProgram& dm = it->second;
+  const T* K = sizeof(T) == 8 ? reinterpret_cast<const T*>(dm.K64.p)
+                              : reinterpret_cast<const T*>(dm.K32.p);
+  launch(c, k_coarse_apply<T>, blocks_for(int64_t(dm.n_root) * 32, 256), 256, dm.n_root,
+         dm.ncols, dm.nb, K, static_cast<const T*>(dm.b_root),
+         static_cast<const T*>(dm.u_in), static_cast<T*>(const_cast<void*>(dm.u_out)));
+  u = static_cast<T*>(const_cast<void*>(dm.u_out));
+  tmp = static_cast<T*>(const_cast<void*>(dm.tmp_out));
+  p0 = dm.p0_out;
+  return false;
+}
+
 // StdMultiLevelSolver::mgstep (Solver/stdmultilevelsolver.cc:462-531). Steps
 // that only feed CGInfo (the norms and the final residual) are not computed:
 // they do not change u. HNDistribute/HNAverage/HNZero are identities on meshes
@@ -1512,6 +1599,8 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
   Context& c = E.c;
   if (!E.rec && c.coarse_on && l <= c.coarse_root)
     return run_coarse<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b, u_zero);
+  if (!E.rec && c.coarse_on && l <= c.dense_root && u_zero && l != E.no_dense_at)
+    return run_dense<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b);
   const gb_params& P = c.params;
   if (l == coarselevel) {
     if (p == 'F')
