@@ -47,6 +47,12 @@ class Level:
     # Vanka patches: [npatch, nodes per patch] node indices (DofHandler::
     # GetElement(2, p)); None when the level has none
     patches: Optional[np.ndarray] = None
+    # hanging nodes: rows [node, 3 parents] (edges, hnq2) and [node, 9 parents]
+    # (3D faces, hnq2face), and the discretisation of the HNStructure acting
+    # on them: 0 Q12d, 1 Q13d, 2 Q22d, 3 Q23d
+    hn_edges: Optional[np.ndarray] = None
+    hn_faces: Optional[np.ndarray] = None
+    hn_disc: int = 0
 
     @property
     def nnzb(self) -> int:
@@ -153,6 +159,13 @@ def load_reference_dump(d: str) -> Problem:
             pt = _i64(p + "patches.i64")
             npp = 3 ** dim
             lv.patches = pt.reshape(-1, npp)
+        he = _i64(p + "hnedge.i64") if os.path.exists(p + "hnedge.i64") else None
+        hf = _i64(p + "hnface.i64") if os.path.exists(p + "hnface.i64") else None
+        if (he is not None and he.size) or (hf is not None and hf.size):
+            lv.hn_edges = (he if he is not None else np.zeros(0, np.int64)).reshape(-1, 4)
+            lv.hn_faces = (hf if hf is not None else np.zeros(0, np.int64)).reshape(-1, 10)
+            q2 = summ.get("disc", ["Q1"])[0] == "Q2"
+            lv.hn_disc = (2 if q2 else 0) + (1 if dim == 3 else 0)
         levels.append(lv)
     for l in range(nl - 1):
         p = os.path.join(d, f"T{l}_")

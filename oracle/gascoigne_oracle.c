@@ -49,6 +49,14 @@ typedef struct
   int64_t npatch;
   int npp;                /* nodes per patch */
   const int64_t* patches; /* npatch * npp node indices */
+  /* hanging nodes (HangingIndexHandler hnq2 / hnq2face, Mesh/
+   * hangingindexhandler.h:40,65) and the discretisation whose HNStructure
+   * acts on them: 0 Q12d, 1 Q13d, 2 Q22d, 3 Q23d */
+  int hn_disc;
+  int64_t nhedge;
+  const int64_t* hnedge;  /* nhedge rows [node, 3 parents], ascending node */
+  int64_t nhface;
+  const int64_t* hnface;  /* nhface rows [node, 9 parents], ascending node */
 } or_level;
 
 /* Transfer level l (coarse) <-> l+1 (fine) in the form MgInterpolatorMatrix
@@ -391,6 +399,132 @@ or_vanka_solve(const or_level* A, const double* lu, const int* perm, double* x,
   }
 }
 
+/* ------------------------------------------------------- hanging nodes */
+/* HNStructureQ12d/Q13d/Q22d/Q23d Average, Distribute, Zero
+ * (Discretization/Q1/hnstructureq12d.cc:196-243, hnstructureq13d.cc:148-188,
+ *  Discretization/Q2/hnstructureq22d.cc:50-76, hnstructureq23d.cc:118-153),
+ * with CompVector::equ_node/add_node's expression order
+ * (Common/compvector.h:190-262). */
+static const double or_q2w[3] = { 0.375, 0.75, -0.125 };
+
+static void
+or_hn_edges_average(const or_level* A, double* u)
+{
+  const int B = A->B;
+  const int q2 = A->hn_disc >= 2;
+  for (int64_t k = 0; k < A->nhedge; ++k) {
+    const int64_t* e = A->hnedge + 4 * k;
+    for (int c = 0; c < B; ++c) {
+      const double u0 = u[e[1] * B + c], u1 = u[e[2] * B + c];
+      if (q2)
+        u[e[0] * B + c] = or_q2w[0] * u0 + or_q2w[1] * u1 + or_q2w[2] * u[e[3] * B + c];
+      else
+        u[e[0] * B + c] = 0.5 * u0 + 0.5 * u1;
+    }
+  }
+}
+
+static void
+or_hn_faces_average(const or_level* A, double* u)
+{
+  const int B = A->B;
+  for (int64_t k = 0; k < A->nhface; ++k) {
+    const int64_t* f = A->hnface + 10 * k;
+    const int64_t* p = f + 1;
+    for (int c = 0; c < B; ++c) {
+#define U_(j) u[p[j] * B + c]
+      if (A->hn_disc == 3) {
+        double w[9];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            w[3 * i + j] = or_q2w[i] * or_q2w[j];
+        double v = w[0] * U_(0) + w[1] * U_(1) + w[2] * U_(2);
+        v += w[3] * U_(3) + w[4] * U_(4) + w[5] * U_(5);
+        v += w[6] * U_(6) + w[7] * U_(7) + w[8] * U_(8);
+        u[f[0] * B + c] = v;
+      } else {
+        u[f[0] * B + c] = 0.25 * U_(0) + 0.25 * U_(1) + 0.25 * U_(3) + 0.25 * U_(4);
+      }
+#undef U_
+    }
+  }
+}
+
+static void
+or_hn_edges_distribute(const or_level* A, double* u)
+{
+  const int B = A->B;
+  const int q2 = A->hn_disc >= 2;
+  for (int64_t k = 0; k < A->nhedge; ++k) {
+    const int64_t* e = A->hnedge + 4 * k;
+    for (int j = 0; j < (q2 ? 3 : 2); ++j)
+      for (int c = 0; c < B; ++c)
+        u[e[1 + j] * B + c] += (q2 ? or_q2w[j] : 0.5) * u[e[0] * B + c];
+    for (int c = 0; c < B; ++c)
+      u[e[0] * B + c] = 0.0;
+  }
+}
+
+static void
+or_hn_faces_distribute(const or_level* A, double* u)
+{
+  const int B = A->B;
+  for (int64_t k = 0; k < A->nhface; ++k) {
+    const int64_t* f = A->hnface + 10 * k;
+    if (A->hn_disc == 3) {
+      for (int j = 0; j < 9; ++j)
+        for (int c = 0; c < B; ++c)
+          u[f[1 + j] * B + c] += (or_q2w[j / 3] * or_q2w[j % 3]) * u[f[0] * B + c];
+    } else {
+      static const int q1f[4] = { 0, 1, 3, 4 };
+      for (int j = 0; j < 4; ++j)
+        for (int c = 0; c < B; ++c)
+          u[f[1 + q1f[j]] * B + c] += 0.25 * u[f[0] * B + c];
+    }
+    for (int c = 0; c < B; ++c)
+      u[f[0] * B + c] = 0.0;
+  }
+}
+
+void
+or_hn_average(const or_level* A, double* u)
+{
+  if (A->hn_disc == 3) { /* Q23d: faces, then edges */
+    or_hn_faces_average(A, u);
+    or_hn_edges_average(A, u);
+  } else {              /* Q12d, Q22d: edges; Q13d: edges, then faces */
+    or_hn_edges_average(A, u);
+    if (A->hn_disc == 1)
+      or_hn_faces_average(A, u);
+  }
+}
+
+void
+or_hn_distribute(const or_level* A, double* u)
+{
+  if (A->hn_disc == 3) {
+    or_hn_faces_distribute(A, u);
+    or_hn_edges_distribute(A, u);
+  } else {
+    or_hn_edges_distribute(A, u);
+    if (A->hn_disc == 1)
+      or_hn_faces_distribute(A, u);
+  }
+}
+
+void
+or_hn_zero(const or_level* A, double* u)
+{
+  const int B = A->B;
+  for (int64_t k = 0; k < A->nhedge; ++k)
+    for (int c = 0; c < B; ++c)
+      u[A->hnedge[4 * k] * B + c] = 0.0;
+  if (A->hn_disc == 1 || A->hn_disc == 3)
+    for (int64_t k = 0; k < A->nhface; ++k)
+      for (int c = 0; c < B; ++c)
+        u[A->hnface[10 * k] * B + c] = 0.0;
+}
+
 /* ---------------------------------------------------------- transfers */
 
 static int
@@ -661,7 +795,7 @@ or_mgstep(or_mg* M, double* res, double* rw, int l, int finelevel,
     or_smooth(M, l, M->iterpre, u[l], b[l], v[l]);
     or_matrix_residual(&M->L[l], v[l], u[l], b[l]);
     or_restrict_zero(&M->T[l - 1], M->L[l].B, b[l - 1], v[l]);
-    /* HNDistribute: no hanging nodes on these meshes */
+    or_hn_distribute(&M->L[l - 1], b[l - 1]);
     or_dirichlet_zero(&M->L[l - 1], b[l - 1]);
     memset(u[l - 1], 0, sizeof(double) * ndof(M, l - 1));
     int j = (*p0 == 'V') ? 1 : (*p0 == 'W') ? 2 : (*p0 == 'F') ? 3 : 0;
@@ -671,9 +805,10 @@ or_mgstep(or_mg* M, double* res, double* rw, int l, int finelevel,
       *p0 = 'W';
     rw[l] = or_norm(ndof(M, l - 1), u[l - 1]);
     memset(v[l], 0, sizeof(double) * ndof(M, l));
-    /* HNAverage: none */
+    or_hn_average(&M->L[l - 1], u[l - 1]);
     or_prolongate_add(&M->T[l - 1], M->L[l].B, v[l], u[l - 1]);
-    /* HNZero (coarse, fine): none */
+    or_hn_zero(&M->L[l - 1], u[l - 1]);
+    or_hn_zero(&M->L[l], v[l]);
     or_dirichlet_zero(&M->L[l], v[l]);
     for (int64_t i = 0; i < ndof(M, l); ++i)
       u[l][i] += M->mgomega * v[l][i];

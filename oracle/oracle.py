@@ -28,7 +28,9 @@ class _Level(C.Structure):
                 ("diag", _P64), ("val", _PD), ("ndir", C.c_int64), ("dir", _P64),
                 ("dircomp_mask", C.c_int), ("pf_mask", C.c_int), ("pf_w", _PD),
                 ("pf_domain", C.c_double), ("nhanging", C.c_int64),
-                ("npatch", C.c_int64), ("npp", C.c_int), ("patches", _P64)]
+                ("npatch", C.c_int64), ("npp", C.c_int), ("patches", _P64),
+                ("hn_disc", C.c_int), ("nhedge", C.c_int64), ("hnedge", _P64),
+                ("nhface", C.c_int64), ("hnface", _P64)]
 
 
 class _Transfer(C.Structure):
@@ -75,6 +77,8 @@ def lib():
                                       C.POINTER(C.c_int)]
         L.or_vanka_solve.argtypes = [C.POINTER(_Level), _PD, C.POINTER(C.c_int), _PD,
                                      _PD, C.POINTER(C.c_int)]
+        for f in ("or_hn_average", "or_hn_distribute", "or_hn_zero"):
+            getattr(L, f).argtypes = [C.POINTER(_Level), _PD]
         L.or_dot.restype = C.c_double
         L.or_dot.argtypes = [C.c_int64, _PD, _PD]
         _lib = L
@@ -114,6 +118,17 @@ class Oracle:
                 pt = np.ascontiguousarray(lv.patches, dtype=np.int64)
                 self._keep.append(pt)
                 lev.npatch, lev.npp, lev.patches = pt.shape[0], pt.shape[1], _p64(pt)
+            if lv.hn_edges is not None or lv.hn_faces is not None:
+                he = np.ascontiguousarray(
+                    lv.hn_edges if lv.hn_edges is not None else np.zeros((0, 4)),
+                    dtype=np.int64).reshape(-1, 4)
+                hf = np.ascontiguousarray(
+                    lv.hn_faces if lv.hn_faces is not None else np.zeros((0, 10)),
+                    dtype=np.int64).reshape(-1, 10)
+                self._keep += [he, hf]
+                lev.hn_disc = lv.hn_disc
+                lev.nhedge, lev.hnedge = he.shape[0], _p64(he)
+                lev.nhface, lev.hnface = hf.shape[0], _p64(hf)
             self.levels[l] = lev
         self.transfers = (_Transfer * max(nl - 1, 1))()
         for l, t in enumerate(prob.transfers):
@@ -188,6 +203,12 @@ class Oracle:
         lib().or_prolongate_add(C.byref(self.transfers[level]), B, _pd(fine),
                                 _pd(np.ascontiguousarray(coarse, dtype=np.float64)))
         return fine
+
+    def hn(self, op, level, u):
+        """op: "average", "distribute" or "zero" (HNStructure*::Average ...)."""
+        u = np.array(u, dtype=np.float64)
+        getattr(lib(), "or_hn_" + op)(C.byref(self.levels[level]), _pd(u))
+        return u
 
     def subtract_mean(self, level, u, algebraic=False):
         u = np.array(u, dtype=np.float64)

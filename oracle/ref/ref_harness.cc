@@ -28,6 +28,14 @@
 // ilu: VankaSmoother, LinAlg/vankasmoother.cc) or smoother=jacobi (block
 // Jacobi). The right-hand side file then holds ncomp values per node.
 //
+// disc=Q2 selects CGQ2 (Q2 elements on patches of 2^dim cells); ball=r refines,
+// after the global refinements, once more every leaf cell whose centroid lies
+// within distance r of the domain's centre (MeshAgent::refine_cells: whole
+// patches, hanging nodes at the interface); diff=eps replaces the coefficient
+// by the constant eps (needed with ball refinement, where cell widths differ);
+// rhsres=N reads the right-hand side on the (N+1)^dim lexicographic grid
+// (N = 2 * coarse * 2^refine covers the nodes of the extra refinement).
+//
 // Usage: ref_harness key=value ...   (see parse() for the keys)
 // Output (directory out=): summary.txt, and with dump=1 raw little-endian arrays
 //   L<l>_rowptr.i64 L<l>_col.i64 L<l>_diag.i64 L<l>_val.f64 L<l>_coord.f64
@@ -39,7 +47,9 @@
 //   L<l>_val.f64 holds nnzb*ncomp^2 values (row-major blocks); for
 //   problem=stokes also L<l>_pfw.f64 (pressure-filter weights) and
 //   L<l>_patches.i64 (Vanka patches, npatches x nodes_per_patch), with
-//   pfdomain_L<l>, ncomp and dircomps in summary.txt
+//   pfdomain_L<l>, ncomp and dircomps in summary.txt; the hanging nodes of
+//   every level as L<l>_hnedge.i64 (rows [node, 3 parents]) and
+//   L<l>_hnface.i64 (3D, rows [node, 9 parents]) with disc in summary.txt
 // and with dualrhs= (a nodal vector like rhs): dual_summary.txt,
 //   dual_rhs.f64 dual_solution.f64, and with dump=1 L<l>_dualval.f64 (the
 //   dual matrices' values in the stencil of L<l>_col.i64)
@@ -59,6 +69,8 @@
 #include "fmatrixblock.h"
 #include "functionalcontainer.h"
 #include "gascoignemeshtransfer.h"
+#include "hierarchicalmesh2d.h"
+#include "hierarchicalmesh3d.h"
 #include "meshagent.h"
 #include "paramfile.h"
 #include "problemcontainer.h"
@@ -87,6 +99,9 @@ struct Config
   std::string problem = "diffusion", smoother = "jacobi";
   double visc = 1.0, stab = 0.1;
   int pfilter = 1;
+  std::string disc = "Q1";
+  double ball = 0.0, diff = -1.0;
+  int rhsres = 0;
 };
 
 // kappa per cell, one array per resolution N = coarse * 2^l (cells per dim),
@@ -111,6 +126,7 @@ struct KappaPyramid
   }
 };
 KappaPyramid g_kappa;
+double g_diff = -1.0; // constant coefficient (diff=), or -1: the kappa pyramid
 
 class DiffusionEquation : public virtual Equation
 {
@@ -135,11 +151,19 @@ public:
   // (ElementIntegrator::Matrix, DofHandler/elementintegrator.xx:369-379).
   void point(double h, const FemFunction&, const Vertex2d& v) const override
   {
+    if (g_diff >= 0.0) {
+      kappa_ = g_diff;
+      return;
+    }
     int N = static_cast<int>(std::lround(1.0 / h));
     kappa_ = g_kappa.at(N, v.x(), v.y(), 0.0);
   }
   void point(double h, const FemFunction&, const Vertex3d& v) const override
   {
+    if (g_diff >= 0.0) {
+      kappa_ = g_diff;
+      return;
+    }
     int N = static_cast<int>(std::lround(1.0 / h));
     kappa_ = g_kappa.at(N, v.x(), v.y(), v.z());
   }
@@ -282,6 +306,10 @@ parse(int argc, char** argv)
     else if (k == "visc") c.visc = atof(v.c_str());
     else if (k == "stab") c.stab = atof(v.c_str());
     else if (k == "pfilter") c.pfilter = atoi(v.c_str());
+    else if (k == "disc") c.disc = v;
+    else if (k == "ball") c.ball = atof(v.c_str());
+    else if (k == "diff") c.diff = atof(v.c_str());
+    else if (k == "rhsres") c.rhsres = atoi(v.c_str());
     else if (k == "conv") {
       std::stringstream ss(v);
       std::string t;
@@ -416,7 +444,7 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "coarselevel 0\n\n"
     << "//Block Solver\n"
     << "matrixtype " << (c.smoother == "vanka" ? "vanka" : "block") << "\n"
-    << "discname CGQ1\n"
+    << "discname " << (c.disc == "Q2" ? "CGQ2" : "CGQ1") << "\n"
     << "ndirect " << c.ndirect << "\n"
     << "iterpre " << c.iterpre << "\n"
     << "iterpost " << c.iterpost << "\n"
@@ -508,8 +536,36 @@ main(int argc, char** argv)
                                     : static_cast<ProblemDescriptorInterface*>(&PD));
   FunctionalContainer FC;
 
+  g_diff = c.diff;
   MeshAgent MA;
   MA.BasicInit(pf);
+  if (c.ball > 0.0) {
+    // one more refinement of the leaf cells whose centroid is in the ball
+    HierarchicalMesh* HM = MA.GetHierarchicalMesh();
+    IntVector ref;
+    const int nv = c.dim == 3 ? 8 : 4;
+    for (int cell = 0; cell < HM->ncells(); ++cell) {
+      if (HM->sleep(cell))
+        continue;
+      double x[3] = { 0, 0, 0 };
+      for (int j = 0; j < nv; ++j) {
+        const int vtx = HM->vertex_of_cell(cell, j);
+        if (c.dim == 3) {
+          const Vertex3d& w = dynamic_cast<HierarchicalMesh3d*>(HM)->vertex3d(vtx);
+          x[0] += w.x() / nv, x[1] += w.y() / nv, x[2] += w.z() / nv;
+        } else {
+          const Vertex2d& w = dynamic_cast<HierarchicalMesh2d*>(HM)->vertex2d(vtx);
+          x[0] += w.x() / nv, x[1] += w.y() / nv;
+        }
+      }
+      double r2 = 0;
+      for (int d = 0; d < c.dim; ++d)
+        r2 += (x[d] - 0.5) * (x[d] - 0.5);
+      if (r2 < c.ball * c.ball)
+        ref.push_back(cell);
+    }
+    MA.refine_cells(ref);
+  }
   StdMultiLevelSolver MLS;
   MLS.BasicInit(&MA, pf, &PC, &FC);
   MLS.ReInit();
@@ -527,7 +583,7 @@ main(int argc, char** argv)
   auto t_as1 = std::chrono::steady_clock::now();
 
   const int nl = MLS.nlevels();
-  const int Nf = c.coarse << c.refine;
+  const int Nf = c.rhsres > 0 ? c.rhsres : (c.coarse << c.refine);
   StdSolver* S = MLS.GetSolver();
   const GascoigneMesh* Mf = S->GetMesh();
   const int nf = Mf->nnodes();
@@ -554,6 +610,7 @@ main(int argc, char** argv)
         F(i, cc) = r[((iz * (Nf + 1) + iy) * (Nf + 1) + ix) * ncomp + cc];
     }
   }
+  S->HNZero(f); // hanging dofs are constrained, not unknowns
   S->SetBoundaryVectorZero(f);
 
   std::vector<double> times;
@@ -586,6 +643,7 @@ main(int argc, char** argv)
     o << "residual " << info.control().residual() << "\n";
     o << "true_rel_residual " << rnorm / fnorm << "\n";
     o << "ncomp " << ncomp << "\n";
+    o << "disc " << c.disc << "\n";
     o << "dircomps";
     if (stokes)
       for (int d = 1; d <= c.dim; ++d)
@@ -653,6 +711,22 @@ main(int argc, char** argv)
         for (int i : *bv)
           dn.push_back(i);
       write_raw(L + "dirichlet.i64", dn);
+      {
+        const HangingIndexHandler& HI = ML->GetHangingIndexHandler();
+        std::vector<long> he, hf;
+        for (const auto& e : *HI.GetStructure()) {
+          he.push_back(e.first);
+          for (int q : e.second)
+            he.push_back(q);
+        }
+        for (const auto& e : *HI.GetStructureFace()) {
+          hf.push_back(e.first);
+          for (int q : e.second)
+            hf.push_back(q);
+        }
+        write_raw(L + "hnedge.i64", he);
+        write_raw(L + "hnface.i64", hf);
+      }
       if (stokes) {
         const PressureFilter& PF = SolverView::pfilter(SL);
         std::vector<double> w(PF.begin(), PF.end());
@@ -690,6 +764,27 @@ main(int argc, char** argv)
       write_raw(T + "zweier.i64", z);
       write_raw(T + "vierer.i64", v4);
       write_raw(T + "achter.i64", a8);
+    }
+    // the finest level's hanging-node operations on a test vector
+    // t(i, c) = sin(1 + i * ncomp + c): HNAverage, HNDistribute, HNZero
+    {
+      Vector t("t");
+      MLS.ReInitVector(t);
+      GlobalVector& T = S->GetGV(t);
+      auto fill = [&]() {
+        for (int i = 0; i < nf; ++i)
+          for (int cc = 0; cc < ncomp; ++cc)
+            T(i, cc) = std::sin(1.0 + i * ncomp + cc);
+      };
+      fill();
+      S->HNAverage(t);
+      write_raw(c.out + "/hn_average.f64", std::vector<double>(T.begin(), T.end()));
+      fill();
+      S->HNDistribute(t);
+      write_raw(c.out + "/hn_distribute.f64", std::vector<double>(T.begin(), T.end()));
+      fill();
+      S->HNZero(t);
+      write_raw(c.out + "/hn_zero.f64", std::vector<double>(T.begin(), T.end()));
     }
     std::vector<double> rhs(F.begin(), F.end());
     write_raw(c.out + "/rhs.f64", rhs);

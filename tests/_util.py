@@ -35,6 +35,10 @@ def load_golden(name):
             lv.pf_domain = float(z[f"L{l}_pfdomain"])
         if f"L{l}_patches" in z.files:
             lv.patches = z[f"L{l}_patches"].astype(np.int64)
+        if f"L{l}_hnedge" in z.files:
+            lv.hn_edges = z[f"L{l}_hnedge"].astype(np.int64).reshape(-1, 4)
+            lv.hn_faces = z[f"L{l}_hnface"].astype(np.int64).reshape(-1, 10)
+            lv.hn_disc = int(z[f"L{l}_hndisc"])
         levels.append(lv)
     for l in range(nl - 1):
         transfers.append(Transfer(c2f=z[f"T{l}_c2f"].astype(np.int64),
@@ -47,6 +51,9 @@ def load_golden(name):
     ref = {"solution": z["solution"], "iterations": int(z["iterations"]),
            "firstresidual": float(z["firstresidual"]), "residual": float(z["residual"]),
            "status": str(z["status"]), "keys": keys}
+    if "hn_average" in z.files:
+        ref.update(hn_average=z["hn_average"], hn_distribute=z["hn_distribute"],
+                   hn_zero=z["hn_zero"])
     if "dual_solution" in z.files:
         ref.update(dual_rhs=z["dual_rhs"], dual_solution=z["dual_solution"],
                    dual_iterations=int(z["dual_iterations"]),
@@ -55,6 +62,10 @@ def load_golden(name):
                    dual_status=str(z["dual_status"]),
                    dualval=[z[f"L{l}_dualval"] for l in range(nl)])
     return P, ref
+
+
+def golden_hn_cases():
+    return [n for n in golden_cases() if n.startswith("hn_")]
 
 
 def golden_stokes_cases():

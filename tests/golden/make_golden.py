@@ -11,7 +11,9 @@ Q1 mass matrix, u the forward solution of a first run) and the dual solution.
 The "stokes_" cases are the Q1/Q1 Stokes system (ncomp = dim+1, block
 matrices) with the pressure filter and the Vanka or block-Jacobi smoother; the
 harness runs them on one OpenMP thread, so Vanka's patch contributions are
-summed in patch order.
+summed in patch order. The "hn_" cases refine a ball once more (hanging
+nodes, Q1 or Q2 elements) and also record the reference's HNAverage,
+HNDistribute and HNZero of a test vector on the finest level.
 
     python tests/golden/make_golden.py
 """
@@ -47,6 +49,11 @@ CASES = {
     "stokes_3d_c1_r3_vanka": (3, 1, 3, True, 1e-8,
                               {"problem": "stokes", "smoother": "vanka", "omega": 1.0,
                                "gmressize": 31}),
+    "hn_2d_q1_c2_r3_ball": (2, 2, 3, True, 1e-10,
+                            {"disc": "Q1", "ball": 0.25, "diff": 1.0}),
+    "hn_2d_q2_c2_r3_conv_ball": (2, 2, 3, True, 1e-10,
+                                 {"disc": "Q2", "ball": 0.25, "diff": 0.1,
+                                  "conv": "1,0.5"}),
 }
 
 
@@ -94,6 +101,12 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
     stokes = extra.get("problem") == "stokes"
     if stokes:
         kw = write_inputs(d, None, stokes_rhs(dim, coarse, refine))
+    elif "ball" in extra:
+        # nodes of the extra refinement sit on the twice finer lexicographic grid
+        res = 2 * (coarse << refine)
+        rhs = np.random.default_rng(1002).uniform(-1.0, 1.0, size=(res + 1) ** dim)
+        kw = write_inputs(d, None, rhs)
+        kw["rhsres"] = res
     elif seeded:
         kappa, rhs = seeded_inputs(dim, coarse, refine)
         kw = write_inputs(d, kappa, rhs)
@@ -135,7 +148,14 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
             arrs[f"L{l}_dualval"] = np.fromfile(os.path.join(out, f"L{l}_dualval.f64"))
     arrs["B"] = P.finest.B
     arrs["dircomp_mask"] = P.finest.dircomp_mask
+    if "ball" in extra:
+        for op in ("average", "distribute", "zero"):
+            arrs["hn_" + op] = np.fromfile(os.path.join(out, f"hn_{op}.f64"))
     for l, lv in enumerate(P.levels):
+        if lv.hn_edges is not None:
+            arrs[f"L{l}_hnedge"] = lv.hn_edges.astype(np.int32)
+            arrs[f"L{l}_hnface"] = lv.hn_faces.astype(np.int32)
+            arrs[f"L{l}_hndisc"] = lv.hn_disc
         if lv.pf_mask:
             arrs[f"L{l}_pfw"] = lv.pf_weights
             arrs[f"L{l}_pfdomain"] = lv.pf_domain

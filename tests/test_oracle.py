@@ -189,3 +189,44 @@ def test_structured_stokes_matches_reference_assembly(name):
         ds = np.zeros(Ls.n, bool)
         ds[Ls.dirichlet] = True
         assert np.array_equal(dr, ds)
+
+
+def _hn_test_vector(P):
+    n, B = P.finest.n, P.finest.B
+    return np.sin(1.0 + np.arange(n * B))
+
+
+@pytest.mark.parametrize("name", [n for n in golden_cases() if n.startswith("hn_")])
+def test_oracle_hanging_node_ops_match_reference(name):
+    """HNAverage / HNDistribute / HNZero of the reference's HNStructure on the
+    finest level (ball refinement), bit for bit."""
+    P, ref = load_golden(name)
+    O = Oracle(P, **solver_keys(ref["keys"]))
+    t = _hn_test_vector(P)
+    l = P.nlevels - 1
+    assert P.finest.hn_edges.shape[0] > 0
+    for op in ("average", "distribute", "zero"):
+        assert np.array_equal(O.hn(op, l, t), ref["hn_" + op]), op
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="compiled reference not present")
+@pytest.mark.parametrize("disc", ["Q1", "Q2"])
+def test_oracle_hanging_nodes_3d_live(disc):
+    """3D ball refinement (edge and face hanging nodes; Q13d / Q23d weights):
+    HN operations and the solve against the compiled reference."""
+    d = tempfile.mkdtemp()
+    res = 2 * (2 << 3)
+    rhs = np.random.default_rng(1002).uniform(-1.0, 1.0, size=(res + 1) ** 3)
+    kw = write_inputs(d, None, rhs)
+    out, summ = run_reference(d, threads=1, dim=3, coarse=2, refine=3, disc=disc,
+                              ball=0.25, diff=1.0, rhsres=res, dump=1, tol=1e-8, **kw)
+    P = load_reference_dump(out)
+    assert P.finest.hn_faces.shape[0] > 0 and P.finest.hn_edges.shape[0] > 0
+    O = Oracle(P)
+    t = _hn_test_vector(P)
+    l = P.nlevels - 1
+    for op in ("average", "distribute", "zero"):
+        assert np.array_equal(O.hn(op, l, t), np.fromfile(os.path.join(out, f"hn_{op}.f64")))
+    x, info = O.gmres(vmax=21, tol=1e-8)
+    assert info["iterations"] == int(summ["iterations"][0])
+    assert np.array_equal(x, np.fromfile(os.path.join(out, "solution.f64")))
