@@ -436,3 +436,77 @@ k_vanka_gather(int n, const int* __restrict__ nptr, const int* __restrict__ ent,
 }
 
 } // namespace gb
+
+namespace gb {
+
+// ------------------------------------------------------------ hanging nodes
+//
+// HNStructureQ12d/Q13d/Q22d/Q23d (Discretization/Q1/hnstructureq12d.cc,
+// hnstructureq13d.cc, Discretization/Q2/hnstructureq22d.cc,
+// hnstructureq23d.cc) act in phases (edges, faces, in the discretisation's
+// order); within a phase no hanging node is a parent of another. Products and
+// sums are rounded separately (no fused multiply-add) and associated as
+// CompVector::equ_node/add_node write them, so the FP64 results are the
+// reference's bit for bit.
+__device__ __forceinline__ double hn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double hn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float hn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float hn_add(float a, float b) { return __fadd_rn(a, b); }
+
+// u(h) = sum over groups (left to right inside a group, groups added in
+// turn); parents slot-major: par[s * nh + k], weights w[s].
+template<class T>
+__global__ void
+k_hn_average(int nh, int B, const int* __restrict__ node, const int* __restrict__ par,
+             int nslots, int gsize, const double* __restrict__ w, T* __restrict__ u)
+{
+  GB_PDL_ENTRY();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nh)
+    return;
+  for (int c = 0; c < B; ++c) {
+    T acc = T(0);
+    for (int g = 0; g < nslots; g += gsize) {
+      T sg = hn_mul(static_cast<T>(w[g]), u[int64_t(par[g * nh + k]) * B + c]);
+      for (int s = g + 1; s < g + gsize; ++s)
+        sg = hn_add(sg, hn_mul(static_cast<T>(w[s]), u[int64_t(par[s * nh + k]) * B + c]));
+      acc = g == 0 ? sg : hn_add(acc, sg);
+    }
+    u[int64_t(node[k]) * B + c] = acc;
+  }
+}
+
+// parents += w * u(h) in ascending hanging-node order (one thread per parent:
+// its contributions in the reference's sequence)
+template<class T>
+__global__ void
+k_hn_distribute(int np, int B, const int* __restrict__ pnode, const int* __restrict__ ptr,
+                const int* __restrict__ hnode, const double* __restrict__ wt,
+                T* __restrict__ u)
+{
+  GB_PDL_ENTRY();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= np)
+    return;
+  const int64_t p = pnode[k];
+  for (int c = 0; c < B; ++c) {
+    T acc = u[p * B + c];
+    for (int e = ptr[k]; e < ptr[k + 1]; ++e)
+      acc = hn_add(acc, hn_mul(static_cast<T>(wt[e]), u[int64_t(hnode[e]) * B + c]));
+    u[p * B + c] = acc;
+  }
+}
+
+template<class T>
+__global__ void
+k_hn_zero(int nh, int B, const int* __restrict__ node, T* __restrict__ u)
+{
+  GB_PDL_ENTRY();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nh)
+    return;
+  for (int c = 0; c < B; ++c)
+    u[int64_t(node[k]) * B + c] = T(0);
+}
+
+} // namespace gb

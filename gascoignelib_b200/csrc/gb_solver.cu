@@ -290,6 +290,18 @@ struct Level
   DeviceArray<int> vk_pn, vk_nptr, vk_ent;
   DeviceArray<double> vk_inv64, vk_out64; // inverses [patch][j][i], solutions
   DeviceArray<float> vk_inv32, vk_out32;
+  // hanging nodes (gb_level_set_hn): phases in the discretisation's order
+  struct HnPhase
+  {
+    int nh = 0, nslots = 0, gsize = 0, np = 0;
+    DeviceArray<int> node, par, pnode, ptr, hnode;
+    DeviceArray<double> w, wt;
+  };
+  std::vector<HnPhase> hn;
+  std::vector<int> h_hnnodes;  // all hanging nodes
+  DeviceArray<int> hn_all;
+  DeviceArray<uint8_t> pmask;  // Dirichlet | hanging dofs (prolongation mask)
+  bool has_hn() const { return !hn.empty(); }
   int64_t ndof() const { return n * B; }
 };
 
@@ -896,10 +908,24 @@ ensure_work(Context& c)
   }
   for (int l = 0; l < c.nlevels; ++l)
     ensure_pf_scratch(c, c.L[l].n);
-  // the single-CTA coarse-level program covers scalar Jacobi cycles
+  for (int l = 0; l < c.nlevels; ++l) {
+    Level& L = c.L[l];
+    if (!L.has_hn())
+      continue;
+    std::vector<uint8_t> m(L.ndof(), 0);
+    GB_CUDA(cudaMemcpy(m.data(), L.dirmask.p, m.size(), cudaMemcpyDeviceToHost));
+    for (int h : L.h_hnnodes)
+      for (int cc = 0; cc < L.B; ++cc)
+        m[int64_t(h) * L.B + cc] = 1;
+    GB_CUDA(L.pmask.alloc(m.size()));
+    GB_CUDA(cudaMemcpy(L.pmask.p, m.data(), m.size(), cudaMemcpyHostToDevice));
+  }
+  // the single-CTA coarse-level program covers scalar Jacobi cycles without
+  // hanging-node steps
   bool simple = c.params.smoother == 0;
   for (int l = 0; l < c.nlevels; ++l)
-    simple = simple && c.L[l].B == 1 && !c.L[l].pf_mask;
+    simple = simple && c.L[l].B == 1 && !c.L[l].pf_mask &&
+             (l == c.nlevels - 1 || !c.L[l].has_hn());
   c.coarse_root = -1;
   for (int l = 0; l < c.nlevels && simple; ++l) {
     if (c.L[l].ndof() > kCoarseMaxRows)
@@ -924,6 +950,14 @@ ensure_work(Context& c)
 // Every step of the cycle goes through Emit: it either launches the step's
 // kernel on the context stream, or (rec set) appends it to the program of the
 // coarse-level kernel.
+// mask of the prolonged correction on a fine level: SetBoundaryVectorZero and
+// HNZero (the hanging dofs), Solver/stdmultilevelsolver.cc:515-517
+static const uint8_t*
+pmask_of(const Level& L)
+{
+  return L.has_hn() ? L.pmask.p : L.dirmask.p;
+}
+
 template<class T>
 struct Emit
 {
@@ -1121,6 +1155,44 @@ struct Emit
     launch(c, k_comp_sub<T>, stream_blocks(L.n), 256, (int)L.n, L.B, pf_comp(L), x, mean,
            1.0);
   }
+  // HNStructure::Average / Distribute / Zero on level l
+  void hn_average(int l, T* u)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    for (const auto& ph : L.hn)
+      launch(c, k_hn_average<T>, blocks_for(ph.nh, 128), 128, ph.nh, L.B,
+             (const int*)ph.node.p, (const int*)ph.par.p, ph.nslots, ph.gsize,
+             (const double*)ph.w.p, u);
+  }
+  void hn_distribute(int l, T* u)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    for (const auto& ph : L.hn) {
+      launch(c, k_hn_distribute<T>, blocks_for(ph.np, 128), 128, ph.np, L.B,
+             (const int*)ph.pnode.p, (const int*)ph.ptr.p, (const int*)ph.hnode.p,
+             (const double*)ph.wt.p, u);
+      launch(c, k_hn_zero<T>, blocks_for(ph.nh, 128), 128, ph.nh, L.B,
+             (const int*)ph.node.p, u);
+    }
+  }
+  void hn_zero(int l, T* u)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    if (!L.h_hnnodes.empty())
+      launch(c, k_hn_zero<T>, blocks_for(L.h_hnnodes.size(), 128), 128,
+             (int)L.h_hnnodes.size(), L.B, (const int*)L.hn_all.p, u);
+  }
+  void dirichlet_zero(int l, T* u)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    if (L.ndir)
+      launch(c, k_dirichlet_zero<T>, blocks_for(L.ndir, 256), 256, L.ndir,
+             (const int*)L.dirlist.p, u);
+  }
   // pressure filter on x: weighted (SubtractMean) or algebraic
   // (SubtractMeanAlgebraic) mean of every filtered component removed
   void pf_sub(int l, T* x, bool weighted)
@@ -1225,13 +1297,13 @@ struct Emit
       o.out = fine;
       o.in = coarse;
       o.in_n = Tr.nc;
-      o.mask = c.L[l + 1].dirmask.p;
+      o.mask = pmask_of(c.L[l + 1]);
       o.tptr = Tr.pptr.p;
       o.tent = Tr.pent.p;
       o.alpha = c.params.mgomega;
       return rec->push_back(o);
     }
-    const uint8_t* fm = c.L[l + 1].dirmask.p;
+    const uint8_t* fm = pmask_of(c.L[l + 1]);
     const double mw = c.params.mgomega;
     const int nb = blocks_for(Tr.nf, 256);
     switch (c.L[l + 1].B) {
@@ -1632,6 +1704,10 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
     E.resid(l, u, tmp, b);
     E.restrict_to(l - 1, tmp, W.b[l - 1].p);
   }
+  if (c.L[l - 1].has_hn()) { // HNDistribute, then SetBoundaryVectorZero again
+    E.hn_distribute(l - 1, W.b[l - 1].p);
+    E.dirichlet_zero(l - 1, W.b[l - 1].p);
+  }
   int j = (p0 == 'V') ? 1 : (p0 == 'W') ? 2 : (p0 == 'F') ? 3 : 0;
   T* uc = W.u[l - 1].p;
   T* tc = W.v[l - 1].p;
@@ -1645,7 +1721,11 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
     p0 = 'W';
   if (u_zero)
     E.fill0(l, u);
-  // Zero(v); prolongate_add; HNZero; SetBoundaryVectorZero(v); Add(u, mgomega, v)
+  // HNAverage(u_c); Zero(v); prolongate_add; HNZero(v); SetBoundaryVectorZero(v);
+  // Add(u, mgomega, v). (HNZero(u_c) after it is dead: u_c is zeroed before
+  // its next use.)
+  if (c.L[l - 1].has_hn())
+    E.hn_average(l - 1, uc);
   E.prolong(l - 1, uc, u);
   bool post_zero = false;
   smooth<T>(E, l, P.iterpost, u, tmp, b, post_zero);
@@ -2548,6 +2628,7 @@ gb_level_set_dirichlet(gb_ctx* ctx, int lvl, int64_t nnodes, const int64_t* node
     GB_CUDA(cudaMemcpy(L.dirlist.p, dofs.data(), dofs.size() * sizeof(int),
                        cudaMemcpyHostToDevice));
   L.ndir = static_cast<int>(dofs.size());
+  ctx->work_ready = false; // the prolongation mask of hanging levels includes it
   GB_API_END
 }
 
@@ -2924,6 +3005,180 @@ gb_level_set_pfilter(gb_ctx* ctx, int lvl, int comp_mask, const double* weights,
   L.pf_domain = domain;
   L.nhanging = nhanging;
   ctx->work_ready = false;
+  GB_API_END
+}
+
+int
+gb_level_set_hn(gb_ctx* ctx, int lvl, int disc, int64_t nedge, const int64_t* edges,
+                int64_t nface, const int64_t* faces)
+{
+  GB_API_BEGIN
+  ctx->version++;
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(disc >= 0 && disc <= 3, GB_EINVAL, "disc must be 0 (Q12d) .. 3 (Q23d)");
+  GB_REQUIRE(nedge >= 0 && nface >= 0 && (nedge == 0 || edges) && (nface == 0 || faces),
+             GB_EINVAL, "bad hanging-node lists");
+  const bool q2 = disc >= 2, d3 = disc == 1 || disc == 3;
+  GB_REQUIRE(d3 || nface == 0, GB_EINVAL, "face hanging nodes need a 3D discretisation");
+  auto check = [&](int64_t v) {
+    GB_REQUIRE(v >= 0 && v < L.n, GB_EINVAL, "hanging-node index out of range");
+  };
+  for (int64_t k = 0; k < nedge * 4; ++k)
+    check(edges[k]);
+  for (int64_t k = 0; k < nface * 10; ++k)
+    check(faces[k]);
+  // the phases' slots and weights, as the HNStructure classes use them
+  struct Spec
+  {
+    std::vector<int64_t> node;
+    std::vector<std::vector<int64_t>> par; // per hanging node, slot order
+    std::vector<double> w;
+    int gsize;
+  };
+  const double q2w[3] = { 0.375, 0.75, -0.125 };
+  Spec se, sf;
+  for (int64_t k = 0; k < nedge; ++k) {
+    se.node.push_back(edges[4 * k]);
+    std::vector<int64_t> pp;
+    for (int j = 0; j < (q2 ? 3 : 2); ++j)
+      pp.push_back(edges[4 * k + 1 + j]);
+    se.par.push_back(pp);
+  }
+  if (q2)
+    se.w = { q2w[0], q2w[1], q2w[2] }, se.gsize = 3;
+  else
+    se.w = { 0.5, 0.5 }, se.gsize = 2;
+  for (int64_t k = 0; k < nface; ++k) {
+    sf.node.push_back(faces[10 * k]);
+    std::vector<int64_t> pp;
+    if (q2)
+      for (int j = 0; j < 9; ++j)
+        pp.push_back(faces[10 * k + 1 + j]);
+    else
+      for (int j : { 0, 1, 3, 4 })
+        pp.push_back(faces[10 * k + 1 + j]);
+    sf.par.push_back(pp);
+  }
+  if (q2) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        sf.w.push_back(q2w[i] * q2w[j]);
+    sf.gsize = 3;
+  } else {
+    sf.w = { 0.25, 0.25, 0.25, 0.25 };
+    sf.gsize = 4;
+  }
+  std::vector<Spec*> order;
+  if (disc == 3)
+    order = { &sf, &se };
+  else if (disc == 1)
+    order = { &se, &sf };
+  else
+    order = { &se };
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  L.hn.clear();
+  L.h_hnnodes.clear();
+  std::vector<uint8_t> inphase(L.n, 0);
+  for (Spec* sp : order) {
+    const int nh = static_cast<int>(sp->node.size());
+    if (nh == 0)
+      continue;
+    // ascending hanging nodes (std::map order) and no chains inside a phase
+    std::fill(inphase.begin(), inphase.end(), 0);
+    for (int k = 0; k < nh; ++k) {
+      GB_REQUIRE(k == 0 || sp->node[k] > sp->node[k - 1], GB_EINVAL,
+                 "hanging nodes must be listed in ascending order");
+      inphase[sp->node[k]] = 1;
+    }
+    for (const auto& pp : sp->par)
+      for (int64_t q : pp)
+        GB_REQUIRE(!inphase[q], GB_EINVAL,
+                   "a hanging node is a parent of another of the same kind");
+    const int ns = static_cast<int>(sp->w.size());
+    std::vector<int> node(nh), par(size_t(ns) * nh);
+    for (int k = 0; k < nh; ++k) {
+      node[k] = static_cast<int>(sp->node[k]);
+      L.h_hnnodes.push_back(node[k]);
+      for (int s2 = 0; s2 < ns; ++s2)
+        par[size_t(s2) * nh + k] = static_cast<int>(sp->par[k][s2]);
+    }
+    // distribute: per parent, (hanging node, weight) in ascending hanging order
+    std::map<int, std::vector<std::pair<int, double>>> byp;
+    for (int k = 0; k < nh; ++k)
+      for (int s2 = 0; s2 < ns; ++s2)
+        byp[static_cast<int>(sp->par[k][s2])].push_back({ node[k], sp->w[s2] });
+    std::vector<int> pnode, ptr(1, 0), hnode;
+    std::vector<double> wt;
+    for (auto& kv : byp) {
+      pnode.push_back(kv.first);
+      for (auto& e : kv.second) {
+        hnode.push_back(e.first);
+        wt.push_back(e.second);
+      }
+      ptr.push_back(static_cast<int>(hnode.size()));
+    }
+    Level::HnPhase ph;
+    ph.nh = nh;
+    ph.nslots = ns;
+    ph.gsize = sp->gsize;
+    ph.np = static_cast<int>(pnode.size());
+    GB_CUDA(ph.node.alloc(nh));
+    GB_CUDA(ph.par.alloc(par.size()));
+    GB_CUDA(ph.w.alloc(ns));
+    GB_CUDA(ph.pnode.alloc(pnode.size()));
+    GB_CUDA(ph.ptr.alloc(ptr.size()));
+    GB_CUDA(ph.hnode.alloc(hnode.size()));
+    GB_CUDA(ph.wt.alloc(wt.size()));
+    GB_CUDA(cudaMemcpy(ph.node.p, node.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpy(ph.par.p, par.data(), par.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpy(ph.w.p, sp->w.data(), ns * sizeof(double), cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpy(ph.pnode.p, pnode.data(), pnode.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpy(ph.ptr.p, ptr.data(), ptr.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpy(ph.hnode.p, hnode.data(), hnode.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+    GB_CUDA(cudaMemcpy(ph.wt.p, wt.data(), wt.size() * sizeof(double),
+                       cudaMemcpyHostToDevice));
+    L.hn.push_back(std::move(ph));
+  }
+  if (!L.h_hnnodes.empty()) {
+    GB_CUDA(L.hn_all.alloc(L.h_hnnodes.size()));
+    GB_CUDA(cudaMemcpy(L.hn_all.p, L.h_hnnodes.data(), L.h_hnnodes.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+  }
+  ctx->work_ready = false;
+  GB_API_END
+}
+
+int
+gb_hn_average(gb_ctx* ctx, int lvl, int id)
+{
+  GB_API_BEGIN
+  level_with_matrix(*ctx, lvl);
+  Emit<double> E{ *ctx, nullptr };
+  E.hn_average(lvl, vec(*ctx, lvl, id));
+  GB_API_END
+}
+
+int
+gb_hn_distribute(gb_ctx* ctx, int lvl, int id)
+{
+  GB_API_BEGIN
+  level_with_matrix(*ctx, lvl);
+  Emit<double> E{ *ctx, nullptr };
+  E.hn_distribute(lvl, vec(*ctx, lvl, id));
+  GB_API_END
+}
+
+int
+gb_hn_zero(gb_ctx* ctx, int lvl, int id)
+{
+  GB_API_BEGIN
+  level_with_matrix(*ctx, lvl);
+  Emit<double> E{ *ctx, nullptr };
+  E.hn_zero(lvl, vec(*ctx, lvl, id));
   GB_API_END
 }
 

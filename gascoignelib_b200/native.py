@@ -86,6 +86,10 @@ _SIGS = {
     "gb_subtract_mean_algebraic": [C.c_void_p, C.c_int, C.c_int],
     "gb_level_set_patches": [C.c_void_p, C.c_int, C.c_int64, C.c_int, _P64],
     "gb_level_set_pfilter": [C.c_void_p, C.c_int, C.c_int, _PD, C.c_double, C.c_int64],
+    "gb_level_set_hn": [C.c_void_p, C.c_int, C.c_int, C.c_int64, _P64, C.c_int64, _P64],
+    "gb_hn_average": [C.c_void_p, C.c_int, C.c_int],
+    "gb_hn_distribute": [C.c_void_p, C.c_int, C.c_int],
+    "gb_hn_zero": [C.c_void_p, C.c_int, C.c_int],
     "gb_dirichlet_zero": [C.c_void_p, C.c_int, C.c_int],
     "gb_level_get_inverse_diagonal": [C.c_void_p, C.c_int, _PD, C.c_int64],
     "gb_restrict_zero": [C.c_void_p, C.c_int, C.c_int, C.c_int],
@@ -215,6 +219,13 @@ class Context:
                 pt = np.ascontiguousarray(lv.patches, dtype=np.int64)
                 self._chk(self._L.gb_level_set_patches(self.h, l, pt.shape[0], pt.shape[1],
                                                        _p64(pt)))
+            if getattr(lv, "hn_edges", None) is not None:
+                he = np.ascontiguousarray(lv.hn_edges, dtype=np.int64).reshape(-1, 4)
+                hf = np.ascontiguousarray(
+                    lv.hn_faces if lv.hn_faces is not None else np.zeros((0, 10)),
+                    dtype=np.int64).reshape(-1, 10)
+                self._chk(self._L.gb_level_set_hn(self.h, l, lv.hn_disc, he.shape[0],
+                                                  _p64(he), hf.shape[0], _p64(hf)))
             if getattr(lv, "pf_mask", 0):
                 w = np.ascontiguousarray(lv.pf_weights, dtype=np.float64)
                 self._chk(self._L.gb_level_set_pfilter(self.h, l, lv.pf_mask, _pd(w),
@@ -306,6 +317,10 @@ class Context:
 
     def smooth(self, level, niter, x, y, h):
         self._chk(self._L.gb_smooth(self.h, level, niter, x, y, h))
+
+    def hn(self, op, level, vid):
+        """op: "average", "distribute" or "zero"."""
+        self._chk(getattr(self._L, "gb_hn_" + op)(self.h, level, vid))
 
     def subtract_mean(self, level, vid, algebraic=False):
         f = self._L.gb_subtract_mean_algebraic if algebraic else self._L.gb_subtract_mean

@@ -132,6 +132,23 @@ int gb_level_size(const gb_ctx* ctx, int level, int64_t* n, int* B,
  * when a solve first needs them after a matrix or patch upload. */
 int gb_level_set_patches(gb_ctx* ctx, int level, int64_t npatch, int npp,
                          const int64_t* patches);
+/* Hanging nodes of a level as the mesh's HangingIndexHandler holds them
+ * (Mesh/hangingindexhandler.h:40,65): nedge rows [node, 3 parents] (hnq2) and,
+ * in 3D, nface rows [node, 9 parents] (hnq2face), nodes ascending, and the
+ * discretisation whose HNStructure acts on them (disc 0 Q12d, 1 Q13d, 2 Q22d,
+ * 3 Q23d: Discretization/Q1/hnstructureq12d.cc, hnstructureq13d.cc,
+ * Discretization/Q2/hnstructureq22d.cc, hnstructureq23d.cc; CGDisc::ReInit,
+ * DofHandler/cgdisc.cc:24-50). Replaces CudaSolver::NewMesh's HN matrices
+ * (cuda/cudasolver.cc:161-247). The cycle then applies HNDistribute after
+ * each restriction, HNAverage before each prolongation and HNZero to the
+ * prolonged correction (Solver/stdmultilevelsolver.cc:492-517). */
+int gb_level_set_hn(gb_ctx* ctx, int level, int disc, int64_t nedge,
+                    const int64_t* edges, int64_t nface, const int64_t* faces);
+/* StdSolver::HNAverage / HNDistribute / HNZero (Solver/stdsolver.h:365-367),
+ * CudaSolver's HN* overrides (cuda/cudasolver.cc:449-489). */
+int gb_hn_average(gb_ctx* ctx, int level, int id);
+int gb_hn_distribute(gb_ctx* ctx, int level, int id);
+int gb_hn_zero(gb_ctx* ctx, int level, int id);
 /* Pressure filter of a level (PressureFilter, Discretization/Q1/
  * pressurefilter.h:31-54; set up by StdSolver::NewMesh ->
  * CGDisc::InitFilter, Solver/stdsolver.cc:214-227, DofHandler/cgdisc.h:
