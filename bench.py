@@ -277,6 +277,49 @@ def stokes_c3(local, steps, warmup, flush):
     return out
 
 
+def q2_c4(local, steps, warmup, flush):
+    """C4 without the ball refinement: 3D CGQ2 convection-diffusion
+    -0.01 Laplace u + (1, 0.5, 0.25) . grad u = f on 80^3 cells (40^3 Q2
+    patches, 531,441 dofs, 33.1 M matrix entries, rows of up to 125),
+    Jacobi V(2,2) with omega 0.3 (0.5 and above stall on this convection-
+    dominated Q2 operator), GMRES(30) to 1e-8: mixed and FP64 solves,
+    device time, L2 flushed before every solve. (Hanging nodes are covered by
+    the parity tests; they add three small kernels per cycle.)"""
+    import torch
+
+    from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
+    from gascoignelib_b200.problem import structured_q2
+
+    P = structured_q2(3, 5, 4, eps=1e-2, beta=(1.0, 0.5, 0.25))
+    c = Context(local)
+    c.load_problem(P)
+    c.set_params(iterpre=2, iterpost=2, iterexact=10, omega=0.3, mgomega=1.0,
+                 mgtype="V", gmressize=31, tol=1e-8, globaltol=1e-300, maxiter=600)
+    l = P.nlevels - 1
+    x, b = c.vec(), c.vec()
+    c.upload(l, b, P.rhs)
+    out = {}
+    for name, prec in (("mixed", GB_FP32), ("fp64", GB_FP64)):
+        for _ in range(warmup):
+            c.fgmres(x, b, prec, check=False)
+        ms = []
+        for _ in range(steps):
+            flush.random_(0, 255)
+            torch.cuda.synchronize()
+            info = c.fgmres(x, b, prec, check=False)
+            ms.append(info["device_ms"])
+        t = sum(ms) / len(ms)
+        out[name] = {"value": P.finest.ndof / (t * 1e-3), "unit": "DoF/s",
+                     "ms_per_step": t, "iterations": info["iterations"],
+                     "restarts": info["restarts"], "status": info["status_name"],
+                     "true_rel_residual": info["true_rel_residual"]}
+    c.close()
+    out["workload"] = ("3D CGQ2 convection-diffusion eps 1e-2, beta (1,0.5,0.25), 80^3 cells, "
+                       "531,441 dofs, Jacobi V(2,2) omega 0.3, GMRES(30), tol 1e-8")
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -288,6 +331,8 @@ def main():
                     help="skip the 96^3 forward+adjoint+gradient measurement")
     ap.add_argument("--no-stokes", action="store_true",
                     help="skip the 512^2 Stokes/Vanka measurement")
+    ap.add_argument("--no-q2", action="store_true",
+                    help="skip the 80^3 Q2 convection-diffusion measurement")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -397,6 +442,9 @@ def main():
     stk = None
     if not args.no_stokes:
         stk = stokes_c3(local, min(args.steps, 5), 2, flush)
+    q2 = None
+    if not args.no_q2:
+        q2 = q2_c4(local, min(args.steps, 3), 1, flush)
 
     if rank == 0:
         cb = None
@@ -442,6 +490,7 @@ def main():
             "cpu_baseline": cb,
             "adjoint_c5": adj,
             "stokes_c3": stk,
+            "q2_c4": q2,
         }
         print(json.dumps(line))
     ctx.close()

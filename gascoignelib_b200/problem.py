@@ -508,3 +508,84 @@ def structured_stokes(dim: int, coarse: int, refine: int, visc: float = 1.0,
                    info={"generator": "structured-stokes", "coarse": coarse,
                          "refine": refine, "smoother": smoother, "visc": visc,
                          "stab": stab})
+
+
+# ------------------------------------------------------------------ Q2
+
+def _q2_1d(H: float):
+    """1D quadratic Lagrange element on [0, H] (nodes 0, H/2, H): mass,
+    stiffness and D[i, j] = integral of phi_j' phi_i."""
+    M = np.array([[4.0, 2.0, -1.0], [2.0, 16.0, 2.0], [-1.0, 2.0, 4.0]]) * (H / 30.0)
+    K = np.array([[7.0, -8.0, 1.0], [-8.0, 16.0, -8.0], [1.0, -8.0, 7.0]]) / (3.0 * H)
+    D = np.array([[-3.0, 4.0, -1.0], [-4.0, 0.0, 4.0], [1.0, -4.0, 3.0]]) / 6.0
+    return M, K, D
+
+
+def _q2_local(dim: int, H: float, eps: float, beta) -> np.ndarray:
+    """Q2 element matrix of -eps Laplace u + beta . grad u on a cube of width
+    H (a patch of 2^dim cells), local nodes lexicographic (x fastest)."""
+    M, K, D = _q2_1d(H)
+    if dim == 2:
+        A = eps * (np.kron(M, K) + np.kron(K, M))
+        if beta is not None:
+            A = A + beta[0] * np.kron(M, D) + beta[1] * np.kron(D, M)
+        return A
+    A = eps * (np.kron(np.kron(M, M), K) + np.kron(np.kron(M, K), M)
+               + np.kron(np.kron(K, M), M))
+    if beta is not None:
+        A = A + (beta[0] * np.kron(np.kron(M, M), D) + beta[1] * np.kron(np.kron(M, D), M)
+                 + beta[2] * np.kron(np.kron(D, M), M))
+    return A
+
+
+def _assemble_q2_level(dim: int, N: int, eps: float, beta) -> Level:
+    """CGQ2 on N^dim cells: Q2 elements on the (N/2)^dim patches, strong zero
+    Dirichlet on the whole boundary."""
+    import scipy.sparse as sp
+    h = 1.0 / N
+    n1 = N + 1
+    n = n1 ** dim
+    E = _q2_local(dim, 2.0 * h, eps, beta)
+    nodes = _patches(dim, N)
+    nl = nodes.shape[1]
+    rows = np.repeat(nodes, nl, axis=1).ravel()
+    cols = np.tile(nodes, (1, nl)).ravel()
+    vals = np.tile(E.ravel(), nodes.shape[0])
+    A = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+    A.sum_duplicates()
+    A.sort_indices()
+    idx = np.arange(n)
+    coords = [(idx // n1 ** d) % n1 for d in range(dim)]
+    onb = np.zeros(n, dtype=bool)
+    for c in coords:
+        onb |= (c == 0) | (c == N)
+    rowptr = A.indptr.astype(np.int64)
+    col = A.indices.astype(np.int64)
+    val = A.data.astype(np.float64).copy()
+    rowidx = np.repeat(np.arange(n), np.diff(rowptr))
+    val[onb[rowidx] | onb[col]] = 0.0
+    isdiag = rowidx == col
+    val[isdiag & onb[rowidx]] = 1.0
+    return Level(n=n, B=1, rowptr=rowptr, col=col, diag=np.nonzero(isdiag)[0].astype(np.int64),
+                 val=val, dirichlet=np.nonzero(onb)[0].astype(np.int64),
+                 coord=np.stack([c * h for c in coords], axis=1).astype(np.float64))
+
+
+def structured_q2(dim: int, coarse: int, refine: int, eps: float = 1e-2,
+                  beta=(1.0, 0.5, 0.25), rhs: Optional[np.ndarray] = None,
+                  seed: int = 1002) -> Problem:
+    """The reference's CGQ2 system (discname CGQ2, patchdepth 1) for
+    -eps Laplace u + beta . grad u = f on the unit square/cube of
+    (coarse*2^refine)^dim cells, lexicographic numbering, f ~ U[-1, 1] per
+    node (seeded), zero Dirichlet; the multigrid transfers are the nodal ones
+    of MgInterpolatorMatrix, as the reference uses them for Q2 as well."""
+    beta = None if beta is None else tuple(beta)[:dim]
+    levels = [_assemble_q2_level(dim, (2 * coarse) << l, eps, beta) for l in range(refine)]
+    transfers = [_structured_transfer(dim, (2 * coarse) << l) for l in range(refine - 1)]
+    nf = levels[-1].n
+    b = (np.random.default_rng(seed).uniform(-1.0, 1.0, size=nf) if rhs is None
+         else np.array(rhs, dtype=np.float64))
+    b[levels[-1].dirichlet] = 0.0
+    return Problem(dim=dim, levels=levels, transfers=transfers, rhs=b,
+                   info={"generator": "structured-q2", "coarse": coarse, "refine": refine,
+                         "eps": eps, "beta": None if beta is None else list(beta)})

@@ -230,3 +230,33 @@ def test_oracle_hanging_nodes_3d_live(disc):
     x, info = O.gmres(vmax=21, tol=1e-8)
     assert info["iterations"] == int(summ["iterations"][0])
     assert np.array_equal(x, np.fromfile(os.path.join(out, "solution.f64")))
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="compiled reference not present")
+@pytest.mark.parametrize("dim,coarse,refine", [(2, 2, 3), (3, 1, 3)])
+def test_structured_q2_matches_reference_assembly(dim, coarse, refine):
+    """problem.structured_q2 builds the reference's CGQ2 convection-diffusion
+    matrices (the bench's Q2 workload) in lexicographic numbering."""
+    import scipy.sparse as sp
+    from gascoignelib_b200.problem import structured_q2
+    N = coarse << refine
+    rhs = np.random.default_rng(1002).uniform(-1, 1, size=(N + 1) ** dim)
+    d = tempfile.mkdtemp()
+    out, summ = run_reference(d, threads=1, dim=dim, coarse=coarse, refine=refine,
+                              disc="Q2", diff=0.1, conv="1,0.5,0.25", dump=1,
+                              **write_inputs(d, None, rhs))
+    R = load_reference_dump(out)
+    P = structured_q2(dim, coarse, refine, eps=0.1, rhs=rhs)
+    for Lr, Lp in zip(R.levels, P.levels):
+        Nl = round(Lp.n ** (1.0 / dim)) - 1
+        perm = _lex_permutation(Lr, Nl, dim)
+        Ar = sp.csr_matrix((Lr.val, Lr.col, Lr.rowptr), shape=(Lr.n, Lr.n)).tocoo()
+        Ar = sp.csr_matrix((Ar.data, (perm[Ar.row], perm[Ar.col])), shape=(Lr.n, Lr.n))
+        Ap = sp.csr_matrix((Lp.val, Lp.col, Lp.rowptr), shape=(Lp.n, Lp.n))
+        assert Ar.nnz == Ap.nnz
+        assert abs(Ar - Ap).max() <= 1e-12 * abs(Ap).max()
+    x, info = Oracle(P).gmres(vmax=21, tol=1e-8)
+    u_ref = np.empty(P.finest.n)
+    u_ref[_lex_permutation(R.finest, N, dim)] = np.fromfile(os.path.join(out, "solution.f64"))
+    assert abs(info["iterations"] - int(summ["iterations"][0])) <= 1
+    assert rel_l2(x, u_ref) < 1e-7
