@@ -407,6 +407,9 @@ class Context:
             self._chk(rc)
         return x, info.as_dict()
 
+    def synchronize(self):
+        self._chk(self._L.gb_ctx_synchronize(self.h))
+
     def kernel_count(self):
         v = C.c_int64()
         self._chk(self._L.gb_get_kernel_count(self.h, C.byref(v)))

@@ -24,6 +24,9 @@ def main(argv=None):
     ap.add_argument("--solves", type=int, default=2)
     ap.add_argument("--refine", type=int, default=6)
     ap.add_argument("--spmv", type=int, default=0)
+    ap.add_argument("--smooth", type=int, default=0,
+                    help="only K FP64 smoothing sweeps on the finest level (StdSolver::smooth "
+                         "with the problem's smoother), after the set-up")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--problem", default="diffusion", choices=["diffusion", "stokes", "q2"],
                     help="stokes: 2D Q1/Q1 Stokes with Vanka on (2*2^(refine-1))^2 cells")
@@ -53,6 +56,16 @@ def main(argv=None):
         keys.setdefault("maxiter", 200)
         ctx.set_params(tol=1e-8, globaltol=1e-300, iterpre=2, iterpost=2, **keys)
         fl = P.nlevels - 1
+        if a.smooth:
+            x, y, h = ctx.vec(), ctx.vec(), ctx.vec()
+            ctx.upload(fl, y, P.rhs)
+            ctx.smooth(fl, 1, x, y, h)  # set-up (Vanka factors) outside the count
+            ctx.synchronize()
+            k0 = ctx.kernel_count()
+            ctx.smooth(fl, a.smooth, x, y, h)
+            ctx.synchronize()
+            print(json.dumps({"sweeps": a.smooth, "kernels": ctx.kernel_count() - k0}))
+            return
         if a.spmv:
             prec = GB_FP32 if a.precision == "fp32" else GB_FP64
             ms, by = ctx.bench_spmv(fl, prec, reps=a.spmv, flush_l2=2)
