@@ -36,7 +36,7 @@ k_bspmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
 #pragma unroll
   for (int r = 0; r < B; ++r)
     acc[r] = NEG ? static_cast<TA>(b[int64_t(row) * B + r]) : TA(0);
-#pragma unroll 2
+#pragma unroll 4
   for (int j = 0; j < w; ++j) {
     const int c = PAT ? row + ldg(cp + j) : ldg(cp + j * kSlice);
     TA xv[B], m[B2];
@@ -113,7 +113,7 @@ k_bspmv_resid_mean(SellView<TV> A, const T* __restrict__ x, T* __restrict__ y,
 #pragma unroll
     for (int r = 0; r < B; ++r)
       acc[r] = static_cast<TA>(b[int64_t(row) * B + r]);
-#pragma unroll 2
+#pragma unroll 4
     for (int j = 0; j < w; ++j) {
       const int c = PAT ? row + ldg(cp + j) : ldg(cp + j * kSlice);
       TA xv[B], m[B2];
@@ -387,6 +387,45 @@ k_vanka_inv(int npatch, int M, int B, const int* __restrict__ pn,
   for (int k = 0; k < R; ++k)
     if (lane + 32 * k < M)
       hout[int64_t(p) * M + lane + 32 * k] = static_cast<T>(acc[k]);
+}
+
+// The same for a patch size known at compile time (M <= 32: one row per lane):
+// every load of the warp's 27 (or 9) inverse columns is issued up front.
+template<int M, class TL, class T>
+__global__ void __launch_bounds__(32 * kVankaWarps)
+k_vanka_inv_ct(int npatch, int B, const int* __restrict__ pn, const TL* __restrict__ inv,
+               const T* __restrict__ h, int pc, const double* __restrict__ hmean,
+               T* __restrict__ hout)
+{
+  GB_PDL_ENTRY();
+  static_assert(M <= 32, "one row per lane");
+  using TA = typename Acc<TL, T>::type;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.x * kVankaWarps + wid;
+  if (p >= npatch)
+    return; // whole warp
+  const int64_t np = npatch;
+  const bool act = lane < M;
+  // this lane's row of the inverse (column j at ip[j * M]) and its residual entry
+  const TL* ip = inv + int64_t(p) * M * M + (act ? lane : 0);
+  TL a[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j)
+    a[j] = __ldg(ip + j * M);
+  TA hv = TA(0);
+  if (act) {
+    const int r = lane / B, c = lane - r * B;
+    const int node = __ldg(pn + r * np + p);
+    const T x = __ldg(h + int64_t(node) * B + c);
+    hv = (hmean && c == pc) ? static_cast<TA>(static_cast<double>(x) - *hmean)
+                            : static_cast<TA>(x);
+  }
+  TA acc = TA(0);
+#pragma unroll
+  for (int j = 0; j < M; ++j)
+    acc = fma(static_cast<TA>(a[j]), __shfl_sync(0xffffffffu, hv, j), acc);
+  if (act)
+    hout[int64_t(p) * M + lane] = static_cast<T>(acc);
 }
 
 // u(i, c) = (u_zero ? 0 : u(i, c)) + omega * ((sum over the node's patches of

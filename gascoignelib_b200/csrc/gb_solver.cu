@@ -1036,7 +1036,14 @@ struct Emit
     T* out = vk_out(L);
     const int pc = pf_comp(L);
     const int nbp = blocks_for(L.npatch, kVankaWarps);
-    switch ((L.vk_M + 31) / 32) {
+    if (L.vk_M == 27 || L.vk_M == 9) {
+      if (L.vk_M == 27)
+        launch(c, k_vanka_inv_ct<27, T, T>, nbp, 32 * kVankaWarps, L.npatch, L.B,
+               (const int*)L.vk_pn.p, inv, h, pc, hmean, out);
+      else
+        launch(c, k_vanka_inv_ct<9, T, T>, nbp, 32 * kVankaWarps, L.npatch, L.B,
+               (const int*)L.vk_pn.p, inv, h, pc, hmean, out);
+    } else switch ((L.vk_M + 31) / 32) {
       case 1:
         launch(c, k_vanka_inv<1, T, T>, nbp, 32 * kVankaWarps, L.npatch, L.vk_M, L.B,
                (const int*)L.vk_pn.p, inv, h, pc, hmean, out);
