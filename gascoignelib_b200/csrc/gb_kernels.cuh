@@ -28,7 +28,9 @@ enum SpmvMode
   kAddAx = 1,    // y = y + alpha * (A x)
   kResid = 2,    // y = b - A x
   kResidDir = 3, // y = b - A x, then 0 on Dirichlet dofs
-  kJacobi = 4    // y = x + alpha * dinv * (b - A x)     (y != x)
+  kJacobi = 4,   // y = x + alpha * dinv * (b - A x)     (y != x)
+  kJacobi2 = 5   // two sweeps from x = 0: x1 = alpha * dinv * b formed on the
+                 // fly (rounded to the vector type), y = x1 + alpha dinv (b - A x1)
 };
 
 // Accumulator type: FP64 when matrix or output is FP64, FP32 only when
@@ -134,8 +136,15 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
   const TV* vp = A.val + beg + lane;
   const int* cp = PAT ? (A.ptab + int(A.pid[row]) * A.W) : (A.col + beg + lane);
   const TA alpha = static_cast<TA>(alpha_);
-  constexpr bool NEG = (MODE == kResid || MODE == kResidDir || MODE == kJacobi);
+  constexpr bool NEG =
+    (MODE == kResid || MODE == kResidDir || MODE == kJacobi || MODE == kJacobi2);
   TA acc = NEG ? static_cast<TA>(b[row]) : TA(0);
+  // kJacobi2: the first sweep's iterate, exactly as k_jacobi_from_zero stores it
+  auto x1 = [&](int c) {
+    return static_cast<TA>(static_cast<TX>(
+      static_cast<TA>(alpha_) *
+      (static_cast<TA>(ldg(dinv + c)) * static_cast<TA>(ldg(b + c)))));
+  };
   for (int j0 = 0; j0 < w; j0 += kChunk) {
     TA av[kChunk], xv[kChunk];
 #pragma unroll
@@ -144,7 +153,7 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
       if (j < w) {
         const int c = PAT ? row + ldg(cp + j) : ldg(cp + j * kSlice);
         av[q] = static_cast<TA>(ldg(vp + j * kSlice));
-        xv[q] = static_cast<TA>(ldg(x + c));
+        xv[q] = MODE == kJacobi2 ? x1(c) : static_cast<TA>(ldg(x + c));
       } else {
         av[q] = TA(0);
         xv[q] = TA(0);
@@ -167,9 +176,12 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
     y[row] = static_cast<TO>(acc);
   } else if (MODE == kResidDir) {
     y[row] = dirmask[row] ? TO(0) : static_cast<TO>(acc);
-  } else { // kJacobi: reference order h = d*h; x = x + omega*h
+  } else if (MODE == kJacobi) { // reference order h = d*h; x = x + omega*h
     const TA h = static_cast<TA>(dinv[row]) * acc;
     y[row] = static_cast<TO>(static_cast<TA>(x[row]) + alpha * h);
+  } else { // kJacobi2: the second sweep on top of x1
+    const TA h = static_cast<TA>(dinv[row]) * acc;
+    y[row] = static_cast<TO>(x1(row) + alpha * h);
   }
 }
 

@@ -396,6 +396,10 @@ struct gb_ctx
   bool coarse_dense = true; // apply the coarse sub-cycle as its precomputed map
   bool use_graph = true; // flexible solver as one CUDA graph (GB_GRAPH=0: host loops)
   bool pdl = true;       // programmatic dependent launch between kernels
+  // first two sweeps from zero in one pass (GB_JACOBI2=1); off by default:
+  // the saved launch costs more in the second sweep's extra gathers (C2: mixed
+  // 1.680 vs 1.670 ms, FP64 1.91 vs 1.86 ms)
+  bool jacobi2 = false;
   // per-kernel timing
   bool ktime = false;
   struct KtPending
@@ -999,6 +1003,13 @@ struct Emit
     else
       jacobi_apply(l, b, u, true);
   }
+  // out = two Jacobi sweeps from 0 (scalar levels)
+  void jacobi_two_from_zero(int l, T* out, const T* b)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    spmv<kJacobi2, T, T, T>(c, L, opA(c, L), b, out, b, dinv_of<T>(L), c.params.omega);
+  }
   // u = (u_zero ? 0 : u) + omega D^-1 h (block Jacobi update, h given;
   // h's filtered component read minus *hmean when set; the weighted mean of
   // the new u reduced into scal[9] when the level has one filtered component)
@@ -1376,7 +1387,14 @@ smooth(Emit<T>& E, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
   const bool fused = fused_smoother(c, L);
   for (int it = 0; it < niter; ++it) {
     if (fused) {
-      if (u_zero) {
+      if (u_zero && it + 1 < niter && L.B == 1 && !E.rec && c.jacobi2) {
+        // the first two sweeps from u = 0 in one pass (the first iterate is
+        // formed on the fly where the second reads it)
+        E.jacobi_two_from_zero(l, tmp, b);
+        std::swap(u, tmp);
+        u_zero = false;
+        ++it;
+      } else if (u_zero) {
         E.jacobi_zero(l, u, b);
         u_zero = false;
       } else {
@@ -2435,6 +2453,8 @@ gb_ctx_create(gb_ctx** out, int device)
       ctx->use_graph = atoi(e) != 0;
     if (const char* e = getenv("GB_COARSE_DENSE"))
       ctx->coarse_dense = atoi(e) != 0;
+    if (const char* e = getenv("GB_JACOBI2"))
+      ctx->jacobi2 = atoi(e) != 0;
     if (const char* e = getenv("GB_PDL"))
       ctx->pdl = atoi(e) != 0;
     GB_CUDA(cudaSetDevice(device));
