@@ -429,6 +429,12 @@ def _patches(dim: int, N: int) -> np.ndarray:
     return (base[:, None] + loc[None, :]).astype(np.int64)
 
 
+def cell_patches(dim: int, N: int) -> np.ndarray:
+    """Single-cell Vanka patches (2^dim nodes): the 4-node (2D) cell patches of
+    the 12 x 12 Stokes variant, one per cell, lexicographic."""
+    return cell_nodes(dim, N)
+
+
 def _assemble_stokes_level(dim: int, N: int, visc: float, stab: float) -> Level:
     import scipy.sparse as sp
     h = 1.0 / N
@@ -490,15 +496,20 @@ def stokes_rhs(dim: int, coarse: int, refine: int, seed: int = 1002) -> np.ndarr
 
 def structured_stokes(dim: int, coarse: int, refine: int, visc: float = 1.0,
                       stab: float = 0.1, rhs: Optional[np.ndarray] = None,
-                      smoother: str = "vanka") -> Problem:
+                      smoother: str = "vanka", patches: str = "patch") -> Problem:
     """The reference's multilevel Stokes system (Q1/Q1, Brezzi-Pitkaranta
     pressure stabilisation, velocity Dirichlet on the whole boundary, pressure
     filter on component 0, Vanka patches of 2^dim cells) on the unit
     square/cube in lexicographic numbering: what the oracle harness assembles
-    with problem=stokes, in another node order."""
+    with problem=stokes, in another node order. patches="cell" puts the Vanka
+    smoother on single cells instead (2^dim-node patches; the reference's
+    VankaSmoother uses 2^dim-cell patches only)."""
     nlev = refine
     levels = [_assemble_stokes_level(dim, (2 * coarse) << l, visc, stab)
               for l in range(nlev)]
+    if patches == "cell":  # Vanka on single cells (12 x 12 local systems in 2D)
+        for l, lv in enumerate(levels):
+            lv.patches = cell_patches(dim, (2 * coarse) << l)
     transfers = [_structured_transfer(dim, (2 * coarse) << l) for l in range(nlev - 1)]
     b = stokes_rhs(dim, coarse, refine) if rhs is None else np.array(rhs, dtype=np.float64)
     fin = levels[-1]
@@ -507,7 +518,7 @@ def structured_stokes(dim: int, coarse: int, refine: int, visc: float = 1.0,
     return Problem(dim=dim, levels=levels, transfers=transfers, rhs=bd.ravel(),
                    info={"generator": "structured-stokes", "coarse": coarse,
                          "refine": refine, "smoother": smoother, "visc": visc,
-                         "stab": stab})
+                         "stab": stab, "patches": patches})
 
 
 # ------------------------------------------------------------------ Q2

@@ -157,3 +157,30 @@ def test_c3_stokes_vanka_full_size(ctx):
         assert rel_l2(ctx.download(l, x), xo) < 1e-5
     ctx.free(x)
     ctx.free(b)
+
+
+def test_vanka_cell_patches_match_oracle(ctx):
+    """The 12 x 12 variant (Vanka on single cells, 4 nodes x 3 components):
+    sweeps and the GMRES solve against the oracle with the same patches."""
+    from gascoignelib_b200.problem import structured_stokes
+    P = structured_stokes(2, 2, 5, patches="cell")
+    assert P.finest.patches.shape[1] == 4
+    O = Oracle(P, omega=1.0)
+    ctx.load_problem(P)
+    ctx.set_params(gmressize=31, tol=1e-8, globaltol=1e-16, maxiter=200, omega=1.0)
+    rng = np.random.default_rng(6)
+    l = P.nlevels - 1
+    xv, yv = rng.normal(size=P.finest.ndof), rng.normal(size=P.finest.ndof)
+    x, y, h = ctx.vec(), ctx.vec(), ctx.vec()
+    ctx.upload(l, x, xv)
+    ctx.upload(l, y, yv)
+    ctx.smooth(l, 2, x, y, h)
+    assert rel(ctx.download(l, x), O.smooth(l, 2, xv, yv)) < 1e-11
+    xo, io = O.gmres(vmax=31, tol=1e-8, maxiter=200)
+    ctx.upload(l, y, P.rhs)
+    info = ctx.gmres(x, y)
+    assert info["status_name"] == "converged"
+    assert abs(info["iterations"] - io["iterations"]) <= 1
+    assert rel_l2(ctx.download(l, x), xo) < 1e-8
+    for v in (x, y, h):
+        ctx.free(v)
