@@ -23,10 +23,11 @@ k_bspmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
   GB_PDL_ENTRY();
   using TA = typename Acc<TV, TO>::type;
   constexpr int B2 = B * B;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= A.n)
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= A.n)
     return;
-  const int s = row >> 5, lane = row & 31;
+  const int row = A.perm ? __ldg(A.perm + slot) : slot;
+  const int s = slot >> 5, lane = slot & 31;
   const int beg = A.sptr[s];
   const int w = (A.sptr[s + 1] - beg) >> 5;
   const TV* vp = A.val + int64_t(beg) * B2 + lane;
@@ -101,10 +102,11 @@ k_bspmv_resid_mean(SellView<TV> A, const T* __restrict__ x, T* __restrict__ y,
   using TA = typename Acc<TV, T>::type;
   constexpr int B2 = B * B;
   __shared__ double sh[32];
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   double v = 0.0;
-  if (row < A.n) {
-    const int s = row >> 5, lane = row & 31;
+  if (slot < A.n) {
+    const int row = A.perm ? __ldg(A.perm + slot) : slot;
+    const int s = slot >> 5, lane = slot & 31;
     const int beg = A.sptr[s];
     const int w = (A.sptr[s + 1] - beg) >> 5;
     const TV* vp = A.val + int64_t(beg) * B2 + lane;

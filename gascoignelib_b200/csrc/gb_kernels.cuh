@@ -94,8 +94,11 @@ ld8(uint32_t (&v)[8], const uint32_t* const (&p)[8])
                : "l"(p[0]), "l"(p[1]), "l"(p[2]), "l"(p[3]), "l"(p[4]), "l"(p[5]),
                  "l"(p[6]), "l"(p[7]));
 }
-// Device view of one SELL-32 matrix. Slice s holds rows 32s..32s+31,
-// column-major: entry j of lane l at sptr[s] + 32 j + l. Column indices are
+// Device view of one SELL-32 matrix. Slice s holds slots 32s..32s+31,
+// column-major: entry j of lane l at sptr[s] + 32 j + l; slot t holds row
+// perm[t] (identity when perm is null; with perm the rows of each window of
+// 256 are ordered by length, which removes the padding of matrices whose rows
+// alternate in length, e.g. Q2; every row keeps its own entry order). Column indices are
 // either explicit (col) or, when the rows of the level share few column-offset
 // patterns, implicit: row + ptab[pid[row] * W + j] (pattern-compressed SELL).
 template<class TV>
@@ -108,6 +111,7 @@ struct SellView
   const int* ptab;     // [npatterns][W] offsets col - row (0-padded)
   int W;
   const TV* val;
+  const int* perm;     // slot -> row (rows sorted by length in windows), or null
 };
 
 // y = f(A x) for one row per thread, columns in the reference's stored order.
@@ -127,10 +131,11 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
 {
   GB_PDL_ENTRY();
   using TA = typename Acc<TV, TO>::type;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= A.n)
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= A.n)
     return;
-  const int s = row >> 5, lane = row & 31;
+  const int row = A.perm ? __ldg(A.perm + slot) : slot;
+  const int s = slot >> 5, lane = slot & 31;
   const int beg = A.sptr[s];
   const int w = (A.sptr[s + 1] - beg) >> 5;
   const TV* vp = A.val + beg + lane;

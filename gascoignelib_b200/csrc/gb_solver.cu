@@ -120,6 +120,9 @@ struct Sell
   int npat = 0, W = 0;
   DeviceArray<uint8_t> pid;
   DeviceArray<int> ptab;
+  // slot -> row when the rows are ordered by length in windows (SELL-C-sigma)
+  bool sorted = false;
+  DeviceArray<int> rperm;
 };
 
 template<class TV>
@@ -128,7 +131,7 @@ view(const Sell& S, const TV* val)
 {
   return SellView<TV>{ S.n, S.sptr.p, S.pat ? nullptr : S.col.p,
                        S.pat ? S.pid.p : nullptr, S.pat ? S.ptab.p : nullptr,
-                       S.W, val };
+                       S.W, val, S.sorted ? S.rperm.p : nullptr };
 }
 
 // Rows whose column lists, relative to the row, coincide share one pattern. A
@@ -184,13 +187,43 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
   S.n = static_cast<int>(n);
   S.nslices = static_cast<int>((n + kSlice - 1) / kSlice);
   S.nnz = rowptr[n];
+  // Slot order: rows sorted by length (descending, stable) inside windows of
+  // kSortWindow rows when that saves more than a tenth of the padded slots
+  // (levels above the single-CTA coarse size only).
+  constexpr int64_t kSortWindow = 256;
+  std::vector<int> perm(n);
+  for (int64_t r = 0; r < n; ++r)
+    perm[r] = static_cast<int>(r);
+  auto padded = [&](const std::vector<int>& pm) {
+    int64_t tot = 0;
+    for (int64_t s0 = 0; s0 < n; s0 += kSlice) {
+      int64_t w = 0;
+      for (int64_t t = s0; t < std::min<int64_t>(n, s0 + kSlice); ++t)
+        w = std::max<int64_t>(w, rowptr[pm[t] + 1] - rowptr[pm[t]]);
+      tot += w * kSlice;
+    }
+    return tot;
+  };
+  S.sorted = false;
+  if (n > 1024) {
+    std::vector<int> sp(perm);
+    for (int64_t w0 = 0; w0 < n; w0 += kSortWindow)
+      std::stable_sort(sp.begin() + w0, sp.begin() + std::min<int64_t>(n, w0 + kSortWindow),
+                       [&](int a, int b) {
+                         return rowptr[a + 1] - rowptr[a] > rowptr[b + 1] - rowptr[b];
+                       });
+    if (padded(sp) * 10 < padded(perm) * 9) {
+      perm.swap(sp);
+      S.sorted = true;
+    }
+  }
   std::vector<int> sptr(S.nslices + 1, 0);
   for (int s = 0; s < S.nslices; ++s) {
     int64_t w = 0;
     for (int l = 0; l < kSlice; ++l) {
-      int64_t r = int64_t(s) * kSlice + l;
-      if (r < n)
-        w = std::max<int64_t>(w, rowptr[r + 1] - rowptr[r]);
+      int64_t t = int64_t(s) * kSlice + l;
+      if (t < n)
+        w = std::max<int64_t>(w, rowptr[perm[t] + 1] - rowptr[perm[t]]);
     }
     int64_t next = int64_t(sptr[s]) + w * kSlice;
     GB_REQUIRE(next < (int64_t(1) << 31), GB_EINVAL,
@@ -204,8 +237,9 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
   for (int s = 0; s < S.nslices; ++s) {
     int w = (sptr[s + 1] - sptr[s]) / kSlice;
     for (int l = 0; l < kSlice; ++l) {
-      int64_t r = int64_t(s) * kSlice + l;
-      int64_t len = r < n ? rowptr[r + 1] - rowptr[r] : 0;
+      const int64_t t = int64_t(s) * kSlice + l;
+      const int64_t r = t < n ? perm[t] : t;
+      int64_t len = t < n ? rowptr[r + 1] - rowptr[r] : 0;
       for (int j = 0; j < w; ++j) {
         int64_t e = sptr[s] + int64_t(j) * kSlice + l;
         if (j < len) {
@@ -236,6 +270,11 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
                             cudaMemcpyHostToDevice, st));
     GB_CUDA(cudaMemcpyAsync(S.v32.p, v32.data(), v32.size() * sizeof(float),
                             cudaMemcpyHostToDevice, st));
+  }
+  if (S.sorted) {
+    GB_CUDA(S.rperm.alloc(n));
+    GB_CUDA(cudaMemcpyAsync(S.rperm.p, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                            st));
   }
   // host vectors must outlive the async copies
   GB_CUDA(cudaStreamSynchronize(st));
@@ -981,6 +1020,7 @@ struct Emit
     o.in_n = in ? o.n : 0;
     o.b_n = b ? o.n : 0;
     const Sell& A = opA(c, L);
+    GB_REQUIRE(!A.sorted, GB_EINVAL, "coarse-level program on a row-sorted matrix");
     o.sptr = A.sptr.p;
     o.col = A.pat ? nullptr : A.col.p;
     o.pid = A.pat ? A.pid.p : nullptr;
