@@ -1078,7 +1078,9 @@ enum CoarseOpKind
   kOpResid = 2,      // out = b - A in
   kOpRestrict = 3,   // out = R in, 0 on mask
   kOpFill0 = 4,      // out = 0
-  kOpProlong = 5     // out += omega * (mask ? 0 : P in)
+  kOpProlong = 5,    // out += omega * (mask ? 0 : P in)
+  kOpDense = 6       // out = K in (n x in_n, row-major K in val): a coarse
+                     // sub-cycle's precomputed map (multi-CTA program only)
 };
 
 struct CoarseOp
@@ -1100,6 +1102,7 @@ struct CoarseOp
   const int* tptr;
   const uint32_t* tent;
   double alpha;
+  const int* perm;   // SELL slot -> row of a row-sorted level (multi-CTA only)
 };
 
 
@@ -1276,6 +1279,169 @@ k_coarse_cycle(const CoarseOp* __restrict__ ops, int nops,
     const T* sv = reinterpret_cast<const T*>(smem + cb.off);
     for (int q = t; q < cb.bytes / int(sizeof(T)); q += kCoarseThreads)
       g[q] = sv[q];
+  }
+}
+
+// ----------------------------------------------------- multi-CTA program
+//
+// The same op program over the middle levels (between the finest level and
+// the single-CTA coarse levels), run by one persistent cooperative grid: the
+// vectors stay in global memory (they fit in L2), every op is spread over all
+// threads, and a grid barrier separates the ops. Vector reads go through L2
+// (ld.global.cg): other CTAs wrote them earlier in the same launch. The
+// barrier's wait is bounded: after kMidSpinLimit polls it sets *err and the
+// kernel runs to its end (results then invalid; the host reports the flag).
+constexpr int kMidThreads = 256;
+constexpr unsigned long long kMidSpinLimit = 1ull << 26;
+
+__device__ __forceinline__ void
+mid_barrier(unsigned* bar, unsigned target, int* err)
+{
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // release this block's writes with the arrival, acquire the others' with
+    // the observation of the final count
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+    unsigned long long spins = 0;
+    for (;;) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if (v >= target)
+        break;
+      if (++spins > kMidSpinLimit || *reinterpret_cast<volatile int*>(err)) {
+        atomicExch(err, 1);
+        break;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template<class T, bool NEG>
+__device__ __forceinline__ T
+mid_row_spmv(const CoarseOp& op, const T* __restrict__ x, int slot, int r, T acc)
+{
+  const int s = slot >> 5, lane = slot & 31;
+  const int beg = __ldg(op.sptr + s);
+  const int w = (__ldg(op.sptr + s + 1) - beg) >> 5;
+  const T* val = static_cast<const T*>(op.val) + beg + lane;
+  const int* prow = op.pid ? op.ptab + int(__ldg(op.pid + r)) * op.W : nullptr;
+  const int* crow = op.col + beg + lane;
+  for (int j0 = 0; j0 < w; j0 += 8) {
+    const T* pa[8];
+    int c[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int j = min(j0 + q, w - 1);
+      pa[q] = val + j * kSlice;
+      c[q] = prow ? r + __ldg(prow + j) : __ldg(crow + j * kSlice);
+    }
+    T av[8], xv[8];
+    ld8(av, pa);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      xv[q] = __ldcg(x + c[q]);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (j0 + q < w)
+        acc = NEG ? fma(-av[q], xv[q], acc) : fma(av[q], xv[q], acc);
+  }
+  return acc;
+}
+
+template<class T>
+__device__ __forceinline__ T
+mid_row_transfer(const CoarseOp& op, const T* __restrict__ src, int i)
+{
+  const int beg = __ldg(op.tptr + (i >> 5));
+  const int w = (__ldg(op.tptr + (i >> 5) + 1) - beg) >> 5;
+  const uint32_t* ep = op.tent + beg + (i & 31);
+  T acc = T(0);
+  for (int j0 = 0; j0 < w; j0 += 8) {
+    const uint32_t* pe[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      pe[q] = ep + min(j0 + q, w - 1) * kSlice;
+    uint32_t e[8];
+    ld8(e, pe);
+    T f[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      f[q] = __ldcg(src + (e[q] & kIdxMask));
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (j0 + q < w)
+        acc = fma(wcode<T>(e[q]), f[q], acc);
+  }
+  return acc;
+}
+
+template<class T>
+__global__ void __launch_bounds__(kMidThreads)
+k_mid_cycle(const CoarseOp* __restrict__ ops, int nops, unsigned* bar, int* err)
+{
+  GB_PDL_ENTRY();
+  const int nthr = gridDim.x * blockDim.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int k = 0; k < nops; ++k) {
+    const CoarseOp op = ops[k];
+    T* out = static_cast<T*>(op.out);
+    const T* in = static_cast<const T*>(op.in);
+    const T* b = static_cast<const T*>(op.b);
+    if (op.kind == kOpDense) {
+      // one warp per row, FP64 accumulation in fixed lane order
+      const T* K = static_cast<const T*>(op.val);
+      const int lane = threadIdx.x & 31;
+      for (int i = gt >> 5; i < op.n; i += nthr >> 5) {
+        const T* row = K + int64_t(i) * op.in_n;
+        double acc = 0.0;
+        for (int j = lane; j < op.in_n; j += 32)
+          acc = fma(double(__ldg(row + j)), double(__ldcg(in + j)), acc);
+        for (int o = 16; o > 0; o >>= 1)
+          acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0)
+          out[i] = static_cast<T>(acc);
+      }
+    } else {
+      for (int t = gt; t < op.n; t += nthr) {
+        const int r = op.perm ? __ldg(op.perm + t) : t;
+        switch (op.kind) {
+          case kOpJacobiZero: {
+            const T d = __ldg(static_cast<const T*>(op.dinv) + r);
+            out[r] = static_cast<T>(op.alpha) * (d * __ldcg(b + r));
+            break;
+          }
+          case kOpJacobi: {
+            const T acc = mid_row_spmv<T, true>(op, in, t, r, __ldcg(b + r));
+            const T h = __ldg(static_cast<const T*>(op.dinv) + r) * acc;
+            out[r] = __ldcg(in + r) + static_cast<T>(op.alpha) * h;
+            break;
+          }
+          case kOpResid:
+            out[r] = mid_row_spmv<T, true>(op, in, t, r, __ldcg(b + r));
+            break;
+          case kOpRestrict: {
+            const T acc = mid_row_transfer<T>(op, in, r);
+            out[r] = (op.mask && __ldg(op.mask + r)) ? T(0) : acc;
+            break;
+          }
+          case kOpFill0:
+            out[r] = T(0);
+            break;
+          case kOpProlong: {
+            T acc = mid_row_transfer<T>(op, in, r);
+            if (op.mask && __ldg(op.mask + r))
+              acc = T(0);
+            out[r] = __ldcg(out + r) + static_cast<T>(op.alpha) * acc;
+            break;
+          }
+          default:
+            break;
+        }
+      }
+    }
+    if (k + 1 < nops)
+      mid_barrier(bar, unsigned(k + 1) * gridDim.x, err);
   }
 }
 

@@ -455,6 +455,18 @@ struct gb_ctx
   // (block systems, Vanka, pressure filter): levels 0..dense_root
   int dense_root = -1;
   std::map<gb::CoarseKey, gb::CoarseProgram> dense_maps;
+  // multi-CTA program for the levels below the finest (mid_level and down)
+  // GB_MID=1: the levels below the finest as one cooperative persistent grid
+  // with grid barriers between the ops. Off by default: on C2 it measured
+  // slower than the per-level kernels with programmatic dependent launch
+  // (mixed solve 1.97 vs 1.69 ms): each op there is itself latency-bound
+  // (1-2 rows per thread) and a grid barrier costs about as much as a launch.
+  bool mid_on = false;
+  int mid_level = -1;
+  std::map<gb::CoarseKey, gb::CoarseProgram> mid_progs;
+  gb::DeviceArray<unsigned> midbar;
+  gb::DeviceArray<int> miderr;
+  int mid_grid[2] = { 0, 0 }; // per precision (FP64, FP32)
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
   gb::DeviceArray<float> rhs32, zfix32;
   ~gb_ctx()
@@ -981,8 +993,17 @@ ensure_work(Context& c)
       break;
     c.dense_root = l;
   }
+  c.mid_level = -1;
+  if (simple && c.mid_on && c.coarse_on && c.nlevels >= 2 && c.nlevels - 2 > c.coarse_root)
+    c.mid_level = c.nlevels - 2;
+  if (c.midbar.n < 1) {
+    GB_CUDA(c.midbar.alloc(1));
+    GB_CUDA(c.miderr.alloc(1));
+    GB_CUDA(cudaMemsetAsync(c.miderr.p, 0, sizeof(int), c.stream));
+  }
   c.coarse_progs.clear();
   c.dense_maps.clear();
+  c.mid_progs.clear();
   c.work_ready = true;
 }
 
@@ -1007,6 +1028,7 @@ struct Emit
   Context& c;
   std::vector<CoarseOp>* rec = nullptr;
   int no_dense_at = -1; // level whose dense map is being built (run its steps)
+  bool mid = false;     // recording the multi-CTA program (coarse root: dense op)
 
   CoarseOp level_op(int kind, const Level& L, void* out, const void* in,
                     const void* b, double alpha) const
@@ -1020,13 +1042,14 @@ struct Emit
     o.in_n = in ? o.n : 0;
     o.b_n = b ? o.n : 0;
     const Sell& A = opA(c, L);
-    GB_REQUIRE(!A.sorted, GB_EINVAL, "coarse-level program on a row-sorted matrix");
+    GB_REQUIRE(!A.sorted || mid, GB_EINVAL, "coarse-level program on a row-sorted matrix");
     o.sptr = A.sptr.p;
     o.col = A.pat ? nullptr : A.col.p;
     o.pid = A.pat ? A.pid.p : nullptr;
     o.ptab = A.pat ? A.ptab.p : nullptr;
     o.W = A.W;
     o.val = sell_vals<T>(A);
+    o.perm = A.sorted ? A.rperm.p : nullptr;
     o.dinv = dinv_of<T>(L);
     o.mask = L.dirmask.p;
     o.alpha = alpha;
@@ -1487,6 +1510,11 @@ template<class T>
 static bool mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel,
                    char& p0, char p, T*& u, T*& tmp, const T* b, bool u_zero);
 
+template<class T>
+static const CoarseProgram& coarse_program(Context& c, MgWork<T>& W, int l, int finelevel,
+                                           int coarselevel, char p0, char p, T* u, T* tmp,
+                                           const T* b, bool u_zero);
+
 // Runs mgstep(l) for a level handled by the coarse-level kernel: the step is
 // recorded once per entry state (cached) and launched as one single-CTA kernel.
 template<class T>
@@ -1495,6 +1523,133 @@ run_coarse(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char
            char p, T*& u, T*& tmp, const T* b, bool u_zero)
 {
   Context& c = E.c;
+  const CoarseProgram& prog =
+    coarse_program<T>(c, W, l, finelevel, coarselevel, p0, p, u, tmp, b, u_zero);
+  if (prog.nops > 0 && prog.ncols > 0) {
+    const T* K = sizeof(T) == 8 ? reinterpret_cast<const T*>(prog.K64.p)
+                                : reinterpret_cast<const T*>(prog.K32.p);
+    launch(c, k_coarse_apply<T>, blocks_for(int64_t(prog.n_root) * 32, 256), 256,
+           prog.n_root, prog.ncols, prog.nb, K, static_cast<const T*>(prog.b_root),
+           static_cast<const T*>(prog.u_in),
+           static_cast<T*>(const_cast<void*>(prog.u_out)));
+  } else if (prog.nops > 0) {
+    launch_smem(c, k_coarse_cycle<T>, 1, kCoarseThreads, prog.smem_bytes,
+                (const CoarseOp*)prog.ops.p, prog.nops, (const CoarseBuf*)prog.bufs.p,
+                prog.nbufs, (const CoarsePrefetch*)prog.pre.p, prog.npre,
+                prog.vec_bytes, CoarseBatch{});
+  }
+  u = static_cast<T*>(const_cast<void*>(prog.u_out));
+  tmp = static_cast<T*>(const_cast<void*>(prog.tmp_out));
+  p0 = prog.p0_out;
+  return prog.zero_out;
+}
+
+// In the multi-CTA program, the coarse sub-cycle from u = 0 becomes one
+// kOpDense op with the single-CTA program's precomputed map.
+template<class T>
+static bool
+emit_dense(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
+           char p, T*& u, T*& tmp, const T* b)
+{
+  Context& c = E.c;
+  const CoarseProgram& prog =
+    coarse_program<T>(c, W, l, finelevel, coarselevel, p0, p, u, tmp, b, true);
+  if (prog.nops > 0 && prog.ncols > 0) {
+    CoarseOp o{};
+    o.kind = kOpDense;
+    o.n = prog.n_root;
+    o.in_n = prog.ncols;
+    o.in = prog.b_root;
+    o.out = const_cast<void*>(prog.u_out);
+    o.val = sizeof(T) == 8 ? static_cast<const void*>(prog.K64.p)
+                           : static_cast<const void*>(prog.K32.p);
+    E.rec->push_back(o);
+    u = static_cast<T*>(const_cast<void*>(prog.u_out));
+    tmp = static_cast<T*>(const_cast<void*>(prog.tmp_out));
+    p0 = prog.p0_out;
+    return prog.zero_out;
+  }
+  // no dense map (an empty sub-cycle): record its steps
+  Emit<T> R{ E.c, E.rec, E.no_dense_at, false };
+  return mgstep<T>(R, W, l, finelevel, coarselevel, p0, p, u, tmp, b, true);
+}
+
+// mgstep(l) from u = 0 for the level below the finest and everything under it,
+// as one op program run by a persistent cooperative grid (k_mid_cycle).
+template<class T>
+static bool
+run_mid(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0, char p,
+        T*& u, T*& tmp, const T* b)
+{
+  Context& c = E.c;
+  CoarseKey key{ int(sizeof(T)), l, (const void*)u, (const void*)tmp, (const void*)b,
+                 true, p0, p, c.transposed != 0 };
+  auto it = c.mid_progs.find(key);
+  if (it == c.mid_progs.end()) {
+    std::vector<CoarseOp> ops;
+    Emit<T> R{ c, &ops, -1, true };
+    T* u2 = u;
+    T* t2 = tmp;
+    char p02 = p0;
+    const bool z = mgstep<T>(R, W, l, finelevel, coarselevel, p02, p, u2, t2, b, true);
+    CoarseProgram prog;
+    prog.nops = static_cast<int>(ops.size());
+    GB_CUDA(prog.ops.alloc(std::max<size_t>(ops.size(), 1)));
+    if (!ops.empty())
+      GB_CUDA(cudaMemcpy(prog.ops.p, ops.data(), ops.size() * sizeof(CoarseOp),
+                         cudaMemcpyHostToDevice));
+    int maxn = 1;
+    for (const auto& o : ops)
+      maxn = std::max(maxn, o.kind == kOpDense ? o.n * 32 : o.n);
+    int& grid = c.mid_grid[sizeof(T) == 8 ? 0 : 1];
+    if (grid == 0) {
+      int occ = 0, nsm = 0;
+      GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mid_cycle<T>,
+                                                            kMidThreads, 0));
+      GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
+      grid = std::max(1, occ) * nsm;
+    }
+    prog.n_root = std::min(grid, blocks_for(maxn, kMidThreads)); // launch grid
+    prog.u_out = z ? nullptr : u2;
+    prog.tmp_out = t2;
+    prog.p0_out = p02;
+    prog.zero_out = z;
+    prog.u_in = u2;
+    it = c.mid_progs.emplace(key, std::move(prog)).first;
+  }
+  const CoarseProgram& prog = it->second;
+  if (prog.nops > 0) {
+    GB_CUDA(cudaMemsetAsync(c.midbar.p, 0, sizeof(unsigned), c.stream));
+    cudaEvent_t e0;
+    kt_begin(c, &e0);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(prog.n_root);
+    cfg.blockDim = dim3(kMidThreads);
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative; // all CTAs resident: the barrier ends
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GB_CUDA(cudaLaunchKernelEx(&cfg, k_mid_cycle<T>, (const CoarseOp*)prog.ops.p, prog.nops,
+                               c.midbar.p, c.miderr.p));
+    c.launches++;
+    check_launch(c);
+    kt_end(c, e0, reinterpret_cast<const void*>(k_mid_cycle<T>));
+  }
+  u = static_cast<T*>(const_cast<void*>(prog.u_in));
+  tmp = static_cast<T*>(const_cast<void*>(prog.tmp_out));
+  p0 = prog.p0_out;
+  return prog.zero_out;
+}
+
+// The single-CTA program (and dense map) of mgstep(l) for a coarse level,
+// recorded once per entry state.
+template<class T>
+static const CoarseProgram&
+coarse_program(Context& c, MgWork<T>& W, int l, int finelevel, int coarselevel, char p0,
+               char p, T* u, T* tmp, const T* b, bool u_zero)
+{
   CoarseKey key{ int(sizeof(T)), l, (const void*)u, (const void*)tmp, (const void*)b,
                  u_zero, p0, p, c.transposed != 0 };
   auto it = c.coarse_progs.find(key);
@@ -1628,24 +1783,7 @@ run_coarse(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char
     prog.zero_out = z;
     it = c.coarse_progs.emplace(key, std::move(prog)).first;
   }
-  const CoarseProgram& prog = it->second;
-  if (prog.nops > 0 && prog.ncols > 0) {
-    const T* K = sizeof(T) == 8 ? reinterpret_cast<const T*>(prog.K64.p)
-                                : reinterpret_cast<const T*>(prog.K32.p);
-    launch(c, k_coarse_apply<T>, blocks_for(int64_t(prog.n_root) * 32, 256), 256,
-           prog.n_root, prog.ncols, prog.nb, K, static_cast<const T*>(prog.b_root),
-           static_cast<const T*>(prog.u_in),
-           static_cast<T*>(const_cast<void*>(prog.u_out)));
-  } else if (prog.nops > 0) {
-    launch_smem(c, k_coarse_cycle<T>, 1, kCoarseThreads, prog.smem_bytes,
-                (const CoarseOp*)prog.ops.p, prog.nops, (const CoarseBuf*)prog.bufs.p,
-                prog.nbufs, (const CoarsePrefetch*)prog.pre.p, prog.npre,
-                prog.vec_bytes, CoarseBatch{});
-  }
-  u = static_cast<T*>(const_cast<void*>(prog.u_out));
-  tmp = static_cast<T*>(const_cast<void*>(prog.tmp_out));
-  p0 = prog.p0_out;
-  return prog.zero_out;
+  return it->second;
 }
 
 // mgstep(l) from u = 0 for a level whose sub-cycle the single-CTA program does
@@ -1734,8 +1872,12 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
        char p, T*& u, T*& tmp, const T* b, bool u_zero)
 {
   Context& c = E.c;
+  if (!E.rec && c.coarse_on && l == c.mid_level && u_zero && l != E.no_dense_at)
+    return run_mid<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b);
   if (!E.rec && c.coarse_on && l <= c.coarse_root)
     return run_coarse<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b, u_zero);
+  if (E.rec && E.mid && c.coarse_dense && c.coarse_on && l == c.coarse_root && u_zero)
+    return emit_dense<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b);
   if (!E.rec && c.coarse_on && l <= c.dense_root && u_zero && l != E.no_dense_at)
     return run_dense<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b);
   const gb_params& P = c.params;
@@ -1919,7 +2061,15 @@ fill_info(Context& c, gb_solve_info* info, double* x_for_residual, const double*
   CGInfoDev I;
   GB_CUDA(cudaMemcpyAsync(&I, &c.G.p->info, sizeof(I), cudaMemcpyDeviceToHost,
                           c.stream));
+  int mid_err = 0;
+  if (c.miderr.p)
+    GB_CUDA(cudaMemcpyAsync(&mid_err, c.miderr.p, sizeof(int), cudaMemcpyDeviceToHost,
+                            c.stream));
   GB_CUDA(cudaStreamSynchronize(c.stream));
+  if (mid_err) {
+    GB_CUDA(cudaMemsetAsync(c.miderr.p, 0, sizeof(int), c.stream));
+    throw Error{ GB_ETIMEOUT, "a grid barrier of the multi-CTA cycle gave up waiting" };
+  }
   info->iterations = I.iteration;
   info->status = I.status;
   info->firstresidual = I.firstresidual;
@@ -2493,6 +2643,8 @@ gb_ctx_create(gb_ctx** out, int device)
       ctx->use_graph = atoi(e) != 0;
     if (const char* e = getenv("GB_COARSE_DENSE"))
       ctx->coarse_dense = atoi(e) != 0;
+    if (const char* e = getenv("GB_MID"))
+      ctx->mid_on = atoi(e) != 0;
     if (const char* e = getenv("GB_JACOBI2"))
       ctx->jacobi2 = atoi(e) != 0;
     if (const char* e = getenv("GB_PDL"))

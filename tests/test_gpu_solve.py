@@ -198,3 +198,17 @@ def test_coarse_dense_map_matches_op_program(prec):
     assert abs(idn["iterations"] - io["iterations"]) <= 1
     assert idn["true_rel_residual"] <= 1e-8 and io["true_rel_residual"] <= 1e-8
     assert rel_l2(ud, uo) < (1e-6 if prec == GB_FP32 else 1e-9)
+
+
+@pytest.mark.parametrize("method,prec", [("flex", GB_FP32), ("flex", GB_FP64), ("left", GB_FP64)])
+def test_multi_cta_program_matches_per_level_kernels(method, prec):
+    """GB_MID=1 runs the levels below the finest as one cooperative grid with
+    grid barriers; it does the same per-row operations in the same order, so
+    the solves agree bit for bit."""
+    kappa, rhs = seeded_inputs(3, 1, 5)
+    P = structured_problem(3, 1, 5, kappa, rhs)
+    um, im = _solve_with_env({"GB_MID": "1"}, P, method, prec)
+    u0, i0 = _solve_with_env({"GB_MID": "0"}, P, method, prec)
+    assert im["iterations"] == i0["iterations"]
+    assert np.array_equal(um, u0)
+    assert im["kernel_launches"] < i0["kernel_launches"]
