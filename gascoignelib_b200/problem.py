@@ -600,3 +600,174 @@ def structured_q2(dim: int, coarse: int, refine: int, eps: float = 1e-2,
     return Problem(dim=dim, levels=levels, transfers=transfers, rhs=b,
                    info={"generator": "structured-q2", "coarse": coarse, "refine": refine,
                          "eps": eps, "beta": None if beta is None else list(beta)})
+
+
+# ------------------------------------------------ Q2 with a refined ball
+
+def structured_q2_ball(coarse: int, refine: int, eps: float = 1e-2,
+                       beta=(1.0, 0.5, 0.25), radius: float = 0.25,
+                       seed: int = 1002) -> Problem:
+    """CGQ2 convection-diffusion on the unit cube as structured_q2, plus one
+    more level on which every patch (2x2x2 cells) whose centre lies within
+    `radius` of the cube's centre is refined once (its 8 cells split, giving 8
+    Q2 elements of half the width). Nodes of refined patches on faces and
+    edges of unrefined neighbours hang: edge nodes on the neighbour's
+    quadratic edge trace (3 parents, weights 3/8, 6/8, -1/8, nearest first),
+    face nodes on its face (9 parents, tensor weights) - the hnq2 / hnq2face
+    maps and weights of HNStructureQ23d. The matrix is condensed
+    (C^T A C with the hanging rows and columns replaced by identity), strong
+    zero Dirichlet on the boundary; transfers to the uniform level below are the
+    nodal c2f / zweier / vierer / achter maps. The refinement rule is this
+    generator's own (whole patches by centre), not the reference's."""
+    import scipy.sparse as sp
+    dim = 3
+    base = structured_q2(dim, coarse, refine, eps=eps, beta=beta, seed=seed)
+    N = (2 * coarse) << (refine - 1)          # cells per dimension, uniform level
+    P = N // 2                                # patches per dimension
+    h = 1.0 / N
+    M2 = 2 * N                                # node grid of the refined level
+    pz, py, px = np.meshgrid(np.arange(P), np.arange(P), np.arange(P), indexing="ij")
+    cen = (np.stack([px, py, pz], -1) * 2 + 1) * h
+    refined = np.linalg.norm(cen - 0.5, axis=-1) < radius       # [P, P, P] (z, y, x)
+    # nodes: the uniform level's nodes (even) and every node of refined patches
+    ev = np.arange(0, M2 + 1, 2)
+    Z, Y, X = np.meshgrid(ev, ev, ev, indexing="ij")
+    pts = [np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)]
+    loc5 = np.stack(np.meshgrid(np.arange(5), np.arange(5), np.arange(5), indexing="ij"),
+                    -1).reshape(-1, 3)[:, ::-1]                  # (x, y, z), x fastest
+    rp = np.argwhere(refined)[:, ::-1]                            # (px, py, pz)
+    for p in rp:
+        pts.append(4 * p[None, :] + loc5)
+    allp = np.unique(np.concatenate(pts), axis=0)
+    key = (allp[:, 2] * (M2 + 1) + allp[:, 1]) * (M2 + 1) + allp[:, 0]
+    order = np.argsort(key)
+    allp, key = allp[order], key[order]
+    n = allp.shape[0]
+
+    def ids(q):  # integer points (x, y, z) -> node ids
+        k = (q[..., 2] * (M2 + 1) + q[..., 1]) * (M2 + 1) + q[..., 0]
+        i = np.searchsorted(key, k)
+        assert np.all(key[np.minimum(i, n - 1)] == k)
+        return i
+
+    # elements: unrefined patches (spacing 2) and the 8 halves of refined ones
+    loc3 = np.stack(np.meshgrid(np.arange(3), np.arange(3), np.arange(3), indexing="ij"),
+                    -1).reshape(-1, 3)[:, ::-1]
+    up = np.argwhere(~refined)[:, ::-1]
+    el_c = ids(4 * up[:, None, :] + 2 * loc3[None, :, :])          # [nu, 27]
+    sub = np.stack(np.meshgrid(np.arange(2), np.arange(2), np.arange(2), indexing="ij"),
+                   -1).reshape(-1, 3)[:, ::-1]
+    el_f = ids((4 * rp[:, None, None, :] + 2 * sub[None, :, None, :]
+                + loc3[None, None, :, :]).reshape(-1, 27, 3))       # [nr*8, 27]
+    Ec = _q2_local(dim, 2.0 * h, eps, beta)
+    Ef = _q2_local(dim, h, eps, beta)
+    rows = np.concatenate([np.repeat(el_c, 27, axis=1).ravel(),
+                           np.repeat(el_f, 27, axis=1).ravel()])
+    cols = np.concatenate([np.tile(el_c, (1, 27)).ravel(), np.tile(el_f, (1, 27)).ravel()])
+    vals = np.concatenate([np.tile(Ec.ravel(), el_c.shape[0]),
+                           np.tile(Ef.ravel(), el_f.shape[0])])
+    A = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+    # hanging nodes: odd nodes on the closure of an unrefined patch
+    odd = allp % 2 == 1
+    nodd = odd.sum(1)
+    # a node with one or two odd coordinates hangs when it lies on the closure
+    # of an unrefined patch (whose own nodes are all even)
+    kk = allp // 4
+    on4 = (allp % 4 == 0).astype(np.int64)
+    touches = np.zeros(n, dtype=bool)
+    for bits in range(8):
+        off = np.array([(bits >> d) & 1 for d in range(3)])
+        k = kk - off[None, :] * on4
+        ok = np.all((k >= 0) & (k < P), axis=1)
+        kc = np.clip(k, 0, P - 1)
+        touches |= ok & ~refined[kc[:, 2], kc[:, 1], kc[:, 0]]
+    w3 = np.array([0.375, 0.75, -0.125])
+
+    def line(c):  # the 3 coarse positions along an odd coordinate, nearest first
+        lo = 4 * (c // 4)
+        near = (c % 4) == 1
+        return np.stack([np.where(near, lo, lo + 4), lo + 2, np.where(near, lo + 4, lo)], 1)
+
+    sel_e = np.nonzero(touches & (nodd == 1))[0]
+    q = allp[sel_e]
+    d = np.argmax(odd[sel_e], axis=1)
+    ln = line(q[np.arange(sel_e.size), d])
+    par = np.repeat(q[:, None, :], 3, axis=1)
+    par[np.arange(sel_e.size)[:, None], np.arange(3)[None, :], d[:, None]] = ln
+    edges = np.concatenate([sel_e[:, None], ids(par)], 1)
+    sel_f = np.nonzero(touches & (nodd == 2))[0]
+    q = allp[sel_f]
+    oo = odd[sel_f]
+    d0 = np.argmax(oo, axis=1)
+    d1 = 2 - np.argmax(oo[:, ::-1], axis=1)
+    l0 = line(q[np.arange(sel_f.size), d0])
+    l1 = line(q[np.arange(sel_f.size), d1])
+    par = np.repeat(q[:, None, :], 9, axis=1)
+    r = np.arange(sel_f.size)[:, None]
+    par[r, np.arange(9)[None, :], d0[:, None]] = np.repeat(l0, 3, axis=1)
+    par[r, np.arange(9)[None, :], d1[:, None]] = np.tile(l1, (1, 3))
+    faces = np.concatenate([sel_f[:, None], ids(par)], 1)
+    edges = np.array(edges, dtype=np.int64).reshape(-1, 4)
+    faces = np.array(faces, dtype=np.int64).reshape(-1, 10)
+    # condensation C^T A C, hanging rows and columns -> identity
+    hang = np.concatenate([edges[:, 0], faces[:, 0]])
+    free = np.ones(n, dtype=bool)
+    free[hang] = False
+    cr = [np.nonzero(free)[0]]
+    cc = [np.nonzero(free)[0]]
+    cv = [np.ones(free.sum())]
+    for k in range(3):
+        cr.append(edges[:, 0])
+        cc.append(edges[:, 1 + k])
+        cv.append(np.full(edges.shape[0], w3[k]))
+    for a in range(3):
+        for b in range(3):
+            cr.append(faces[:, 0])
+            cc.append(faces[:, 1 + 3 * a + b])
+            cv.append(np.full(faces.shape[0], w3[a] * w3[b]))
+    Cm = sp.coo_matrix((np.concatenate(cv), (np.concatenate(cr), np.concatenate(cc))),
+                       shape=(n, n)).tocsr()
+    Ac = (Cm.T @ A @ Cm).tocsr()
+    Ac = Ac + sp.coo_matrix((np.ones(hang.size), (hang, hang)), shape=(n, n)).tocsr()
+    Ac.sum_duplicates()
+    Ac.sort_indices()
+    onb = np.any((allp == 0) | (allp == M2), axis=1)
+    rowptr = Ac.indptr.astype(np.int64)
+    col = Ac.indices.astype(np.int64)
+    val = Ac.data.astype(np.float64).copy()
+    ri = np.repeat(np.arange(n), np.diff(rowptr))
+    val[onb[ri] | onb[col]] = 0.0
+    isdiag = ri == col
+    val[isdiag & onb[ri]] = 1.0
+    fine = Level(n=n, B=1, rowptr=rowptr, col=col, diag=np.nonzero(isdiag)[0].astype(np.int64),
+                 val=val, dirichlet=np.nonzero(onb)[0].astype(np.int64),
+                 coord=allp.astype(np.float64) / M2, hn_edges=edges, hn_faces=faces,
+                 hn_disc=3)
+    # transfer from the uniform level (node (x, y, z) there is (2x, 2y, 2z) here)
+    nc1 = N + 1
+    cidx = np.arange(nc1 ** 3)
+    cpos = np.stack([cidx % nc1, (cidx // nc1) % nc1, cidx // nc1 ** 2], 1)
+    c2f = ids(2 * cpos)
+    cid = lambda q: (q[:, 2] * nc1 + q[:, 1]) * nc1 + q[:, 0]
+    maps = []
+    for m in (1, 2, 3):
+        sel = np.nonzero(nodd == m)[0]
+        q = allp[sel]
+        lo = q // 2
+        o = odd[sel].astype(np.int64)
+        par = []
+        for bits in range(8):
+            bb = np.array([(bits >> d) & 1 for d in range(3)])
+            take = np.all((bb[None, :] == 0) | (o == 1), axis=1)
+            par.append((take, cid(lo + bb[None, :] * o)))
+        tk = np.stack([t for t, _ in par], 1)
+        pp = np.stack([c for _, c in par], 1)[tk].reshape(sel.size, 2 ** m)
+        maps.append(np.concatenate([sel[:, None], pp], 1).astype(np.int64))
+    tr = Transfer(c2f=c2f.astype(np.int64), zweier=maps[0], vierer=maps[1], achter=maps[2])
+    b = np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)
+    b[onb] = 0.0
+    b[hang] = 0.0
+    return Problem(dim=dim, levels=base.levels + [fine], transfers=base.transfers + [tr],
+                   rhs=b, info={"generator": "structured-q2-ball", "coarse": coarse,
+                                "refine": refine, "eps": eps, "radius": radius,
+                                "hanging": int(hang.size), "refined_patches": int(rp.shape[0])})

@@ -28,7 +28,7 @@ def main(argv=None):
                     help="only K FP64 smoothing sweeps on the finest level (StdSolver::smooth "
                          "with the problem's smoother), after the set-up")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--problem", default="diffusion", choices=["diffusion", "stokes", "q2"],
+    ap.add_argument("--problem", default="diffusion", choices=["diffusion", "stokes", "q2", "q2ball"],
                     help="stokes: 2D Q1/Q1 Stokes with Vanka on (2*2^(refine-1))^2 cells")
     ap.add_argument("--ktime", action="store_true",
                     help="per-kernel CUDA-event times of the last solve (GB_GRAPH=0)")
@@ -43,9 +43,10 @@ def main(argv=None):
     if a.problem == "stokes":
         P = structured_stokes(2, 2, a.refine)
         keys = dict(gmressize=31, omega=1.0)
-    elif a.problem == "q2":
-        from gascoignelib_b200.problem import structured_q2
-        P = structured_q2(3, 5, a.refine - 2)
+    elif a.problem in ("q2", "q2ball"):
+        from gascoignelib_b200.problem import structured_q2, structured_q2_ball
+        P = (structured_q2(3, 5, a.refine - 2) if a.problem == "q2"
+             else structured_q2_ball(5, a.refine - 2))
         keys = dict(gmressize=31, omega=0.3, maxiter=600)
     else:
         kappa, rhs = seeded_inputs(3, 1, a.refine)

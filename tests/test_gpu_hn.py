@@ -75,3 +75,33 @@ def test_hn_3d_against_reference(ctx, disc):
     assert rel_l2(ctx.download(l, x), np.fromfile(os.path.join(out, "solution.f64"))) < 1e-8
     ctx.free(x)
     ctx.free(b)
+
+
+def test_q2_ball_generator_solve_matches_oracle(ctx):
+    """The bench's Q2 workload with the refined ball (edge and face hanging
+    nodes of Q23d on generated meshes): the reference-semantics solve against
+    the oracle, and the mixed / FP64 flexible solves to 1e-10."""
+    from gascoignelib_b200.problem import structured_q2_ball
+
+    P = structured_q2_ball(2, 3, eps=0.1)
+    O = Oracle(P, omega=0.3)
+    xo, io = O.gmres(vmax=31, tol=1e-8, globaltol=1e-300)
+    assert io["status"] == "converged"
+    ctx.load_problem(P)
+    ctx.set_params(iterpre=2, iterpost=2, iterexact=10, omega=0.3, mgomega=1.0,
+                   mgtype="V", gmressize=31, tol=1e-8, globaltol=1e-300, maxiter=100)
+    l = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(l, b, P.rhs)
+    info = ctx.gmres(x, b)
+    assert abs(info["iterations"] - io["iterations"]) <= 1
+    assert rel_l2(ctx.download(l, x), xo) < 1e-8
+    ctx.set_params(iterpre=2, iterpost=2, iterexact=10, omega=0.3, mgomega=1.0,
+                   mgtype="V", gmressize=31, tol=1e-10, globaltol=1e-300, maxiter=300)
+    for prec in (GB_FP64, GB_FP32):
+        info = ctx.fgmres(x, b, prec)
+        assert info["status_name"] == "converged"
+        assert info["true_rel_residual"] <= 1e-10
+        assert rel_l2(ctx.download(l, x), xo) < 1e-6
+    ctx.free(x)
+    ctx.free(b)
