@@ -1079,8 +1079,10 @@ enum CoarseOpKind
   kOpRestrict = 3,   // out = R in, 0 on mask
   kOpFill0 = 4,      // out = 0
   kOpProlong = 5,    // out += omega * (mask ? 0 : P in)
-  kOpDense = 6       // out = K in (n x in_n, row-major K in val): a coarse
+  kOpDense = 6,      // out = K in (n x in_n, row-major K in val): a coarse
                      // sub-cycle's precomputed map (multi-CTA program only)
+  kOpDirect = 7      // out = A^-1 in (n x n, row-major FP64 inverse in val):
+                     // the coarsest level's direct solve
 };
 
 struct CoarseOp
@@ -1250,6 +1252,15 @@ k_coarse_cycle(const CoarseOp* __restrict__ ops, int nops,
         case kOpFill0:
           out[r] = T(0);
           break;
+        case kOpDirect: {
+          // one row per thread, FP64 in column order (in is in shared memory)
+          const double* row = static_cast<const double*>(op.val) + int64_t(r) * op.n;
+          double acc = 0.0;
+          for (int j = 0; j < op.n; ++j)
+            acc = fma(__ldg(row + j), double(in[j]), acc);
+          out[r] = static_cast<T>(acc);
+          break;
+        }
         case kOpProlong: {
           T acc = coarse_row_transfer<T>(op, in, r);
           if (op.mask && __ldg(op.mask + r))
@@ -1388,15 +1399,19 @@ k_mid_cycle(const CoarseOp* __restrict__ ops, int nops, unsigned* bar, int* err)
     T* out = static_cast<T*>(op.out);
     const T* in = static_cast<const T*>(op.in);
     const T* b = static_cast<const T*>(op.b);
-    if (op.kind == kOpDense) {
-      // one warp per row, FP64 accumulation in fixed lane order
-      const T* K = static_cast<const T*>(op.val);
+    if (op.kind == kOpDense || op.kind == kOpDirect) {
+      // one warp per row, FP64 accumulation in fixed lane order (the map in
+      // the cycle's type, the direct solve's inverse in FP64)
       const int lane = threadIdx.x & 31;
+      const bool k64 = op.kind == kOpDirect;
       for (int i = gt >> 5; i < op.n; i += nthr >> 5) {
-        const T* row = K + int64_t(i) * op.in_n;
+        const int64_t r0 = int64_t(i) * op.in_n;
         double acc = 0.0;
-        for (int j = lane; j < op.in_n; j += 32)
-          acc = fma(double(__ldg(row + j)), double(__ldcg(in + j)), acc);
+        for (int j = lane; j < op.in_n; j += 32) {
+          const double kv = k64 ? __ldg(static_cast<const double*>(op.val) + r0 + j)
+                                : double(__ldg(static_cast<const T*>(op.val) + r0 + j));
+          acc = fma(kv, double(__ldcg(in + j)), acc);
+        }
         for (int o = 16; o > 0; o >>= 1)
           acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0)
@@ -1467,6 +1482,30 @@ k_coarse_apply(int n_root, int ncols, int nb, const T* __restrict__ K,
     acc += __shfl_down_sync(0xffffffffu, acc, o);
   if (lane == 0)
     u_out[warp] = static_cast<T>(acc);
+}
+
+// u = A^-1 b on the coarsest level (the exact solve that replaces the
+// iterexact sweeps on a direct level): warp per row of the row-major FP64
+// inverse, FP64 accumulation in a fixed lane order, the result rounded to the
+// cycle's type once.
+template<class T>
+__global__ void __launch_bounds__(256)
+k_coarse_direct(int n, const double* __restrict__ Ainv, const T* __restrict__ b,
+                T* __restrict__ u)
+{
+  GB_PDL_ENTRY();
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) // whole warps exit together
+    return;
+  const double* row = Ainv + int64_t(warp) * n;
+  double acc = 0.0;
+  for (int j = lane; j < n; j += 32)
+    acc = fma(__ldg(row + j), double(b[j]), acc);
+  for (int o = 16; o > 0; o >>= 1)
+    acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0)
+    u[warp] = static_cast<T>(acc);
 }
 
 // Reads n 16-byte words (an L2 eviction that leaves only clean lines behind);

@@ -398,7 +398,7 @@ struct gb_ctx
   int device = 0;
   cudaStream_t stream = nullptr;
   std::string err;
-  gb_params params{ 4, 4, 10, 1.0, 1.0, 'V', 10, 1e-2, 1e-12, 10 };
+  gb_params params{ 4, 4, 10, 1.0, 1.0, 'V', 10, 1e-2, 1e-12, 10, 0, 0 };
   int nlevels = 0;
   std::vector<gb::Level> L;
   std::vector<gb::Transfer> T;
@@ -451,6 +451,10 @@ struct gb_ctx
   std::map<std::string, std::pair<int64_t, double>> kt_acc;
   int coarse_root = -1;
   std::map<gb::CoarseKey, gb::CoarseProgram> coarse_progs;
+  // coarsest-level direct solve (gb_params.ndirect): the FP64 inverse of level
+  // 0's operator, per orientation (A, A^T)
+  gb::DeviceArray<double> dir_inv[2];
+  bool dir_ready[2] = { false, false };
   // dense maps of coarse sub-cycles that the single-CTA program does not cover
   // (block systems, Vanka, pressure filter): levels 0..dense_root
   int dense_root = -1;
@@ -923,11 +927,97 @@ ensure_vanka(Context& c, Level& L)
   L.vk_ready = true;
 }
 
+// The exact coarsest-level solve of StdSolver::smooth_exact on a direct level
+// (UmfIlu::Solve when the level has fewer than ndirect nodes, Solver/
+// stdsolver.cc:1003-1025 and :218-222): the inverse of level 0's operator (A or
+// its transpose), formed once per assembly in FP64 by Gauss-Jordan elimination
+// with partial pivoting on the host and applied as one GEMV per coarse solve.
+static bool
+direct_on(const Context& c)
+{
+  return c.params.ndirect > 0 && c.nlevels > 0 && c.L[0].n < c.params.ndirect;
+}
+
+static void
+ensure_direct(Context& c)
+{
+  const int t = c.transposed ? 1 : 0;
+  if (!direct_on(c) || c.dir_ready[t])
+    return;
+  const Level& L = c.L[0];
+  const int B = L.B, B2 = B * B;
+  const int64_t N = L.ndof();
+  GB_REQUIRE(N <= 8192, GB_EINVAL, "direct coarse solve: level 0 has more than 8192 dofs");
+  // augmented [A | I] reduced to [I | A^-1], rows swapped for the pivots
+  std::vector<double> a(size_t(N) * N, 0.0), inv(size_t(N) * N, 0.0);
+  for (int64_t i = 0; i < L.n; ++i)
+    for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k)
+      for (int r = 0; r < B; ++r)
+        for (int q = 0; q < B; ++q)
+          a[size_t(i * B + r) * N + L.h_col[k] * B + q] = L.h_val[k * B2 + r * B + q];
+  double anorm = 0.0;
+  for (double v : a)
+    anorm = std::max(anorm, std::fabs(v));
+  for (int64_t i = 0; i < N; ++i)
+    inv[size_t(i) * N + i] = 1.0;
+  for (int64_t k = 0; k < N; ++k) {
+    int64_t piv = k;
+    double best = std::fabs(a[size_t(k) * N + k]);
+    for (int64_t i = k + 1; i < N; ++i)
+      if (std::fabs(a[size_t(i) * N + k]) > best) {
+        best = std::fabs(a[size_t(i) * N + k]);
+        piv = i;
+      }
+    // a pivot at roundoff level: singular (e.g. a Stokes level whose pressure
+    // is fixed only up to a constant)
+    GB_REQUIRE(best > 1e-13 * anorm, GB_EINVAL,
+               "direct coarse solve: level 0 matrix is singular");
+    if (piv != k) {
+      std::swap_ranges(a.begin() + size_t(k) * N, a.begin() + size_t(k + 1) * N,
+                       a.begin() + size_t(piv) * N);
+      std::swap_ranges(inv.begin() + size_t(k) * N, inv.begin() + size_t(k + 1) * N,
+                       inv.begin() + size_t(piv) * N);
+    }
+    const double d = 1.0 / a[size_t(k) * N + k];
+    double* ak = a.data() + size_t(k) * N;
+    double* ik = inv.data() + size_t(k) * N;
+    for (int64_t j = 0; j < N; ++j) {
+      ak[j] *= d;
+      ik[j] *= d;
+    }
+    for (int64_t i = 0; i < N; ++i) {
+      if (i == k)
+        continue;
+      double* ai = a.data() + size_t(i) * N;
+      const double f = ai[k];
+      if (f == 0.0)
+        continue;
+      double* ii = inv.data() + size_t(i) * N;
+      for (int64_t j = k; j < N; ++j)
+        ai[j] -= f * ak[j];
+      for (int64_t j = 0; j < N; ++j)
+        ii[j] -= f * ik[j];
+    }
+  }
+  if (t) { // (A^T)^-1 = (A^-1)^T
+    for (int64_t i = 0; i < N; ++i)
+      for (int64_t j = i + 1; j < N; ++j)
+        std::swap(inv[size_t(i) * N + j], inv[size_t(j) * N + i]);
+  }
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  GB_CUDA(c.dir_inv[t].alloc(size_t(N) * N));
+  GB_CUDA(cudaMemcpy(c.dir_inv[t].p, inv.data(), inv.size() * sizeof(double),
+                     cudaMemcpyHostToDevice));
+  c.dir_ready[t] = true;
+}
+
 static void
 ensure_work(Context& c)
 {
-  if (c.work_ready)
+  if (c.work_ready) {
+    ensure_direct(c); // the other orientation after gb_set_operator
     return;
+  }
   for (int l = 0; l < c.nlevels; ++l) {
     GB_REQUIRE(c.L[l].has_matrix, GB_ESTATE, "every level needs a matrix");
     if (l + 1 < c.nlevels) {
@@ -1004,6 +1094,8 @@ ensure_work(Context& c)
   c.coarse_progs.clear();
   c.dense_maps.clear();
   c.mid_progs.clear();
+  c.dir_ready[0] = c.dir_ready[1] = false;
+  ensure_direct(c);
   c.work_ready = true;
 }
 
@@ -1354,6 +1446,24 @@ struct Emit
         launch(c, k_restrict_b<T, 4>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm,
                pf_comp(c.L[l + 1]), smean);
     }
+  }
+  // u = A^-1 b on level 0 (the direct coarse solve)
+  void direct(int l, T* u, const T* b)
+  {
+    const Level& L = c.L[l];
+    const double* inv = c.dir_inv[c.transposed ? 1 : 0].p;
+    if (rec) {
+      CoarseOp o{};
+      o.kind = kOpDirect;
+      o.n = static_cast<int>(L.ndof());
+      o.out = u;
+      o.in = b;
+      o.in_n = o.n;
+      o.val = inv;
+      return rec->push_back(o);
+    }
+    launch(c, k_coarse_direct<T>, blocks_for(int64_t(L.ndof()) * 32, 256), 256,
+           static_cast<int>(L.ndof()), inv, b, u);
   }
   void fill0(int l, T* u)
   {
@@ -1884,6 +1994,10 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
   if (l == coarselevel) {
     if (p == 'F')
       p0 = 'V';
+    if (l == 0 && direct_on(c)) { // smooth_exact on a direct level
+      E.direct(l, u, b);
+      return false;
+    }
     smooth<T>(E, l, P.iterexact, u, tmp, b, u_zero); // smooth_exact
     return u_zero;
   }
@@ -2716,6 +2830,7 @@ gb_set_params(gb_ctx* ctx, const gb_params* p)
   GB_REQUIRE(p->gmressize >= 2 && p->gmressize <= kMaxV, GB_EINVAL,
              "gmressize out of range [2, 128]");
   GB_REQUIRE(p->maxiter >= 1, GB_EINVAL, "maxiter must be >= 1");
+  GB_REQUIRE(p->ndirect >= 0, GB_EINVAL, "ndirect must be >= 0");
   ctx->params = *p;
   ctx->work_ready = false; // recorded coarse programs depend on the keys
   GB_API_END

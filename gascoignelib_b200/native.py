@@ -28,7 +28,7 @@ class GbParams(C.Structure):
     _fields_ = [("iterpre", C.c_int), ("iterpost", C.c_int), ("iterexact", C.c_int),
                 ("omega", C.c_double), ("mgomega", C.c_double), ("mgtype", C.c_char),
                 ("gmressize", C.c_int), ("tol", C.c_double), ("globaltol", C.c_double),
-                ("maxiter", C.c_int), ("smoother", C.c_int)]
+                ("maxiter", C.c_int), ("smoother", C.c_int), ("ndirect", C.c_int)]
 
 
 class GbSolveInfo(C.Structure):
@@ -182,13 +182,15 @@ class Context:
     # ------------------------------------------------------------- set-up
     def set_params(self, iterpre=2, iterpost=2, iterexact=10, omega=0.8, mgomega=1.0,
                    mgtype="V", gmressize=21, tol=1e-8, globaltol=1e-16, maxiter=100,
-                   smoother=None):
-        """smoother: "jacobi", "vanka" (or 0/1); default: the loaded problem's."""
+                   smoother=None, ndirect=0):
+        """smoother: "jacobi", "vanka" (or 0/1); default: the loaded problem's.
+        ndirect: the coarsest level is solved exactly (FP64 inverse) when it has
+        fewer nodes; 0 keeps the iterexact sweeps."""
         if smoother is None:
             smoother = getattr(self, "smoother", "jacobi")
         sm = {"jacobi": 0, "vanka": 1}.get(smoother, smoother)
         p = GbParams(iterpre, iterpost, iterexact, omega, mgomega, mgtype.encode()[:1],
-                     gmressize, tol, globaltol, maxiter, int(sm))
+                     gmressize, tol, globaltol, maxiter, int(sm), int(ndirect))
         self._chk(self._L.gb_set_params(self.h, C.byref(p)))
 
     def get_params(self):

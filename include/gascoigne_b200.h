@@ -63,6 +63,11 @@ typedef struct gb_params
   int maxiter;       /* linear_maxiter */
   int smoother;      /* 0: linear_smooth jacobi (block Jacobi); 1: linear_smooth
                         ilu with matrixtype vanka (VankaSmoother) */
+  int ndirect;       /* ndirect (Solver/stdsolver.cc:92,218-222,1003-1025): when
+                        level 0 has fewer nodes, smooth_exact there is an exact
+                        solve (the reference's UMFPACK branch) with the FP64
+                        inverse of level 0's operator; 0 keeps the iterexact
+                        sweeps (the reference built without UMFPACK) */
 } gb_params;
 
 typedef struct gb_solve_info

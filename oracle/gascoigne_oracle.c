@@ -90,6 +90,11 @@ typedef struct
   int** vperm;            /* per level: npatch row permutations, npp*B each */
   double* vtmp;           /* finest-size scratch for the Vanka solve */
   int* vcount;
+  /* coarsest-level direct solve (StdSolver::smooth_exact with UMFPACK,
+   * Solver/stdsolver.cc:1003-1025, when the level has fewer than ndirect
+   * nodes, :218-222): dense LU with partial pivoting of level 0 */
+  double* dlu;
+  int* dperm;
 } or_mg;
 
 /* ---------------------------------------------------------------- vectors */
@@ -728,6 +733,8 @@ or_mg_free(or_mg* M)
   free(M->u);
   free(M->b);
   free(M->v);
+  free(M->dlu);
+  free(M->dperm);
   if (M->vlu) {
     for (int l = 0; l < M->nlevels; ++l) {
       free(M->vlu[l]);
@@ -773,6 +780,99 @@ or_smooth(const or_mg* M, int l, int niter, double* x, const double* y,
   }
 }
 
+/* The exact coarsest-level solve that StdSolver::smooth_exact runs when the
+ * level is a direct level (fewer than ndirect nodes) and UMFPACK is compiled
+ * in (Solver/stdsolver.cc:1003-1025, NewMesh :218-222): UmfIlu::Solve gives
+ * x = A^-1 y. UMFPACK (a third-party multifrontal sparse LU, not part of the
+ * reference tree) is restated as what it computes: a dense LU with partial
+ * pivoting of the level's assembled matrix, then the two triangular solves.
+ * Returns 0, or -1 when the level is too large (more than 8192 dofs) or a
+ * pivot is at most 1e-13 times the largest entry (a singular matrix, e.g. a
+ * Stokes level whose pressure is fixed only up to a constant). ndirect <= level-0 nodes turns the
+ * direct solve off (the iterexact sweeps run). */
+int
+or_mg_set_direct(or_mg* M, int ndirect)
+{
+  free(M->dlu);
+  free(M->dperm);
+  M->dlu = NULL;
+  M->dperm = NULL;
+  const or_level* A = &M->L[0];
+  if (A->n >= ndirect)
+    return 0;
+  const int B = A->B, B2 = B * B;
+  const int64_t N = ndof(M, 0);
+  if (N > 8192)
+    return -1;
+  double* a = (double*)calloc((size_t)(N * N), sizeof(double));
+  int* pv = (int*)malloc(sizeof(int) * N);
+  for (int64_t i = 0; i < A->n; ++i)
+    for (int64_t k = A->rowptr[i]; k < A->rowptr[i + 1]; ++k)
+      for (int r = 0; r < B; ++r)
+        for (int q = 0; q < B; ++q)
+          a[(i * B + r) * N + A->col[k] * B + q] = A->val[k * B2 + r * B + q];
+  double anorm = 0.0;
+  for (int64_t i = 0; i < N * N; ++i)
+    anorm = fabs(a[i]) > anorm ? fabs(a[i]) : anorm;
+  for (int64_t i = 0; i < N; ++i)
+    pv[i] = (int)i;
+  for (int64_t k = 0; k < N; ++k) {
+    int64_t piv = k;
+    double best = fabs(a[k * N + k]);
+    for (int64_t i = k + 1; i < N; ++i)
+      if (fabs(a[i * N + k]) > best) {
+        best = fabs(a[i * N + k]);
+        piv = i;
+      }
+    if (best <= 1e-13 * anorm) {
+      free(a);
+      free(pv);
+      return -1;
+    }
+    if (piv != k) {
+      for (int64_t j = 0; j < N; ++j) {
+        const double t = a[k * N + j];
+        a[k * N + j] = a[piv * N + j];
+        a[piv * N + j] = t;
+      }
+      const int t = pv[k];
+      pv[k] = pv[piv];
+      pv[piv] = t;
+    }
+    const double d = a[k * N + k];
+    for (int64_t i = k + 1; i < N; ++i) {
+      const double f = a[i * N + k] / d;
+      a[i * N + k] = f;
+      if (f != 0.0)
+        for (int64_t j = k + 1; j < N; ++j)
+          a[i * N + j] -= f * a[k * N + j];
+    }
+  }
+  M->dlu = a;
+  M->dperm = pv;
+  return 0;
+}
+
+/* x = A^-1 y with the factors of or_mg_set_direct */
+void
+or_direct_solve(const or_mg* M, double* x, const double* y)
+{
+  const int64_t N = ndof(M, 0);
+  const double* a = M->dlu;
+  for (int64_t i = 0; i < N; ++i) {
+    double s = y[M->dperm[i]];
+    for (int64_t q = 0; q < i; ++q)
+      s -= a[i * N + q] * x[q];
+    x[i] = s;
+  }
+  for (int64_t i = N - 1; i >= 0; --i) {
+    double s = x[i];
+    for (int64_t q = i + 1; q < N; ++q)
+      s -= a[i * N + q] * x[q];
+    x[i] = s / a[i * N + i];
+  }
+}
+
 /* StdMultiLevelSolver::mgstep (Solver/stdmultilevelsolver.cc:462-531), the
  * smoothing, residual and transfer steps in the reference's order. The final
  * residual and norms only feed CGInfo and are kept for completeness. */
@@ -786,7 +886,10 @@ or_mgstep(or_mg* M, double* res, double* rw, int l, int finelevel,
   if (l == coarselevel) {
     if (p == 'F')
       *p0 = 'V';
-    or_smooth(M, l, M->iterexact, u[l], b[l], v[l]); /* smooth_exact */
+    if (M->dlu && l == 0)
+      or_direct_solve(M, u[l], b[l]); /* smooth_exact, direct level */
+    else
+      or_smooth(M, l, M->iterexact, u[l], b[l], v[l]); /* smooth_exact */
     if (l == finelevel) {
       or_matrix_residual(&M->L[l], v[l], u[l], b[l]);
       res[l] = or_norm(ndof(M, l), v[l]);

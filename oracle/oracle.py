@@ -54,6 +54,7 @@ def lib():
                                    C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                    C.c_char, C.c_int]
         L.or_mg_free.argtypes = [C.c_void_p]
+        L.or_mg_set_direct.argtypes = [C.c_void_p, C.c_int]
         L.or_transfer_build.argtypes = [C.POINTER(_Transfer), C.c_int64, _P64,
                                         C.c_int64, _P64, C.c_int64, _P64, C.c_int64,
                                         _P64]
@@ -97,7 +98,10 @@ class Oracle:
     """FP64 CPU restatement of the reference's multilevel GMRES on a Problem."""
 
     def __init__(self, prob, iterpre=2, iterpost=2, iterexact=10, omega=0.8,
-                 mgomega=1.0, mgtype="V", smoother=None):
+                 mgomega=1.0, mgtype="V", smoother=None, ndirect=0):
+        """ndirect: the coarsest level is solved exactly (dense LU) when it has
+        fewer nodes (the reference's ndirect key with UMFPACK compiled in);
+        0 keeps the iterexact sweeps."""
         L = lib()
         self.prob = prob
         self._keep = []
@@ -149,6 +153,8 @@ class Oracle:
                                  1 if smoother == "vanka" else 0)
         if not self.mg:
             raise ValueError("or_mg_create failed (Vanka needs patches on every level)")
+        if ndirect and L.or_mg_set_direct(self.mg, int(ndirect)) != 0:
+            raise ValueError("coarsest level too large (> 8192 dofs) or singular")
 
     def close(self):
         if getattr(self, "mg", None):

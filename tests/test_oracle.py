@@ -260,3 +260,28 @@ def test_structured_q2_matches_reference_assembly(dim, coarse, refine):
     u_ref[_lex_permutation(R.finest, N, dim)] = np.fromfile(os.path.join(out, "solution.f64"))
     assert abs(info["iterations"] - int(summ["iterations"][0])) <= 1
     assert rel_l2(x, u_ref) < 1e-7
+
+
+def test_oracle_direct_coarse_solve_is_exact():
+    """The coarsest-level direct solve (ndirect, the reference's UMFPACK
+    branch of smooth_exact): on a one-level problem the preconditioner is the
+    exact inverse, so the first GMRES iterate already solves the system."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    from gascoignelib_b200.problem import Problem, seeded_inputs, structured_problem
+
+    kappa, rhs = seeded_inputs(3, 1, 4)
+    P = structured_problem(3, 1, 4, kappa, rhs)
+    L = P.levels[2]
+    b = np.random.default_rng(0).uniform(-1.0, 1.0, L.n)
+    b[L.dirichlet] = 0.0
+    P1 = Problem(dim=3, levels=[L], transfers=[], rhs=b, info={})
+    A = sp.csr_matrix((L.val, L.col, L.rowptr), shape=(L.n, L.n)).tocsc()
+    x, info = Oracle(P1, ndirect=1000).gmres(vmax=21, tol=1e-8)
+    assert info["status"] == "converged"
+    assert info["firstresidual"] < 1e-12 * np.linalg.norm(b)
+    assert np.linalg.norm(x - spl.spsolve(A, b)) < 1e-13 * np.linalg.norm(x)
+    # below the threshold the iterexact sweeps run (a different preconditioner)
+    _, info2 = Oracle(P1, ndirect=L.n).gmres(vmax=21, tol=1e-8)
+    assert info2["firstresidual"] > 1e-6 * np.linalg.norm(b)
