@@ -112,6 +112,16 @@ struct SellView
   int W;
   const TV* val;
   const int* perm;     // slot -> row (rows sorted by length in windows), or null
+  const int16_t* c16;  // 16-bit offsets col - row in the SELL layout, or null
+};
+
+// Column encodings of the scalar SpMV: explicit int32 columns, the pattern
+// table, or 16-bit offsets from the row (levels whose |col - row| < 2^15).
+enum ColMode
+{
+  kColIdx = 0,
+  kColPat = 1,
+  kColOff16 = 2
 };
 
 // y = f(A x) for one row per thread, columns in the reference's stored order.
@@ -122,7 +132,7 @@ struct SellView
 // xcopy + (*yidx) * ystride.
 constexpr int kChunk = 16;
 
-template<int MODE, class TV, class TX, class TO, bool PAT>
+template<int MODE, class TV, class TX, class TO, int CM>
 __global__ void __launch_bounds__(kSpmvThreads)
 k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
        const TO* __restrict__ b, const TV* __restrict__ dinv,
@@ -139,7 +149,9 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
   const int beg = A.sptr[s];
   const int w = (A.sptr[s + 1] - beg) >> 5;
   const TV* vp = A.val + beg + lane;
+  constexpr bool PAT = CM == kColPat;
   const int* cp = PAT ? (A.ptab + int(A.pid[row]) * A.W) : (A.col + beg + lane);
+  const int16_t* hp = A.c16 + beg + lane;
   const TA alpha = static_cast<TA>(alpha_);
   constexpr bool NEG =
     (MODE == kResid || MODE == kResidDir || MODE == kJacobi || MODE == kJacobi2);
@@ -156,7 +168,9 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
     for (int q = 0; q < kChunk; ++q) {
       const int j = j0 + q;
       if (j < w) {
-        const int c = PAT ? row + ldg(cp + j) : ldg(cp + j * kSlice);
+        const int c = PAT                ? row + ldg(cp + j)
+                      : CM == kColOff16 ? row + int(ldg(hp + j * kSlice))
+                                        : ldg(cp + j * kSlice);
         av[q] = static_cast<TA>(ldg(vp + j * kSlice));
         xv[q] = MODE == kJacobi2 ? x1(c) : static_cast<TA>(ldg(x + c));
       } else {

@@ -123,6 +123,10 @@ struct Sell
   // slot -> row when the rows are ordered by length in windows (SELL-C-sigma)
   bool sorted = false;
   DeviceArray<int> rperm;
+  // without patterns: 16-bit offsets col - row beside col when they all fit
+  // (the scalar SpMV reads these; the op programs read col)
+  bool off16 = false;
+  DeviceArray<int16_t> c16;
 };
 
 template<class TV>
@@ -131,7 +135,8 @@ view(const Sell& S, const TV* val)
 {
   return SellView<TV>{ S.n, S.sptr.p, S.pat ? nullptr : S.col.p,
                        S.pat ? S.pid.p : nullptr, S.pat ? S.ptab.p : nullptr,
-                       S.W, val, S.sorted ? S.rperm.p : nullptr };
+                       S.W, val, S.sorted ? S.rperm.p : nullptr,
+                       !S.pat && S.off16 ? S.c16.p : nullptr };
 }
 
 // Rows whose column lists, relative to the row, coincide share one pattern. A
@@ -279,6 +284,35 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
   // host vectors must outlive the async copies
   GB_CUDA(cudaStreamSynchronize(st));
   build_patterns(S, n, rowptr, col, st);
+  S.off16 = false;
+  if (!S.pat && S.entries) {
+    std::vector<int16_t> h(S.entries, 0);
+    bool fits = true;
+    for (int s = 0; s < S.nslices && fits; ++s) {
+      const int w = (sptr[s + 1] - sptr[s]) / kSlice;
+      for (int l = 0; l < kSlice && fits; ++l) {
+        const int64_t t = int64_t(s) * kSlice + l;
+        if (t >= n)
+          continue; // padding lanes exit before reading
+        const int64_t r = perm[t];
+        for (int j = 0; j < w; ++j) {
+          const int64_t e = sptr[s] + int64_t(j) * kSlice + l;
+          const int64_t d = int64_t(c[e]) - r;
+          if (d < -32768 || d > 32767) {
+            fits = false;
+            break;
+          }
+          h[e] = static_cast<int16_t>(d);
+        }
+      }
+    }
+    if (fits) {
+      GB_CUDA(S.c16.alloc(h.size()));
+      GB_CUDA(cudaMemcpy(S.c16.p, h.data(), h.size() * sizeof(int16_t),
+                         cudaMemcpyHostToDevice));
+      S.off16 = true;
+    }
+  }
 }
 
 template<class T>
@@ -700,14 +734,17 @@ spmv(Context& c, const Level& L, const Sell& S, const TX* x, TO* y, const TO* b,
       throw Error{ GB_EINVAL, "block size must be 1..4" };
   }
   const SellView<TV> A = view<TV>(S, sell_vals<TV>(S));
+  const int nb = blocks_for(S.n, kSpmvThreads);
+  const uint8_t* dm = L.dirmask.p;
   if (S.pat)
-    launch(c, k_spmv<MODE, TV, TX, TO, true>, blocks_for(S.n, kSpmvThreads),
-           kSpmvThreads, A, x, y, b, dinv, (const uint8_t*)L.dirmask.p, alpha, yidx,
-           ystride, xcopy);
+    launch(c, k_spmv<MODE, TV, TX, TO, kColPat>, nb, kSpmvThreads, A, x, y, b, dinv, dm,
+           alpha, yidx, ystride, xcopy);
+  else if (A.c16)
+    launch(c, k_spmv<MODE, TV, TX, TO, kColOff16>, nb, kSpmvThreads, A, x, y, b, dinv, dm,
+           alpha, yidx, ystride, xcopy);
   else
-    launch(c, k_spmv<MODE, TV, TX, TO, false>, blocks_for(S.n, kSpmvThreads),
-           kSpmvThreads, A, x, y, b, dinv, (const uint8_t*)L.dirmask.p, alpha, yidx,
-           ystride, xcopy);
+    launch(c, k_spmv<MODE, TV, TX, TO, kColIdx>, nb, kSpmvThreads, A, x, y, b, dinv, dm,
+           alpha, yidx, ystride, xcopy);
 }
 
 template<class T>
