@@ -130,10 +130,35 @@ enum ColMode
 // Optional device-indexed output (flexible GMRES, graph-resident): when yidx is
 // set, y += (*yidx + 1) * ystride and x[row] is also copied to
 // xcopy + (*yidx) * ystride.
-constexpr int kChunk = 16;
+// Compile-time tuning of the scalar SpMV: entries per predicated chunk, and
+// the minimum resident CTAs per SM handed to the register allocator, per value
+// type and mode. FP32 values: 8 (32 registers, full occupancy). FP64 values: 4
+// for the smoother and residual modes (64 registers: more loads in flight),
+// 8 for the plain product y = A x. Measured on one B200 against chunks of 8 /
+// 16 / 32 and bounds of 2 / 3 / 4 / 8: C2 solve 1.66 -> 1.64 ms mixed and
+// 1.84 -> 1.75 ms FP64, C4 (uniform) 54.8 -> 53.8 ms mixed, 74.6 -> 65.7 ms FP64.
+#ifndef GB_SPMV_CHUNK
+#define GB_SPMV_CHUNK 32
+#endif
+#ifndef GB_SPMV_MINB_F32
+#define GB_SPMV_MINB_F32 8
+#endif
+#ifndef GB_SPMV_MINB_F64
+#define GB_SPMV_MINB_F64 4
+#endif
+#ifndef GB_SPMV_MINB_F64AX
+#define GB_SPMV_MINB_F64AX 8
+#endif
+constexpr int kChunk = GB_SPMV_CHUNK;
+template<int MODE, class TV>
+constexpr int spmv_min_blocks()
+{
+  return sizeof(TV) == 4 ? GB_SPMV_MINB_F32
+                         : (MODE == 0 ? GB_SPMV_MINB_F64AX : GB_SPMV_MINB_F64);
+}
 
 template<int MODE, class TV, class TX, class TO, int CM>
-__global__ void __launch_bounds__(kSpmvThreads)
+__global__ void __launch_bounds__(kSpmvThreads, (spmv_min_blocks<MODE, TV>()))
 k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
        const TO* __restrict__ b, const TV* __restrict__ dinv,
        const uint8_t* __restrict__ dirmask, double alpha_,
