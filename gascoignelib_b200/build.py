@@ -12,8 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", "gb_solver.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("gb_kernels.cuh", "gb_block.cuh")] + [
-    os.path.join(ROOT, "include", "gascoigne_b200.h")]
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in sorted(os.listdir(os.path.join(HERE, "csrc")))
+              if f.endswith(".cuh")] + [os.path.join(ROOT, "include", "gascoigne_b200.h")]
 OUT = os.path.join(HERE, "_lib", "libgascoigne_b200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]

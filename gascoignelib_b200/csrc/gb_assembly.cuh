@@ -1,0 +1,201 @@
+// Device-side matrix assembly of the scalar Q1 equation
+// -div(kappa grad u) + beta . grad u on quadrilateral / hexahedral cells with
+// one coefficient kappa per cell: element matrices, their summation into the
+// level's SELL-32 values, the strong Dirichlet rows and columns, and the
+// coarsening of kappa to the next coarser level. Included by gb_solver.cu after
+// gb_block.cuh.
+#pragma once
+#include "gb_kernels.cuh"
+
+namespace gb {
+
+// Element matrices of the cells, one thread per cell (CGDisc::Matrix,
+// DofHandler/cgdisc.h:599-635, with ElementIntegrator::Matrix,
+// DofHandler/elementintegrator.xx:350-395, and the matrix formula QuadGauss4 /
+// HexGauss8 of ElementIntegratorQ12d / Q13d): at the 2^DIM Gauss points
+// 1/2 -+ g of the unit cell the multilinear map's Jacobian J, the physical
+// gradients of the Q1 basis, and
+//   E[a][b] += w |J| (kappa grad phi_b . grad phi_a + (beta . grad phi_b) phi_a)
+// (row a: test function, column b: trial function). Local node a has the
+// corner bits (a & 1, a >> 1 & 1, a >> 2 & 1). cells: node of local a of cell
+// c at cells[a * ncells + c]; coords: node-major, DIM per node. E: entry (a, b)
+// of cell c at E[(a * NL + b) * ncells + c] (coalesced per entry).
+template<int DIM>
+__global__ void __launch_bounds__(128)
+k_q1_element(int ncells, const int* __restrict__ cells, const double* __restrict__ coords,
+             const double* __restrict__ kappa, double b0, double b1, double b2, double g,
+             double* __restrict__ E)
+{
+  GB_PDL_ENTRY();
+  constexpr int NL = 1 << DIM;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells)
+    return;
+  double X[NL][DIM];
+#pragma unroll
+  for (int a = 0; a < NL; ++a) {
+    const int64_t node = __ldg(cells + int64_t(a) * ncells + c);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      X[a][d] = __ldg(coords + node * DIM + d);
+  }
+  const double kap = __ldg(kappa + c);
+  const double beta[3] = { b0, b1, b2 };
+  const double gp[2] = { 0.5 - g, 0.5 + g };
+  constexpr double wq = DIM == 3 ? 0.125 : 0.25;
+  double e[NL * NL];
+#pragma unroll
+  for (int p = 0; p < NL * NL; ++p)
+    e[p] = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < NL; ++q) {
+    double xi[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      xi[d] = gp[(q >> d) & 1];
+    // reference values and gradients of the basis
+    double phi[NL], gr[NL][DIM];
+#pragma unroll
+    for (int a = 0; a < NL; ++a) {
+      phi[a] = 1.0;
+#pragma unroll
+      for (int k = 0; k < DIM; ++k)
+        gr[a][k] = 1.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const bool bit = (a >> d) & 1;
+        const double f = bit ? xi[d] : 1.0 - xi[d];
+        phi[a] *= f;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k)
+          gr[a][k] *= k == d ? (bit ? 1.0 : -1.0) : f;
+      }
+    }
+    // J[d][k] = d x_d / d xi_k, its determinant and inverse
+    double J[DIM][DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) {
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < NL; ++a)
+          s = fma(X[a][d], gr[a][k], s);
+        J[d][k] = s;
+      }
+    double det, Ji[DIM][DIM]; // Ji[k][d] = d xi_k / d x_d
+    if (DIM == 2) {
+      det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+      Ji[0][0] = J[1][1] / det;
+      Ji[0][1] = -J[0][1] / det;
+      Ji[1][0] = -J[1][0] / det;
+      Ji[1][1] = J[0][0] / det;
+    } else {
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+      const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+      const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      Ji[0][0] = c00 / det;
+      Ji[1][0] = c01 / det;
+      Ji[2][0] = c02 / det;
+      Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+      Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+      Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+      Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+      Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+      Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    }
+    const double w = wq * fabs(det);
+    // physical gradients and beta . grad phi
+    double gx[NL][DIM], bg[NL];
+#pragma unroll
+    for (int a = 0; a < NL; ++a) {
+      double s = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k)
+          t = fma(gr[a][k], Ji[k][d], t);
+        gx[a][d] = t;
+        s = fma(beta[d], t, s);
+      }
+      bg[a] = s;
+    }
+#pragma unroll
+    for (int a = 0; a < NL; ++a)
+#pragma unroll
+      for (int b = 0; b < NL; ++b) {
+        double dg = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          dg = fma(gx[b][d], gx[a][d], dg);
+        e[a * NL + b] = fma(w, fma(kap, dg, bg[b] * phi[a]), e[a * NL + b]);
+      }
+  }
+#pragma unroll
+  for (int p = 0; p < NL * NL; ++p)
+    E[int64_t(p) * ncells + c] = e[p];
+}
+
+// The level's SELL values from the element matrices, one thread per slot
+// (LocalToGlobal + MatrixInterface::entry, DofHandler/cgdisc.h:353-366): entry
+// e sums E[clist[k]] for k in [cptr[e], cptr[e+1]), the contributions in
+// ascending cell order (the reference's cell loop). Then the strong Dirichlet
+// condition (SparseBlockMatrix::dirichlet, LinAlg/sparseblockmatrix.xx:207-218):
+// a Dirichlet row keeps only its diagonal, set to 1, and a Dirichlet column is
+// zero elsewhere. Writes the FP64 and FP32 values and the diagonal (dd) for the
+// block-diagonal inverse.
+__global__ void __launch_bounds__(kSpmvThreads)
+k_asm_gather(int n, const int* __restrict__ sptr, const int* __restrict__ perm,
+             const int* __restrict__ col, const int* __restrict__ cptr,
+             const int* __restrict__ clist, const double* __restrict__ E,
+             const uint8_t* __restrict__ dirmask, const int* __restrict__ diagpos,
+             double* __restrict__ v64, float* __restrict__ v32, double* __restrict__ dd)
+{
+  GB_PDL_ENTRY();
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= n)
+    return;
+  const int row = perm ? __ldg(perm + slot) : slot;
+  const int s = slot >> 5, lane = slot & 31;
+  const int beg = __ldg(sptr + s);
+  const int w = (__ldg(sptr + s + 1) - beg) >> 5;
+  const bool drow = __ldg(dirmask + row) != 0;
+  const int dpos = __ldg(diagpos + row);
+  for (int j = 0; j < w; ++j) {
+    const int e = beg + j * kSlice + lane;
+    double v = 0.0;
+    if (drow) {
+      v = e == dpos ? 1.0 : 0.0;
+    } else if (!__ldg(dirmask + __ldg(col + e))) {
+      const int k1 = __ldg(cptr + e + 1);
+      for (int k = __ldg(cptr + e); k < k1; ++k)
+        v += __ldg(E + __ldg(clist + k));
+    }
+    v64[e] = v;
+    v32[e] = static_cast<float>(v);
+    if (e == dpos)
+      dd[row] = v;
+  }
+}
+
+// kappa of each coarse cell: the sum of its children's values in ascending
+// order divided by their number (the harness's coefficient pyramid; a
+// per-cell coefficient of the coarser mesh, Application::SetCellData).
+__global__ void
+k_kappa_coarsen(int nc, const int* __restrict__ cptr, const int* __restrict__ child,
+                const double* __restrict__ kf, double* __restrict__ kc)
+{
+  GB_PDL_ENTRY();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc)
+    return;
+  const int k0 = __ldg(cptr + c), k1 = __ldg(cptr + c + 1);
+  double s = 0.0;
+  for (int k = k0; k < k1; ++k)
+    s += __ldg(kf + __ldg(child + k));
+  kc[c] = s / double(k1 - k0);
+}
+
+} // namespace gb

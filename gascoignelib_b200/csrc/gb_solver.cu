@@ -26,6 +26,7 @@
 #include "../../include/gascoigne_b200.h"
 #include "gb_kernels.cuh"
 #include "gb_block.cuh"
+#include "gb_assembly.cuh"
 
 namespace gb {
 
@@ -128,6 +129,19 @@ struct Sell
   bool off16 = false;
   DeviceArray<int16_t> c16;
 };
+
+// Host-to-device copy ordered on `st` (the context's stream) and complete on
+// return. A plain cudaMemcpy from pageable host memory can return before its
+// DMA has reached the device, and kernels on a non-blocking stream do not wait
+// for the legacy stream it runs on.
+static cudaError_t
+h2d(cudaStream_t st, void* dst, const void* src, size_t bytes)
+{
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(st);
+  return e;
+}
 
 template<class TV>
 static SellView<TV>
@@ -308,8 +322,7 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
     }
     if (fits) {
       GB_CUDA(S.c16.alloc(h.size()));
-      GB_CUDA(cudaMemcpy(S.c16.p, h.data(), h.size() * sizeof(int16_t),
-                         cudaMemcpyHostToDevice));
+      GB_CUDA(h2d(st, S.c16.p, h.data(), h.size() * sizeof(int16_t)));
       S.off16 = true;
     }
   }
@@ -374,6 +387,18 @@ struct Level
   std::vector<int> h_hnnodes;  // all hanging nodes
   DeviceArray<int> hn_all;
   DeviceArray<uint8_t> pmask;  // Dirichlet | hanging dofs (prolongation mask)
+  // Q1 mesh for the device assembly (gb_level_set_mesh): cells [a][c], node
+  // coordinates, per SELL entry the element-matrix entries summed into it
+  // (ascending cells), the diagonal's SELL position per row, this level's
+  // cell coefficients, and the parent cell (level - 1) of every cell
+  int mesh_dim = 0;
+  int64_t mesh_ncells = 0, mesh_n = -1;
+  DeviceArray<int> m_cells, m_cptr, m_clist, m_diagpos, m_child_ptr, m_child;
+  DeviceArray<double> m_coords, m_kappa, m_dd;
+  std::vector<int64_t> h_parent;
+  int64_t child_n = -1; // coarse cells the child lists were built for
+  // values assembled on the device since the host copy was made
+  bool h_val_stale = false;
   bool has_hn() const { return !hn.empty(); }
   int64_t ndof() const { return n * B; }
 };
@@ -506,6 +531,7 @@ struct gb_ctx
   gb::DeviceArray<int> miderr;
   int mid_grid[2] = { 0, 0 }; // per precision (FP64, FP32)
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
+  gb::DeviceArray<double> asm_E; // element matrices of the level being assembled
   gb::DeviceArray<float> rhs32, zfix32;
   ~gb_ctx()
   {
@@ -777,11 +803,39 @@ opA(const Context& c, const Level& L)
 // uploaded matrix are both identity, so A^T is the reference's dual matrix
 // (transpose, then DirichletMatrixOnlyRow) wherever it meets a vector that is
 // zero on the Dirichlet dofs, which every vector of the dual solve is.
+// The host copy of a level's values after a device assembly (gb_assemble),
+// for the set-up steps that read it (transpose, Vanka factors, direct coarse
+// inverse): the FP64 SELL values read back and put in stencil order.
+static void
+host_values(Context& c, Level& L)
+{
+  if (!L.h_val_stale)
+    return;
+  const Sell& A = L.A;
+  std::vector<double> v(A.entries);
+  std::vector<int> sptr(A.nslices + 1), perm;
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  GB_CUDA(cudaMemcpy(v.data(), A.v64.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  GB_CUDA(cudaMemcpy(sptr.data(), A.sptr.p, sptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  if (A.sorted) {
+    perm.resize(L.n);
+    GB_CUDA(cudaMemcpy(perm.data(), A.rperm.p, L.n * sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  for (int64_t t = 0; t < L.n; ++t) {
+    const int64_t r = A.sorted ? perm[t] : t;
+    const int64_t s0 = sptr[t / kSlice] + t % kSlice;
+    for (int64_t k = L.h_rowptr[r]; k < L.h_rowptr[r + 1]; ++k)
+      L.h_val[k] = v[s0 + (k - L.h_rowptr[r]) * kSlice];
+  }
+  L.h_val_stale = false;
+}
+
 static void
 ensure_AT(Context& c, Level& L)
 {
   if (L.has_AT)
     return;
+  host_values(c, L);
   const int B = L.B, B2 = B * B;
   const int64_t n = L.n, nnz = L.h_rowptr[n];
   std::vector<int64_t> tp(n + 1, 0), tc(nnz);
@@ -858,6 +912,7 @@ ensure_vanka(Context& c, Level& L)
 {
   if (L.vk_ready)
     return;
+  host_values(c, L);
   GB_REQUIRE(L.npatch > 0, GB_ESTATE, "Vanka needs the patches of every level "
                                       "(gb_level_set_patches)");
   const int B = L.B, npp = L.npp, M = npp * B, B2 = B * B;
@@ -950,16 +1005,11 @@ ensure_vanka(Context& c, Level& L)
   GB_CUDA(L.vk_ent.alloc(ent.size()));
   GB_CUDA(L.vk_out64.alloc(size_t(np) * M));
   GB_CUDA(L.vk_out32.alloc(size_t(np) * M));
-  GB_CUDA(cudaMemcpy(L.vk_inv64.p, inv.data(), inv.size() * sizeof(double),
-                     cudaMemcpyHostToDevice));
-  GB_CUDA(cudaMemcpy(L.vk_inv32.p, inv32.data(), inv32.size() * sizeof(float),
-                     cudaMemcpyHostToDevice));
-  GB_CUDA(cudaMemcpy(L.vk_pn.p, pn.data(), pn.size() * sizeof(int),
-                     cudaMemcpyHostToDevice));
-  GB_CUDA(cudaMemcpy(L.vk_nptr.p, nptr.data(), nptr.size() * sizeof(int),
-                     cudaMemcpyHostToDevice));
-  GB_CUDA(cudaMemcpy(L.vk_ent.p, ent.data(), ent.size() * sizeof(int),
-                     cudaMemcpyHostToDevice));
+  GB_CUDA(h2d(c.stream, L.vk_inv64.p, inv.data(), inv.size() * sizeof(double)));
+  GB_CUDA(h2d(c.stream, L.vk_inv32.p, inv32.data(), inv32.size() * sizeof(float)));
+  GB_CUDA(h2d(c.stream, L.vk_pn.p, pn.data(), pn.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.vk_nptr.p, nptr.data(), nptr.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.vk_ent.p, ent.data(), ent.size() * sizeof(int)));
   L.vk_M = M;
   L.vk_ready = true;
 }
@@ -981,7 +1031,8 @@ ensure_direct(Context& c)
   const int t = c.transposed ? 1 : 0;
   if (!direct_on(c) || c.dir_ready[t])
     return;
-  const Level& L = c.L[0];
+  Level& L = c.L[0];
+  host_values(c, L);
   const int B = L.B, B2 = B * B;
   const int64_t N = L.ndof();
   GB_REQUIRE(N <= 8192, GB_EINVAL, "direct coarse solve: level 0 has more than 8192 dofs");
@@ -1043,8 +1094,7 @@ ensure_direct(Context& c)
   }
   GB_CUDA(cudaStreamSynchronize(c.stream));
   GB_CUDA(c.dir_inv[t].alloc(size_t(N) * N));
-  GB_CUDA(cudaMemcpy(c.dir_inv[t].p, inv.data(), inv.size() * sizeof(double),
-                     cudaMemcpyHostToDevice));
+  GB_CUDA(h2d(c.stream, c.dir_inv[t].p, inv.data(), inv.size() * sizeof(double)));
   c.dir_ready[t] = true;
 }
 
@@ -1100,7 +1150,7 @@ ensure_work(Context& c)
       for (int cc = 0; cc < L.B; ++cc)
         m[int64_t(h) * L.B + cc] = 1;
     GB_CUDA(L.pmask.alloc(m.size()));
-    GB_CUDA(cudaMemcpy(L.pmask.p, m.data(), m.size(), cudaMemcpyHostToDevice));
+    GB_CUDA(h2d(c.stream, L.pmask.p, m.data(), m.size()));
   }
   // the single-CTA coarse-level program covers scalar Jacobi cycles without
   // hanging-node steps
@@ -1743,8 +1793,7 @@ run_mid(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p
     prog.nops = static_cast<int>(ops.size());
     GB_CUDA(prog.ops.alloc(std::max<size_t>(ops.size(), 1)));
     if (!ops.empty())
-      GB_CUDA(cudaMemcpy(prog.ops.p, ops.data(), ops.size() * sizeof(CoarseOp),
-                         cudaMemcpyHostToDevice));
+      GB_CUDA(h2d(c.stream, prog.ops.p, ops.data(), ops.size() * sizeof(CoarseOp)));
     int maxn = 1;
     for (const auto& o : ops)
       maxn = std::max(maxn, o.kind == kOpDense ? o.n * 32 : o.n);
@@ -1882,14 +1931,11 @@ coarse_program(Context& c, MgWork<T>& W, int l, int finelevel, int coarselevel, 
     GB_CUDA(prog.bufs.alloc(std::max<size_t>(bufs.size(), 1)));
     GB_CUDA(prog.pre.alloc(std::max<size_t>(pre.size(), 1)));
     if (!ops.empty())
-      GB_CUDA(cudaMemcpy(prog.ops.p, ops.data(), ops.size() * sizeof(CoarseOp),
-                         cudaMemcpyHostToDevice));
+      GB_CUDA(h2d(c.stream, prog.ops.p, ops.data(), ops.size() * sizeof(CoarseOp)));
     if (!bufs.empty())
-      GB_CUDA(cudaMemcpy(prog.bufs.p, bufs.data(), bufs.size() * sizeof(CoarseBuf),
-                         cudaMemcpyHostToDevice));
+      GB_CUDA(h2d(c.stream, prog.bufs.p, bufs.data(), bufs.size() * sizeof(CoarseBuf)));
     if (!pre.empty())
-      GB_CUDA(cudaMemcpy(prog.pre.p, pre.data(), pre.size() * sizeof(CoarsePrefetch),
-                         cudaMemcpyHostToDevice));
+      GB_CUDA(h2d(c.stream, prog.pre.p, pre.data(), pre.size() * sizeof(CoarsePrefetch)));
     if (prog.smem_bytes > 48 * 1024)
       GB_CUDA(cudaFuncSetAttribute(k_coarse_cycle<T>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2775,6 +2821,96 @@ with_transposed(gb_ctx* ctx, F f)
   }                                                                            \
   return GB_OK;
 
+namespace gb {
+
+// Element matrices and their sum into level l's values (FP64 and FP32), the
+// Dirichlet rows and columns, and the block-diagonal inverse; the kappa of the
+// level's cells is in L.m_kappa.
+static void
+assemble_level(Context& c, int l, const double* beta)
+{
+  Level& L = c.L[l];
+  const int dim = L.mesh_dim, nl = 1 << dim;
+  const int nc = static_cast<int>(L.mesh_ncells);
+  GB_CUDA(c.asm_E.n >= size_t(nc) * nl * nl ? cudaSuccess
+                                             : c.asm_E.alloc(size_t(nc) * nl * nl));
+  const double b0 = beta ? beta[0] : 0.0, b1 = beta ? beta[1] : 0.0;
+  const double b2 = beta && dim == 3 ? beta[2] : 0.0;
+  const double g = 0.5 / std::sqrt(3.0);
+  if (dim == 2)
+    launch(c, k_q1_element<2>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,
+           (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p);
+  else
+    launch(c, k_q1_element<3>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,
+           (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p);
+  const Sell& A = L.A;
+  launch(c, k_asm_gather, blocks_for(L.n, kSpmvThreads), kSpmvThreads, (int)L.n,
+         (const int*)A.sptr.p, (const int*)(A.sorted ? A.rperm.p : nullptr),
+         (const int*)A.col.p, (const int*)L.m_cptr.p, (const int*)L.m_clist.p,
+         (const double*)c.asm_E.p, (const uint8_t*)L.dirmask.p, (const int*)L.m_diagpos.p,
+         A.v64.p, A.v32.p, L.m_dd.p);
+  launch(c, k_blockdiag_inverse<1>, blocks_for(L.n, 128), 128, (int)L.n,
+         (const double*)L.m_dd.p, L.dinv64.p, L.dinv32.p);
+  L.h_val_stale = true;
+  L.has_AT = false;
+  L.vk_ready = false;
+  c.work_ready = false;
+  c.version++;
+  if (c.transposed)
+    ensure_AT(c, L); // the operator in use stays current
+}
+
+// kappa of level l's cells from level l + 1's (mean of the children)
+static void
+coarsen_kappa(Context& c, int l)
+{
+  Level& C = c.L[l];
+  Level& F = c.L[l + 1];
+  if (C.child_n != C.mesh_ncells) {
+    std::vector<int> ptr(C.mesh_ncells + 1, 0), ch(F.mesh_ncells);
+    for (int64_t f = 0; f < F.mesh_ncells; ++f) {
+      GB_REQUIRE(F.h_parent[f] < C.mesh_ncells, GB_EINVAL, "parent cell out of range");
+      ptr[F.h_parent[f] + 1]++;
+    }
+    for (int64_t k = 0; k < C.mesh_ncells; ++k) {
+      GB_REQUIRE(ptr[k + 1] > 0, GB_EINVAL, "a coarse cell without children");
+      ptr[k + 1] += ptr[k];
+    }
+    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+    for (int64_t f = 0; f < F.mesh_ncells; ++f) // ascending children
+      ch[fill[F.h_parent[f]]++] = static_cast<int>(f);
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+    GB_CUDA(C.m_child_ptr.alloc(ptr.size()));
+    GB_CUDA(C.m_child.alloc(ch.size()));
+    GB_CUDA(h2d(c.stream, C.m_child_ptr.p, ptr.data(), ptr.size() * sizeof(int)));
+    GB_CUDA(h2d(c.stream, C.m_child.p, ch.data(), ch.size() * sizeof(int)));
+    C.child_n = C.mesh_ncells;
+  }
+  launch(c, k_kappa_coarsen, blocks_for(C.mesh_ncells, 256), 256, (int)C.mesh_ncells,
+         (const int*)C.m_child_ptr.p, (const int*)C.m_child.p, (const double*)F.m_kappa.p,
+         C.m_kappa.p);
+}
+
+static void
+check_mesh(const Level& L)
+{
+  GB_REQUIRE(L.mesh_ncells > 0 && L.mesh_n == L.n, GB_ESTATE,
+             "no mesh for this level's matrix (gb_level_set_mesh)");
+}
+
+static void
+load_kappa(Context& c, Level& L, const double* kappa, int where)
+{
+  GB_REQUIRE(kappa, GB_EINVAL, "null kappa");
+  GB_REQUIRE(where == 0 || where == 1, GB_EINVAL, "kappa location must be 0 (host) or 1 (device)");
+  GB_CUDA(cudaMemcpyAsync(L.m_kappa.p, kappa, L.mesh_ncells * sizeof(double),
+                          where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+  if (!where)
+    GB_CUDA(cudaStreamSynchronize(c.stream)); // the host array ends with the call
+}
+
+} // namespace gb
+
 extern "C" {
 
 int
@@ -2929,6 +3065,9 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   build_sell(L.A, n, rowptr, col, val, ctx->stream, B);
   L.has_AT = false;
   L.vk_ready = false;
+  L.h_val_stale = false;
+  L.mesh_ncells = 0; // the mesh maps point into the old pattern
+  L.mesh_n = -1;
   if (ctx->transposed)
     ensure_AT(*ctx, L);
   // block-diagonal inverse on the device (get_inverse_diagonal / K1)
@@ -2993,11 +3132,10 @@ gb_level_set_dirichlet(gb_ctx* ctx, int lvl, int64_t nnodes, const int64_t* node
   }
   GB_CUDA(cudaStreamSynchronize(ctx->stream));
   GB_CUDA(L.dirmask.alloc(mask.size()));
-  GB_CUDA(cudaMemcpy(L.dirmask.p, mask.data(), mask.size(), cudaMemcpyHostToDevice));
+  GB_CUDA(h2d(ctx->stream, L.dirmask.p, mask.data(), mask.size()));
   GB_CUDA(L.dirlist.alloc(std::max<size_t>(dofs.size(), 1)));
   if (!dofs.empty())
-    GB_CUDA(cudaMemcpy(L.dirlist.p, dofs.data(), dofs.size() * sizeof(int),
-                       cudaMemcpyHostToDevice));
+    GB_CUDA(h2d(ctx->stream, L.dirlist.p, dofs.data(), dofs.size() * sizeof(int)));
   L.ndir = static_cast<int>(dofs.size());
   ctx->work_ready = false; // the prolongation mask of hanging levels includes it
   GB_API_END
@@ -3079,16 +3217,12 @@ gb_level_set_transfer(gb_ctx* ctx, int lvl, int64_t ncoarse, const int64_t* c2f,
   GB_CUDA(T.rptr.alloc(rptr.size()));
   GB_CUDA(T.pent.alloc(std::max<size_t>(pent.size(), 1)));
   GB_CUDA(T.rent.alloc(std::max<size_t>(rent.size(), 1)));
-  GB_CUDA(cudaMemcpy(T.pptr.p, pptr.data(), pptr.size() * sizeof(int),
-                     cudaMemcpyHostToDevice));
-  GB_CUDA(cudaMemcpy(T.rptr.p, rptr.data(), rptr.size() * sizeof(int),
-                     cudaMemcpyHostToDevice));
+  GB_CUDA(h2d(ctx->stream, T.pptr.p, pptr.data(), pptr.size() * sizeof(int)));
+  GB_CUDA(h2d(ctx->stream, T.rptr.p, rptr.data(), rptr.size() * sizeof(int)));
   if (!pent.empty())
-    GB_CUDA(cudaMemcpy(T.pent.p, pent.data(), pent.size() * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice));
+    GB_CUDA(h2d(ctx->stream, T.pent.p, pent.data(), pent.size() * sizeof(uint32_t)));
   if (!rent.empty())
-    GB_CUDA(cudaMemcpy(T.rent.p, rent.data(), rent.size() * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice));
+    GB_CUDA(h2d(ctx->stream, T.rent.p, rent.data(), rent.size() * sizeof(uint32_t)));
   T.set = true;
   ctx->work_ready = false;
   GB_API_END
@@ -3368,7 +3502,7 @@ gb_level_set_pfilter(gb_ctx* ctx, int lvl, int comp_mask, const double* weights,
   if (comp_mask) {
     GB_CUDA(cudaStreamSynchronize(ctx->stream));
     GB_CUDA(L.pf_w.alloc(L.n));
-    GB_CUDA(cudaMemcpy(L.pf_w.p, weights, L.n * sizeof(double), cudaMemcpyHostToDevice));
+    GB_CUDA(h2d(ctx->stream, L.pf_w.p, weights, L.n * sizeof(double)));
   }
   if (comp_mask)
     ensure_pf_scratch(*ctx, L.n);
@@ -3500,24 +3634,18 @@ gb_level_set_hn(gb_ctx* ctx, int lvl, int disc, int64_t nedge, const int64_t* ed
     GB_CUDA(ph.ptr.alloc(ptr.size()));
     GB_CUDA(ph.hnode.alloc(hnode.size()));
     GB_CUDA(ph.wt.alloc(wt.size()));
-    GB_CUDA(cudaMemcpy(ph.node.p, node.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
-    GB_CUDA(cudaMemcpy(ph.par.p, par.data(), par.size() * sizeof(int),
-                       cudaMemcpyHostToDevice));
-    GB_CUDA(cudaMemcpy(ph.w.p, sp->w.data(), ns * sizeof(double), cudaMemcpyHostToDevice));
-    GB_CUDA(cudaMemcpy(ph.pnode.p, pnode.data(), pnode.size() * sizeof(int),
-                       cudaMemcpyHostToDevice));
-    GB_CUDA(cudaMemcpy(ph.ptr.p, ptr.data(), ptr.size() * sizeof(int),
-                       cudaMemcpyHostToDevice));
-    GB_CUDA(cudaMemcpy(ph.hnode.p, hnode.data(), hnode.size() * sizeof(int),
-                       cudaMemcpyHostToDevice));
-    GB_CUDA(cudaMemcpy(ph.wt.p, wt.data(), wt.size() * sizeof(double),
-                       cudaMemcpyHostToDevice));
+    GB_CUDA(h2d(ctx->stream, ph.node.p, node.data(), nh * sizeof(int)));
+    GB_CUDA(h2d(ctx->stream, ph.par.p, par.data(), par.size() * sizeof(int)));
+    GB_CUDA(h2d(ctx->stream, ph.w.p, sp->w.data(), ns * sizeof(double)));
+    GB_CUDA(h2d(ctx->stream, ph.pnode.p, pnode.data(), pnode.size() * sizeof(int)));
+    GB_CUDA(h2d(ctx->stream, ph.ptr.p, ptr.data(), ptr.size() * sizeof(int)));
+    GB_CUDA(h2d(ctx->stream, ph.hnode.p, hnode.data(), hnode.size() * sizeof(int)));
+    GB_CUDA(h2d(ctx->stream, ph.wt.p, wt.data(), wt.size() * sizeof(double)));
     L.hn.push_back(std::move(ph));
   }
   if (!L.h_hnnodes.empty()) {
     GB_CUDA(L.hn_all.alloc(L.h_hnnodes.size()));
-    GB_CUDA(cudaMemcpy(L.hn_all.p, L.h_hnnodes.data(), L.h_hnnodes.size() * sizeof(int),
-                       cudaMemcpyHostToDevice));
+    GB_CUDA(h2d(ctx->stream, L.hn_all.p, L.h_hnnodes.data(), L.h_hnnodes.size() * sizeof(int)));
   }
   ctx->work_ready = false;
   GB_API_END
@@ -3877,6 +4005,156 @@ gb_level_set_functional(gb_ctx* ctx, int lvl, const double* mloc, const double* 
   GB_CUDA(cudaStreamSynchronize(ctx->stream));
   build_sell(L.M, n, L.h_rowptr.data(), L.h_col.data(), mv.data(), ctx->stream);
   L.func_n = n;
+  GB_API_END
+}
+
+int
+gb_level_set_mesh(gb_ctx* ctx, int lvl, int dim, int64_t ncells, const int64_t* cell_nodes,
+                  const double* coords, const int64_t* parent)
+{
+  GB_API_BEGIN
+  ctx->version++;
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(dim == 2 || dim == 3, GB_EINVAL, "dim must be 2 or 3");
+  GB_REQUIRE(L.B == 1, GB_EINVAL, "device assembly needs block size 1");
+  GB_REQUIRE(!L.has_hn(), GB_EINVAL, "device assembly of a level with hanging nodes");
+  const int nl = 1 << dim;
+  GB_REQUIRE(ncells >= 1 && ncells * nl * nl < (int64_t(1) << 31), GB_EINVAL,
+             "ncells out of range");
+  GB_REQUIRE(cell_nodes && coords, GB_EINVAL, "null array");
+  GB_REQUIRE(lvl == 0 || parent, GB_EINVAL, "parent cells are needed above level 0");
+  const Sell& A = L.A;
+  const int64_t n = L.n;
+  // SELL position of row r's stencil entry k: sptr[t / 32] + (k - rowptr[r]) * 32 + t % 32
+  std::vector<int> sptr(A.nslices + 1), perm(n), slot(n);
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_CUDA(cudaMemcpy(sptr.data(), A.sptr.p, sptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  if (A.sorted)
+    GB_CUDA(cudaMemcpy(perm.data(), A.rperm.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+  else
+    for (int64_t t = 0; t < n; ++t)
+      perm[t] = static_cast<int>(t);
+  for (int64_t t = 0; t < n; ++t)
+    slot[perm[t]] = static_cast<int>(t);
+  auto sell_pos = [&](int64_t r, int64_t k) {
+    const int64_t t = slot[r];
+    return sptr[t / kSlice] + (k - L.h_rowptr[r]) * kSlice + t % kSlice;
+  };
+  std::vector<std::pair<int64_t, int64_t>> sc(L.h_col.size());
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k)
+      sc[k] = { L.h_col[k], k };
+    std::sort(sc.begin() + L.h_rowptr[i], sc.begin() + L.h_rowptr[i + 1]);
+  }
+  // positions of every (cell, a, b), then the contributions per position in
+  // ascending cell order (counting sort)
+  const int64_t np = ncells * nl * nl;
+  std::vector<int> pos(np), cn(size_t(ncells) * nl);
+  std::vector<int> cptr(A.entries + 1, 0);
+  for (int64_t c = 0; c < ncells; ++c)
+    for (int a = 0; a < nl; ++a) {
+      const int64_t r = cell_nodes[c * nl + a];
+      GB_REQUIRE(r >= 0 && r < n, GB_EINVAL, "cell node out of range");
+      cn[size_t(a) * ncells + c] = static_cast<int>(r);
+      auto b0 = sc.begin() + L.h_rowptr[r], b1 = sc.begin() + L.h_rowptr[r + 1];
+      for (int b = 0; b < nl; ++b) {
+        const int64_t q = cell_nodes[c * nl + b];
+        GB_REQUIRE(q >= 0 && q < n, GB_EINVAL, "cell node out of range");
+        auto it = std::lower_bound(b0, b1, std::make_pair(q, int64_t(-1)));
+        GB_REQUIRE(it != b1 && it->first == q, GB_EINVAL,
+                   "a cell couples two nodes that the matrix pattern does not");
+        const int e = static_cast<int>(sell_pos(r, it->second));
+        pos[(c * nl + a) * nl + b] = e;
+        cptr[e + 1]++;
+      }
+    }
+  for (size_t e = 0; e < A.entries; ++e)
+    cptr[e + 1] += cptr[e];
+  std::vector<int> fill(cptr.begin(), cptr.end() - 1), clist(np);
+  for (int64_t c = 0; c < ncells; ++c)
+    for (int p = 0; p < nl * nl; ++p)
+      clist[fill[pos[c * nl * nl + p]]++] = static_cast<int>(int64_t(p) * ncells + c);
+  std::vector<int> dpos(n);
+  for (int64_t r = 0; r < n; ++r)
+    dpos[r] = static_cast<int>(sell_pos(r, L.h_diag[r]));
+  std::vector<int64_t> par;
+  if (lvl > 0) {
+    par.assign(parent, parent + ncells);
+    for (int64_t c = 0; c < ncells; ++c)
+      GB_REQUIRE(par[c] >= 0, GB_EINVAL, "negative parent cell");
+  }
+  GB_CUDA(L.m_cells.alloc(cn.size()));
+  GB_CUDA(L.m_coords.alloc(size_t(n) * dim));
+  GB_CUDA(L.m_cptr.alloc(cptr.size()));
+  GB_CUDA(L.m_clist.alloc(clist.size()));
+  GB_CUDA(L.m_diagpos.alloc(n));
+  GB_CUDA(L.m_kappa.alloc(ncells));
+  GB_CUDA(L.m_dd.alloc(n));
+  GB_CUDA(h2d(ctx->stream, L.m_cells.p, cn.data(), cn.size() * sizeof(int)));
+  GB_CUDA(h2d(ctx->stream, L.m_coords.p, coords, size_t(n) * dim * sizeof(double)));
+  GB_CUDA(h2d(ctx->stream, L.m_cptr.p, cptr.data(), cptr.size() * sizeof(int)));
+  GB_CUDA(h2d(ctx->stream, L.m_clist.p, clist.data(), clist.size() * sizeof(int)));
+  GB_CUDA(h2d(ctx->stream, L.m_diagpos.p, dpos.data(), n * sizeof(int)));
+  L.h_parent.swap(par);
+  L.mesh_dim = dim;
+  L.mesh_ncells = ncells;
+  L.mesh_n = n;
+  if (lvl > 0)
+    ctx->L[lvl - 1].child_n = -1; // its child lists follow this level's parents
+  GB_API_END
+}
+
+int
+gb_assemble(gb_ctx* ctx, int lvl, const double* kappa, int where, const double* beta)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  check_mesh(L);
+  load_kappa(*ctx, L, kappa, where);
+  assemble_level(*ctx, lvl, beta);
+  GB_API_END
+}
+
+int
+gb_assemble_levels(gb_ctx* ctx, const double* kappa, int where, const double* beta)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(ctx->nlevels >= 1, GB_ESTATE, "no levels");
+  for (int l = 0; l < ctx->nlevels; ++l) {
+    GB_REQUIRE(ctx->L[l].has_matrix, GB_ESTATE, "every level needs a matrix");
+    check_mesh(ctx->L[l]);
+  }
+  const int fl = ctx->nlevels - 1;
+  load_kappa(*ctx, ctx->L[fl], kappa, where);
+  assemble_level(*ctx, fl, beta);
+  for (int l = fl - 1; l >= 0; --l) {
+    coarsen_kappa(*ctx, l);
+    assemble_level(*ctx, l, beta);
+  }
+  GB_API_END
+}
+
+int
+gb_level_get_values(gb_ctx* ctx, int lvl, double* val)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(val, GB_EINVAL, "null array");
+  host_values(*ctx, L);
+  std::memcpy(val, L.h_val.data(), L.h_val.size() * sizeof(double));
+  GB_API_END
+}
+
+int
+gb_level_get_kappa(gb_ctx* ctx, int lvl, double* kappa)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  check_mesh(L);
+  GB_REQUIRE(kappa, GB_EINVAL, "null array");
+  GB_CUDA(cudaMemcpyAsync(kappa, L.m_kappa.p, L.mesh_ncells * sizeof(double),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
   GB_API_END
 }
 

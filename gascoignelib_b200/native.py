@@ -106,6 +106,11 @@ _SIGS = {
     "gb_coeff_gradient": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD, C.c_int64],
     "gb_level_set_functional": [C.c_void_p, C.c_int, _PD, _PD],
     "gb_functional": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD],
+    "gb_level_set_mesh": [C.c_void_p, C.c_int, C.c_int, C.c_int64, _P64, _PD, _P64],
+    "gb_assemble": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, _PD],
+    "gb_assemble_levels": [C.c_void_p, C.c_void_p, C.c_int, _PD],
+    "gb_level_get_kappa": [C.c_void_p, C.c_int, _PD],
+    "gb_level_get_values": [C.c_void_p, C.c_int, _PD],
     "gb_ctx_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
@@ -257,6 +262,58 @@ class Context:
         if cells.mloc is not None:
             ml = np.ascontiguousarray(cells.mloc, dtype=np.float64)
             self._chk(self._L.gb_level_set_functional(self.h, level, _pd(ml), None))
+
+    # ------------------------------------------------------- device assembly
+    def set_mesh(self, level, dim, cells, coords, parent=None):
+        """Q1 cells (int64 [ncells, 2^dim], local node a at corner bits
+        (a&1, a>>1&1, a>>2&1)), node coordinates [n, dim] and, above level 0,
+        the parent cell on level-1 of every cell (gb_level_set_mesh)."""
+        nd = np.ascontiguousarray(cells, dtype=np.int64)
+        xy = np.ascontiguousarray(coords, dtype=np.float64)
+        pa = None if parent is None else np.ascontiguousarray(parent, dtype=np.int64)
+        self._chk(self._L.gb_level_set_mesh(self.h, level, dim, nd.shape[0], _p64(nd),
+                                            _pd(xy), _p64(pa) if pa is not None else None))
+
+    @staticmethod
+    def _kappa_arg(kappa):
+        """(pointer, where) for a numpy array (host) or a CUDA torch tensor."""
+        if hasattr(kappa, "data_ptr"):
+            if kappa.is_cuda:
+                import torch
+                assert kappa.dtype == torch.float64 and kappa.is_contiguous()
+                # the library reads it on its own stream: finish torch's writes
+                torch.cuda.current_stream(kappa.device).synchronize()
+                return C.c_void_p(kappa.data_ptr()), 1, None
+            kappa = kappa.numpy()
+        k = np.ascontiguousarray(kappa, dtype=np.float64)
+        return k.ctypes.data_as(C.c_void_p), 0, k
+
+    def assemble(self, level, kappa, beta=None):
+        """gb_assemble: the level's matrix from per-cell kappa (numpy: host,
+        CUDA tensor: device) and an optional convection vector."""
+        p, where, keep = self._kappa_arg(kappa)
+        b = None if beta is None else np.ascontiguousarray(beta, dtype=np.float64)
+        self._chk(self._L.gb_assemble(self.h, level, p, where,
+                                      _pd(b) if b is not None else None))
+        del keep
+
+    def assemble_levels(self, kappa, beta=None):
+        """gb_assemble_levels: every level from the finest level's kappa."""
+        p, where, keep = self._kappa_arg(kappa)
+        b = None if beta is None else np.ascontiguousarray(beta, dtype=np.float64)
+        self._chk(self._L.gb_assemble_levels(self.h, p, where,
+                                             _pd(b) if b is not None else None))
+        del keep
+
+    def level_values(self, level, nvals):
+        v = np.zeros(nvals)
+        self._chk(self._L.gb_level_get_values(self.h, level, _pd(v)))
+        return v
+
+    def level_kappa(self, level, ncells):
+        k = np.zeros(ncells)
+        self._chk(self._L.gb_level_get_kappa(self.h, level, _pd(k)))
+        return k
 
     # ------------------------------------------------------------ vectors
     def vec(self):

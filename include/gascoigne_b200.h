@@ -299,6 +299,48 @@ int gb_coeff_gradient(gb_ctx* ctx, int level, int u, int lam, double* grad,
 int gb_level_set_functional(gb_ctx* ctx, int level, const double* mloc,
                             const double* cell_scale);
 int gb_functional(gb_ctx* ctx, int level, int u, int g, double* J);
+/* Device-side assembly of the scalar Q1 equation -div(kappa grad u) +
+ * beta . grad u with one coefficient kappa per cell, into the sparsity
+ * pattern of the level's matrix (CGDisc::Matrix, DofHandler/cgdisc.h:599-635,
+ * with ElementIntegrator::Matrix, DofHandler/elementintegrator.xx:350-395,
+ * Gauss formulas QuadGauss4 / HexGauss8, DofHandler/elementintegrator.h:
+ * 214-222; strong Dirichlet rows and columns as SparseBlockMatrix::dirichlet,
+ * LinAlg/sparseblockmatrix.xx:207-218). No counterpart on the reference's GPU,
+ * which assembles on the host and uploads (cuda/cudacsrmatrixinterface.cc:
+ * 176-230).
+ * gb_level_set_mesh: the level's quadrilateral (dim 2) or hexahedral (dim 3)
+ * cells, cell c with nodes cell_nodes[c*2^dim + a], local node a at the
+ * reference-cell corner (a & 1, a >> 1 & 1, a >> 2 & 1); node coordinates
+ * coords[node*dim + d]; above level 0, parent[c] = the cell of level - 1 that
+ * contains cell c (for gb_assemble_levels). The level's matrix (gb_level_set_
+ * matrix, block size 1, its Dirichlet dofs and no hanging nodes) must be set
+ * first: every pair of nodes of a cell must be in its pattern. Setting the
+ * matrix again drops the mesh. */
+int gb_level_set_mesh(gb_ctx* ctx, int level, int dim, int64_t ncells,
+                      const int64_t* cell_nodes, const double* coords,
+                      const int64_t* parent);
+/* Assembles the level's matrix (FP64 and FP32 values, block-diagonal inverse)
+ * from kappa (ncells doubles; where = 0: host memory, 1: device memory,
+ * copied on the context's stream (gb_ctx_get_stream), so writes to it on other
+ * streams must be complete and it must stay valid until that copy ran) and
+ * beta (dim doubles in host memory, NULL for none): element matrices at the
+ * Gauss points, summed per matrix entry in ascending cell order, then the
+ * Dirichlet rows (identity) and columns (zero). */
+int gb_assemble(gb_ctx* ctx, int level, const double* kappa, int where,
+                const double* beta);
+/* gb_assemble on the finest level from kappa, then on each coarser level from
+ * the mean of its cells' children (summed in ascending child order): the
+ * coefficient of a coarse cell as the test harness's reference runs define it. */
+int gb_assemble_levels(gb_ctx* ctx, const double* kappa, int where,
+                       const double* beta);
+/* The level's cell coefficients last used by gb_assemble(_levels) (host
+ * array of ncells doubles). */
+int gb_level_get_kappa(gb_ctx* ctx, int level, double* kappa);
+/* The level's current FP64 matrix values in the order of the pattern given to
+ * gb_level_set_matrix (nnzb * B * B doubles, host array): the uploaded values,
+ * or those of the last device assembly; blocks row-major as NodeMatrix stores
+ * them (LinAlg/nodematrix.h:44-48). */
+int gb_level_get_values(gb_ctx* ctx, int level, double* val);
 /* The context's CUDA stream (a cudaStream_t): every gb_* call enqueues its
  * work there, so callers can order their own work or record events on it. */
 int gb_ctx_get_stream(const gb_ctx* ctx, void** stream);

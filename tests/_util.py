@@ -124,3 +124,55 @@ def rel(a, b):
 def rel_l2(a, b):
     nb = np.linalg.norm(b)
     return np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)
+
+
+def uniform_meshes(P):
+    """Per level (cells, parents) of a uniform unit square/cube hierarchy in the
+    problem's node numbering, for gb_level_set_mesh (parents None on level 0)."""
+    from oracle.assembly import uniform_cells, uniform_parents
+    out = []
+    for l, L in enumerate(P.levels):
+        cells = uniform_cells(L.coord, P.dim)
+        N = round(cells.shape[0] ** (1.0 / P.dim))
+        out.append((cells, uniform_parents(P.dim, N) if l > 0 else None))
+    return out
+
+
+def set_uniform_meshes(ctx, P):
+    for l, (cells, parents) in enumerate(uniform_meshes(P)):
+        ctx.set_mesh(l, P.dim, cells, P.levels[l].coord, parents)
+
+
+def oracle_level_values(P, kappa_fine, beta=None):
+    """The oracle's assembled values of every level from the finest kappa
+    (coarse kappa: mean of the children)."""
+    from oracle.assembly import assemble, coarsen_kappa, q1_element_matrices
+    meshes = uniform_meshes(P)
+    kap = [None] * P.nlevels
+    kap[-1] = np.asarray(kappa_fine, dtype=np.float64)
+    for l in range(P.nlevels - 2, -1, -1):
+        kap[l] = coarsen_kappa(kap[l + 1], meshes[l + 1][1], meshes[l][0].shape[0])
+    vals = []
+    for l, L in enumerate(P.levels):
+        cells = meshes[l][0]
+        E = q1_element_matrices(P.dim, L.coord[cells], kap[l], beta)
+        vals.append(assemble(L.n, L.rowptr, L.col, cells, E, L.dirichlet))
+    return vals, kap
+
+
+def golden_assembly_cases():
+    """Golden Q1 cases whose matrices the device assembly rebuilds: (name,
+    finest kappa, beta)."""
+    from gascoignelib_b200.problem import seeded_inputs
+    out = []
+    for name, seeded in (("q1_2d_c2_r3_seeded", True), ("q1_3d_c1_r3_seeded", True),
+                         ("q1_2d_c2_r4_poisson", False), ("q1_3d_c1_r3_conv_dual", True),
+                         ("q1_2d_c2_r4_conv_dual", True)):
+        z = np.load(os.path.join(GOLDEN, name + ".npz"))
+        dim, coarse, refine = int(z["key_dim"]), int(z["key_coarse"]), int(z["key_refine"])
+        kap = (seeded_inputs(dim, coarse, refine)[0] if seeded
+               else np.ones((coarse << refine) ** dim))
+        beta = ([float(t) for t in str(z["key_conv"]).split(",")] if "key_conv" in z.files
+                else None)
+        out.append((name, kap, beta))
+    return out

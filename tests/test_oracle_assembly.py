@@ -1,0 +1,45 @@
+"""The oracle's Q1 assembly (oracle/assembly.py) against the matrices the
+reference assembled (golden fixtures: every level, seeded per-cell kappa,
+with and without convection), and against the generator's assembly."""
+import numpy as np
+import pytest
+
+from _util import golden_assembly_cases, load_golden, oracle_level_values
+from gascoignelib_b200.problem import seeded_inputs, structured_problem
+from oracle.assembly import q1_element_matrices
+
+
+@pytest.mark.parametrize("name,kappa,beta", golden_assembly_cases(),
+                         ids=[c[0] for c in golden_assembly_cases()])
+def test_oracle_assembly_matches_reference(name, kappa, beta):
+    P, _ = load_golden(name)
+    vals, _ = oracle_level_values(P, kappa, beta)
+    for L, v in zip(P.levels, vals):
+        assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max()
+
+
+def test_element_matrix_of_a_distorted_cell():
+    """A non-affine hexahedron: rows of the diffusion part sum to zero (constants
+    are in its kernel) and the matrix is symmetric; an affine map of the unit
+    cube gives the tensor-product matrix of a box."""
+    rng = np.random.default_rng(3)
+    corners = np.array([[(a >> d) & 1 for d in range(3)] for a in range(8)], dtype=float)
+    x = corners + 0.15 * rng.uniform(-1, 1, size=corners.shape)
+    E = q1_element_matrices(3, x[None], np.array([2.0]))[0]
+    assert np.abs(E.sum(axis=1)).max() < 1e-14
+    assert np.abs(E - E.T).max() < 1e-14
+    box = corners * np.array([0.5, 0.25, 2.0])
+    Eb = q1_element_matrices(3, box[None], np.array([1.0]))[0]
+    m = lambda h: np.array([[1 / 3, 1 / 6], [1 / 6, 1 / 3]]) * h
+    s = lambda h: np.array([[1.0, -1.0], [-1.0, 1.0]]) / h
+    ref = (np.kron(np.kron(m(2.0), m(0.25)), s(0.5)) + np.kron(np.kron(m(2.0), s(0.25)), m(0.5))
+           + np.kron(np.kron(s(2.0), m(0.25)), m(0.5)))
+    assert np.abs(Eb - ref).max() < 1e-14 * np.abs(ref).max()
+
+
+def test_oracle_assembly_matches_generator():
+    kappa, rhs = seeded_inputs(3, 1, 4)
+    P = structured_problem(3, 1, 4, kappa, rhs, beta=(1.0, -0.5, 0.25))
+    vals, _ = oracle_level_values(P, kappa, (1.0, -0.5, 0.25))
+    for L, v in zip(P.levels, vals):
+        assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max()
