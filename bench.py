@@ -123,7 +123,8 @@ def cpu_baseline(kappa_rhs, ndof, threads):
                            f"({med:.3f} s/solve, {s['iterations'][0]} iterations, true rel "
                            f"residual {float(s['true_rel_residual'][0]):.2e}; "
                            f"harness wall {wall:.1f} s incl. mesh+assembly)"),
-                "solve_s": med, "iterations": int(s["iterations"][0])}
+                "solve_s": med, "iterations": int(s["iterations"][0]),
+                "assemble_s": float(s["assemble_s"][0]) if "assemble_s" in s else None}
     from gascoignelib_b200.problem import structured_problem
     P = structured_problem(DIM, COARSE, REFINE, kappa, rhs)
     O = Oracle(P)
@@ -175,6 +176,46 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line))
 
 
+def assembly_leg(c, P, kappa, steps, warmup, flush, dev):
+    """Device assembly of every level from the finest level's kappa (a CUDA
+    tensor): element matrices, their sum into the SELL values (FP64 + FP32),
+    Dirichlet rows/columns, block-diagonal inverse, kappa coarsening. Device
+    time with CUDA events on the solver's stream, L2 flushed before each."""
+    import torch
+
+    from gascoignelib_b200.problem import structured_meshes
+
+    for l, (cells, coord, par) in enumerate(structured_meshes(P)):
+        c.set_mesh(l, P.dim, cells, coord, par)
+    kd = torch.tensor(kappa, dtype=torch.float64, device=dev)
+    st = torch.cuda.ExternalStream(c.stream(), device=dev)
+    for _ in range(warmup):
+        c.assemble_levels(kd)
+    ms = []
+    for _ in range(steps):
+        flush.random_(0, 255)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        c.assemble_levels(kd)
+        e1.record(st)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    # algorithmic bytes: per cell 2^d node indices, kappa, element matrix
+    # written and read back, its entry list; per stored entry column, entry
+    # pointer, FP64 + FP32 value; per row mask, diagonal, inverse (FP64 + FP32)
+    nl = 1 << P.dim
+    by = 0
+    for L in P.levels:
+        nc = (round(L.n ** (1.0 / P.dim)) - 1) ** P.dim
+        by += nc * (4 * nl + 8 + 2 * 8 * nl * nl + 4 * nl * nl)
+        by += L.val.size * (4 + 4 + 8 + 4) + L.n * (1 + 4 + 8 + 8 + 8 + 4 + 8 * P.dim)
+    t = sorted(ms)[len(ms) // 2]
+    return {"ms": t, "levels": P.nlevels, "cells_finest": int(nc),
+            "algorithmic_bytes": by, "achieved_gbs": by / (t * 1e-3) / 1e9}
+
+
 def adjoint_c5(local, steps, warmup, flush):
     """Forward + adjoint + coefficient gradient at 96^3 cells (912,673 dofs):
     mixed forward solve, J = int u^2 and dJ/du = 2 M u on the device, mixed
@@ -221,6 +262,26 @@ def adjoint_c5(local, steps, warmup, flush):
     J = c.functional(l, u, g)
     grad = c.coeff_gradient(l, u, lam)
     t = sum(ms) / len(ms)
+    # one design step with a new kappa: device assembly of all levels, then
+    # the same forward + adjoint + gradient
+    asm = assembly_leg(c, P, kappa, steps, warmup, flush, dev)
+    kd = torch.tensor(kappa, dtype=torch.float64, device=dev)
+    for _ in range(warmup):
+        c.assemble_levels(kd)
+        step()
+    ms2 = []
+    for _ in range(steps):
+        flush.random_(0, 255)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        c.assemble_levels(kd)
+        step()
+        e1.record(st)
+        e1.synchronize()
+        ms2.append(e0.elapsed_time(e1))
+    asm["assemble_forward_adjoint_gradient_ms"] = sum(ms2) / len(ms2)
     out = {"workload": "3D diffusion, kappa = exp(N(0,1)) per cell, 96^3 Q1 cells, "
                        "J = int u^2: forward solve + dJ/du + adjoint solve + dJ/dkappa",
            "dofs": P.finest.ndof, "cells": P.cells.ncells, "ms_per_step": t,
@@ -230,6 +291,7 @@ def adjoint_c5(local, steps, warmup, flush):
            "adjoint": {"ms": ai["device_ms"], "iterations": ai["iterations"],
                        "true_rel_residual": ai["true_rel_residual"]},
            "J": J, "grad_norm": float(np.linalg.norm(grad)),
+           "assembly": asm,
            "l2": "flushed (256 MB write) before every step"}
     c.close()
     return out
@@ -468,6 +530,8 @@ def main():
     if os.path.exists(pj):
         prof = json.load(open(pj))
 
+    asm = assembly_leg(ctx, P, kappa, min(args.steps, 5), 2, flush, torch.device(f"cuda:{local}"))
+
     adj = None
     if not args.no_adjoint:
         adj = adjoint_c5(local, min(args.steps, 5), 2, flush)
@@ -520,6 +584,11 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "cpu_baseline": cb,
+            "assembly_c2": dict(asm, workload="Q1 matrices of all 6 levels of the 64^3 "
+                                "problem from the per-cell kappa (device)",
+                                reference_cpu_s=(cb or {}).get("assemble_s"),
+                                reference_cpu_note="reference AssembleMatrix + ComputeIlu "
+                                "on all levels, host threads as cpu_baseline.cores"),
             "adjoint_c5": adj,
             "stokes_c3": stk,
             "q2_c4": q2,

@@ -16,11 +16,12 @@ namespace gb {
 // 1/2 -+ g of the unit cell the multilinear map's Jacobian J, the physical
 // gradients of the Q1 basis, and
 //   E[a][b] += w |J| (kappa grad phi_b . grad phi_a + (beta . grad phi_b) phi_a)
-// (row a: test function, column b: trial function). Local node a has the
+// (row a: test function, column b: trial function; CONV: beta is not zero).
+// Local node a has the
 // corner bits (a & 1, a >> 1 & 1, a >> 2 & 1). cells: node of local a of cell
 // c at cells[a * ncells + c]; coords: node-major, DIM per node. E: entry (a, b)
 // of cell c at E[(a * NL + b) * ncells + c] (coalesced per entry).
-template<int DIM>
+template<int DIM, bool CONV>
 __global__ void __launch_bounds__(128)
 k_q1_element(int ncells, const int* __restrict__ cells, const double* __restrict__ coords,
              const double* __restrict__ kappa, double b0, double b1, double b2, double g,
@@ -83,27 +84,29 @@ k_q1_element(int ncells, const int* __restrict__ cells, const double* __restrict
           s = fma(X[a][d], gr[a][k], s);
         J[d][k] = s;
       }
-    double det, Ji[DIM][DIM]; // Ji[k][d] = d xi_k / d x_d
+    double det, Ji[DIM][DIM]; // Ji[k][d] = d xi_k / d x_d (cofactors / det)
     if (DIM == 2) {
       det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
-      Ji[0][0] = J[1][1] / det;
-      Ji[0][1] = -J[0][1] / det;
-      Ji[1][0] = -J[1][0] / det;
-      Ji[1][1] = J[0][0] / det;
+      const double r = 1.0 / det;
+      Ji[0][0] = J[1][1] * r;
+      Ji[0][1] = -J[0][1] * r;
+      Ji[1][0] = -J[1][0] * r;
+      Ji[1][1] = J[0][0] * r;
     } else {
       const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
       const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
       const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
       det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
-      Ji[0][0] = c00 / det;
-      Ji[1][0] = c01 / det;
-      Ji[2][0] = c02 / det;
-      Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
-      Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
-      Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
-      Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
-      Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
-      Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+      const double r = 1.0 / det;
+      Ji[0][0] = c00 * r;
+      Ji[1][0] = c01 * r;
+      Ji[2][0] = c02 * r;
+      Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * r;
+      Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * r;
+      Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * r;
+      Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * r;
+      Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * r;
+      Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * r;
     }
     const double w = wq * fabs(det);
     // physical gradients and beta . grad phi
@@ -122,31 +125,48 @@ k_q1_element(int ncells, const int* __restrict__ cells, const double* __restrict
       }
       bg[a] = s;
     }
+    // the diffusion part is symmetric: each product once, added to both
+    const double wk = w * kap;
 #pragma unroll
     for (int a = 0; a < NL; ++a)
 #pragma unroll
-      for (int b = 0; b < NL; ++b) {
+      for (int b = a; b < NL; ++b) {
         double dg = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d)
           dg = fma(gx[b][d], gx[a][d], dg);
-        e[a * NL + b] = fma(w, fma(kap, dg, bg[b] * phi[a]), e[a * NL + b]);
+        e[a * NL + b] = fma(wk, dg, e[a * NL + b]);
+        if (b != a)
+          e[b * NL + a] = fma(wk, dg, e[b * NL + a]);
       }
+    if (CONV) {
+#pragma unroll
+      for (int a = 0; a < NL; ++a) {
+        const double wp = w * phi[a];
+#pragma unroll
+        for (int b = 0; b < NL; ++b)
+          e[a * NL + b] = fma(wp, bg[b], e[a * NL + b]);
+      }
+    }
   }
 #pragma unroll
   for (int p = 0; p < NL * NL; ++p)
     E[int64_t(p) * ncells + c] = e[p];
 }
 
-// The level's SELL values from the element matrices, one thread per slot
-// (LocalToGlobal + MatrixInterface::entry, DofHandler/cgdisc.h:353-366): entry
-// e sums E[clist[k]] for k in [cptr[e], cptr[e+1]), the contributions in
-// ascending cell order (the reference's cell loop). Then the strong Dirichlet
-// condition (SparseBlockMatrix::dirichlet, LinAlg/sparseblockmatrix.xx:207-218):
-// a Dirichlet row keeps only its diagonal, set to 1, and a Dirichlet column is
+// The level's SELL values from the element matrices (LocalToGlobal +
+// MatrixInterface::entry, DofHandler/cgdisc.h:353-366): entry e sums
+// E[clist[k]] for k in [cptr[e], cptr[e+1]), the contributions in ascending
+// cell order (the reference's cell loop). Then the strong Dirichlet condition
+// (SparseBlockMatrix::dirichlet, LinAlg/sparseblockmatrix.xx:207-218): a
+// Dirichlet row keeps only its diagonal, set to 1, and a Dirichlet column is
 // zero elsewhere. Writes the FP64 and FP32 values and the diagonal (dd) for the
-// block-diagonal inverse.
-__global__ void __launch_bounds__(kSpmvThreads)
+// block-diagonal inverse. kAsmSplit warps per slice: warp g of slice s takes
+// the entries j = g, g + kAsmSplit, .. of the slice's 32 rows (lane = row), so
+// that a row's entries are summed by several threads at once.
+constexpr int kAsmSplit = 4;
+
+__global__ void __launch_bounds__(256)
 k_asm_gather(int n, const int* __restrict__ sptr, const int* __restrict__ perm,
              const int* __restrict__ col, const int* __restrict__ cptr,
              const int* __restrict__ clist, const double* __restrict__ E,
@@ -154,24 +174,41 @@ k_asm_gather(int n, const int* __restrict__ sptr, const int* __restrict__ perm,
              double* __restrict__ v64, float* __restrict__ v32, double* __restrict__ dd)
 {
   GB_PDL_ENTRY();
-  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int lane = static_cast<int>(t & 31);
+  const int64_t wq = t >> 5;
+  const int s = static_cast<int>(wq / kAsmSplit), g = static_cast<int>(wq % kAsmSplit);
+  const int slot = s * kSlice + lane;
   if (slot >= n)
     return;
   const int row = perm ? __ldg(perm + slot) : slot;
-  const int s = slot >> 5, lane = slot & 31;
   const int beg = __ldg(sptr + s);
   const int w = (__ldg(sptr + s + 1) - beg) >> 5;
   const bool drow = __ldg(dirmask + row) != 0;
   const int dpos = __ldg(diagpos + row);
-  for (int j = 0; j < w; ++j) {
+  for (int j = g; j < w; j += kAsmSplit) {
     const int e = beg + j * kSlice + lane;
     double v = 0.0;
     if (drow) {
       v = e == dpos ? 1.0 : 0.0;
     } else if (!__ldg(dirmask + __ldg(col + e))) {
+      // the entry's contributions in groups of 8: their indices, then their
+      // values, are loaded together; summed in ascending order
       const int k1 = __ldg(cptr + e + 1);
-      for (int k = __ldg(cptr + e); k < k1; ++k)
-        v += __ldg(E + __ldg(clist + k));
+      for (int k0 = __ldg(cptr + e); k0 < k1; k0 += 8) {
+        int idx[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          idx[q] = k0 + q < k1 ? __ldg(clist + k0 + q) : -1;
+        double ev[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          ev[q] = idx[q] >= 0 ? __ldg(E + idx[q]) : 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (idx[q] >= 0)
+            v += ev[q];
+      }
     }
     v64[e] = v;
     v32[e] = static_cast<float>(v);
@@ -196,6 +233,22 @@ k_kappa_coarsen(int nc, const int* __restrict__ cptr, const int* __restrict__ ch
   for (int k = k0; k < k1; ++k)
     s += __ldg(kf + __ldg(child + k));
   kc[c] = s / double(k1 - k0);
+}
+
+// v[e] = src[map[e]] (0 where map[e] < 0), FP64 and FP32: the transpose's
+// values from the matrix's after a device assembly.
+__global__ void
+k_gather_values(int64_t ne, const int* __restrict__ map, const double* __restrict__ src,
+                double* __restrict__ v64, float* __restrict__ v32)
+{
+  GB_PDL_ENTRY();
+  const int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (e >= ne)
+    return;
+  const int m = __ldg(map + e);
+  const double v = m >= 0 ? __ldg(src + m) : 0.0;
+  v64[e] = v;
+  v32[e] = static_cast<float>(v);
 }
 
 } // namespace gb

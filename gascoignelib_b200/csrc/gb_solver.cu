@@ -399,6 +399,9 @@ struct Level
   int64_t child_n = -1; // coarse cells the child lists were built for
   // values assembled on the device since the host copy was made
   bool h_val_stale = false;
+  // per A^T SELL entry the A SELL entry it copies (-1: padding), block size 1:
+  // the transpose's values follow a device assembly without the host
+  DeviceArray<int> at_map;
   bool has_hn() const { return !hn.empty(); }
   int64_t ndof() const { return n * B; }
 };
@@ -442,6 +445,10 @@ struct CoarseProgram
   const void* tmp_out = nullptr;
   char p0_out = 'V';
   bool zero_out = false;
+  // the batch launch that formed K, kept to form it again in place after the
+  // matrix values change (a device assembly)
+  CoarseBatch batch{};
+  int tsize = 0;
 };
 
 template<class T>
@@ -532,6 +539,9 @@ struct gb_ctx
   int mid_grid[2] = { 0, 0 }; // per precision (FP64, FP32)
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
   gb::DeviceArray<double> asm_E; // element matrices of the level being assembled
+  // matrix values changed on the device since the solver's set-up (dense
+  // coarse maps, direct inverse): refreshed in place at the next solve
+  bool values_dirty = false;
   gb::DeviceArray<float> rhs32, zfix32;
   ~gb_ctx()
   {
@@ -830,6 +840,28 @@ host_values(Context& c, Level& L)
   L.h_val_stale = false;
 }
 
+// SELL position of every stored entry k (CSR order of rowptr) of S.
+static std::vector<int>
+sell_positions(Context& c, const Sell& S, const int64_t* rowptr, int64_t n)
+{
+  std::vector<int> sptr(S.nslices + 1), perm(n), slot(n), pos(rowptr[n]);
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  GB_CUDA(cudaMemcpy(sptr.data(), S.sptr.p, sptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  if (S.sorted)
+    GB_CUDA(cudaMemcpy(perm.data(), S.rperm.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+  else
+    for (int64_t t = 0; t < n; ++t)
+      perm[t] = static_cast<int>(t);
+  for (int64_t t = 0; t < n; ++t)
+    slot[perm[t]] = static_cast<int>(t);
+  for (int64_t r = 0; r < n; ++r) {
+    const int64_t t = slot[r];
+    for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k)
+      pos[k] = static_cast<int>(sptr[t / kSlice] + (k - rowptr[r]) * kSlice + t % kSlice);
+  }
+  return pos;
+}
+
 static void
 ensure_AT(Context& c, Level& L)
 {
@@ -840,8 +872,10 @@ ensure_AT(Context& c, Level& L)
   const int64_t n = L.n, nnz = L.h_rowptr[n];
   std::vector<int64_t> tp(n + 1, 0), tc(nnz);
   std::vector<double> tv(nnz * B2);
+  std::vector<int64_t> srcidx(nnz);
   // block (j, i) of A, transposed, as block (i, j) of A^T
   auto put = [&](int64_t dst, int64_t src) {
+    srcidx[dst] = src;
     for (int r = 0; r < B; ++r)
       for (int q = 0; q < B; ++q)
         tv[dst * B2 + r * B + q] = L.h_val[src * B2 + q * B + r];
@@ -878,6 +912,17 @@ ensure_AT(Context& c, Level& L)
   GB_CUDA(cudaStreamSynchronize(c.stream));
   build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), c.stream, B);
   L.has_AT = true;
+  if (B == 1 && L.mesh_ncells > 0) { // device-assembled level: keep A^T current on the GPU
+    const std::vector<int> pa = sell_positions(c, L.A, L.h_rowptr.data(), n);
+    const std::vector<int> pt = sell_positions(c, L.AT, tp.data(), n);
+    std::vector<int> map(L.AT.entries, -1);
+    for (int64_t q = 0; q < nnz; ++q)
+      map[pt[q]] = pa[srcidx[q]];
+    GB_CUDA(L.at_map.alloc(map.size()));
+    GB_CUDA(h2d(c.stream, L.at_map.p, map.data(), map.size() * sizeof(int)));
+  } else {
+    L.at_map.release();
+  }
 }
 
 // ---------------------------------------------------------- level set-up
@@ -1098,10 +1143,46 @@ ensure_direct(Context& c)
   c.dir_ready[t] = true;
 }
 
+// After a device assembly: the dense maps of the single-CTA coarse programs
+// formed again into their own buffers (the captured solver graphs keep
+// pointing at them), generic dense maps dropped (rebuilt at first use, with
+// the graphs), the direct coarse inverse formed again at its next use.
+static void
+refresh_values(Context& c)
+{
+  const int64_t launches0 = c.launches;
+  for (auto& kv : c.coarse_progs) {
+    CoarseProgram& p = kv.second;
+    if (p.ncols == 0 || p.tsize == 0)
+      continue;
+    if (kv.first.tr)
+      for (int l = 0; l <= kv.first.level; ++l)
+        ensure_AT(c, c.L[l]);
+    if (p.tsize == 8)
+      launch_smem(c, k_coarse_cycle<double>, p.ncols, kCoarseThreads, p.smem_bytes,
+                  (const CoarseOp*)p.ops.p, p.nops, (const CoarseBuf*)p.bufs.p, p.nbufs,
+                  (const CoarsePrefetch*)p.pre.p, p.npre, p.vec_bytes, p.batch);
+    else
+      launch_smem(c, k_coarse_cycle<float>, p.ncols, kCoarseThreads, p.smem_bytes,
+                  (const CoarseOp*)p.ops.p, p.nops, (const CoarseBuf*)p.bufs.p, p.nbufs,
+                  (const CoarsePrefetch*)p.pre.p, p.npre, p.vec_bytes, p.batch);
+  }
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  c.launches = launches0; // set-up, not part of a solve
+  if (!c.dense_maps.empty()) {
+    c.dense_maps.clear();
+    c.version++;
+  }
+  c.dir_ready[0] = c.dir_ready[1] = false;
+  c.values_dirty = false;
+}
+
 static void
 ensure_work(Context& c)
 {
   if (c.work_ready) {
+    if (c.values_dirty)
+      refresh_values(c);
     ensure_direct(c); // the other orientation after gb_set_operator
     return;
   }
@@ -1182,6 +1263,7 @@ ensure_work(Context& c)
   c.dense_maps.clear();
   c.mid_progs.clear();
   c.dir_ready[0] = c.dir_ready[1] = false;
+  c.values_dirty = false;
   ensure_direct(c);
   c.work_ready = true;
 }
@@ -1969,6 +2051,8 @@ coarse_program(Context& c, MgWork<T>& W, int l, int finelevel, int coarselevel, 
                   prog.vec_bytes, bt);
       GB_CUDA(cudaStreamSynchronize(c.stream));
       c.launches--; // set-up, not part of a solve
+      prog.batch = bt;
+      prog.tsize = int(sizeof(T));
     }
     prog.u_out = u2;
     prog.tmp_out = t2;
@@ -2837,14 +2921,19 @@ assemble_level(Context& c, int l, const double* beta)
   const double b0 = beta ? beta[0] : 0.0, b1 = beta ? beta[1] : 0.0;
   const double b2 = beta && dim == 3 ? beta[2] : 0.0;
   const double g = 0.5 / std::sqrt(3.0);
-  if (dim == 2)
-    launch(c, k_q1_element<2>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,
-           (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p);
-  else
-    launch(c, k_q1_element<3>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,
-           (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p);
+  const bool conv = b0 != 0.0 || b1 != 0.0 || b2 != 0.0;
+#define GB_ELEM(D, CV)                                                                   \
+  launch(c, k_q1_element<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,  \
+         (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p)
+  if (dim == 2) {
+    if (conv) GB_ELEM(2, true); else GB_ELEM(2, false);
+  } else {
+    if (conv) GB_ELEM(3, true); else GB_ELEM(3, false);
+  }
+#undef GB_ELEM
   const Sell& A = L.A;
-  launch(c, k_asm_gather, blocks_for(L.n, kSpmvThreads), kSpmvThreads, (int)L.n,
+  launch(c, k_asm_gather, blocks_for(int64_t(A.nslices) * kAsmSplit * kSlice, 256), 256,
+         (int)L.n,
          (const int*)A.sptr.p, (const int*)(A.sorted ? A.rperm.p : nullptr),
          (const int*)A.col.p, (const int*)L.m_cptr.p, (const int*)L.m_clist.p,
          (const double*)c.asm_E.p, (const uint8_t*)L.dirmask.p, (const int*)L.m_diagpos.p,
@@ -2852,10 +2941,18 @@ assemble_level(Context& c, int l, const double* beta)
   launch(c, k_blockdiag_inverse<1>, blocks_for(L.n, 128), 128, (int)L.n,
          (const double*)L.m_dd.p, L.dinv64.p, L.dinv32.p);
   L.h_val_stale = true;
-  L.has_AT = false;
-  L.vk_ready = false;
-  c.work_ready = false;
-  c.version++;
+  if (L.has_AT && L.at_map.n) // A^T: the same values, gathered in its order
+    launch(c, k_gather_values, blocks_for(int64_t(L.AT.entries), 256), 256,
+           (int64_t)L.AT.entries, (const int*)L.at_map.p, (const double*)A.v64.p, L.AT.v64.p,
+           L.AT.v32.p);
+  else
+    L.has_AT = false;
+  if (c.params.smoother != 0 || L.vk_ready) { // Vanka factors: full set-up again
+    L.vk_ready = false;
+    c.work_ready = false;
+    c.version++;
+  }
+  c.values_dirty = true;
   if (c.transposed)
     ensure_AT(c, L); // the operator in use stays current
 }
@@ -4099,6 +4196,10 @@ gb_level_set_mesh(gb_ctx* ctx, int lvl, int dim, int64_t ncells, const int64_t* 
   L.mesh_dim = dim;
   L.mesh_ncells = ncells;
   L.mesh_n = n;
+  if (L.has_AT) { // the transpose again, with its map for device refreshes
+    L.has_AT = false;
+    ensure_AT(*ctx, L);
+  }
   if (lvl > 0)
     ctx->L[lvl - 1].child_n = -1; // its child lists follow this level's parents
   GB_API_END

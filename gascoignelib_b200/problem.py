@@ -374,6 +374,29 @@ def structured_problem(dim: int, coarse: int, refine: int,
                    cells=cells)
 
 
+def cell_parents(dim: int, N: int) -> np.ndarray:
+    """Parent cell on the N/2 mesh of every cell of the uniform N mesh (both
+    lexicographic, x fastest)."""
+    i = np.arange(N)
+    h = N // 2
+    if dim == 3:
+        k, j, ii = np.meshgrid(i, i, i, indexing="ij")
+        return (((k // 2) * h + j // 2) * h + ii // 2).ravel().astype(np.int64)
+    j, ii = np.meshgrid(i, i, indexing="ij")
+    return ((j // 2) * h + ii // 2).ravel().astype(np.int64)
+
+
+def structured_meshes(P: Problem):
+    """Per level (cells, coordinates, parents) of a structured_problem
+    hierarchy for gb_level_set_mesh (lexicographic cells, local nodes
+    lexicographic; parents None on level 0)."""
+    out = []
+    for l, L in enumerate(P.levels):
+        N = int(round(L.n ** (1.0 / P.dim))) - 1
+        out.append((cell_nodes(P.dim, N), L.coord, cell_parents(P.dim, N) if l else None))
+    return out
+
+
 def seeded_inputs(dim: int, coarse: int, refine: int, kappa_seed: int = 1001,
                   rhs_seed: int = 1002, sigma: float = 1.0):
     """Seeded synthetic coefficient and load: kappa = exp(N(0, sigma)) per finest

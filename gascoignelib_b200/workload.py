@@ -30,6 +30,8 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--problem", default="diffusion", choices=["diffusion", "stokes", "q2", "q2ball"],
                     help="stokes: 2D Q1/Q1 Stokes with Vanka on (2*2^(refine-1))^2 cells")
+    ap.add_argument("--assemble", type=int, default=0,
+                    help="only K device assemblies of every level (diffusion problem)")
     ap.add_argument("--ktime", action="store_true",
                     help="per-kernel CUDA-event times of the last solve (GB_GRAPH=0)")
     a = ap.parse_args(argv)
@@ -57,6 +59,21 @@ def main(argv=None):
         keys.setdefault("maxiter", 200)
         ctx.set_params(tol=1e-8, globaltol=1e-300, iterpre=2, iterpost=2, **keys)
         fl = P.nlevels - 1
+        if a.assemble:
+            import time
+            from gascoignelib_b200.problem import structured_meshes
+            for l, (cells, coord, par) in enumerate(structured_meshes(P)):
+                ctx.set_mesh(l, P.dim, cells, coord, par)
+            ctx.assemble_levels(kappa)  # set-up outside the count
+            ctx.synchronize()
+            k0 = ctx.kernel_count()
+            t0 = time.time()
+            for _ in range(a.assemble):
+                ctx.assemble_levels(kappa)
+            ctx.synchronize()
+            print(json.dumps({"assemblies": a.assemble, "kernels": ctx.kernel_count() - k0,
+                              "wall_ms_each": 1e3 * (time.time() - t0) / a.assemble}))
+            return
         if a.smooth:
             x, y, h = ctx.vec(), ctx.vec(), ctx.vec()
             ctx.upload(fl, y, P.rhs)

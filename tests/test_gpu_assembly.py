@@ -152,3 +152,49 @@ def test_assembly_full_size_against_generator(ctx):
     assert info["status_name"] == "converged" and info["iterations"] <= 12
     ctx.free(x)
     ctx.free(b)
+
+
+@pytest.mark.parametrize("nd", [0, 1000])
+def test_reassembly_after_solves(ctx, nd):
+    """Solves (captured solver graphs, dense coarse maps, the transpose, the
+    direct coarse inverse) first, then a new kappa assembled on the device: the
+    next forward, adjoint and mixed solves use the new matrices."""
+    kappa, rhs = seeded_inputs(3, 1, 4)
+    beta = (1.0, 0.5, 0.25)
+    P = structured_problem(3, 1, 4, kappa, rhs, beta=beta)
+    ctx.load_problem(P)
+    set_uniform_meshes(ctx, P)
+    keys = dict(iterpre=2, iterpost=2, omega=0.8, gmressize=21, ndirect=nd)
+    ctx.set_params(tol=1e-8, globaltol=1e-300, maxiter=100, **keys)
+    fl = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(fl, b, P.rhs)
+    ctx.assemble_levels(kappa, beta)
+    ctx.gmres(x, b)
+    ctx.adjoint_gmres(x, b)
+    ctx.fgmres(x, b, GB_FP32)
+    ctx.adjoint_fgmres(x, b, GB_FP32)
+    k2 = 1.0 / kappa
+    ctx.assemble_levels(torch.tensor(k2, device="cuda"), beta)
+    ovals, _ = oracle_level_values(P, k2, beta)
+    Q = _with_values(P, ovals)
+    xo, io = Oracle(Q, ndirect=nd, omega=0.8).gmres(vmax=21, tol=1e-8, globaltol=1e-300)
+    info = ctx.gmres(x, b)
+    assert abs(info["iterations"] - io["iterations"]) <= 1
+    assert rel_l2(ctx.download(fl, x), xo) < 1e-8
+    lo, jo = Oracle(transposed_problem(Q), ndirect=nd, omega=0.8).gmres(
+        vmax=21, tol=1e-8, globaltol=1e-300)
+    ai = ctx.adjoint_gmres(x, b)
+    assert abs(ai["iterations"] - jo["iterations"]) <= 1
+    assert rel_l2(ctx.download(fl, x), lo) < 1e-8
+    ctx.set_params(tol=1e-10, globaltol=1e-300, maxiter=300, **keys)
+    A = sp.csr_matrix((ovals[-1], P.finest.col, P.finest.rowptr), shape=(P.finest.n,) * 2)
+    fi = ctx.fgmres(x, b, GB_FP32)
+    u = ctx.download(fl, x)
+    assert np.linalg.norm(P.rhs - A @ u) <= 1e-9 * np.linalg.norm(P.rhs)
+    af = ctx.adjoint_fgmres(x, b, GB_FP32)
+    lam = ctx.download(fl, x)
+    assert np.linalg.norm(P.rhs - A.T @ lam) <= 1e-9 * np.linalg.norm(P.rhs)
+    assert fi["status_name"] == "converged" and af["status_name"] == "converged"
+    ctx.free(x)
+    ctx.free(b)
