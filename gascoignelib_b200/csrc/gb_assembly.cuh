@@ -251,4 +251,175 @@ k_gather_values(int64_t ne, const int* __restrict__ map, const double* __restric
   v32[e] = static_cast<float>(v);
 }
 
+// Element residuals of the same equation for a given vector x, one thread per
+// cell (CGDisc::Form, DofHandler/cgdisc.h:415-450, with the element
+// integrator's Form at the Gauss points of the matrix formula): with grad u =
+// sum_b x_b grad phi_b,
+//   F[a] += w |J| (kappa grad u . grad phi_a + (beta . grad u) phi_a),
+// written F[a * ncells + c].
+template<int DIM, bool CONV>
+__global__ void __launch_bounds__(128)
+k_q1_form(int ncells, const int* __restrict__ cells, const double* __restrict__ coords,
+          const double* __restrict__ kappa, double b0, double b1, double b2, double g,
+          const double* __restrict__ x, double* __restrict__ F)
+{
+  GB_PDL_ENTRY();
+  constexpr int NL = 1 << DIM;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells)
+    return;
+  double X[NL][DIM], u[NL];
+#pragma unroll
+  for (int a = 0; a < NL; ++a) {
+    const int64_t node = __ldg(cells + int64_t(a) * ncells + c);
+    u[a] = __ldg(x + node);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      X[a][d] = __ldg(coords + node * DIM + d);
+  }
+  const double kap = __ldg(kappa + c);
+  const double beta[3] = { b0, b1, b2 };
+  const double gp[2] = { 0.5 - g, 0.5 + g };
+  constexpr double wq = DIM == 3 ? 0.125 : 0.25;
+  double f[NL];
+#pragma unroll
+  for (int a = 0; a < NL; ++a)
+    f[a] = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < NL; ++q) {
+    double xi[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      xi[d] = gp[(q >> d) & 1];
+    double phi[NL], gr[NL][DIM];
+#pragma unroll
+    for (int a = 0; a < NL; ++a) {
+      phi[a] = 1.0;
+#pragma unroll
+      for (int k = 0; k < DIM; ++k)
+        gr[a][k] = 1.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const bool bit = (a >> d) & 1;
+        const double fd = bit ? xi[d] : 1.0 - xi[d];
+        phi[a] *= fd;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k)
+          gr[a][k] *= k == d ? (bit ? 1.0 : -1.0) : fd;
+      }
+    }
+    double J[DIM][DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) {
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < NL; ++a)
+          s = fma(X[a][d], gr[a][k], s);
+        J[d][k] = s;
+      }
+    double det, Ji[DIM][DIM];
+    if (DIM == 2) {
+      det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+      const double r = 1.0 / det;
+      Ji[0][0] = J[1][1] * r;
+      Ji[0][1] = -J[0][1] * r;
+      Ji[1][0] = -J[1][0] * r;
+      Ji[1][1] = J[0][0] * r;
+    } else {
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+      const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+      const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      const double r = 1.0 / det;
+      Ji[0][0] = c00 * r;
+      Ji[1][0] = c01 * r;
+      Ji[2][0] = c02 * r;
+      Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * r;
+      Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * r;
+      Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * r;
+      Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * r;
+      Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * r;
+      Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * r;
+    }
+    const double w = wq * fabs(det);
+    double gx[NL][DIM], gu[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      gu[d] = 0.0;
+#pragma unroll
+    for (int a = 0; a < NL; ++a)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k)
+          t = fma(gr[a][k], Ji[k][d], t);
+        gx[a][d] = t;
+        gu[d] = fma(u[a], t, gu[d]);
+      }
+    double bu = 0.0;
+    if (CONV) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        bu = fma(beta[d], gu[d], bu);
+    }
+    const double wk = w * kap;
+#pragma unroll
+    for (int a = 0; a < NL; ++a) {
+      double dg = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        dg = fma(gu[d], gx[a][d], dg);
+      f[a] = fma(wk, dg, f[a]);
+      if (CONV)
+        f[a] = fma(w * phi[a], bu, f[a]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < NL; ++a)
+    F[int64_t(a) * ncells + c] = f[a];
+}
+
+// y[r] += d * (the element residuals of the cells of node r, in ascending cell
+// order: LocalToGlobal, DofHandler/cgdisc.h:367-380); nodes whose entries in
+// nptr are empty keep y.
+__global__ void
+k_form_gather(int n, const int* __restrict__ nptr, const int* __restrict__ nlist,
+              const double* __restrict__ F, double d, double* __restrict__ y)
+{
+  GB_PDL_ENTRY();
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n)
+    return;
+  double acc = y[r];
+  const int k1 = __ldg(nptr + r + 1);
+  for (int k = __ldg(nptr + r); k < k1; ++k)
+    acc += d * __ldg(F + __ldg(nlist + k));
+  y[r] = acc;
+}
+
+// y = 0 on the Dirichlet dofs, and the largest |y| into *m (the bit pattern of
+// a non-negative double orders like the number: atomicMax on it is exact and
+// independent of the order)
+__global__ void
+k_dirichlet_absmax(int n, const uint8_t* __restrict__ dirmask, double* __restrict__ y,
+                   unsigned long long* m)
+{
+  GB_PDL_ENTRY();
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (r < n) {
+    if (__ldg(dirmask + r))
+      y[r] = 0.0;
+    else
+      v = fabs(y[r]);
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v > 0.0)
+    atomicMax(m, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
 } // namespace gb

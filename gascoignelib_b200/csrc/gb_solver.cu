@@ -394,6 +394,9 @@ struct Level
   int mesh_dim = 0;
   int64_t mesh_ncells = 0, mesh_n = -1;
   DeviceArray<int> m_cells, m_cptr, m_clist, m_diagpos, m_child_ptr, m_child;
+  DeviceArray<int> m_nptr, m_nlist; // per node its (cell, local index) pairs
+  double m_beta[3] = { 0.0, 0.0, 0.0 }; // convection of the last assembly
+  bool m_assembled = false;
   DeviceArray<double> m_coords, m_kappa, m_dd;
   std::vector<int64_t> h_parent;
   int64_t child_n = -1; // coarse cells the child lists were built for
@@ -539,6 +542,7 @@ struct gb_ctx
   int mid_grid[2] = { 0, 0 }; // per precision (FP64, FP32)
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
   gb::DeviceArray<double> asm_E; // element matrices of the level being assembled
+  gb::DeviceArray<unsigned long long> nrm; // largest |y| of gb_newton_residual
   // matrix values changed on the device since the solver's set-up (dense
   // coarse maps, direct inverse): refreshed in place at the next solve
   bool values_dirty = false;
@@ -2922,6 +2926,10 @@ assemble_level(Context& c, int l, const double* beta)
   const double b2 = beta && dim == 3 ? beta[2] : 0.0;
   const double g = 0.5 / std::sqrt(3.0);
   const bool conv = b0 != 0.0 || b1 != 0.0 || b2 != 0.0;
+  L.m_beta[0] = b0;
+  L.m_beta[1] = b1;
+  L.m_beta[2] = b2;
+  L.m_assembled = true;
 #define GB_ELEM(D, CV)                                                                   \
   launch(c, k_q1_element<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,  \
          (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p)
@@ -2986,6 +2994,34 @@ coarsen_kappa(Context& c, int l)
   launch(c, k_kappa_coarsen, blocks_for(C.mesh_ncells, 256), 256, (int)C.mesh_ncells,
          (const int*)C.m_child_ptr.p, (const int*)C.m_child.p, (const double*)F.m_kappa.p,
          C.m_kappa.p);
+}
+
+// y += d * Form(x) on level l with the coefficient and convection of its
+// last assembly (StdSolver::Form without hanging nodes: the element residuals
+// summed per node in ascending cell order)
+static void
+form_level(Context& c, int l, double* y, const double* x, double d)
+{
+  Level& L = c.L[l];
+  GB_REQUIRE(L.m_assembled, GB_ESTATE, "Form needs an assembled level (gb_assemble)");
+  const int dim = L.mesh_dim, nl = 1 << dim;
+  const int nc = static_cast<int>(L.mesh_ncells);
+  GB_CUDA(c.asm_E.n >= size_t(nc) * nl ? cudaSuccess : c.asm_E.alloc(size_t(nc) * nl));
+  const double b0 = L.m_beta[0], b1 = L.m_beta[1], b2 = L.m_beta[2];
+  const bool conv = b0 != 0.0 || b1 != 0.0 || b2 != 0.0;
+  const double g = 0.5 / std::sqrt(3.0);
+#define GB_FORM(D, CV)                                                                 \
+  launch(c, k_q1_form<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,   \
+         (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, x,     \
+         c.asm_E.p)
+  if (dim == 2) {
+    if (conv) GB_FORM(2, true); else GB_FORM(2, false);
+  } else {
+    if (conv) GB_FORM(3, true); else GB_FORM(3, false);
+  }
+#undef GB_FORM
+  launch(c, k_form_gather, blocks_for(L.n, 256), 256, (int)L.n, (const int*)L.m_nptr.p,
+         (const int*)L.m_nlist.p, (const double*)c.asm_E.p, d, y);
 }
 
 static void
@@ -4174,6 +4210,18 @@ gb_level_set_mesh(gb_ctx* ctx, int lvl, int dim, int64_t ncells, const int64_t* 
   std::vector<int> dpos(n);
   for (int64_t r = 0; r < n; ++r)
     dpos[r] = static_cast<int>(sell_pos(r, L.h_diag[r]));
+  std::vector<int> nptr(n + 1, 0), nlist(size_t(ncells) * nl);
+  for (int64_t c = 0; c < ncells; ++c)
+    for (int a = 0; a < nl; ++a)
+      nptr[cell_nodes[c * nl + a] + 1]++;
+  for (int64_t r = 0; r < n; ++r)
+    nptr[r + 1] += nptr[r];
+  {
+    std::vector<int> fill(nptr.begin(), nptr.end() - 1);
+    for (int64_t c = 0; c < ncells; ++c) // ascending cells
+      for (int a = 0; a < nl; ++a)
+        nlist[fill[cell_nodes[c * nl + a]]++] = static_cast<int>(int64_t(a) * ncells + c);
+  }
   std::vector<int64_t> par;
   if (lvl > 0) {
     par.assign(parent, parent + ncells);
@@ -4192,6 +4240,11 @@ gb_level_set_mesh(gb_ctx* ctx, int lvl, int dim, int64_t ncells, const int64_t* 
   GB_CUDA(h2d(ctx->stream, L.m_cptr.p, cptr.data(), cptr.size() * sizeof(int)));
   GB_CUDA(h2d(ctx->stream, L.m_clist.p, clist.data(), clist.size() * sizeof(int)));
   GB_CUDA(h2d(ctx->stream, L.m_diagpos.p, dpos.data(), n * sizeof(int)));
+  GB_CUDA(L.m_nptr.alloc(nptr.size()));
+  GB_CUDA(L.m_nlist.alloc(nlist.size()));
+  GB_CUDA(h2d(ctx->stream, L.m_nptr.p, nptr.data(), nptr.size() * sizeof(int)));
+  GB_CUDA(h2d(ctx->stream, L.m_nlist.p, nlist.data(), nlist.size() * sizeof(int)));
+  L.m_assembled = false;
   L.h_parent.swap(par);
   L.mesh_dim = dim;
   L.mesh_ncells = ncells;
@@ -4243,6 +4296,119 @@ gb_level_get_values(gb_ctx* ctx, int lvl, double* val)
   GB_REQUIRE(val, GB_EINVAL, "null array");
   host_values(*ctx, L);
   std::memcpy(val, L.h_val.data(), L.h_val.size() * sizeof(double));
+  GB_API_END
+}
+
+int
+gb_form(gb_ctx* ctx, int lvl, int y, int x, double d)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  check_mesh(L);
+  GB_REQUIRE(y != x, GB_EINVAL, "y and x must differ");
+  form_level(*ctx, lvl, vec(*ctx, lvl, y), vec(*ctx, lvl, x), d);
+  GB_API_END
+}
+
+int
+gb_newton_residual(gb_ctx* ctx, int y, int x, int b, double* norm)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(ctx->nlevels >= 1, GB_ESTATE, "no levels");
+  const int fl = ctx->nlevels - 1;
+  Level& L = level_with_matrix(*ctx, fl);
+  check_mesh(L);
+  GB_REQUIRE(y != x && y != b, GB_EINVAL, "y must differ from x and b");
+  GB_REQUIRE(!L.pf_mask, GB_EINVAL, "Newton residual with a pressure filter");
+  double* yv = vec(*ctx, fl, y);
+  launch(*ctx, k_equ<double, double>, stream_blocks(L.n), 256, (int64_t)L.n, yv, 1.0,
+         (const double*)vec(*ctx, fl, b));
+  form_level(*ctx, fl, yv, vec(*ctx, fl, x), -1.0);
+  GB_CUDA(ctx->nrm.alloc(1));
+  GB_CUDA(cudaMemsetAsync(ctx->nrm.p, 0, sizeof(unsigned long long), ctx->stream));
+  launch(*ctx, k_dirichlet_absmax, blocks_for(L.n, 256), 256, (int)L.n,
+         (const uint8_t*)L.dirmask.p, yv, ctx->nrm.p);
+  if (norm) {
+    unsigned long long m = 0;
+    GB_CUDA(cudaMemcpyAsync(&m, ctx->nrm.p, sizeof(m), cudaMemcpyDeviceToHost, ctx->stream));
+    GB_CUDA(cudaStreamSynchronize(ctx->stream));
+    double v;
+    std::memcpy(&v, &m, sizeof(v));
+    *norm = v;
+  }
+  GB_API_END
+}
+
+int
+gb_vec_write_backup(gb_ctx* ctx, int lvl, int id, const char* path, int binary)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(path, GB_EINVAL, "null path");
+  std::vector<double> v(L.ndof());
+  GB_CUDA(cudaMemcpyAsync(v.data(), vec(*ctx, lvl, id), v.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  FILE* f = std::fopen(path, binary ? "wb" : "w");
+  GB_REQUIRE(f, GB_EINVAL, std::string("cannot open ") + path + " for writing");
+  bool ok = true;
+  if (binary) { // CompVector::BinWrite + "BackUpEnd"
+    ok = std::fprintf(f, "%d %lld\n[", L.B, (long long)L.n) > 0 &&
+         std::fwrite(v.data(), sizeof(double), v.size(), f) == v.size() &&
+         std::fprintf(f, "]BackUpEnd\n") > 0;
+  } else { // WriteBackUp: scientific, 16 digits, one node per line
+    ok = std::fprintf(f, "%lld %d\n", (long long)L.n, L.B) > 0;
+    for (int64_t i = 0; i < L.n && ok; ++i) {
+      for (int c = 0; c < L.B && ok; ++c)
+        ok = std::fprintf(f, "%.16e ", v[i * L.B + c]) > 0;
+      ok = ok && std::fputc('\n', f) != EOF;
+    }
+    ok = ok && std::fprintf(f, "BackUpEnd\n") > 0;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  GB_REQUIRE(ok, GB_EINVAL, std::string("write error on ") + path);
+  GB_API_END
+}
+
+int
+gb_vec_read_backup(gb_ctx* ctx, int lvl, int id, const char* path, int binary, int add)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(path, GB_EINVAL, "null path");
+  FILE* f = std::fopen(path, binary ? "rb" : "r");
+  GB_REQUIRE(f, GB_EINVAL, std::string("backup file ") + path + " not found");
+  std::vector<double> v(L.ndof());
+  long long n = -1;
+  int comp = -1;
+  bool ok;
+  char tail[16] = { 0 };
+  if (binary) { // "ncomp n\n[" raw values "]" then "BackUpEnd"
+    char br = 0;
+    ok = std::fscanf(f, "%d %lld %c", &comp, &n, &br) == 3 && br == '[' && n == L.n &&
+         comp == L.B && std::fread(v.data(), sizeof(double), v.size(), f) == v.size() &&
+         std::fscanf(f, " %c", &br) == 1 && br == ']';
+  } else { // "n ncomp", n * ncomp numbers, "BackUpEnd"
+    ok = std::fscanf(f, "%lld %d", &n, &comp) == 2 && n == L.n && comp == L.B;
+    for (size_t k = 0; k < v.size() && ok; ++k)
+      ok = std::fscanf(f, "%lf", &v[k]) == 1;
+  }
+  ok = ok && std::fscanf(f, " %15s", tail) == 1 && std::string(tail) == "BackUpEnd";
+  std::fclose(f);
+  GB_REQUIRE(ok, GB_EINVAL,
+             std::string("backup file ") + path + " does not hold " +
+               std::to_string(L.n) + " nodes of " + std::to_string(L.B) +
+               " components ending in BackUpEnd");
+  double* dst = vec(*ctx, lvl, id);
+  if (add) { // ReadBackUp adds the file to the vector
+    std::vector<double> cur(v.size());
+    GB_CUDA(cudaMemcpyAsync(cur.data(), dst, v.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    GB_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t k = 0; k < v.size(); ++k)
+      v[k] = cur[k] + v[k];
+  }
+  GB_CUDA(h2d(ctx->stream, dst, v.data(), v.size() * sizeof(double)));
   GB_API_END
 }
 

@@ -111,6 +111,10 @@ _SIGS = {
     "gb_assemble_levels": [C.c_void_p, C.c_void_p, C.c_int, _PD],
     "gb_level_get_kappa": [C.c_void_p, C.c_int, _PD],
     "gb_level_get_values": [C.c_void_p, C.c_int, _PD],
+    "gb_form": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double],
+    "gb_newton_residual": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD],
+    "gb_vec_write_backup": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_int],
+    "gb_vec_read_backup": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_int],
     "gb_ctx_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
@@ -304,6 +308,23 @@ class Context:
         self._chk(self._L.gb_assemble_levels(self.h, p, where,
                                              _pd(b) if b is not None else None))
         del keep
+
+    def form(self, level, y, x, d=1.0):
+        """gb_form: y += d * Form(x) on the level (its last assembled equation)."""
+        self._chk(self._L.gb_form(self.h, level, y, x, d))
+
+    def newton_residual(self, y, x, b):
+        """gb_newton_residual on the finest level; returns max |y|."""
+        nr = C.c_double()
+        self._chk(self._L.gb_newton_residual(self.h, y, x, b, C.byref(nr)))
+        return nr.value
+
+    def write_backup(self, level, vid, path, binary=False):
+        self._chk(self._L.gb_vec_write_backup(self.h, level, vid, path.encode(), int(binary)))
+
+    def read_backup(self, level, vid, path, binary=False, add=False):
+        self._chk(self._L.gb_vec_read_backup(self.h, level, vid, path.encode(), int(binary),
+                                             int(add)))
 
     def level_values(self, level, nvals):
         v = np.zeros(nvals)

@@ -341,6 +341,28 @@ int gb_level_get_kappa(gb_ctx* ctx, int level, double* kappa);
  * or those of the last device assembly; blocks row-major as NodeMatrix stores
  * them (LinAlg/nodematrix.h:44-48). */
 int gb_level_get_values(gb_ctx* ctx, int level, double* val);
+/* StdSolver::Form (Solver/stdsolver.cc:1041-1063 -> CGDisc::Form,
+ * DofHandler/cgdisc.h:415-450) of the equation last assembled on the level
+ * (gb_assemble: its kappa and beta): y += d * sum over cells of the element
+ * residuals of x, summed per node in ascending cell order (matrix-free, no
+ * hanging nodes). Vectors are level vector ids. */
+int gb_form(gb_ctx* ctx, int level, int y, int x, double d);
+/* StdMultiLevelSolver::NewtonResidual (Solver/stdmultilevelsolver.cc:609-623)
+ * on the finest level: y = b - Form(x), zero on the Dirichlet dofs; *norm (may
+ * be NULL) = NewtonNorm(y) = max |y_i| (StdSolver::NewtonNorm,
+ * Solver/stdsolver.cc:693-696). No pressure filter. */
+int gb_newton_residual(gb_ctx* ctx, int y, int x, int b, double* norm);
+/* Solution files of Common/backup.cc. binary = 0: WriteBackUp's text format
+ * (".bup": "n ncomp", then per node the ncomp values as %.16e, then
+ * "BackUpEnd"); binary = 1: WriteBackUpBinary's (".bip": "ncomp n", "[", the
+ * raw doubles, "]", "BackUpEnd"). path is the whole file name (the reference
+ * appends the suffix to its base name). The file must hold the level's node
+ * count and block size. Reading with add = 1 adds the file's values to the
+ * vector (ReadBackUp), add = 0 replaces them (ReadBackUpResize on a vector of
+ * the right size, ReadBackUpBinary). */
+int gb_vec_write_backup(gb_ctx* ctx, int level, int id, const char* path, int binary);
+int gb_vec_read_backup(gb_ctx* ctx, int level, int id, const char* path, int binary,
+                       int add);
 /* The context's CUDA stream (a cudaStream_t): every gb_* call enqueues its
  * work there, so callers can order their own work or record events on it. */
 int gb_ctx_get_stream(const gb_ctx* ctx, void** stream);

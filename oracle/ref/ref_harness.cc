@@ -53,6 +53,10 @@
 // and with dualrhs= (a nodal vector like rhs): dual_summary.txt,
 //   dual_rhs.f64 dual_solution.f64, and with dump=1 L<l>_dualval.f64 (the
 //   dual matrices' values in the stencil of L<l>_col.i64)
+// backup=1: solution.bup and solution.bip (WriteBackUp, WriteBackUpBinary);
+// formx=<raw f64 finest-level vector x>: form.f64 = Form(0, x, 1),
+//   newton_residual.f64 = NewtonResidual(x, rhs) and newton.txt (its norm).
+#include "backup.h"
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -102,6 +106,8 @@ struct Config
   std::string disc = "Q1";
   double ball = 0.0, diff = -1.0;
   int rhsres = 0;
+  int backup = 0;     // write the solution with WriteBackUp / WriteBackUpBinary
+  std::string formx;  // Form and NewtonResidual of this finest-level vector
 };
 
 // kappa per cell, one array per resolution N = coarse * 2^l (cells per dim),
@@ -299,6 +305,8 @@ parse(int argc, char** argv)
     else if (k == "ndirect") c.ndirect = atoi(v.c_str());
     else if (k == "mgtype") c.mgtype = v;
     else if (k == "dump") c.dump = atoi(v.c_str());
+    else if (k == "backup") c.backup = atoi(v.c_str());
+    else if (k == "formx") c.formx = v;
     else if (k == "repeat") c.repeat = atoi(v.c_str());
     else if (k == "patchdepth") c.patchdepth = atoi(v.c_str());
     else if (k == "problem") c.problem = v;
@@ -791,6 +799,33 @@ main(int argc, char** argv)
     const GlobalVector& U = S->GetGV(u);
     std::vector<double> sol(U.begin(), U.end());
     write_raw(c.out + "/solution.f64", sol);
+    // Common/backup.cc: the text (.bup) and binary (.bip) solution files
+    if (c.backup) {
+      WriteBackUp(U, c.out + "/solution");
+      WriteBackUpBinary(U, c.out + "/solution");
+    }
+    // StdSolver::Form (Solver/stdsolver.cc:1041-1063) of a given vector with
+    // d = 1 on the finest level, and StdMultiLevelSolver::NewtonResidual
+    // (Solver/stdmultilevelsolver.cc:609-623) y = f - Form(x), boundary zero,
+    // with its norm
+    if (!c.formx.empty()) {
+      Vector x("fx"), y("fy");
+      MLS.ReInitVector(x);
+      MLS.ReInitVector(y);
+      GlobalVector& X = S->GetGV(x);
+      std::vector<double> xv = read_f64(c.formx, X.size());
+      std::copy(xv.begin(), xv.end(), X.begin());
+      S->Zero(y);
+      S->Form(y, x, 1.);
+      const GlobalVector& Y = S->GetGV(y);
+      write_raw(c.out + "/form.f64", std::vector<double>(Y.begin(), Y.end()));
+      std::copy(xv.begin(), xv.end(), X.begin()); // Form averaged/zeroed hanging values
+      const double nr = MLS.NewtonResidual(y, x, f);
+      write_raw(c.out + "/newton_residual.f64", std::vector<double>(Y.begin(), Y.end()));
+      std::ofstream o(c.out + "/newton.txt");
+      o.precision(17);
+      o << "newton_norm " << nr << "\n";
+    }
   }
   // Dual problem (optional): StdMultiLevelSolver::AssembleDualMatrix
   // (Solver/stdmultilevelsolver.cc:920-926, Solver/stdsolver.cc:1815-1834:

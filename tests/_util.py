@@ -61,6 +61,11 @@ def load_golden(name):
                    dual_residual=float(z["dual_residual"]),
                    dual_status=str(z["dual_status"]),
                    dualval=[z[f"L{l}_dualval"] for l in range(nl)])
+    for k in ("formx", "form", "newton_residual", "backup_bup", "backup_bip"):
+        if k in z.files:
+            ref[k] = z[k]
+    if "newton_norm" in z.files:
+        ref["newton_norm"] = float(z["newton_norm"])
     return P, ref
 
 
@@ -176,3 +181,17 @@ def golden_assembly_cases():
                 else None)
         out.append((name, kap, beta))
     return out
+
+
+def golden_form_cases():
+    return [n for n in golden_cases() if n.startswith("form_")]
+
+
+def golden_kappa_beta(name):
+    """Finest kappa and beta of a seeded golden case."""
+    from gascoignelib_b200.problem import seeded_inputs
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    dim, coarse, refine = int(z["key_dim"]), int(z["key_coarse"]), int(z["key_refine"])
+    beta = ([float(t) for t in str(z["key_conv"]).split(",")] if "key_conv" in z.files
+            else None)
+    return seeded_inputs(dim, coarse, refine)[0], beta

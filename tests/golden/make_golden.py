@@ -13,7 +13,10 @@ matrices) with the pressure filter and the Vanka or block-Jacobi smoother; the
 harness runs them on one OpenMP thread, so Vanka's patch contributions are
 summed in patch order. The "hn_" cases refine a ball once more (hanging
 nodes, Q1 or Q2 elements) and also record the reference's HNAverage,
-HNDistribute and HNZero of a test vector on the finest level.
+HNDistribute and HNZero of a test vector on the finest level. The "form_"
+cases also record StdSolver::Form and StdMultiLevelSolver::NewtonResidual of a
+seeded vector and the solution as written by WriteBackUp (.bup) and
+WriteBackUpBinary (.bip).
 
     python tests/golden/make_golden.py
 """
@@ -49,6 +52,9 @@ CASES = {
     "stokes_3d_c1_r3_vanka": (3, 1, 3, True, 1e-8,
                               {"problem": "stokes", "smoother": "vanka", "omega": 1.0,
                                "gmressize": 31}),
+    "form_3d_c1_r3_conv": (3, 1, 3, True, 1e-8, {"conv": "1,0.5,0.25", "backup": 1,
+                                                 "formx": 1005}),
+    "form_2d_c2_r3": (2, 2, 3, True, 1e-10, {"backup": 1, "formx": 1006}),
     "hn_2d_q1_c2_r3_ball": (2, 2, 3, True, 1e-10,
                             {"disc": "Q1", "ball": 0.25, "diff": 1.0}),
     "hn_2d_q2_c2_r3_conv_ball": (2, 2, 3, True, 1e-10,
@@ -113,6 +119,12 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
     keys = dict(dim=dim, coarse=coarse, refine=refine, dump=1, tol=tol,
                 gmressize=21, iterpre=2, iterpost=2, iterexact=10, omega=0.8)
     keys.update(extra)
+    formx = None
+    if "formx" in keys:  # a seeded vector on the finest nodes (any numbering)
+        n1 = (coarse << refine) + 1
+        formx = np.random.default_rng(keys["formx"]).uniform(-1.0, 1.0, size=n1 ** dim)
+        keys["formx"] = os.path.join(d, "formx.f64")
+        formx.tofile(keys["formx"])
     dual = name.endswith("_dual")
     if dual:
         out0, _ = run_reference(d, **keys, **kw)
@@ -131,7 +143,18 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
             "status": summ["status"][0] if len(summ["status"]) == 1
             else " ".join(summ["status"])}
     for k, v in keys.items():
-        arrs["key_" + k] = v
+        if k != "formx":
+            arrs["key_" + k] = v
+    if formx is not None:
+        arrs["formx"] = formx
+        arrs["form"] = np.fromfile(os.path.join(out, "form.f64"))
+        arrs["newton_residual"] = np.fromfile(os.path.join(out, "newton_residual.f64"))
+        with open(os.path.join(out, "newton.txt")) as f:
+            arrs["newton_norm"] = float(f.read().split()[1])
+    if keys.get("backup"):
+        for ext in ("bup", "bip"):
+            with open(os.path.join(out, "solution." + ext), "rb") as f:
+                arrs["backup_" + ext] = np.frombuffer(f.read(), dtype=np.uint8)
     if dual:
         ds = {}
         with open(os.path.join(out, "dual_summary.txt")) as f:

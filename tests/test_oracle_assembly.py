@@ -43,3 +43,40 @@ def test_oracle_assembly_matches_generator():
     vals, _ = oracle_level_values(P, kappa, (1.0, -0.5, 0.25))
     for L, v in zip(P.levels, vals):
         assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max()
+
+
+@pytest.mark.parametrize("name", __import__("_util").golden_form_cases())
+def test_oracle_form_and_newton_residual_match_reference(name):
+    """StdSolver::Form and StdMultiLevelSolver::NewtonResidual of a seeded
+    vector, restated as the sum of the element matrices applied per cell."""
+    from _util import golden_kappa_beta, uniform_meshes
+    P, ref = load_golden(name)
+    kappa, beta = golden_kappa_beta(name)
+    L = P.finest
+    cells = uniform_meshes(P)[-1][0]
+    E = q1_element_matrices(P.dim, L.coord[cells], kappa, beta)
+    x = ref["formx"]
+    F = np.zeros(L.n)
+    for c in range(cells.shape[0]):
+        F[cells[c]] += E[c] @ x[cells[c]]
+    assert np.abs(F - ref["form"]).max() <= 1e-13 * np.abs(ref["form"]).max()
+    y = P.rhs - F
+    y[L.dirichlet] = 0.0
+    assert np.abs(y - ref["newton_residual"]).max() <= 1e-13 * np.abs(y).max()
+    assert abs(np.abs(y).max() - ref["newton_norm"]) <= 1e-13 * ref["newton_norm"]
+
+
+@pytest.mark.parametrize("name", __import__("_util").golden_form_cases())
+def test_backup_formats_match_reference_files(name):
+    """WriteBackUp / WriteBackUpBinary layouts restated in numpy reproduce the
+    reference's files byte for byte (the library's writer is checked against
+    the same bytes on the GPU)."""
+    P, ref = load_golden(name)
+    u = ref["solution"]
+    B = P.finest.B
+    txt = f"{P.finest.n} {B}\n" + "".join(
+        "".join(f"{u[i * B + c]:.16e} " for c in range(B)) + "\n" for i in range(P.finest.n))
+    txt += "BackUpEnd\n"
+    assert txt.encode() == ref["backup_bup"].tobytes()
+    bip = f"{B} {P.finest.n}\n[".encode() + u.astype("<f8").tobytes() + b"]BackUpEnd\n"
+    assert bip == ref["backup_bip"].tobytes()
