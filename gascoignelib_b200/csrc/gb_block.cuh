@@ -550,4 +550,122 @@ k_hn_zero(int nh, int B, const int* __restrict__ node, T* __restrict__ u)
     u[int64_t(node[k]) * B + c] = T(0);
 }
 
+// --------------------------------------------------------- block ILU
+
+template<class T>
+__device__ __forceinline__ T ilu_mul(T a, T b);
+template<>
+__device__ __forceinline__ double ilu_mul(double a, double b) { return __dmul_rn(a, b); }
+template<>
+__device__ __forceinline__ float ilu_mul(float a, float b) { return __fmul_rn(a, b); }
+template<class T>
+__device__ __forceinline__ T ilu_sub(T a, T b);
+template<>
+__device__ __forceinline__ double ilu_sub(double a, double b) { return __dsub_rn(a, b); }
+template<>
+__device__ __forceinline__ float ilu_sub(float a, float b) { return __fsub_rn(a, b); }
+template<class T>
+__device__ __forceinline__ T ilu_add(T a, T b);
+template<>
+__device__ __forceinline__ double ilu_add(double a, double b) { return __dadd_rn(a, b); }
+template<>
+__device__ __forceinline__ float ilu_add(float a, float b) { return __fadd_rn(a, b); }
+
+// One level of the forward substitution with the unit lower factor
+// (SparseBlockIlu::forward, LinAlg/sparseblockilu.xx:202-214): for each row of
+// the level, y_i -= L_ik y_k over its lower blocks in stored (ascending column)
+// order, block entries as FMatrixBlock::subtract (LinAlg/fmatrixblock.h:
+// 136-145). The rows of one level depend only on rows of earlier levels
+// (earlier launches), so the result equals the sequential sweep bit for bit.
+template<int B, class T>
+__global__ void
+k_ilu_lower(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
+            const int* __restrict__ col, const int* __restrict__ diag,
+            const T* __restrict__ val, T* __restrict__ y)
+{
+  GB_PDL_ENTRY();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nr)
+    return;
+  const int i = __ldg(rows + t);
+  T yi[B];
+#pragma unroll
+  for (int r = 0; r < B; ++r)
+    yi[r] = y[int64_t(i) * B + r];
+  const int e = __ldg(diag + i);
+  for (int pos = __ldg(ptr + i); pos < e; ++pos) {
+    const int64_t k = __ldg(col + pos);
+    const T* m = val + int64_t(pos) * B * B;
+    T yk[B];
+#pragma unroll
+    for (int c = 0; c < B; ++c)
+      yk[c] = y[k * B + c];
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+#pragma unroll
+      for (int c = 0; c < B; ++c)
+        yi[r] = ilu_sub(yi[r], ilu_mul(__ldg(m + r * B + c), yk[c]));
+  }
+#pragma unroll
+  for (int r = 0; r < B; ++r)
+    y[int64_t(i) * B + r] = yi[r];
+}
+
+// One level of the backward substitution (SparseBlockIlu::backward,
+// LinAlg/sparseblockilu.xx:217-231): y_i -= U_ik y_k over the upper blocks in
+// descending order, then y_i = D_i^-1 y_i with the inverted diagonal block
+// (FMatrixBlock::vmult, LinAlg/fmatrixblock.h:194-217).
+template<int B, class T>
+__global__ void
+k_ilu_upper(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
+            const int* __restrict__ col, const int* __restrict__ diag,
+            const T* __restrict__ val, T* __restrict__ y)
+{
+  GB_PDL_ENTRY();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nr)
+    return;
+  const int i = __ldg(rows + t);
+  T yi[B];
+#pragma unroll
+  for (int r = 0; r < B; ++r)
+    yi[r] = y[int64_t(i) * B + r];
+  const int d = __ldg(diag + i);
+  for (int pos = __ldg(ptr + i + 1) - 1; pos > d; --pos) {
+    const int64_t k = __ldg(col + pos);
+    const T* m = val + int64_t(pos) * B * B;
+    T yk[B];
+#pragma unroll
+    for (int c = 0; c < B; ++c)
+      yk[c] = y[k * B + c];
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+#pragma unroll
+      for (int c = 0; c < B; ++c)
+        yi[r] = ilu_sub(yi[r], ilu_mul(__ldg(m + r * B + c), yk[c]));
+  }
+  const T* D = val + int64_t(d) * B * B;
+#pragma unroll
+  for (int r = 0; r < B; ++r) {
+    T acc = ilu_mul(__ldg(D + r * B), yi[0]);
+#pragma unroll
+    for (int c = 1; c < B; ++c)
+      acc = ilu_add(acc, ilu_mul(__ldg(D + r * B + c), yi[c]));
+    y[int64_t(i) * B + r] = acc;
+  }
+}
+
+// u = (u_zero ? 0 : u) + omega h (StdSolver::Add after the ILU solve, unfused)
+template<class T>
+__global__ void
+k_ilu_axpy(int64_t n, T* __restrict__ u, double omega, const T* __restrict__ h, int u_zero)
+{
+  GB_PDL_ENTRY();
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n)
+    return;
+  const T w = ilu_mul(static_cast<T>(omega), h[i]);
+  u[i] = u_zero ? w : ilu_add(u[i], w);
+}
+
 } // namespace gb

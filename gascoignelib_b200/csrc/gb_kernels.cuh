@@ -523,20 +523,45 @@ k_mgs(int64_t n, double* __restrict__ vv, const double* __restrict__ vi,
 
 // Block-diagonal inverse by NodeMatrix::gauss_jordan (LinAlg/nodematrix.h:
 // 159-213), same pivot order; one thread per node, the block in registers.
-template<int B>
-__global__ void
-k_blockdiag_inverse(int n, const double* __restrict__ dblocks, double* __restrict__ dinv64,
-                    float* __restrict__ dinv32)
+// Unfused double multiply and subtract on the device (__dmul_rn / __dsub_rn,
+// never contracted into an FMA) and plain ones on the host, whose compiler
+// targets no FMA: the same roundings on both sides.
+__host__ __device__ __forceinline__ double
+rn_mul(double a, double b)
 {
-  GB_PDL_ENTRY();
-  int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node >= n)
-    return;
-  double a[B * B];
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ double
+rn_sub(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+  return __dsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
+__host__ __device__ __forceinline__ double
+rn_add(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+
+// In-place inverse of a row-major B x B block by NodeMatrix::gauss_jordan
+// (LinAlg/nodematrix.h:159-213): same pivot order and roundings; on the host
+// for the ILU factorisation, on the device for the block-diagonal inverse.
+template<int B>
+__host__ __device__ inline void
+gauss_jordan(double* a)
+{
   int p[B];
-#pragma unroll
-  for (int q = 0; q < B * B; ++q)
-    a[q] = dblocks[(int64_t)node * B * B + q];
 #define A_(i, j) a[(i) * B + (j)]
   for (int i = 0; i < B; i++)
     p[i] = i;
@@ -568,7 +593,7 @@ k_blockdiag_inverse(int n, const double* __restrict__ dblocks, double* __restric
           continue;
         // (a_ij * a_jk) * hr, then the subtraction: no contraction, so the
         // rounding is the reference's
-        A_(i, k) = __dsub_rn(A_(i, k), __dmul_rn(__dmul_rn(A_(i, j), A_(j, k)), hr));
+        A_(i, k) = rn_sub(A_(i, k), rn_mul(rn_mul(A_(i, j), A_(j, k)), hr));
       }
     }
     for (int i = 0; i < B; i++) {
@@ -585,6 +610,22 @@ k_blockdiag_inverse(int n, const double* __restrict__ dblocks, double* __restric
       A_(i, k) = hv[k];
   }
 #undef A_
+}
+
+template<int B>
+__global__ void
+k_blockdiag_inverse(int n, const double* __restrict__ dblocks, double* __restrict__ dinv64,
+                    float* __restrict__ dinv32)
+{
+  GB_PDL_ENTRY();
+  int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= n)
+    return;
+  double a[B * B];
+#pragma unroll
+  for (int q = 0; q < B * B; ++q)
+    a[q] = dblocks[(int64_t)node * B * B + q];
+  gauss_jordan<B>(a);
 #pragma unroll
   for (int q = 0; q < B * B; ++q) {
     dinv64[(int64_t)node * B * B + q] = a[q];

@@ -400,6 +400,14 @@ struct Level
   DeviceArray<double> m_coords, m_kappa, m_dd;
   std::vector<int64_t> h_parent;
   int64_t child_n = -1; // coarse cells the child lists were built for
+  // block ILU (smoother 2, SparseBlockIlu): the factors in the matrix's row
+  // order with ascending columns, the diagonal blocks inverted, and the rows
+  // grouped in dependency levels for the two substitutions
+  bool ilu_ready = false;
+  DeviceArray<int> ilu_ptr, ilu_col, ilu_diag, ilu_lrows, ilu_urows;
+  DeviceArray<double> ilu_v64;
+  DeviceArray<float> ilu_v32;
+  std::vector<int> ilu_lptr, ilu_uptr; // level offsets into ilu_lrows / ilu_urows
   // values assembled on the device since the host copy was made
   bool h_val_stale = false;
   // per A^T SELL entry the A SELL entry it copies (-1: padding), block size 1:
@@ -1147,6 +1155,140 @@ ensure_direct(Context& c)
   c.dir_ready[t] = true;
 }
 
+// SparseBlockIlu on the host (ConstructStructure with the identity order,
+// copy_entries, compute_ilu: LinAlg/sparseblockilu.xx:72-135, 140-175,
+// 246-276), the block products in FMatrixBlock's order (operator*=,
+// LinAlg/fmatrixblock.h:174-190; submult, :73-93) and the diagonal blocks by
+// gauss_jordan; then the dependency levels of both triangular solves.
+template<int B>
+static void
+ilu_factor(std::vector<int>& ptr, std::vector<int>& col, std::vector<int>& diag,
+           std::vector<double>& v, int64_t n)
+{
+  constexpr int B2 = B * B;
+  double tmp[B2];
+  for (int64_t i = 0; i < n; ++i) {
+    for (int pk = ptr[i]; pk < diag[i]; ++pk) {
+      const int k = col[pk];
+      double* a = v.data() + size_t(pk) * B2;
+      const double* dk = v.data() + size_t(diag[k]) * B2;
+      for (int q = 0; q < B2; ++q)
+        tmp[q] = a[q];
+      for (int r = 0; r < B; ++r) // a(i,k) *= a(k,k)
+        for (int cc = 0; cc < B; ++cc) {
+          double acc = 0.0;
+          for (int t = 0; t < B; ++t)
+            acc = rn_add(acc, rn_mul(tmp[r * B + t], dk[t * B + cc]));
+          a[r * B + cc] = acc;
+        }
+      for (int pj = diag[k] + 1; pj < ptr[k + 1]; ++pj) {
+        const int j = col[pj];
+        for (int ph = ptr[i]; ph < ptr[i + 1]; ++ph) {
+          if (col[ph] != j)
+            continue;
+          double* h = v.data() + size_t(ph) * B2;
+          const double* cj = v.data() + size_t(pj) * B2;
+          for (int r = 0; r < B; ++r) // a(i,j) -= a(i,k) a(k,j)
+            for (int cc = 0; cc < B; ++cc)
+              for (int t = 0; t < B; ++t)
+                h[r * B + cc] = rn_sub(h[r * B + cc], rn_mul(a[r * B + t], cj[t * B + cc]));
+          break;
+        }
+      }
+    }
+    gauss_jordan<B>(v.data() + size_t(diag[i]) * B2);
+  }
+}
+
+static void
+ensure_ilu(Context& c, Level& L)
+{
+  if (L.ilu_ready)
+    return;
+  host_values(c, L);
+  const int B = L.B, B2 = B * B;
+  const int64_t n = L.n, nnz = L.h_rowptr[n];
+  std::vector<int> ptr(n + 1), col(nnz), diag(n, -1);
+  std::vector<double> v(size_t(nnz) * B2);
+  std::vector<int64_t> idx;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t b = L.h_rowptr[i], e = L.h_rowptr[i + 1];
+    ptr[i] = static_cast<int>(b);
+    idx.resize(e - b);
+    for (int64_t k = b; k < e; ++k)
+      idx[k - b] = k;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int64_t x, int64_t y) { return L.h_col[x] < L.h_col[y]; });
+    for (int64_t q = 0; q < e - b; ++q) {
+      col[b + q] = static_cast<int>(L.h_col[idx[q]]);
+      if (col[b + q] == i)
+        diag[i] = static_cast<int>(b + q);
+      std::memcpy(v.data() + size_t(b + q) * B2, L.h_val.data() + size_t(idx[q]) * B2,
+                  B2 * sizeof(double));
+    }
+    GB_REQUIRE(diag[i] >= 0, GB_EINVAL, "ILU: a row without its diagonal");
+  }
+  ptr[n] = static_cast<int>(nnz);
+  switch (B) {
+    case 1: ilu_factor<1>(ptr, col, diag, v, n); break;
+    case 2: ilu_factor<2>(ptr, col, diag, v, n); break;
+    case 3: ilu_factor<3>(ptr, col, diag, v, n); break;
+    default: ilu_factor<4>(ptr, col, diag, v, n);
+  }
+  // levels: a row waits for the rows it reads (lower part forward, upper part
+  // backward); rows of one level ascending
+  std::vector<int> lev(n, 0);
+  int nl = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    int m = 0;
+    for (int p = ptr[i]; p < diag[i]; ++p)
+      m = std::max(m, lev[col[p]] + 1);
+    lev[i] = m;
+    nl = std::max(nl, m + 1);
+  }
+  auto group = [&](const std::vector<int>& lv, int nlev, std::vector<int>& off,
+                   std::vector<int>& rows) {
+    off.assign(nlev + 1, 0);
+    for (int64_t i = 0; i < n; ++i)
+      off[lv[i] + 1]++;
+    for (int q = 0; q < nlev; ++q)
+      off[q + 1] += off[q];
+    rows.resize(n);
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+      rows[fill[lv[i]]++] = static_cast<int>(i);
+  };
+  std::vector<int> lrows, urows;
+  group(lev, nl, L.ilu_lptr, lrows);
+  int nu = 0;
+  for (int64_t i = n - 1; i >= 0; --i) {
+    int m = 0;
+    for (int p = diag[i] + 1; p < ptr[i + 1]; ++p)
+      m = std::max(m, lev[col[p]] + 1);
+    lev[i] = m;
+    nu = std::max(nu, m + 1);
+  }
+  group(lev, nu, L.ilu_uptr, urows);
+  std::vector<float> v32(v.size());
+  for (size_t q = 0; q < v.size(); ++q)
+    v32[q] = static_cast<float>(v[q]);
+  GB_CUDA(L.ilu_ptr.alloc(ptr.size()));
+  GB_CUDA(L.ilu_col.alloc(std::max<size_t>(col.size(), 1)));
+  GB_CUDA(L.ilu_diag.alloc(n));
+  GB_CUDA(L.ilu_lrows.alloc(n));
+  GB_CUDA(L.ilu_urows.alloc(n));
+  GB_CUDA(L.ilu_v64.alloc(std::max<size_t>(v.size(), 1)));
+  GB_CUDA(L.ilu_v32.alloc(std::max<size_t>(v32.size(), 1)));
+  GB_CUDA(h2d(c.stream, L.ilu_ptr.p, ptr.data(), ptr.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_col.p, col.data(), col.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_diag.p, diag.data(), n * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_lrows.p, lrows.data(), n * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_urows.p, urows.data(), n * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_v64.p, v.data(), v.size() * sizeof(double)));
+  GB_CUDA(h2d(c.stream, L.ilu_v32.p, v32.data(), v32.size() * sizeof(float)));
+  L.ilu_ready = true;
+}
+
 // After a device assembly: the dense maps of the single-CTA coarse programs
 // formed again into their own buffers (the captured solver graphs keep
 // pointing at them), generic dense maps dropped (rebuilt at first use, with
@@ -1216,12 +1358,17 @@ ensure_work(Context& c)
   if (c.transposed)
     for (int l = 0; l < c.nlevels; ++l)
       ensure_AT(c, c.L[l]);
-  GB_REQUIRE(c.params.smoother == 0 || c.params.smoother == 1, GB_EINVAL,
-             "smoother must be 0 (jacobi) or 1 (vanka)");
+  GB_REQUIRE(c.params.smoother >= 0 && c.params.smoother <= 2, GB_EINVAL,
+             "smoother must be 0 (jacobi), 1 (vanka) or 2 (ilu)");
   if (c.params.smoother == 1) {
     GB_REQUIRE(!c.transposed, GB_EINVAL, "Vanka with the transposed operator");
     for (int l = 0; l < c.nlevels; ++l)
       ensure_vanka(c, c.L[l]);
+  }
+  if (c.params.smoother == 2) {
+    GB_REQUIRE(!c.transposed, GB_EINVAL, "ILU with the transposed operator");
+    for (int l = 0; l < c.nlevels; ++l)
+      ensure_ilu(c, c.L[l]);
   }
   for (int l = 0; l < c.nlevels; ++l)
     ensure_pf_scratch(c, c.L[l].n);
@@ -1562,6 +1709,49 @@ struct Emit
     launch(c, k_equ<T, T>, stream_blocks(c.L[l].ndof()), 256, (int64_t)c.L[l].ndof(), dst,
            1.0, src);
   }
+  // h = ILU^-1 h in place (SparseBlockIlu::solve with the identity order: the
+  // level kernels of the forward, then of the backward substitution)
+  void ilu_solve(int l, T* h)
+  {
+    const Level& L = c.L[l];
+    no_rec();
+    const T* val = sizeof(T) == 8 ? reinterpret_cast<const T*>(L.ilu_v64.p)
+                                  : reinterpret_cast<const T*>(L.ilu_v32.p);
+    const int nl = static_cast<int>(L.ilu_lptr.size()) - 1;
+    const int nu = static_cast<int>(L.ilu_uptr.size()) - 1;
+    for (int q = 0; q < nl + nu; ++q) {
+      const bool up = q >= nl;
+      const std::vector<int>& off = up ? L.ilu_uptr : L.ilu_lptr;
+      const int lv = up ? q - nl : q;
+      const int cnt = off[lv + 1] - off[lv];
+      if (cnt == 0)
+        continue;
+      const int* rows = (up ? L.ilu_urows.p : L.ilu_lrows.p) + off[lv];
+#define GB_ILU(BB)                                                                       \
+  if (up)                                                                                \
+    launch(c, k_ilu_upper<BB, T>, blocks_for(cnt, 128), 128, cnt, rows,                 \
+           (const int*)L.ilu_ptr.p, (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p,   \
+           val, h);                                                                      \
+  else                                                                                   \
+    launch(c, k_ilu_lower<BB, T>, blocks_for(cnt, 128), 128, cnt, rows,                 \
+           (const int*)L.ilu_ptr.p, (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p,   \
+           val, h)
+      switch (L.B) {
+        case 1: GB_ILU(1); break;
+        case 2: GB_ILU(2); break;
+        case 3: GB_ILU(3); break;
+        default: GB_ILU(4);
+      }
+#undef GB_ILU
+    }
+  }
+  // u = (u_zero ? 0 : u) + omega h
+  void ilu_axpy(int l, T* u, const T* h, bool u_zero)
+  {
+    no_rec();
+    launch(c, k_ilu_axpy<T>, blocks_for(c.L[l].ndof(), 256), 256, (int64_t)c.L[l].ndof(), u,
+           c.params.omega, h, int(u_zero));
+  }
   void no_rec() const
   {
     if (rec)
@@ -1732,6 +1922,22 @@ smooth(Emit<T>& E, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
   const Level& L = c.L[l];
   const bool fused = fused_smoother(c, L);
   for (int it = 0; it < niter; ++it) {
+    if (c.params.smoother == 2) {
+      // linear_smooth ilu: h = y - A u (filtered), the ILU solve of h in
+      // place, u += omega h, SubtractMean(u) (StdSolver::smooth)
+      if (u_zero)
+        E.copy(l, tmp, b);
+      else
+        E.resid(l, u, tmp, b);
+      if (L.pf_mask)
+        E.pf_sub(l, tmp, false);
+      E.ilu_solve(l, tmp);
+      E.ilu_axpy(l, u, tmp, u_zero);
+      u_zero = false;
+      if (L.pf_mask)
+        E.pf_sub(l, u, true);
+      continue;
+    }
     if (fused) {
       if (u_zero && it + 1 < niter && L.B == 1 && !E.rec && c.jacobi2) {
         // the first two sweeps from u = 0 in one pass (the first iterate is
@@ -2955,7 +3161,8 @@ assemble_level(Context& c, int l, const double* beta)
            L.AT.v32.p);
   else
     L.has_AT = false;
-  if (c.params.smoother != 0 || L.vk_ready) { // Vanka factors: full set-up again
+  L.ilu_ready = false;
+  if (c.params.smoother != 0 || L.vk_ready) { // Vanka / ILU factors: full set-up again
     L.vk_ready = false;
     c.work_ready = false;
     c.version++;
@@ -3198,6 +3405,7 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   build_sell(L.A, n, rowptr, col, val, ctx->stream, B);
   L.has_AT = false;
   L.vk_ready = false;
+  L.ilu_ready = false;
   L.h_val_stale = false;
   L.mesh_ncells = 0; // the mesh maps point into the old pattern
   L.mesh_n = -1;
@@ -3547,9 +3755,14 @@ smooth_api(gb_ctx* ctx, int lvl, int niter, int x, int y, int h, int smoother)
   GB_REQUIRE(niter >= 0, GB_EINVAL, "niter < 0");
   GB_REQUIRE(x != y && x != h && y != h, GB_EINVAL, "x, y, h must differ");
   Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(smoother >= 0 && smoother <= 2, GB_EINVAL, "smoother must be 0, 1 or 2");
   if (smoother == 1) {
     GB_REQUIRE(!ctx->transposed, GB_EINVAL, "Vanka with the transposed operator");
     ensure_vanka(*ctx, L);
+  }
+  if (smoother == 2) {
+    GB_REQUIRE(!ctx->transposed, GB_EINVAL, "ILU with the transposed operator");
+    ensure_ilu(*ctx, L);
   }
   double* xd = vec(*ctx, lvl, x);
   double* hd = vec(*ctx, lvl, h);

@@ -197,7 +197,7 @@ class Context:
         fewer nodes; 0 keeps the iterexact sweeps."""
         if smoother is None:
             smoother = getattr(self, "smoother", "jacobi")
-        sm = {"jacobi": 0, "vanka": 1}.get(smoother, smoother)
+        sm = {"jacobi": 0, "vanka": 1, "ilu": 2}.get(smoother, smoother)
         p = GbParams(iterpre, iterpost, iterexact, omega, mgomega, mgtype.encode()[:1],
                      gmressize, tol, globaltol, maxiter, int(sm), int(ndirect))
         self._chk(self._L.gb_set_params(self.h, C.byref(p)))

@@ -62,7 +62,9 @@ typedef struct gb_params
   double globaltol;  /* linear_globaltol (absolute) */
   int maxiter;       /* linear_maxiter */
   int smoother;      /* 0: linear_smooth jacobi (block Jacobi); 1: linear_smooth
-                        ilu with matrixtype vanka (VankaSmoother) */
+                        ilu with matrixtype vanka (VankaSmoother); 2: linear_smooth
+                        ilu with matrixtype block (SparseBlockIlu in the
+                        matrix's own node order) */
   int ndirect;       /* ndirect (Solver/stdsolver.cc:92,218-222,1003-1025): when
                         level 0 has fewer nodes, smooth_exact there is an exact
                         solve (the reference's UMFPACK branch) with the FP64

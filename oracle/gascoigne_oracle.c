@@ -95,6 +95,10 @@ typedef struct
    * nodes, :218-222): dense LU with partial pivoting of level 0 */
   double* dlu;
   int* dperm;
+  /* linear_smooth ilu with matrixtype block (smoother 2): per level the
+   * factors of SparseBlockIlu in the identity order, columns ascending */
+  int64_t **iptr, **icol, **idiag;
+  double** ival;
 } or_mg;
 
 /* ---------------------------------------------------------------- vectors */
@@ -675,6 +679,122 @@ ndof(const or_mg* M, int l)
   return M->L[l].n * M->L[l].B;
 }
 
+/* SparseBlockIlu (LinAlg/sparseblockilu.xx): ConstructStructure with the
+ * identity order (:72-135; columns of each row ascending), copy_entries
+ * (:140-175), compute_ilu (:246-276) with FMatrixBlock's operator*= and
+ * submult (LinAlg/fmatrixblock.h:73-93, 174-190) and gauss_jordan on the
+ * diagonal blocks. */
+static void
+or_ilu_factor(const or_level* A, int64_t** pptr, int64_t** pcol, int64_t** pdiag,
+              double** pval)
+{
+  const int B = A->B, B2 = B * B;
+  const int64_t n = A->n, nnz = A->rowptr[n];
+  int64_t* ptr = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  int64_t* col = (int64_t*)malloc(sizeof(int64_t) * (nnz > 0 ? nnz : 1));
+  int64_t* diag = (int64_t*)malloc(sizeof(int64_t) * n);
+  double* v = (double*)malloc(sizeof(double) * (nnz > 0 ? nnz * B2 : 1));
+  double tmp[OR_MAXB * OR_MAXB];
+  for (int64_t i = 0; i <= n; ++i)
+    ptr[i] = A->rowptr[i];
+  for (int64_t i = 0; i < n; ++i) {
+    /* insertion sort of the row by column (rows are short) */
+    const int64_t b = ptr[i], e = ptr[i + 1];
+    for (int64_t k = b; k < e; ++k) {
+      col[k] = A->col[k];
+      memcpy(v + k * B2, A->val + k * B2, sizeof(double) * B2);
+    }
+    for (int64_t k = b + 1; k < e; ++k) {
+      const int64_t c = col[k];
+      double blk[OR_MAXB * OR_MAXB];
+      memcpy(blk, v + k * B2, sizeof(double) * B2);
+      int64_t q = k - 1;
+      while (q >= b && col[q] > c) {
+        col[q + 1] = col[q];
+        memcpy(v + (q + 1) * B2, v + q * B2, sizeof(double) * B2);
+        --q;
+      }
+      col[q + 1] = c;
+      memcpy(v + (q + 1) * B2, blk, sizeof(double) * B2);
+    }
+    diag[i] = -1;
+    for (int64_t k = b; k < e; ++k)
+      if (col[k] == i)
+        diag[i] = k;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t pk = ptr[i]; pk < diag[i]; ++pk) {
+      const int64_t k = col[pk];
+      double* a = v + pk * B2;
+      const double* dk = v + diag[k] * B2;
+      memcpy(tmp, a, sizeof(double) * B2);
+      for (int r = 0; r < B; ++r)
+        for (int c = 0; c < B; ++c) {
+          double acc = 0.0;
+          for (int t = 0; t < B; ++t)
+            acc += tmp[r * B + t] * dk[t * B + c];
+          a[r * B + c] = acc;
+        }
+      for (int64_t pj = diag[k] + 1; pj < ptr[k + 1]; ++pj) {
+        const int64_t j = col[pj];
+        for (int64_t ph = ptr[i]; ph < ptr[i + 1]; ++ph) {
+          if (col[ph] != j)
+            continue;
+          double* h = v + ph * B2;
+          const double* cj = v + pj * B2;
+          for (int r = 0; r < B; ++r)
+            for (int c = 0; c < B; ++c)
+              for (int t = 0; t < B; ++t)
+                h[r * B + c] -= a[r * B + t] * cj[t * B + c];
+          break;
+        }
+      }
+    }
+    or_gauss_jordan(B, v + diag[i] * B2);
+  }
+  *pptr = ptr;
+  *pcol = col;
+  *pdiag = diag;
+  *pval = v;
+}
+
+/* SparseBlockIlu::solve with the identity order: forward (:202-214), then
+ * backward with the inverted diagonal blocks (:217-231; FMatrixBlock::vmult) */
+static void
+or_ilu_solve(const or_mg* M, int l, double* y)
+{
+  const or_level* A = &M->L[l];
+  const int B = A->B, B2 = B * B;
+  const int64_t n = A->n;
+  const int64_t *ptr = M->iptr[l], *col = M->icol[l], *diag = M->idiag[l];
+  const double* v = M->ival[l];
+  for (int64_t i = 1; i < n; ++i)
+    for (int64_t pos = ptr[i]; pos < diag[i]; ++pos) {
+      const double* m = v + pos * B2;
+      for (int r = 0; r < B; ++r)
+        for (int c = 0; c < B; ++c)
+          y[i * B + r] -= m[r * B + c] * y[col[pos] * B + c];
+    }
+  for (int64_t i = n - 1; i >= 0; --i) {
+    for (int64_t pos = ptr[i + 1] - 1; pos > diag[i]; --pos) {
+      const double* m = v + pos * B2;
+      for (int r = 0; r < B; ++r)
+        for (int c = 0; c < B; ++c)
+          y[i * B + r] -= m[r * B + c] * y[col[pos] * B + c];
+    }
+    double old[OR_MAXB];
+    for (int r = 0; r < B; ++r)
+      old[r] = y[i * B + r];
+    const double* d = v + diag[i] * B2;
+    for (int r = 0; r < B; ++r) {
+      double acc = 0.0;
+      for (int c = 0; c < B; ++c)
+        acc += d[r * B + c] * old[c];
+      y[i * B + r] = acc;
+    }
+  }
+}
+
 or_mg*
 or_mg_create(int nlevels, or_level* L, or_transfer* T, int iterpre,
              int iterpost, int iterexact, double omega, double mgomega,
@@ -719,6 +839,20 @@ or_mg_create(int nlevels, or_level* L, or_transfer* T, int iterpre,
     M->vtmp = (double*)malloc(sizeof(double) * nmax);
     M->vcount = (int*)malloc(sizeof(int) * nmax);
   }
+  if (smoother == 2) {
+    M->iptr = (int64_t**)calloc(nlevels, sizeof(int64_t*));
+    M->icol = (int64_t**)calloc(nlevels, sizeof(int64_t*));
+    M->idiag = (int64_t**)calloc(nlevels, sizeof(int64_t*));
+    M->ival = (double**)calloc(nlevels, sizeof(double*));
+    for (int l = 0; l < nlevels; ++l) {
+      if (L[l].B > OR_MAXB)
+        return NULL;
+      or_ilu_factor(&L[l], &M->iptr[l], &M->icol[l], &M->idiag[l], &M->ival[l]);
+      for (int64_t i = 0; i < L[l].n; ++i)
+        if (M->idiag[l][i] < 0)
+          return NULL;
+    }
+  }
   return M;
 }
 
@@ -735,6 +869,18 @@ or_mg_free(or_mg* M)
   free(M->v);
   free(M->dlu);
   free(M->dperm);
+  if (M->iptr) {
+    for (int l = 0; l < M->nlevels; ++l) {
+      free(M->iptr[l]);
+      free(M->icol[l]);
+      free(M->idiag[l]);
+      free(M->ival[l]);
+    }
+    free(M->iptr);
+    free(M->icol);
+    free(M->idiag);
+    free(M->ival);
+  }
   if (M->vlu) {
     for (int l = 0; l < M->nlevels; ++l) {
       free(M->vlu[l]);
@@ -770,7 +916,9 @@ or_smooth(const or_mg* M, int l, int niter, double* x, const double* y,
   const int64_t n = ndof(M, l);
   for (int it = 0; it < niter; ++it) {
     or_matrix_residual(A, h, x, y);
-    if (M->smoother == 1)
+    if (M->smoother == 2)
+      or_ilu_solve(M, l, h);
+    else if (M->smoother == 1)
       or_vanka_solve(A, M->vlu[l], M->vperm[l], h, M->vtmp, M->vcount);
     else
       or_jacobi(A, h);

@@ -150,7 +150,7 @@ class Oracle:
         self.smoother = smoother
         self.mg = L.or_mg_create(nl, self.levels, self.transfers, iterpre, iterpost,
                                  iterexact, omega, mgomega, mgtype.encode()[:1],
-                                 1 if smoother == "vanka" else 0)
+                                 {"vanka": 1, "ilu": 2}.get(smoother, 0))
         if not self.mg:
             raise ValueError("or_mg_create failed (Vanka needs patches on every level)")
         if ndirect and L.or_mg_set_direct(self.mg, int(ndirect)) != 0:

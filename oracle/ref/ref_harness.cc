@@ -25,7 +25,10 @@
 // Q1/Q1 with Brezzi-Pitkaranta pressure stabilisation, h the cell width),
 // velocity Dirichlet on the whole boundary, the pressure filter on component 0
 // (pfilter=1), and the smoother smoother=vanka (matrixtype vanka, linear_smooth
-// ilu: VankaSmoother, LinAlg/vankasmoother.cc) or smoother=jacobi (block
+// ilu: VankaSmoother, LinAlg/vankasmoother.cc), smoother=ilu (matrixtype block,
+// linear_smooth ilu: SparseBlockIlu in the order of ilusort's default
+// cuthillmckee, which the METIS-free build keeps as the identity) or
+// smoother=jacobi (block
 // Jacobi). The right-hand side file then holds ncomp values per node.
 //
 // disc=Q2 selects CGQ2 (Q2 elements on patches of 2^dim cells); ball=r refines,
@@ -457,7 +460,8 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "iterpre " << c.iterpre << "\n"
     << "iterpost " << c.iterpost << "\n"
     << "iterexact " << c.iterexact << "\n"
-    << "linear_smooth " << (c.smoother == "vanka" ? "ilu" : "jacobi") << "\n"
+    << "linear_smooth " << (c.smoother == "vanka" || c.smoother == "ilu" ? "ilu" : "jacobi")
+    << "\n"
     << "omega " << c.omega << "\n";
   if (c.problem == "stokes" && c.pfilter)
     o << "pfilter 1 0\n";
