@@ -383,6 +383,61 @@ def stokes_c3(local, steps, warmup, flush):
     return out
 
 
+def ilu_c2(local, P, steps, warmup, flush, threads, with_ref):
+    """The C2 solve with the block ILU smoother (linear_smooth ilu, omega 1):
+    mixed and FP64 flexible solves, device time, L2 flushed; and, when asked,
+    the reference's own CPU solve with its SparseBlockIlu on the same problem
+    (the harness's identity ILU order)."""
+    import torch
+
+    from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
+
+    c = Context(local)
+    c.load_problem(P)
+    c.set_params(**dict(PARAMS, smoother="ilu", omega=1.0))
+    l = P.nlevels - 1
+    x, b = c.vec(), c.vec()
+    c.upload(l, b, P.rhs)
+    out = {"workload": "C2 (3D Q1 64^3, log-normal kappa) with linear_smooth ilu, omega 1"}
+    for name, prec in (("mixed", GB_FP32), ("fp64", GB_FP64)):
+        for _ in range(warmup):
+            c.fgmres(x, b, prec, check=False)
+        ms = []
+        for _ in range(steps):
+            flush.random_(0, 255)
+            torch.cuda.synchronize()
+            info = c.fgmres(x, b, prec, check=False)
+            ms.append(info["device_ms"])
+        t = sum(ms) / len(ms)
+        out[name] = {"value": P.finest.ndof / (t * 1e-3), "unit": "DoF/s", "ms_per_step": t,
+                     "iterations": info["iterations"],
+                     "true_rel_residual": info["true_rel_residual"],
+                     "kernel_launches": info["kernel_launches"]}
+    c.close()
+    if with_ref:
+        from oracle.oracle import REF_HARNESS, run_reference, write_inputs
+        if os.path.exists(REF_HARNESS):
+            from gascoignelib_b200.problem import seeded_inputs
+            kappa, rhs = seeded_inputs(DIM, COARSE, REFINE)
+            d = tempfile.mkdtemp(prefix="gb_ilu_")
+            env = os.environ.get("OMP_NUM_THREADS")
+            os.environ["OMP_NUM_THREADS"] = str(threads)
+            try:
+                _, s = run_reference(d, dim=DIM, coarse=COARSE, refine=REFINE, repeat=1,
+                                     tol=1e-8, globaltol=1e-16, gmressize=21, iterpre=2,
+                                     iterpost=2, omega=1.0, smoother="ilu",
+                                     **write_inputs(d, kappa, rhs))
+            finally:
+                if env is None:
+                    os.environ.pop("OMP_NUM_THREADS", None)
+                else:
+                    os.environ["OMP_NUM_THREADS"] = env
+            out["reference_cpu"] = {"solve_s": float(s["solve_s"][0]),
+                                    "iterations": int(s["iterations"][0]),
+                                    "cores": threads}
+    return out
+
+
 def q2_c4(local, steps, warmup, flush):
     """C4: 3D CGQ2 convection-diffusion -0.01 Laplace u + (1, 0.5, 0.25) .
     grad u = f on 80^3 cells (40^3 Q2 patches, 531,441 dofs), refined once more
@@ -564,6 +619,8 @@ def main():
     q2 = None
     if not args.no_q2:
         q2 = q2_c4(local, min(args.steps, 3), 1, flush)
+    ilu = ilu_c2(local, P, min(args.steps, 3), 1, flush, os.cpu_count() or 1,
+                 rank == 0 and not args.no_cpu_baseline)
 
     if rank == 0:
         cb = None
@@ -615,6 +672,7 @@ def main():
             "adjoint_c5": adj,
             "stokes_c3": stk,
             "q2_c4": q2,
+            "ilu_c2": ilu,
         }
         print(json.dumps(line))
     ctx.close()

@@ -30,6 +30,8 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--problem", default="diffusion", choices=["diffusion", "stokes", "q2", "q2ball"],
                     help="stokes: 2D Q1/Q1 Stokes with Vanka on (2*2^(refine-1))^2 cells")
+    ap.add_argument("--smoother", default=None, choices=["jacobi", "vanka", "ilu"],
+                    help="override the problem's smoother (ilu: omega 1)")
     ap.add_argument("--assemble", type=int, default=0,
                     help="only K device assemblies of every level (diffusion problem)")
     ap.add_argument("--ktime", action="store_true",
@@ -57,6 +59,10 @@ def main(argv=None):
     with Context(0) as ctx:
         ctx.load_problem(P)
         keys.setdefault("maxiter", 200)
+        if a.smoother:
+            keys["smoother"] = a.smoother
+            if a.smoother == "ilu":
+                keys["omega"] = 1.0
         ctx.set_params(tol=1e-8, globaltol=1e-300, iterpre=2, iterpost=2, **keys)
         fl = P.nlevels - 1
         if a.assemble:
