@@ -391,7 +391,7 @@ struct Level
   // coordinates, per SELL entry the element-matrix entries summed into it
   // (ascending cells), the diagonal's SELL position per row, this level's
   // cell coefficients, and the parent cell (level - 1) of every cell
-  int mesh_dim = 0;
+  int mesh_dim = 0, mesh_deg = 1;
   int64_t mesh_ncells = 0, mesh_n = -1;
   DeviceArray<int> m_cells, m_cptr, m_clist, m_diagpos, m_child_ptr, m_child;
   DeviceArray<int> m_nptr, m_nlist; // per node its (cell, local index) pairs
@@ -3124,7 +3124,8 @@ static void
 assemble_level(Context& c, int l, const double* beta)
 {
   Level& L = c.L[l];
-  const int dim = L.mesh_dim, nl = 1 << dim;
+  const int dim = L.mesh_dim;
+  const int nl = L.mesh_deg == 1 ? 1 << dim : (dim == 3 ? 27 : 9);
   const int nc = static_cast<int>(L.mesh_ncells);
   GB_CUDA(c.asm_E.n >= size_t(nc) * nl * nl ? cudaSuccess
                                              : c.asm_E.alloc(size_t(nc) * nl * nl));
@@ -3139,12 +3140,23 @@ assemble_level(Context& c, int l, const double* beta)
 #define GB_ELEM(D, CV)                                                                   \
   launch(c, k_q1_element<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,  \
          (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p)
-  if (dim == 2) {
+#define GB_ELEM2(D, CV)                                                                  \
+  launch(c, k_q2_element<D, CV>, blocks_for(int64_t(nc) * nl, 128), 128, nc,            \
+         (const int*)L.m_cells.p, (const double*)L.m_coords.p, (const double*)L.m_kappa.p, \
+         b0, b1, b2, c.asm_E.p)
+  if (L.mesh_deg == 2) {
+    if (dim == 2) {
+      if (conv) GB_ELEM2(2, true); else GB_ELEM2(2, false);
+    } else {
+      if (conv) GB_ELEM2(3, true); else GB_ELEM2(3, false);
+    }
+  } else if (dim == 2) {
     if (conv) GB_ELEM(2, true); else GB_ELEM(2, false);
   } else {
     if (conv) GB_ELEM(3, true); else GB_ELEM(3, false);
   }
 #undef GB_ELEM
+#undef GB_ELEM2
   const Sell& A = L.A;
   launch(c, k_asm_gather, blocks_for(int64_t(A.nslices) * kAsmSplit * kSlice, 256), 256,
          (int)L.n,
@@ -3211,6 +3223,7 @@ form_level(Context& c, int l, double* y, const double* x, double d)
 {
   Level& L = c.L[l];
   GB_REQUIRE(L.m_assembled, GB_ESTATE, "Form needs an assembled level (gb_assemble)");
+  GB_REQUIRE(L.mesh_deg == 1, GB_EINVAL, "Form is built for Q1 elements only");
   const int dim = L.mesh_dim, nl = 1 << dim;
   const int nc = static_cast<int>(L.mesh_ncells);
   GB_CUDA(c.asm_E.n >= size_t(nc) * nl ? cudaSuccess : c.asm_E.alloc(size_t(nc) * nl));
@@ -4358,13 +4371,22 @@ int
 gb_level_set_mesh(gb_ctx* ctx, int lvl, int dim, int64_t ncells, const int64_t* cell_nodes,
                   const double* coords, const int64_t* parent)
 {
+  return gb_level_set_mesh_degree(ctx, lvl, dim, 1, ncells, cell_nodes, coords, parent);
+}
+
+int
+gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncells,
+                         const int64_t* cell_nodes, const double* coords,
+                         const int64_t* parent)
+{
   GB_API_BEGIN
   ctx->version++;
   Level& L = level_with_matrix(*ctx, lvl);
   GB_REQUIRE(dim == 2 || dim == 3, GB_EINVAL, "dim must be 2 or 3");
+  GB_REQUIRE(degree == 1 || degree == 2, GB_EINVAL, "degree must be 1 (Q1) or 2 (Q2)");
   GB_REQUIRE(L.B == 1, GB_EINVAL, "device assembly needs block size 1");
   GB_REQUIRE(!L.has_hn(), GB_EINVAL, "device assembly of a level with hanging nodes");
-  const int nl = 1 << dim;
+  const int nl = degree == 1 ? 1 << dim : (dim == 3 ? 27 : 9);
   GB_REQUIRE(ncells >= 1 && ncells * nl * nl < (int64_t(1) << 31), GB_EINVAL,
              "ncells out of range");
   GB_REQUIRE(cell_nodes && coords, GB_EINVAL, "null array");
@@ -4460,6 +4482,7 @@ gb_level_set_mesh(gb_ctx* ctx, int lvl, int dim, int64_t ncells, const int64_t* 
   L.m_assembled = false;
   L.h_parent.swap(par);
   L.mesh_dim = dim;
+  L.mesh_deg = degree;
   L.mesh_ncells = ncells;
   L.mesh_n = n;
   if (L.has_AT) { // the transpose again, with its map for device refreshes

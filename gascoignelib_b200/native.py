@@ -107,6 +107,8 @@ _SIGS = {
     "gb_level_set_functional": [C.c_void_p, C.c_int, _PD, _PD],
     "gb_functional": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD],
     "gb_level_set_mesh": [C.c_void_p, C.c_int, C.c_int, C.c_int64, _P64, _PD, _P64],
+    "gb_level_set_mesh_degree": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, _P64, _PD,
+                                 _P64],
     "gb_assemble": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, _PD],
     "gb_assemble_levels": [C.c_void_p, C.c_void_p, C.c_int, _PD],
     "gb_level_get_kappa": [C.c_void_p, C.c_int, _PD],
@@ -268,15 +270,16 @@ class Context:
             self._chk(self._L.gb_level_set_functional(self.h, level, _pd(ml), None))
 
     # ------------------------------------------------------- device assembly
-    def set_mesh(self, level, dim, cells, coords, parent=None):
+    def set_mesh(self, level, dim, cells, coords, parent=None, degree=1):
         """Q1 cells (int64 [ncells, 2^dim], local node a at corner bits
         (a&1, a>>1&1, a>>2&1)), node coordinates [n, dim] and, above level 0,
         the parent cell on level-1 of every cell (gb_level_set_mesh)."""
         nd = np.ascontiguousarray(cells, dtype=np.int64)
         xy = np.ascontiguousarray(coords, dtype=np.float64)
         pa = None if parent is None else np.ascontiguousarray(parent, dtype=np.int64)
-        self._chk(self._L.gb_level_set_mesh(self.h, level, dim, nd.shape[0], _p64(nd),
-                                            _pd(xy), _p64(pa) if pa is not None else None))
+        self._chk(self._L.gb_level_set_mesh_degree(self.h, level, dim, degree, nd.shape[0],
+                                                   _p64(nd), _pd(xy),
+                                                   _p64(pa) if pa is not None else None))
 
     @staticmethod
     def _kappa_arg(kappa):

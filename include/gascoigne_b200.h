@@ -321,6 +321,15 @@ int gb_functional(gb_ctx* ctx, int level, int u, int g, double* J);
 int gb_level_set_mesh(gb_ctx* ctx, int level, int dim, int64_t ncells,
                       const int64_t* cell_nodes, const double* coords,
                       const int64_t* parent);
+/* The same for elements of degree 1 (Q1, as gb_level_set_mesh) or 2 (CGQ2:
+ * 3^dim nodes per element on a patch of 2^dim cells, local node
+ * a = a_x + 3 a_y + 9 a_z at the reference coordinates (a_d / 2); integrated
+ * with QuadGauss9 / HexGauss27 as LineGauss3 states its points and weights,
+ * Discretization/Q1/integrationformula1d.cc:82-92; kappa per element, parents
+ * = the element of level - 1 that contains it). gb_form is built for Q1 only. */
+int gb_level_set_mesh_degree(gb_ctx* ctx, int level, int dim, int degree,
+                             int64_t ncells, const int64_t* cell_nodes,
+                             const double* coords, const int64_t* parent);
 /* Assembles the level's matrix (FP64 and FP32 values, block-diagonal inverse)
  * from kappa (ncells doubles; where = 0: host memory, 1: device memory,
  * copied on the context's stream (gb_ctx_get_stream), so writes to it on other

@@ -1,4 +1,4 @@
-"""CPU restatement (numpy) of the reference's Q1 matrix assembly, for the
+"""CPU restatement (numpy) of the reference's Q1 and Q2 matrix assembly, for the
 device assembly's tests. Test infrastructure: nothing in the library imports it.
 
 What it restates:
@@ -147,3 +147,89 @@ def assemble(n: int, rowptr, col, cells, E, dirichlet) -> np.ndarray:
     val[dm[ri] | dm[col]] = 0.0
     val[(ri == col) & dm[ri]] = 1.0
     return val
+
+
+# ------------------------------------------------------------------ Q2
+
+# LineGauss3 as the reference states it (Discretization/Q1/integrationformula1d.cc
+# :82-92): points to 20 digits, weights rounded to 12 (so 5/18, 8/18 are off by
+# about 2e-13 relative; the tensor rules QuadGauss9 / HexGauss27 inherit it)
+_P3 = (0.11270166537925831148, 0.5, 0.88729833462074168852)
+_W3 = (0.277777777778, 0.444444444444, 0.277777777778)
+
+
+def gauss_points_q2(dim: int):
+    """The reference's 3-point Gauss rule per direction on [0, 1]^dim
+    (QuadGauss9 / HexGauss27): points [3^dim, dim] (x fastest), weights."""
+    p1 = np.array(_P3)
+    w1 = np.array(_W3)
+    grids = np.meshgrid(*([np.arange(3)] * dim), indexing="ij")
+    idx = np.stack([g.ravel() for g in reversed(grids)], 1)     # x fastest
+    return p1[idx], np.prod(w1[idx], axis=1)
+
+
+def q2_shape(dim: int, xi: np.ndarray):
+    """Q2 (tensor quadratic Lagrange, nodes 0, 1/2, 1) values [3^dim] and
+    reference gradients [3^dim, dim]; local node a = sum_d a_d 3^d."""
+    def L(k, t):
+        return (2 * (t - 0.5) * (t - 1.0), -4.0 * t * (t - 1.0), 2.0 * t * (t - 0.5))[k]
+
+    def dL(k, t):
+        return (4.0 * t - 3.0, -8.0 * t + 4.0, 4.0 * t - 1.0)[k]
+
+    nloc = 3 ** dim
+    phi = np.ones(nloc)
+    grad = np.ones((nloc, dim))
+    for a in range(nloc):
+        digits = [(a // 3 ** d) % 3 for d in range(dim)]
+        for d in range(dim):
+            f, df = L(digits[d], xi[d]), dL(digits[d], xi[d])
+            phi[a] *= f
+            for e in range(dim):
+                grad[a, e] *= df if e == d else f
+    return phi, grad
+
+
+def q2_element_matrices(dim: int, xcell: np.ndarray, kappa: np.ndarray,
+                        beta=None) -> np.ndarray:
+    """As q1_element_matrices for Q2 elements (3^dim nodes, the isoparametric
+    quadratic map) with the 3-point Gauss rule."""
+    pts, wts = gauss_points_q2(dim)
+    nc, nloc = xcell.shape[0], 3 ** dim
+    E = np.zeros((nc, nloc, nloc))
+    b = np.zeros(dim) if beta is None else np.asarray(beta, dtype=np.float64)[:dim]
+    for q in range(pts.shape[0]):
+        phi, gref = q2_shape(dim, pts[q])
+        J = np.einsum("cad,ae->cde", xcell, gref)
+        det = np.linalg.det(J)
+        Jinv = np.linalg.inv(J)
+        g = np.einsum("ae,ced->cad", gref, Jinv)
+        w = wts[q] * det
+        E += (w * kappa)[:, None, None] * np.einsum("cad,cbd->cab", g, g)
+        conv = np.einsum("cbd,d->cb", g, b)
+        E += w[:, None, None] * phi[None, :, None] * conv[:, None, :]
+    return E
+
+
+def uniform_patches(coord: np.ndarray, dim: int) -> np.ndarray:
+    """Q2 elements (patches of 2^dim cells, 3^dim nodes, local order
+    lexicographic) of a uniform mesh in a given node numbering."""
+    n = coord.shape[0]
+    N = int(round(n ** (1.0 / dim))) - 1
+    c = np.rint(coord * N).astype(np.int64)
+    lex = np.zeros(n, dtype=np.int64)
+    for d in reversed(range(dim)):
+        lex = lex * (N + 1) + c[:, d]
+    inv = np.empty_like(lex)
+    inv[lex] = np.arange(n)
+    n1, P = N + 1, N // 2
+    if dim == 3:
+        k, j, i = np.meshgrid(np.arange(P), np.arange(P), np.arange(P), indexing="ij")
+        base = ((2 * k * n1 + 2 * j) * n1 + 2 * i).ravel()
+        loc = np.array([(a * n1 + b) * n1 + e for a in range(3) for b in range(3)
+                        for e in range(3)])
+    else:
+        j, i = np.meshgrid(np.arange(P), np.arange(P), indexing="ij")
+        base = (2 * j * n1 + 2 * i).ravel()
+        loc = np.array([b * n1 + e for b in range(3) for e in range(3)])
+    return inv[base[:, None] + loc[None, :]]

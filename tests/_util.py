@@ -195,3 +195,38 @@ def golden_kappa_beta(name):
     beta = ([float(t) for t in str(z["key_conv"]).split(",")] if "key_conv" in z.files
             else None)
     return seeded_inputs(dim, coarse, refine)[0], beta
+
+
+def uniform_meshes_q2(P):
+    """Per level (elements, parents) of a uniform CGQ2 hierarchy (elements =
+    patches of 2^dim cells) in the problem's node numbering."""
+    from oracle.assembly import uniform_parents, uniform_patches
+    out = []
+    for l, L in enumerate(P.levels):
+        el = uniform_patches(L.coord, P.dim)
+        N = round(el.shape[0] ** (1.0 / P.dim))
+        out.append((el, uniform_parents(P.dim, N) if l > 0 else None))
+    return out
+
+
+def q2_element_kappa(dim, kappa_cells, Ncells):
+    """kappa per finest Q2 element: the mean of its 2^dim cells (the harness's
+    coefficient at the element's resolution)."""
+    from oracle.assembly import coarsen_kappa, uniform_parents
+    return coarsen_kappa(np.asarray(kappa_cells), uniform_parents(dim, Ncells),
+                         (Ncells // 2) ** dim)
+
+
+def oracle_level_values_q2(P, kappa_elements, beta=None):
+    from oracle.assembly import assemble, coarsen_kappa, q2_element_matrices
+    meshes = uniform_meshes_q2(P)
+    kap = [None] * P.nlevels
+    kap[-1] = np.asarray(kappa_elements, dtype=np.float64)
+    for l in range(P.nlevels - 2, -1, -1):
+        kap[l] = coarsen_kappa(kap[l + 1], meshes[l + 1][1], meshes[l][0].shape[0])
+    vals = []
+    for l, L in enumerate(P.levels):
+        el = meshes[l][0]
+        E = q2_element_matrices(P.dim, L.coord[el], kap[l], beta)
+        vals.append(assemble(L.n, L.rowptr, L.col, el, E, L.dirichlet))
+    return vals, kap

@@ -13,7 +13,8 @@ matrices) with the pressure filter and the Vanka or block-Jacobi smoother; the
 harness runs them on one OpenMP thread, so Vanka's patch contributions are
 summed in patch order. The "hn_" cases refine a ball once more (hanging
 nodes, Q1 or Q2 elements) and also record the reference's HNAverage,
-HNDistribute and HNZero of a test vector on the finest level. The "ilu_"
+HNDistribute and HNZero of a test vector on the finest level. The "q2_"
+cases are CGQ2 elements with the seeded per-cell kappa. The "ilu_"
 cases use linear_smooth ilu with matrixtype block (SparseBlockIlu). The "form_"
 cases also record StdSolver::Form and StdMultiLevelSolver::NewtonResidual of a
 seeded vector and the solution as written by WriteBackUp (.bup) and
@@ -56,6 +57,8 @@ CASES = {
     "ilu_3d_c1_r3_seeded": (3, 1, 3, True, 1e-10, {"smoother": "ilu", "omega": 1.0}),
     "ilu_2d_c2_r4_conv": (2, 2, 4, True, 1e-10, {"smoother": "ilu", "omega": 1.0,
                                                  "conv": "4,2"}),
+    "q2_3d_c1_r3_kappa_conv": (3, 1, 3, True, 1e-8, {"disc": "Q2", "conv": "1,0.5,0.25"}),
+    "q2_2d_c2_r3_kappa": (2, 2, 3, True, 1e-10, {"disc": "Q2"}),
     "form_3d_c1_r3_conv": (3, 1, 3, True, 1e-8, {"conv": "1,0.5,0.25", "backup": 1,
                                                  "formx": 1005}),
     "form_2d_c2_r3": (2, 2, 3, True, 1e-10, {"backup": 1, "formx": 1006}),

@@ -198,3 +198,51 @@ def test_reassembly_after_solves(ctx, nd):
     assert fi["status_name"] == "converged" and af["status_name"] == "converged"
     ctx.free(x)
     ctx.free(b)
+
+
+@pytest.mark.parametrize("name", [n for n in __import__("_util").golden_cases()
+                                  if n.startswith("q2_")])
+def test_q2_assembly_matches_reference_and_solves(ctx, name):
+    """CGQ2 (27-node hexahedra, 9-node quadrilaterals) assembled on the device:
+    the reference's matrices on every level, and its solve."""
+    from _util import golden_kappa_beta, q2_element_kappa, uniform_meshes_q2
+    P, ref = load_golden(name)
+    kappa, beta = golden_kappa_beta(name)
+    Nc = round(len(kappa) ** (1.0 / P.dim))
+    ctx.load_problem(_zero_values(P))
+    for l, (el, par) in enumerate(uniform_meshes_q2(P)):
+        ctx.set_mesh(l, P.dim, el, P.levels[l].coord, par, degree=2)
+    ctx.assemble_levels(q2_element_kappa(P.dim, kappa, Nc), beta)
+    for l, L in enumerate(P.levels):
+        v = ctx.level_values(l, L.val.size)
+        assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
+    keys = ref["keys"]
+    ctx.set_params(**solver_keys(keys), gmressize=int(keys["gmressize"]),
+                   tol=float(keys["tol"]), globaltol=1e-16, maxiter=100)
+    fl = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(fl, b, P.rhs)
+    info = ctx.gmres(x, b)
+    assert abs(info["iterations"] - ref["iterations"]) <= 1
+    assert rel_l2(ctx.download(fl, x), ref["solution"]) < 1e-8
+    with pytest.raises(GBError, match="Q1 elements only"):
+        ctx.form(fl, x, b)
+    ctx.free(x)
+    ctx.free(b)
+
+
+def test_q2_assembly_c4_size_against_generator(ctx):
+    """The 40^3-element Q2 hierarchy of the C4 bench line (constant eps, beta):
+    the generator's exact-integral matrices within the reference's own 12-digit
+    Gauss weights (1e-12)."""
+    from gascoignelib_b200.problem import structured_q2
+    from _util import uniform_meshes_q2
+    P = structured_q2(3, 5, 4, eps=1e-2, beta=(1.0, 0.5, 0.25))
+    ctx.load_problem(_zero_values(P))
+    for l, (el, par) in enumerate(uniform_meshes_q2(P)):
+        ctx.set_mesh(l, 3, el, P.levels[l].coord, par, degree=2)
+    ne = uniform_meshes_q2(P)[-1][0].shape[0]
+    ctx.assemble_levels(np.full(ne, 1e-2), (1.0, 0.5, 0.25))
+    for l, L in enumerate(P.levels):
+        v = ctx.level_values(l, L.val.size)
+        assert np.abs(v - L.val).max() <= 1e-12 * np.abs(L.val).max(), l

@@ -80,3 +80,21 @@ def test_backup_formats_match_reference_files(name):
     assert txt.encode() == ref["backup_bup"].tobytes()
     bip = f"{B} {P.finest.n}\n[".encode() + u.astype("<f8").tobytes() + b"]BackUpEnd\n"
     assert bip == ref["backup_bip"].tobytes()
+
+
+def _q2_golden():
+    from _util import golden_cases
+    return [n for n in golden_cases() if n.startswith("q2_")]
+
+
+@pytest.mark.parametrize("name", _q2_golden())
+def test_oracle_q2_assembly_matches_reference(name):
+    """CGQ2 elements with the per-cell kappa (per element: the mean of its
+    cells) and LineGauss3 as the reference states it."""
+    from _util import golden_kappa_beta, oracle_level_values_q2, q2_element_kappa
+    P, _ = load_golden(name)
+    kappa, beta = golden_kappa_beta(name)
+    Nc = round(len(kappa) ** (1.0 / P.dim))
+    vals, _ = oracle_level_values_q2(P, q2_element_kappa(P.dim, kappa, Nc), beta)
+    for L, v in zip(P.levels, vals):
+        assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max()
