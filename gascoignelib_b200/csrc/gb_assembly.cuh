@@ -305,6 +305,134 @@ k_q2_element(int ncells, const int* __restrict__ cells, const double* __restrict
     E[(int64_t(a) * NL + b) * ncells + c] = e[b];
 }
 
+// The same element matrices with one warp per element: lane b (< 3^DIM) holds
+// node b. At each Gauss point the lanes form their terms of J and sum them
+// with a butterfly of shuffles (the same sum, in the same order, on every
+// lane), then each lane computes its own physical gradient once and hands it
+// to the other lanes by shuffles; lane a accumulates row a. Per element and
+// point this forms each basis gradient once instead of once per row.
+template<int DIM, bool CONV>
+__global__ void __launch_bounds__(128)
+k_q2_element_warp(int ncells, const int* __restrict__ cells,
+                  const double* __restrict__ coords, const double* __restrict__ kappa,
+                  double b0, double b1, double b2, double* __restrict__ E)
+{
+  GB_PDL_ENTRY();
+  constexpr int NL = DIM == 3 ? 27 : 9;
+  const int64_t wid = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= ncells) // whole warps leave together
+    return;
+  const int c = static_cast<int>(wid);
+  const bool act = lane < NL;
+  const double P3[3] = { 0.11270166537925831148, 0.5, 0.88729833462074168852 };
+  const double W3[3] = { 0.277777777778, 0.444444444444, 0.277777777778 };
+  const double beta[3] = { b0, b1, b2 };
+  const double kap = __ldg(kappa + c);
+  int ld[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+    ld[d] = (lane / (d == 0 ? 1 : d == 1 ? 3 : 9)) % 3;
+  double X[DIM];
+  {
+    const int64_t node = act ? __ldg(cells + int64_t(lane) * ncells + c) : 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      X[d] = act ? __ldg(coords + node * DIM + d) : 0.0;
+  }
+  double e[NL];
+#pragma unroll
+  for (int b = 0; b < NL; ++b)
+    e[b] = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < NL; ++q) {
+    double L[DIM][3], dL[DIM][3], wq = 1.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const int qd = (q / (d == 0 ? 1 : d == 1 ? 3 : 9)) % 3;
+      q2_basis_1d(P3[qd], L[d], dL[d]);
+      wq *= W3[qd];
+    }
+    // this lane's basis function: value and reference gradient
+    double phi = 1.0, gr[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      phi *= L[d][ld[d]];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      double g = 1.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        g *= d == k ? dL[d][ld[d]] : L[d][ld[d]];
+      gr[k] = act ? g : 0.0;
+    }
+    // J[d][k] = sum over nodes of X[d] gr[k]
+    double J[DIM][DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) {
+        double v = X[d] * gr[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+          v += __shfl_xor_sync(0xffffffffu, v, o);
+        J[d][k] = v;
+      }
+    double det, Ji[DIM][DIM];
+    if (DIM == 2) {
+      det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+      const double r = 1.0 / det;
+      Ji[0][0] = J[1][1] * r;
+      Ji[0][1] = -J[0][1] * r;
+      Ji[1][0] = -J[1][0] * r;
+      Ji[1][1] = J[0][0] * r;
+    } else {
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+      const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+      const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      const double r = 1.0 / det;
+      Ji[0][0] = c00 * r;
+      Ji[1][0] = c01 * r;
+      Ji[2][0] = c02 * r;
+      Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * r;
+      Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * r;
+      Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * r;
+      Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * r;
+      Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * r;
+      Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * r;
+    }
+    const double w = wq * fabs(det);
+    double gx[DIM], bg = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      double t = 0.0;
+#pragma unroll
+      for (int k = 0; k < DIM; ++k)
+        t = fma(gr[k], Ji[k][d], t);
+      gx[d] = t;
+      if (CONV)
+        bg = fma(beta[d], t, bg);
+    }
+    const double wk = w * kap, wp = w * phi;
+#pragma unroll
+    for (int b = 0; b < NL; ++b) {
+      double dg = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        dg = fma(__shfl_sync(0xffffffffu, gx[d], b), gx[d], dg);
+      e[b] = fma(wk, dg, e[b]);
+      if (CONV)
+        e[b] = fma(wp, __shfl_sync(0xffffffffu, bg, b), e[b]);
+    }
+  }
+  if (act) {
+#pragma unroll
+    for (int b = 0; b < NL; ++b)
+      E[(int64_t(lane) * NL + b) * ncells + c] = e[b];
+  }
+}
+
 // The level's SELL values from the element matrices (LocalToGlobal +
 // MatrixInterface::entry, DofHandler/cgdisc.h:353-366): entry e sums
 // E[clist[k]] for k in [cptr[e], cptr[e+1]), the contributions in ascending

@@ -3141,7 +3141,7 @@ assemble_level(Context& c, int l, const double* beta)
   launch(c, k_q1_element<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,  \
          (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p)
 #define GB_ELEM2(D, CV)                                                                  \
-  launch(c, k_q2_element<D, CV>, blocks_for(int64_t(nc) * nl, 128), 128, nc,            \
+  launch(c, k_q2_element_warp<D, CV>, blocks_for(int64_t(nc) * 32, 128), 128, nc,       \
          (const int*)L.m_cells.p, (const double*)L.m_coords.p, (const double*)L.m_kappa.p, \
          b0, b1, b2, c.asm_E.p)
   if (L.mesh_deg == 2) {
