@@ -154,14 +154,6 @@ k_q1_element(int ncells, const int* __restrict__ cells, const double* __restrict
     E[int64_t(p) * ncells + c] = e[p];
 }
 
-// Q2 element matrices (CGQ2: 3^DIM-node elements on patches of 2^DIM cells,
-// the isoparametric quadratic map, the matrix formula QuadGauss9 / HexGauss27
-// with LineGauss3's points and 12-digit weights as the reference states them,
-// Discretization/Q1/integrationformula1d.cc:82-92). One thread per (cell, row
-// a): thread t takes cell t % ncells and row t / ncells; at each Gauss point it
-// forms J from all nodes, then row a of
-//   w |J| (kappa grad phi_b . grad phi_a + (beta . grad phi_b) phi_a).
-// Local node a = sum_d a_d 3^d (x fastest), basis nodes 0, 1/2, 1 per axis.
 __device__ __forceinline__ void
 q2_basis_1d(double t, double* L, double* dL)
 {
@@ -173,139 +165,13 @@ q2_basis_1d(double t, double* L, double* dL)
   dL[2] = 4.0 * t - 1.0;
 }
 
-template<int DIM, bool CONV>
-__global__ void __launch_bounds__(128)
-k_q2_element(int ncells, const int* __restrict__ cells, const double* __restrict__ coords,
-             const double* __restrict__ kappa, double b0, double b1, double b2,
-             double* __restrict__ E)
-{
-  GB_PDL_ENTRY();
-  constexpr int NL = DIM == 3 ? 27 : 9;
-  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (t >= int64_t(ncells) * NL)
-    return;
-  const int c = static_cast<int>(t % ncells), a = static_cast<int>(t / ncells);
-  const double P3[3] = { 0.11270166537925831148, 0.5, 0.88729833462074168852 };
-  const double W3[3] = { 0.277777777778, 0.444444444444, 0.277777777778 };
-  const double beta[3] = { b0, b1, b2 };
-  const double kap = __ldg(kappa + c);
-  int ad[DIM];
-#pragma unroll
-  for (int d = 0; d < DIM; ++d)
-    ad[d] = (a / (d == 0 ? 1 : d == 1 ? 3 : 9)) % 3;
-  double e[NL];
-#pragma unroll
-  for (int b = 0; b < NL; ++b)
-    e[b] = 0.0;
-#pragma unroll 1
-  for (int q = 0; q < NL; ++q) {
-    double L[DIM][3], dL[DIM][3], wq = 1.0;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      const int qd = (q / (d == 0 ? 1 : d == 1 ? 3 : 9)) % 3;
-      q2_basis_1d(P3[qd], L[d], dL[d]);
-      wq *= W3[qd];
-    }
-    double J[DIM][DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-#pragma unroll
-      for (int k = 0; k < DIM; ++k)
-        J[d][k] = 0.0;
-#pragma unroll 1
-    for (int b = 0; b < NL; ++b) {
-      const int64_t node = __ldg(cells + int64_t(b) * ncells + c);
-      const int b0i = b % 3, b1i = (b / 3) % 3, b2i = b / 9;
-      const int bd[3] = { b0i, b1i, b2i };
-#pragma unroll
-      for (int k = 0; k < DIM; ++k) {
-        double g = 1.0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d)
-          g *= d == k ? dL[d][bd[d]] : L[d][bd[d]];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d)
-          J[d][k] = fma(__ldg(coords + node * DIM + d), g, J[d][k]);
-      }
-    }
-    double det, Ji[DIM][DIM];
-    if (DIM == 2) {
-      det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
-      const double r = 1.0 / det;
-      Ji[0][0] = J[1][1] * r;
-      Ji[0][1] = -J[0][1] * r;
-      Ji[1][0] = -J[1][0] * r;
-      Ji[1][1] = J[0][0] * r;
-    } else {
-      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
-      const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
-      const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-      det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
-      const double r = 1.0 / det;
-      Ji[0][0] = c00 * r;
-      Ji[1][0] = c01 * r;
-      Ji[2][0] = c02 * r;
-      Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * r;
-      Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * r;
-      Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * r;
-      Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * r;
-      Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * r;
-      Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * r;
-    }
-    const double w = wq * fabs(det);
-    // row a: value and physical gradient
-    double phia = 1.0, ga[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-      phia *= L[d][ad[d]];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k < DIM; ++k) {
-        double g = 1.0;
-#pragma unroll
-        for (int dd = 0; dd < DIM; ++dd)
-          g *= dd == k ? dL[dd][ad[dd]] : L[dd][ad[dd]];
-        s = fma(g, Ji[k][d], s);
-      }
-      ga[d] = s;
-    }
-    const double wk = w * kap, wp = w * phia;
-#pragma unroll
-    for (int b = 0; b < NL; ++b) {
-      const int bd[3] = { b % 3, (b / 3) % 3, b / 9 };
-      double gr[DIM];
-#pragma unroll
-      for (int k = 0; k < DIM; ++k) {
-        double g = 1.0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d)
-          g *= d == k ? dL[d][bd[d]] : L[d][bd[d]];
-        gr[k] = g;
-      }
-      double dg = 0.0, bgv = 0.0;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        double gx = 0.0;
-#pragma unroll
-        for (int k = 0; k < DIM; ++k)
-          gx = fma(gr[k], Ji[k][d], gx);
-        dg = fma(gx, ga[d], dg);
-        if (CONV)
-          bgv = fma(beta[d], gx, bgv);
-      }
-      e[b] = fma(wk, dg, e[b]);
-      if (CONV)
-        e[b] = fma(wp, bgv, e[b]);
-    }
-  }
-#pragma unroll
-  for (int b = 0; b < NL; ++b)
-    E[(int64_t(a) * NL + b) * ncells + c] = e[b];
-}
-
-// The same element matrices with one warp per element: lane b (< 3^DIM) holds
+// Q2 element matrices (CGQ2: 3^DIM-node elements on patches of 2^DIM cells,
+// the isoparametric quadratic map, the matrix formula QuadGauss9 / HexGauss27
+// with LineGauss3's points and 12-digit weights as the reference states them,
+// Discretization/Q1/integrationformula1d.cc:82-92): row a of
+//   w |J| (kappa grad phi_b . grad phi_a + (beta . grad phi_b) phi_a),
+// local node a = sum_d a_d 3^d (x fastest), basis nodes 0, 1/2, 1 per axis.
+// One warp per element: lane b (< 3^DIM) holds
 // node b. At each Gauss point the lanes form their terms of J and sum them
 // with a butterfly of shuffles (the same sum, in the same order, on every
 // lane), then each lane computes its own physical gradient once and hands it
