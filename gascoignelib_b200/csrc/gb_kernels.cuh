@@ -304,6 +304,61 @@ k_restrict(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ ten
   coarse[i] = (cdir && cdir[i]) ? T(0) : acc;
 }
 
+// The same restriction with four lanes per coarse row: lane q of the quad
+// loads entries 8q..8q+7 of the row (rows of at most 32 entries), so that a
+// row's gathers are in flight at once, and lane 0 of the quad sums all of them
+// in ascending order with the same fused multiply-adds as transfer_row (the
+// entries and values reach it by shuffles): the result is bit-identical.
+template<class T>
+__global__ void __launch_bounds__(256)
+k_restrict4(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
+            const T* __restrict__ fine, T* __restrict__ coarse,
+            const uint8_t* __restrict__ cdir)
+{
+  GB_PDL_ENTRY();
+  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int i = static_cast<int>(t >> 2), q = static_cast<int>(t & 3);
+  const bool ok = i < nc; // every lane stays for the shuffles
+  int w = 0;
+  uint32_t e[8];
+  T f[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    e[k] = kPadEntry;
+    f[k] = T(0);
+  }
+  if (ok) {
+    const int beg = __ldg(tsp + (i >> 5));
+    w = (__ldg(tsp + (i >> 5) + 1) - beg) >> 5;
+    const uint32_t* ep = tent + beg + (i & 31);
+    if (q * 8 < w) {
+      const uint32_t* pe[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        pe[k] = ep + min(q * 8 + k, w - 1) * kSlice;
+      ld8(e, pe);
+      const T* ps[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        ps[k] = fine + (e[k] & kIdxMask);
+      ld8(f, ps);
+    }
+  }
+  const int lead = (threadIdx.x & 31) & ~3;
+  T acc = T(0);
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t ek = __shfl_sync(0xffffffffu, e[k], lead + s);
+      const T fk = __shfl_sync(0xffffffffu, f[k], lead + s);
+      if (s * 8 + k < w)
+        acc = fma(wcode<T>(ek), fk, acc);
+    }
+  if (ok && q == 0)
+    coarse[i] = (cdir && cdir[i]) ? T(0) : acc;
+}
+
 // fine += P coarse (prolongate_add order), optionally masked by the fine
 // Dirichlet dofs and scaled: MODE 0: fine += P c; MODE 1 (coarse-grid
 // correction): u += mgomega * (dir ? 0 : P c).

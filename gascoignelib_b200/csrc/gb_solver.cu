@@ -421,6 +421,7 @@ struct Transfer
 {
   bool set = false;
   int nc = 0, nf = 0;
+  int rmaxw = 0; // widest restriction row (k_restrict4 takes rows of <= 32)
   int64_t nent = 0;
   DeviceArray<int> rptr, pptr;
   DeviceArray<uint32_t> rent, pent;
@@ -1795,7 +1796,11 @@ struct Emit
     const int nb = blocks_for(Tr.nc, 256);
     switch (c.L[l].B) {
       case 1:
-        launch(c, k_restrict<T>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        if (Tr.rmaxw <= 32)
+          launch(c, k_restrict4<T>, blocks_for(int64_t(Tr.nc) * 4, 256), 256, Tr.nc,
+                 Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        else
+          launch(c, k_restrict<T>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
         break;
       case 2:
         launch(c, k_restrict_b<T, 2>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm,
@@ -3566,6 +3571,9 @@ gb_level_set_transfer(gb_ctx* ctx, int lvl, int64_t ncoarse, const int64_t* c2f,
   Transfer& T = ctx->T[lvl];
   T.nc = static_cast<int>(ncoarse);
   T.nf = static_cast<int>(nf);
+  T.rmaxw = 0;
+  for (size_t sl = 0; sl + 1 < rptr.size(); ++sl)
+    T.rmaxw = std::max(T.rmaxw, (rptr[sl + 1] - rptr[sl]) / kSlice);
   T.nent = static_cast<int64_t>(pairs.size());
   GB_CUDA(T.pptr.alloc(pptr.size()));
   GB_CUDA(T.rptr.alloc(rptr.size()));
@@ -4099,7 +4107,11 @@ gb_restrict_zero(gb_ctx* ctx, int lvl, int coarse_id, int fine_id)
   const uint8_t* nm = nullptr;
   switch (B) {
     case 1:
-      launch(*ctx, k_restrict<double>, nb, 256, T.nc, tp, te, f, cc, nm);
+      if (T.rmaxw <= 32)
+        launch(*ctx, k_restrict4<double>, blocks_for(int64_t(T.nc) * 4, 256), 256, T.nc, tp,
+               te, f, cc, nm);
+      else
+        launch(*ctx, k_restrict<double>, nb, 256, T.nc, tp, te, f, cc, nm);
       break;
     case 2:
       launch(*ctx, k_restrict_b<double, 2>, nb, 256, T.nc, tp, te, f, cc, nm, -1,
