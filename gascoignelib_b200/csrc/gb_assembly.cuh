@@ -299,13 +299,82 @@ k_q2_element_warp(int ncells, const int* __restrict__ cells,
   }
 }
 
+// One step of the hanging-node condensation of an element matrix: with t >= 0
+// column t += w column s, then row t += w row s (a parent of the hanging node
+// in slot s that the element holds in slot t); with t < 0 column s and row s
+// scaled by w (the one parent the element lacks, which takes slot s).
+struct CondOp
+{
+  int s, t;
+  double w;
+};
+
+// The element matrices of the cells with hanging nodes condensed in place
+// (CGDisc::LocalToGlobal, DofHandler/cgdisc.h:354-364, with the
+// HNStructure::CondenseHanging of the discretisation: Q1 2D/3D,
+// Discretization/Q1/hnstructureq12d.cc:129-158, hnstructureq13d.cc:275-438;
+// Q2 2D/3D, Discretization/Q2/hnstructureq22d.cc:84-110,
+// hnstructureq23d.cc:161-378). The host orders each cell's steps (edges,
+// then faces, ascending slots). One warp per cell, lane i holding row /
+// column i; a product and a sum per entry, rounded separately.
+__global__ void __launch_bounds__(128)
+k_condense(int nh, const int* __restrict__ hcells, const int* __restrict__ opptr,
+           const CondOp* __restrict__ ops, int nl, int ncells, double* __restrict__ E)
+{
+  GB_PDL_ENTRY();
+  const int64_t wid = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= nh) // whole warps leave together
+    return;
+  const int64_t c = __ldg(hcells + wid), nc = ncells;
+  const bool act = lane < nl;
+  const int k1 = __ldg(opptr + wid + 1);
+  for (int k = __ldg(opptr + wid); k < k1; ++k) {
+    const CondOp op = ops[k];
+    if (act) { // column step: entry (lane, .)
+      double* es = E + (int64_t(lane) * nl + op.s) * nc + c;
+      if (op.t >= 0) {
+        double* et = E + (int64_t(lane) * nl + op.t) * nc + c;
+        *et = __dadd_rn(*et, __dmul_rn(op.w, *es));
+      } else {
+        *es = __dmul_rn(*es, op.w);
+      }
+    }
+    __syncwarp();
+    if (act) { // row step: entry (., lane)
+      double* es = E + (int64_t(op.s) * nl + lane) * nc + c;
+      if (op.t >= 0) {
+        double* et = E + (int64_t(op.t) * nl + lane) * nc + c;
+        *et = __dadd_rn(*et, __dmul_rn(op.w, *es));
+      } else {
+        *es = __dmul_rn(*es, op.w);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// mask[list[k]] = 1 for k < nl (the hanging nodes into the assembly's
+// Dirichlet-or-hanging row mask)
+__global__ void
+k_mark_nodes(int nl, const int* __restrict__ list, uint8_t* __restrict__ mask)
+{
+  GB_PDL_ENTRY();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nl)
+    mask[__ldg(list + k)] = 1;
+}
+
 // The level's SELL values from the element matrices (LocalToGlobal +
 // MatrixInterface::entry, DofHandler/cgdisc.h:353-366): entry e sums
 // E[clist[k]] for k in [cptr[e], cptr[e+1]), the contributions in ascending
 // cell order (the reference's cell loop). Then the strong Dirichlet condition
 // (SparseBlockMatrix::dirichlet, LinAlg/sparseblockmatrix.xx:207-218): a
 // Dirichlet row keeps only its diagonal, set to 1, and a Dirichlet column is
-// zero elsewhere. Writes the FP64 and FP32 values and the diagonal (dd) for the
+// zero elsewhere. On a level with hanging nodes the mask also holds the
+// hanging rows, whose only entry is the diagonal, set to 1 like a Dirichlet
+// row (HNStructure::MatrixDiag, DofHandler/cgdisc.h:634). Writes the FP64 and
+// FP32 values and the diagonal (dd) for the
 // block-diagonal inverse. kAsmSplit warps per slice: warp g of slice s takes
 // the entries j = g, g + kAsmSplit, .. of the slice's 32 rows (lane = row), so
 // that a row's entries are summed by several threads at once.

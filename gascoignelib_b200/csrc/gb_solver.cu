@@ -398,6 +398,22 @@ struct Level
   double m_beta[3] = { 0.0, 0.0, 0.0 }; // convection of the last assembly
   bool m_assembled = false;
   DeviceArray<double> m_coords, m_kappa, m_dd;
+  // hanging nodes in the device assembly: per hanging node (h_hnidx[node],
+  // -1 elsewhere) its phase (0 edges, 1 faces), parents and weights in the
+  // HNStructure's parent order; the cells with a hanging node, their
+  // condensation steps (m_hopptr per cell), and the Dirichlet-or-hanging mask
+  struct HnCond
+  {
+    int phase = 0, np = 0;
+    int par[9];
+    double w[9];
+  };
+  std::vector<HnCond> h_hncond;
+  std::vector<int> h_hnidx;
+  int m_nhcells = 0;
+  DeviceArray<int> m_hcells, m_hopptr;
+  DeviceArray<CondOp> m_hops;
+  DeviceArray<uint8_t> m_hmask;
   std::vector<int64_t> h_parent;
   int64_t child_n = -1; // coarse cells the child lists were built for
   // block ILU (smoother 2, SparseBlockIlu): the factors in the matrix's row
@@ -3162,13 +3178,24 @@ assemble_level(Context& c, int l, const double* beta)
   }
 #undef GB_ELEM
 #undef GB_ELEM2
+  if (L.m_nhcells > 0)
+    launch(c, k_condense, blocks_for(int64_t(L.m_nhcells) * 32, 128), 128, L.m_nhcells,
+           (const int*)L.m_hcells.p, (const int*)L.m_hopptr.p, (const CondOp*)L.m_hops.p, nl,
+           nc, c.asm_E.p);
+  const uint8_t* rmask = L.dirmask.p; // rows kept as the identity
+  if (L.has_hn() && !L.h_hnnodes.empty()) {
+    GB_CUDA(cudaMemcpyAsync(L.m_hmask.p, L.dirmask.p, L.n, cudaMemcpyDeviceToDevice, c.stream));
+    launch(c, k_mark_nodes, blocks_for(int64_t(L.h_hnnodes.size()), 128), 128,
+           (int)L.h_hnnodes.size(), (const int*)L.hn_all.p, L.m_hmask.p);
+    rmask = L.m_hmask.p;
+  }
   const Sell& A = L.A;
   launch(c, k_asm_gather, blocks_for(int64_t(A.nslices) * kAsmSplit * kSlice, 256), 256,
          (int)L.n,
          (const int*)A.sptr.p, (const int*)(A.sorted ? A.rperm.p : nullptr),
          (const int*)A.col.p, (const int*)L.m_cptr.p, (const int*)L.m_clist.p,
-         (const double*)c.asm_E.p, (const uint8_t*)L.dirmask.p, (const int*)L.m_diagpos.p,
-         A.v64.p, A.v32.p, L.m_dd.p);
+         (const double*)c.asm_E.p, rmask, (const int*)L.m_diagpos.p, A.v64.p, A.v32.p,
+         L.m_dd.p);
   launch(c, k_blockdiag_inverse<1>, blocks_for(L.n, 128), 128, (int)L.n,
          (const double*)L.m_dd.p, L.dinv64.p, L.dinv32.p);
   L.h_val_stale = true;
@@ -3229,6 +3256,7 @@ form_level(Context& c, int l, double* y, const double* x, double d)
   Level& L = c.L[l];
   GB_REQUIRE(L.m_assembled, GB_ESTATE, "Form needs an assembled level (gb_assemble)");
   GB_REQUIRE(L.mesh_deg == 1, GB_EINVAL, "Form is built for Q1 elements only");
+  GB_REQUIRE(!L.has_hn(), GB_EINVAL, "Form on a level with hanging nodes");
   const int dim = L.mesh_dim, nl = 1 << dim;
   const int nc = static_cast<int>(L.mesh_ncells);
   GB_CUDA(c.asm_E.n >= size_t(nc) * nl ? cudaSuccess : c.asm_E.alloc(size_t(nc) * nl));
@@ -3950,6 +3978,27 @@ gb_level_set_hn(gb_ctx* ctx, int lvl, int disc, int64_t nedge, const int64_t* ed
   GB_CUDA(cudaStreamSynchronize(ctx->stream));
   L.hn.clear();
   L.h_hnnodes.clear();
+  // the assembly's condensation table; a mesh set before it is dropped
+  L.h_hncond.clear();
+  L.h_hnidx.assign(L.n, -1);
+  L.mesh_ncells = 0;
+  for (int ph = 0; ph < 2; ++ph) {
+    const Spec& sp = ph == 0 ? se : sf;
+    for (size_t k = 0; k < sp.node.size(); ++k) {
+      Level::HnCond hc;
+      hc.phase = ph;
+      hc.np = static_cast<int>(sp.w.size());
+      for (int j = 0; j < hc.np; ++j) {
+        hc.par[j] = static_cast<int>(sp.par[k][j]);
+        hc.w[j] = sp.w[j];
+      }
+      GB_REQUIRE(L.h_hnidx[sp.node[k]] < 0, GB_EINVAL, "a node hangs twice");
+      L.h_hnidx[sp.node[k]] = static_cast<int>(L.h_hncond.size());
+      L.h_hncond.push_back(hc);
+    }
+  }
+  if (L.h_hncond.empty())
+    L.h_hnidx.clear();
   std::vector<uint8_t> inphase(L.n, 0);
   for (Spec* sp : order) {
     const int nh = static_cast<int>(sp->node.size());
@@ -4397,7 +4446,8 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
   GB_REQUIRE(dim == 2 || dim == 3, GB_EINVAL, "dim must be 2 or 3");
   GB_REQUIRE(degree == 1 || degree == 2, GB_EINVAL, "degree must be 1 (Q1) or 2 (Q2)");
   GB_REQUIRE(L.B == 1, GB_EINVAL, "device assembly needs block size 1");
-  GB_REQUIRE(!L.has_hn(), GB_EINVAL, "device assembly of a level with hanging nodes");
+  GB_REQUIRE(!L.has_hn() || L.h_hnidx.size() == size_t(L.n), GB_EINVAL,
+             "the hanging nodes were set for another matrix size");
   const int nl = degree == 1 ? 1 << dim : (dim == 3 ? 27 : 9);
   GB_REQUIRE(ncells >= 1 && ncells * nl * nl < (int64_t(1) << 31), GB_EINVAL,
              "ncells out of range");
@@ -4420,6 +4470,50 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
     const int64_t t = slot[r];
     return sptr[t / kSlice] + (k - L.h_rowptr[r]) * kSlice + t % kSlice;
   };
+  for (int64_t k = 0; k < ncells * nl; ++k)
+    GB_REQUIRE(cell_nodes[k] >= 0 && cell_nodes[k] < n, GB_EINVAL, "cell node out of range");
+  // The matrix couples the condensed element indices: on a level with hanging
+  // nodes every hanging node of a cell (edges, then faces, ascending slots)
+  // gives way to the one parent that the cell lacks, and the cell's element
+  // matrix is condensed by the steps recorded here (CondOp).
+  std::vector<int64_t> ci(cell_nodes, cell_nodes + ncells * nl);
+  std::vector<int> hcells, hopptr(1, 0);
+  std::vector<CondOp> hops;
+  if (L.has_hn()) {
+    for (int64_t c = 0; c < ncells; ++c) {
+      int64_t* id = ci.data() + c * nl;
+      const size_t op0 = hops.size();
+      for (int ph = 0; ph < 2; ++ph)
+        for (int s = 0; s < nl; ++s) {
+          const int hi = L.h_hnidx[id[s]];
+          if (hi < 0 || L.h_hncond[hi].phase != ph)
+            continue;
+          const Level::HnCond& hc = L.h_hncond[hi];
+          int miss = -1, at[9];
+          for (int j = 0; j < hc.np; ++j) {
+            at[j] = -1;
+            for (int t = 0; t < nl; ++t)
+              if (id[t] == hc.par[j])
+                at[j] = t;
+            if (at[j] < 0) {
+              GB_REQUIRE(miss < 0, GB_EINVAL,
+                         "a cell lacks more than one parent of its hanging node");
+              miss = j;
+            }
+          }
+          GB_REQUIRE(miss >= 0, GB_EINVAL, "a cell holds every parent of its hanging node");
+          for (int j = 0; j < hc.np; ++j)
+            if (at[j] >= 0)
+              hops.push_back(CondOp{ s, at[j], hc.w[j] });
+          hops.push_back(CondOp{ s, -1, hc.w[miss] });
+          id[s] = hc.par[miss];
+        }
+      if (hops.size() > op0) {
+        hcells.push_back(static_cast<int>(c));
+        hopptr.push_back(static_cast<int>(hops.size()));
+      }
+    }
+  }
   std::vector<std::pair<int64_t, int64_t>> sc(L.h_col.size());
   for (int64_t i = 0; i < n; ++i) {
     for (int64_t k = L.h_rowptr[i]; k < L.h_rowptr[i + 1]; ++k)
@@ -4433,13 +4527,11 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
   std::vector<int> cptr(A.entries + 1, 0);
   for (int64_t c = 0; c < ncells; ++c)
     for (int a = 0; a < nl; ++a) {
-      const int64_t r = cell_nodes[c * nl + a];
-      GB_REQUIRE(r >= 0 && r < n, GB_EINVAL, "cell node out of range");
-      cn[size_t(a) * ncells + c] = static_cast<int>(r);
+      const int64_t r = ci[c * nl + a];
+      cn[size_t(a) * ncells + c] = static_cast<int>(cell_nodes[c * nl + a]); // geometry
       auto b0 = sc.begin() + L.h_rowptr[r], b1 = sc.begin() + L.h_rowptr[r + 1];
       for (int b = 0; b < nl; ++b) {
-        const int64_t q = cell_nodes[c * nl + b];
-        GB_REQUIRE(q >= 0 && q < n, GB_EINVAL, "cell node out of range");
+        const int64_t q = ci[c * nl + b];
         auto it = std::lower_bound(b0, b1, std::make_pair(q, int64_t(-1)));
         GB_REQUIRE(it != b1 && it->first == q, GB_EINVAL,
                    "a cell couples two nodes that the matrix pattern does not");
@@ -4460,14 +4552,14 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
   std::vector<int> nptr(n + 1, 0), nlist(size_t(ncells) * nl);
   for (int64_t c = 0; c < ncells; ++c)
     for (int a = 0; a < nl; ++a)
-      nptr[cell_nodes[c * nl + a] + 1]++;
+      nptr[ci[c * nl + a] + 1]++;
   for (int64_t r = 0; r < n; ++r)
     nptr[r + 1] += nptr[r];
   {
     std::vector<int> fill(nptr.begin(), nptr.end() - 1);
     for (int64_t c = 0; c < ncells; ++c) // ascending cells
       for (int a = 0; a < nl; ++a)
-        nlist[fill[cell_nodes[c * nl + a]]++] = static_cast<int>(int64_t(a) * ncells + c);
+        nlist[fill[ci[c * nl + a]]++] = static_cast<int>(int64_t(a) * ncells + c);
   }
   std::vector<int64_t> par;
   if (lvl > 0) {
@@ -4491,6 +4583,17 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
   GB_CUDA(L.m_nlist.alloc(nlist.size()));
   GB_CUDA(h2d(ctx->stream, L.m_nptr.p, nptr.data(), nptr.size() * sizeof(int)));
   GB_CUDA(h2d(ctx->stream, L.m_nlist.p, nlist.data(), nlist.size() * sizeof(int)));
+  L.m_nhcells = static_cast<int>(hcells.size());
+  if (!hcells.empty()) {
+    GB_CUDA(L.m_hcells.alloc(hcells.size()));
+    GB_CUDA(L.m_hopptr.alloc(hopptr.size()));
+    GB_CUDA(L.m_hops.alloc(hops.size()));
+    GB_CUDA(h2d(ctx->stream, L.m_hcells.p, hcells.data(), hcells.size() * sizeof(int)));
+    GB_CUDA(h2d(ctx->stream, L.m_hopptr.p, hopptr.data(), hopptr.size() * sizeof(int)));
+    GB_CUDA(h2d(ctx->stream, L.m_hops.p, hops.data(), hops.size() * sizeof(CondOp)));
+  }
+  if (L.has_hn())
+    GB_CUDA(L.m_hmask.alloc(n));
   L.m_assembled = false;
   L.h_parent.swap(par);
   L.mesh_dim = dim;

@@ -271,9 +271,14 @@ class Context:
 
     # ------------------------------------------------------- device assembly
     def set_mesh(self, level, dim, cells, coords, parent=None, degree=1):
-        """Q1 cells (int64 [ncells, 2^dim], local node a at corner bits
-        (a&1, a>>1&1, a>>2&1)), node coordinates [n, dim] and, above level 0,
-        the parent cell on level-1 of every cell (gb_level_set_mesh)."""
+        """Elements (int64 [ncells, nloc]: Q1 cells, local node a at corner
+        bits (a&1, a>>1&1, a>>2&1); degree 2: Q2 patches of 3^dim nodes,
+        x fastest), node coordinates [n, dim] and, above level 0, the parent
+        element on level-1 of every element (gb_level_set_mesh_degree). On a
+        level whose hanging nodes are set (load_problem does), the elements
+        hold the hanging nodes themselves; the assembly condenses them. Call it
+        after load_problem: setting the matrix or the hanging nodes again
+        drops the mesh."""
         nd = np.ascontiguousarray(cells, dtype=np.int64)
         xy = np.ascontiguousarray(coords, dtype=np.float64)
         pa = None if parent is None else np.ascontiguousarray(parent, dtype=np.int64)

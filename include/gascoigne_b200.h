@@ -315,9 +315,20 @@ int gb_functional(gb_ctx* ctx, int level, int u, int g, double* J);
  * reference-cell corner (a & 1, a >> 1 & 1, a >> 2 & 1); node coordinates
  * coords[node*dim + d]; above level 0, parent[c] = the cell of level - 1 that
  * contains cell c (for gb_assemble_levels). The level's matrix (gb_level_set_
- * matrix, block size 1, its Dirichlet dofs and no hanging nodes) must be set
- * first: every pair of nodes of a cell must be in its pattern. Setting the
- * matrix again drops the mesh. */
+ * matrix, block size 1, its Dirichlet dofs and its hanging nodes,
+ * gb_level_set_hn) must be set first: every pair of condensed nodes of a cell
+ * must be in its pattern. Setting the matrix or the hanging nodes again drops
+ * the mesh.
+ * Hanging nodes: a cell lists its own nodes, hanging ones included; the
+ * element matrix of a cell with hanging nodes is condensed on the device
+ * (CGDisc::LocalToGlobal, DofHandler/cgdisc.h:354-364, with
+ * HNStructureQ12d/Q13d/Q22d/Q23d::CondenseHanging, Discretization/Q1/
+ * hnstructureq12d.cc:129-158, hnstructureq13d.cc:275-438, Discretization/Q2/
+ * hnstructureq22d.cc:84-110, hnstructureq23d.cc:161-378): edge nodes, then
+ * face nodes, each gives way to the one parent the cell lacks, the parents it
+ * holds take the weighted row and column; the hanging rows keep a unit
+ * diagonal (HNStructure::MatrixDiag, DofHandler/cgdisc.h:634). A cell that
+ * lacks more than one parent of a hanging node, or none, is an error. */
 int gb_level_set_mesh(gb_ctx* ctx, int level, int dim, int64_t ncells,
                       const int64_t* cell_nodes, const double* coords,
                       const int64_t* parent);
@@ -326,7 +337,8 @@ int gb_level_set_mesh(gb_ctx* ctx, int level, int dim, int64_t ncells,
  * a = a_x + 3 a_y + 9 a_z at the reference coordinates (a_d / 2); integrated
  * with QuadGauss9 / HexGauss27 as LineGauss3 states its points and weights,
  * Discretization/Q1/integrationformula1d.cc:82-92; kappa per element, parents
- * = the element of level - 1 that contains it). gb_form is built for Q1 only. */
+ * = the element of level - 1 that contains it). gb_form is built for Q1
+ * levels without hanging nodes only. */
 int gb_level_set_mesh_degree(gb_ctx* ctx, int level, int dim, int degree,
                              int64_t ncells, const int64_t* cell_nodes,
                              const double* coords, const int64_t* parent);

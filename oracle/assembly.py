@@ -233,3 +233,128 @@ def uniform_patches(coord: np.ndarray, dim: int) -> np.ndarray:
         base = (2 * j * n1 + 2 * i).ravel()
         loc = np.array([b * n1 + e for b in range(3) for e in range(3)])
     return inv[base[:, None] + loc[None, :]]
+
+
+# ------------------------------------------------------------------ hanging nodes
+
+# Q2 interpolation weights of the node at 1/4 of a coarse edge (hnstructureq22d.cc,
+# hnstructureq23d.cc:35-45: wei = 0.375, 0.75, -0.125; faces: wei[i] * wei[j])
+_Q2W = (0.375, 0.75, -0.125)
+
+
+def refined_elements(coord: np.ndarray, dim: int, degree: int, N: int):
+    """Elements of a uniform mesh of N cells per direction in which some cells
+    (Q1) or patches of 2^dim cells (Q2) were refined once, found from the node
+    coordinates (every node on the 2N grid). Returns (elements [ne, nloc] in
+    the node numbering of coord, parents [ne]: the element of the uniform
+    coarser mesh - the N-cell mesh for Q1, the N/2-patch mesh for Q2 - each one
+    lies in). Coarse elements are taken lexicographically (x fastest); a refined
+    one is replaced by its 2^dim children in corner-bit order. Local node order:
+    corner bits for Q1 (as q1_shape), lexicographic 3^dim for Q2 (as q2_shape)."""
+    M = 2 * N
+    c = np.rint(coord * M).astype(np.int64)
+    lex = np.zeros(c.shape[0], dtype=np.int64)
+    for d in reversed(range(dim)):
+        lex = lex * (M + 1) + c[:, d]
+    look = np.full((M + 1) ** dim, -1, dtype=np.int64)
+    look[lex] = np.arange(c.shape[0])
+
+    def node(p):
+        k = 0
+        for d in reversed(range(dim)):
+            k = k * (M + 1) + int(p[d])
+        return int(look[k])
+
+    if degree == 1:
+        span, nc = 2, N                      # coarse cell: 2 fine units
+        offs = [[(a >> d) & 1 for d in range(dim)] for a in range(1 << dim)]
+    else:
+        span, nc = 4, N // 2                 # coarse patch: 4 fine units
+        offs = [[(a // 3 ** d) % 3 for d in range(dim)] for a in range(3 ** dim)]
+    els, par = [], []
+    for k in range(nc ** dim):
+        base = [((k // nc ** d) % nc) * span for d in range(dim)]
+        if node([b + 1 for b in base]) >= 0:  # refined: its first inner fine node exists
+            sub = span // 2
+            for ch in range(1 << dim):
+                b2 = [base[d] + sub * ((ch >> d) & 1) for d in range(dim)]
+                step = sub // (1 if degree == 1 else 2)
+                els.append([node([b2[d] + step * o[d] for d in range(dim)]) for o in offs])
+                par.append(k)
+        else:
+            step = span // (1 if degree == 1 else 2)
+            els.append([node([base[d] + step * o[d] for d in range(dim)]) for o in offs])
+            par.append(k)
+    el = np.array(els, dtype=np.int64)
+    assert (el >= 0).all(), "node missing from the refined mesh"
+    return el, np.array(par, dtype=np.int64)
+
+
+def hn_maps(level, dim: int):
+    """The level's hanging nodes as two dicts (edges, faces): node -> list of
+    (parent, weight) in the reference's parent order (HNStructureQ12d/Q13d:
+    2 edge parents 0.5, 4 face parents {0, 1, 3, 4} of the 9 with 0.25;
+    HNStructureQ22d/Q23d: 3 edge parents 0.375, 0.75, -0.125, 9 face parents
+    with the tensor products)."""
+    q2 = level.hn_disc >= 2
+    edges, faces = {}, {}
+    for row in np.asarray(level.hn_edges).reshape(-1, 4):
+        if q2:
+            edges[int(row[0])] = [(int(row[1 + j]), _Q2W[j]) for j in range(3)]
+        else:
+            edges[int(row[0])] = [(int(row[1 + j]), 0.5) for j in range(2)]
+    if level.hn_faces is not None:
+        for row in np.asarray(level.hn_faces).reshape(-1, 10):
+            if q2:
+                faces[int(row[0])] = [(int(row[1 + s]), _Q2W[s // 3] * _Q2W[s % 3])
+                                      for s in range(9)]
+            else:
+                faces[int(row[0])] = [(int(row[1 + s]), 0.25) for s in (0, 1, 3, 4)]
+    return edges, faces
+
+
+def condense(E: np.ndarray, cells: np.ndarray, hn):
+    """Element condensation of hanging nodes (CGDisc::LocalToGlobal,
+    DofHandler/cgdisc.h:354-364, with HNStructureQ12d::CondenseHanging,
+    Discretization/Q1/hnstructureq12d.cc:129-158, HNStructureQ13d,
+    Discretization/Q1/hnstructureq13d.cc:275-331 and 401-438,
+    HNStructureQ22d, Discretization/Q2/hnstructureq22d.cc:84-110, and
+    HNStructureQ23d, Discretization/Q2/hnstructureq23d.cc:161-378): edge
+    hanging nodes first, then face hanging nodes, each phase over the local
+    slots in ascending order. A hanging node h in slot s with parents p_j,
+    weights w_j: every parent already in the element (slot t_j) takes
+    column t_j += w_j column s and row t_j += w_j row s; the one parent that is
+    missing takes slot s, whose column and row are scaled by its weight
+    (C^T E C for u_h = sum w_j u_pj). Returns (E', indices')."""
+    E = np.array(E, dtype=np.float64, copy=True)
+    idx = np.array(cells, dtype=np.int64, copy=True)
+    for c in range(idx.shape[0]):
+        for phase in hn:
+            for s in range(idx.shape[1]):
+                h = int(idx[c, s])
+                if h not in phase:
+                    continue
+                where = {int(v): t for t, v in enumerate(idx[c])}
+                miss = [(p, w) for p, w in phase[h] if p not in where]
+                assert len(miss) == 1, "a hanging node needs exactly one missing parent"
+                for p, w in phase[h]:
+                    if p in where:
+                        t = where[p]
+                        E[c, :, t] += w * E[c, :, s]
+                        E[c, t, :] += w * E[c, s, :]
+                E[c, :, s] *= miss[0][1]
+                E[c, s, :] *= miss[0][1]
+                idx[c, s] = miss[0][0]
+    return E, idx
+
+
+def assemble_hn(n, rowptr, col, cells, E, dirichlet, hanging) -> np.ndarray:
+    """assemble() of condensed elements (cells: condensed indices), then the
+    hanging rows' diagonal set to 1 (HNStructure::MatrixDiag, called by
+    CGDisc::Matrix, DofHandler/cgdisc.h:634) before the Dirichlet rows."""
+    val = assemble(n, rowptr, col, cells, E, dirichlet)
+    ri = np.repeat(np.arange(n), np.diff(rowptr))
+    hm = np.zeros(n, dtype=bool)
+    hm[np.asarray(hanging, dtype=np.int64)] = True
+    val[hm[ri] & (ri == col)] = 1.0
+    return val

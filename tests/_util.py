@@ -230,3 +230,87 @@ def oracle_level_values_q2(P, kappa_elements, beta=None):
         E = q2_element_matrices(P.dim, L.coord[el], kap[l], beta)
         vals.append(assemble(L.n, L.rowptr, L.col, el, E, L.dirichlet))
     return vals, kap
+
+
+def ball_meshes(P, degree):
+    """Per level (elements, parents) of a hierarchy whose finest level is a
+    uniform mesh with some cells (Q1) or patches (Q2) refined once (hanging
+    nodes), the coarser levels uniform."""
+    import copy
+    from oracle.assembly import refined_elements
+    below = copy.copy(P)
+    below.levels = P.levels[:-1]
+    um = uniform_meshes(below) if degree == 1 else uniform_meshes_q2(below)
+    Nc = round(P.levels[-2].n ** (1.0 / P.dim)) - 1      # cells per dim below the ball level
+    el, par = refined_elements(P.finest.coord, P.dim, degree, Nc)
+    return um + [(el, par)]
+
+
+def oracle_ball_values(P, degree, kappa_elements, beta=None):
+    """The oracle's values of every level of a ball hierarchy (kappa per finest
+    element, coarser levels the mean of the children), the finest condensed."""
+    from oracle.assembly import (assemble, assemble_hn, coarsen_kappa, condense, hn_maps,
+                                 q1_element_matrices, q2_element_matrices)
+    meshes = ball_meshes(P, degree)
+    f = q1_element_matrices if degree == 1 else q2_element_matrices
+    kap = [None] * P.nlevels
+    kap[-1] = np.asarray(kappa_elements, dtype=np.float64)
+    for l in range(P.nlevels - 2, -1, -1):
+        kap[l] = coarsen_kappa(kap[l + 1], meshes[l + 1][1], meshes[l][0].shape[0])
+    vals = []
+    for l, L in enumerate(P.levels):
+        el = meshes[l][0]
+        E = f(P.dim, L.coord[el], kap[l], beta)
+        if L.hn_edges is not None:
+            hn = hn_maps(L, P.dim)
+            Ec, ic = condense(E, el, hn)
+            vals.append(assemble_hn(L.n, L.rowptr, L.col, ic, Ec, L.dirichlet,
+                                    list(hn[0]) + list(hn[1])))
+        else:
+            vals.append(assemble(L.n, L.rowptr, L.col, el, E, L.dirichlet))
+    return vals, kap
+
+
+def with_condensed_pattern(P, degree):
+    """P with the finest level's pattern replaced by the couplings of the
+    condensed elements plus every diagonal (the reference's SparseStructure of
+    a level with hanging nodes, CGDisc::Structure) and its values carried over
+    (zero where P had no entry)."""
+    import copy
+    import scipy.sparse as sp
+    from oracle.assembly import condense, hn_maps
+    el = ball_meshes(P, degree)[-1][0]
+    L = P.finest
+    hn = hn_maps(L, P.dim)
+    _, ic = condense(np.zeros((el.shape[0], el.shape[1], el.shape[1])), el, hn)
+    nl = ic.shape[1]
+    r = np.concatenate([np.repeat(ic, nl, axis=1).ravel(), np.arange(L.n)])
+    c = np.concatenate([np.tile(ic, (1, nl)).ravel(), np.arange(L.n)])
+    S = sp.coo_matrix((np.ones(r.size), (r, c)), shape=(L.n, L.n)).tocsr()
+    S.sum_duplicates()
+    S.sort_indices()
+    A = sp.csr_matrix((L.val, L.col, L.rowptr), shape=(L.n, L.n))
+    out = (abs(A) > 0).astype(np.int8) - (abs(A) > 0).multiply(S > 0).astype(np.int8)
+    out.eliminate_zeros()
+    assert out.nnz == 0, "an entry outside the element couplings"
+    rr = np.repeat(np.arange(L.n), np.diff(S.indptr))
+    vals = np.asarray(A[rr, S.indices]).ravel()
+    Q = copy.deepcopy(P)
+    F = Q.levels[-1]
+    F.rowptr = S.indptr.astype(np.int64)
+    F.col = S.indices.astype(np.int64)
+    F.val = vals
+    F.diag = np.nonzero(rr == S.indices)[0].astype(np.int64)
+    return Q
+
+
+def golden_hn_assembly_cases():
+    """Golden ball cases (hanging nodes) whose matrices the device assembly
+    rebuilds: (name, degree, constant kappa, beta)."""
+    out = []
+    for name in golden_hn_cases():
+        z = np.load(os.path.join(GOLDEN, name + ".npz"))
+        beta = ([float(t) for t in str(z["key_conv"]).split(",")] if "key_conv" in z.files
+                else None)
+        out.append((name, 2 if str(z["key_disc"]) == "Q2" else 1, float(z["key_diff"]), beta))
+    return out

@@ -4,8 +4,9 @@ with and without convection), and against the generator's assembly."""
 import numpy as np
 import pytest
 
-from _util import golden_assembly_cases, load_golden, oracle_level_values
-from gascoignelib_b200.problem import seeded_inputs, structured_problem
+from _util import (ball_meshes, golden_assembly_cases, golden_hn_assembly_cases, load_golden,
+                   oracle_ball_values, oracle_level_values, with_condensed_pattern)
+from gascoignelib_b200.problem import seeded_inputs, structured_problem, structured_q2_ball
 from oracle.assembly import q1_element_matrices
 
 
@@ -98,3 +99,46 @@ def test_oracle_q2_assembly_matches_reference(name):
     vals, _ = oracle_level_values_q2(P, q2_element_kappa(P.dim, kappa, Nc), beta)
     for L, v in zip(P.levels, vals):
         assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max()
+
+
+@pytest.mark.parametrize("name,degree,diff,beta", golden_hn_assembly_cases(),
+                         ids=[c[0] for c in golden_hn_assembly_cases()])
+def test_oracle_hn_assembly_matches_reference(name, degree, diff, beta):
+    """The condensed element matrices of a ball-refined level (hanging nodes)
+    and the uniform levels below it reproduce the reference's matrices."""
+    P, _ = load_golden(name)
+    ne = ball_meshes(P, degree)[-1][0].shape[0]
+    vals, _ = oracle_ball_values(P, degree, np.full(ne, diff), beta)
+    for l, L in enumerate(P.levels):
+        assert np.abs(vals[l] - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
+
+
+def test_oracle_hn_condensation_matches_generator():
+    """3D Q2 with hanging edge and face nodes: the oracle's element condensation
+    equals the generator's global C^T A C (whose Gauss weights are exact, hence
+    1e-12), and the generator's pattern lies inside the condensed couplings."""
+    P = with_condensed_pattern(structured_q2_ball(1, 3, eps=0.1), 2)
+    assert P.finest.hn_faces.shape[0] > 0 and P.finest.hn_edges.shape[0] > 0
+    ne = ball_meshes(P, 2)[-1][0].shape[0]
+    vals, _ = oracle_ball_values(P, 2, np.full(ne, 0.1), (1.0, 0.5, 0.25))
+    for l, L in enumerate(P.levels):
+        assert np.abs(vals[l] - L.val).max() <= 1e-12 * np.abs(L.val).max(), l
+
+
+def test_condense_plants():
+    """A planted wrong weight changes the condensed matrix (the comparison is
+    sensitive to the condensation), and a cell holding every parent of its
+    hanging node is rejected."""
+    from oracle.assembly import condense
+    E = np.arange(16.0).reshape(1, 4, 4) + 1.0
+    cells = np.array([[0, 1, 2, 3]])
+    Eg, ig = condense(E, cells, ({1: [(0, 0.5), (7, 0.5)]}, {}))
+    Eb, _ = condense(E, cells, ({1: [(0, 0.5), (7, 0.25)]}, {}))
+    assert ig.tolist() == [[0, 7, 2, 3]] and not np.allclose(Eg, Eb)
+    # C^T E C with u_1 = (u_0 + u_7) / 2, the element now on (0, 7, 2, 3)
+    C = np.zeros((4, 4))
+    C[0, 0] = C[2, 2] = C[3, 3] = 1.0
+    C[1, 0] = C[1, 1] = 0.5
+    assert np.allclose(Eg[0], C.T @ E[0] @ C)
+    with pytest.raises(AssertionError):
+        condense(E, cells, ({1: [(0, 0.5), (2, 0.5)]}, {}))
