@@ -450,7 +450,7 @@ def q2_c4(local, steps, warmup, flush):
     import torch
 
     from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
-    from gascoignelib_b200.problem import structured_q2, structured_q2_ball
+    from gascoignelib_b200.problem import q2_meshes, structured_q2, structured_q2_ball
 
     def run(P):
         c = Context(local)
@@ -479,50 +479,50 @@ def q2_c4(local, steps, warmup, flush):
         res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
         return res
 
+    def assembly_ms(P):
+        """Median device time of assembling every level (Q2 elements, the
+        finest level's hanging nodes condensed) from a per-element
+        coefficient, L2 flushed before each."""
+        c = Context(local)
+        c.load_problem(P)
+        meshes = q2_meshes(P)
+        for l, (el, par) in enumerate(meshes):
+            c.set_mesh(l, 3, el, P.levels[l].coord, par, degree=2)
+        dev = torch.device(f"cuda:{local}")
+        kd = torch.full((meshes[-1][0].shape[0],), 1e-2, dtype=torch.float64, device=dev)
+        st = torch.cuda.ExternalStream(c.stream(), device=dev)
+        for _ in range(warmup):
+            c.assemble_levels(kd, (1.0, 0.5, 0.25))
+        ms = []
+        for _ in range(steps):
+            flush.random_(0, 255)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            c.assemble_levels(kd, (1.0, 0.5, 0.25))
+            e1.record(st)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        c.close()
+        return sorted(ms)[len(ms) // 2]
+
     P = structured_q2_ball(5, 4, eps=1e-2, beta=(1.0, 0.5, 0.25), radius=0.25)
     out = run(P)
     out["workload"] = ("3D CGQ2 convection-diffusion eps 1e-2, beta (1,0.5,0.25), 80^3 cells "
                        "refined once inside |x-0.5|<0.25, %d dofs, %d hanging, 5 levels, "
                        "Jacobi V(2,2) omega 0.3, GMRES(30), tol 1e-8"
                        % (P.finest.ndof, P.info["hanging"]))
+    # device assembly of the ball hierarchy (5 levels; 93,568 elements of 27
+    # nodes on the finest, 6,896 of them with hanging nodes condensed)
+    out["assembly_ms"] = assembly_ms(P)
     del P
     U = structured_q2(3, 5, 4, eps=1e-2, beta=(1.0, 0.5, 0.25))
     out["uniform_no_ball"] = run(U)
     out["uniform_no_ball"]["workload"] = "the same on the uniform 80^3 cells, 531,441 dofs"
     # device assembly of the uniform Q2 hierarchy (4 levels, 40^3 elements of
-    # 27 nodes on the finest) from a per-element coefficient
-    import numpy as np
-    from gascoignelib_b200.problem import cell_parents
-
-    c = Context(local)
-    c.load_problem(U)
-    for l, L in enumerate(U.levels):
-        Np = (round(L.n ** (1.0 / 3)) - 1) // 2
-        n1 = 2 * Np + 1
-        k, j, i = np.meshgrid(np.arange(Np), np.arange(Np), np.arange(Np), indexing="ij")
-        base = ((2 * k * n1 + 2 * j) * n1 + 2 * i).ravel()
-        loc = np.array([(a * n1 + b) * n1 + e for a in range(3) for b in range(3)
-                        for e in range(3)])
-        c.set_mesh(l, 3, base[:, None] + loc[None, :], L.coord,
-                   cell_parents(3, Np) if l else None, degree=2)
-    kd = torch.full((40 ** 3,), 1e-2, dtype=torch.float64, device=f"cuda:{local}")
-    dev = torch.device(f"cuda:{local}")
-    st = torch.cuda.ExternalStream(c.stream(), device=dev)
-    for _ in range(warmup):
-        c.assemble_levels(kd, (1.0, 0.5, 0.25))
-    ms = []
-    for _ in range(steps):
-        flush.random_(0, 255)
-        torch.cuda.synchronize(dev)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        c.assemble_levels(kd, (1.0, 0.5, 0.25))
-        e1.record(st)
-        e1.synchronize()
-        ms.append(e0.elapsed_time(e1))
-    c.close()
-    out["uniform_no_ball"]["assembly_ms"] = sorted(ms)[len(ms) // 2]
+    # 27 nodes on the finest)
+    out["uniform_no_ball"]["assembly_ms"] = assembly_ms(U)
     return out
 
 

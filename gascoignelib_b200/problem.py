@@ -638,10 +638,14 @@ def structured_q2_ball(coarse: int, refine: int, eps: float = 1e-2,
     quadratic edge trace (3 parents, weights 3/8, 6/8, -1/8, nearest first),
     face nodes on its face (9 parents, tensor weights) - the hnq2 / hnq2face
     maps and weights of HNStructureQ23d. The matrix is condensed
-    (C^T A C with the hanging rows and columns replaced by identity), strong
-    zero Dirichlet on the boundary; transfers to the uniform level below are the
-    nodal c2f / zweier / vierer / achter maps. The refinement rule is this
-    generator's own (whole patches by centre), not the reference's."""
+    (C^T A C with the hanging rows and columns replaced by identity) on the
+    pattern of the condensed elements' couplings plus every diagonal (as
+    CGDisc::Structure builds it), strong zero Dirichlet on the boundary;
+    transfers to the uniform level below are the nodal c2f / zweier / vierer /
+    achter maps. The refinement rule is this generator's own (whole patches by
+    centre), not the reference's. info["elements"] / info["parents"]: the
+    finest level's Q2 elements (27 nodes, x fastest, hanging nodes included)
+    and the patch of the level below each lies in, for the device assembly."""
     import scipy.sparse as sp
     dim = 3
     base = structured_q2(dim, coarse, refine, eps=eps, beta=beta, seed=seed)
@@ -751,9 +755,29 @@ def structured_q2_ball(coarse: int, refine: int, eps: float = 1e-2,
     Cm = sp.coo_matrix((np.concatenate(cv), (np.concatenate(cr), np.concatenate(cc))),
                        shape=(n, n)).tocsr()
     Ac = (Cm.T @ A @ Cm).tocsr()
-    Ac = Ac + sp.coo_matrix((np.ones(hang.size), (hang, hang)), shape=(n, n)).tocsr()
     Ac.sum_duplicates()
     Ac.sort_indices()
+    # the pattern is the condensed elements' couplings plus every diagonal (a
+    # product of nonnegative patterns: couplings whose values cancel stay)
+    Cp = Cm.copy()
+    Cp.data[:] = 1.0
+    Ap = A.copy()
+    Ap.data[:] = 1.0
+    Sp = (Cp.T @ (Ap + sp.identity(n, format="csr")) @ Cp).tocsr()
+    Sp = (Sp + sp.coo_matrix((np.ones(hang.size), (hang, hang)), shape=(n, n))).tocsr()
+    Sp.sum_duplicates()
+    Sp.sort_indices()
+    ks = np.repeat(np.arange(n, dtype=np.int64), np.diff(Sp.indptr)) * n + Sp.indices
+    ka = np.repeat(np.arange(n, dtype=np.int64), np.diff(Ac.indptr)) * n + Ac.indices
+    at = np.searchsorted(ks, ka)
+    assert np.array_equal(ks[at], ka)
+    vals = np.zeros(ks.size)
+    vals[at] = Ac.data
+    hrow = np.zeros(n, dtype=bool)
+    hrow[hang] = True
+    vals[hrow[ks // n] & (ks // n == Sp.indices)] = 1.0   # hanging rows: identity
+    Sp.data = vals
+    Ac = Sp
     onb = np.any((allp == 0) | (allp == M2), axis=1)
     rowptr = Ac.indptr.astype(np.int64)
     col = Ac.indices.astype(np.int64)
@@ -793,4 +817,33 @@ def structured_q2_ball(coarse: int, refine: int, eps: float = 1e-2,
     return Problem(dim=dim, levels=base.levels + [fine], transfers=base.transfers + [tr],
                    rhs=b, info={"generator": "structured-q2-ball", "coarse": coarse,
                                 "refine": refine, "eps": eps, "radius": radius,
-                                "hanging": int(hang.size), "refined_patches": int(rp.shape[0])})
+                                "hanging": int(hang.size), "refined_patches": int(rp.shape[0]),
+                                "elements": np.concatenate([el_c, el_f]).astype(np.int64),
+                                "parents": np.concatenate([
+                                    (up[:, 2] * P + up[:, 1]) * P + up[:, 0],
+                                    np.repeat((rp[:, 2] * P + rp[:, 1]) * P + rp[:, 0], 8)
+                                ]).astype(np.int64)})
+
+
+def q2_meshes(prob: Problem):
+    """Per level (Q2 elements [ne, 3^dim], parent element on the level below
+    or None) of a structured_q2 / structured_q2_ball problem, for
+    gb_level_set_mesh_degree: uniform levels as lexicographic patches, a ball
+    level as the generator recorded it."""
+    out = []
+    for l, L in enumerate(prob.levels):
+        if l == prob.nlevels - 1 and "elements" in prob.info:
+            out.append((prob.info["elements"], prob.info["parents"]))
+            continue
+        dim = prob.dim
+        Np = (round(L.n ** (1.0 / dim)) - 1) // 2
+        n1 = 2 * Np + 1
+        g = np.meshgrid(*([np.arange(Np)] * dim), indexing="ij")
+        base = 0
+        for d in range(dim):                       # g[0] slowest (z), g[-1] x
+            base = base * n1 + 2 * g[d].ravel()
+        loc = np.zeros(1, dtype=np.int64)
+        for d in range(dim):
+            loc = (loc[:, None] * n1 + np.arange(3)[None, :]).ravel()
+        out.append((base[:, None] + loc[None, :], cell_parents(dim, Np) if l else None))
+    return out

@@ -314,3 +314,22 @@ def golden_hn_assembly_cases():
                 else None)
         out.append((name, 2 if str(z["key_disc"]) == "Q2" else 1, float(z["key_diff"]), beta))
     return out
+
+
+def reference_ball_3d(disc, diff, conv=None):
+    """Runs the compiled reference on the 3D ball case (coarse 2, refine 3,
+    ball 0.25: edge and face hanging nodes) and returns (problem, summary,
+    output directory). A ball on a coarser 3D mesh refines every cell (the
+    mesh's patch rules), so no smaller 3D case has hanging nodes."""
+    import tempfile
+    from gascoignelib_b200.problem import load_reference_dump
+    from oracle.oracle import run_reference, write_inputs
+    d = tempfile.mkdtemp()
+    res = 2 * (2 << 3)
+    rhs = np.random.default_rng(1002).uniform(-1.0, 1.0, size=(res + 1) ** 3)
+    keys = dict(threads=1, dim=3, coarse=2, refine=3, disc=disc, ball=0.25, diff=diff,
+                rhsres=res, dump=1, tol=1e-8)
+    if conv is not None:
+        keys["conv"] = ",".join(str(c) for c in conv)
+    out, summ = run_reference(d, **keys, **write_inputs(d, None, rhs))
+    return load_reference_dump(out), summ, out

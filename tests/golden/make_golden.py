@@ -67,11 +67,6 @@ CASES = {
     "hn_2d_q2_c2_r3_conv_ball": (2, 2, 3, True, 1e-10,
                                  {"disc": "Q2", "ball": 0.25, "diff": 0.1,
                                   "conv": "1,0.5"}),
-    "hn_3d_q1_c1_r3_ball": (3, 1, 3, True, 1e-8,
-                            {"disc": "Q1", "ball": 0.25, "diff": 1.0}),
-    "hn_3d_q2_c1_r3_conv_ball": (3, 1, 3, True, 1e-8,
-                                 {"disc": "Q2", "ball": 0.25, "diff": 0.1,
-                                  "conv": "1,0.5,0.25"}),
 }
 
 

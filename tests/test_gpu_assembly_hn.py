@@ -1,17 +1,19 @@
 """Device assembly on levels with hanging nodes (one more refinement of a
 ball): the element matrices of the cells with hanging nodes condensed on the
-device, against the reference's matrices (golden ball cases, 2D and 3D, Q1
-and Q2), the oracle's condensation, the 3D Q2 ball generator, and the solves
-on the assembled levels."""
+device, against the reference's matrices (2D golden ball cases; 3D cases run
+on the compiled reference; Q1 and Q2), the oracle's condensation, the 3D Q2
+ball generator, and the solves on the assembled levels."""
 import copy
+import os
 
 import numpy as np
 import pytest
 
 from _util import (ball_meshes, golden_hn_assembly_cases, load_golden, oracle_ball_values,
-                   rel_l2, solver_keys, with_condensed_pattern)
+                   reference_ball_3d, rel_l2, solver_keys, with_condensed_pattern)
 from gascoignelib_b200.native import GB_FP32, GBError
-from gascoignelib_b200.problem import structured_q2_ball
+from gascoignelib_b200.problem import q2_meshes, structured_q2_ball
+from oracle.oracle import REF_HARNESS
 
 pytestmark = pytest.mark.gpu
 
@@ -61,6 +63,32 @@ def test_hn_assembly_matches_reference_and_solves(ctx, name, degree, diff, beta)
     ctx.free(b)
 
 
+@pytest.mark.skipif(not os.path.exists(REF_HARNESS), reason="compiled reference not present")
+@pytest.mark.parametrize("disc,diff,conv", [("Q1", 1.0, None), ("Q2", 0.1, (1.0, 0.5, 0.25))])
+def test_hn_assembly_3d_against_reference(ctx, disc, diff, conv):
+    """3D ball refinement (edge and face hanging nodes, Q13d / Q23d): the
+    device-assembled levels against the reference's matrices, then the solve
+    against the reference's iteration count and solution."""
+    P, summ, out = reference_ball_3d(disc, diff, conv)
+    assert P.finest.hn_faces.shape[0] > 0 and P.finest.hn_edges.shape[0] > 0
+    degree = 2 if disc == "Q2" else 1
+    ctx.load_problem(_zero_values(P))
+    meshes = _set_ball_meshes(ctx, P, degree)
+    ctx.assemble_levels(np.full(meshes[-1][0].shape[0], diff), conv)
+    for l, L in enumerate(P.levels):
+        v = ctx.level_values(l, L.val.size)
+        assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
+    ctx.set_params(gmressize=21, tol=1e-8, globaltol=1e-16, maxiter=100)
+    fl = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(fl, b, P.rhs)
+    info = ctx.gmres(x, b)
+    assert abs(info["iterations"] - int(summ["iterations"][0])) <= 1
+    assert rel_l2(ctx.download(fl, x), np.fromfile(os.path.join(out, "solution.f64"))) < 1e-8
+    ctx.free(x)
+    ctx.free(b)
+
+
 @pytest.mark.parametrize("coarse,refine", [(1, 4), (2, 5)])
 def test_hn_assembly_matches_q2_ball_generator(ctx, coarse, refine):
     """3D Q2 with hanging edge and face nodes: the device's condensed element
@@ -70,9 +98,18 @@ def test_hn_assembly_matches_q2_ball_generator(ctx, coarse, refine):
     ctx.load_problem(_zero_values(P))
     meshes = _set_ball_meshes(ctx, P, 2)
     ctx.assemble_levels(np.full(meshes[-1][0].shape[0], 0.1), (1.0, 0.5, 0.25))
+    first = []
     for l, L in enumerate(P.levels):
         v = ctx.level_values(l, L.val.size)
         assert np.abs(v - L.val).max() <= 1e-12 * np.abs(L.val).max(), l
+        first.append(v)
+    # the generator's own element lists (q2_meshes, the bench's meshes)
+    for l, (el, par) in enumerate(q2_meshes(P)):
+        ctx.set_mesh(l, 3, el, P.levels[l].coord, par, degree=2)
+    ctx.assemble_levels(np.full(P.info["elements"].shape[0], 0.1), (1.0, 0.5, 0.25))
+    for l, L in enumerate(P.levels):
+        v = ctx.level_values(l, L.val.size)
+        assert np.abs(v - first[l]).max() <= 1e-13 * np.abs(first[l]).max(), l
     ctx.set_params(tol=1e-8, globaltol=1e-300, maxiter=300, gmressize=21, omega=0.8)
     fl = P.nlevels - 1
     x, b = ctx.vec(), ctx.vec()

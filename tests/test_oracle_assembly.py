@@ -1,13 +1,17 @@
 """The oracle's Q1 assembly (oracle/assembly.py) against the matrices the
 reference assembled (golden fixtures: every level, seeded per-cell kappa,
 with and without convection), and against the generator's assembly."""
+import os
+
 import numpy as np
 import pytest
 
 from _util import (ball_meshes, golden_assembly_cases, golden_hn_assembly_cases, load_golden,
-                   oracle_ball_values, oracle_level_values, with_condensed_pattern)
+                   oracle_ball_values, oracle_level_values, reference_ball_3d,
+                   with_condensed_pattern)
 from gascoignelib_b200.problem import seeded_inputs, structured_problem, structured_q2_ball
 from oracle.assembly import q1_element_matrices
+from oracle.oracle import REF_HARNESS
 
 
 @pytest.mark.parametrize("name,kappa,beta", golden_assembly_cases(),
@@ -142,3 +146,17 @@ def test_condense_plants():
     assert np.allclose(Eg[0], C.T @ E[0] @ C)
     with pytest.raises(AssertionError):
         condense(E, cells, ({1: [(0, 0.5), (2, 0.5)]}, {}))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_HARNESS), reason="compiled reference not present")
+@pytest.mark.parametrize("disc,diff,conv", [("Q1", 1.0, None), ("Q2", 0.1, (1.0, 0.5, 0.25))])
+def test_oracle_hn_assembly_3d_live(disc, diff, conv):
+    """3D ball refinement (edge and face hanging nodes, HNStructureQ13d /
+    Q23d condensation): the oracle's levels against the reference's matrices."""
+    P, _, _ = reference_ball_3d(disc, diff, conv)
+    assert P.finest.hn_faces.shape[0] > 0 and P.finest.hn_edges.shape[0] > 0
+    degree = 2 if disc == "Q2" else 1
+    ne = ball_meshes(P, degree)[-1][0].shape[0]
+    vals, _ = oracle_ball_values(P, degree, np.full(ne, diff), conv)
+    for l, L in enumerate(P.levels):
+        assert np.abs(vals[l] - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
