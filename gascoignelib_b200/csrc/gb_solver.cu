@@ -4722,6 +4722,83 @@ gb_vec_write_backup(gb_ctx* ctx, int lvl, int id, const char* path, int binary)
 }
 
 int
+gb_vec_write_vtk(gb_ctx* ctx, int lvl, int id, const char* name, int step, int dim,
+                 int64_t ncells, int nodes_per_cell, const int64_t* cell_nodes,
+                 const double* coords, double time, const char* title)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(name && cell_nodes && coords, GB_EINVAL, "null argument");
+  GB_REQUIRE(dim == 2 || dim == 3, GB_EINVAL, "dim must be 2 or 3");
+  GB_REQUIRE(nodes_per_cell == (1 << dim), GB_EINVAL,
+             "cells need 4 (2D) or 8 (3D) nodes");
+  GB_REQUIRE(ncells >= 0 && step >= 0, GB_EINVAL, "bad cell count or step");
+  for (int64_t k = 0; k < ncells * nodes_per_cell; ++k)
+    GB_REQUIRE(cell_nodes[k] >= 0 && cell_nodes[k] < L.n, GB_EINVAL,
+               "cell node out of range");
+  // the hanging values averaged (CGDisc::VisuVtk) on a copy of the vector
+  std::vector<double> v(L.ndof());
+  const double* src = vec(*ctx, lvl, id);
+  if (L.has_hn()) {
+    DeviceArray<double> t;
+    GB_CUDA(t.alloc(v.size()));
+    GB_CUDA(cudaMemcpyAsync(t.p, src, v.size() * sizeof(double), cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+    Emit<double> E{ *ctx, nullptr };
+    E.hn_average(lvl, t.p);
+    GB_CUDA(cudaMemcpyAsync(v.data(), t.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  } else {
+    GB_CUDA(cudaMemcpyAsync(v.data(), src, v.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  // Visualization::step + compose_name: <name>.%05d, then ".vtk"
+  char fn[4096];
+  GB_REQUIRE(std::snprintf(fn, sizeof fn, "%s.%05d.vtk", name, step) < int(sizeof fn),
+             GB_EINVAL, "file name too long");
+  FILE* f = std::fopen(fn, "w");
+  GB_REQUIRE(f, GB_EINVAL, std::string("cannot open ") + fn + " for writing");
+  // Visualization::vtk (Discretization/Q1/vtk.cc): legacy ASCII; doubles as a
+  // C++ stream prints them by default (%g, 6 digits); a vertex prints each
+  // coordinate followed by a tab, 2D points add " 0"
+  bool ok = std::fprintf(f, "# vtk DataFile Version 2.0 \noutput from GascoigneStd, %s\n"
+                            "ASCII\nDATASET UNSTRUCTURED_GRID\nFIELD FieldData 1\n"
+                            "TIME 1 1 double\n%g\n", title ? title : "", time) > 0;
+  ok = ok && std::fprintf(f, "POINTS %lld DOUBLE \n", (long long)L.n) > 0;
+  for (int64_t i = 0; i < L.n && ok; ++i) {
+    for (int d = 0; d < dim && ok; ++d)
+      ok = std::fprintf(f, "%g\t", coords[i * dim + d]) > 0;
+    ok = ok && std::fputs(dim == 2 ? " 0\n" : "\n", f) >= 0;
+  }
+  ok = ok && std::fprintf(f, "\n\nCELLS %lld %lld\n", (long long)ncells,
+                          (long long)(ncells * (nodes_per_cell + 1))) > 0;
+  for (int64_t c = 0; c < ncells && ok; ++c) {
+    ok = std::fprintf(f, "%d ", nodes_per_cell) > 0;
+    for (int a = 0; a < nodes_per_cell && ok; ++a)
+      ok = std::fprintf(f, "%lld ", (long long)cell_nodes[c * nodes_per_cell + a]) > 0;
+    ok = ok && std::fputc('\n', f) != EOF;
+  }
+  ok = ok && std::fprintf(f, "\nCELL_TYPES %lld\n", (long long)ncells) > 0;
+  for (int64_t c = 0; c < ncells && ok; ++c)
+    ok = std::fputs(dim == 2 ? "9 " : "12 ", f) >= 0;
+  ok = ok && std::fputc('\n', f) != EOF;
+  // _vtk_pointdata: one scalar per component, u000, u001, ...
+  for (int comp = 0; comp < L.B && ok; ++comp) {
+    if (comp == 0)
+      ok = std::fprintf(f, "POINT_DATA %lld\n", (long long)L.n) > 0;
+    ok = ok && std::fprintf(f, "SCALARS u%03d DOUBLE \nLOOKUP_TABLE default\n", comp) > 0;
+    for (int64_t i = 0; i < L.n && ok; ++i)
+      ok = std::fprintf(f, "%g\n", v[i * L.B + comp]) > 0;
+    ok = ok && std::fputs("\n\n", f) >= 0;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  GB_REQUIRE(ok, GB_EINVAL, std::string("write error on ") + fn);
+  GB_API_END
+}
+
+int
 gb_vec_read_backup(gb_ctx* ctx, int lvl, int id, const char* path, int binary, int add)
 {
   GB_API_BEGIN

@@ -117,6 +117,8 @@ _SIGS = {
     "gb_newton_residual": [C.c_void_p, C.c_int, C.c_int, C.c_int, _PD],
     "gb_vec_write_backup": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_int],
     "gb_vec_read_backup": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_int],
+    "gb_vec_write_vtk": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_int,
+                         C.c_int64, C.c_int, _P64, _PD, C.c_double, C.c_char_p],
     "gb_ctx_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
@@ -329,6 +331,15 @@ class Context:
 
     def write_backup(self, level, vid, path, binary=False):
         self._chk(self._L.gb_vec_write_backup(self.h, level, vid, path.encode(), int(binary)))
+
+    def write_vtk(self, level, vid, name, step, dim, cells, coords, time=0.0, title=""):
+        """gb_vec_write_vtk: <name>.<step %05d>.vtk with the mesh's cells
+        (int64 [ncells, 2^dim], the mesh's vertex order) and node coordinates."""
+        cl = np.ascontiguousarray(cells, dtype=np.int64)
+        xy = np.ascontiguousarray(coords, dtype=np.float64)
+        self._chk(self._L.gb_vec_write_vtk(self.h, level, vid, name.encode(), int(step), dim,
+                                           cl.shape[0], cl.shape[1], _p64(cl), _pd(xy),
+                                           float(time), title.encode()))
 
     def read_backup(self, level, vid, path, binary=False, add=False):
         self._chk(self._L.gb_vec_read_backup(self.h, level, vid, path.encode(), int(binary),

@@ -386,6 +386,21 @@ int gb_newton_residual(gb_ctx* ctx, int y, int x, int b, double* norm);
 int gb_vec_write_backup(gb_ctx* ctx, int level, int id, const char* path, int binary);
 int gb_vec_read_backup(gb_ctx* ctx, int level, int id, const char* path, int binary,
                        int add);
+/* The vector as the reference's VTK file (StdSolver::Visu -> CGDisc::VisuVtk,
+ * DofHandler/cgdisc.h:136-158, and Visualization::vtk,
+ * Discretization/Q1/vtk.cc:29-244): <name>.<step as %05d>.vtk, legacy ASCII
+ * unstructured grid with the level's nodes (coords[node*dim + d]) and the
+ * mesh's cells (ncells x nodes_per_cell node indices in the mesh's vertex
+ * order: counterclockwise quads, hexes bottom face then top face; VTK cell
+ * types 9 / 12), the given time and title in the header, and one scalar per
+ * component named u000, u001, ... (the names of a problem without a
+ * ComponentInformation of its own). Numbers are printed as a C++ stream prints
+ * them by default (6 significant digits). On a level with hanging nodes the
+ * written values are HNAverage'd; the vector itself is not changed (the
+ * reference averages in place and zeroes the hanging values after). */
+int gb_vec_write_vtk(gb_ctx* ctx, int level, int id, const char* name, int step, int dim,
+                     int64_t ncells, int nodes_per_cell, const int64_t* cell_nodes,
+                     const double* coords, double time, const char* title);
 /* The context's CUDA stream (a cudaStream_t): every gb_* call enqueues its
  * work there, so callers can order their own work or record events on it. */
 int gb_ctx_get_stream(const gb_ctx* ctx, void** stream);

@@ -57,6 +57,7 @@
 //   dual_rhs.f64 dual_solution.f64, and with dump=1 L<l>_dualval.f64 (the
 //   dual matrices' values in the stencil of L<l>_col.i64)
 // backup=1: solution.bup and solution.bip (WriteBackUp, WriteBackUpBinary);
+// vtk=1: solution.00000.vtk (StdSolver::Visu);
 // formx=<raw f64 finest-level vector x>: form.f64 = Form(0, x, 1),
 //   newton_residual.f64 = NewtonResidual(x, rhs) and newton.txt (its norm).
 #include "backup.h"
@@ -110,6 +111,7 @@ struct Config
   double ball = 0.0, diff = -1.0;
   int rhsres = 0;
   int backup = 0;     // write the solution with WriteBackUp / WriteBackUpBinary
+  int vtk = 0;        // write the solution with StdSolver::Visu (VTK)
   std::string formx;  // Form and NewtonResidual of this finest-level vector
 };
 
@@ -309,6 +311,7 @@ parse(int argc, char** argv)
     else if (k == "mgtype") c.mgtype = v;
     else if (k == "dump") c.dump = atoi(v.c_str());
     else if (k == "backup") c.backup = atoi(v.c_str());
+    else if (k == "vtk") c.vtk = atoi(v.c_str());
     else if (k == "formx") c.formx = v;
     else if (k == "repeat") c.repeat = atoi(v.c_str());
     else if (k == "patchdepth") c.patchdepth = atoi(v.c_str());
@@ -808,6 +811,11 @@ main(int argc, char** argv)
       WriteBackUp(U, c.out + "/solution");
       WriteBackUpBinary(U, c.out + "/solution");
     }
+    // StdSolver::Visu -> CGDisc::VisuVtk (DofHandler/cgdisc.h:136-158): the
+    // finest level's solution as solution.00000.vtk (Visualization::vtk,
+    // Discretization/Q1/vtk.cc), hanging values averaged first
+    if (c.vtk)
+      S->Visu(c.out + "/solution", u, 0);
     // StdSolver::Form (Solver/stdsolver.cc:1041-1063) of a given vector with
     // d = 1 on the finest level, and StdMultiLevelSolver::NewtonResidual
     // (Solver/stdmultilevelsolver.cc:609-623) y = f - Form(x), boundary zero,

@@ -61,7 +61,7 @@ def load_golden(name):
                    dual_residual=float(z["dual_residual"]),
                    dual_status=str(z["dual_status"]),
                    dualval=[z[f"L{l}_dualval"] for l in range(nl)])
-    for k in ("formx", "form", "newton_residual", "backup_bup", "backup_bip"):
+    for k in ("formx", "form", "newton_residual", "backup_bup", "backup_bip", "vtk"):
         if k in z.files:
             ref[k] = z[k]
     if "newton_norm" in z.files:
@@ -333,3 +333,22 @@ def reference_ball_3d(disc, diff, conv=None):
         keys["conv"] = ",".join(str(c) for c in conv)
     out, summ = run_reference(d, **keys, **write_inputs(d, None, rhs))
     return load_reference_dump(out), summ, out
+
+
+def golden_vtk_cases():
+    """Golden cases that hold the reference's VTK file of the solution."""
+    out = []
+    for n in golden_cases():
+        with np.load(os.path.join(GOLDEN, n + ".npz")) as z:
+            if "vtk" in z.files:
+                out.append(n)
+    return out
+
+
+def vtk_cells(vtk_bytes):
+    """The CELLS section of a legacy VTK file: int64 [ncells, nodes per cell]."""
+    lines = bytes(vtk_bytes).decode().split("\n")
+    i = next(k for k, s in enumerate(lines) if s.startswith("CELLS "))
+    ne = int(lines[i].split()[1])
+    rows = [[int(t) for t in lines[i + 1 + c].split()][1:] for c in range(ne)]
+    return np.array(rows, dtype=np.int64)

@@ -18,7 +18,8 @@ cases are CGQ2 elements with the seeded per-cell kappa. The "ilu_"
 cases use linear_smooth ilu with matrixtype block (SparseBlockIlu). The "form_"
 cases also record StdSolver::Form and StdMultiLevelSolver::NewtonResidual of a
 seeded vector and the solution as written by WriteBackUp (.bup) and
-WriteBackUpBinary (.bip).
+WriteBackUpBinary (.bip); cases with "vtk" the solution as StdSolver::Visu
+writes it (VTK).
 
     python tests/golden/make_golden.py
 """
@@ -60,10 +61,10 @@ CASES = {
     "q2_3d_c1_r3_kappa_conv": (3, 1, 3, True, 1e-8, {"disc": "Q2", "conv": "1,0.5,0.25"}),
     "q2_2d_c2_r3_kappa": (2, 2, 3, True, 1e-10, {"disc": "Q2"}),
     "form_3d_c1_r3_conv": (3, 1, 3, True, 1e-8, {"conv": "1,0.5,0.25", "backup": 1,
-                                                 "formx": 1005}),
-    "form_2d_c2_r3": (2, 2, 3, True, 1e-10, {"backup": 1, "formx": 1006}),
+                                                 "formx": 1005, "vtk": 1}),
+    "form_2d_c2_r3": (2, 2, 3, True, 1e-10, {"backup": 1, "formx": 1006, "vtk": 1}),
     "hn_2d_q1_c2_r3_ball": (2, 2, 3, True, 1e-10,
-                            {"disc": "Q1", "ball": 0.25, "diff": 1.0}),
+                            {"disc": "Q1", "ball": 0.25, "diff": 1.0, "vtk": 1}),
     "hn_2d_q2_c2_r3_conv_ball": (2, 2, 3, True, 1e-10,
                                  {"disc": "Q2", "ball": 0.25, "diff": 0.1,
                                   "conv": "1,0.5"}),
@@ -158,6 +159,9 @@ def make(name, dim, coarse, refine, seeded, tol, extra):
         arrs["newton_residual"] = np.fromfile(os.path.join(out, "newton_residual.f64"))
         with open(os.path.join(out, "newton.txt")) as f:
             arrs["newton_norm"] = float(f.read().split()[1])
+    if keys.get("vtk"):
+        with open(os.path.join(out, "solution.00000.vtk"), "rb") as f:
+            arrs["vtk"] = np.frombuffer(f.read(), dtype=np.uint8)
     if keys.get("backup"):
         for ext in ("bup", "bip"):
             with open(os.path.join(out, "solution." + ext), "rb") as f:

@@ -1,14 +1,15 @@
 """Matrix-free Form, the Newton residual and the solution files on the GPU:
 StdSolver::Form / StdMultiLevelSolver::NewtonResidual of a seeded vector and
-the WriteBackUp / WriteBackUpBinary files, against what the reference itself
-computed and wrote (golden fixtures)."""
+the WriteBackUp / WriteBackUpBinary files and the StdSolver::Visu VTK file,
+against what the reference itself computed and wrote (golden fixtures)."""
 import os
 import tempfile
 
 import numpy as np
 import pytest
 
-from _util import golden_form_cases, golden_kappa_beta, load_golden, set_uniform_meshes
+from _util import (golden_form_cases, golden_kappa_beta, golden_vtk_cases, load_golden,
+                   set_uniform_meshes, vtk_cells)
 from gascoignelib_b200.native import GBError
 
 pytestmark = pytest.mark.gpu
@@ -79,4 +80,27 @@ def test_backup_files_match_reference(ctx, name):
         ctx.read_backup(0, u, os.path.join(d, "solution.bup"))
     with pytest.raises(GBError, match="not found"):
         ctx.read_backup(fl, u, os.path.join(d, "missing.bup"))
+    ctx.free(u)
+
+
+@pytest.mark.parametrize("name", golden_vtk_cases())
+def test_vtk_file_matches_reference(ctx, name):
+    """gb_vec_write_vtk writes the reference's VTK file (StdSolver::Visu) byte
+    for byte from the device vector, the level's coordinates and the mesh's
+    cells; on a level with hanging nodes the written values are averaged and
+    the vector is left as it was."""
+    P, ref = load_golden(name)
+    ctx.load_problem(P)
+    fl = P.nlevels - 1
+    u = ctx.vec()
+    ctx.upload(fl, u, ref["solution"])
+    d = tempfile.mkdtemp()
+    ctx.write_vtk(fl, u, os.path.join(d, "mine"), 0, P.dim, vtk_cells(ref["vtk"]),
+                  P.finest.coord)
+    assert open(os.path.join(d, "mine.00000.vtk"), "rb").read() == ref["vtk"].tobytes()
+    assert np.array_equal(ctx.download(fl, u), ref["solution"])
+    with pytest.raises(GBError, match="out of range"):
+        bad = vtk_cells(ref["vtk"])
+        bad[0, 0] = P.finest.n
+        ctx.write_vtk(fl, u, os.path.join(d, "bad"), 0, P.dim, bad, P.finest.coord)
     ctx.free(u)

@@ -6,9 +6,9 @@ import os
 import numpy as np
 import pytest
 
-from _util import (ball_meshes, golden_assembly_cases, golden_hn_assembly_cases, load_golden,
-                   oracle_ball_values, oracle_level_values, reference_ball_3d,
-                   with_condensed_pattern)
+from _util import (ball_meshes, golden_assembly_cases, golden_hn_assembly_cases, golden_vtk_cases,
+                   load_golden, oracle_ball_values, oracle_level_values, reference_ball_3d,
+                   vtk_cells, with_condensed_pattern)
 from gascoignelib_b200.problem import seeded_inputs, structured_problem, structured_q2_ball
 from oracle.assembly import q1_element_matrices
 from oracle.oracle import REF_HARNESS
@@ -160,3 +160,32 @@ def test_oracle_hn_assembly_3d_live(disc, diff, conv):
     vals, _ = oracle_ball_values(P, degree, np.full(ne, diff), conv)
     for l, L in enumerate(P.levels):
         assert np.abs(vals[l] - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
+
+
+@pytest.mark.parametrize("name", golden_vtk_cases())
+def test_vtk_layout_matches_reference_file(name):
+    """Visualization::vtk's layout (Discretization/Q1/vtk.cc) restated in
+    Python reproduces the reference's file byte for byte from the level's
+    coordinates, the file's cells and the HN-averaged solution (the library's
+    writer is checked against the same bytes on the GPU)."""
+    from oracle.oracle import Oracle
+    P, ref = load_golden(name)
+    F = P.finest
+    u = ref["solution"]
+    if F.hn_edges is not None:
+        u = Oracle(P).hn("average", P.nlevels - 1, u)
+    cells = vtk_cells(ref["vtk"])
+    dim = P.dim
+    t = ("# vtk DataFile Version 2.0 \noutput from GascoigneStd, \nASCII\n"
+         "DATASET UNSTRUCTURED_GRID\nFIELD FieldData 1\nTIME 1 1 double\n0\n")
+    t += f"POINTS {F.n} DOUBLE \n"
+    t += "".join("".join(f"{x:g}\t" for x in F.coord[i]) + (" 0\n" if dim == 2 else "\n")
+                 for i in range(F.n))
+    t += f"\n\nCELLS {cells.shape[0]} {cells.size + cells.shape[0]}\n"
+    t += "".join(f"{cells.shape[1]} " + "".join(f"{v} " for v in c) + "\n" for c in cells)
+    t += f"\nCELL_TYPES {cells.shape[0]}\n" + ("9 " if dim == 2 else "12 ") * cells.shape[0]
+    t += f"\nPOINT_DATA {F.n}\n"
+    for comp in range(F.B):
+        t += f"SCALARS u{comp:03d} DOUBLE \nLOOKUP_TABLE default\n"
+        t += "".join(f"{u[i * F.B + comp]:g}\n" for i in range(F.n)) + "\n\n"
+    assert t.encode() == ref["vtk"].tobytes()
