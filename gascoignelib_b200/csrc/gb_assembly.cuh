@@ -177,11 +177,21 @@ q2_basis_1d(double t, double* L, double* dL)
 // lane), then each lane computes its own physical gradient once and hands it
 // to the other lanes by shuffles; lane a accumulates row a. Per element and
 // point this forms each basis gradient once instead of once per row.
-template<int DIM, bool CONV>
+// LPS (with CONV): the local projection stabilisation of the convection
+// (CGQ2Lps, ElementLpsIntegrator::Matrix, DofHandler/elementlpsintegrator.h:
+// 168-211): at each Gauss point h = |J|^(1/DIM), delta = s0 / (xeta kappa /
+// h^2 + bnorm / h) (LpsStabilization::ConvectionDiffusion,
+// Problems/lpsstabilization.cc), and E(a, b) += delta (beta . grad N_a)
+// (w |J| beta . grad N_b) with the projected functions N of
+// ElementLpsIntegrator::Projection (:66-110): a corner node's function is
+// -(1/2)^k times each node of its quarter of the patch that has k digits
+// moved to the middle, the other nodes keep theirs.
+template<int DIM, bool CONV, bool LPS = false>
 __global__ void __launch_bounds__(128)
 k_q2_element_warp(int ncells, const int* __restrict__ cells,
                   const double* __restrict__ coords, const double* __restrict__ kappa,
-                  double b0, double b1, double b2, double* __restrict__ E)
+                  double b0, double b1, double b2, double* __restrict__ E,
+                  double s0 = 0.0, double xeta = 0.0, double bnorm = 0.0)
 {
   GB_PDL_ENTRY();
   constexpr int NL = DIM == 3 ? 27 : 9;
@@ -281,6 +291,30 @@ k_q2_element_warp(int ncells, const int* __restrict__ cells,
         bg = fma(beta[d], t, bg);
     }
     const double wk = w * kap, wp = w * phi;
+    double bn = 0.0, dl = 0.0; // beta . grad N of this lane's projected function
+    if (LPS) {
+      bool corner = true;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        corner = corner && ld[d] != 1;
+      bn = corner ? 0.0 : bg;
+#pragma unroll
+      for (int m = 1; m < (1 << DIM); ++m) {
+        int src = lane;
+        double wt = -1.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          if ((m >> d) & 1) {
+            src += (1 - ld[d]) * (d == 0 ? 1 : d == 1 ? 3 : 9);
+            wt *= 0.5;
+          }
+        const double v = __shfl_sync(0xffffffffu, bg, act ? src : lane);
+        if (corner)
+          bn = fma(wt, v, bn);
+      }
+      const double h = pow(fabs(det), 1.0 / DIM);
+      dl = s0 / (xeta * kap / (h * h) + bnorm / h);
+    }
 #pragma unroll
     for (int b = 0; b < NL; ++b) {
       double dg = 0.0;
@@ -290,6 +324,8 @@ k_q2_element_warp(int ncells, const int* __restrict__ cells,
       e[b] = fma(wk, dg, e[b]);
       if (CONV)
         e[b] = fma(wp, __shfl_sync(0xffffffffu, bg, b), e[b]);
+      if (LPS)
+        e[b] = fma(dl * bn, w * __shfl_sync(0xffffffffu, bn, b), e[b]);
     }
   }
   if (act) {

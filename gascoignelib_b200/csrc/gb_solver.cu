@@ -567,6 +567,7 @@ struct gb_ctx
   int mid_grid[2] = { 0, 0 }; // per precision (FP64, FP32)
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
   gb::DeviceArray<double> asm_E; // element matrices of the level being assembled
+  double lps_s0 = 0.0, lps_xeta = 6.0; // LPS of the convection in Q2 assemblies (0: off)
   gb::DeviceArray<unsigned long long> nrm; // largest |y| of gb_newton_residual
   // matrix values changed on the device since the solver's set-up (dense
   // coarse maps, direct inverse): refreshed in place at the next solve
@@ -3161,15 +3162,23 @@ assemble_level(Context& c, int l, const double* beta)
 #define GB_ELEM(D, CV)                                                                   \
   launch(c, k_q1_element<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,  \
          (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p)
-#define GB_ELEM2(D, CV)                                                                  \
-  launch(c, k_q2_element_warp<D, CV>, blocks_for(int64_t(nc) * 32, 128), 128, nc,       \
+#define GB_ELEM2(D, CV, LP)                                                              \
+  launch(c, k_q2_element_warp<D, CV, LP>, blocks_for(int64_t(nc) * 32, 128), 128, nc,   \
          (const int*)L.m_cells.p, (const double*)L.m_coords.p, (const double*)L.m_kappa.p, \
-         b0, b1, b2, c.asm_E.p)
+         b0, b1, b2, c.asm_E.p, c.lps_s0, c.lps_xeta, bnorm)
+  GB_REQUIRE(c.lps_s0 == 0.0 || L.mesh_deg == 2, GB_EINVAL,
+             "LPS is built for Q2 elements only");
+  const bool lps = conv && c.lps_s0 > 0.0;
+  const double bnorm = std::sqrt(b0 * b0 + b1 * b1 + b2 * b2) + 1e-6;
   if (L.mesh_deg == 2) {
     if (dim == 2) {
-      if (conv) GB_ELEM2(2, true); else GB_ELEM2(2, false);
+      if (lps) GB_ELEM2(2, true, true);
+      else if (conv) GB_ELEM2(2, true, false);
+      else GB_ELEM2(2, false, false);
     } else {
-      if (conv) GB_ELEM2(3, true); else GB_ELEM2(3, false);
+      if (lps) GB_ELEM2(3, true, true);
+      else if (conv) GB_ELEM2(3, true, false);
+      else GB_ELEM2(3, false, false);
     }
   } else if (dim == 2) {
     if (conv) GB_ELEM(2, true); else GB_ELEM(2, false);
@@ -4606,6 +4615,17 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
   }
   if (lvl > 0)
     ctx->L[lvl - 1].child_n = -1; // its child lists follow this level's parents
+  GB_API_END
+}
+
+int
+gb_set_assembly_lps(gb_ctx* ctx, double sdelta0, double xeta0)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(sdelta0 >= 0.0 && std::isfinite(sdelta0), GB_EINVAL, "sdelta0 must be >= 0");
+  GB_REQUIRE(xeta0 > 0.0 && std::isfinite(xeta0), GB_EINVAL, "xeta0 must be > 0");
+  ctx->lps_s0 = sdelta0;
+  ctx->lps_xeta = xeta0;
   GB_API_END
 }
 

@@ -109,6 +109,7 @@ _SIGS = {
     "gb_level_set_mesh": [C.c_void_p, C.c_int, C.c_int, C.c_int64, _P64, _PD, _P64],
     "gb_level_set_mesh_degree": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, _P64, _PD,
                                  _P64],
+    "gb_set_assembly_lps": [C.c_void_p, C.c_double, C.c_double],
     "gb_assemble": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, _PD],
     "gb_assemble_levels": [C.c_void_p, C.c_void_p, C.c_int, _PD],
     "gb_level_get_kappa": [C.c_void_p, C.c_int, _PD],
@@ -301,6 +302,11 @@ class Context:
             kappa = kappa.numpy()
         k = np.ascontiguousarray(kappa, dtype=np.float64)
         return k.ctypes.data_as(C.c_void_p), 0, k
+
+    def set_assembly_lps(self, sdelta0, xeta0=6.0):
+        """gb_set_assembly_lps: LPS of the convection in later Q2 assemblies
+        (sdelta0 = 0: off)."""
+        self._chk(self._L.gb_set_assembly_lps(self.h, float(sdelta0), float(xeta0)))
 
     def assemble(self, level, kappa, beta=None):
         """gb_assemble: the level's matrix from per-cell kappa (numpy: host,

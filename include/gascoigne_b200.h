@@ -342,6 +342,20 @@ int gb_level_set_mesh(gb_ctx* ctx, int level, int dim, int64_t ncells,
 int gb_level_set_mesh_degree(gb_ctx* ctx, int level, int dim, int degree,
                              int64_t ncells, const int64_t* cell_nodes,
                              const double* coords, const int64_t* parent);
+/* Local projection stabilisation of the convection in the following device
+ * assemblies of Q2 levels (discretisation CGQ2Lps: ElementLpsIntegrator::Matrix,
+ * DofHandler/elementlpsintegrator.h:168-211, with the projection of :66-110):
+ * at every Gauss point h = |J|^(1/dim) and
+ * delta = sdelta0 / (xeta0 kappa / h^2 + (|beta| + 1e-6) / h) as
+ * LpsStabilization::ConvectionDiffusion computes it
+ * (Problems/lpsstabilization.cc, kappa the element's coefficient), and the
+ * element matrix gains delta (beta . grad N_i)(beta . grad N_j) w |J| over the
+ * projected functions N (a corner node's function replaced by minus its
+ * patch-quarter neighbours weighted 1/2, 1/4, 1/8). sdelta0 = 0 turns it off
+ * (the default); the reference's default xeta0 is 6. Only levels of degree 2
+ * with a nonzero beta are affected; a Q1 level assembled with it on is an
+ * error. */
+int gb_set_assembly_lps(gb_ctx* ctx, double sdelta0, double xeta0);
 /* Assembles the level's matrix (FP64 and FP32 values, block-diagonal inverse)
  * from kappa (ncells doubles; where = 0: host memory, 1: device memory,
  * copied on the context's stream (gb_ctx_get_stream), so writes to it on other

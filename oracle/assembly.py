@@ -190,14 +190,40 @@ def q2_shape(dim: int, xi: np.ndarray):
     return phi, grad
 
 
+def lps_projection(dim: int) -> np.ndarray:
+    """ElementLpsIntegrator::Projection (DofHandler/elementlpsintegrator.h:
+    66-110) as a matrix P (nloc x nloc, projected function i = sum_j P[i, j]
+    phi_j): the middle and edge nodes keep their basis function; a corner's is
+    replaced by -(1/2)^k times each node of its quarter of the patch whose k
+    digits moved from the corner to the middle."""
+    nloc = 3 ** dim
+    P = np.eye(nloc)
+    for c in range(nloc):
+        dig = [(c // 3 ** d) % 3 for d in range(dim)]
+        if 1 in dig:
+            continue
+        P[c, c] = 0.0
+        for m in range(1, 1 << dim):
+            j = sum((1 if (m >> d) & 1 else dig[d]) * 3 ** d for d in range(dim))
+            P[c, j] = -(0.5 ** bin(m).count("1"))
+    return P
+
+
 def q2_element_matrices(dim: int, xcell: np.ndarray, kappa: np.ndarray,
-                        beta=None) -> np.ndarray:
+                        beta=None, lps=None) -> np.ndarray:
     """As q1_element_matrices for Q2 elements (3^dim nodes, the isoparametric
-    quadratic map) with the 3-point Gauss rule."""
+    quadratic map) with the 3-point Gauss rule. lps = (sdelta0, xeta0) adds
+    the local projection stabilisation of the convection (CGQ2Lps,
+    ElementLpsIntegrator::Matrix, DofHandler/elementlpsintegrator.h:168-211):
+    at each Gauss point h = |J|^(1/dim), delta = sdelta0 / (xeta0 kappa / h^2
+    + (|beta| + 1e-6) / h) (LpsStabilization::ConvectionDiffusion,
+    Problems/lpsstabilization.cc) and E += w |J| delta (beta . grad N_i)
+    (beta . grad N_j) over the projected functions N."""
     pts, wts = gauss_points_q2(dim)
     nc, nloc = xcell.shape[0], 3 ** dim
     E = np.zeros((nc, nloc, nloc))
     b = np.zeros(dim) if beta is None else np.asarray(beta, dtype=np.float64)[:dim]
+    P = lps_projection(dim) if lps else None
     for q in range(pts.shape[0]):
         phi, gref = q2_shape(dim, pts[q])
         J = np.einsum("cad,ae->cde", xcell, gref)
@@ -208,6 +234,13 @@ def q2_element_matrices(dim: int, xcell: np.ndarray, kappa: np.ndarray,
         E += (w * kappa)[:, None, None] * np.einsum("cad,cbd->cab", g, g)
         conv = np.einsum("cbd,d->cb", g, b)
         E += w[:, None, None] * phi[None, :, None] * conv[:, None, :]
+        if P is not None:
+            s0, xeta = lps
+            h = np.abs(det) ** (1.0 / dim)
+            nb = np.sqrt(np.sum(b * b)) + 1e-6
+            delta = s0 / (xeta * kappa / (h * h) + nb / h)
+            bn = np.einsum("ij,cj->ci", P, conv)          # beta . grad N_i
+            E += (w * delta)[:, None, None] * bn[:, :, None] * bn[:, None, :]
     return E
 
 

@@ -36,6 +36,8 @@
 // within distance r of the domain's centre (MeshAgent::refine_cells: whole
 // patches, hanging nodes at the interface); diff=eps replaces the coefficient
 // by the constant eps (needed with ball refinement, where cell widths differ);
+// lps=s0 (with disc=Q2 and diff=) adds local projection stabilisation of the
+// convection (CGQ2Lps, DiffusionLpsEquation below);
 // rhsres=N reads the right-hand side on the (N+1)^dim lexicographic grid
 // (N = 2 * coarse * 2^refine covers the nodes of the extra refinement).
 //
@@ -87,6 +89,8 @@
 #include "stdmultilevelsolver.h"
 #include "stdsolver.h"
 #include "pressurefilter.h"
+#include "lpsequation.h"
+#include "lpsstabilization.h"
 #include "zerodirichletdata.h"
 
 using namespace Gascoigne;
@@ -96,6 +100,7 @@ namespace {
 struct Config
 {
   int dim = 3;
+  double lps = 0.0; // sdelta0 of the LPS convection stabilisation (disc=Q2), 0: none
   int coarse = 1; // coarse mesh cells per dimension (1 or 2)
   int refine = 3; // global refinements
   std::string kappa, rhs, dualrhs, out = ".";
@@ -196,6 +201,67 @@ public:
   }
 };
 
+// The same equation with local projection stabilisation of the convection
+// (lps=sdelta0, with disc=Q2 and diff=: discretisation CGQ2Lps,
+// ElementLpsIntegrator, DofHandler/elementlpsintegrator.h): at each Gauss point
+// delta = LpsStabilization::ConvectionDiffusion's sdelta0 / (xeta0 visc / h^2 +
+// |beta| / h) (Problems/lpsstabilization.cc; xeta0 = 6, |beta| + 1e-6, h = the
+// patch width), and the term delta (beta . grad Np)(beta . grad Mp) of the
+// projected test functions.
+class DiffusionLpsEquation : public DiffusionEquation, public LpsEquation
+{
+  int dim_;
+  double beta_[3], sdelta0_;
+  mutable LpsStabilization ST_;
+
+public:
+  DiffusionLpsEquation(int dim, const double* beta, double sdelta0)
+    : DiffusionEquation(dim, beta)
+    , dim_(dim)
+    , sdelta0_(sdelta0)
+  {
+    for (int i = 0; i < 3; ++i)
+      beta_[i] = beta[i];
+    ST_.BasicInit(1);
+    ST_.sdelta0 = sdelta0;
+  }
+  DiffusionLpsEquation* createNew() const override
+  {
+    return new DiffusionLpsEquation(dim_, beta_, sdelta0_);
+  }
+  std::string GetName() const override { return "OracleDiffusionLps"; }
+  void lpspoint(double h, const FemFunction&, const Vertex2d&) const override
+  {
+    ST_.ReInit(h, g_diff, beta_[0], beta_[1]);
+    ST_.ConvectionDiffusion(g_diff);
+  }
+  void lpspoint(double h, const FemFunction&, const Vertex3d&) const override
+  {
+    ST_.ReInit(h, g_diff, beta_[0], beta_[1], beta_[2]);
+    ST_.ConvectionDiffusion(g_diff);
+  }
+  void StabForm(VectorIterator b, const FemFunction&, const FemFunction& UP,
+                const TestFunction& N) const override
+  {
+    double bu = 0.0, bn = 0.0;
+    for (int i = 0; i < dim_; ++i) {
+      bu += beta_[i] * UP[0][i + 1];
+      bn += beta_[i] * N[i + 1];
+    }
+    b[0] += ST_.delta(0) * bu * bn;
+  }
+  void StabMatrix(EntryMatrix& A, const FemFunction&, const TestFunction& Np,
+                  const TestFunction& Mp) const override
+  {
+    double bn = 0.0, bm = 0.0;
+    for (int i = 0; i < dim_; ++i) {
+      bn += beta_[i] * Np[i + 1];
+      bm += beta_[i] * Mp[i + 1];
+    }
+    A(0, 0) += ST_.delta(0) * bn * bm;
+  }
+};
+
 // Stokes, components (p, v_1, .., v_dim) as Problems/navierstokes.h:144-168
 // orders them (M trial, N test function).
 class StokesEquation : public virtual Equation
@@ -270,10 +336,13 @@ struct SolverView : public StdSolver
 class DiffusionProblem : public ProblemDescriptorBase
 {
 public:
-  void BasicInit(const ParamFile& pf, int dim, const double* beta)
+  void BasicInit(const ParamFile& pf, int dim, const double* beta, double lps)
   {
     GetParamFile() = pf;
-    GetEquationPointer() = new DiffusionEquation(dim, beta);
+    if (lps > 0.0)
+      GetEquationPointer() = new DiffusionLpsEquation(dim, beta, lps);
+    else
+      GetEquationPointer() = new DiffusionEquation(dim, beta);
     GetDirichletDataPointer() = new ZeroDirichletData(pf);
     ProblemDescriptorBase::BasicInit(pf);
   }
@@ -323,6 +392,7 @@ parse(int argc, char** argv)
     else if (k == "disc") c.disc = v;
     else if (k == "ball") c.ball = atof(v.c_str());
     else if (k == "diff") c.diff = atof(v.c_str());
+    else if (k == "lps") c.lps = atof(v.c_str());
     else if (k == "rhsres") c.rhsres = atoi(v.c_str());
     else if (k == "conv") {
       std::stringstream ss(v);
@@ -458,7 +528,7 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "coarselevel 0\n\n"
     << "//Block Solver\n"
     << "matrixtype " << (c.smoother == "vanka" ? "vanka" : "block") << "\n"
-    << "discname " << (c.disc == "Q2" ? "CGQ2" : "CGQ1") << "\n"
+    << "discname " << (c.disc == "Q2" ? (c.lps > 0.0 ? "CGQ2Lps" : "CGQ2") : "CGQ1") << "\n"
     << "ndirect " << c.ndirect << "\n"
     << "iterpre " << c.iterpre << "\n"
     << "iterpost " << c.iterpost << "\n"
@@ -544,7 +614,7 @@ main(int argc, char** argv)
   if (stokes)
     PS.BasicInit(pf, c.dim, c.visc, c.stab);
   else
-    PD.BasicInit(pf, c.dim, c.conv);
+    PD.BasicInit(pf, c.dim, c.conv, c.lps);
   const int ncomp = stokes ? c.dim + 1 : 1;
   ProblemContainer PC;
   PC.AddProblem("diffusion", stokes ? static_cast<ProblemDescriptorInterface*>(&PS)

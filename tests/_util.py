@@ -352,3 +352,15 @@ def vtk_cells(vtk_bytes):
     ne = int(lines[i].split()[1])
     rows = [[int(t) for t in lines[i + 1 + c].split()][1:] for c in range(ne)]
     return np.array(rows, dtype=np.int64)
+
+
+def golden_lps_cases():
+    """Golden CGQ2Lps cases: (name, constant kappa, beta, (sdelta0, xeta0))."""
+    out = []
+    for n in golden_cases():
+        if n.startswith("lps_"):
+            z = np.load(os.path.join(GOLDEN, n + ".npz"))
+            out.append((n, float(z["key_diff"]),
+                        [float(t) for t in str(z["key_conv"]).split(",")],
+                        (float(z["key_lps"]), 6.0)))
+    return out

@@ -246,3 +246,57 @@ def test_q2_assembly_c4_size_against_generator(ctx):
     for l, L in enumerate(P.levels):
         v = ctx.level_values(l, L.val.size)
         assert np.abs(v - L.val).max() <= 1e-12 * np.abs(L.val).max(), l
+
+
+@pytest.mark.parametrize("name,diff,beta,lps", __import__("_util").golden_lps_cases(),
+                         ids=[c[0] for c in __import__("_util").golden_lps_cases()])
+def test_lps_assembly_matches_reference_and_solves(ctx, name, diff, beta, lps):
+    """CGQ2Lps (LPS of the convection) assembled on the device: the reference's
+    matrices on every level, the oracle's, and the reference's solve; then the
+    same assembly with the stabilisation off differs, and LPS on a Q1 level is
+    refused."""
+    from _util import uniform_meshes_q2
+    from oracle.assembly import assemble, q2_element_matrices
+    P, ref = load_golden(name)
+    ctx.load_problem(_zero_values(P))
+    meshes = uniform_meshes_q2(P)
+    for l, (el, par) in enumerate(meshes):
+        ctx.set_mesh(l, P.dim, el, P.levels[l].coord, par, degree=2)
+    kap = np.full(meshes[-1][0].shape[0], diff)
+    try:
+        ctx.set_assembly_lps(*lps)
+        ctx.assemble_levels(kap, beta)
+    finally:
+        ctx.set_assembly_lps(0.0)
+    for l, L in enumerate(P.levels):
+        v = ctx.level_values(l, L.val.size)
+        el = meshes[l][0]
+        o = assemble(L.n, L.rowptr, L.col, el,
+                     q2_element_matrices(P.dim, L.coord[el], np.full(el.shape[0], diff), beta,
+                                         lps), L.dirichlet)
+        assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
+        assert np.abs(v - o).max() <= 1e-13 * np.abs(L.val).max(), l
+    keys = ref["keys"]
+    ctx.set_params(**solver_keys(keys), gmressize=int(keys["gmressize"]),
+                   tol=float(keys["tol"]), globaltol=1e-16, maxiter=100)
+    fl = P.nlevels - 1
+    x, b = ctx.vec(), ctx.vec()
+    ctx.upload(fl, b, P.rhs)
+    info = ctx.gmres(x, b)
+    assert abs(info["iterations"] - ref["iterations"]) <= 1
+    assert rel_l2(ctx.download(fl, x), ref["solution"]) < 1e-8
+    ctx.free(x)
+    ctx.free(b)
+    ctx.assemble_levels(kap, beta)  # stabilisation off again
+    v = ctx.level_values(fl, P.finest.val.size)
+    assert np.abs(v - P.finest.val).max() > 1e-3 * np.abs(P.finest.val).max()
+    # LPS on a Q1 level is refused
+    Q, _ = load_golden("q1_2d_c2_r3_seeded")
+    ctx.load_problem(Q)
+    set_uniform_meshes(ctx, Q)
+    try:
+        ctx.set_assembly_lps(*lps)
+        with pytest.raises(GBError, match="Q2 elements only"):
+            ctx.assemble(Q.nlevels - 1, np.ones(uniform_meshes(Q)[-1][0].shape[0]), beta)
+    finally:
+        ctx.set_assembly_lps(0.0)

@@ -6,7 +6,8 @@ import os
 import numpy as np
 import pytest
 
-from _util import (ball_meshes, golden_assembly_cases, golden_hn_assembly_cases, golden_vtk_cases,
+from _util import (ball_meshes, golden_assembly_cases, golden_hn_assembly_cases, golden_lps_cases,
+                   golden_vtk_cases,
                    load_golden, oracle_ball_values, oracle_level_values, reference_ball_3d,
                    vtk_cells, with_condensed_pattern)
 from gascoignelib_b200.problem import seeded_inputs, structured_problem, structured_q2_ball
@@ -189,3 +190,23 @@ def test_vtk_layout_matches_reference_file(name):
         t += f"SCALARS u{comp:03d} DOUBLE \nLOOKUP_TABLE default\n"
         t += "".join(f"{u[i * F.B + comp]:g}\n" for i in range(F.n)) + "\n\n"
     assert t.encode() == ref["vtk"].tobytes()
+
+
+@pytest.mark.parametrize("name,diff,beta,lps", golden_lps_cases(),
+                         ids=[c[0] for c in golden_lps_cases()])
+def test_oracle_lps_assembly_matches_reference(name, diff, beta, lps):
+    """CGQ2Lps (local projection stabilisation of the convection): the oracle's
+    Q2 element matrices with the projected LPS term reproduce the reference's
+    matrices on every level; without the term they do not."""
+    from _util import uniform_meshes_q2
+    from oracle.assembly import assemble, q2_element_matrices
+    P, _ = load_golden(name)
+    for l, (el, _) in enumerate(uniform_meshes_q2(P)):
+        L = P.levels[l]
+        kap = np.full(el.shape[0], diff)
+        v = assemble(L.n, L.rowptr, L.col, el,
+                     q2_element_matrices(P.dim, L.coord[el], kap, beta, lps), L.dirichlet)
+        assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
+        w = assemble(L.n, L.rowptr, L.col, el,
+                     q2_element_matrices(P.dim, L.coord[el], kap, beta), L.dirichlet)
+        assert np.abs(w - L.val).max() > 1e-3 * np.abs(L.val).max(), l
