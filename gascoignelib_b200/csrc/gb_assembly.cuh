@@ -165,6 +165,24 @@ q2_basis_1d(double t, double* L, double* dL)
   dL[2] = 4.0 * t - 1.0;
 }
 
+// The piecewise linear basis of a patch of two cells in one direction (nodes 0,
+// 1/2, 1) at Gauss point qd of the 4 of the patch: LineGauss2 (1/2 -+ g) in cell
+// qd / 2, mapped to it (PatchFormula2d/3d,
+// Discretization/Q2/patchintegrationformula.xx:55-83; BaseQ12dPatch,
+// Discretization/Q2/baseq1patch.h: the cell's Q1 functions, derivatives times 2).
+__device__ __forceinline__ void
+q1patch_basis_1d(int qd, double g, double* L, double* dL)
+{
+  const int k = qd >> 1;                    // the cell
+  const double s = (qd & 1) ? 0.5 + g : 0.5 - g;
+  L[0] = L[1] = L[2] = 0.0;
+  dL[0] = dL[1] = dL[2] = 0.0;
+  L[k] = 1.0 - s;
+  L[k + 1] = s;
+  dL[k] = -2.0;
+  dL[k + 1] = 2.0;
+}
+
 // Q2 element matrices (CGQ2: 3^DIM-node elements on patches of 2^DIM cells,
 // the isoparametric quadratic map, the matrix formula QuadGauss9 / HexGauss27
 // with LineGauss3's points and 12-digit weights as the reference states them,
@@ -186,12 +204,16 @@ q2_basis_1d(double t, double* L, double* dL)
 // ElementLpsIntegrator::Projection (:66-110): a corner node's function is
 // -(1/2)^k times each node of its quarter of the patch that has k digits
 // moved to the middle, the other nodes keep theirs.
-template<int DIM, bool CONV, bool LPS = false>
+// PQ1: the patch's Q1 functions instead (CGQ1Lps / CGQ1Patch: BaseQ12dPatch /
+// BaseQ13dPatch, bilinear / trilinear on each cell of the patch) with the
+// patch formula of QuadGauss4 / HexGauss8 in every cell (4 points per
+// direction, weight 1/4 each); g = 1/(2 sqrt 3).
+template<int DIM, bool CONV, bool LPS = false, bool PQ1 = false>
 __global__ void __launch_bounds__(128)
 k_q2_element_warp(int ncells, const int* __restrict__ cells,
                   const double* __restrict__ coords, const double* __restrict__ kappa,
                   double b0, double b1, double b2, double* __restrict__ E,
-                  double s0 = 0.0, double xeta = 0.0, double bnorm = 0.0)
+                  double s0 = 0.0, double xeta = 0.0, double bnorm = 0.0, double g = 0.0)
 {
   GB_PDL_ENTRY();
   constexpr int NL = DIM == 3 ? 27 : 9;
@@ -220,14 +242,21 @@ k_q2_element_warp(int ncells, const int* __restrict__ cells,
 #pragma unroll
   for (int b = 0; b < NL; ++b)
     e[b] = 0.0;
+  constexpr int NQ = PQ1 ? 4 : 3;            // Gauss points per direction
+  constexpr int NQT = DIM == 3 ? NQ * NQ * NQ : NQ * NQ;
 #pragma unroll 1
-  for (int q = 0; q < NL; ++q) {
+  for (int q = 0; q < NQT; ++q) {
     double L[DIM][3], dL[DIM][3], wq = 1.0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-      const int qd = (q / (d == 0 ? 1 : d == 1 ? 3 : 9)) % 3;
-      q2_basis_1d(P3[qd], L[d], dL[d]);
-      wq *= W3[qd];
+      const int qd = (q / (d == 0 ? 1 : d == 1 ? NQ : NQ * NQ)) % NQ;
+      if (PQ1) {
+        q1patch_basis_1d(qd, g, L[d], dL[d]);
+        wq *= 0.25;
+      } else {
+        q2_basis_1d(P3[qd], L[d], dL[d]);
+        wq *= W3[qd];
+      }
     }
     // this lane's basis function: value and reference gradient
     double phi = 1.0, gr[DIM];

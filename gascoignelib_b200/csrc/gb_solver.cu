@@ -3149,6 +3149,7 @@ assemble_level(Context& c, int l, const double* beta)
   const int dim = L.mesh_dim;
   const int nl = L.mesh_deg == 1 ? 1 << dim : (dim == 3 ? 27 : 9);
   const int nc = static_cast<int>(L.mesh_ncells);
+  const bool pq1 = L.mesh_deg == 3; // Q1 functions on patches
   GB_CUDA(c.asm_E.n >= size_t(nc) * nl * nl ? cudaSuccess
                                              : c.asm_E.alloc(size_t(nc) * nl * nl));
   const double b0 = beta ? beta[0] : 0.0, b1 = beta ? beta[1] : 0.0;
@@ -3162,23 +3163,25 @@ assemble_level(Context& c, int l, const double* beta)
 #define GB_ELEM(D, CV)                                                                   \
   launch(c, k_q1_element<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,  \
          (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, c.asm_E.p)
-#define GB_ELEM2(D, CV, LP)                                                              \
-  launch(c, k_q2_element_warp<D, CV, LP>, blocks_for(int64_t(nc) * 32, 128), 128, nc,   \
+#define GB_ELEM2(D, CV, LP, PQ)                                                          \
+  launch(c, k_q2_element_warp<D, CV, LP, PQ>, blocks_for(int64_t(nc) * 32, 128), 128, nc, \
          (const int*)L.m_cells.p, (const double*)L.m_coords.p, (const double*)L.m_kappa.p, \
-         b0, b1, b2, c.asm_E.p, c.lps_s0, c.lps_xeta, bnorm)
-  GB_REQUIRE(c.lps_s0 == 0.0 || L.mesh_deg == 2, GB_EINVAL,
-             "LPS is built for Q2 elements only");
+         b0, b1, b2, c.asm_E.p, c.lps_s0, c.lps_xeta, bnorm, g)
+#define GB_ELEM2K(D, PQ)                                                                 \
+  do {                                                                                   \
+    if (lps) GB_ELEM2(D, true, true, PQ);                                                \
+    else if (conv) GB_ELEM2(D, true, false, PQ);                                         \
+    else GB_ELEM2(D, false, false, PQ);                                                  \
+  } while (0)
+  GB_REQUIRE(c.lps_s0 == 0.0 || L.mesh_deg >= 2, GB_EINVAL,
+             "LPS is built for patch elements only (Q2, or Q1 on patches)");
   const bool lps = conv && c.lps_s0 > 0.0;
   const double bnorm = std::sqrt(b0 * b0 + b1 * b1 + b2 * b2) + 1e-6;
-  if (L.mesh_deg == 2) {
+  if (L.mesh_deg >= 2) {
     if (dim == 2) {
-      if (lps) GB_ELEM2(2, true, true);
-      else if (conv) GB_ELEM2(2, true, false);
-      else GB_ELEM2(2, false, false);
+      if (pq1) GB_ELEM2K(2, true); else GB_ELEM2K(2, false);
     } else {
-      if (lps) GB_ELEM2(3, true, true);
-      else if (conv) GB_ELEM2(3, true, false);
-      else GB_ELEM2(3, false, false);
+      if (pq1) GB_ELEM2K(3, true); else GB_ELEM2K(3, false);
     }
   } else if (dim == 2) {
     if (conv) GB_ELEM(2, true); else GB_ELEM(2, false);
@@ -3187,6 +3190,7 @@ assemble_level(Context& c, int l, const double* beta)
   }
 #undef GB_ELEM
 #undef GB_ELEM2
+#undef GB_ELEM2K
   if (L.m_nhcells > 0)
     launch(c, k_condense, blocks_for(int64_t(L.m_nhcells) * 32, 128), 128, L.m_nhcells,
            (const int*)L.m_hcells.p, (const int*)L.m_hopptr.p, (const CondOp*)L.m_hops.p, nl,
@@ -4453,7 +4457,8 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
   ctx->version++;
   Level& L = level_with_matrix(*ctx, lvl);
   GB_REQUIRE(dim == 2 || dim == 3, GB_EINVAL, "dim must be 2 or 3");
-  GB_REQUIRE(degree == 1 || degree == 2, GB_EINVAL, "degree must be 1 (Q1) or 2 (Q2)");
+  GB_REQUIRE(degree >= 1 && degree <= 3, GB_EINVAL,
+             "degree must be 1 (Q1 cells), 2 (Q2 patches) or 3 (Q1 patches)");
   GB_REQUIRE(L.B == 1, GB_EINVAL, "device assembly needs block size 1");
   GB_REQUIRE(!L.has_hn() || L.h_hnidx.size() == size_t(L.n), GB_EINVAL,
              "the hanging nodes were set for another matrix size");

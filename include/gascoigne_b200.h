@@ -337,13 +337,18 @@ int gb_level_set_mesh(gb_ctx* ctx, int level, int dim, int64_t ncells,
  * a = a_x + 3 a_y + 9 a_z at the reference coordinates (a_d / 2); integrated
  * with QuadGauss9 / HexGauss27 as LineGauss3 states its points and weights,
  * Discretization/Q1/integrationformula1d.cc:82-92; kappa per element, parents
- * = the element of level - 1 that contains it). gb_form is built for Q1
+ * = the element of level - 1 that contains it). degree = 3: the same patches
+ * with the Q1 functions of their cells (CGQ1Patch / CGQ1Lps: BaseQ12dPatch /
+ * BaseQ13dPatch, Discretization/Q2/baseq1patch.h; QuadGauss4 / HexGauss8 in
+ * every cell, PatchFormula2d/3d, Discretization/Q2/patchintegrationformula.xx:
+ * 55-83); the matrix equals the Q1 cells' up to rounding, and LPS needs it. gb_form is built for Q1
  * levels without hanging nodes only. */
 int gb_level_set_mesh_degree(gb_ctx* ctx, int level, int dim, int degree,
                              int64_t ncells, const int64_t* cell_nodes,
                              const double* coords, const int64_t* parent);
 /* Local projection stabilisation of the convection in the following device
- * assemblies of Q2 levels (discretisation CGQ2Lps: ElementLpsIntegrator::Matrix,
+ * assemblies of patch levels (degree 2: CGQ2Lps, degree 3: CGQ1Lps;
+ * ElementLpsIntegrator::Matrix,
  * DofHandler/elementlpsintegrator.h:168-211, with the projection of :66-110):
  * at every Gauss point h = |J|^(1/dim) and
  * delta = sdelta0 / (xeta0 kappa / h^2 + (|beta| + 1e-6) / h) as
@@ -352,9 +357,9 @@ int gb_level_set_mesh_degree(gb_ctx* ctx, int level, int dim, int degree,
  * element matrix gains delta (beta . grad N_i)(beta . grad N_j) w |J| over the
  * projected functions N (a corner node's function replaced by minus its
  * patch-quarter neighbours weighted 1/2, 1/4, 1/8). sdelta0 = 0 turns it off
- * (the default); the reference's default xeta0 is 6. Only levels of degree 2
- * with a nonzero beta are affected; a Q1 level assembled with it on is an
- * error. */
+ * (the default); the reference's default xeta0 is 6. Only patch levels
+ * (degree 2 or 3) with a nonzero beta are affected; a level of Q1 cells
+ * assembled with it on is an error. */
 int gb_set_assembly_lps(gb_ctx* ctx, double sdelta0, double xeta0);
 /* Assembles the level's matrix (FP64 and FP32 values, block-diagonal inverse)
  * from kappa (ncells doubles; where = 0: host memory, 1: device memory,

@@ -209,8 +209,51 @@ def lps_projection(dim: int) -> np.ndarray:
     return P
 
 
+def q1patch_shape(dim: int, xi: np.ndarray):
+    """The Q1 functions of a patch of 2^dim cells (BaseQ12dPatch /
+    BaseQ13dPatch, Discretization/Q2/baseq1patch.h: bilinear / trilinear on
+    each cell, nodes 0, 1/2, 1 per direction, x fastest): values [3^dim] and
+    reference gradients [3^dim, dim] at xi (not on a cell boundary)."""
+    def hat(t):
+        if t <= 0.5:
+            return (1.0 - 2.0 * t, 2.0 * t, 0.0), (-2.0, 2.0, 0.0)
+        return (0.0, 2.0 - 2.0 * t, 2.0 * t - 1.0), (0.0, -2.0, 2.0)
+    nloc = 3 ** dim
+    phi = np.ones(nloc)
+    grad = np.ones((nloc, dim))
+    hs = [hat(xi[d]) for d in range(dim)]
+    for a in range(nloc):
+        digits = [(a // 3 ** d) % 3 for d in range(dim)]
+        for d in range(dim):
+            f, df = hs[d][0][digits[d]], hs[d][1][digits[d]]
+            phi[a] *= f
+            for e in range(dim):
+                grad[a, e] *= df if e == d else f
+    return phi, grad
+
+
+def gauss_points_q1patch(dim: int):
+    """PatchFormula2d<4, QuadGauss4> / PatchFormula3d<8, HexGauss8>
+    (Discretization/Q2/patchintegrationformula.xx:55-83): the 2-point rule in
+    each cell of the patch, weights / 2^dim."""
+    g = 0.5 / np.sqrt(3.0)
+    p1 = np.array([0.5 * (0.5 - g), 0.5 * (0.5 + g), 0.5 + 0.5 * (0.5 - g),
+                   0.5 + 0.5 * (0.5 + g)])
+    grids = np.meshgrid(*([np.arange(4)] * dim), indexing="ij")
+    idx = np.stack([gg.ravel() for gg in reversed(grids)], 1)
+    return p1[idx], np.full(idx.shape[0], 0.25 ** dim)
+
+
+def q1patch_element_matrices(dim: int, xcell: np.ndarray, kappa: np.ndarray,
+                             beta=None, lps=None) -> np.ndarray:
+    """q2_element_matrices for the Q1 functions of patches (CGQ1Patch /
+    CGQ1Lps) with the patch formula."""
+    return q2_element_matrices(dim, xcell, kappa, beta, lps, shape=q1patch_shape,
+                               rule=gauss_points_q1patch)
+
+
 def q2_element_matrices(dim: int, xcell: np.ndarray, kappa: np.ndarray,
-                        beta=None, lps=None) -> np.ndarray:
+                        beta=None, lps=None, shape=None, rule=None) -> np.ndarray:
     """As q1_element_matrices for Q2 elements (3^dim nodes, the isoparametric
     quadratic map) with the 3-point Gauss rule. lps = (sdelta0, xeta0) adds
     the local projection stabilisation of the convection (CGQ2Lps,
@@ -219,13 +262,13 @@ def q2_element_matrices(dim: int, xcell: np.ndarray, kappa: np.ndarray,
     + (|beta| + 1e-6) / h) (LpsStabilization::ConvectionDiffusion,
     Problems/lpsstabilization.cc) and E += w |J| delta (beta . grad N_i)
     (beta . grad N_j) over the projected functions N."""
-    pts, wts = gauss_points_q2(dim)
+    pts, wts = (rule or gauss_points_q2)(dim)
     nc, nloc = xcell.shape[0], 3 ** dim
     E = np.zeros((nc, nloc, nloc))
     b = np.zeros(dim) if beta is None else np.asarray(beta, dtype=np.float64)[:dim]
     P = lps_projection(dim) if lps else None
     for q in range(pts.shape[0]):
-        phi, gref = q2_shape(dim, pts[q])
+        phi, gref = (shape or q2_shape)(dim, pts[q])
         J = np.einsum("cad,ae->cde", xcell, gref)
         det = np.linalg.det(J)
         Jinv = np.linalg.inv(J)

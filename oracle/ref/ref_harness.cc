@@ -36,8 +36,9 @@
 // within distance r of the domain's centre (MeshAgent::refine_cells: whole
 // patches, hanging nodes at the interface); diff=eps replaces the coefficient
 // by the constant eps (needed with ball refinement, where cell widths differ);
-// lps=s0 (with disc=Q2 and diff=) adds local projection stabilisation of the
-// convection (CGQ2Lps, DiffusionLpsEquation below);
+// lps=s0 (with diff=) adds local projection stabilisation of the convection
+// (CGQ2Lps, or CGQ1Lps with disc=Q1: Q1 functions on patches;
+// DiffusionLpsEquation below);
 // rhsres=N reads the right-hand side on the (N+1)^dim lexicographic grid
 // (N = 2 * coarse * 2^refine covers the nodes of the extra refinement).
 //
@@ -202,7 +203,7 @@ public:
 };
 
 // The same equation with local projection stabilisation of the convection
-// (lps=sdelta0, with disc=Q2 and diff=: discretisation CGQ2Lps,
+// (lps=sdelta0, with diff=: discretisation CGQ2Lps or CGQ1Lps,
 // ElementLpsIntegrator, DofHandler/elementlpsintegrator.h): at each Gauss point
 // delta = LpsStabilization::ConvectionDiffusion's sdelta0 / (xeta0 visc / h^2 +
 // |beta| / h) (Problems/lpsstabilization.cc; xeta0 = 6, |beta| + 1e-6, h = the
@@ -528,7 +529,9 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "coarselevel 0\n\n"
     << "//Block Solver\n"
     << "matrixtype " << (c.smoother == "vanka" ? "vanka" : "block") << "\n"
-    << "discname " << (c.disc == "Q2" ? (c.lps > 0.0 ? "CGQ2Lps" : "CGQ2") : "CGQ1") << "\n"
+    << "discname "
+    << (c.disc == "Q2" ? (c.lps > 0.0 ? "CGQ2Lps" : "CGQ2") : (c.lps > 0.0 ? "CGQ1Lps" : "CGQ1"))
+    << "\n"
     << "ndirect " << c.ndirect << "\n"
     << "iterpre " << c.iterpre << "\n"
     << "iterpost " << c.iterpost << "\n"

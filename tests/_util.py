@@ -355,12 +355,14 @@ def vtk_cells(vtk_bytes):
 
 
 def golden_lps_cases():
-    """Golden CGQ2Lps cases: (name, constant kappa, beta, (sdelta0, xeta0))."""
+    """Golden CGQ2Lps / CGQ1Lps cases: (name, mesh degree code for
+    set_mesh - 2 Q2 patches, 3 Q1 patches - constant kappa, beta,
+    (sdelta0, xeta0))."""
     out = []
     for n in golden_cases():
         if n.startswith("lps_"):
             z = np.load(os.path.join(GOLDEN, n + ".npz"))
-            out.append((n, float(z["key_diff"]),
+            out.append((n, 2 if str(z["key_disc"]) == "Q2" else 3, float(z["key_diff"]),
                         [float(t) for t in str(z["key_conv"]).split(",")],
                         (float(z["key_lps"]), 6.0)))
     return out

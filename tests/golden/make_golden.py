@@ -19,8 +19,9 @@ cases use linear_smooth ilu with matrixtype block (SparseBlockIlu). The "form_"
 cases also record StdSolver::Form and StdMultiLevelSolver::NewtonResidual of a
 seeded vector and the solution as written by WriteBackUp (.bup) and
 WriteBackUpBinary (.bip); cases with "vtk" the solution as StdSolver::Visu
-writes it (VTK). The "lps_" cases are CGQ2Lps: Q2 convection-diffusion with
-local projection stabilisation of the convection (constant coefficient).
+writes it (VTK). The "lps_" cases are CGQ2Lps / CGQ1Lps: Q2 or patch-Q1
+convection-diffusion with local projection stabilisation of the convection
+(constant coefficient).
 
     python tests/golden/make_golden.py
 """
@@ -68,6 +69,12 @@ CASES = {
                                                     "omega": 0.3, "gmressize": 41,
                                                     "conv": "1,0.5"}),
     "lps_3d_q2_c1_r3_conv": (3, 1, 3, True, 1e-8, {"disc": "Q2", "diff": 0.01, "lps": 0.5,
+                                                   "omega": 0.3, "gmressize": 41,
+                                                   "conv": "1,0.5,0.25"}),
+    "lps_2d_q1_c2_r3_conv": (2, 2, 3, True, 1e-10, {"disc": "Q1", "diff": 0.01, "lps": 0.5,
+                                                    "omega": 0.3, "gmressize": 41,
+                                                    "conv": "1,0.5"}),
+    "lps_3d_q1_c1_r3_conv": (3, 1, 3, True, 1e-8, {"disc": "Q1", "diff": 0.01, "lps": 0.5,
                                                    "omega": 0.3, "gmressize": 41,
                                                    "conv": "1,0.5,0.25"}),
     "hn_2d_q1_c2_r3_ball": (2, 2, 3, True, 1e-10,

@@ -248,20 +248,21 @@ def test_q2_assembly_c4_size_against_generator(ctx):
         assert np.abs(v - L.val).max() <= 1e-12 * np.abs(L.val).max(), l
 
 
-@pytest.mark.parametrize("name,diff,beta,lps", __import__("_util").golden_lps_cases(),
+@pytest.mark.parametrize("name,kind,diff,beta,lps", __import__("_util").golden_lps_cases(),
                          ids=[c[0] for c in __import__("_util").golden_lps_cases()])
-def test_lps_assembly_matches_reference_and_solves(ctx, name, diff, beta, lps):
-    """CGQ2Lps (LPS of the convection) assembled on the device: the reference's
-    matrices on every level, the oracle's, and the reference's solve; then the
-    same assembly with the stabilisation off differs, and LPS on a Q1 level is
-    refused."""
+def test_lps_assembly_matches_reference_and_solves(ctx, name, kind, diff, beta, lps):
+    """CGQ2Lps / CGQ1Lps (LPS of the convection; Q2 or Q1 functions on
+    patches) assembled on the device: the reference's matrices on every level,
+    the oracle's, and the reference's solve; then the same assembly with the
+    stabilisation off differs, and LPS on a level of Q1 cells is refused."""
     from _util import uniform_meshes_q2
-    from oracle.assembly import assemble, q2_element_matrices
+    from oracle.assembly import assemble, q1patch_element_matrices, q2_element_matrices
+    f = q2_element_matrices if kind == 2 else q1patch_element_matrices
     P, ref = load_golden(name)
     ctx.load_problem(_zero_values(P))
     meshes = uniform_meshes_q2(P)
     for l, (el, par) in enumerate(meshes):
-        ctx.set_mesh(l, P.dim, el, P.levels[l].coord, par, degree=2)
+        ctx.set_mesh(l, P.dim, el, P.levels[l].coord, par, degree=kind)
     kap = np.full(meshes[-1][0].shape[0], diff)
     try:
         ctx.set_assembly_lps(*lps)
@@ -272,8 +273,7 @@ def test_lps_assembly_matches_reference_and_solves(ctx, name, diff, beta, lps):
         v = ctx.level_values(l, L.val.size)
         el = meshes[l][0]
         o = assemble(L.n, L.rowptr, L.col, el,
-                     q2_element_matrices(P.dim, L.coord[el], np.full(el.shape[0], diff), beta,
-                                         lps), L.dirichlet)
+                     f(P.dim, L.coord[el], np.full(el.shape[0], diff), beta, lps), L.dirichlet)
         assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
         assert np.abs(v - o).max() <= 1e-13 * np.abs(L.val).max(), l
     keys = ref["keys"]
@@ -296,7 +296,7 @@ def test_lps_assembly_matches_reference_and_solves(ctx, name, diff, beta, lps):
     set_uniform_meshes(ctx, Q)
     try:
         ctx.set_assembly_lps(*lps)
-        with pytest.raises(GBError, match="Q2 elements only"):
+        with pytest.raises(GBError, match="patch elements only"):
             ctx.assemble(Q.nlevels - 1, np.ones(uniform_meshes(Q)[-1][0].shape[0]), beta)
     finally:
         ctx.set_assembly_lps(0.0)

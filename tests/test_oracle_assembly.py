@@ -192,21 +192,22 @@ def test_vtk_layout_matches_reference_file(name):
     assert t.encode() == ref["vtk"].tobytes()
 
 
-@pytest.mark.parametrize("name,diff,beta,lps", golden_lps_cases(),
+@pytest.mark.parametrize("name,kind,diff,beta,lps", golden_lps_cases(),
                          ids=[c[0] for c in golden_lps_cases()])
-def test_oracle_lps_assembly_matches_reference(name, diff, beta, lps):
-    """CGQ2Lps (local projection stabilisation of the convection): the oracle's
-    Q2 element matrices with the projected LPS term reproduce the reference's
-    matrices on every level; without the term they do not."""
+def test_oracle_lps_assembly_matches_reference(name, kind, diff, beta, lps):
+    """CGQ2Lps / CGQ1Lps (local projection stabilisation of the convection):
+    the oracle's patch element matrices (Q2, or Q1 functions on patches) with
+    the projected LPS term reproduce the reference's matrices on every level;
+    without the term they do not."""
     from _util import uniform_meshes_q2
-    from oracle.assembly import assemble, q2_element_matrices
+    from oracle.assembly import assemble, q1patch_element_matrices, q2_element_matrices
+    f = q2_element_matrices if kind == 2 else q1patch_element_matrices
     P, _ = load_golden(name)
     for l, (el, _) in enumerate(uniform_meshes_q2(P)):
         L = P.levels[l]
         kap = np.full(el.shape[0], diff)
-        v = assemble(L.n, L.rowptr, L.col, el,
-                     q2_element_matrices(P.dim, L.coord[el], kap, beta, lps), L.dirichlet)
+        v = assemble(L.n, L.rowptr, L.col, el, f(P.dim, L.coord[el], kap, beta, lps),
+                     L.dirichlet)
         assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
-        w = assemble(L.n, L.rowptr, L.col, el,
-                     q2_element_matrices(P.dim, L.coord[el], kap, beta), L.dirichlet)
+        w = assemble(L.n, L.rowptr, L.col, el, f(P.dim, L.coord[el], kap, beta), L.dirichlet)
         assert np.abs(w - L.val).max() > 1e-3 * np.abs(L.val).max(), l
