@@ -661,6 +661,34 @@ k_q1_form(int ncells, const int* __restrict__ cells, const double* __restrict__ 
     F[int64_t(a) * ncells + c] = f[a];
 }
 
+// The element residuals R = E x of elements given by their matrices (entry-major
+// E, as the element kernels write them): one warp per element, lane a holding
+// node a's value of x and forming row a (the equation is linear in u, so its
+// element form is its element matrix times the local values).
+template<int NL>
+__global__ void __launch_bounds__(128)
+k_elem_apply(int ncells, const int* __restrict__ cells, const double* __restrict__ E,
+             const double* __restrict__ x, double* __restrict__ R)
+{
+  GB_PDL_ENTRY();
+  const int64_t wid = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= ncells) // whole warps leave together
+    return;
+  const int64_t c = wid, nc = ncells;
+  const bool act = lane < NL;
+  const double xb = act ? __ldg(x + __ldg(cells + int64_t(lane) * nc + c)) : 0.0;
+  double acc = 0.0;
+#pragma unroll
+  for (int b = 0; b < NL; ++b) {
+    const double v = __shfl_sync(0xffffffffu, xb, b);
+    if (act)
+      acc = fma(__ldg(E + (int64_t(lane) * NL + b) * nc + c), v, acc);
+  }
+  if (act)
+    R[int64_t(lane) * nc + c] = acc;
+}
+
 // y[r] += d * (the element residuals of the cells of node r, in ascending cell
 // order: LocalToGlobal, DofHandler/cgdisc.h:367-380); nodes whose entries in
 // nptr are empty keep y.

@@ -396,6 +396,7 @@ struct Level
   DeviceArray<int> m_cells, m_cptr, m_clist, m_diagpos, m_child_ptr, m_child;
   DeviceArray<int> m_nptr, m_nlist; // per node its (cell, local index) pairs
   double m_beta[3] = { 0.0, 0.0, 0.0 }; // convection of the last assembly
+  double m_lps_s0 = 0.0, m_lps_xeta = 6.0; // its LPS (sdelta0 0: none)
   bool m_assembled = false;
   DeviceArray<double> m_coords, m_kappa, m_dd;
   // hanging nodes in the device assembly: per hanging node (h_hnidx[node],
@@ -567,6 +568,7 @@ struct gb_ctx
   int mid_grid[2] = { 0, 0 }; // per precision (FP64, FP32)
   gb::DeviceArray<double> xg, bg, rhs64, zfix64;
   gb::DeviceArray<double> asm_E; // element matrices of the level being assembled
+  gb::DeviceArray<double> asm_R; // element residuals (Form of patch elements)
   double lps_s0 = 0.0, lps_xeta = 6.0; // LPS of the convection in Q2 assemblies (0: off)
   gb::DeviceArray<unsigned long long> nrm; // largest |y| of gb_newton_residual
   // matrix values changed on the device since the solver's set-up (dense
@@ -3159,6 +3161,8 @@ assemble_level(Context& c, int l, const double* beta)
   L.m_beta[0] = b0;
   L.m_beta[1] = b1;
   L.m_beta[2] = b2;
+  L.m_lps_s0 = L.mesh_deg >= 2 ? c.lps_s0 : 0.0;
+  L.m_lps_xeta = c.lps_xeta;
   L.m_assembled = true;
 #define GB_ELEM(D, CV)                                                                   \
   launch(c, k_q1_element<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,  \
@@ -3260,34 +3264,72 @@ coarsen_kappa(Context& c, int l)
          C.m_kappa.p);
 }
 
-// y += d * Form(x) on level l with the coefficient and convection of its
-// last assembly (StdSolver::Form without hanging nodes: the element residuals
-// summed per node in ascending cell order)
+// y += d * Form(x) on level l with the coefficient, convection and LPS of its
+// last assembly (StdSolver::Form, Solver/stdsolver.cc:1041-1063): HNAverage(x),
+// the element residuals added at the cells' own nodes in ascending cell order
+// (CGDisc::Form and LocalToGlobal, DofHandler/cgdisc.h:367-380, 415-470),
+// HNZero(x) and HNDistribute(y), as the reference does on a level with hanging
+// nodes. Q1 cells: matrix-free residuals; patch elements (Q2, Q1 on patches,
+// with LPS): the element matrices, then E x per element.
 static void
-form_level(Context& c, int l, double* y, const double* x, double d)
+form_level(Context& c, int l, double* y, double* x, double d)
 {
   Level& L = c.L[l];
   GB_REQUIRE(L.m_assembled, GB_ESTATE, "Form needs an assembled level (gb_assemble)");
-  GB_REQUIRE(L.mesh_deg == 1, GB_EINVAL, "Form is built for Q1 elements only");
-  GB_REQUIRE(!L.has_hn(), GB_EINVAL, "Form on a level with hanging nodes");
-  const int dim = L.mesh_dim, nl = 1 << dim;
+  const int dim = L.mesh_dim;
+  const int nl = L.mesh_deg == 1 ? 1 << dim : (dim == 3 ? 27 : 9);
   const int nc = static_cast<int>(L.mesh_ncells);
-  GB_CUDA(c.asm_E.n >= size_t(nc) * nl ? cudaSuccess : c.asm_E.alloc(size_t(nc) * nl));
   const double b0 = L.m_beta[0], b1 = L.m_beta[1], b2 = L.m_beta[2];
   const bool conv = b0 != 0.0 || b1 != 0.0 || b2 != 0.0;
   const double g = 0.5 / std::sqrt(3.0);
+  Emit<double> Em{ c, nullptr };
+  if (L.has_hn())
+    Em.hn_average(l, x);
+  GB_CUDA(c.asm_R.n >= size_t(nc) * nl ? cudaSuccess : c.asm_R.alloc(size_t(nc) * nl));
+  if (L.mesh_deg == 1) {
 #define GB_FORM(D, CV)                                                                 \
   launch(c, k_q1_form<D, CV>, blocks_for(nc, 128), 128, nc, (const int*)L.m_cells.p,   \
-         (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g, x,     \
-         c.asm_E.p)
-  if (dim == 2) {
-    if (conv) GB_FORM(2, true); else GB_FORM(2, false);
-  } else {
-    if (conv) GB_FORM(3, true); else GB_FORM(3, false);
-  }
+         (const double*)L.m_coords.p, (const double*)L.m_kappa.p, b0, b1, b2, g,        \
+         (const double*)x, c.asm_R.p)
+    if (dim == 2) {
+      if (conv) GB_FORM(2, true); else GB_FORM(2, false);
+    } else {
+      if (conv) GB_FORM(3, true); else GB_FORM(3, false);
+    }
 #undef GB_FORM
+  } else {
+    GB_CUDA(c.asm_E.n >= size_t(nc) * nl * nl ? cudaSuccess
+                                               : c.asm_E.alloc(size_t(nc) * nl * nl));
+    const bool pq1 = L.mesh_deg == 3, lps = conv && L.m_lps_s0 > 0.0;
+    const double bnorm = std::sqrt(b0 * b0 + b1 * b1 + b2 * b2) + 1e-6;
+#define GB_ELEM2(D, CV, LP, PQ)                                                          \
+  launch(c, k_q2_element_warp<D, CV, LP, PQ>, blocks_for(int64_t(nc) * 32, 128), 128, nc, \
+         (const int*)L.m_cells.p, (const double*)L.m_coords.p, (const double*)L.m_kappa.p, \
+         b0, b1, b2, c.asm_E.p, L.m_lps_s0, L.m_lps_xeta, bnorm, g)
+#define GB_ELEM2K(D, PQ)                                                                 \
+  do {                                                                                   \
+    if (lps) GB_ELEM2(D, true, true, PQ);                                                \
+    else if (conv) GB_ELEM2(D, true, false, PQ);                                         \
+    else GB_ELEM2(D, false, false, PQ);                                                  \
+  } while (0)
+    if (dim == 2) {
+      if (pq1) GB_ELEM2K(2, true); else GB_ELEM2K(2, false);
+      launch(c, k_elem_apply<9>, blocks_for(int64_t(nc) * 32, 128), 128, nc,
+             (const int*)L.m_cells.p, (const double*)c.asm_E.p, (const double*)x, c.asm_R.p);
+    } else {
+      if (pq1) GB_ELEM2K(3, true); else GB_ELEM2K(3, false);
+      launch(c, k_elem_apply<27>, blocks_for(int64_t(nc) * 32, 128), 128, nc,
+             (const int*)L.m_cells.p, (const double*)c.asm_E.p, (const double*)x, c.asm_R.p);
+    }
+#undef GB_ELEM2
+#undef GB_ELEM2K
+  }
   launch(c, k_form_gather, blocks_for(L.n, 256), 256, (int)L.n, (const int*)L.m_nptr.p,
-         (const int*)L.m_nlist.p, (const double*)c.asm_E.p, d, y);
+         (const int*)L.m_nlist.p, (const double*)c.asm_R.p, d, y);
+  if (L.has_hn()) {
+    Em.hn_zero(l, x);
+    Em.hn_distribute(l, y);
+  }
 }
 
 static void
@@ -4564,16 +4606,16 @@ gb_level_set_mesh_degree(gb_ctx* ctx, int lvl, int dim, int degree, int64_t ncel
   for (int64_t r = 0; r < n; ++r)
     dpos[r] = static_cast<int>(sell_pos(r, L.h_diag[r]));
   std::vector<int> nptr(n + 1, 0), nlist(size_t(ncells) * nl);
-  for (int64_t c = 0; c < ncells; ++c)
+  for (int64_t c = 0; c < ncells; ++c) // the cells' own nodes (Form, then HNDistribute)
     for (int a = 0; a < nl; ++a)
-      nptr[ci[c * nl + a] + 1]++;
+      nptr[cell_nodes[c * nl + a] + 1]++;
   for (int64_t r = 0; r < n; ++r)
     nptr[r + 1] += nptr[r];
   {
     std::vector<int> fill(nptr.begin(), nptr.end() - 1);
     for (int64_t c = 0; c < ncells; ++c) // ascending cells
       for (int a = 0; a < nl; ++a)
-        nlist[fill[ci[c * nl + a]]++] = static_cast<int>(int64_t(a) * ncells + c);
+        nlist[fill[cell_nodes[c * nl + a]]++] = static_cast<int>(int64_t(a) * ncells + c);
   }
   std::vector<int64_t> par;
   if (lvl > 0) {

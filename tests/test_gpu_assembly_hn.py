@@ -122,8 +122,7 @@ def test_hn_assembly_matches_q2_ball_generator(ctx, coarse, refine):
 
 def test_hn_reassembly_and_mesh_rules(ctx):
     """A second kappa (per element, varying) on the hanging-node level against
-    the oracle; the hanging-node lists set again drop the mesh; Form refuses a
-    level with hanging nodes."""
+    the oracle; the hanging-node lists set again drop the mesh."""
     name, degree, diff, beta = golden_hn_assembly_cases()[0]
     P, _ = load_golden(name)
     ctx.load_problem(P)
@@ -137,13 +136,6 @@ def test_hn_reassembly_and_mesh_rules(ctx):
         assert np.abs(v - ovals[l]).max() <= 1e-13 * np.abs(ovals[l]).max(), l
         assert np.array_equal(ctx.level_kappa(l, okap[l].size), okap[l])
     fl = P.nlevels - 1
-    with pytest.raises(GBError, match="hanging"):
-        x, y = ctx.vec(), ctx.vec()
-        try:
-            ctx.form(fl, y, x)
-        finally:
-            ctx.free(x)
-            ctx.free(y)
     ctx.load_problem(P)  # the matrix and hanging nodes again: the mesh is gone
     with pytest.raises(GBError, match="no mesh"):
         ctx.assemble(fl, kap)

@@ -104,3 +104,66 @@ def test_vtk_file_matches_reference(ctx, name):
         bad[0, 0] = P.finest.n
         ctx.write_vtk(fl, u, os.path.join(d, "bad"), 0, P.dim, bad, P.finest.coord)
     ctx.free(u)
+
+
+def _form_cases():
+    from _util import golden_cases
+    out = []
+    for n in golden_cases():
+        if n.startswith("form_"):
+            continue
+        with np.load(os.path.join(os.path.dirname(__file__), "golden", n + ".npz")) as z:
+            if "formx" in z.files:
+                out.append(n)
+    return out
+
+
+@pytest.mark.parametrize("name", _form_cases())
+def test_form_on_patch_and_hanging_levels_matches_reference(ctx, name):
+    """StdSolver::Form and NewtonResidual on levels of Q2 elements, of Q1
+    functions on patches with LPS, and with hanging nodes (HNAverage of x, the
+    residuals at the cells' own nodes, HNZero of x, HNDistribute of y): the
+    reference's vectors within 1e-13."""
+    from _util import (ball_meshes, golden_kappa_beta, golden_lps_cases, q2_element_kappa,
+                       uniform_meshes_q2)
+    P, ref = load_golden(name)
+    ctx.load_problem(P)
+    keys = ref["keys"]
+    lps = None
+    if name.startswith("hn_"):
+        deg = 2 if str(keys["disc"]) == "Q2" else 1
+        meshes = ball_meshes(P, deg)
+        kap = np.full(meshes[-1][0].shape[0], float(keys["diff"]))
+        beta = ([float(t) for t in str(keys["conv"]).split(",")] if "conv" in keys else None)
+    elif name.startswith("lps_"):
+        _, deg, diff, beta, lps = next(c for c in golden_lps_cases() if c[0] == name)
+        meshes = uniform_meshes_q2(P)
+        kap = np.full(meshes[-1][0].shape[0], diff)
+    else:  # q2_: the seeded per-cell kappa, per element the mean of its cells
+        deg = 2
+        kappa, beta = golden_kappa_beta(name)
+        meshes = uniform_meshes_q2(P)
+        kap = q2_element_kappa(P.dim, kappa, round(len(kappa) ** (1.0 / P.dim)))
+    for l, (el, par) in enumerate(meshes):
+        ctx.set_mesh(l, P.dim, el, P.levels[l].coord, par if l else None, degree=deg)
+    try:
+        if lps:
+            ctx.set_assembly_lps(*lps)
+        ctx.assemble_levels(kap, beta)
+    finally:
+        ctx.set_assembly_lps(0.0)
+    fl = P.nlevels - 1
+    x, y, b = ctx.vec(), ctx.vec(), ctx.vec()
+    ctx.upload(fl, x, ref["formx"])
+    ctx.upload(fl, y, np.zeros(P.finest.ndof))
+    ctx.form(fl, y, x, 1.0)
+    scale = np.abs(ref["form"]).max()
+    assert np.abs(ctx.download(fl, y) - ref["form"]).max() <= 1e-13 * scale
+    ctx.upload(fl, x, ref["formx"])
+    ctx.upload(fl, b, P.rhs)
+    nr = ctx.newton_residual(y, x, b)
+    scale = np.abs(ref["newton_residual"]).max()
+    assert np.abs(ctx.download(fl, y) - ref["newton_residual"]).max() <= 1e-13 * scale
+    assert abs(nr - ref["newton_norm"]) <= 1e-13 * ref["newton_norm"]
+    for v in (x, y, b):
+        ctx.free(v)
