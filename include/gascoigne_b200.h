@@ -341,8 +341,7 @@ int gb_level_set_mesh(gb_ctx* ctx, int level, int dim, int64_t ncells,
  * with the Q1 functions of their cells (CGQ1Patch / CGQ1Lps: BaseQ12dPatch /
  * BaseQ13dPatch, Discretization/Q2/baseq1patch.h; QuadGauss4 / HexGauss8 in
  * every cell, PatchFormula2d/3d, Discretization/Q2/patchintegrationformula.xx:
- * 55-83); the matrix equals the Q1 cells' up to rounding, and LPS needs it. gb_form is built for Q1
- * levels without hanging nodes only. */
+ * 55-83); the matrix equals the Q1 cells' up to rounding, and LPS needs it. */
 int gb_level_set_mesh_degree(gb_ctx* ctx, int level, int dim, int degree,
                              int64_t ncells, const int64_t* cell_nodes,
                              const double* coords, const int64_t* parent);
@@ -385,9 +384,12 @@ int gb_level_get_kappa(gb_ctx* ctx, int level, double* kappa);
 int gb_level_get_values(gb_ctx* ctx, int level, double* val);
 /* StdSolver::Form (Solver/stdsolver.cc:1041-1063 -> CGDisc::Form,
  * DofHandler/cgdisc.h:415-450) of the equation last assembled on the level
- * (gb_assemble: its kappa and beta): y += d * sum over cells of the element
- * residuals of x, summed per node in ascending cell order (matrix-free, no
- * hanging nodes). Vectors are level vector ids. */
+ * (gb_assemble: its kappa, beta and LPS): y += d * sum over cells of the
+ * element residuals of x, summed per node in ascending cell order (Q1 cells:
+ * matrix-free; patch elements: the element matrices times the local values).
+ * On a level with hanging nodes x is HNAverage'd first and HNZero'd after, and
+ * y is HNDistribute'd, as the reference's Form does (x is changed the same
+ * way). Vectors are level vector ids. */
 int gb_form(gb_ctx* ctx, int level, int y, int x, double d);
 /* StdMultiLevelSolver::NewtonResidual (Solver/stdmultilevelsolver.cc:609-623)
  * on the finest level: y = b - Form(x), zero on the Dirichlet dofs; *norm (may

@@ -211,3 +211,57 @@ def test_oracle_lps_assembly_matches_reference(name, kind, diff, beta, lps):
         assert np.abs(v - L.val).max() <= 1e-13 * np.abs(L.val).max(), l
         w = assemble(L.n, L.rowptr, L.col, el, f(P.dim, L.coord[el], kap, beta), L.dirichlet)
         assert np.abs(w - L.val).max() > 1e-3 * np.abs(L.val).max(), l
+
+
+def _patch_form_cases():
+    from _util import golden_cases
+    out = []
+    for n in golden_cases():
+        if not n.startswith("form_"):
+            with np.load(os.path.join(os.path.dirname(__file__), "golden", n + ".npz")) as z:
+                if "formx" in z.files:
+                    out.append(n)
+    return out
+
+
+@pytest.mark.parametrize("name", _patch_form_cases())
+def test_oracle_form_on_patch_and_hanging_levels_matches_reference(name):
+    """StdSolver::Form restated (Solver/stdsolver.cc:1041-1063): HNAverage of x,
+    the uncondensed element matrices times the local values added at the
+    cells' own nodes, HNDistribute of the result; the reference's Form of a
+    seeded vector within 1e-13 (Q2, Q1 on patches with LPS, hanging nodes)."""
+    from _util import golden_kappa_beta, golden_lps_cases, q2_element_kappa, uniform_meshes_q2
+    from oracle.assembly import (q1_element_matrices, q1patch_element_matrices,
+                                 q2_element_matrices)
+    from oracle.oracle import Oracle
+    P, ref = load_golden(name)
+    keys = ref["keys"]
+    F = P.finest
+    lps = None
+    if name.startswith("hn_"):
+        deg = 2 if str(keys["disc"]) == "Q2" else 1
+        el = ball_meshes(P, deg)[-1][0]
+        kap = np.full(el.shape[0], float(keys["diff"]))
+        beta = ([float(t) for t in str(keys["conv"]).split(",")] if "conv" in keys else None)
+    elif name.startswith("lps_"):
+        _, deg, diff, beta, lps = next(c for c in golden_lps_cases() if c[0] == name)
+        el = uniform_meshes_q2(P)[-1][0]
+        kap = np.full(el.shape[0], diff)
+    else:
+        deg = 2
+        kappa, beta = golden_kappa_beta(name)
+        el = uniform_meshes_q2(P)[-1][0]
+        kap = q2_element_kappa(P.dim, kappa, round(len(kappa) ** (1.0 / P.dim)))
+    f = {1: q1_element_matrices, 2: q2_element_matrices, 3: q1patch_element_matrices}[deg]
+    E = f(P.dim, F.coord[el], kap, beta) if lps is None else f(P.dim, F.coord[el], kap, beta,
+                                                               lps)
+    x = ref["formx"]
+    O = Oracle(P)
+    fl = P.nlevels - 1
+    if F.hn_edges is not None:
+        x = O.hn("average", fl, x)
+    y = np.zeros(F.n)
+    np.add.at(y, el, np.einsum("cab,cb->ca", E, x[el]))
+    if F.hn_edges is not None:
+        y = O.hn("distribute", fl, y)
+    assert np.abs(y - ref["form"]).max() <= 1e-13 * np.abs(ref["form"]).max()
