@@ -33,7 +33,7 @@ def main(argv=None):
     ap.add_argument("--smoother", default=None, choices=["jacobi", "vanka", "ilu"],
                     help="override the problem's smoother (ilu: omega 1)")
     ap.add_argument("--assemble", type=int, default=0,
-                    help="only K device assemblies of every level (diffusion problem)")
+                    help="only K device assemblies of every level (diffusion, q2, q2ball)")
     ap.add_argument("--ktime", action="store_true",
                     help="per-kernel CUDA-event times of the last solve (GB_GRAPH=0)")
     a = ap.parse_args(argv)
@@ -67,15 +67,25 @@ def main(argv=None):
         fl = P.nlevels - 1
         if a.assemble:
             import time
-            from gascoignelib_b200.problem import structured_meshes
-            for l, (cells, coord, par) in enumerate(structured_meshes(P)):
-                ctx.set_mesh(l, P.dim, cells, coord, par)
-            ctx.assemble_levels(kappa)  # set-up outside the count
+            beta = None
+            if a.problem in ("q2", "q2ball"):  # Q2 elements (ball: hanging nodes condensed)
+                import numpy as np
+                from gascoignelib_b200.problem import q2_meshes
+                meshes = q2_meshes(P)
+                for l, (el, par) in enumerate(meshes):
+                    ctx.set_mesh(l, P.dim, el, P.levels[l].coord, par, degree=2)
+                kappa = np.full(meshes[-1][0].shape[0], P.info["eps"])
+                beta = P.info.get("beta") or (1.0, 0.5, 0.25)
+            else:
+                from gascoignelib_b200.problem import structured_meshes
+                for l, (cells, coord, par) in enumerate(structured_meshes(P)):
+                    ctx.set_mesh(l, P.dim, cells, coord, par)
+            ctx.assemble_levels(kappa, beta)  # set-up outside the count
             ctx.synchronize()
             k0 = ctx.kernel_count()
             t0 = time.time()
             for _ in range(a.assemble):
-                ctx.assemble_levels(kappa)
+                ctx.assemble_levels(kappa, beta)
             ctx.synchronize()
             print(json.dumps({"assemblies": a.assemble, "kernels": ctx.kernel_count() - k0,
                               "wall_ms_each": 1e3 * (time.time() - t0) / a.assemble}))
