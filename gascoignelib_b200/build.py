@@ -44,8 +44,11 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
 def build_oracle() -> None:
     """Compiles the oracle's C restatement and, when the reference sources are
     present, the reference CPU solver (test infrastructure only)."""
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True,
-                   capture_output=True)
+    cmd = ["make", "-C", os.path.join(ROOT, "oracle")]
+    ref = os.environ.get("GB_REFERENCE_SRC", "/root/reference/src")
+    if os.path.isdir(ref):
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True, capture_output=True)
 
 
 def build(force: bool = False) -> None:

@@ -1002,10 +1002,13 @@ k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
 //  MODE 0: c1[i] = <w, V_i>;                         H[j][i]  = c1[i]
 //  MODE 1: w -= sum_i c1[i] V_i; c2[i] = <w, V_i>;   H[j][i] += c2[i]
 //  MODE 2: w -= sum_i c2[i] V_i; s = ||w||;          H[j][j+1] = s
-// One pass over the j+1 basis vectors; per-thread dot accumulators live in
-// shared memory (column per thread); block and grid reductions are warp-parallel
-// and deterministic (fixed grid, fixed order).
-constexpr int kCgsThreads = 1024;
+// A streaming pass over the j+1 basis vectors: each thread visits rows
+// grid-strided and keeps its j+1 partial dot products in registers (the
+// accumulator array is indexed by compile-time constants under a runtime
+// guard), so a row costs j+1 independent loads and FMAs and no shuffle. One
+// warp-shuffle block reduction per launch, then the last block sums the
+// per-block partials in block order: deterministic for a fixed grid.
+constexpr int kCgsThreads = 256;
 
 __device__ void fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m,
                         int use_cond);
@@ -1019,6 +1022,7 @@ k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
 {
   GB_PDL_ENTRY();
   constexpr int kWarps = kCgsThreads / 32;
+  constexpr int kAcc = (MODE == 2) ? 1 : kCgsMaxJ;
   __shared__ double s_coef[kCgsMaxJ];
   __shared__ double s_warp[kWarps][kCgsMaxJ];
   __shared__ bool am_last;
@@ -1029,34 +1033,37 @@ k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
   double* w = V + int64_t(j + 1) * n;
   if (MODE >= 1 && tid < kCgsMaxJ)
     s_coef[tid] = (tid < nv) ? (MODE == 1 ? G->d[tid] : G->d2[tid]) : 0.0;
-  s_warp[wid][lane] = 0.0;
   __syncthreads();
-  // warp-uniform loop: every lane takes part in the shuffles
-  for (int64_t base = int64_t(blockIdx.x) * kCgsThreads + wid * 32; base < n;
-       base += int64_t(gridDim.x) * kCgsThreads) {
-    const int64_t r = base + lane;
-    const bool ok = r < n;
-    double t = ok ? w[r] : 0.0;
+  double acc[kAcc];
+#pragma unroll
+  for (int i = 0; i < kAcc; ++i)
+    acc[i] = 0.0;
+  const int64_t stride = int64_t(gridDim.x) * kCgsThreads;
+  for (int64_t r = int64_t(blockIdx.x) * kCgsThreads + tid; r < n; r += stride) {
+    double t = w[r];
     if (MODE >= 1) {
+#pragma unroll 4
       for (int i = 0; i < nv; ++i)
-        t = fma(-s_coef[i], ok ? V[int64_t(i) * n + r] : 0.0, t);
-      if (ok)
-        w[r] = t;
+        t = fma(-s_coef[i], V[int64_t(i) * n + r], t);
+      w[r] = t;
     }
     if (MODE <= 1) {
-      for (int i = 0; i < nv; ++i) {
-        double p = ok ? t * V[int64_t(i) * n + r] : 0.0;
-        for (int o = 16; o > 0; o >>= 1)
-          p += __shfl_down_sync(0xffffffffu, p, o);
-        if (lane == 0)
-          s_warp[wid][i] += p;
-      }
+#pragma unroll
+      for (int i = 0; i < kAcc; ++i)
+        if (i < nv)
+          acc[i] = fma(t, V[int64_t(i) * n + r], acc[i]);
     } else {
-      double p = t * t;
+      acc[0] = fma(t, t, acc[0]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kAcc; ++i) {
+    if (i < nred) {
+      double p = acc[i];
       for (int o = 16; o > 0; o >>= 1)
         p += __shfl_down_sync(0xffffffffu, p, o);
       if (lane == 0)
-        s_warp[wid][0] += p;
+        s_warp[wid][i] = p;
     }
   }
   __syncthreads();

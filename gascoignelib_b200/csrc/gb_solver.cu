@@ -2914,8 +2914,9 @@ fg_inner(Context& c, const FBufs<T>& F, cudaGraphConditionalHandle hInner, int u
   precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true);
   spmv<kAx, double, T, double>(c, L, opA(c, L), (const T*)F.zfix, V, nullptr, nullptr, 1.0,
                                (const int*)&G->j, n, F.Z);
+  // one block of kCgsThreads per 2 kCgsThreads rows, at most two per SM
   const int rg = static_cast<int>(std::max<int64_t>(
-    1, std::min<int64_t>((n + kCgsThreads - 1) / kCgsThreads, kMaxRedBlocks)));
+    1, std::min<int64_t>((n + 2 * kCgsThreads - 1) / (2 * kCgsThreads), kMaxRedBlocks)));
   const int m = c.params.gmressize - 1;
   launch(c, k_cgs<0>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m, 0);
   launch(c, k_cgs<1>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m, 0);
@@ -3556,14 +3557,26 @@ int
 gb_level_set_dirichlet(gb_ctx* ctx, int lvl, int64_t nnodes, const int64_t* nodes,
                        int comp_mask)
 {
+  if (nnodes < 0)
+    return gb_level_set_dirichlet_masks(ctx, lvl, nnodes, nodes, nullptr);
+  std::vector<int> masks(static_cast<size_t>(nnodes), comp_mask);
+  return gb_level_set_dirichlet_masks(ctx, lvl, nnodes, nodes, masks.data());
+}
+
+int
+gb_level_set_dirichlet_masks(gb_ctx* ctx, int lvl, int64_t nnodes, const int64_t* nodes,
+                             const int* comp_masks)
+{
   GB_API_BEGIN
   ctx->version++;
   Level& L = level_with_matrix(*ctx, lvl);
-  GB_REQUIRE(nnodes >= 0 && (nnodes == 0 || nodes), GB_EINVAL, "bad node list");
+  GB_REQUIRE(nnodes >= 0 && (nnodes == 0 || (nodes && comp_masks)), GB_EINVAL,
+             "bad node list");
   std::vector<uint8_t> mask(L.ndof(), 0);
   std::vector<int> dofs;
   for (int64_t k = 0; k < nnodes; ++k) {
     GB_REQUIRE(nodes[k] >= 0 && nodes[k] < L.n, GB_EINVAL, "Dirichlet node out of range");
+    const int comp_mask = comp_masks[k];
     for (int c = 0; c < L.B; ++c)
       if (comp_mask & (1 << c)) {
         int64_t d = nodes[k] * L.B + c;
@@ -5081,6 +5094,19 @@ gb_bench_spmv(gb_ctx* ctx, int lvl, int precision, int reps, int flush_l2,
   GB_API_END
 }
 
+int
+gb_kernel_arch(int* binary_version, int* ptx_version)
+{
+  if (!binary_version || !ptx_version)
+    return GB_EINVAL;
+  cudaFuncAttributes a{};
+  if (cudaFuncGetAttributes(&a, gb::k_dot<double, double>) != cudaSuccess)
+    return GB_ECUDA;
+  *binary_version = a.binaryVersion;
+  *ptx_version = a.ptxVersion;
+  return GB_OK;
+}
+
 // ------------------------------------------------- allocation-free dot product
 //
 // Scratch of gb_dot_noalloc: one FP64 partial per block plus the last-block
@@ -5118,9 +5144,17 @@ gb_dot_noalloc(const double* a, const double* b, int64_t n, double* out, void* s
             (long long)n, (long long)kNoAllocMaxN, kNoAllocBlocks);
     return GB_EINVAL;
   }
+  // an error the caller's own earlier work left pending is reported, not
+  // consumed: cudaGetLastError after our launch would otherwise clear it
+  if (cudaPeekAtLastError() != cudaSuccess) {
+    fprintf(stderr, "gb_dot_noalloc: a CUDA error is already pending\n");
+    return GB_ECUDA;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
     return GB_ECUDA;
+  // the address is looked up once per device ordinal and kept for the life of
+  // the process (it does not survive cudaDeviceReset of that device)
   NoAllocAddr addr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mutex);

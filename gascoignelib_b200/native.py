@@ -62,6 +62,8 @@ _SIGS = {
     "gb_set_nlevels": [C.c_void_p, C.c_int],
     "gb_level_set_matrix": [C.c_void_p, C.c_int, C.c_int64, C.c_int, _P64, _P64, _P64, _PD],
     "gb_level_set_dirichlet": [C.c_void_p, C.c_int, C.c_int64, _P64, C.c_int],
+    "gb_level_set_dirichlet_masks": [C.c_void_p, C.c_int, C.c_int64, _P64,
+                                     C.POINTER(C.c_int)],
     "gb_level_set_transfer": [C.c_void_p, C.c_int, C.c_int64, _P64, C.c_int64, _P64,
                               C.c_int64, _P64, C.c_int64, _P64],
     "gb_level_size": [C.c_void_p, C.c_int, _P64, C.POINTER(C.c_int), _P64],
@@ -124,6 +126,7 @@ _SIGS = {
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
     "gb_bench_spmv": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
+    "gb_kernel_arch": [C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "gb_dot_noalloc": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
     "gb_get_kernel_times": [C.c_void_p, C.c_char_p, C.c_int64],
 }

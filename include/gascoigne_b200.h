@@ -5,7 +5,7 @@
  * backend (cuda/): the drop-in subclasses B200Solver : StdSolver,
  * B200MultiLevelSolver : StdMultiLevelSolver and B200MgInterpolatorNested :
  * MgInterpolatorNested forward their virtual overrides to these functions
- * (see INTEGRATION.md). Plain pointers and sizes only.
+ * (gascoignelib_b200/binding/b200solver.h). Plain pointers and sizes only.
  *
  * Conventions
  *  - Every function returns int status: GB_OK (0) or a GB_E* code; the message
@@ -120,6 +120,12 @@ int gb_level_set_matrix(gb_ctx* ctx, int level, int64_t n, int B,
  * (DofHandler/cgdisc.h:1162-1179). */
 int gb_level_set_dirichlet(gb_ctx* ctx, int level, int64_t nnodes,
                            const int64_t* nodes, int comp_mask);
+/* The same with one component mask per node: the union over the Dirichlet
+ * colours of each colour's components (DirichletData::components_on_color,
+ * CGDisc::StrongDirichletVectorZero loops colours, DofHandler/cgdisc.h:
+ * 1162-1179). Nodes must be distinct. */
+int gb_level_set_dirichlet_masks(gb_ctx* ctx, int level, int64_t nnodes,
+                                 const int64_t* nodes, const int* comp_masks);
 /* Mesh-transfer maps between coarse level `level` and level+1, as
  * GascoigneMeshTransfer holds them (Mesh/gascoignemeshtransfer.h:48-51):
  * c2f[ncoarse]; zweier rows [fine, c0, c1]; vierer [fine, c0..c3]; achter
@@ -444,20 +450,35 @@ int gb_get_kernel_count(const gb_ctx* ctx, int64_t* launches);
 int gb_bench_spmv(gb_ctx* ctx, int level, int precision, int reps,
                   int flush_l2, double* ms_per_launch, double* bytes_per_launch);
 
+/* The compute capability the library's kernels were compiled for, read at run
+ * time from a kernel's attributes on the current device (cudaFuncGetAttributes:
+ * binaryVersion, ptxVersion; 100 for sm_100a). Needs a device. */
+int gb_kernel_arch(int* binary_version, int* ptx_version);
+
 /* ---- allocation-free dot product -----------------------------------------
  * No counterpart in the reference. For callers that cannot allocate device
- * memory: code running while a CUDA stream is being captured into a graph
- * (cudaMalloc is not capturable), applications that hand all device memory
- * to their own pool up front, and host callbacks that must not allocate.
+ * memory once they run: an application that hands all device memory to its
+ * own pool allocator at start-up (a larger simulation code or framework that
+ * owns the GPU), where a cudaMalloc in the middle of a solve fails or splits
+ * the pool, and latency-critical loops that cannot afford the device-wide
+ * synchronisation a cudaMalloc / cudaFree pair implies.
  * Computes *out = <a, b> over n doubles; a, b and out are device pointers
  * the caller owns; work is enqueued on `stream` (a cudaStream_t, NULL for the
  * default stream). It allocates nothing: its reduction scratch is a
  * file-scope device array of 4096 partial sums (32 KiB) that every GPU which
  * loads this library keeps until the process exits, so n is limited to
- * 4096 * 2048 = 8,388,608; larger n returns GB_EINVAL. The first call on a
- * device looks up that array's device address and should come before any
- * stream capture. Calls share the array: two calls that overlap on the GPU
- * (other streams, other host threads) race and give wrong sums. Same
+ * 4096 * 2048 = 8,388,608; larger n returns GB_EINVAL.
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress, with that device current) and keeps it for the life
+ * of the process; that first call should come before any stream capture. The
+ * kept address does not survive cudaDeviceReset: a caller that resets a
+ * device must not call this function on it again in the same process.
+ * The function makes CUDA runtime calls, so it must not be called from a CUDA
+ * host function (cudaLaunchHostFunc, stream callbacks). Calls share the
+ * array, and each call clears its ticket before use: two calls that overlap
+ * on the GPU (other streams, other host threads) race and give wrong sums.
+ * An error that an earlier launch of the caller left pending is reported as
+ * GB_ECUDA before anything is enqueued, and is not cleared. Same
  * deterministic reduction as gb_vec_dot; for n <= 606,208 the two use the
  * same partition and return the same bits. */
 int gb_dot_noalloc(const double* a, const double* b, int64_t n, double* out,

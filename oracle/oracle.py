@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libgascoigne_oracle.so")
 REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
+REF_HARNESS_B200 = os.path.join(HERE, "_ref", "ref_harness_b200")
 
 _P64 = C.POINTER(C.c_int64)
 _PD = C.POINTER(C.c_double)
@@ -256,18 +257,24 @@ class Oracle:
                    "history": hist[:max(it.value, 0)]}
 
 
-def run_reference(out_dir=None, threads=None, **kw):
+def run_reference(out_dir=None, threads=None, harness=None, **kw):
     """Runs the compiled reference harness; returns (out_dir, summary dict).
-    threads: OpenMP threads (1 makes Vanka's patch sums ordered)."""
-    if not os.path.exists(REF_HARNESS):
-        raise FileNotFoundError(REF_HARNESS)
+    threads: OpenMP threads (1 makes Vanka's patch sums ordered); harness:
+    REF_HARNESS_B200 runs the build that links the B200 binding (key
+    backend=b200 or b200host selects B200MultiLevelSolver)."""
+    exe = harness or REF_HARNESS
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
     if out_dir is None:
         out_dir = tempfile.mkdtemp(prefix="gb_ref_")
-    args = [REF_HARNESS, f"out={out_dir}"] + [f"{k}={v}" for k, v in kw.items()]
+    args = [exe, f"out={out_dir}"] + [f"{k}={v}" for k, v in kw.items()]
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
-    subprocess.run(args, check=True, capture_output=True, env=env)
+    r = subprocess.run(args, capture_output=True, env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(exe)} failed ({r.returncode}): "
+                           + r.stderr.decode(errors="replace")[-2000:])
     summ = {}
     with open(os.path.join(out_dir, "summary.txt")) as f:
         for line in f:

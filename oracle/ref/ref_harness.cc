@@ -70,12 +70,15 @@
 #include <cstdlib>
 #include <fstream>
 #include <map>
+#include <memory>
 #include <sstream>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "cginfo.h"
 #include "columndiagstencil.h"
+#include "domainfunctional.h"
 #include "equation.h"
 #include "fmatrixblock.h"
 #include "functionalcontainer.h"
@@ -92,7 +95,11 @@
 #include "pressurefilter.h"
 #include "lpsequation.h"
 #include "lpsstabilization.h"
+#include "navierstokes.h"
 #include "zerodirichletdata.h"
+#ifdef GB_B200_BINDING
+#include "b200solver.h"
+#endif
 
 using namespace Gascoigne;
 
@@ -119,6 +126,13 @@ struct Config
   int backup = 0;     // write the solution with WriteBackUp / WriteBackUpBinary
   int vtk = 0;        // write the solution with StdSolver::Visu (VTK)
   std::string formx;  // Form and NewtonResidual of this finest-level vector
+  std::string backend = "cpu"; // cpu: StdMultiLevelSolver; b200 / b200host /
+                               // b200mixed: B200MultiLevelSolver (binary built
+                               // with the binding): the whole solve as one
+                               // device call, the reference's GMRES over device
+                               // operations, or the mixed-precision device solve
+  int savesol = 0;    // write rhs.f64 and solution.f64 without the full dump
+  int functional = 0; // functional_l2 in summary.txt: J(u) of L2Functional
 };
 
 // kappa per cell, one array per resolution N = coarse * 2^l (cells per dim),
@@ -319,6 +333,107 @@ public:
   }
 };
 
+// Stokes with LPS pressure stabilisation (problem=stokeslps): the reference's
+// NavierStokesLps (Problems/navierstokes.h:91-280, discretisation CGQ1Lps)
+// linearised at u = 0. Its Jacobian at U = 0 is already the Stokes operator
+// plus alpha (grad p - pi grad p, grad q - pi grad q) with alpha = alpha0 h^2 /
+// visc (lpspoint at zero velocity); Form drops the convection term so that the
+// residual of the lid data is that same linear operator's.
+template<int DIM>
+class StokesLpsEquation : public NavierStokesLps<DIM>
+{
+public:
+  explicit StokesLpsEquation(const NavierStokesData& d)
+    : NavierStokesLps<DIM>(d)
+  {}
+  StokesLpsEquation* createNew() const override
+  {
+    return new StokesLpsEquation(this->data);
+  }
+  std::string GetName() const override { return "OracleStokesLps"; }
+  void Form(VectorIterator b, const FemFunction& U, const TestFunction& N) const override
+  {
+    for (int i = 0; i < DIM; ++i) {
+      b[0] += U[i + 1][i + 1] * N.m();
+      for (int j = 0; j < DIM; ++j)
+        b[i + 1] += this->data.visc * U[i + 1][j + 1] * N[j + 1];
+      b[i + 1] -= U[0].m() * N[i + 1];
+    }
+  }
+};
+
+// Lid-driven cavity data: velocity (1, 0[, 0]) on the top face (y = 1 in 2D,
+// z = 1 in 3D, its edges included), 0 on the rest of the boundary.
+class LidDirichletData : public DirichletData
+{
+public:
+  explicit LidDirichletData(const ParamFile& pf)
+    : DirichletData(pf)
+  {}
+  std::string GetName() const override { return "OracleLid"; }
+  void operator()(DoubleVector& b, const Vertex2d& v, int) const override
+  {
+    b.zero();
+    if (v.y() > 1.0 - 1e-12)
+      b[1] = 1.0;
+  }
+  void operator()(DoubleVector& b, const Vertex3d& v, int) const override
+  {
+    b.zero();
+    if (v.z() > 1.0 - 1e-12)
+      b[1] = 1.0;
+  }
+};
+
+class StokesLpsProblem : public ProblemDescriptorBase
+{
+public:
+  void BasicInit(const ParamFile& pf, int dim, double visc, double alpha0)
+  {
+    GetParamFile() = pf;
+    NavierStokesData d;
+    d.visc = visc;
+    d.alpha = alpha0;
+    d.delta = 0.0;
+    d.symmetrictensor = false;
+    d.outflowcolor = -1;
+    d.dt = 0.0;
+    d.theta = 0.0;
+    if (dim == 2)
+      GetEquationPointer() = new StokesLpsEquation<2>(d);
+    else
+      GetEquationPointer() = new StokesLpsEquation<3>(d);
+    GetDirichletDataPointer() = new LidDirichletData(pf);
+    ProblemDescriptorBase::BasicInit(pf);
+  }
+};
+
+// J(u) = int sum_c u_c^2 over the components c (the scalar unknown, or the
+// velocity of a Stokes system), evaluated by the reference's own
+// StdSolver::ComputeFunctional -> ComputeDomainFunctional (hanging values
+// averaged first, Solver/stdsolver.cc:1186-1246).
+class L2Functional : public DomainFunctional
+{
+  std::vector<int> comps_;
+
+public:
+  explicit L2Functional(std::vector<int> comps)
+    : comps_(std::move(comps))
+  {}
+  std::string GetName() const override { return "OracleL2"; }
+  double J(const FemFunction& U, const Vertex2d&) const override { return sq(U); }
+  double J(const FemFunction& U, const Vertex3d&) const override { return sq(U); }
+
+private:
+  double sq(const FemFunction& U) const
+  {
+    double s = 0.0;
+    for (int c : comps_)
+      s += U[c].m() * U[c].m();
+    return s;
+  }
+};
+
 // the pressure filter's domain size is not exposed by PressureFilter, and
 // StdSolver::GetPfilter is protected: read both through derived-class access
 struct PressureFilterView : public PressureFilter
@@ -395,6 +510,9 @@ parse(int argc, char** argv)
     else if (k == "diff") c.diff = atof(v.c_str());
     else if (k == "lps") c.lps = atof(v.c_str());
     else if (k == "rhsres") c.rhsres = atoi(v.c_str());
+    else if (k == "backend") c.backend = v;
+    else if (k == "savesol") c.savesol = atoi(v.c_str());
+    else if (k == "functional") c.functional = atoi(v.c_str());
     else if (k == "conv") {
       std::stringstream ss(v);
       std::string t;
@@ -512,7 +630,7 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "gridname " << grid << "\n\n"
     << "//Block BoundaryManager\n"
     << "dirichlet 1 1\n";
-  if (c.problem == "stokes") {
+  if (c.problem == "stokes" || c.problem == "stokeslps") {
     o << "dirichletcomp 1 " << c.dim;
     for (int d = 1; d <= c.dim; ++d)
       o << " " << d;
@@ -530,7 +648,8 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "//Block Solver\n"
     << "matrixtype " << (c.smoother == "vanka" ? "vanka" : "block") << "\n"
     << "discname "
-    << (c.disc == "Q2" ? (c.lps > 0.0 ? "CGQ2Lps" : "CGQ2") : (c.lps > 0.0 ? "CGQ1Lps" : "CGQ1"))
+    << (c.disc == "Q2" ? (c.lps > 0.0 ? "CGQ2Lps" : "CGQ2")
+                       : (c.lps > 0.0 || c.problem == "stokeslps" ? "CGQ1Lps" : "CGQ1"))
     << "\n"
     << "ndirect " << c.ndirect << "\n"
     << "iterpre " << c.iterpre << "\n"
@@ -539,7 +658,7 @@ write_param(const Config& c, const std::string& path, const std::string& grid)
     << "linear_smooth " << (c.smoother == "vanka" || c.smoother == "ilu" ? "ilu" : "jacobi")
     << "\n"
     << "omega " << c.omega << "\n";
-  if (c.problem == "stokes" && c.pfilter)
+  if ((c.problem == "stokes" || c.problem == "stokeslps") && c.pfilter)
     o << "pfilter 1 0\n";
 }
 
@@ -601,7 +720,7 @@ block_values(const MatrixInterface& MI, std::vector<double>& val,
 } // namespace
 
 int
-main(int argc, char** argv)
+run(int argc, char** argv)
 {
   Config c = parse(argc, argv);
   std::string grid = c.out + "/oracle_mesh.inp";
@@ -613,15 +732,20 @@ main(int argc, char** argv)
   ParamFile pf(pfile);
   DiffusionProblem PD;
   StokesProblem PS;
-  const bool stokes = c.problem == "stokes";
-  if (stokes)
+  StokesLpsProblem PL;
+  const bool lid = c.problem == "stokeslps";
+  const bool stokes = c.problem == "stokes" || lid;
+  if (lid)
+    PL.BasicInit(pf, c.dim, c.visc, c.stab);
+  else if (stokes)
     PS.BasicInit(pf, c.dim, c.visc, c.stab);
   else
     PD.BasicInit(pf, c.dim, c.conv, c.lps);
   const int ncomp = stokes ? c.dim + 1 : 1;
   ProblemContainer PC;
-  PC.AddProblem("diffusion", stokes ? static_cast<ProblemDescriptorInterface*>(&PS)
-                                    : static_cast<ProblemDescriptorInterface*>(&PD));
+  PC.AddProblem("diffusion", lid ? static_cast<ProblemDescriptorInterface*>(&PL)
+                             : stokes ? static_cast<ProblemDescriptorInterface*>(&PS)
+                                      : static_cast<ProblemDescriptorInterface*>(&PD));
   FunctionalContainer FC;
 
   g_diff = c.diff;
@@ -654,7 +778,23 @@ main(int argc, char** argv)
     }
     MA.refine_cells(ref);
   }
-  StdMultiLevelSolver MLS;
+  std::unique_ptr<StdMultiLevelSolver> MLSp;
+  if (c.backend == "cpu")
+    MLSp.reset(new StdMultiLevelSolver);
+#ifdef GB_B200_BINDING
+  else if (c.backend == "b200" || c.backend == "b200host" || c.backend == "b200mixed") {
+    auto* B = new B200MultiLevelSolver(0);
+    B->SetDeviceGmres(c.backend != "b200host");
+    B->SetMixedPrecision(c.backend == "b200mixed");
+    MLSp.reset(B);
+  }
+#endif
+  else {
+    fprintf(stderr, "ref_harness: backend %s is not built into this binary\n",
+            c.backend.c_str());
+    return 2;
+  }
+  StdMultiLevelSolver& MLS = *MLSp;
   MLS.BasicInit(&MA, pf, &PC, &FC);
   MLS.ReInit();
   MLS.SetProblem("diffusion");
@@ -676,7 +816,18 @@ main(int argc, char** argv)
   const GascoigneMesh* Mf = S->GetMesh();
   const int nf = Mf->nnodes();
   GlobalVector& F = S->GetGV(f);
-  {
+  if (lid) {
+    // the right-hand side of the Newton update from the lid data u_D:
+    // f = 0 - Form(u_D), Dirichlet-zeroed, algebraically mean-free
+    // (StdMultiLevelSolver::NewtonResidual, Solver/stdmultilevelsolver.cc:609-623)
+    Vector ud("ud"), z0("z0");
+    MLS.ReInitVector(ud);
+    MLS.ReInitVector(z0);
+    S->Zero(ud);
+    S->Zero(z0);
+    S->SetBoundaryVector(ud);
+    MLS.NewtonResidual(f, ud, z0);
+  } else {
     size_t nlex = 1;
     for (int d = 0; d < c.dim; ++d)
       nlex *= Nf + 1;
@@ -716,6 +867,19 @@ main(int argc, char** argv)
   MLS.ReInitVector(r);
   S->residualgmres(A, r, u, f);
   double rnorm = S->Norm(r), fnorm = S->Norm(f);
+  double Jl2 = 0.0;
+  if (c.functional) {
+    std::vector<int> jc;
+    if (stokes)
+      for (int d = 1; d <= c.dim; ++d)
+        jc.push_back(d);
+    else
+      jc.push_back(0);
+    L2Functional JF(jc);
+    Vector jh("jh");
+    MLS.ReInitVector(jh);
+    Jl2 = S->ComputeFunctional(jh, u, &JF);
+  }
 
   {
     std::ofstream o(c.out + "/summary.txt");
@@ -730,6 +894,8 @@ main(int argc, char** argv)
     o << "firstresidual " << info.control().firstresidual() << "\n";
     o << "residual " << info.control().residual() << "\n";
     o << "true_rel_residual " << rnorm / fnorm << "\n";
+    if (c.functional)
+      o << "functional_l2 " << Jl2 << "\n";
     o << "ncomp " << ncomp << "\n";
     o << "disc " << c.disc << "\n";
     o << "dircomps";
@@ -747,12 +913,23 @@ main(int argc, char** argv)
           << "\n";
     o << "assemble_s "
       << std::chrono::duration<double>(t_as1 - t_as0).count() << "\n";
+    o << "backend " << c.backend << "\n";
+#ifdef GB_B200_BINDING
+    if (auto* B = dynamic_cast<B200MultiLevelSolver*>(&MLS))
+      o << "device_ms " << B->LastSolveInfo().device_ms << "\n"
+        << "device_launches " << B->LastSolveInfo().kernel_launches << "\n";
+#endif
     o << "solve_s";
     for (double t : times)
       o << " " << t;
     o << "\n";
   }
 
+  if (c.savesol && !c.dump) {
+    write_raw(c.out + "/rhs.f64", std::vector<double>(F.begin(), F.end()));
+    const GlobalVector& U = S->GetGV(u);
+    write_raw(c.out + "/solution.f64", std::vector<double>(U.begin(), U.end()));
+  }
   if (c.dump) {
     for (int l = 0; l < nl; ++l) {
       StdSolver* SL = MLS.GetSolver(l);
@@ -985,4 +1162,15 @@ main(int argc, char** argv)
   }
 
   return 0;
+}
+
+int
+main(int argc, char** argv)
+{
+  try {
+    return run(argc, argv);
+  } catch (const std::exception& e) {
+    fprintf(stderr, "ref_harness: %s\n", e.what());
+    return 4;
+  }
 }

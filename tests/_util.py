@@ -366,3 +366,13 @@ def golden_lps_cases():
                         [float(t) for t in str(z["key_conv"]).split(",")],
                         (float(z["key_lps"]), 6.0)))
     return out
+
+
+def stokes_rhs(dim, coarse, refine, seed=1002):
+    """f ~ U[-1, 1] per node and component (p, v_1..v_dim) on the lexicographic
+    grid the harness reads, the pressure part made algebraically mean-free so
+    that the system with its constant-pressure null space is consistent."""
+    n1 = (coarse << refine) + 1
+    r = np.random.default_rng(seed).uniform(-1.0, 1.0, size=(n1 ** dim, dim + 1))
+    r[:, 0] -= r[:, 0].mean()
+    return r.ravel()

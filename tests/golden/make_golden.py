@@ -9,7 +9,9 @@ nonsymmetric operator) and the reference's dual solve
 values, the dual right-hand side dJ/du = 2 M u of J(u) = integral of u^2 (M the
 Q1 mass matrix, u the forward solution of a first run) and the dual solution.
 The "stokes_" cases are the Q1/Q1 Stokes system (ncomp = dim+1, block
-matrices) with the pressure filter and the Vanka or block-Jacobi smoother; the
+matrices) with the pressure filter and the Vanka or block-Jacobi smoother
+("_lps_lid": the reference's NavierStokesLps at u = 0, CGQ1Lps, with the
+lid-driven cavity data, right-hand side -Form(u_D)); the
 harness runs them on one OpenMP thread, so Vanka's patch contributions are
 summed in patch order. The "hn_" cases refine a ball once more (hanging
 nodes, Q1 or Q2 elements) and also record the reference's HNAverage,
@@ -54,6 +56,9 @@ CASES = {
     "stokes_2d_c2_r3_jacobi": (2, 2, 3, True, 1e-8,
                                {"problem": "stokes", "smoother": "jacobi", "omega": 0.5,
                                 "gmressize": 31}),
+    "stokes_2d_c2_r4_lps_lid": (2, 2, 4, False, 1e-8,
+                                {"problem": "stokeslps", "smoother": "vanka", "omega": 1.0,
+                                 "gmressize": 31, "stab": 0.1}),
     "stokes_3d_c1_r3_vanka": (3, 1, 3, True, 1e-8,
                               {"problem": "stokes", "smoother": "vanka", "omega": 1.0,
                                "gmressize": 31}),
@@ -129,8 +134,10 @@ def l2_dual_rhs(P, u_ref):
 def make(name, dim, coarse, refine, seeded, tol, extra):
     d = tempfile.mkdtemp(prefix="gb_golden_")
     kw = {}
-    stokes = extra.get("problem") == "stokes"
-    if stokes:
+    stokes = extra.get("problem") in ("stokes", "stokeslps")
+    if extra.get("problem") == "stokeslps":
+        kw = {}  # the harness forms the right-hand side from the lid data
+    elif stokes:
         kw = write_inputs(d, None, stokes_rhs(dim, coarse, refine))
     elif "ball" in extra:
         # nodes of the extra refinement sit on the twice finer lexicographic grid

@@ -2,7 +2,6 @@
 entry point include/gascoigne_b200.h declares (no compute calls here)."""
 import ctypes
 import os
-import subprocess
 
 import pytest
 
@@ -29,11 +28,20 @@ def test_binding_covers_header():
     assert names == bound, names ^ bound
 
 
-def test_library_is_sm100a_only(so_path):
-    r = subprocess.run(["cuobjdump", "--list-elf", so_path], capture_output=True, text=True)
-    if r.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in r.stdout
+def test_library_is_built_for_sm100a():
+    from gascoignelib_b200.build import NVCC_FLAGS
+    assert "arch=compute_100a,code=sm_100a" in NVCC_FLAGS
+    assert not any("compute_" in f and "100a" not in f for f in NVCC_FLAGS)
+
+
+@pytest.mark.gpu
+def test_kernels_run_as_sm100(so_path):
+    """The kernels the device loads carry compute capability 10.0 (sm_100a),
+    read at run time from a kernel's attributes."""
+    L = ctypes.CDLL(so_path)
+    bv, pv = ctypes.c_int(0), ctypes.c_int(0)
+    assert L.gb_kernel_arch(ctypes.byref(bv), ctypes.byref(pv)) == 0
+    assert bv.value == 100, bv.value
 
 
 def test_structs_match_header():

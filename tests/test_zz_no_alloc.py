@@ -1,9 +1,10 @@
 """The allocation-free dot product (gb_dot_noalloc) against gb_vec_dot.
 
-gb_dot_noalloc serves callers that cannot allocate device memory (code running
-during CUDA stream capture, applications whose device memory belongs to their
-own pool, host callbacks). It uses a fixed file-scope scratch array instead of
-allocating, so this test checks, through the C-ABI, that two calls in a row
+gb_dot_noalloc serves callers that cannot allocate device memory once they run
+(applications whose device memory belongs to their own pool allocator from
+start-up, loops that cannot take cudaMalloc's device-wide synchronisation). It
+uses a fixed file-scope scratch array instead of allocating, so this test
+checks, through the C-ABI, that two calls in a row
 agree with the context-based gb_vec_dot within the tolerance of the other dot
 tests (1e-13 relative to sum |a_i b_i|), and that sizes beyond the scratch
 capacity are rejected. This file is named to be collected last.
