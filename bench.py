@@ -108,7 +108,8 @@ def cpu_baseline(kappa_rhs, ndof, threads):
             t0 = time.time()
             out, s = run_reference(d, dim=DIM, coarse=COARSE, refine=REFINE, repeat=3,
                                    tol=1e-8, globaltol=1e-16, gmressize=21, iterpre=2,
-                                   iterpost=2, omega=0.8, **write_inputs(d, kappa, rhs))
+                                   iterpost=2, omega=0.8, savesol=1, functional=1,
+                                   **write_inputs(d, kappa, rhs))
             wall = time.time() - t0
         finally:
             if env_threads is None:
@@ -124,7 +125,9 @@ def cpu_baseline(kappa_rhs, ndof, threads):
                            f"residual {float(s['true_rel_residual'][0]):.2e}; "
                            f"harness wall {wall:.1f} s incl. mesh+assembly)"),
                 "solve_s": med, "iterations": int(s["iterations"][0]),
-                "assemble_s": float(s["assemble_s"][0]) if "assemble_s" in s else None}
+                "assemble_s": float(s["assemble_s"][0]) if "assemble_s" in s else None,
+                "solution_lex": _reference_solution_lex(out, DIM, COARSE << REFINE),
+                "J": float(s["functional_l2"][0])}
     from gascoignelib_b200.problem import structured_problem
     P = structured_problem(DIM, COARSE, REFINE, kappa, rhs)
     O = Oracle(P)
@@ -134,6 +137,21 @@ def cpu_baseline(kappa_rhs, ndof, threads):
     return {"value": ndof / dt, "unit": "DoF/s", "cores": 1, "kind": "port",
             "sample": f"oracle C restatement, one solve ({dt:.2f} s, {info['iterations']} it)",
             "solve_s": dt, "iterations": info["iterations"]}
+
+
+def _reference_solution_lex(out, dim, N, name="solution.f64", ncomp=1):
+    """A solution the reference harness wrote (its node numbering), in the
+    lexicographic order of the structured problems."""
+    import numpy as np
+
+    from gascoignelib_b200.problem import to_lex
+    coord = np.fromfile(os.path.join(out, "coord.f64")).reshape(-1, dim)
+    return to_lex(np.fromfile(os.path.join(out, name)), coord, N, ncomp)
+
+
+def _rel(a, b):
+    import numpy as np
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
 
 
 def run_reference_arm(args, world, rank):
@@ -239,7 +257,7 @@ def assembly_leg(c, P, kappa, steps, warmup, flush, dev):
             "newton_residual_ms": sorted(msr)[len(msr) // 2]}
 
 
-def adjoint_c5(local, steps, warmup, flush):
+def adjoint_c5(local, steps, warmup, flush, with_ref=False, threads=1):
     """Forward + adjoint + coefficient gradient at 96^3 cells (912,673 dofs):
     mixed forward solve, J = int u^2 and dJ/du = 2 M u on the device, mixed
     adjoint solve, per-cell dJ/dkappa. Device time with CUDA events on the
@@ -284,6 +302,7 @@ def adjoint_c5(local, steps, warmup, flush):
         ms.append(e0.elapsed_time(e1))
     J = c.functional(l, u, g)
     grad = c.coeff_gradient(l, u, lam)
+    u_dev, g_dev, lam_dev = c.download(l, u), c.download(l, g), c.download(l, lam)
     t = sum(ms) / len(ms)
     # one design step with a new kappa: device assembly of all levels, then
     # the same forward + adjoint + gradient
@@ -317,29 +336,130 @@ def adjoint_c5(local, steps, warmup, flush):
            "assembly": asm,
            "l2": "flushed (256 MB write) before every step"}
     c.close()
+    if with_ref:
+        out.update(_adjoint_reference(kappa, rhs, g_dev, u_dev, lam_dev, grad, J,
+                                      P.finest.ndof, t, threads))
     return out
 
 
-def stokes_c3(local, steps, warmup, flush):
-    """C3: 2D Q1/Q1 Stokes on 512^2 cells (789,507 dofs, ncomp 3), Vanka
-    V(2,2) smoother with the pressure filter, GMRES(30) to 1e-8: mixed
-    (FP32 Vanka cycle in FP64 flexible GMRES) and FP64 solves, device time
-    with the L2 flushed before every solve; and the finest-level Vanka local
-    solve timed alone (its LU factors dominate the traffic)."""
+def _adjoint_reference(kappa, rhs, g_dev, u_dev, lam_dev, grad, J, ndof, t_dev, threads):
+    """The reference's FP64 CPU forward solve and dual solve (AssembleDualMatrix
+    + the same Gmres, right-hand side the device's dJ/du = 2 M u) of the 96^3
+    problem: its time is the CPU baseline of the adjoint line, its solutions
+    the FP64 oracle for u, J, lambda and dJ/dkappa."""
+    import numpy as np
+
+    from gascoignelib_b200.problem import boundary_lex, q1_cell_gradient
+    from oracle.oracle import REF_HARNESS, run_reference, write_inputs
+    if not os.path.exists(REF_HARNESS):
+        return {}
+    d = tempfile.mkdtemp(prefix="gb_c5ref_")
+    kw = write_inputs(d, kappa, rhs)
+    gp = os.path.join(d, "dual_in.f64")
+    np.ascontiguousarray(g_dev).tofile(gp)
+    env = os.environ.get("OMP_NUM_THREADS")
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    try:
+        t0 = time.time()
+        out, s = run_reference(d, dim=3, coarse=3, refine=5, tol=1e-8, globaltol=1e-16,
+                               gmressize=21, iterpre=2, iterpost=2, omega=0.8, savesol=1,
+                               functional=1, dualrhs=gp, **kw)
+        wall = time.time() - t0
+    finally:
+        if env is None:
+            os.environ.pop("OMP_NUM_THREADS", None)
+        else:
+            os.environ["OMP_NUM_THREADS"] = env
+    ds = {}
+    with open(os.path.join(out, "dual_summary.txt")) as f:
+        for line in f:
+            k, *v = line.split()
+            ds[k] = v
+    N = 96
+    u_ref = _reference_solution_lex(out, 3, N)
+    lam_ref = _reference_solution_lex(out, 3, N, "dual_solution.f64")
+    g_ref = q1_cell_gradient(u_ref, lam_ref, 3, N, boundary_lex(3, N))
+    J_ref = float(s["functional_l2"][0])
+    t_cpu = float(s["solve_s"][0]) + float(ds["dual_solve_s"][0])
+    return {
+        "cpu_baseline": {"value": ndof / t_cpu, "unit": "DoF/s (forward+adjoint)",
+                         "cores": threads, "kind": "reference",
+                         "sample": (f"reference CPU forward solve ({float(s['solve_s'][0]):.2f} "
+                                    f"s, {s['iterations'][0]} it) + AssembleDualMatrix + dual "
+                                    f"solve ({float(ds['dual_solve_s'][0]):.2f} s, "
+                                    f"{ds['dual_iterations'][0]} it), one run; harness wall "
+                                    f"{wall:.0f} s incl. mesh + assembly")},
+        "speedup_vs_cpu": t_cpu / (t_dev * 1e-3),
+        "accuracy": {"reference": "the reference's FP64 CPU forward and dual solutions",
+                     "rel_err_u": _rel(u_dev, u_ref),
+                     "rel_err_J": abs(J - J_ref) / abs(J_ref),
+                     "rel_err_lambda": _rel(lam_dev, lam_ref),
+                     "rel_err_grad": _rel(grad, g_ref)}}
+
+
+def stokes_c3(local, steps, warmup, flush, threads=1):
+    """C3: 2D equal-order Stokes, ncomp 3 (p, u, v), on 512^2 cells (789,507
+    dofs): the reference's NavierStokesLps at u = 0 (CGQ1Lps: LPS pressure
+    stabilisation) with the lid-driven cavity data (u = (1, 0) on the top,
+    0 elsewhere; right-hand side -Form(u_D)), Vanka V(2,2) on 3x3-node
+    patches (27x27 local systems), pressure filter, GMRES(30) to 1e-8.
+    The reference builds the problem (its mesh, numbering and assembled block
+    matrices, written by the harness) and solves it on the host cores (the CPU
+    baseline and the FP64 oracle of u and J); the device runs the mixed solve
+    (FP32 Vanka cycle in FP64 flexible GMRES), its FP64 twin and the
+    reference-semantics left GMRES of the same system, device time with the L2
+    flushed before every solve; the finest level's FP32 Vanka sweep is timed
+    alone for the roofline. The 12x12 variant repeats the mixed solve with
+    single-cell patches."""
+    import shutil
+
+    import numpy as np
     import torch
 
     from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
-    from gascoignelib_b200.problem import structured_stokes
+    from gascoignelib_b200.problem import (cell_patches, lex_index, load_reference_dump,
+                                           q1_l2_squared, to_lex)
+    from oracle.oracle import REF_HARNESS, run_reference
 
-    P = structured_stokes(2, 2, 8)
+    if not os.path.exists(REF_HARNESS):
+        return {"unavailable": "the reference harness (oracle/_ref) is not built"}
+    d = tempfile.mkdtemp(prefix="gb_c3_")
+    env = os.environ.get("OMP_NUM_THREADS")
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    try:
+        t0 = time.time()
+        out, s = run_reference(d, dim=2, coarse=2, refine=8, problem="stokeslps",
+                               smoother="vanka", omega=1.0, gmressize=31, stab=0.1,
+                               tol=1e-8, globaltol=1e-16, maxiter=300, dump=1,
+                               functional=1)
+        wall = time.time() - t0
+    finally:
+        if env is None:
+            os.environ.pop("OMP_NUM_THREADS", None)
+        else:
+            os.environ["OMP_NUM_THREADS"] = env
+    P = load_reference_dump(out)
+    P.info["smoother"] = "vanka"
+    u_ref = np.fromfile(os.path.join(out, "solution.f64"))
+    J_ref = float(s["functional_l2"][0])
+    t_cpu = float(s["solve_s"][0])
+    shutil.rmtree(d, ignore_errors=True)
+    N = 512
+    coord = P.finest.coord
+
+    def J_of(u):
+        return q1_l2_squared(to_lex(u, coord, N, 3), 2, N, ncomp=3, comps=(1, 2))
+
+    keys = dict(iterpre=2, iterpost=2, iterexact=10, omega=1.0, mgomega=1.0, mgtype="V",
+                gmressize=31, tol=1e-8, globaltol=1e-300, maxiter=300, smoother="vanka")
     c = Context(local)
     c.load_problem(P)
-    c.set_params(iterpre=2, iterpost=2, iterexact=10, omega=1.0, mgomega=1.0,
-                 mgtype="V", gmressize=31, tol=1e-8, globaltol=1e-300, maxiter=300)
+    c.set_params(**keys)
     l = P.nlevels - 1
     x, b = c.vec(), c.vec()
     c.upload(l, b, P.rhs)
     out = {}
+    sols = {}
     for name, prec in (("mixed", GB_FP32), ("fp64", GB_FP64)):
         for _ in range(warmup):
             c.fgmres(x, b, prec)
@@ -349,20 +469,52 @@ def stokes_c3(local, steps, warmup, flush):
             torch.cuda.synchronize()
             info = c.fgmres(x, b, prec)
             ms.append(info["device_ms"])
+        sols[name] = c.download(l, x)
         t = sum(ms) / len(ms)
         out[name] = {"value": P.finest.ndof / (t * 1e-3), "unit": "DoF/s",
                      "ms_per_step": t, "iterations": info["iterations"],
                      "restarts": info["restarts"],
                      "true_rel_residual": info["true_rel_residual"]}
+    info = c.gmres(x, b)
+    sols["fp64_left"] = c.download(l, x)
+    out["fp64_left"] = {"ms_per_step": info["device_ms"], "iterations": info["iterations"],
+                        "reference_iterations": int(s["iterations"][0])}
+    peak, peak_kind = _peaks()
+    sw_ms, sw_b = c.bench_sweep(l, GB_FP32, reps=10, flush_l2=2)
+    ach = sw_b / (sw_ms * 1e-3) / 1e9
+    out["roofline"] = {"bound": "hbm", "kernel": "k_vanka_inv_ct<27,float> patch solves + "
+                       "k_vanka_gather<3,float>, finest level (one FP32 Vanka sweep)",
+                       "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                       "ms_per_launch": sw_ms, "algorithmic_bytes": sw_b,
+                       "peak_kind": peak_kind + " (burst copy)"}
     c.close()
+    acc = {"reference": "the reference's FP64 CPU solution (same assembled system)",
+           "functional": "J(u) = int |v|^2 over the velocity update (reference: its own "
+                         "ComputeDomainFunctional; device: exact Q1 mass)",
+           "J_reference": J_ref}
+    for name, u in sols.items():
+        acc[f"rel_err_u_{name}"] = _rel(u, u_ref)
+        acc[f"rel_err_J_{name}"] = abs(J_of(u) - J_ref) / abs(J_ref)
+    out["accuracy"] = acc
+    out["cpu_baseline"] = {"value": P.finest.ndof / t_cpu, "unit": "DoF/s", "cores": threads,
+                           "kind": "reference",
+                           "sample": (f"reference CPU StdMultiLevelSolver GMRES + Vanka "
+                                      f"V-cycle on the same system, one solve "
+                                      f"({t_cpu:.2f} s, {s['iterations'][0]} iterations; "
+                                      f"harness wall {wall:.0f} s incl. mesh, assembly, "
+                                      f"dump)")}
+    out["speedup_vs_cpu_mixed"] = t_cpu / (out["mixed"]["ms_per_step"] * 1e-3)
     # the 12 x 12 variant: Vanka on single cells (4 nodes x 3 components)
-    Pc = structured_stokes(2, 2, 8, patches="cell")
+    for lv in P.levels:
+        Nl = round(lv.n ** 0.5) - 1
+        inv = np.empty(lv.n, dtype=np.int64)
+        inv[lex_index(lv.coord, Nl)] = np.arange(lv.n)
+        lv.patches = inv[cell_patches(2, Nl)]
     c = Context(local)
-    c.load_problem(Pc)
-    c.set_params(iterpre=2, iterpost=2, iterexact=10, omega=1.0, mgomega=1.0,
-                 mgtype="V", gmressize=31, tol=1e-8, globaltol=1e-300, maxiter=300)
+    c.load_problem(P)
+    c.set_params(**keys)
     x, b = c.vec(), c.vec()
-    c.upload(l, b, Pc.rhs)
+    c.upload(l, b, P.rhs)
     for _ in range(warmup):
         c.fgmres(x, b, GB_FP32)
     ms = []
@@ -373,12 +525,14 @@ def stokes_c3(local, steps, warmup, flush):
         ms.append(info["device_ms"])
     t = sum(ms) / len(ms)
     out["mixed_cell_patches_12x12"] = {
-        "value": Pc.finest.ndof / (t * 1e-3), "unit": "DoF/s", "ms_per_step": t,
-        "iterations": info["iterations"], "true_rel_residual": info["true_rel_residual"]}
+        "value": P.finest.ndof / (t * 1e-3), "unit": "DoF/s", "ms_per_step": t,
+        "iterations": info["iterations"], "true_rel_residual": info["true_rel_residual"],
+        "rel_err_u": _rel(c.download(l, x), u_ref)}
     c.close()
-    out["workload"] = ("2D Stokes Q1/Q1 (Brezzi-Pitkaranta), 512^2 cells, 789,507 dofs, "
-                       "Vanka 3x3-node patches (27x27 local systems), pressure filter, "
-                       "V(2,2), GMRES(30), tol 1e-8; 12x12 variant: single-cell patches")
+    out["workload"] = ("2D Stokes Q1/Q1, NavierStokesLps at u=0 (CGQ1Lps, alpha0 0.1, visc 1), "
+                       "lid-driven cavity, 512^2 cells, 789,507 dofs, the reference's own mesh "
+                       "and matrices, Vanka 3x3-node patches (27x27), pressure filter, V(2,2), "
+                       "GMRES(30), tol 1e-8; 12x12 variant: single-cell patches")
     out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     return out
 
@@ -438,19 +592,125 @@ def ilu_c2(local, P, steps, warmup, flush, threads, with_ref):
     return out
 
 
-def q2_c4(local, steps, warmup, flush):
+def q2_c4_reference_mesh(steps, threads):
+    """C4 on the reference's own mesh, through the reference-side binding: the
+    binding harness (oracle/_ref/ref_harness_b200) builds the 80^3-cell CGQ2
+    mesh and refines, with MeshAgent::refine_cells, the leaf cells whose
+    centroid lies within 0.25 of the centre (1,017,329 dofs on the finest of 5
+    levels, hanging nodes on edges and faces), assembles -0.01 Laplace u +
+    (1, 0.5, 0.25) . grad u = f (f ~ U[-1, 1], seed 1002) with the reference's
+    CGDisc, and hands it to B200MultiLevelSolver. On the device: the
+    reference-semantics FP64 GMRES (one cycle of up to 127 steps: the FP64
+    oracle of this line, pinned to the reference's CPU solve by the tests),
+    then `steps` flexible solves with the same Krylov memory (128: restarted
+    flexible GMRES(30) stalls on this operator, over 600 steps) and an FP64
+    cycle, and `steps` in mixed precision (FP32 cycle), each timed by CUDA
+    events inside the
+    binding (the finest matrix, about 0.9 GB in FP64, is larger than L2); the
+    finest level's SpMV and FP32 Jacobi sweep timed alone. The reference's CPU
+    solver runs 3 GMRES steps on the same mesh and right-hand side (the
+    bounded CPU baseline sample)."""
+    import numpy as np
+
+    from oracle.oracle import REF_HARNESS_B200, run_reference, write_inputs
+    if not os.path.exists(REF_HARNESS_B200):
+        return {"unavailable": "the binding harness (oracle/_ref/ref_harness_b200) is not built"}
+    res = 2 * (5 << 4)
+    d = tempfile.mkdtemp(prefix="gb_c4_")
+    rhs = np.random.default_rng(1002).uniform(-1.0, 1.0, size=(res + 1) ** 3)
+    env = os.environ.get("OMP_NUM_THREADS")
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    try:
+        t0 = time.time()
+        out, s = run_reference(d, harness=REF_HARNESS_B200, backend="b200", dim=3, coarse=5,
+                               refine=4, disc="Q2", ball=0.25, diff=0.01, conv="1,0.5,0.25",
+                               rhsres=res, tol=1e-8, globaltol=1e-16, gmressize=128,
+                               maxiter=600, iterpre=2, iterpost=2, omega=0.3, functional=1,
+                               flexreps=steps, flexgmressize=0, benchspmv=1, cpusample=3,
+                               savesol=1, **write_inputs(d, None, rhs))
+        wall = time.time() - t0
+    finally:
+        if env is None:
+            os.environ.pop("OMP_NUM_THREADS", None)
+        else:
+            os.environ["OMP_NUM_THREADS"] = env
+    ndof = int(s["nnodes_L4"][0])
+    u64 = np.fromfile(os.path.join(out, "solution.f64"))
+    um = np.fromfile(os.path.join(out, "solution_mixed.f64"))
+    J64 = float(s["functional_l2"][0])
+    peak, peak_kind = _peaks()
+
+    def med(key):
+        v = sorted(float(t) for t in s[key])
+        return v[len(v) // 2]
+
+    res_ = {}
+    for tag, name in (("mixed", "mixed"), ("flex64", "fp64")):
+        t = med(f"{tag}_device_ms_all")
+        res_[name] = {"value": ndof / (t * 1e-3), "unit": "DoF/s", "ms_per_step": t,
+                      "iterations": int(s[f"{tag}_iterations"][0]),
+                      "restarts": int(s[f"{tag}_restarts"][0]),
+                      "kernel_launches": int(s[f"{tag}_launches"][0]),
+                      "true_rel_residual": float(s[f"{tag}_true_rel_residual"][0])}
+    sw_ms, sw_b = float(s["sweep32_ms"][0]), float(s["sweep32_bytes"][0])
+    sp_ms, sp_b = float(s["spmv64_ms"][0]), float(s["spmv64_bytes"][0])
+    it_ref = int(s["iterations"][0])
+    cpu_it = int(s["cpu_sample_iterations"][0])
+    cpu_s = float(s["cpu_sample_s"][0])
+    cpu_est = cpu_s / max(cpu_it, 1) * it_ref
+    res_.update({
+        "workload": ("3D CGQ2 convection-diffusion eps 1e-2, beta (1,0.5,0.25), 80^3 cells "
+                     "refined once by the reference (MeshAgent::refine_cells on leaf cells "
+                     "whose centroid is in |x-0.5|<0.25), %d dofs, 5 levels, the reference's "
+                     "mesh and CGDisc matrices through the binding, Jacobi V(2,2) omega 0.3, "
+                     "flexible GMRES with Krylov memory 128, tol 1e-8" % ndof),
+        "dofs": ndof,
+        "mixed_over_fp64": res_["mixed"]["value"] / res_["fp64"]["value"],
+        "fp64_reference_semantics": {"ms_per_step": med("device_ms_all"),
+                                     "iterations": it_ref, "status": s["status"][0],
+                                     "true_rel_residual": float(s["true_rel_residual"][0])},
+        "accuracy": {"reference": "the reference-semantics FP64 device solve of the same "
+                                  "system (within 1e-8 of the reference's CPU solve: "
+                                  "tests/test_gpu_binding.py)",
+                     "functional": "J(u) = int u^2 (the reference's ComputeDomainFunctional "
+                                   "on each solution)",
+                     "rel_err_u_mixed": _rel(um, u64),
+                     "rel_err_J_mixed":
+                         abs(float(s["mixed_functional_l2"][0]) - J64) / abs(J64),
+                     "rel_err_J_fp64_flexible":
+                         abs(float(s["flex64_functional_l2"][0]) - J64) / abs(J64)},
+        "roofline": {"bound": "hbm", "kernel": "k_spmv<kJacobi,float> FP32 Jacobi sweep, "
+                     "finest level (ball-refined, hanging nodes)",
+                     "achieved": sw_b / (sw_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": sw_b / (sw_ms * 1e-3) / 1e9 / peak, "ms_per_launch": sw_ms,
+                     "algorithmic_bytes": sw_b, "peak_kind": peak_kind + " (burst copy)",
+                     "fp64_spmv": {"ms_per_launch": sp_ms, "algorithmic_bytes": sp_b,
+                                   "frac": sp_b / (sp_ms * 1e-3) / 1e9 / peak}},
+        "cpu_baseline": {"value": ndof / cpu_est, "unit": "DoF/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": (f"reference CPU StdMultiLevelSolver on the same mesh and "
+                                    f"right-hand side: {cpu_it} GMRES steps in {cpu_s:.2f} s, "
+                                    f"scaled to the {it_ref} steps its one-cycle solve takes "
+                                    f"({cpu_est:.1f} s); binding harness wall {wall:.0f} s "
+                                    f"incl. mesh, two CPU assemblies and the device runs")},
+        "speedup_vs_cpu_mixed": cpu_est / (res_["mixed"]["ms_per_step"] * 1e-3),
+    })
+    return res_
+
+
+def q2_c4(local, steps, warmup, flush, with_ref=True, threads=1):
     """C4: 3D CGQ2 convection-diffusion -0.01 Laplace u + (1, 0.5, 0.25) .
-    grad u = f on 80^3 cells (40^3 Q2 patches, 531,441 dofs), refined once more
-    inside the ball |x - 0.5| < 0.25 (patches whose centre is inside: 779,481
-    dofs, 22,752 hanging nodes on edges and faces, 47.6 M matrix entries, rows
-    of up to 125), five levels, Jacobi V(2,2) with omega 0.3 (0.5 and above
-    stall on this convection-dominated Q2 operator), GMRES(30) to 1e-8: mixed
-    and FP64 solves, device time, L2 flushed before every solve. The same solve
-    without the ball (531,441 dofs, four levels) is reported beside it."""
+    grad u = f on 80^3 cells refined once more inside the ball |x - 0.5| <
+    0.25: on the reference's own mesh through the binding
+    (q2_c4_reference_mesh). Beside it, the same operator on the uniform 80^3
+    cells (531,441 dofs, four levels, this package's generator): Jacobi V(2,2)
+    with omega 0.3 (the reference's cycle stalls with 0.5 and above on this
+    convection-dominated Q2 operator), GMRES(30) to 1e-8, mixed and FP64
+    solves, device time, L2 flushed before every solve."""
     import torch
 
     from gascoignelib_b200.native import GB_FP32, GB_FP64, Context
-    from gascoignelib_b200.problem import q2_meshes, structured_q2, structured_q2_ball
+    from gascoignelib_b200.problem import q2_meshes, structured_q2
 
     def run(P):
         c = Context(local)
@@ -507,19 +767,11 @@ def q2_c4(local, steps, warmup, flush):
         c.close()
         return sorted(ms)[len(ms) // 2]
 
-    P = structured_q2_ball(5, 4, eps=1e-2, beta=(1.0, 0.5, 0.25), radius=0.25)
-    out = run(P)
-    out["workload"] = ("3D CGQ2 convection-diffusion eps 1e-2, beta (1,0.5,0.25), 80^3 cells "
-                       "refined once inside |x-0.5|<0.25, %d dofs, %d hanging, 5 levels, "
-                       "Jacobi V(2,2) omega 0.3, GMRES(30), tol 1e-8"
-                       % (P.finest.ndof, P.info["hanging"]))
-    # device assembly of the ball hierarchy (5 levels; 93,568 elements of 27
-    # nodes on the finest, 6,896 of them with hanging nodes condensed)
-    out["assembly_ms"] = assembly_ms(P)
-    del P
+    out = q2_c4_reference_mesh(steps, threads) if with_ref else {}
     U = structured_q2(3, 5, 4, eps=1e-2, beta=(1.0, 0.5, 0.25))
     out["uniform_no_ball"] = run(U)
-    out["uniform_no_ball"]["workload"] = "the same on the uniform 80^3 cells, 531,441 dofs"
+    out["uniform_no_ball"]["workload"] = ("the same operator on the uniform 80^3 cells "
+                                          "(531,441 dofs, this package's generator)")
     # device assembly of the uniform Q2 hierarchy (4 levels, 40^3 elements of
     # 27 nodes on the finest)
     out["uniform_no_ball"]["assembly_ms"] = assembly_ms(U)
@@ -627,6 +879,14 @@ def main():
         e2e_ms.append(info["device_ms"])
     e2e_val = ndof * args.steps * world / (sum(e2e_ms) / 1e3)
 
+    # the solutions of the three solvers, for the accuracy keys (untimed)
+    ctx.fgmres(xv, bv, GB_FP32)
+    u_mixed = ctx.download(fl, xv)
+    ctx.fgmres(xv, bv, GB_FP64)
+    u_fp64 = ctx.download(fl, xv)
+    ctx.gmres(xv, bv)
+    u_left = ctx.download(fl, xv)
+
     # roofline: finest-level SpMV timed alone (CUDA events on the solver's
     # stream), the L2 emptied before each launch by reading a 256 MB buffer
     # (a write flush would leave dirty lines whose write-back the SpMV pays;
@@ -637,6 +897,11 @@ def main():
     spmv_ms64w, _ = ctx.bench_spmv(fl, GB_FP64, reps=20, flush_l2=1)
     ach64 = spmv_b64 / (spmv_ms64 * 1e-3) / 1e9
     ach32 = spmv_b32 / (spmv_ms32 * 1e-3) / 1e9
+    # the mixed solve's dominant kernel: the finest level's FP32 Jacobi sweep
+    sw_ms32, sw_b32 = ctx.bench_sweep(fl, GB_FP32, reps=20, flush_l2=2)
+    sw_ms64, sw_b64 = ctx.bench_sweep(fl, GB_FP64, reps=20, flush_l2=2)
+    achsw32 = sw_b32 / (sw_ms32 * 1e-3) / 1e9
+    achsw64 = sw_b64 / (sw_ms64 * 1e-3) / 1e9
     prof = {}
     pj = os.path.join(ROOT, "profiles", "spmv_fp64_c2_finest.json")
     if os.path.exists(pj):
@@ -646,20 +911,41 @@ def main():
 
     adj = None
     if not args.no_adjoint:
-        adj = adjoint_c5(local, min(args.steps, 5), 2, flush)
+        adj = adjoint_c5(local, min(args.steps, 5), 2, flush,
+                         with_ref=rank == 0 and not args.no_cpu_baseline,
+                         threads=os.cpu_count() or 1)
     stk = None
     if not args.no_stokes:
-        stk = stokes_c3(local, min(args.steps, 5), 2, flush)
+        stk = stokes_c3(local, min(args.steps, 5), 2, flush, threads=os.cpu_count() or 1)
     q2 = None
     if not args.no_q2:
-        q2 = q2_c4(local, min(args.steps, 3), 1, flush)
+        q2 = q2_c4(local, min(args.steps, 3), 1, flush,
+                   with_ref=rank == 0 and not args.no_cpu_baseline,
+                   threads=os.cpu_count() or 1)
     ilu = ilu_c2(local, P, min(args.steps, 3), 1, flush, os.cpu_count() or 1,
                  rank == 0 and not args.no_cpu_baseline)
 
     if rank == 0:
         cb = None
+        acc = None
         if not args.no_cpu_baseline:
+            from gascoignelib_b200.problem import q1_l2_squared
             cb = cpu_baseline((kappa, rhs), ndof, os.cpu_count() or 1)
+            uref = cb.pop("solution_lex", None)
+            Jref = cb.pop("J", None)
+            if uref is not None:
+                N = COARSE << REFINE
+                acc = {"reference": "the reference's FP64 CPU solution of the same problem "
+                                    "(cpu_baseline run, its node numbering mapped by "
+                                    "coordinates)",
+                       "functional": "J(u) = int u^2 (reference: its own "
+                                     "ComputeDomainFunctional; device solutions: exact "
+                                     "Q1 mass)",
+                       "J_reference": Jref}
+                for name, u in (("mixed", u_mixed), ("fp64", u_fp64), ("fp64_left", u_left)):
+                    J = q1_l2_squared(u, DIM, N)
+                    acc[f"rel_err_u_{name}"] = _rel(u, uref)
+                    acc[f"rel_err_J_{name}"] = abs(J - Jref) / abs(Jref)
         i32 = info32[-1]
         line = {
             "metric": METRIC, "value": value, "unit": "DoF/s", "n_gpus": world,
@@ -694,7 +980,17 @@ def main():
                          "traffic_source": "profiles/spmv_fp64_c2_finest.md (ncu)",
                          "fp32": {"achieved": ach32, "frac": ach32 / peak,
                                   "ms_per_launch": spmv_ms32,
-                                  "algorithmic_bytes": spmv_b32}},
+                                  "algorithmic_bytes": spmv_b32},
+                         "mixed_dominant_kernel": {
+                             "kernel": "k_spmv<kJacobi,float> fused FP32 Jacobi sweep, "
+                                       "finest level (the mixed solve's largest share)",
+                             "achieved": achsw32, "peak": peak, "unit": "GB/s",
+                             "frac": achsw32 / peak, "ms_per_launch": sw_ms32,
+                             "algorithmic_bytes": sw_b32},
+                         "fp64_sweep": {"achieved": achsw64, "frac": achsw64 / peak,
+                                        "ms_per_launch": sw_ms64,
+                                        "algorithmic_bytes": sw_b64}},
+            "accuracy": acc,
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "cpu_baseline": cb,

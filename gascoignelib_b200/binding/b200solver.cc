@@ -743,7 +743,7 @@ B200MultiLevelSolver::push_params(const CGInfo& info)
   p.omega = SD.GetOmega();
   p.mgomega = DataP.MgOmega();
   p.mgtype = DataP.MgType().empty() ? 'V' : DataP.MgType()[0];
-  p.gmressize = DataP.GmresMemSize();
+  p.gmressize = (solver_ != kReference && flex_m_ > 0) ? flex_m_ : DataP.GmresMemSize();
   p.tol = info.user().tol();
   p.globaltol = info.user().globaltol();
   p.maxiter = info.user().maxiter();
@@ -779,10 +779,12 @@ B200MultiLevelSolver::NewtonLinearSolve(const Matrix& A, Vector& x, const Vector
   const int ib = S->dev_in(b);
   const int ix = S->dev_out(x);
   last_ = gb_solve_info{};
-  const int rc = mixed_ ? gb_fgmres(D_->ctx(), ix, ib, GB_FP32, &last_)
-                        : gb_gmres(D_->ctx(), ix, ib, &last_);
+  const int rc =
+    solver_ == kReference
+      ? gb_gmres(D_->ctx(), ix, ib, &last_)
+      : gb_fgmres(D_->ctx(), ix, ib, solver_ == kFlexible32 ? GB_FP32 : GB_FP64, &last_);
   if (rc != GB_OK && rc != GB_ENOTCONV)
-    D_->check(rc, mixed_ ? "gb_fgmres" : "gb_gmres");
+    D_->check(rc, solver_ == kReference ? "gb_gmres" : "gb_fgmres");
   // CGInfo as GMRES::solve leaves it (Common/cginfo.cc:201-255)
   static const char* kStatus[] = { "waiting", "running", "converged", "too many iterations",
                                    "exploded" };

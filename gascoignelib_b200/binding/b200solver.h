@@ -205,12 +205,19 @@ public:
   // device GMRES (default) or the reference's host-driven GMRES over device
   // operations
   void SetDeviceGmres(bool on) { device_gmres_ = on; }
-  // the device solve as the mixed-precision flexible GMRES (gb_fgmres: FP32
-  // multigrid cycle inside FP64 flexible GMRES, restarted on the true FP64
-  // residual until ||b - A x|| <= tol ||b||) instead of the reference's
-  // left-preconditioned GMRES; its stopping test is the true residual, so
-  // iteration counts differ from the reference's
-  void SetMixedPrecision(bool on) { mixed_ = on; }
+  // which device solver NewtonLinearSolve runs: kReference (gb_gmres, the
+  // reference's left-preconditioned GMRES step for step), kFlexible64 or
+  // kFlexible32 (gb_fgmres: FP64 flexible GMRES around an FP64 or FP32
+  // multigrid cycle, restarted on the true FP64 residual until
+  // ||b - A x|| <= tol ||b||; its stopping test is the true residual, so its
+  // iteration counts differ from the reference's)
+  enum DeviceSolver { kReference = 0, kFlexible64 = 1, kFlexible32 = 2 };
+  void SetDeviceSolver(DeviceSolver s) { solver_ = s; }
+  void SetMixedPrecision(bool on) { solver_ = on ? kFlexible32 : kReference; }
+  // Krylov memory of the flexible solves (0: the parameter file's gmressize)
+  void SetFlexibleMemory(int gmressize) { flex_m_ = gmressize; }
+  // the C-ABI context (for instrumentation such as gb_bench_spmv)
+  gb_ctx* DeviceContext() const { return D_->ctx(); }
   // the last device solve's record (iterations, residuals, device time)
   const gb_solve_info& LastSolveInfo() const { return last_; }
 
@@ -221,7 +228,8 @@ private:
 
   std::shared_ptr<B200Device> D_;
   bool device_gmres_ = true;
-  bool mixed_ = false;
+  DeviceSolver solver_ = kReference;
+  int flex_m_ = 0;
   gb_solve_info last_{};
 };
 

@@ -348,6 +348,108 @@ k_comp_sub(int n, int B, int c, T* __restrict__ x, const double* __restrict__ su
 constexpr int kVankaMaxM = 128;
 constexpr int kVankaWarps = 4;
 
+// Per assembly, the patches' local matrices and their inverses on the device
+// (VankaSmoother::copy_entries_sparseblockmatrix, LinAlg/vankasmoother.cc:
+// 65-113, then the LU solves of VankaSmoother::solve, :192-237, applied to the
+// unit vectors). One CTA per patch, the M x M matrix in shared memory:
+//  - gather: entry (B r + cr, B q + cc) from the level's FP64 SELL values at
+//    map[p][r][q] + 32 (cr B + cc) (a host-built offset per node pair of the
+//    patch, -1 where the matrix holds no block), zero elsewhere;
+//  - LU with partial pivoting in the order of the partial-pivot LU the
+//    reference calls (pivot = the first row of largest |a_ik|, rows swapped,
+//    column scaled by the pivot when it is nonzero, rank-1 update of the
+//    trailing block), each product and difference rounded separately;
+//  - column j of the inverse (thread j): forward substitution with the unit
+//    lower factor on P e_j, backward with the upper, the same operation order;
+//    stored transposed ([patch][j][i]), FP64 and FP32.
+// The result equals the host factorisation of the same arithmetic bit for bit.
+constexpr int kVankaFactorThreads = 128;
+
+__global__ void __launch_bounds__(kVankaFactorThreads)
+k_vanka_factor(int npatch, int npp, int B, int M, const int* __restrict__ map,
+               const double* __restrict__ val, double* __restrict__ inv64,
+               float* __restrict__ inv32)
+{
+  GB_PDL_ENTRY();
+  extern __shared__ double sm_vf[];
+  const int ld = M + 1;
+  double* A = sm_vf;                                   // [M][M + 1]
+  int* pv = reinterpret_cast<int*>(A + M * ld);        // [M]
+  __shared__ int s_piv;
+  const int p = blockIdx.x;
+  if (p >= npatch)
+    return; // whole CTA
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int e = t; e < M * M; e += nt) {
+    const int i = e / M, jc = e - i * M;
+    const int r = i / B, cr = i - r * B, q = jc / B, cc = jc - q * B;
+    const int base = __ldg(map + (int64_t(p) * npp + r) * npp + q);
+    A[i * ld + jc] = base < 0 ? 0.0 : __ldg(val + int64_t(base) + int64_t(kSlice) * (cr * B + cc));
+  }
+  for (int i = t; i < M; i += nt)
+    pv[i] = i;
+  __syncthreads();
+  for (int k = 0; k < M; ++k) {
+    if (t == 0) {
+      int piv = k;
+      double best = fabs(A[k * ld + k]);
+      for (int i = k + 1; i < M; ++i) {
+        const double v = fabs(A[i * ld + k]);
+        if (v > best) {
+          best = v;
+          piv = i;
+        }
+      }
+      s_piv = piv;
+      if (piv != k) {
+        const int tmp = pv[k];
+        pv[k] = pv[piv];
+        pv[piv] = tmp;
+      }
+    }
+    __syncthreads();
+    const int piv = s_piv;
+    if (piv != k)
+      for (int j = t; j < M; j += nt) {
+        const double tmp = A[k * ld + j];
+        A[k * ld + j] = A[piv * ld + j];
+        A[piv * ld + j] = tmp;
+      }
+    __syncthreads();
+    const double akk = A[k * ld + k];
+    if (akk != 0.0)
+      for (int i = k + 1 + t; i < M; i += nt)
+        A[i * ld + k] = __ddiv_rn(A[i * ld + k], akk);
+    __syncthreads();
+    const int rem = M - k - 1;
+    for (int e = t; e < rem * rem; e += nt) {
+      const int i = k + 1 + e / rem, j = k + 1 + e % rem;
+      A[i * ld + j] = __dsub_rn(A[i * ld + j], __dmul_rn(A[i * ld + k], A[k * ld + j]));
+    }
+    __syncthreads();
+  }
+  for (int j = t; j < M; j += nt) {
+    double* x = inv64 + (int64_t(p) * M + j) * M; // the column, built in place
+    for (int i = 0; i < M; ++i)
+      x[i] = pv[i] == j ? 1.0 : 0.0;
+    for (int i = 1; i < M; ++i) {
+      double sacc = x[i];
+      for (int q = 0; q < i; ++q)
+        sacc = __dsub_rn(sacc, __dmul_rn(A[i * ld + q], x[q]));
+      x[i] = sacc;
+    }
+    for (int i = M - 1; i >= 0; --i) {
+      double sacc = x[i];
+      for (int q = i + 1; q < M; ++q)
+        sacc = __dsub_rn(sacc, __dmul_rn(A[i * ld + q], x[q]));
+      x[i] = __ddiv_rn(sacc, A[i * ld + i]);
+    }
+    float* y = inv32 + (int64_t(p) * M + j) * M;
+    for (int i = 0; i < M; ++i)
+      y[i] = static_cast<float>(x[i]);
+  }
+}
+
 template<int R, class TL, class T>
 __global__ void __launch_bounds__(32 * kVankaWarps)
 k_vanka_inv(int npatch, int M, int B, const int* __restrict__ pn,
@@ -577,6 +679,92 @@ __device__ __forceinline__ float ilu_add(float a, float b) { return __fadd_rn(a,
 // order, block entries as FMatrixBlock::subtract (LinAlg/fmatrixblock.h:
 // 136-145). The rows of one level depend only on rows of earlier levels
 // (earlier launches), so the result equals the sequential sweep bit for bit.
+// SparseBlockIlu::compute_ilu (LinAlg/sparseblockilu.xx:246-275) on the
+// device, one dependency level per launch, one thread per row: a row waits
+// only for the rows of its lower part (earlier levels), exactly as in the
+// forward substitution. Each row runs the host factorisation's steps in its
+// order: for every lower entry k ascending, a(i,k) times the inverted
+// diagonal block of row k, then a(i,j) -= a(i,k) a(k,j) over row k's upper
+// entries (the target found by a search of row i), and finally the
+// Gauss-Jordan inverse of the diagonal block; products and sums rounded
+// separately, as on the host: the factors are the host's bit for bit.
+template<int B>
+__global__ void __launch_bounds__(128)
+k_ilu_factor(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
+             const int* __restrict__ col, const int* __restrict__ diag,
+             double* __restrict__ v)
+{
+  GB_PDL_ENTRY();
+  constexpr int B2 = B * B;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nr)
+    return;
+  const int i = rows[t];
+  const int pb = ptr[i], pe = ptr[i + 1], pd = diag[i];
+  double tmp[B2];
+  for (int pk = pb; pk < pd; ++pk) {
+    const int k = col[pk];
+    double* a = v + int64_t(pk) * B2;
+    const double* dk = v + int64_t(diag[k]) * B2;
+#pragma unroll
+    for (int q = 0; q < B2; ++q)
+      tmp[q] = a[q];
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+#pragma unroll
+      for (int cc = 0; cc < B; ++cc) {
+        double acc = 0.0;
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+          acc = rn_add(acc, rn_mul(tmp[r * B + u], dk[u * B + cc]));
+        a[r * B + cc] = acc;
+      }
+    const int ke = ptr[k + 1];
+    for (int pj = diag[k] + 1; pj < ke; ++pj) {
+      const int j = col[pj];
+      for (int ph = pb; ph < pe; ++ph) {
+        if (col[ph] != j)
+          continue;
+        double* h = v + int64_t(ph) * B2;
+        const double* cj = v + int64_t(pj) * B2;
+#pragma unroll
+        for (int r = 0; r < B; ++r)
+#pragma unroll
+          for (int cc = 0; cc < B; ++cc)
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+              h[r * B + cc] = rn_sub(h[r * B + cc], rn_mul(a[r * B + u], cj[u * B + cc]));
+        break;
+      }
+    }
+  }
+  gauss_jordan<B>(v + int64_t(pd) * B2);
+}
+
+// The ILU's values in its row-sorted layout from the level's SELL values:
+// entry e, component q at val[map[e] + 32 q].
+__global__ void
+k_ilu_gather(int64_t nnz, int B2, const int* __restrict__ map,
+             const double* __restrict__ val, double* __restrict__ v)
+{
+  GB_PDL_ENTRY();
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < nnz;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t base = map[e];
+    for (int q = 0; q < B2; ++q)
+      v[e * B2 + q] = __ldg(val + base + int64_t(kSlice) * q);
+  }
+}
+
+__global__ void
+k_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ b)
+{
+  GB_PDL_ENTRY();
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    b[i] = static_cast<float>(a[i]);
+}
+
 template<int B, class T>
 __global__ void
 k_ilu_lower(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,

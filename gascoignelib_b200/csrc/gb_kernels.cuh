@@ -926,9 +926,12 @@ k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
   GB_PDL_ENTRY();
   const double beta = G->beta_tmp;
   const double aim = fmax(G->info.tol * G->bnorm, G->info.globaltol);
-  const int conv = (beta <= aim) || beta == 0.0;
+  // a non-finite residual or right-hand side never counts as converged
+  // (inf <= inf would): the solve stops as exploded
+  const int finite = isfinite(beta) && isfinite(G->bnorm);
+  const int conv = finite && ((beta <= aim) || beta == 0.0);
   const int stop = conv || G->total >= G->info.maxiter ||
-                   G->restarts >= maxrestarts || !(beta == beta);
+                   G->restarts >= maxrestarts || !finite;
   G->converged = conv;
   G->j = 0;
   if (G->restarts == 0)
@@ -937,7 +940,7 @@ k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
   if (stop) {
     G->stop = 1;
     G->inv = 0.0;
-    G->info.status = conv ? 2 : 3;
+    G->info.status = conv ? 2 : (finite ? 3 : 4);
     if (use_cond) {
       cudaGraphSetConditional(outer, 0);
       cudaGraphSetConditional(inner, 0);
@@ -961,27 +964,75 @@ k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
     cudaGraphSetConditional(inner, 1);
 }
 
-// y = (TO) V[(*jp) * n + i]   (Arnoldi vector j into the cycle's right-hand side)
-// y = (TO) v_j with v_j = V[(*jp) * n + i]; for j > 0 the pending
-// normalisation v_j *= 1/h[j][j-1] (G->inv) is applied first and stored back
-// (v_0 was normalised at the restart).
+// y = (TO) v_j, v_j = V[j * n + i] with j = G->j. For j > 0, v_j still holds
+// w' of the previous Arnoldi step, after the first CGS pass only: the second
+// pass's update w'' = w' - sum_{k<j} d2[k] V_k and the normalisation
+// v_j = w'' / s (s = ||w''||, formed from ||w'|| and the coefficients by the
+// previous step's k_cgs<1>) are applied here and stored back (v_0 was
+// normalised at the restart).
+template<class TO, int NV>
+__device__ __forceinline__ void
+load_idx_pass(int64_t n, TO* __restrict__ y, double* __restrict__ V,
+              const volatile double* coef, double s)
+{
+  constexpr int kGroup = 8;
+  const int j = NV; // the vector being loaded has NV basis vectors before it
+  double* v = V + int64_t(j) * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double t = v[i];
+#pragma unroll
+    for (int g = 0; g < NV; g += kGroup) {
+      double vk[kGroup];
+#pragma unroll
+      for (int k = 0; k < kGroup; ++k)
+        if (g + k < NV)
+          vk[k] = __ldg(V + int64_t(g + k) * n + i);
+#pragma unroll
+      for (int k = 0; k < kGroup; ++k)
+        if (g + k < NV)
+          t = fma(-coef[g + k], vk[k], t);
+    }
+    t = s * t;
+    v[i] = t;
+    y[i] = static_cast<TO>(t);
+  }
+}
+
 template<class TO>
-__global__ void
+__global__ void __launch_bounds__(256)
 k_load_idx(int64_t n, TO* __restrict__ y, double* __restrict__ V,
            const GmresDev* __restrict__ G)
 {
   GB_PDL_ENTRY();
+  __shared__ double s_coef[kMaxV];
   const int j = G->j;
-  double* v = V + int64_t(j) * n;
+  if (threadIdx.x < j && threadIdx.x < kMaxV)
+    s_coef[threadIdx.x] = G->d2[threadIdx.x];
+  __syncthreads();
+  if (j == 0) {
+    const double* v = V;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+      y[i] = static_cast<TO>(v[i]);
+    return;
+  }
   const double s = G->inv;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double t = v[i];
-    if (j > 0) {
-      t = s * t;
-      v[i] = t;
-    }
-    y[i] = static_cast<TO>(t);
+  switch (j) {
+#define GB_LOAD_CASE(K)                                                         \
+  case K:                                                                      \
+    load_idx_pass<TO, K>(n, y, V, s_coef, s);                                  \
+    break;
+    GB_LOAD_CASE(1) GB_LOAD_CASE(2) GB_LOAD_CASE(3) GB_LOAD_CASE(4) GB_LOAD_CASE(5)
+    GB_LOAD_CASE(6) GB_LOAD_CASE(7) GB_LOAD_CASE(8) GB_LOAD_CASE(9) GB_LOAD_CASE(10)
+    GB_LOAD_CASE(11) GB_LOAD_CASE(12) GB_LOAD_CASE(13) GB_LOAD_CASE(14) GB_LOAD_CASE(15)
+    GB_LOAD_CASE(16) GB_LOAD_CASE(17) GB_LOAD_CASE(18) GB_LOAD_CASE(19) GB_LOAD_CASE(20)
+    GB_LOAD_CASE(21) GB_LOAD_CASE(22) GB_LOAD_CASE(23) GB_LOAD_CASE(24) GB_LOAD_CASE(25)
+    GB_LOAD_CASE(26) GB_LOAD_CASE(27) GB_LOAD_CASE(28) GB_LOAD_CASE(29) GB_LOAD_CASE(30)
+    GB_LOAD_CASE(31) GB_LOAD_CASE(32)
+#undef GB_LOAD_CASE
+    default:
+      break; // j <= kCgsMaxJ: the host checks gmressize <= kCgsMaxJ + 1
   }
 }
 
@@ -1002,69 +1053,134 @@ k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
 //  MODE 0: c1[i] = <w, V_i>;                         H[j][i]  = c1[i]
 //  MODE 1: w -= sum_i c1[i] V_i; c2[i] = <w, V_i>;   H[j][i] += c2[i]
 //  MODE 2: w -= sum_i c2[i] V_i; s = ||w||;          H[j][j+1] = s
-// A streaming pass over the j+1 basis vectors: each thread visits rows
-// grid-strided and keeps its j+1 partial dot products in registers (the
-// accumulator array is indexed by compile-time constants under a runtime
-// guard), so a row costs j+1 independent loads and FMAs and no shuffle. One
-// warp-shuffle block reduction per launch, then the last block sums the
-// per-block partials in block order: deterministic for a fixed grid.
+// A streaming pass over the j+1 basis vectors. The number of vectors NV = j+1
+// is a template parameter (one instantiation per value, selected by a switch
+// on the device-side j), so that every loop over the basis unrolls with
+// constant indices: the loads of a group of basis entries are issued back to
+// back and the NV partial dot products accumulate in registers; rows are
+// grid-strided. One warp-shuffle block reduction per launch, then the last
+// block sums the per-block partials in block order: deterministic for a fixed
+// grid.
 constexpr int kCgsThreads = 256;
+constexpr int kCgsMaxBlocks = 4 * 148;
 
 __device__ void fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m,
                         int use_cond);
 
-// MODE 2 also performs the Givens update and the loop test (fg_step) in its
-// last block, after the norm is known.
-template<int MODE>
-__global__ void __launch_bounds__(kCgsThreads)
-k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
-      unsigned* ticket, cudaGraphConditionalHandle inner, int m, int use_cond)
+template<int MODE, int NV>
+__device__ __forceinline__ void
+cgs_pass(int64_t n, const double* __restrict__ V, double* __restrict__ w,
+         const volatile double* coef, double (*s_warp)[kCgsMaxJ + 1])
 {
-  GB_PDL_ENTRY();
-  constexpr int kWarps = kCgsThreads / 32;
-  constexpr int kAcc = (MODE == 2) ? 1 : kCgsMaxJ;
-  __shared__ double s_coef[kCgsMaxJ];
-  __shared__ double s_warp[kWarps][kCgsMaxJ];
-  __shared__ bool am_last;
-  const int j = G->j;
-  const int nv = j + 1;
-  const int nred = (MODE == 2) ? 1 : nv;
+  // coef (shared memory) is read where it is used: volatile keeps the
+  // compiler from holding all NV coefficients in registers across the rows
+  // The basis entries of a row are loaded in groups of kGroup, each group's
+  // loads issued back to back; the update pass keeps only the running t, the
+  // dot pass reloads the group (cache hits) and accumulates into registers.
+  constexpr int kGroup = 8;
+  constexpr int NA = (MODE == 2) ? 1 : NV;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  double* w = V + int64_t(j + 1) * n;
-  if (MODE >= 1 && tid < kCgsMaxJ)
-    s_coef[tid] = (tid < nv) ? (MODE == 1 ? G->d[tid] : G->d2[tid]) : 0.0;
-  __syncthreads();
-  double acc[kAcc];
+  double acc[NA];
 #pragma unroll
-  for (int i = 0; i < kAcc; ++i)
+  for (int i = 0; i < NA; ++i)
     acc[i] = 0.0;
+  double accn = 0.0; // MODE 1: ||w'||^2
   const int64_t stride = int64_t(gridDim.x) * kCgsThreads;
   for (int64_t r = int64_t(blockIdx.x) * kCgsThreads + tid; r < n; r += stride) {
     double t = w[r];
     if (MODE >= 1) {
-#pragma unroll 4
-      for (int i = 0; i < nv; ++i)
-        t = fma(-s_coef[i], V[int64_t(i) * n + r], t);
+#pragma unroll
+      for (int g = 0; g < NV; g += kGroup) {
+        double v[kGroup];
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+          if (g + k < NV)
+            v[k] = __ldg(V + int64_t(g + k) * n + r);
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+          if (g + k < NV)
+            t = fma(-coef[g + k], v[k], t);
+      }
       w[r] = t;
+      if (MODE == 1)
+        accn = fma(t, t, accn);
     }
     if (MODE <= 1) {
 #pragma unroll
-      for (int i = 0; i < kAcc; ++i)
-        if (i < nv)
-          acc[i] = fma(t, V[int64_t(i) * n + r], acc[i]);
+      for (int g = 0; g < NV; g += kGroup) {
+        double v[kGroup];
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+          if (g + k < NV)
+            v[k] = __ldg(V + int64_t(g + k) * n + r);
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+          if (g + k < NV)
+            acc[g + k < NA ? g + k : 0] = fma(t, v[k], acc[g + k < NA ? g + k : 0]);
+      }
     } else {
       acc[0] = fma(t, t, acc[0]);
     }
   }
 #pragma unroll
-  for (int i = 0; i < kAcc; ++i) {
-    if (i < nred) {
-      double p = acc[i];
-      for (int o = 16; o > 0; o >>= 1)
-        p += __shfl_down_sync(0xffffffffu, p, o);
-      if (lane == 0)
-        s_warp[wid][i] = p;
-    }
+  for (int i = 0; i < NA; ++i) {
+    double p = acc[i];
+    for (int o = 16; o > 0; o >>= 1)
+      p += __shfl_down_sync(0xffffffffu, p, o);
+    if (lane == 0)
+      s_warp[wid][i] = p;
+  }
+  if (MODE == 1) {
+    for (int o = 16; o > 0; o >>= 1)
+      accn += __shfl_down_sync(0xffffffffu, accn, o);
+    if (lane == 0)
+      s_warp[wid][NV] = accn;
+  }
+}
+
+// MODE 1 also forms the norm of the new basis vector and performs the Givens
+// update and the loop test (fg_step) in its last block: with w' the vector
+// after the first pass and c2 the second pass's coefficients, the basis is
+// orthonormal, so ||w''||^2 = ||w'||^2 - ||c2||^2 (c2 is tiny against w' after
+// a first CGS pass, so the difference loses no digits; it is clamped at 0,
+// which only a breakdown reaches, and there the Givens step ends the loop).
+// The second pass's update w'' = w' - V c2 and the scaling by 1/||w''|| are
+// deferred to the next step's k_load_idx, which reads v_{j+1} anyway. MODE 2
+// (the update-and-norm pass of the plain CGS2 order) is not launched.
+template<int MODE>
+__global__ void __launch_bounds__(kCgsThreads, 2)
+k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
+      unsigned* ticket, cudaGraphConditionalHandle inner, int m, int use_cond)
+{
+  GB_PDL_ENTRY();
+  constexpr int kWarps = kCgsThreads / 32;
+  __shared__ double s_coef[kCgsMaxJ];
+  __shared__ double s_warp[kWarps][kCgsMaxJ + 1];
+  __shared__ double s_red[kCgsMaxJ + 1];
+  __shared__ bool am_last;
+  const int j = G->j;
+  const int nv = j + 1;
+  const int nred = (MODE == 2) ? 1 : (MODE == 1 ? nv + 1 : nv);
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double* w = V + int64_t(j + 1) * n;
+  if (MODE >= 1 && tid < kCgsMaxJ)
+    s_coef[tid] = (tid < nv) ? (MODE == 1 ? G->d[tid] : G->d2[tid]) : 0.0;
+  __syncthreads();
+  switch (nv) {
+#define GB_CGS_CASE(K)                                                          \
+  case K:                                                                      \
+    cgs_pass<MODE, K>(n, V, w, s_coef, s_warp);                                \
+    break;
+    GB_CGS_CASE(1) GB_CGS_CASE(2) GB_CGS_CASE(3) GB_CGS_CASE(4) GB_CGS_CASE(5)
+    GB_CGS_CASE(6) GB_CGS_CASE(7) GB_CGS_CASE(8) GB_CGS_CASE(9) GB_CGS_CASE(10)
+    GB_CGS_CASE(11) GB_CGS_CASE(12) GB_CGS_CASE(13) GB_CGS_CASE(14) GB_CGS_CASE(15)
+    GB_CGS_CASE(16) GB_CGS_CASE(17) GB_CGS_CASE(18) GB_CGS_CASE(19) GB_CGS_CASE(20)
+    GB_CGS_CASE(21) GB_CGS_CASE(22) GB_CGS_CASE(23) GB_CGS_CASE(24) GB_CGS_CASE(25)
+    GB_CGS_CASE(26) GB_CGS_CASE(27) GB_CGS_CASE(28) GB_CGS_CASE(29) GB_CGS_CASE(30)
+    GB_CGS_CASE(31) GB_CGS_CASE(32)
+#undef GB_CGS_CASE
+    default:
+      break; // nv <= kCgsMaxJ: the host checks gmressize <= kCgsMaxJ + 1
   }
   __syncthreads();
   if (tid < nred) {
@@ -1087,23 +1203,33 @@ k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
       v += __ldcg(partials + int64_t(i) * gridDim.x + q);
     for (int o = 16; o > 0; o >>= 1)
       v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) {
-      if (MODE == 0) {
-        G->d[i] = v;
-        G->H[j][i] = v;
-      } else if (MODE == 1) {
-        G->d2[i] = v;
-        G->H[j][i] += v;
-      } else {
-        const double sv = sqrt(v);
-        G->H[j][j + 1] = sv;
-        G->s = sv;
-      }
-    }
+    if (lane == 0)
+      s_red[i] = v;
   }
+  __syncthreads();
   if (tid == 0) {
+    if (MODE == 0) {
+      for (int i = 0; i < nv; ++i) {
+        G->d[i] = s_red[i];
+        G->H[j][i] = s_red[i];
+      }
+    } else if (MODE == 1) {
+      double c2 = 0.0;
+      for (int i = 0; i < nv; ++i) {
+        G->d2[i] = s_red[i];
+        G->H[j][i] += s_red[i];
+        c2 = fma(s_red[i], s_red[i], c2);
+      }
+      const double sv = sqrt(fmax(s_red[nv] - c2, 0.0));
+      G->H[j][j + 1] = sv;
+      G->s = sv;
+    } else {
+      const double sv = sqrt(s_red[0]);
+      G->H[j][j + 1] = sv;
+      G->s = sv;
+    }
     *ticket = 0u;
-    if (MODE == 2) {
+    if (MODE >= 1) {
       __threadfence_block();
       fg_step(G, inner, m, use_cond);
     }
@@ -1442,26 +1568,34 @@ k_coarse_cycle(const CoarseOp* __restrict__ ops, int nops,
 // vectors stay in global memory (they fit in L2), every op is spread over all
 // threads, and a grid barrier separates the ops. Vector reads go through L2
 // (ld.global.cg): other CTAs wrote them earlier in the same launch. The
-// barrier's wait is bounded: after kMidSpinLimit polls it sets *err and the
-// kernel runs to its end (results then invalid; the host reports the flag).
+// barrier's wait is bounded in time: after wait_ns nanoseconds (the global
+// timer) it sets *err and the kernel runs to its end (results then invalid;
+// the host reports GB_ETIMEOUT and clears the flag).
 constexpr int kMidThreads = 256;
-constexpr unsigned long long kMidSpinLimit = 1ull << 26;
+
+__device__ __forceinline__ unsigned long long
+global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ void
-mid_barrier(unsigned* bar, unsigned target, int* err)
+mid_barrier(unsigned* bar, unsigned target, int* err, unsigned long long wait_ns)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
     // release this block's writes with the arrival, acquire the others' with
     // the observation of the final count
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
-    unsigned long long spins = 0;
+    const unsigned long long t0 = global_ns();
     for (;;) {
       unsigned v;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
       if (v >= target)
         break;
-      if (++spins > kMidSpinLimit || *reinterpret_cast<volatile int*>(err)) {
+      if (*reinterpret_cast<volatile int*>(err) || global_ns() - t0 > wait_ns) {
         atomicExch(err, 1);
         break;
       }
@@ -1529,9 +1663,27 @@ mid_row_transfer(const CoarseOp& op, const T* __restrict__ src, int i)
   return acc;
 }
 
-template<class T>
-__global__ void __launch_bounds__(kMidThreads)
-k_mid_cycle(const CoarseOp* __restrict__ ops, int nops, unsigned* bar, int* err)
+// The cluster form: the whole program runs in one thread-block cluster (up to
+// 16 CTAs, one per SM), and the ops are separated by the cluster's hardware
+// barrier (release/acquire at cluster scope) instead of the software grid
+// barrier. A cluster is co-scheduled as a whole and every thread reaches every
+// barrier, so the barrier cannot wait for a CTA that is not running.
+constexpr int kMidClusterThreads = 512;
+
+__device__ __forceinline__ void
+cluster_barrier()
+{
+  asm volatile("barrier.cluster.arrive.release;\n\t"
+               "barrier.cluster.wait.acquire;" ::
+                 : "memory");
+}
+
+// phantoms: arrivals each grid barrier waits for beyond the grid's own CTAs
+// (0 in every solve; a test sets it to make the bounded wait run out).
+template<class T, int THREADS, bool CLUSTER>
+__global__ void __launch_bounds__(THREADS)
+k_mid_cycle(const CoarseOp* __restrict__ ops, int nops, unsigned* bar, int* err,
+            unsigned long long wait_ns, unsigned phantoms)
 {
   GB_PDL_ENTRY();
   const int nthr = gridDim.x * blockDim.x;
@@ -1597,8 +1749,12 @@ k_mid_cycle(const CoarseOp* __restrict__ ops, int nops, unsigned* bar, int* err)
         }
       }
     }
-    if (k + 1 < nops)
-      mid_barrier(bar, unsigned(k + 1) * gridDim.x, err);
+    if (k + 1 < nops) {
+      if (CLUSTER)
+        cluster_barrier();
+      else
+        mid_barrier(bar, unsigned(k + 1) * (gridDim.x + phantoms), err, wait_ns);
+    }
   }
 }
 

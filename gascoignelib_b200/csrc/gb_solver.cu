@@ -12,6 +12,7 @@
 // Device vectors stay resident for the whole solve; nothing is copied between
 // host and device inside a solve except 8-byte status words.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -31,6 +32,24 @@
 namespace gb {
 
 // ------------------------------------------------------------------ memory
+
+// Host-side fault injection for the tests of the out-of-memory path
+// (gb_debug_fail_alloc): when set to k > 0, the k-th device allocation from
+// then on fails as cudaMalloc does when the device is out of memory.
+static std::atomic<long long> g_fail_alloc_countdown{ 0 };
+
+static cudaError_t
+device_malloc(void** p, size_t bytes)
+{
+  long long k = g_fail_alloc_countdown.load();
+  while (k > 0 && !g_fail_alloc_countdown.compare_exchange_weak(k, k - 1)) {
+  }
+  if (k == 1) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
 
 template<class T>
 struct DeviceArray
@@ -73,7 +92,7 @@ struct DeviceArray
     release();
     if (count == 0)
       return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    cudaError_t e = device_malloc(reinterpret_cast<void**>(&p), count * sizeof(T));
     if (e == cudaSuccess)
       n = count;
     else
@@ -128,6 +147,9 @@ struct Sell
   // (the scalar SpMV reads these; the op programs read col)
   bool off16 = false;
   DeviceArray<int16_t> c16;
+  // host copies of the layout: slice starts and slot -> row (device-side
+  // gathers built on the host, e.g. the Vanka patch matrices, address these)
+  std::vector<int> h_sptr, h_perm;
 };
 
 // Host-to-device copy ordered on `st` (the context's stream) and complete on
@@ -297,6 +319,8 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
   }
   // host vectors must outlive the async copies
   GB_CUDA(cudaStreamSynchronize(st));
+  S.h_sptr = sptr;
+  S.h_perm = perm;
   build_patterns(S, n, rowptr, col, st);
   S.off16 = false;
   if (!S.pat && S.entries) {
@@ -373,7 +397,8 @@ struct Level
   std::vector<int64_t> h_patches;
   int npatch = 0, npp = 0, vk_M = 0;
   bool vk_ready = false;
-  DeviceArray<int> vk_pn, vk_nptr, vk_ent;
+  bool vk_struct = false; // patch lists, node map and gather offsets built
+  DeviceArray<int> vk_pn, vk_nptr, vk_ent, vk_map;
   DeviceArray<double> vk_inv64, vk_out64; // inverses [patch][j][i], solutions
   DeviceArray<float> vk_inv32, vk_out32;
   // hanging nodes (gb_level_set_hn): phases in the discretisation's order
@@ -421,7 +446,8 @@ struct Level
   // order with ascending columns, the diagonal blocks inverted, and the rows
   // grouped in dependency levels for the two substitutions
   bool ilu_ready = false;
-  DeviceArray<int> ilu_ptr, ilu_col, ilu_diag, ilu_lrows, ilu_urows;
+  DeviceArray<int> ilu_ptr, ilu_col, ilu_diag, ilu_lrows, ilu_urows, ilu_map;
+  bool ilu_struct = false; // the sorted layout, levels and gather map built
   DeviceArray<double> ilu_v64;
   DeviceArray<float> ilu_v32;
   std::vector<int> ilu_lptr, ilu_uptr; // level offsets into ilu_lrows / ilu_urows
@@ -511,6 +537,15 @@ struct gb_ctx
   gb::DeviceArray<double> krylov, zb64, pbuf, fine32_rhs_dummy;
   gb::DeviceArray<float> zb32, fine_rhs32;
   int* h_flags = nullptr; // pinned
+  // pinned staging of a solve's closing status read (one transfer, one sync)
+  struct SolveStatus
+  {
+    gb::CGInfoDev info;
+    double true_res, rhs_norm;
+    int total, restarts, converged, mid_err;
+  };
+  SolveStatus* h_status = nullptr;
+  cudaEvent_t evh0 = nullptr, evh1 = nullptr; // gb_solve_host's window
   int64_t launches = 0;
   gb::DeviceArray<unsigned char> flush;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -561,6 +596,25 @@ struct gb_ctx
   // (mixed solve 1.97 vs 1.69 ms): each op there is itself latency-bound
   // (1-2 rows per thread) and a grid barrier costs about as much as a launch.
   bool mid_on = false;
+  // GB_VANKA_HOST=1: Vanka patch inverses formed on the host (the default is
+  // the device kernel k_vanka_factor, which gives the same bits)
+  bool vanka_host = false;
+  bool ilu_host = false; // GB_ILU_HOST=1: block ILU factors formed on the host
+  // GB_CLUSTER=1: the levels of at most cluster_rows dofs below the finest
+  // (and above the single-CTA coarse levels) as one op program run by one
+  // thread-block cluster of 16 CTAs with the hardware cluster barrier between
+  // ops (GB_CLUSTER_ROWS: the bound). Off by default: on C2 it measured slower
+  // than the per-level kernels with programmatic dependent launch (mixed solve
+  // 1.88 ms with the 17^3 level and below, 2.85 ms with the 33^3 level and
+  // below, against 1.60 ms): 16 SMs run each op of a level of 5,000 to 36,000
+  // rows at L2 latency, row after row, slower than a whole-GPU launch does.
+  bool cluster_on = false;
+  int64_t cluster_rows = 8192;
+  int cluster_size[2] = { 0, 0 }; // CTAs of the cluster per cycle type (0: not queried)
+  // bound of every device-side wait (grid barriers), and the phantom
+  // arrivals a test adds so that a wait runs out (gb_set_wait_limit)
+  unsigned long long wait_ns = 1000000000ull;
+  unsigned barrier_phantoms = 0;
   int mid_level = -1;
   std::map<gb::CoarseKey, gb::CoarseProgram> mid_progs;
   gb::DeviceArray<unsigned> midbar;
@@ -985,7 +1039,100 @@ ensure_pf_scratch(Context& c, int64_t n)
 // transposed per patch, with the patch node lists and, per node, the (patch,
 // local node) pairs in ascending patch order for the averaging gather.
 static void
+ensure_vanka_host(Context& c, Level& L);
+
+// The patch structure of a level (once per matrix structure and patch list):
+// patch node lists, the node -> (patch, slot) map of the averaging gather, and
+// per node pair of a patch the offset of its block in the SELL values (-1
+// where the matrix has no block), with the factor and solution buffers.
+static void
+vanka_structure(Context& c, Level& L)
+{
+  const int B = L.B, npp = L.npp, M = npp * B, B2 = B * B;
+  const int64_t np = L.npatch;
+  std::vector<int> pn(size_t(np) * npp), map(size_t(np) * npp * npp, -1);
+  std::vector<int> slot_of(L.n);
+  const Sell& S = L.A;
+  for (int64_t t = 0; t < L.n; ++t)
+    slot_of[S.h_perm[t]] = static_cast<int>(t);
+  for (int64_t p = 0; p < np; ++p) {
+    const int64_t* nodes = L.h_patches.data() + p * npp;
+    for (int r = 0; r < npp; ++r) {
+      const int64_t row = nodes[r];
+      const int t = slot_of[row], sl = t / kSlice, lane = t % kSlice;
+      for (int64_t pos = L.h_rowptr[row]; pos < L.h_rowptr[row + 1]; ++pos) {
+        int q = -1;
+        for (int k = 0; k < npp; ++k)
+          if (nodes[k] == L.h_col[pos]) {
+            q = k;
+            break;
+          }
+        if (q < 0)
+          continue;
+        const int64_t j = pos - L.h_rowptr[row];
+        const int64_t base = (int64_t(S.h_sptr[sl]) + j * kSlice) * B2 + lane;
+        GB_REQUIRE(base < (int64_t(1) << 31), GB_EINVAL, "Vanka gather offset too large");
+        map[(size_t(p) * npp + r) * npp + q] = static_cast<int>(base);
+      }
+      pn[size_t(r) * np + p] = static_cast<int>(row);
+    }
+  }
+  // node -> (patch, local node), patches ascending
+  std::vector<int> nptr(L.n + 1, 0), ent(size_t(np) * npp);
+  for (size_t k = 0; k < L.h_patches.size(); ++k)
+    nptr[L.h_patches[k] + 1]++;
+  for (int64_t i = 0; i < L.n; ++i) {
+    GB_REQUIRE(nptr[i + 1] > 0, GB_EINVAL, "a node lies in no Vanka patch");
+    nptr[i + 1] += nptr[i];
+  }
+  std::vector<int> fill(nptr.begin(), nptr.end() - 1);
+  for (int64_t p = 0; p < np; ++p)
+    for (int r = 0; r < npp; ++r)
+      ent[fill[L.h_patches[p * npp + r]]++] = static_cast<int>(p * 32 + r);
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+  GB_CUDA(L.vk_inv64.alloc(size_t(np) * M * M));
+  GB_CUDA(L.vk_inv32.alloc(size_t(np) * M * M));
+  GB_CUDA(L.vk_pn.alloc(pn.size()));
+  GB_CUDA(L.vk_map.alloc(map.size()));
+  GB_CUDA(L.vk_nptr.alloc(nptr.size()));
+  GB_CUDA(L.vk_ent.alloc(ent.size()));
+  GB_CUDA(L.vk_out64.alloc(size_t(np) * M));
+  GB_CUDA(L.vk_out32.alloc(size_t(np) * M));
+  GB_CUDA(h2d(c.stream, L.vk_pn.p, pn.data(), pn.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.vk_map.p, map.data(), map.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.vk_nptr.p, nptr.data(), nptr.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.vk_ent.p, ent.data(), ent.size() * sizeof(int)));
+  L.vk_M = M;
+  L.vk_struct = true;
+}
+
+// The patches' inverses from the level's current values, on the device
+// (k_vanka_factor); GB_VANKA_HOST=1 forms them on the host instead (the same
+// arithmetic, for comparison).
+static void
 ensure_vanka(Context& c, Level& L)
+{
+  if (L.vk_ready)
+    return;
+  GB_REQUIRE(L.npatch > 0, GB_ESTATE, "Vanka needs the patches of every level "
+                                      "(gb_level_set_patches)");
+  const int M = L.npp * L.B;
+  GB_REQUIRE(M <= kVankaMaxM && L.npp <= 32, GB_EINVAL, "Vanka patch too large");
+  if (c.vanka_host)
+    return ensure_vanka_host(c, L);
+  if (!L.vk_struct)
+    vanka_structure(c, L);
+  const int smem = M * (M + 1) * int(sizeof(double)) + M * int(sizeof(int));
+  GB_CUDA(cudaFuncSetAttribute(k_vanka_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem));
+  const int threads = std::min(kVankaFactorThreads, std::max(32, (M + 31) / 32 * 32));
+  launch_smem(c, k_vanka_factor, L.npatch, threads, smem, L.npatch, L.npp, L.B, M,
+              (const int*)L.vk_map.p, (const double*)L.A.v64.p, L.vk_inv64.p, L.vk_inv32.p);
+  L.vk_ready = true;
+}
+
+static void
+ensure_vanka_host(Context& c, Level& L)
 {
   if (L.vk_ready)
     return;
@@ -1089,6 +1236,7 @@ ensure_vanka(Context& c, Level& L)
   GB_CUDA(h2d(c.stream, L.vk_ent.p, ent.data(), ent.size() * sizeof(int)));
   L.vk_M = M;
   L.vk_ready = true;
+  L.vk_struct = false; // the device path rebuilds its gather map
 }
 
 // The exact coarsest-level solve of StdSolver::smooth_exact on a direct level
@@ -1220,8 +1368,140 @@ ilu_factor(std::vector<int>& ptr, std::vector<int>& col, std::vector<int>& diag,
   }
 }
 
+// The ILU's row-sorted layout, dependency levels and gather map (once per
+// matrix structure): columns ascending per row (SparseBlockIlu's order), the
+// forward and backward levels of the substitutions (the forward ones are also
+// the factorisation's), and per entry the offset of its block in the SELL
+// values.
+static void
+ilu_structure(Context& c, Level& L)
+{
+  const int B = L.B, B2 = B * B;
+  const int64_t n = L.n, nnz = L.h_rowptr[n];
+  std::vector<int> ptr(n + 1), col(nnz), diag(n, -1), map(nnz);
+  std::vector<int> slot_of(n);
+  const Sell& S = L.A;
+  for (int64_t t = 0; t < n; ++t)
+    slot_of[S.h_perm[t]] = static_cast<int>(t);
+  std::vector<int64_t> idx;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t b = L.h_rowptr[i], e = L.h_rowptr[i + 1];
+    ptr[i] = static_cast<int>(b);
+    idx.resize(e - b);
+    for (int64_t k = b; k < e; ++k)
+      idx[k - b] = k;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int64_t x, int64_t y) { return L.h_col[x] < L.h_col[y]; });
+    const int t = slot_of[i], sl = t / kSlice, lane = t % kSlice;
+    for (int64_t q = 0; q < e - b; ++q) {
+      col[b + q] = static_cast<int>(L.h_col[idx[q]]);
+      if (col[b + q] == i)
+        diag[i] = static_cast<int>(b + q);
+      const int64_t j = idx[q] - b; // the entry's place in the row: its SELL column
+      const int64_t base = (int64_t(S.h_sptr[sl]) + j * kSlice) * B2 + lane;
+      GB_REQUIRE(base < (int64_t(1) << 31), GB_EINVAL, "ILU gather offset too large");
+      map[b + q] = static_cast<int>(base);
+    }
+    GB_REQUIRE(diag[i] >= 0, GB_EINVAL, "ILU: a row without its diagonal");
+  }
+  ptr[n] = static_cast<int>(nnz);
+  std::vector<int> lev(n, 0);
+  int nl = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    int m = 0;
+    for (int p = ptr[i]; p < diag[i]; ++p)
+      m = std::max(m, lev[col[p]] + 1);
+    lev[i] = m;
+    nl = std::max(nl, m + 1);
+  }
+  auto group = [&](const std::vector<int>& lv, int nlev, std::vector<int>& off,
+                   std::vector<int>& rows) {
+    off.assign(nlev + 1, 0);
+    for (int64_t i = 0; i < n; ++i)
+      off[lv[i] + 1]++;
+    for (int q = 0; q < nlev; ++q)
+      off[q + 1] += off[q];
+    rows.resize(n);
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+      rows[fill[lv[i]]++] = static_cast<int>(i);
+  };
+  std::vector<int> lrows, urows;
+  group(lev, nl, L.ilu_lptr, lrows);
+  int nu = 0;
+  for (int64_t i = n - 1; i >= 0; --i) {
+    int m = 0;
+    for (int p = diag[i] + 1; p < ptr[i + 1]; ++p)
+      m = std::max(m, lev[col[p]] + 1);
+    lev[i] = m;
+    nu = std::max(nu, m + 1);
+  }
+  group(lev, nu, L.ilu_uptr, urows);
+  GB_CUDA(L.ilu_ptr.alloc(ptr.size()));
+  GB_CUDA(L.ilu_col.alloc(std::max<size_t>(col.size(), 1)));
+  GB_CUDA(L.ilu_diag.alloc(n));
+  GB_CUDA(L.ilu_lrows.alloc(n));
+  GB_CUDA(L.ilu_urows.alloc(n));
+  GB_CUDA(L.ilu_map.alloc(std::max<size_t>(map.size(), 1)));
+  GB_CUDA(L.ilu_v64.alloc(std::max<size_t>(size_t(nnz) * B2, 1)));
+  GB_CUDA(L.ilu_v32.alloc(std::max<size_t>(size_t(nnz) * B2, 1)));
+  GB_CUDA(h2d(c.stream, L.ilu_ptr.p, ptr.data(), ptr.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_col.p, col.data(), col.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_diag.p, diag.data(), n * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_lrows.p, lrows.data(), n * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_urows.p, urows.data(), n * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_map.p, map.data(), map.size() * sizeof(int)));
+  L.ilu_struct = true;
+}
+
+static void ensure_ilu_host(Context& c, Level& L);
+
+// The block ILU factors from the level's current values, on the device: the
+// values gathered into the row-sorted layout, then one k_ilu_factor launch per
+// dependency level, then the FP32 copy. GB_ILU_HOST=1 factors on the host
+// instead (the same arithmetic, for comparison).
 static void
 ensure_ilu(Context& c, Level& L)
+{
+  if (L.ilu_ready)
+    return;
+  if (c.ilu_host)
+    return ensure_ilu_host(c, L);
+  if (!L.ilu_struct)
+    ilu_structure(c, L);
+  const int B = L.B, B2 = B * B;
+  const int64_t nnz = L.h_rowptr[L.n];
+  launch(c, k_ilu_gather, stream_blocks(nnz), 256, nnz, B2, (const int*)L.ilu_map.p,
+         (const double*)L.A.v64.p, L.ilu_v64.p);
+  for (size_t q = 0; q + 1 < L.ilu_lptr.size(); ++q) {
+    const int nr = L.ilu_lptr[q + 1] - L.ilu_lptr[q];
+    const int* rows = L.ilu_lrows.p + L.ilu_lptr[q];
+    const int nb = blocks_for(nr, 128);
+    switch (B) {
+      case 1:
+        launch(c, k_ilu_factor<1>, nb, 128, nr, rows, (const int*)L.ilu_ptr.p,
+               (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p, L.ilu_v64.p);
+        break;
+      case 2:
+        launch(c, k_ilu_factor<2>, nb, 128, nr, rows, (const int*)L.ilu_ptr.p,
+               (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p, L.ilu_v64.p);
+        break;
+      case 3:
+        launch(c, k_ilu_factor<3>, nb, 128, nr, rows, (const int*)L.ilu_ptr.p,
+               (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p, L.ilu_v64.p);
+        break;
+      default:
+        launch(c, k_ilu_factor<4>, nb, 128, nr, rows, (const int*)L.ilu_ptr.p,
+               (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p, L.ilu_v64.p);
+    }
+  }
+  launch(c, k_to_float, stream_blocks(nnz * B2), 256, nnz * B2, (const double*)L.ilu_v64.p,
+         L.ilu_v32.p);
+  L.ilu_ready = true;
+}
+
+static void
+ensure_ilu_host(Context& c, Level& L)
 {
   if (L.ilu_ready)
     return;
@@ -1307,6 +1587,7 @@ ensure_ilu(Context& c, Level& L)
   GB_CUDA(h2d(c.stream, L.ilu_v64.p, v.data(), v.size() * sizeof(double)));
   GB_CUDA(h2d(c.stream, L.ilu_v32.p, v32.data(), v32.size() * sizeof(float)));
   L.ilu_ready = true;
+  L.ilu_struct = false; // the device path rebuilds its gather map
 }
 
 // After a device assembly: the dense maps of the single-CTA coarse programs
@@ -1425,6 +1706,14 @@ ensure_work(Context& c)
   c.mid_level = -1;
   if (simple && c.mid_on && c.coarse_on && c.nlevels >= 2 && c.nlevels - 2 > c.coarse_root)
     c.mid_level = c.nlevels - 2;
+  else if (simple && c.cluster_on && c.coarse_on && c.nlevels >= 2) {
+    // the highest level below the finest that the cluster program takes
+    for (int l = c.nlevels - 2; l > c.coarse_root; --l)
+      if (c.L[l].ndof() <= c.cluster_rows) {
+        c.mid_level = l;
+        break;
+      }
+  }
   if (c.midbar.n < 1) {
     GB_CUDA(c.midbar.alloc(1));
     GB_CUDA(c.miderr.alloc(1));
@@ -2089,6 +2378,38 @@ emit_dense(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char
 
 // mgstep(l) from u = 0 for the level below the finest and everything under it,
 // as one op program run by a persistent cooperative grid (k_mid_cycle).
+// The CTAs of the cluster that runs the mid-level program: 16 (one GPC's
+// worth of SMs, a non-portable size) when the device can schedule it, else 8.
+template<class T>
+static int
+cluster_size_for(Context& c)
+{
+  int& cached = c.cluster_size[sizeof(T) == 8 ? 0 : 1];
+  if (cached > 0)
+    return cached;
+  auto* kern = k_mid_cycle<T, kMidClusterThreads, true>;
+  int size = 8;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+      cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16);
+    cfg.blockDim = dim3(kMidClusterThreads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 16;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) == cudaSuccess && nclusters > 0)
+      size = 16;
+  }
+  cudaGetLastError(); // a refused query leaves no error behind
+  cached = size;
+  return size;
+}
+
 template<class T>
 static bool
 run_mid(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0, char p,
@@ -2113,15 +2434,19 @@ run_mid(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p
     int maxn = 1;
     for (const auto& o : ops)
       maxn = std::max(maxn, o.kind == kOpDense ? o.n * 32 : o.n);
-    int& grid = c.mid_grid[sizeof(T) == 8 ? 0 : 1];
-    if (grid == 0) {
-      int occ = 0, nsm = 0;
-      GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mid_cycle<T>,
-                                                            kMidThreads, 0));
-      GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
-      grid = std::max(1, occ) * nsm;
+    if (c.mid_on) {
+      int& grid = c.mid_grid[sizeof(T) == 8 ? 0 : 1];
+      if (grid == 0) {
+        int occ = 0, nsm = 0;
+        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &occ, k_mid_cycle<T, kMidThreads, false>, kMidThreads, 0));
+        GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
+        grid = std::max(1, occ) * nsm;
+      }
+      prog.n_root = std::min(grid, blocks_for(maxn, kMidThreads)); // launch grid
+    } else {
+      prog.n_root = cluster_size_for<T>(c); // one cluster
     }
-    prog.n_root = std::min(grid, blocks_for(maxn, kMidThreads)); // launch grid
     prog.u_out = z ? nullptr : u2;
     prog.tmp_out = t2;
     prog.p0_out = p02;
@@ -2130,7 +2455,7 @@ run_mid(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p
     it = c.mid_progs.emplace(key, std::move(prog)).first;
   }
   const CoarseProgram& prog = it->second;
-  if (prog.nops > 0) {
+  if (prog.nops > 0 && c.mid_on) {
     GB_CUDA(cudaMemsetAsync(c.midbar.p, 0, sizeof(unsigned), c.stream));
     cudaEvent_t e0;
     kt_begin(c, &e0);
@@ -2143,11 +2468,34 @@ run_mid(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    GB_CUDA(cudaLaunchKernelEx(&cfg, k_mid_cycle<T>, (const CoarseOp*)prog.ops.p, prog.nops,
-                               c.midbar.p, c.miderr.p));
+    GB_CUDA(cudaLaunchKernelEx(&cfg, k_mid_cycle<T, kMidThreads, false>,
+                               (const CoarseOp*)prog.ops.p, prog.nops, c.midbar.p,
+                               c.miderr.p, c.wait_ns, c.barrier_phantoms));
     c.launches++;
     check_launch(c);
-    kt_end(c, e0, reinterpret_cast<const void*>(k_mid_cycle<T>));
+    kt_end(c, e0, reinterpret_cast<const void*>(k_mid_cycle<T, kMidThreads, false>));
+  } else if (prog.nops > 0) {
+    cudaEvent_t e0;
+    kt_begin(c, &e0);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(prog.n_root);
+    cfg.blockDim = dim3(kMidClusterThreads);
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = prog.n_root;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = c.pdl ? 2 : 1;
+    GB_CUDA(cudaLaunchKernelEx(&cfg, k_mid_cycle<T, kMidClusterThreads, true>,
+                               (const CoarseOp*)prog.ops.p, prog.nops, c.midbar.p,
+                               c.miderr.p, c.wait_ns, 0u));
+    c.launches++;
+    check_launch(c);
+    kt_end(c, e0, reinterpret_cast<const void*>(k_mid_cycle<T, kMidClusterThreads, true>));
   }
   u = static_cast<T*>(const_cast<void*>(prog.u_in));
   tmp = static_cast<T*>(const_cast<void*>(prog.tmp_out));
@@ -2571,24 +2919,15 @@ read_flags(Context& c)
 }
 
 static void
-fill_info(Context& c, gb_solve_info* info, double* x_for_residual, const double* b)
+fill_info_enqueue(Context& c, const double* x_for_residual, const double* b)
 {
-  CGInfoDev I;
-  GB_CUDA(cudaMemcpyAsync(&I, &c.G.p->info, sizeof(I), cudaMemcpyDeviceToHost,
+  auto* st = c.h_status;
+  GB_CUDA(cudaMemcpyAsync(&st->info, &c.G.p->info, sizeof(CGInfoDev), cudaMemcpyDeviceToHost,
                           c.stream));
-  int mid_err = 0;
+  st->mid_err = 0;
   if (c.miderr.p)
-    GB_CUDA(cudaMemcpyAsync(&mid_err, c.miderr.p, sizeof(int), cudaMemcpyDeviceToHost,
+    GB_CUDA(cudaMemcpyAsync(&st->mid_err, c.miderr.p, sizeof(int), cudaMemcpyDeviceToHost,
                             c.stream));
-  GB_CUDA(cudaStreamSynchronize(c.stream));
-  if (mid_err) {
-    GB_CUDA(cudaMemsetAsync(c.miderr.p, 0, sizeof(int), c.stream));
-    throw Error{ GB_ETIMEOUT, "a grid barrier of the multi-CTA cycle gave up waiting" };
-  }
-  info->iterations = I.iteration;
-  info->status = I.status;
-  info->firstresidual = I.firstresidual;
-  info->residual = I.residual;
   // true residual ||b - A x|| and ||b|| (FP64)
   const int fl = c.nlevels - 1;
   Level& L = c.L[fl];
@@ -2596,12 +2935,34 @@ fill_info(Context& c, gb_solve_info* info, double* x_for_residual, const double*
                                        nullptr, 0.0);
   dot_dev(c, L.ndof(), c.pbuf.p, c.pbuf.p, RedOut{ c.scal.p + 4, nullptr, nullptr, 1 });
   dot_dev(c, L.ndof(), b, b, RedOut{ c.scal.p + 5, nullptr, nullptr, 1 });
-  double two[2];
-  GB_CUDA(cudaMemcpyAsync(two, c.scal.p + 4, 2 * sizeof(double),
+  GB_CUDA(cudaMemcpyAsync(&st->true_res, c.scal.p + 4, 2 * sizeof(double),
                           cudaMemcpyDeviceToHost, c.stream));
+}
+
+// After the stream has been synchronised: the staged status into info.
+static void
+fill_info_finish(Context& c, gb_solve_info* info)
+{
+  auto* st = c.h_status;
+  if (st->mid_err) {
+    GB_CUDA(cudaMemsetAsync(c.miderr.p, 0, sizeof(int), c.stream));
+    throw Error{ GB_ETIMEOUT, "a grid barrier of the multi-CTA cycle gave up waiting" };
+  }
+  info->iterations = st->info.iteration;
+  info->status = st->info.status;
+  info->firstresidual = st->info.firstresidual;
+  info->residual = st->info.residual;
+  info->true_residual = st->true_res;
+  info->rhs_norm = st->rhs_norm;
+}
+
+// The closing status and true residual of a solve, read with one sync.
+static void
+fill_info(Context& c, gb_solve_info* info, double* x_for_residual, const double* b)
+{
+  fill_info_enqueue(c, x_for_residual, b);
   GB_CUDA(cudaStreamSynchronize(c.stream));
-  info->true_residual = two[0];
-  info->rhs_norm = two[1];
+  fill_info_finish(c, info);
 }
 
 // NewtonLinearSolve's closing SubtractMean(x) on the finest level
@@ -2708,7 +3069,7 @@ gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* 
          c.params.maxiter);
   dot_dev(c, n, b, b, RedOut{ &G->bnorm, nullptr, nullptr, 1 });
   GB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), c.stream));
-  int total = 0, restarts = 0, converged = 0;
+  int total = 0, restarts = 0, converged = 0, exploded = 0;
   double bnorm = -1.0;
   for (;;) {
     // r = b - A x (Dirichlet zero) into V_0, beta = ||r||
@@ -2723,6 +3084,10 @@ gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* 
     GB_CUDA(cudaStreamSynchronize(c.stream));
     const double beta = hv[0];
     bnorm = hv[1];
+    if (!std::isfinite(beta) || !std::isfinite(bnorm)) {
+      exploded = 1; // a non-finite residual never counts as converged
+      break;
+    }
     if (beta <= c.params.tol * bnorm || beta < c.params.globaltol || beta == 0.0) {
       converged = 1;
       break;
@@ -2774,7 +3139,7 @@ gmres_flexible(Context& c, double* x, const double* b, int prec, gb_solve_info* 
   if (info) {
     fill_info(c, info, x, b);
     info->iterations = total;
-    info->status = converged ? 2 : 3;
+    info->status = converged ? 2 : (exploded ? 4 : 3);
     info->restarts = restarts;
     info->kernel_launches = static_cast<int>(c.launches - l0);
     info->device_ms = ms;
@@ -2914,14 +3279,14 @@ fg_inner(Context& c, const FBufs<T>& F, cudaGraphConditionalHandle hInner, int u
   precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true);
   spmv<kAx, double, T, double>(c, L, opA(c, L), (const T*)F.zfix, V, nullptr, nullptr, 1.0,
                                (const int*)&G->j, n, F.Z);
-  // one block of kCgsThreads per 2 kCgsThreads rows, at most two per SM
+  // one block of kCgsThreads per 2 kCgsThreads rows, at most four per SM
   const int rg = static_cast<int>(std::max<int64_t>(
-    1, std::min<int64_t>((n + 2 * kCgsThreads - 1) / (2 * kCgsThreads), kMaxRedBlocks)));
+    1, std::min<int64_t>((n + 2 * kCgsThreads - 1) / (2 * kCgsThreads), kCgsMaxBlocks)));
   const int m = c.params.gmressize - 1;
   launch(c, k_cgs<0>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m, 0);
-  launch(c, k_cgs<1>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m, 0);
-  // norm, Givens update, loop test; v_{j+1} is normalised by the next k_load_idx
-  launch(c, k_cgs<2>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m,
+  // second pass, norm, Givens update, loop test; v_{j+1} gets the second
+  // pass's update and its normalisation from the next k_load_idx
+  launch(c, k_cgs<1>, rg, kCgsThreads, n, V, G, c.partials.p, c.ticket.p, hInner, m,
          use_cond);
 }
 
@@ -3030,7 +3395,8 @@ fgmres_eager(Context& c, int prec)
 // Runs the graph on b (device), result into x (device); info as gb_fgmres.
 static int
 fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* info,
-             bool copy_in = true, bool copy_out = true)
+             bool copy_in = true, bool copy_out = true, double* host_x = nullptr,
+             cudaEvent_t after_copy = nullptr)
 {
   auto& F = c.fg[c.transposed][prec];
   if (c.use_graph && (!F.exec || F.version != c.version)) {
@@ -3061,31 +3427,40 @@ fgmres_graph(Context& c, double* x, const double* b, int prec, gb_solve_info* in
   const int64_t l_filter = c.launches;
   final_filter(c, c.xg.p);
   const int64_t filter_k = c.launches - l_filter;
+  const int64_t l_solved = c.launches; // the status read below launches more
   GB_CUDA(cudaEventRecord(c.ev1, c.stream));
   if (copy_out && x != c.xg.p)
     GB_CUDA(cudaMemcpyAsync(x, c.xg.p, n * sizeof(double), cudaMemcpyDeviceToDevice,
                             c.stream));
-  int cnt[3];
-  GB_CUDA(cudaMemcpyAsync(cnt, &c.G.p->total, 3 * sizeof(int), cudaMemcpyDeviceToHost,
+  // a host-buffer caller's solution goes out before the status read, inside
+  // its timing window
+  if (host_x)
+    GB_CUDA(cudaMemcpyAsync(host_x, c.xg.p, n * sizeof(double), cudaMemcpyDeviceToHost,
+                            c.stream));
+  if (after_copy)
+    GB_CUDA(cudaEventRecord(after_copy, c.stream));
+  auto* st = c.h_status;
+  GB_CUDA(cudaMemcpyAsync(&st->total, &c.G.p->total, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                           c.stream));
-  int conv = 0;
-  GB_CUDA(cudaMemcpyAsync(&conv, &c.G.p->converged, sizeof(int), cudaMemcpyDeviceToHost,
-                          c.stream));
+  GB_CUDA(cudaMemcpyAsync(&st->converged, &c.G.p->converged, sizeof(int),
+                          cudaMemcpyDeviceToHost, c.stream));
+  if (info)
+    fill_info_enqueue(c, c.xg.p, c.bg.p);
   GB_CUDA(cudaStreamSynchronize(c.stream));
   float ms = 0;
   GB_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
-  const int total = cnt[0], restarts = cnt[1];
-  int64_t kernels = c.launches - l_before;
+  const int total = st->total, restarts = st->restarts, conv = st->converged;
+  int64_t kernels = l_solved - l_before;
   if (c.use_graph) {
     kernels = F.setup_k + int64_t(restarts + 1) * F.outer_k + int64_t(total) * F.inner_k;
     c.launches += kernels;
     kernels += filter_k;
   }
   if (info) {
-    fill_info(c, info, c.xg.p, c.bg.p);
+    fill_info_finish(c, info);
     info->iterations = total;
     info->restarts = restarts;
-    info->status = conv ? 2 : 3;
+    info->status = conv ? 2 : (info->status == 4 ? 4 : 3); // 4: non-finite residual
     info->kernel_launches = static_cast<int>(kernels);
     info->device_ms = ms;
   }
@@ -3374,6 +3749,14 @@ gb_ctx_create(gb_ctx** out, int device)
       ctx->coarse_dense = atoi(e) != 0;
     if (const char* e = getenv("GB_MID"))
       ctx->mid_on = atoi(e) != 0;
+    if (const char* e = getenv("GB_ILU_HOST"))
+      ctx->ilu_host = atoi(e) != 0;
+    if (const char* e = getenv("GB_VANKA_HOST"))
+      ctx->vanka_host = atoi(e) != 0;
+    if (const char* e = getenv("GB_CLUSTER"))
+      ctx->cluster_on = atoi(e) != 0;
+    if (const char* e = getenv("GB_CLUSTER_ROWS"))
+      ctx->cluster_rows = atoll(e);
     if (const char* e = getenv("GB_JACOBI2"))
       ctx->jacobi2 = atoi(e) != 0;
     if (const char* e = getenv("GB_PDL"))
@@ -3382,11 +3765,15 @@ gb_ctx_create(gb_ctx** out, int device)
     GB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     GB_CUDA(cudaEventCreate(&ctx->ev0));
     GB_CUDA(cudaEventCreate(&ctx->ev1));
-    GB_CUDA(ctx->partials.alloc(size_t(kCgsMaxJ + 1) * kMaxRedBlocks));
+    GB_CUDA(ctx->partials.alloc(size_t(kCgsMaxJ + 1) *
+                                std::max(kMaxRedBlocks, kCgsMaxBlocks)));
     GB_CUDA(ctx->ticket.alloc(1));
     GB_CUDA(cudaMemset(ctx->ticket.p, 0, sizeof(unsigned)));
     GB_CUDA(ctx->scal.alloc(16));
     GB_CUDA(cudaMallocHost(&ctx->h_flags, 16 * sizeof(int)));
+    GB_CUDA(cudaMallocHost(&ctx->h_status, sizeof(gb_ctx::SolveStatus)));
+    GB_CUDA(cudaEventCreate(&ctx->evh0));
+    GB_CUDA(cudaEventCreate(&ctx->evh1));
   } catch (const gb::Error& e) {
     fprintf(stderr, "gb_ctx_create: %s\n", e.msg.c_str());
     int code = e.code;
@@ -3407,6 +3794,12 @@ gb_ctx_destroy(gb_ctx* ctx)
     cudaStreamSynchronize(ctx->stream);
   if (ctx->h_flags)
     cudaFreeHost(ctx->h_flags);
+  if (ctx->h_status)
+    cudaFreeHost(ctx->h_status);
+  if (ctx->evh0)
+    cudaEventDestroy(ctx->evh0);
+  if (ctx->evh1)
+    cudaEventDestroy(ctx->evh1);
   if (ctx->ev0)
     cudaEventDestroy(ctx->ev0);
   if (ctx->ev1)
@@ -3507,7 +3900,9 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   build_sell(L.A, n, rowptr, col, val, ctx->stream, B);
   L.has_AT = false;
   L.vk_ready = false;
+  L.vk_struct = false;
   L.ilu_ready = false;
+  L.ilu_struct = false;
   L.h_val_stale = false;
   L.mesh_ncells = 0; // the mesh maps point into the old pattern
   L.mesh_n = -1;
@@ -3947,6 +4342,7 @@ gb_level_set_patches(gb_ctx* ctx, int lvl, int64_t npatch, int npp, const int64_
   L.npatch = static_cast<int>(npatch);
   L.npp = npp;
   L.vk_ready = false;
+  L.vk_struct = false;
   ctx->work_ready = false;
   GB_API_END
 }
@@ -4338,35 +4734,43 @@ gb_solve_host(gb_ctx* ctx, int method, const double* b, double* x, int64_t len,
   GB_REQUIRE(b && x && len == ctx->L[fl].ndof(), GB_EINVAL, "length differs from level size");
   GB_REQUIRE(method >= 0 && method <= 2, GB_EINVAL, "method must be 0, 1 or 2");
   ensure_work(*ctx);
-  // resident work vectors for the host-buffer call
-  static const int kB = -1, kX = -2;
-  auto& bv = ctx->vecs[kB];
-  auto& xv = ctx->vecs[kX];
-  (void)bv;
-  (void)xv;
-  double* bd = vec(*ctx, fl, kB);
-  double* xd = vec(*ctx, fl, kX);
-  cudaEvent_t e0, e1;
-  GB_CUDA(cudaEventCreate(&e0));
-  GB_CUDA(cudaEventCreate(&e1));
-  GB_CUDA(cudaEventRecord(e0, ctx->stream));
+  const int prec = method == 1 ? GB_FP64 : GB_FP32;
+  const bool graph = method != 0 && ctx->use_graph && ctx->params.gmressize <= kCgsMaxJ;
+  double* bd;
+  double* xd;
+  if (graph) {
+    // the graph's own right-hand side and solution buffers: b goes straight
+    // in, x straight out, with no device-side staging copies
+    if (prec == GB_FP32)
+      fg_buffers<float>(*ctx, prec);
+    else
+      fg_buffers<double>(*ctx, prec);
+    bd = ctx->bg.p;
+    xd = ctx->xg.p;
+  } else {
+    // resident work vectors of the host-buffer call (created on first use)
+    static const int kB = -1, kX = -2;
+    ctx->vecs[kB];
+    ctx->vecs[kX];
+    bd = vec(*ctx, fl, kB);
+    xd = vec(*ctx, fl, kX);
+  }
+  GB_CUDA(cudaEventRecord(ctx->evh0, ctx->stream));
   GB_CUDA(cudaMemcpyAsync(bd, b, len * sizeof(double), cudaMemcpyHostToDevice,
                           ctx->stream));
   int rc;
-  if (method == 0)
-    rc = gmres_left(*ctx, xd, bd, info);
-  else if (ctx->params.gmressize <= kCgsMaxJ)
-    rc = fgmres_graph(*ctx, xd, bd, method == 1 ? GB_FP64 : GB_FP32, info);
-  else
-    rc = gmres_flexible(*ctx, xd, bd, method == 1 ? GB_FP64 : GB_FP32, info);
-  GB_CUDA(cudaMemcpyAsync(x, xd, len * sizeof(double), cudaMemcpyDeviceToHost,
-                          ctx->stream));
-  GB_CUDA(cudaEventRecord(e1, ctx->stream));
-  GB_CUDA(cudaEventSynchronize(e1));
+  if (graph) {
+    rc = fgmres_graph(*ctx, xd, bd, prec, info, false, false, x, ctx->evh1);
+  } else {
+    rc = method == 0 ? gmres_left(*ctx, xd, bd, info)
+                     : gmres_flexible(*ctx, xd, bd, prec, info);
+    GB_CUDA(cudaMemcpyAsync(x, xd, len * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    GB_CUDA(cudaEventRecord(ctx->evh1, ctx->stream));
+  }
+  GB_CUDA(cudaEventSynchronize(ctx->evh1));
   float ms = 0;
-  GB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  GB_CUDA(cudaEventElapsedTime(&ms, ctx->evh0, ctx->evh1));
   if (info)
     info->device_ms = ms;
   return rc;
@@ -5092,6 +5496,114 @@ gb_bench_spmv(gb_ctx* ctx, int lvl, int precision, int reps, int flush_l2,
   if (bytes_per_launch) // SpMV algorithmic bytes: values + indices + rowptr + x + y
     *bytes_per_launch = nnz * sv + 4.0 * nnz + 4.0 * (n + 1) + 2.0 * n * sv;
   GB_API_END
+}
+
+int
+gb_bench_sweep(gb_ctx* ctx, int lvl, int precision, int reps, int flush_l2,
+               double* ms_per_launch, double* bytes_per_launch)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(reps >= 1, GB_EINVAL, "reps < 1");
+  Level& L = level_with_matrix(*ctx, lvl);
+  const bool vk = ctx->params.smoother == 1 && L.npatch > 0;
+  GB_REQUIRE(vk || L.B == 1, GB_EINVAL,
+             "a sweep of the fused Jacobi kernel (B = 1) or of the Vanka smoother");
+  ensure_work(*ctx);
+  if (vk)
+    ensure_vanka(*ctx, L);
+  const int64_t n = L.ndof();
+  const size_t flush_bytes = size_t(256) << 20; // > 126 MB L2
+  if (flush_l2 && ctx->flush.n < flush_bytes)
+    GB_CUDA(ctx->flush.alloc(flush_bytes));
+  // three vectors of the level (u, b, out) in the sweep's precision
+  DeviceArray<double> buf;
+  GB_CUDA(buf.alloc(size_t(3) * n));
+  GB_CUDA(cudaMemsetAsync(buf.p, 0, size_t(3) * n * sizeof(double), ctx->stream));
+  cudaEvent_t a, bq;
+  GB_CUDA(cudaEventCreate(&a));
+  GB_CUDA(cudaEventCreate(&bq));
+  double total = 0;
+  if (flush_l2 == 2)
+    GB_CUDA(cudaMemsetAsync(ctx->flush.p, 0, flush_bytes, ctx->stream));
+  for (int r = 0; r < reps; ++r) {
+    if (flush_l2 == 1)
+      GB_CUDA(cudaMemsetAsync(ctx->flush.p, r & 0xff, flush_bytes, ctx->stream));
+    else if (flush_l2 == 2)
+      k_read_flush<<<4 * 148, 512, 0, ctx->stream>>>(
+        reinterpret_cast<const uint4*>(ctx->flush.p), int64_t(flush_bytes / 16), nullptr);
+    GB_CUDA(cudaEventRecord(a, ctx->stream));
+    if (vk && precision == GB_FP32) {
+      float* f = reinterpret_cast<float*>(buf.p);
+      Emit<float>{ *ctx }.vanka(lvl, f + n, f, false);
+    } else if (vk) {
+      Emit<double>{ *ctx }.vanka(lvl, buf.p + n, buf.p, false);
+    } else if (precision == GB_FP32) {
+      float* f = reinterpret_cast<float*>(buf.p);
+      spmv<kJacobi, float, float, float>(*ctx, L, opA(*ctx, L), (const float*)f, f + 2 * n,
+                                         (const float*)(f + n), L.dinv32.p, ctx->params.omega);
+    } else {
+      double* f = buf.p;
+      spmv<kJacobi, double, double, double>(*ctx, L, opA(*ctx, L), (const double*)f,
+                                            f + 2 * n, (const double*)(f + n), L.dinv64.p,
+                                            ctx->params.omega);
+    }
+    GB_CUDA(cudaEventRecord(bq, ctx->stream));
+    GB_CUDA(cudaEventSynchronize(bq));
+    float ms = 0;
+    GB_CUDA(cudaEventElapsedTime(&ms, a, bq));
+    total += ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(bq);
+  const double sv = precision == GB_FP32 ? 4.0 : 8.0;
+  const double nnz = static_cast<double>(L.A.nnz), nd = static_cast<double>(n);
+  if (ms_per_launch)
+    *ms_per_launch = total / reps;
+  if (bytes_per_launch && vk) {
+    // patch solves: inverses, patch lists, gathered residual, patch solutions;
+    // averaging gather: patch solutions, node -> (patch, slot) map, u read and
+    // written
+    const double np = L.npatch, M = L.vk_M, npp = L.npp;
+    *bytes_per_launch = np * M * M * sv + np * npp * 4.0 + 2.0 * np * M * sv +
+                        np * M * sv + np * npp * 4.0 + 4.0 * (L.n + 1) + 2.0 * nd * sv;
+  } else if (bytes_per_launch) // SpMV bytes + b + D^-1 + the new iterate
+    *bytes_per_launch = nnz * sv + 4.0 * nnz + 4.0 * (nd + 1) + 4.0 * nd * sv;
+  GB_API_END
+}
+
+int
+gb_level_get_vanka_inverse(gb_ctx* ctx, int lvl, double* host, int64_t len)
+{
+  GB_API_BEGIN
+  Level& L = level_with_matrix(*ctx, lvl);
+  GB_REQUIRE(host, GB_EINVAL, "null output");
+  ensure_vanka(*ctx, L);
+  const int64_t m = int64_t(L.npatch) * L.vk_M * L.vk_M;
+  GB_REQUIRE(len == m, GB_EINVAL, "length differs from npatch * M * M");
+  GB_CUDA(cudaMemcpyAsync(host, L.vk_inv64.p, m * sizeof(double), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  GB_CUDA(cudaStreamSynchronize(ctx->stream));
+  GB_API_END
+}
+
+int
+gb_set_wait_limit(gb_ctx* ctx, uint64_t wait_ns, int phantoms)
+{
+  GB_API_BEGIN
+  GB_REQUIRE(wait_ns > 0 && phantoms >= 0, GB_EINVAL, "bad wait limit");
+  ctx->version++; // captured solver graphs hold the old values
+  ctx->wait_ns = wait_ns;
+  ctx->barrier_phantoms = static_cast<unsigned>(phantoms);
+  GB_API_END
+}
+
+int
+gb_debug_fail_alloc(int64_t nth)
+{
+  if (nth < 0)
+    return GB_EINVAL;
+  g_fail_alloc_countdown.store(nth);
+  return GB_OK;
 }
 
 int

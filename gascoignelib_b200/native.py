@@ -126,6 +126,10 @@ _SIGS = {
     "gb_set_timing": [C.c_void_p, C.c_int],
     "gb_get_kernel_count": [C.c_void_p, _P64],
     "gb_bench_spmv": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
+    "gb_bench_sweep": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _PD, _PD],
+    "gb_level_get_vanka_inverse": [C.c_void_p, C.c_int, _PD, C.c_int64],
+    "gb_set_wait_limit": [C.c_void_p, C.c_uint64, C.c_int],
+    "gb_debug_fail_alloc": [C.c_int64],
     "gb_kernel_arch": [C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "gb_dot_noalloc": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
     "gb_get_kernel_times": [C.c_void_p, C.c_char_p, C.c_int64],
@@ -538,6 +542,20 @@ class Context:
         ms, by = C.c_double(), C.c_double()
         self._chk(self._L.gb_bench_spmv(self.h, level, precision, reps, int(flush_l2),
                                         C.byref(ms), C.byref(by)))
+        return ms.value, by.value
+
+    def vanka_inverse(self, level, npatch, M):
+        """The level's patch inverses [npatch, M, M] (row j = column j of the
+        inverse), formed from its current values."""
+        out = np.empty(int(npatch) * M * M)
+        self._chk(self._L.gb_level_get_vanka_inverse(self.h, level, _pd(out), out.size))
+        return out.reshape(int(npatch), M, M)
+
+    def bench_sweep(self, level, precision=GB_FP32, reps=10, flush_l2=2):
+        """One fused damped-Jacobi sweep of a scalar level, timed alone."""
+        ms, by = C.c_double(), C.c_double()
+        self._chk(self._L.gb_bench_sweep(self.h, level, precision, reps, int(flush_l2),
+                                         C.byref(ms), C.byref(by)))
         return ms.value, by.value
 
 

@@ -847,3 +847,73 @@ def q2_meshes(prob: Problem):
             loc = (loc[:, None] * n1 + np.arange(3)[None, :]).ravel()
         out.append((base[:, None] + loc[None, :], cell_parents(dim, Np) if l else None))
     return out
+
+
+# ------------------------------------------------------- accuracy helpers
+#
+# The benchmark reports each result's error against the reference's FP64
+# solution of the same problem. The reference numbers its nodes
+# hierarchically; these helpers map a uniform mesh's nodes to the
+# lexicographic order by their coordinates and evaluate J(u) = int u^2 exactly
+# for Q1 functions (the reference's Gauss rules integrate it exactly too).
+
+def lex_index(coord: np.ndarray, N: int) -> np.ndarray:
+    """Lexicographic index (x fastest) of every node of a uniform mesh of N
+    cells per dimension on the unit square/cube, from its coordinates."""
+    c = np.rint(np.asarray(coord) * N).astype(np.int64)
+    idx = np.zeros(c.shape[0], dtype=np.int64)
+    for d in reversed(range(c.shape[1])):
+        idx = idx * (N + 1) + c[:, d]
+    return idx
+
+
+def to_lex(values: np.ndarray, coord: np.ndarray, N: int, ncomp: int = 1) -> np.ndarray:
+    """A nodal vector (ncomp values per node, node-major) in the numbering of
+    `coord`, reordered lexicographically."""
+    v = np.asarray(values).reshape(-1, ncomp)
+    out = np.empty_like(v)
+    out[lex_index(coord, N)] = v
+    return out.reshape(-1)
+
+
+def q1_l2_squared(u_lex: np.ndarray, dim: int, N: int, ncomp: int = 1,
+                  comps=(0,)) -> float:
+    """int sum_{c in comps} u_c^2 over the unit square/cube for Q1 nodal
+    values on the lexicographic grid: u^T M u with the consistent mass matrix,
+    applied as the tensor product of 1D mass matrices (h/6 [1 4 1])."""
+    h = 1.0 / N
+    u = np.asarray(u_lex, dtype=np.float64).reshape(-1, ncomp)
+    total = 0.0
+    for c in comps:
+        g = u[:, c].reshape((N + 1,) * dim)
+        m = g.copy()
+        for ax in range(dim):
+            s = np.moveaxis(m, ax, 0)
+            t = 4.0 * s
+            t[1:] += s[:-1]
+            t[:-1] += s[1:]
+            t[0] -= 2.0 * s[0]   # boundary rows: h/6 [2 1]
+            t[-1] -= 2.0 * s[-1]
+            m = np.moveaxis(t * (h / 6.0), 0, ax)
+        total += float(np.sum(g * m))
+    return total
+
+
+def q1_cell_gradient(u_lex: np.ndarray, lam_lex: np.ndarray, dim: int, N: int,
+                     dirichlet_lex: np.ndarray) -> np.ndarray:
+    """dJ/dkappa_c = -lambda_c^T K_c u_c per cell (K_c the unit-coefficient Q1
+    stiffness of the uniform cell), with u and lambda read as zero on the
+    Dirichlet nodes: the gradient the device's gb_coeff_gradient forms."""
+    u = np.asarray(u_lex, dtype=np.float64).copy()
+    lam = np.asarray(lam_lex, dtype=np.float64).copy()
+    u[dirichlet_lex] = 0.0
+    lam[dirichlet_lex] = 0.0
+    cn = cell_nodes(dim, N)
+    K = _q1_local_stiffness(dim, 1.0 / N)
+    return -np.einsum("ca,ab,cb->c", lam[cn], K, u[cn])
+
+
+def boundary_lex(dim: int, N: int) -> np.ndarray:
+    """Lexicographic indices of the boundary nodes of the unit square/cube."""
+    g = np.indices((N + 1,) * dim).reshape(dim, -1)
+    return np.nonzero(((g == 0) | (g == N)).any(0))[0]

@@ -2,6 +2,7 @@
 
     python -m gascoignelib_b200.workload --method mixed --solves 2 [--refine 6]
     python -m gascoignelib_b200.workload --spmv 3 [--precision fp64]
+    python -m gascoignelib_b200.workload --sweep 3 [--precision fp32]
 
 --method: mixed (FP32 cycle, flexible FP64 GMRES), fp64 (FP64 cycle, flexible),
 left (reference-semantics left-preconditioned FP64 GMRES). --spmv K runs only K
@@ -27,6 +28,10 @@ def main(argv=None):
     ap.add_argument("--smooth", type=int, default=0,
                     help="only K FP64 smoothing sweeps on the finest level (StdSolver::smooth "
                          "with the problem's smoother), after the set-up")
+    ap.add_argument("--sweep", type=int, default=0,
+                    help="only K finest-level sweeps of the smoother's dominant kernel "
+                         "(the fused Jacobi sweep, or Vanka's patch solves and gather), "
+                         "timed alone with the L2 flushed before each (gb_bench_sweep)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--problem", default="diffusion", choices=["diffusion", "stokes", "q2", "q2ball"],
                     help="stokes: 2D Q1/Q1 Stokes with Vanka on (2*2^(refine-1))^2 cells")
@@ -99,6 +104,11 @@ def main(argv=None):
             ctx.smooth(fl, a.smooth, x, y, h)
             ctx.synchronize()
             print(json.dumps({"sweeps": a.smooth, "kernels": ctx.kernel_count() - k0}))
+            return
+        if a.sweep:
+            prec = GB_FP32 if a.precision == "fp32" else GB_FP64
+            ms, by = ctx.bench_sweep(fl, prec, reps=a.sweep, flush_l2=2)
+            print(json.dumps({"sweep_ms": ms, "bytes": by, "GBps": by / ms / 1e6}))
             return
         if a.spmv:
             prec = GB_FP32 if a.precision == "fp32" else GB_FP64

@@ -145,6 +145,12 @@ int gb_level_size(const gb_ctx* ctx, int level, int64_t* n, int* B,
  * when a solve first needs them after a matrix or patch upload. */
 int gb_level_set_patches(gb_ctx* ctx, int level, int64_t npatch, int npp,
                          const int64_t* patches);
+/* The inverses of a level's patch matrices, FP64, [patch][j][i] (column j of
+ * the inverse of patch p at (p * M + j) * M, M = npp * B), formed on the device
+ * from the level's current values by the partial-pivot LU of
+ * VankaSmoother::copy_entries_sparseblockmatrix and its solves
+ * (LinAlg/vankasmoother.cc:65-113,192-237) when they are stale. */
+int gb_level_get_vanka_inverse(gb_ctx* ctx, int level, double* host, int64_t len);
 /* Hanging nodes of a level as the mesh's HangingIndexHandler holds them
  * (Mesh/hangingindexhandler.h:40,65): nedge rows [node, 3 parents] (hnq2) and,
  * in 3D, nface rows [node, 9 parents] (hnq2face), nodes ascending, and the
@@ -449,6 +455,29 @@ int gb_get_kernel_count(const gb_ctx* ctx, int64_t* launches);
  * algorithmic bytes per launch. */
 int gb_bench_spmv(gb_ctx* ctx, int level, int precision, int reps,
                   int flush_l2, double* ms_per_launch, double* bytes_per_launch);
+
+/* The same for one smoothing step of a level, the kernel that dominates the
+ * multigrid cycle: with gb_params.smoother 1 (Vanka) on a level with patches,
+ * the patch solves with the inverted patch matrices and the averaging gather
+ * (algorithmic bytes: inverses, patch lists, gathered residual, patch
+ * solutions written and read, node map, u read and written); otherwise one
+ * fused damped-Jacobi sweep of a scalar level (out = u + omega D^-1 (b - A u),
+ * Dirichlet rows kept; the SpMV's bytes plus b, D^-1 and the new iterate). */
+int gb_bench_sweep(gb_ctx* ctx, int level, int precision, int reps,
+                   int flush_l2, double* ms_per_launch, double* bytes_per_launch);
+/* ---- failure detection ------------------------------------------------------
+ * The reference aborts on CUDA errors (cuda/check_cuda.h:28-67); this library
+ * returns codes. gb_set_wait_limit bounds every device-side wait (the grid
+ * barriers of the multi-CTA cycle, GB_MID=1) to wait_ns nanoseconds (default
+ * 1 s): a barrier that runs out sets an error flag, the kernel finishes
+ * without waiting further, and the call returns GB_ETIMEOUT with the context
+ * still usable. phantoms > 0 makes every such barrier wait for that many CTAs
+ * that do not exist, so that its wait runs out (for tests; 0 in normal use).
+ * gb_debug_fail_alloc(k): the k-th device allocation from now on fails as an
+ * out-of-memory cudaMalloc does (host-side fault injection for tests of the
+ * GB_ENOMEM path; 0 turns it off). */
+int gb_set_wait_limit(gb_ctx* ctx, uint64_t wait_ns, int phantoms);
+int gb_debug_fail_alloc(int64_t nth);
 
 /* The compute capability the library's kernels were compiled for, read at run
  * time from a kernel's attributes on the current device (cudaFuncGetAttributes:

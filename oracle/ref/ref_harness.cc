@@ -133,6 +133,15 @@ struct Config
                                // operations, or the mixed-precision device solve
   int savesol = 0;    // write rhs.f64 and solution.f64 without the full dump
   int functional = 0; // functional_l2 in summary.txt: J(u) of L2Functional
+  int flexreps = 0;   // binding binary: that many more device solves with the
+                      // flexible solver, FP64 cycle (flex64_*) and FP32 cycle
+                      // (mixed_*, solution_mixed.f64) in summary.txt
+  int flexgmressize = 0; // binding binary: Krylov memory of the flexible solves
+  int benchspmv = 0;  // binding binary: the finest level's SpMV (FP64, FP32) and
+                      // FP32 Jacobi sweep timed alone (gb_bench_spmv / _sweep)
+  int cpusample = 0;  // that many GMRES steps (maxiter) of the reference's CPU
+                      // solver on the same mesh and right-hand side, timed
+                      // (cpu_sample_* in summary.txt, solution_cpu.f64)
 };
 
 // kappa per cell, one array per resolution N = coarse * 2^l (cells per dim),
@@ -513,6 +522,10 @@ parse(int argc, char** argv)
     else if (k == "backend") c.backend = v;
     else if (k == "savesol") c.savesol = atoi(v.c_str());
     else if (k == "functional") c.functional = atoi(v.c_str());
+    else if (k == "flexreps") c.flexreps = atoi(v.c_str());
+    else if (k == "flexgmressize") c.flexgmressize = atoi(v.c_str());
+    else if (k == "benchspmv") c.benchspmv = atoi(v.c_str());
+    else if (k == "cpusample") c.cpusample = atoi(v.c_str());
     else if (k == "conv") {
       std::stringstream ss(v);
       std::string t;
@@ -785,7 +798,9 @@ run(int argc, char** argv)
   else if (c.backend == "b200" || c.backend == "b200host" || c.backend == "b200mixed") {
     auto* B = new B200MultiLevelSolver(0);
     B->SetDeviceGmres(c.backend != "b200host");
-    B->SetMixedPrecision(c.backend == "b200mixed");
+    B->SetFlexibleMemory(c.flexgmressize);
+    B->SetDeviceSolver(c.backend == "b200mixed" ? B200MultiLevelSolver::kFlexible32
+                                                : B200MultiLevelSolver::kReference);
     MLSp.reset(B);
   }
 #endif
@@ -852,7 +867,7 @@ run(int argc, char** argv)
   S->HNZero(f); // hanging dofs are constrained, not unknowns
   S->SetBoundaryVectorZero(f);
 
-  std::vector<double> times;
+  std::vector<double> times, device_ms_all;
   CGInfo info(c.tol, c.globaltol, 0, c.maxiter, "Lin");
   for (int rep = 0; rep < std::max(1, c.repeat); ++rep) {
     info.reset();
@@ -860,6 +875,10 @@ run(int argc, char** argv)
     MLS.NewtonLinearSolve(A, u, f, info);
     auto t1 = std::chrono::steady_clock::now();
     times.push_back(std::chrono::duration<double>(t1 - t0).count());
+#ifdef GB_B200_BINDING
+    if (auto* B = dynamic_cast<B200MultiLevelSolver*>(&MLS))
+      device_ms_all.push_back(B->LastSolveInfo().device_ms);
+#endif
   }
 
   // true relative residual ||f - A u|| / ||f|| with the reference's own vmult
@@ -916,8 +935,14 @@ run(int argc, char** argv)
     o << "backend " << c.backend << "\n";
 #ifdef GB_B200_BINDING
     if (auto* B = dynamic_cast<B200MultiLevelSolver*>(&MLS))
+    {
       o << "device_ms " << B->LastSolveInfo().device_ms << "\n"
-        << "device_launches " << B->LastSolveInfo().kernel_launches << "\n";
+        << "device_launches " << B->LastSolveInfo().kernel_launches << "\n"
+        << "device_ms_all";
+      for (double t : device_ms_all)
+        o << " " << t;
+      o << "\n";
+    }
 #endif
     o << "solve_s";
     for (double t : times)
@@ -929,6 +954,141 @@ run(int argc, char** argv)
     write_raw(c.out + "/rhs.f64", std::vector<double>(F.begin(), F.end()));
     const GlobalVector& U = S->GetGV(u);
     write_raw(c.out + "/solution.f64", std::vector<double>(U.begin(), U.end()));
+    std::vector<double> xyz;
+    for (int i = 0; i < nf; ++i) {
+      if (c.dim == 3) {
+        const Vertex3d& v = Mf->vertex3d(i);
+        xyz.insert(xyz.end(), { v.x(), v.y(), v.z() });
+      } else {
+        const Vertex2d& v = Mf->vertex2d(i);
+        xyz.insert(xyz.end(), { v.x(), v.y() });
+      }
+    }
+    write_raw(c.out + "/coord.f64", xyz);
+  }
+#ifdef GB_B200_BINDING
+  // more device solves of the same system with the flexible solver: FP64
+  // cycle, then FP32 cycle (mixed precision)
+  if (c.flexreps > 0) {
+    auto* B = dynamic_cast<B200MultiLevelSolver*>(&MLS);
+    if (!B)
+      throw std::runtime_error("flexreps needs a b200 backend");
+    std::vector<int> jc;
+    if (stokes)
+      for (int d = 1; d <= c.dim; ++d)
+        jc.push_back(d);
+    else
+      jc.push_back(0);
+    std::ofstream o(c.out + "/summary.txt", std::ios::app);
+    o.precision(17);
+    for (int kind = 1; kind <= 2; ++kind) {
+      const std::string tag = kind == 1 ? "flex64" : "mixed";
+      Vector um(tag + "_u");
+      MLS.ReInitVector(um);
+      B->SetDeviceSolver(kind == 1 ? B200MultiLevelSolver::kFlexible64
+                                   : B200MultiLevelSolver::kFlexible32);
+      std::vector<double> mms;
+      CGInfo minfo(c.tol, c.globaltol, 0, c.maxiter, tag);
+      for (int rep = 0; rep < c.flexreps; ++rep) {
+        MLS.NewtonLinearSolve(A, um, f, minfo);
+        mms.push_back(B->LastSolveInfo().device_ms);
+      }
+      const gb_solve_info li = B->LastSolveInfo();
+      Vector rm(tag + "_r");
+      MLS.ReInitVector(rm);
+      S->residualgmres(A, rm, um, f);
+      const double rmn = S->Norm(rm) / S->Norm(f);
+      double Jm = 0.0;
+      if (c.functional) {
+        L2Functional JF(jc);
+        Vector jh(tag + "_jh");
+        MLS.ReInitVector(jh);
+        Jm = S->ComputeFunctional(jh, um, &JF);
+      }
+      if (kind == 2) {
+        const GlobalVector& Um = S->GetGV(um);
+        write_raw(c.out + "/solution_mixed.f64", std::vector<double>(Um.begin(), Um.end()));
+      }
+      o << tag << "_iterations " << li.iterations << "\n"
+        << tag << "_restarts " << li.restarts << "\n"
+        << tag << "_launches " << li.kernel_launches << "\n"
+        << tag << "_true_rel_residual " << rmn << "\n"
+        << tag << "_functional_l2 " << Jm << "\n"
+        << tag << "_device_ms_all";
+      for (double t : mms)
+        o << " " << t;
+      o << "\n";
+    }
+    B->SetDeviceSolver(B200MultiLevelSolver::kReference);
+  }
+  if (c.benchspmv) {
+    auto* B = dynamic_cast<B200MultiLevelSolver*>(&MLS);
+    if (!B)
+      throw std::runtime_error("benchspmv needs a b200 backend");
+    gb_ctx* gc = B->DeviceContext();
+    const int fl = nl - 1;
+    double ms = 0, by = 0;
+    std::ofstream o(c.out + "/summary.txt", std::ios::app);
+    o.precision(17);
+    for (int prec = 0; prec <= 1; ++prec) {
+      if (gb_bench_spmv(gc, fl, prec, 20, 2, &ms, &by) != GB_OK)
+        throw std::runtime_error(gb_last_error_string(gc));
+      o << (prec ? "spmv32" : "spmv64") << "_ms " << ms << "\n"
+        << (prec ? "spmv32" : "spmv64") << "_bytes " << by << "\n";
+    }
+    if (ncomp == 1) {
+      if (gb_bench_sweep(gc, fl, 1, 20, 2, &ms, &by) != GB_OK)
+        throw std::runtime_error(gb_last_error_string(gc));
+      o << "sweep32_ms " << ms << "\n"
+        << "sweep32_bytes " << by << "\n";
+    }
+  }
+#endif
+  // the reference's CPU solver on the same mesh, problem and right-hand side,
+  // bounded to cpusample GMRES steps (maxiter), timed after its assembly
+  if (c.cpusample > 0) {
+    StdMultiLevelSolver C;
+    C.BasicInit(&MA, pf, &PC, &FC);
+    C.ReInit();
+    C.SetProblem("diffusion");
+    Matrix Ac("A");
+    Vector uc("u"), fc("f");
+    C.ReInitMatrix(Ac);
+    C.ReInitVector(uc);
+    C.ReInitVector(fc);
+    auto a0 = std::chrono::steady_clock::now();
+    C.AssembleMatrix(Ac, uc);
+    C.ComputeIlu(Ac, uc);
+    auto a1 = std::chrono::steady_clock::now();
+    GlobalVector& Fc = C.GetSolver()->GetGV(fc);
+    const GlobalVector& Fd = S->GetGV(f);
+    std::copy(Fd.begin(), Fd.end(), Fc.begin());
+    CGInfo cinfo(c.tol, c.globaltol, 0, std::min(c.maxiter, c.cpusample), "Cpu");
+    auto t0 = std::chrono::steady_clock::now();
+    C.NewtonLinearSolve(Ac, uc, fc, cinfo);
+    auto t1 = std::chrono::steady_clock::now();
+    const GlobalVector& Uc = C.GetSolver()->GetGV(uc);
+    write_raw(c.out + "/solution_cpu.f64", std::vector<double>(Uc.begin(), Uc.end()));
+    double Jc = 0.0;
+    if (c.functional) {
+      std::vector<int> jc;
+      if (stokes)
+        for (int d = 1; d <= c.dim; ++d)
+          jc.push_back(d);
+      else
+        jc.push_back(0);
+      L2Functional JF(jc);
+      Vector jh("jh3");
+      C.ReInitVector(jh);
+      Jc = C.GetSolver()->ComputeFunctional(jh, uc, &JF);
+    }
+    std::ofstream o(c.out + "/summary.txt", std::ios::app);
+    o.precision(17);
+    o << "cpu_sample_iterations " << cinfo.control().iteration() << "\n"
+      << "cpu_sample_status " << cinfo.control().status() << "\n"
+      << "cpu_sample_s " << std::chrono::duration<double>(t1 - t0).count() << "\n"
+      << "cpu_sample_assemble_s " << std::chrono::duration<double>(a1 - a0).count() << "\n"
+      << "cpu_sample_functional_l2 " << Jc << "\n";
   }
   if (c.dump) {
     for (int l = 0; l < nl; ++l) {

@@ -184,3 +184,36 @@ def test_vanka_cell_patches_match_oracle(ctx):
     assert rel_l2(ctx.download(l, x), xo) < 1e-8
     for v in (x, y, h):
         ctx.free(v)
+
+
+@pytest.mark.parametrize("name", golden_stokes_cases())
+def test_vanka_factors_on_device_equal_host_factors(name):
+    """The patch inverses formed on the device (k_vanka_factor: gather from the
+    SELL values, partial-pivot LU, substitutions) equal, bit for bit, those of
+    the same arithmetic on the host (GB_VANKA_HOST=1), on every level."""
+    import os
+
+    from gascoignelib_b200.native import Context
+    P, ref = load_golden(name)
+    if P.levels[-1].patches is None:
+        pytest.skip("no Vanka patches")
+    inv = {}
+    for mode in ("device", "host"):
+        old = os.environ.get("GB_VANKA_HOST")
+        os.environ["GB_VANKA_HOST"] = "1" if mode == "host" else "0"
+        try:
+            c = Context(0)
+        finally:
+            if old is None:
+                os.environ.pop("GB_VANKA_HOST", None)
+            else:
+                os.environ["GB_VANKA_HOST"] = old
+        try:
+            c.load_problem(P)
+            c.set_params(smoother="vanka")
+            inv[mode] = [c.vanka_inverse(l, L.patches.shape[0], L.patches.shape[1] * L.B)
+                         for l, L in enumerate(P.levels)]
+        finally:
+            c.close()
+    for a, b in zip(inv["device"], inv["host"]):
+        assert np.array_equal(a, b)
