@@ -150,15 +150,25 @@ enum ColMode
 #define GB_SPMV_MINB_F64AX 8
 #endif
 constexpr int kChunk = GB_SPMV_CHUNK;
-template<int MODE, class TV>
+// FP32 levels with fewer rows than kSpmvSmallRows (the middle levels of a
+// hierarchy: one wave or less) take the instantiation with the lower bound of
+// 2 blocks per SM: more registers per thread keep every load of a row in
+// flight, which is what a latency-bound launch of a few hundred warps needs;
+// the large levels keep the occupancy-oriented bounds above.
+#ifndef GB_SPMV_SMALL_ROWS
+#define GB_SPMV_SMALL_ROWS 131072
+#endif
+constexpr int kSpmvSmallRows = GB_SPMV_SMALL_ROWS;
+template<int MODE, class TV, bool SMALL>
 constexpr int spmv_min_blocks()
 {
-  return sizeof(TV) == 4 ? GB_SPMV_MINB_F32
-                         : (MODE == 0 ? GB_SPMV_MINB_F64AX : GB_SPMV_MINB_F64);
+  return SMALL ? 2
+               : (sizeof(TV) == 4 ? GB_SPMV_MINB_F32
+                                  : (MODE == 0 ? GB_SPMV_MINB_F64AX : GB_SPMV_MINB_F64));
 }
 
-template<int MODE, class TV, class TX, class TO, int CM>
-__global__ void __launch_bounds__(kSpmvThreads, (spmv_min_blocks<MODE, TV>()))
+template<int MODE, class TV, class TX, class TO, int CM, bool SMALL = false>
+__global__ void __launch_bounds__(kSpmvThreads, (spmv_min_blocks<MODE, TV, SMALL>()))
 k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
        const TO* __restrict__ b, const TV* __restrict__ dinv,
        const uint8_t* __restrict__ dirmask, double alpha_,
