@@ -673,12 +673,6 @@ __device__ __forceinline__ double ilu_add(double a, double b) { return __dadd_rn
 template<>
 __device__ __forceinline__ float ilu_add(float a, float b) { return __fadd_rn(a, b); }
 
-// One level of the forward substitution with the unit lower factor
-// (SparseBlockIlu::forward, LinAlg/sparseblockilu.xx:202-214): for each row of
-// the level, y_i -= L_ik y_k over its lower blocks in stored (ascending column)
-// order, block entries as FMatrixBlock::subtract (LinAlg/fmatrixblock.h:
-// 136-145). The rows of one level depend only on rows of earlier levels
-// (earlier launches), so the result equals the sequential sweep bit for bit.
 // SparseBlockIlu::compute_ilu (LinAlg/sparseblockilu.xx:246-275) on the
 // device, one dependency level per launch, one thread per row: a row waits
 // only for the rows of its lower part (earlier levels), exactly as in the
@@ -765,74 +759,79 @@ k_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ b)
     b[i] = static_cast<float>(a[i]);
 }
 
-template<int B, class T>
-__global__ void
-k_ilu_lower(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
-            const int* __restrict__ col, const int* __restrict__ diag,
-            const T* __restrict__ val, T* __restrict__ y)
-{
-  GB_PDL_ENTRY();
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nr)
-    return;
-  const int i = __ldg(rows + t);
-  T yi[B];
-#pragma unroll
-  for (int r = 0; r < B; ++r)
-    yi[r] = y[int64_t(i) * B + r];
-  const int e = __ldg(diag + i);
-  for (int pos = __ldg(ptr + i); pos < e; ++pos) {
-    const int64_t k = __ldg(col + pos);
-    const T* m = val + int64_t(pos) * B * B;
-    T yk[B];
-#pragma unroll
-    for (int c = 0; c < B; ++c)
-      yk[c] = y[k * B + c];
-#pragma unroll
-    for (int r = 0; r < B; ++r)
-#pragma unroll
-      for (int c = 0; c < B; ++c)
-        yi[r] = ilu_sub(yi[r], ilu_mul(__ldg(m + r * B + c), yk[c]));
-  }
-#pragma unroll
-  for (int r = 0; r < B; ++r)
-    y[int64_t(i) * B + r] = yi[r];
-}
+// FP64 rows one entry at a time: groups of 4 FP64 entries measured slower
+// (C2 ILU solve 240 against 168 ms with a launch per level), FP32 groups of 8
+// faster (123.9 against 133.7 ms)
+#ifndef GB_ILU_GROUP_F64
+#define GB_ILU_GROUP_F64 1
+#endif
 
-// One level of the backward substitution (SparseBlockIlu::backward,
-// LinAlg/sparseblockilu.xx:217-231): y_i -= U_ik y_k over the upper blocks in
-// descending order, then y_i = D_i^-1 y_i with the inverted diagonal block
-// (FMatrixBlock::vmult, LinAlg/fmatrixblock.h:194-217).
-template<int B, class T>
-__global__ void
-k_ilu_upper(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
-            const int* __restrict__ col, const int* __restrict__ diag,
-            const T* __restrict__ val, T* __restrict__ y)
+// One row of a substitution. Forward, with the unit lower factor
+// (SparseBlockIlu::forward, LinAlg/sparseblockilu.xx:202-214): y_i -= L_ik y_k
+// over the row's lower blocks in stored (ascending column) order, block
+// entries as FMatrixBlock::subtract (LinAlg/fmatrixblock.h:136-145).
+// Backward (SparseBlockIlu::backward, LinAlg/sparseblockilu.xx:217-231):
+// y_i -= U_ik y_k over the upper blocks in descending order, then
+// y_i = D_i^-1 y_i with the inverted diagonal block (FMatrixBlock::vmult,
+// LinAlg/fmatrixblock.h:194-217). The entries are taken G at a time: their
+// columns, then their y blocks and values are loaded together before the
+// subtractions run in the reference's order, so a row waits for about two
+// memory round trips per G entries instead of one per entry. The rows of one
+// dependency level depend only on rows of earlier levels, so running the
+// levels in order gives the sequential sweep bit for bit.
+template<int B, class T, bool UP>
+__device__ __forceinline__ void
+ilu_row(int i, const int* __restrict__ ptr, const int* __restrict__ col,
+        const int* __restrict__ diag, const T* __restrict__ val, T* __restrict__ y)
 {
-  GB_PDL_ENTRY();
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nr)
-    return;
-  const int i = __ldg(rows + t);
+  constexpr int B2 = B * B;
+  // the G value blocks of a group take at most 32 registers; FP64 rows take
+  // GB_ILU_GROUP_F64 entries at a time at most
+  constexpr int G0 = 32 / (B2 * int(sizeof(T) / 4));
+  constexpr int GM = sizeof(T) == 8 ? GB_ILU_GROUP_F64 : 8;
+  constexpr int G = G0 < 1 ? 1 : (G0 > GM ? GM : G0);
   T yi[B];
 #pragma unroll
   for (int r = 0; r < B; ++r)
     yi[r] = y[int64_t(i) * B + r];
   const int d = __ldg(diag + i);
-  for (int pos = __ldg(ptr + i + 1) - 1; pos > d; --pos) {
-    const int64_t k = __ldg(col + pos);
-    const T* m = val + int64_t(pos) * B * B;
-    T yk[B];
+  const int first = UP ? __ldg(ptr + i + 1) - 1 : __ldg(ptr + i);
+  const int cnt = UP ? first - d : d - first;
+  for (int q0 = 0; q0 < cnt; q0 += G) {
+    int pos[G];
+    int64_t k[G];
 #pragma unroll
-    for (int c = 0; c < B; ++c)
-      yk[c] = y[k * B + c];
+    for (int g = 0; g < G; ++g) {
+      pos[g] = UP ? first - (q0 + g) : first + (q0 + g);
+      k[g] = q0 + g < cnt ? __ldg(col + pos[g]) : i; // past the end: a harmless load of y_i
+    }
+    T yk[G][B], m[G][B2];
 #pragma unroll
-    for (int r = 0; r < B; ++r)
+    for (int g = 0; g < G; ++g) {
 #pragma unroll
       for (int c = 0; c < B; ++c)
-        yi[r] = ilu_sub(yi[r], ilu_mul(__ldg(m + r * B + c), yk[c]));
+        yk[g][c] = y[k[g] * B + c];
+#pragma unroll
+      for (int q = 0; q < B2; ++q)
+        m[g][q] = q0 + g < cnt ? __ldg(val + int64_t(pos[g]) * B2 + q) : T(0);
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      if (q0 + g < cnt) {
+#pragma unroll
+        for (int r = 0; r < B; ++r)
+#pragma unroll
+          for (int c = 0; c < B; ++c)
+            yi[r] = ilu_sub(yi[r], ilu_mul(m[g][r * B + c], yk[g][c]));
+      }
   }
-  const T* D = val + int64_t(d) * B * B;
+  if (!UP) {
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+      y[int64_t(i) * B + r] = yi[r];
+    return;
+  }
+  const T* D = val + int64_t(d) * B2;
 #pragma unroll
   for (int r = 0; r < B; ++r) {
     T acc = ilu_mul(__ldg(D + r * B), yi[0]);
@@ -840,6 +839,65 @@ k_ilu_upper(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
     for (int c = 1; c < B; ++c)
       acc = ilu_add(acc, ilu_mul(__ldg(D + r * B + c), yi[c]));
     y[int64_t(i) * B + r] = acc;
+  }
+}
+
+// One wide dependency level of a substitution, one thread per row.
+template<int B, class T, bool UP>
+__global__ void
+k_ilu_level(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
+            const int* __restrict__ col, const int* __restrict__ diag,
+            const T* __restrict__ val, T* __restrict__ y)
+{
+  GB_PDL_ENTRY();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nr)
+    return;
+  ilu_row<B, T, UP>(__ldg(rows + t), ptr, col, diag, val, y);
+}
+
+__device__ __forceinline__ void
+prefetch_l1(const void* p)
+{
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// The consecutive narrow levels lv0..lv1-1 of a substitution in one CTA: the
+// levels run in order with a block barrier between them, which makes the rows
+// one level wrote visible to the threads of the next (y is read by coherent
+// loads). Per level a thread takes rows t, t + 1024, ... of the level. Before
+// the barrier it fetches the first row of its next level, that row's entry
+// range and the cache lines of the row's columns and values into L1, so that
+// after the barrier only the loads of y wait on the previous level. The rows
+// run the same arithmetic in the same order as k_ilu_level's.
+template<int B, class T, bool UP>
+__global__ void __launch_bounds__(kIluCtaThreads, 1)
+k_ilu_levels(int lv0, int lv1, const int* __restrict__ lptr, const int* __restrict__ rows,
+             const int* __restrict__ ptr, const int* __restrict__ col,
+             const int* __restrict__ diag, const T* __restrict__ val, T* __restrict__ y)
+{
+  GB_PDL_ENTRY();
+  int o0 = __ldg(lptr + lv0), o1 = __ldg(lptr + lv0 + 1);
+  for (int lv = lv0; lv < lv1; ++lv) {
+    for (int t = o0 + threadIdx.x; t < o1; t += kIluCtaThreads)
+      ilu_row<B, T, UP>(__ldg(rows + t), ptr, col, diag, val, y);
+    int o2 = o1;
+    if (lv + 1 < lv1) {
+      o2 = __ldg(lptr + lv + 2);
+      const int t = o1 + threadIdx.x;
+      if (t < o2) {
+        const int i = __ldg(rows + t);
+        const int pb = __ldg(ptr + i), pe = __ldg(ptr + i + 1) - 1;
+        prefetch_l1(col + pb);
+        prefetch_l1(col + pe);
+        prefetch_l1(val + int64_t(pb) * B * B);
+        prefetch_l1(val + (int64_t(pb + pe) / 2) * B * B);
+        prefetch_l1(val + (int64_t(pe) + 1) * B * B - 1);
+      }
+    }
+    __syncthreads();
+    o0 = o1;
+    o1 = o2;
   }
 }
 

@@ -20,6 +20,16 @@ constexpr int kSpmvThreads = 256;   // 8 warps = 8 slices per CTA
 constexpr int kRedThreads = 256;
 constexpr int kMaxRedBlocks = 2 * 148;
 constexpr int kMaxV = 128;          // largest gmressize supported
+// block ILU substitutions: the single-CTA kernel over runs of consecutive
+// levels of at most kIluCtaDefaultRows rows each (wider levels: a launch per
+// level). Measured on the C2 ILU solve (mixed / FP64): a launch per level
+// 123.9 / 167.8 ms, runs of levels up to 256 rows 112.4 / 146.9 ms, up to 512
+// rows 117.1 / 147.3 ms, every level in single-CTA runs 242 / 246 ms.
+constexpr int kIluCtaThreads = 1024;
+#ifndef GB_ILU_CTA_DEFAULT_ROWS
+#define GB_ILU_CTA_DEFAULT_ROWS 256
+#endif
+constexpr int kIluCtaDefaultRows = GB_ILU_CTA_DEFAULT_ROWS;
 
 // SpMV epilogue modes
 enum SpmvMode
@@ -236,6 +246,85 @@ k_spmv(SellView<TV> A, const TX* __restrict__ x, TO* __restrict__ y,
   } else { // kJacobi2: the second sweep on top of x1
     const TA h = static_cast<TA>(dinv[row]) * acc;
     y[row] = static_cast<TO>(x1(row) + alpha * h);
+  }
+}
+
+// Row-block SpMV of the large B = 1 levels with FP32 values, an alternative
+// to the SELL kernel kept for comparison (GB_RB=1; measured slower, so off by
+// default): LPR consecutive lanes share a row.
+// The values are a row-major copy (row r's entries at r * Wr + j, Wr a
+// multiple of 4, zero-padded); a lane loads 4 consecutive entries of its row
+// with one 16-byte load and their 4 column offsets (pattern-compressed rows)
+// or columns with another, gathers the 4 x values, and the LPR partial sums
+// are combined by shuffles. The loads of a row are spread over LPR threads and
+// are independent of each other, where the one-row-per-thread SELL kernel has
+// a whole row's loads per thread, more than its registers hold in flight. But
+// a warp's x gathers now go to 8 rows x 4 offsets instead of 32 consecutive
+// rows at one offset, several cache lines per load instead of one or two,
+// and on the C2 finest level the sweep takes about 1.5 times as long as the
+// SELL kernel's. The summation order is not the sequential one (FP32 values
+// only). Modes kResid, kResidDir and kJacobi.
+template<int MODE, int LPR, bool PAT>
+__global__ void __launch_bounds__(256)
+k_spmv_rb(int n, int Wr, const float* __restrict__ val, const int* __restrict__ cols,
+          const uint8_t* __restrict__ pid, const float* __restrict__ x,
+          float* __restrict__ y, const float* __restrict__ b,
+          const float* __restrict__ dinv, const uint8_t* __restrict__ dirmask,
+          float alpha)
+{
+  GB_PDL_ENTRY();
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = g / LPR, sub = g % LPR;
+  float acc = 0.f;
+  if (row < n) {
+    const float* vr = val + int64_t(row) * Wr;
+    const int* cr = PAT ? cols + int(__ldg(pid + row)) * Wr : cols + int64_t(row) * Wr;
+    for (int j = sub * 4; j < Wr; j += LPR * 4) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(vr + j));
+      const int4 o = __ldg(reinterpret_cast<const int4*>(cr + j));
+      const int base = PAT ? row : 0;
+      acc = fmaf(v.x, __ldg(x + base + o.x), acc);
+      acc = fmaf(v.y, __ldg(x + base + o.y), acc);
+      acc = fmaf(v.z, __ldg(x + base + o.z), acc);
+      acc = fmaf(v.w, __ldg(x + base + o.w), acc);
+    }
+  }
+#pragma unroll
+  for (int s = LPR / 2; s > 0; s >>= 1)
+    acc += __shfl_xor_sync(0xffffffffu, acc, s);
+  if (row >= n || sub != 0)
+    return;
+  const float r = b[row] - acc;
+  if (MODE == kResid)
+    y[row] = r;
+  else if (MODE == kResidDir)
+    y[row] = dirmask[row] ? 0.f : r;
+  else // kJacobi: h = dinv * (b - A x); y = x + omega h
+    y[row] = x[row] + alpha * (dinv[row] * r);
+}
+
+// The row-major FP32 copy of a B = 1 SELL level (values, and without
+// patterns the columns): row r's entry j < Wr comes from its slot's lane of
+// the slice; entries past the slice width are value 0, column r (the SELL
+// padding's convention).
+__global__ void
+k_sell_to_rows(int n, int Wr, const int* __restrict__ sptr, const int* __restrict__ rslot,
+               const float* __restrict__ v32, const int* __restrict__ col,
+               float* __restrict__ r32, int* __restrict__ rcol)
+{
+  GB_PDL_ENTRY();
+  const int64_t total = int64_t(n) * Wr;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(e / Wr), j = static_cast<int>(e % Wr);
+    const int t = rslot ? __ldg(rslot + r) : r;
+    const int s = t >> 5, lane = t & 31;
+    const int beg = __ldg(sptr + s), w = (__ldg(sptr + s + 1) - beg) >> 5;
+    const bool in = j < w;
+    const int64_t q = int64_t(beg) + int64_t(j) * kSlice + lane;
+    r32[e] = in ? __ldg(v32 + q) : 0.f;
+    if (rcol)
+      rcol[e] = in ? __ldg(col + q) : r;
   }
 }
 

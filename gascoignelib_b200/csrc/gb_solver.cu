@@ -21,6 +21,7 @@
 #include <memory>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -150,6 +151,13 @@ struct Sell
   // host copies of the layout: slice starts and slot -> row (device-side
   // gathers built on the host, e.g. the Vanka patch matrices, address these)
   std::vector<int> h_sptr, h_perm;
+  // row-major FP32 copy for the row-block SpMV (GB_RB=1, large B = 1 levels):
+  // row r's entries at r * Wr + j, columns from the patterns (rows of Wr
+  // offsets) or from rcol; rslot = row -> slot when the slots are sorted
+  bool rb = false;
+  int Wr = 0;
+  DeviceArray<float> r32;
+  DeviceArray<int> rcol, rslot;
 };
 
 // Host-to-device copy ordered on `st` (the context's stream) and complete on
@@ -204,6 +212,7 @@ build_patterns(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
     }
     pid[r] = static_cast<uint8_t>(it->second);
   }
+  W = (W + 3) / 4 * 4; // rows of 16 bytes: the row-block SpMV loads 4 offsets at once
   std::vector<int> tab(dict.size() * W, 0);
   for (auto& kv : dict)
     for (size_t j = 0; j < kv.first.size(); ++j)
@@ -451,6 +460,14 @@ struct Level
   DeviceArray<double> ilu_v64;
   DeviceArray<float> ilu_v32;
   std::vector<int> ilu_lptr, ilu_uptr; // level offsets into ilu_lrows / ilu_urows
+  DeviceArray<int> ilu_lptr_d, ilu_uptr_d;
+  // the launches of the two substitutions: [lv0, lv1) in one CTA, or one wide level
+  struct IluSeg
+  {
+    int lv0, lv1;
+    bool cta;
+  };
+  std::vector<IluSeg> ilu_lseg, ilu_useg;
   // values assembled on the device since the host copy was made
   bool h_val_stale = false;
   // per A^T SELL entry the A SELL entry it copies (-1: padding), block size 1:
@@ -600,6 +617,10 @@ struct gb_ctx
   // the device kernel k_vanka_factor, which gives the same bits)
   bool vanka_host = false;
   bool ilu_host = false; // GB_ILU_HOST=1: block ILU factors formed on the host
+  bool rb_on = false;    // GB_RB=1: row-block copies and SpMV on the large FP32 levels
+  // widest substitution level run inside a single-CTA launch
+  // (GB_ILU_CTA_ROWS; 0: one launch per level)
+  int ilu_cta_rows = gb::kIluCtaDefaultRows;
   // GB_CLUSTER=1: the levels of at most cluster_rows dofs below the finest
   // (and above the single-CTA coarse levels) as one op program run by one
   // thread-block cluster of 16 CTAs with the hardware cluster barrier between
@@ -825,6 +846,55 @@ read_scalar(Context& c, const double* dptr)
 
 // ----------------------------------------------------------------- SpMV
 
+// The row-major FP32 values of S for the row-block SpMV, from its SELL
+// values (again after every change of those on the device); with
+// `columns`, also the columns of a level without patterns.
+static void
+rows_refresh(Context& c, const Sell& S, bool columns)
+{
+  if (!S.rb)
+    return;
+  const int64_t total = int64_t(S.n) * S.Wr;
+  launch(c, k_sell_to_rows, static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 16)),
+         256, S.n, S.Wr, (const int*)S.sptr.p, (const int*)(S.sorted ? S.rslot.p : nullptr),
+         (const float*)S.v32.p, (const int*)S.col.p, S.r32.p,
+         columns && !S.pat ? S.rcol.p : (int*)nullptr);
+}
+
+// The row-block copy is kept for B = 1 levels of at least kRbMinRows rows
+// whose padding to Wr entries per row (a multiple of 4) adds at most a
+// quarter to the stored entries; other levels use the SELL kernel only.
+constexpr int64_t kRbMinRows = 16384;
+constexpr int kRbLanes = 4; // lanes per row (2, 4 and 8 measured; 2 and 4 fastest)
+
+static void
+build_rows(Context& c, Sell& S, const int64_t* rowptr)
+{
+  S.rb = false;
+  const int64_t n = S.n;
+  if (S.B != 1 || n < kRbMinRows || !c.rb_on)
+    return;
+  int64_t W = 0;
+  for (int64_t r = 0; r < n; ++r)
+    W = std::max<int64_t>(W, rowptr[r + 1] - rowptr[r]);
+  const int64_t Wr = S.pat ? S.W : (W + 3) / 4 * 4;
+  if (Wr * n * 4 > S.nnz * 5 || Wr * n >= (int64_t(1) << 31))
+    return;
+  GB_CUDA(S.r32.alloc(size_t(n * Wr)));
+  if (!S.pat)
+    GB_CUDA(S.rcol.alloc(size_t(n * Wr)));
+  if (S.sorted) {
+    std::vector<int> slot(n);
+    for (int64_t t = 0; t < n; ++t)
+      slot[S.h_perm[t]] = static_cast<int>(t);
+    GB_CUDA(S.rslot.alloc(n));
+    GB_CUDA(h2d(c.stream, S.rslot.p, slot.data(), n * sizeof(int)));
+  }
+  S.Wr = static_cast<int>(Wr);
+  S.rb = true;
+  rows_refresh(c, S, true);
+}
+
 template<int MODE, int B, class TV, class TX, class TO>
 static void
 bspmv(Context& c, const Level& L, const Sell& S, const TX* x, TO* y, const TO* b,
@@ -858,6 +928,22 @@ spmv(Context& c, const Level& L, const Sell& S, const TX* x, TO* y, const TO* b,
       return bspmv<MODE, 4>(c, L, S, x, y, b, dinv, alpha, yidx, ystride, xcopy);
     default:
       throw Error{ GB_EINVAL, "block size must be 1..4" };
+  }
+  if constexpr (std::is_same<TV, float>::value && std::is_same<TX, float>::value &&
+                std::is_same<TO, float>::value &&
+                (MODE == kResid || MODE == kResidDir || MODE == kJacobi)) {
+    if (S.rb && !yidx) {
+      const int nb = blocks_for(int64_t(S.n) * kRbLanes, 256);
+      const float a = static_cast<float>(alpha);
+      const uint8_t* dm = L.dirmask.p;
+      if (S.pat)
+        launch(c, k_spmv_rb<MODE, kRbLanes, true>, nb, 256, S.n, S.Wr, (const float*)S.r32.p,
+               (const int*)S.ptab.p, (const uint8_t*)S.pid.p, x, y, b, dinv, dm, a);
+      else
+        launch(c, k_spmv_rb<MODE, kRbLanes, false>, nb, 256, S.n, S.Wr, (const float*)S.r32.p,
+               (const int*)S.rcol.p, (const uint8_t*)nullptr, x, y, b, dinv, dm, a);
+      return;
+    }
   }
   const SellView<TV> A = view<TV>(S, sell_vals<TV>(S));
   const int nb = blocks_for(S.n, kSpmvThreads);
@@ -1013,6 +1099,7 @@ ensure_AT(Context& c, Level& L)
   }
   GB_CUDA(cudaStreamSynchronize(c.stream));
   build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), c.stream, B);
+  build_rows(c, L.AT, tp.data());
   L.has_AT = true;
   if (B == 1 && L.mesh_ncells > 0) { // device-assembled level: keep A^T current on the GPU
     const std::vector<int> pa = sell_positions(c, L.A, L.h_rowptr.data(), n);
@@ -1389,6 +1476,38 @@ ilu_factor(std::vector<int>& ptr, std::vector<int>& col, std::vector<int>& diag,
 // forward and backward levels of the substitutions (the forward ones are also
 // the factorisation's), and per entry the offset of its block in the SELL
 // values.
+// The dependency levels of both substitutions on the device and as launches:
+// a run of consecutive levels of at most ilu_cta_rows rows each goes to one
+// single-CTA launch (k_ilu_levels, a block barrier between levels instead of
+// a launch), a wider level to a launch of its own (k_ilu_level).
+static void
+ilu_levels_upload(Context& c, Level& L)
+{
+  auto segments = [&](const std::vector<int>& off) {
+    std::vector<Level::IluSeg> seg;
+    const int nlev = static_cast<int>(off.size()) - 1;
+    for (int lv = 0; lv < nlev;) {
+      if (off[lv + 1] - off[lv] > c.ilu_cta_rows) {
+        seg.push_back({ lv, lv + 1, false });
+        ++lv;
+        continue;
+      }
+      int e = lv;
+      while (e < nlev && off[e + 1] - off[e] <= c.ilu_cta_rows)
+        ++e;
+      seg.push_back({ lv, e, true });
+      lv = e;
+    }
+    return seg;
+  };
+  L.ilu_lseg = segments(L.ilu_lptr);
+  L.ilu_useg = segments(L.ilu_uptr);
+  GB_CUDA(L.ilu_lptr_d.alloc(L.ilu_lptr.size()));
+  GB_CUDA(L.ilu_uptr_d.alloc(L.ilu_uptr.size()));
+  GB_CUDA(h2d(c.stream, L.ilu_lptr_d.p, L.ilu_lptr.data(), L.ilu_lptr.size() * sizeof(int)));
+  GB_CUDA(h2d(c.stream, L.ilu_uptr_d.p, L.ilu_uptr.data(), L.ilu_uptr.size() * sizeof(int)));
+}
+
 static void
 ilu_structure(Context& c, Level& L)
 {
@@ -1467,6 +1586,7 @@ ilu_structure(Context& c, Level& L)
   GB_CUDA(h2d(c.stream, L.ilu_lrows.p, lrows.data(), n * sizeof(int)));
   GB_CUDA(h2d(c.stream, L.ilu_urows.p, urows.data(), n * sizeof(int)));
   GB_CUDA(h2d(c.stream, L.ilu_map.p, map.data(), map.size() * sizeof(int)));
+  ilu_levels_upload(c, L);
   L.ilu_struct = true;
 }
 
@@ -1602,6 +1722,7 @@ ensure_ilu_host(Context& c, Level& L)
   GB_CUDA(h2d(c.stream, L.ilu_urows.p, urows.data(), n * sizeof(int)));
   GB_CUDA(h2d(c.stream, L.ilu_v64.p, v.data(), v.size() * sizeof(double)));
   GB_CUDA(h2d(c.stream, L.ilu_v32.p, v32.data(), v32.size() * sizeof(float)));
+  ilu_levels_upload(c, L);
   L.ilu_ready = true;
   L.ilu_struct = false; // the device path rebuilds its gather map
 }
@@ -2042,32 +2163,37 @@ struct Emit
     no_rec();
     const T* val = sizeof(T) == 8 ? reinterpret_cast<const T*>(L.ilu_v64.p)
                                   : reinterpret_cast<const T*>(L.ilu_v32.p);
-    const int nl = static_cast<int>(L.ilu_lptr.size()) - 1;
-    const int nu = static_cast<int>(L.ilu_uptr.size()) - 1;
-    for (int q = 0; q < nl + nu; ++q) {
-      const bool up = q >= nl;
+    const int* ptr = L.ilu_ptr.p;
+    const int* col = L.ilu_col.p;
+    const int* diag = L.ilu_diag.p;
+    for (int up = 0; up < 2; ++up) {
       const std::vector<int>& off = up ? L.ilu_uptr : L.ilu_lptr;
-      const int lv = up ? q - nl : q;
-      const int cnt = off[lv + 1] - off[lv];
-      if (cnt == 0)
-        continue;
-      const int* rows = (up ? L.ilu_urows.p : L.ilu_lrows.p) + off[lv];
-#define GB_ILU(BB)                                                                       \
-  if (up)                                                                                \
-    launch(c, k_ilu_upper<BB, T>, blocks_for(cnt, 128), 128, cnt, rows,                 \
-           (const int*)L.ilu_ptr.p, (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p,   \
-           val, h);                                                                      \
+      const int* lptr = up ? L.ilu_uptr_d.p : L.ilu_lptr_d.p;
+      const int* rows = up ? L.ilu_urows.p : L.ilu_lrows.p;
+      for (const Level::IluSeg& g : up ? L.ilu_useg : L.ilu_lseg) {
+        const int cnt = off[g.lv0 + 1] - off[g.lv0];
+#define GB_ILU_UP(BB, UP)                                                                \
+  if (g.cta)                                                                             \
+    launch(c, k_ilu_levels<BB, T, UP>, 1, kIluCtaThreads, g.lv0, g.lv1, lptr, rows, ptr, \
+           col, diag, val, h);                                                           \
   else                                                                                   \
-    launch(c, k_ilu_lower<BB, T>, blocks_for(cnt, 128), 128, cnt, rows,                 \
-           (const int*)L.ilu_ptr.p, (const int*)L.ilu_col.p, (const int*)L.ilu_diag.p,   \
-           val, h)
-      switch (L.B) {
-        case 1: GB_ILU(1); break;
-        case 2: GB_ILU(2); break;
-        case 3: GB_ILU(3); break;
-        default: GB_ILU(4);
-      }
+    launch(c, k_ilu_level<BB, T, UP>, blocks_for(cnt, 128), 128, cnt, rows + off[g.lv0], \
+           ptr, col, diag, val, h)
+#define GB_ILU(BB)                                                                       \
+  if (up) {                                                                              \
+    GB_ILU_UP(BB, true);                                                                 \
+  } else {                                                                               \
+    GB_ILU_UP(BB, false);                                                                \
+  }
+        switch (L.B) {
+          case 1: GB_ILU(1); break;
+          case 2: GB_ILU(2); break;
+          case 3: GB_ILU(3); break;
+          default: GB_ILU(4);
+        }
 #undef GB_ILU
+#undef GB_ILU_UP
+      }
     }
   }
   // u = (u_zero ? 0 : u) + omega h
@@ -3608,11 +3734,13 @@ assemble_level(Context& c, int l, const double* beta)
   launch(c, k_blockdiag_inverse<1>, blocks_for(L.n, 128), 128, (int)L.n,
          (const double*)L.m_dd.p, L.dinv64.p, L.dinv32.p);
   L.h_val_stale = true;
-  if (L.has_AT && L.at_map.n) // A^T: the same values, gathered in its order
+  rows_refresh(c, A, false);
+  if (L.has_AT && L.at_map.n) { // A^T: the same values, gathered in its order
     launch(c, k_gather_values, blocks_for(int64_t(L.AT.entries), 256), 256,
            (int64_t)L.AT.entries, (const int*)L.at_map.p, (const double*)A.v64.p, L.AT.v64.p,
            L.AT.v32.p);
-  else
+    rows_refresh(c, L.AT, false);
+  } else
     L.has_AT = false;
   L.ilu_ready = false;
   if (c.params.smoother != 0 || L.vk_ready) { // Vanka / ILU factors: full set-up again
@@ -3767,6 +3895,10 @@ gb_ctx_create(gb_ctx** out, int device)
       ctx->mid_on = atoi(e) != 0;
     if (const char* e = getenv("GB_ILU_HOST"))
       ctx->ilu_host = atoi(e) != 0;
+    if (const char* e = getenv("GB_RB"))
+      ctx->rb_on = atoi(e) != 0;
+    if (const char* e = getenv("GB_ILU_CTA_ROWS"))
+      ctx->ilu_cta_rows = std::max(0, atoi(e));
     if (const char* e = getenv("GB_VANKA_HOST"))
       ctx->vanka_host = atoi(e) != 0;
     if (const char* e = getenv("GB_CLUSTER"))
@@ -3914,6 +4046,7 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   L.h_diag.assign(diag, diag + n);
   L.h_val.assign(val, val + nnzb * B * B);
   build_sell(L.A, n, rowptr, col, val, ctx->stream, B);
+  build_rows(*ctx, L.A, rowptr);
   L.has_AT = false;
   L.vk_ready = false;
   L.vk_struct = false;

@@ -84,3 +84,59 @@ def test_block_ilu_stokes_bitexact(ctx):
     assert rel_l2(ctx.download(fl, x), xo) < 1e-8
     ctx.free(x)
     ctx.free(b)
+
+
+def _context_with(env):
+    import os
+
+    from gascoignelib_b200.native import Context
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return Context(0)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("cta_rows", ["4096", "600"])
+def test_single_cta_level_runs_equal_level_launches(cta_rows):
+    """The substitution levels run inside one CTA (a block barrier between
+    levels) give the same results as one launch per level (the default), bit
+    for bit: FP64 sweeps on the 33^3 and 65^3 Q1 levels (225 and 449
+    dependency levels of up to 1073 rows) and FP32 and FP64 flexible solves,
+    with every level in single-CTA runs (4096) and with a mix of single-CTA
+    runs and wide-level launches (600)."""
+    from gascoignelib_b200.problem import seeded_inputs, structured_problem
+    kappa, rhs = seeded_inputs(3, 1, 6)
+    P = structured_problem(3, 1, 6, kappa, rhs)
+    fl = P.nlevels - 1
+    out = {}
+    for tag, env in (("launches", {"GB_ILU_CTA_ROWS": "0"}),
+                     ("cta", {"GB_ILU_CTA_ROWS": cta_rows})):
+        c = _context_with(env)
+        try:
+            c.load_problem(P)
+            c.set_params(omega=1.0, smoother="ilu", gmressize=11, tol=1e-30,
+                         globaltol=1e-300, maxiter=10)
+            x, y, h = c.vec(), c.vec(), c.vec()
+            res = []
+            for l in (fl - 1, fl):
+                n = P.levels[l].ndof
+                r = np.random.default_rng(100 + l)
+                c.upload(l, x, r.standard_normal(n))
+                c.upload(l, y, r.standard_normal(n))
+                c.smooth(l, 2, x, y, h)
+                res.append(c.download(l, x))
+            c.upload(fl, y, P.rhs)
+            for prec in (GB_FP64, GB_FP32):
+                c.fgmres(x, y, prec, check=False)
+                res.append(c.download(fl, x))
+            out[tag] = res
+        finally:
+            c.close()
+    for a, b in zip(out["launches"], out["cta"]):
+        assert np.array_equal(a, b)
