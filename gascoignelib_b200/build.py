@@ -11,12 +11,15 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", "gb_solver.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in sorted(os.listdir(os.path.join(HERE, "csrc")))
+CSRC = os.path.join(HERE, "csrc")
+# translation units: level set-up, the cycle, the GMRES drivers, the C-ABI
+SRC = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
+DEPS = SRC + [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
               if f.endswith(".cuh")] + [os.path.join(ROOT, "include", "gascoigne_b200.h")]
 OUT = os.path.join(HERE, "_lib", "libgascoigne_b200.so")
+OBJ = os.path.join(HERE, "_lib", "obj")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
-              "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
+              "-std=c++17", "-Xcompiler", "-fPIC", "-Xfatbin", "-compress-all"]
 
 
 def _nvcc():
@@ -32,10 +35,28 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(d) <= t for d in DEPS):
             return OUT
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", OUT] + SRC
+    os.makedirs(OBJ, exist_ok=True)
+    nvcc = _nvcc()
+    objs, procs = [], []
+    for src in SRC:  # the units compile in parallel
+        obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+        cmd = [nvcc] + NVCC_FLAGS + ["-c", "-o", obj, src]
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                            text=True)))
+        objs.append(obj)
+    errors = []
+    for cmd, p in procs:
+        out, err = p.communicate()
+        if p.returncode != 0:
+            errors.append(" ".join(cmd) + "\n" + out + err)
+        elif verbose:
+            print(" ".join(cmd))
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     if verbose:
         print(" ".join(cmd))
     return OUT

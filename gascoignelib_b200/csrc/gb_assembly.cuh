@@ -2,8 +2,8 @@
 // -div(kappa grad u) + beta . grad u on quadrilateral / hexahedral cells with
 // one coefficient kappa per cell: element matrices, their summation into the
 // level's SELL-32 values, the strong Dirichlet rows and columns, and the
-// coarsening of kappa to the next coarser level. Included by gb_solver.cu after
-// gb_block.cuh.
+// coarsening of kappa to the next coarser level. Included by gb_context.cuh
+// after gb_block.cuh.
 #pragma once
 #include "gb_kernels.cuh"
 
@@ -382,7 +382,7 @@ struct CondOp
 // hnstructureq23d.cc:161-378). The host orders each cell's steps (edges,
 // then faces, ascending slots). One warp per cell, lane i holding row /
 // column i; a product and a sum per entry, rounded separately.
-__global__ void __launch_bounds__(128)
+static __global__ void __launch_bounds__(128)
 k_condense(int nh, const int* __restrict__ hcells, const int* __restrict__ opptr,
            const CondOp* __restrict__ ops, int nl, int ncells, double* __restrict__ E)
 {
@@ -421,7 +421,7 @@ k_condense(int nh, const int* __restrict__ hcells, const int* __restrict__ opptr
 
 // mask[list[k]] = 1 for k < nl (the hanging nodes into the assembly's
 // Dirichlet-or-hanging row mask)
-__global__ void
+static __global__ void
 k_mark_nodes(int nl, const int* __restrict__ list, uint8_t* __restrict__ mask)
 {
   GB_PDL_ENTRY();
@@ -445,7 +445,7 @@ k_mark_nodes(int nl, const int* __restrict__ list, uint8_t* __restrict__ mask)
 // that a row's entries are summed by several threads at once.
 constexpr int kAsmSplit = 4;
 
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 k_asm_gather(int n, const int* __restrict__ sptr, const int* __restrict__ perm,
              const int* __restrict__ col, const int* __restrict__ cptr,
              const int* __restrict__ clist, const double* __restrict__ E,
@@ -499,7 +499,7 @@ k_asm_gather(int n, const int* __restrict__ sptr, const int* __restrict__ perm,
 // kappa of each coarse cell: the sum of its children's values in ascending
 // order divided by their number (the harness's coefficient pyramid; a
 // per-cell coefficient of the coarser mesh, Application::SetCellData).
-__global__ void
+static __global__ void
 k_kappa_coarsen(int nc, const int* __restrict__ cptr, const int* __restrict__ child,
                 const double* __restrict__ kf, double* __restrict__ kc)
 {
@@ -516,7 +516,7 @@ k_kappa_coarsen(int nc, const int* __restrict__ cptr, const int* __restrict__ ch
 
 // v[e] = src[map[e]] (0 where map[e] < 0), FP64 and FP32: the transpose's
 // values from the matrix's after a device assembly.
-__global__ void
+static __global__ void
 k_gather_values(int64_t ne, const int* __restrict__ map, const double* __restrict__ src,
                 double* __restrict__ v64, float* __restrict__ v32)
 {
@@ -692,7 +692,7 @@ k_elem_apply(int ncells, const int* __restrict__ cells, const double* __restrict
 // y[r] += d * (the element residuals of the cells of node r, in ascending cell
 // order: LocalToGlobal, DofHandler/cgdisc.h:367-380); nodes whose entries in
 // nptr are empty keep y.
-__global__ void
+static __global__ void
 k_form_gather(int n, const int* __restrict__ nptr, const int* __restrict__ nlist,
               const double* __restrict__ F, double d, double* __restrict__ y)
 {
@@ -710,7 +710,7 @@ k_form_gather(int n, const int* __restrict__ nptr, const int* __restrict__ nlist
 // y = 0 on the Dirichlet dofs, and the largest |y| into *m (the bit pattern of
 // a non-negative double orders like the number: atomicMax on it is exact and
 // independent of the order)
-__global__ void
+static __global__ void
 k_dirichlet_absmax(int n, const uint8_t* __restrict__ dirmask, double* __restrict__ y,
                    unsigned long long* m)
 {

@@ -1,6 +1,6 @@
 // Block-system kernels (ncomp = B > 1 components per node, Stokes-type
-// systems), the pressure filter and the Vanka smoother. Included by
-// gb_solver.cu after gb_kernels.cuh.
+// systems), the pressure filter, the Vanka smoother and the block ILU.
+// Included by gb_context.cuh after gb_kernels.cuh.
 #pragma once
 #include "gb_kernels.cuh"
 
@@ -365,7 +365,7 @@ constexpr int kVankaWarps = 4;
 // The result equals the host factorisation of the same arithmetic bit for bit.
 constexpr int kVankaFactorThreads = 128;
 
-__global__ void __launch_bounds__(kVankaFactorThreads)
+static __global__ void __launch_bounds__(kVankaFactorThreads)
 k_vanka_factor(int npatch, int npp, int B, int M, const int* __restrict__ map,
                const double* __restrict__ val, double* __restrict__ inv64,
                float* __restrict__ inv32)
@@ -737,7 +737,7 @@ k_ilu_factor(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
 
 // The ILU's values in its row-sorted layout from the level's SELL values:
 // entry e, component q at val[map[e] + 32 q].
-__global__ void
+static __global__ void
 k_ilu_gather(int64_t nnz, int B2, const int* __restrict__ map,
              const double* __restrict__ val, double* __restrict__ v)
 {
@@ -750,7 +750,7 @@ k_ilu_gather(int64_t nnz, int B2, const int* __restrict__ map,
   }
 }
 
-__global__ void
+static __global__ void
 k_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ b)
 {
   GB_PDL_ENTRY();

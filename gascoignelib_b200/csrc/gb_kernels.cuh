@@ -307,7 +307,7 @@ k_spmv_rb(int n, int Wr, const float* __restrict__ val, const int* __restrict__ 
 // patterns the columns): row r's entry j < Wr comes from its slot's lane of
 // the slice; entries past the slice width are value 0, column r (the SELL
 // padding's convention).
-__global__ void
+static __global__ void
 k_sell_to_rows(int n, int Wr, const int* __restrict__ sptr, const int* __restrict__ rslot,
                const float* __restrict__ v32, const int* __restrict__ col,
                float* __restrict__ r32, int* __restrict__ rcol)
@@ -518,7 +518,7 @@ k_convert(int64_t n, TO* __restrict__ y, const TI* __restrict__ x)
 }
 
 // y += s * x   (Add)
-__global__ void
+static __global__ void
 k_add(int64_t n, double* __restrict__ y, double s, const double* __restrict__ x)
 {
   GB_PDL_ENTRY();
@@ -528,7 +528,7 @@ k_add(int64_t n, double* __restrict__ y, double s, const double* __restrict__ x)
 }
 
 // y *= *scale (device scalar): Equ(v, 1/s, v) with the reciprocal formed first
-__global__ void
+static __global__ void
 k_scale_dev(int64_t n, double* __restrict__ y, const double* __restrict__ scale)
 {
   GB_PDL_ENTRY();
@@ -650,7 +650,7 @@ k_dot(int64_t n, const TA* __restrict__ a, const TB* __restrict__ b,
 
 // Modified Gram-Schmidt step (GMRES::orthogonalization, LinAlg/gmres.cc:
 // 108-118), fused: vv -= d * vi (if vi), then partial <vv, vnext>.
-__global__ void __launch_bounds__(kRedThreads)
+static __global__ void __launch_bounds__(kRedThreads)
 k_mgs(int64_t n, double* __restrict__ vv, const double* __restrict__ vi,
       const double* __restrict__ dcoef, const double* __restrict__ vnext,
       double* partials, unsigned* ticket, RedOut ro)
@@ -900,7 +900,7 @@ cginfo_check(CGInfoDev& I, double resi)
 }
 
 // gamma[0] = rho, inv = 1/rho (GMRES::solve, LinAlg/gmres.cc:182-192)
-__global__ void
+static __global__ void
 k_gmres_init(GmresDev* G, const double* rho_p)
 {
   GB_PDL_ENTRY();
@@ -915,7 +915,7 @@ k_gmres_init(GmresDev* G, const double* rho_p)
 // (LinAlg/gmres.cc:122-135), 1/s, givens_rotation (:88-104), CGInfo check.
 // mode 1 = left-preconditioned (CGInfo rule); mode 2 = flexible (stop when
 // |gamma| <= tol * bnorm or maxsteps).
-__global__ void
+static __global__ void
 k_gmres_step(GmresDev* G, int dim, int second_pass, int mode, int maxsteps)
 {
   GB_PDL_ENTRY();
@@ -957,7 +957,7 @@ k_gmres_step(GmresDev* G, int dim, int second_pass, int mode, int maxsteps)
 }
 
 // GMRES::solution's backward (Common/mult.h:130-141) on H1(i,j) = H[j][i].
-__global__ void
+static __global__ void
 k_gmres_backward(GmresDev* G, int dim)
 {
   GB_PDL_ENTRY();
@@ -970,7 +970,7 @@ k_gmres_backward(GmresDev* G, int dim)
 }
 
 // Flexible GMRES restart: gamma[0] = beta, inv = 1/beta, reset the Hessenberg.
-__global__ void
+static __global__ void
 k_fgmres_restart(GmresDev* G, const double* beta_p, int vmax)
 {
   GB_PDL_ENTRY();
@@ -998,7 +998,7 @@ k_fgmres_restart(GmresDev* G, const double* beta_p, int vmax)
 
 constexpr int kCgsMaxJ = 32; // graph path: gmressize <= 33
 
-__global__ void
+static __global__ void
 k_fg_setup(GmresDev* G, double tol, double globaltol, int maxiter)
 {
   GB_PDL_ENTRY();
@@ -1018,7 +1018,7 @@ k_fg_setup(GmresDev* G, double tol, double globaltol, int maxiter)
 // Refinement cycle start: beta = ||b - A x|| (in beta_tmp). Stops both loops
 // when converged, out of iterations or non-finite; otherwise resets the
 // Hessenberg system of the cycle.
-__global__ void
+static __global__ void
 k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
              cudaGraphConditionalHandle inner, int m, int maxrestarts, int use_cond)
 {
@@ -1136,7 +1136,7 @@ k_load_idx(int64_t n, TO* __restrict__ y, double* __restrict__ V,
 }
 
 // V[(*jp) * n + i] *= *s
-__global__ void
+static __global__ void
 k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
             const double* __restrict__ sp)
 {
@@ -1163,7 +1163,7 @@ k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
 constexpr int kCgsThreads = 256;
 constexpr int kCgsMaxBlocks = 4 * 148;
 
-__device__ void fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m,
+static __device__ void fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m,
                         int use_cond);
 
 template<int MODE, int NV>
@@ -1338,7 +1338,7 @@ k_cgs(int64_t n, double* __restrict__ V, GmresDev* G, double* partials,
 // Givens update of column j (LinAlg/gmres.cc:88-104 applied to the flexible
 // Hessenberg), residual estimate |gamma[j+1]| = ||b - A x_j|| in exact
 // arithmetic, then j += 1 and the inner loop condition.
-__device__ void
+static __device__ void
 fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
 {
   const int last = G->j, dim = last + 1;
@@ -1371,7 +1371,7 @@ fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
     cudaGraphSetConditional(inner, reached ? 0 : 1);
 }
 
-__global__ void
+static __global__ void
 k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
 {
   GB_PDL_ENTRY();
@@ -1379,7 +1379,7 @@ k_fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m, int use_cond)
 }
 
 // hs = H^-1 gamma on the first G->j columns (Common/mult.h:130-141)
-__global__ void
+static __global__ void
 k_fg_backward(GmresDev* G)
 {
   GB_PDL_ENTRY();
@@ -1907,7 +1907,7 @@ k_coarse_direct(int n, const double* __restrict__ Ainv, const T* __restrict__ b,
 
 // Reads n 16-byte words (an L2 eviction that leaves only clean lines behind);
 // the sink write never happens for real data.
-__global__ void
+static __global__ void
 k_read_flush(const uint4* __restrict__ p, int64_t n, unsigned* sink)
 {
   GB_PDL_ENTRY();
