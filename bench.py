@@ -49,30 +49,72 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and throttle reasons during the timed region, read (never set)
+    through NVML every 5 ms, with one reading on entry and one on exit; the GPU
+    is found by its UUID. Falls back to nvidia-smi every 200 ms when NVML is
+    not available."""
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period=0.005):
         self.index = index
+        self.period = period
         self.samples = []
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        self._h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            self._h = pynvml.nvmlDeviceGetHandleByUUID(
+                uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self._nvml = pynvml
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        n, h = self._nvml, self._h
+        try:
+            r = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+            bits = (n.nvmlClocksEventReasonHwSlowdown, n.nvmlClocksEventReasonHwThermalSlowdown,
+                    n.nvmlClocksEventReasonSwThermalSlowdown, n.nvmlClocksEventReasonSwPowerCap)
+            self.samples.append([str(n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)),
+                                 str(n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM)),
+                                 str(n.nvmlDeviceGetPowerUsage(h) / 1000.0)] +
+                                ["Active" if r & b else "Not Active" for b in bits])
+        except Exception:
+            pass
+
+    def _sample_smi(self):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        idx = ids[self.index] if self.index < len(ids) else str(self.index)
+        try:
+            r = subprocess.run(["nvidia-smi", "-i", idx,
+                                f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
+                               capture_output=True, text=True, timeout=5)
+            if r.returncode == 0 and r.stdout.strip():
+                self.samples.append([x.strip() for x in r.stdout.strip().split(",")])
+        except Exception:
+            pass
+
+    def _sample(self):
+        if self._nvml is not None:
+            self._sample_nvml()
+        else:
+            self._sample_smi()
 
     def _run(self):
         while not self._stop.is_set():
-            try:
-                r = subprocess.run(["nvidia-smi", "-i", str(self.index),
-                                    f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
-                                   capture_output=True, text=True, timeout=5)
-                if r.returncode == 0 and r.stdout.strip():
-                    self.samples.append([x.strip() for x in r.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+            self._sample()
+            self._stop.wait(self.period if self._nvml is not None else 0.2)
 
     def __enter__(self):
+        self._sample()
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
         return self
@@ -80,6 +122,7 @@ class ClockSampler:
     def __exit__(self, *a):
         self._stop.set()
         self._t.join(timeout=10)
+        self._sample()
 
     def summary(self):
         if not self.samples:
@@ -90,8 +133,10 @@ class ClockSampler:
         reasons = sorted({names[i] for s in self.samples for i in range(4)
                           if len(s) > 3 + i and s[3 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_min_mhz": min(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(self.samples),
+                "source": "nvml" if self._nvml is not None else "nvidia-smi"}
 
 
 def cpu_baseline(kappa_rhs, ndof, threads):
