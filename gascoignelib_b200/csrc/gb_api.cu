@@ -903,9 +903,10 @@ gb_restrict_zero(gb_ctx* ctx, int lvl, int coarse_id, int fine_id)
     case 1:
       if (T.rmaxw <= 32)
         launch(*ctx, k_restrict4<double>, blocks_for(int64_t(T.nc) * 4, 256), 256, T.nc, tp,
-               te, f, cc, nm);
+               te, f, cc, nm, (const double*)nullptr, (double*)nullptr, 0.0);
       else
-        launch(*ctx, k_restrict<double>, nb, 256, T.nc, tp, te, f, cc, nm);
+        launch(*ctx, k_restrict<double>, nb, 256, T.nc, tp, te, f, cc, nm,
+               (const double*)nullptr, (double*)nullptr, 0.0);
       break;
     case 2:
       launch(*ctx, k_restrict_b<double, 2>, nb, 256, T.nc, tp, te, f, cc, nm, -1,

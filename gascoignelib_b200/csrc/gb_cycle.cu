@@ -339,7 +339,7 @@ void Emit<T>::resid(int l, const T* u, T* out, const T* b)
 }
 
 template<class T>
-void Emit<T>::restrict_to(int l, const T* fine, T* coarse, const double* smean)
+void Emit<T>::restrict_to(int l, const T* fine, T* coarse, const double* smean, T* u1)
 {
   const Transfer& Tr = c.T[l];
   if (rec) {
@@ -356,15 +356,18 @@ void Emit<T>::restrict_to(int l, const T* fine, T* coarse, const double* smean)
   }
   const uint8_t* cm = c.L[l].dirmask.p;
   const int nb = blocks_for(Tr.nc, 256);
+  const T* dv = u1 ? dinv_of<T>(c.L[l]) : nullptr;
   switch (c.L[l].B) {
     case 1:
       if (Tr.rmaxw <= 32)
         launch(c, k_restrict4<T>, blocks_for(int64_t(Tr.nc) * 4, 256), 256, Tr.nc,
-               Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+               Tr.rptr.p, Tr.rent.p, fine, coarse, cm, dv, u1, c.params.omega);
       else
-        launch(c, k_restrict<T>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm);
+        launch(c, k_restrict<T>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm, dv,
+               u1, c.params.omega);
       break;
     case 2:
+      GB_REQUIRE(!u1, GB_EINVAL, "fused first sweep on a block level");
       launch(c, k_restrict_b<T, 2>, nb, 256, Tr.nc, Tr.rptr.p, Tr.rent.p, fine, coarse, cm,
              pf_comp(c.L[l + 1]), smean);
       break;
@@ -549,7 +552,11 @@ smooth(Emit<T>& E, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero)
 
 template<class T>
 bool mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel,
-                   char& p0, char p, T*& u, T*& tmp, const T* b, bool u_zero);
+                   char& p0, char p, T*& u, T*& tmp, const T* b, bool u_zero,
+                   bool first_done = false);
+template<class T>
+bool mgstep_down(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel,
+                 char& p0, char p, T*& u, T*& tmp, const T* b, bool u_zero);
 
 template<class T>
 const CoarseProgram& coarse_program(Context& c, MgWork<T>& W, int l, int finelevel,
@@ -964,12 +971,26 @@ run_dense(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char&
 // they do not change u. HNDistribute/HNAverage/HNZero are identities on meshes
 // without hanging nodes.
 // Returns true when u is still implicitly zero (no sweep has written it).
+// With first_done, the restriction into b has already run this level's first
+// Jacobi sweep from 0 into u (fuse_first_sweep).
 template<class T>
 bool
 mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
-       char p, T*& u, T*& tmp, const T* b, bool u_zero)
+       char p, T*& u, T*& tmp, const T* b, bool u_zero, bool first_done)
 {
   Context& c = E.c;
+  const gb_params& P = c.params;
+  if (first_done) {
+    bool z = false;
+    if (l == coarselevel) {
+      if (p == 'F')
+        p0 = 'V';
+      smooth<T>(E, l, P.iterexact - 1, u, tmp, b, z); // smooth_exact
+      return false;
+    }
+    smooth<T>(E, l, P.iterpre - 1, u, tmp, b, z);
+    return mgstep_down<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b, false);
+  }
   if (!E.rec && c.coarse_on && l == c.mid_level && u_zero && l != E.no_dense_at)
     return run_mid<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b);
   if (!E.rec && c.coarse_on && l <= c.coarse_root)
@@ -978,7 +999,6 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
     return emit_dense<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b);
   if (!E.rec && c.coarse_on && l <= c.dense_root && u_zero && l != E.no_dense_at)
     return run_dense<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b);
-  const gb_params& P = c.params;
   if (l == coarselevel) {
     if (p == 'F')
       p0 = 'V';
@@ -990,8 +1010,43 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
     return u_zero;
   }
   smooth<T>(E, l, P.iterpre, u, tmp, b, u_zero);
+  return mgstep_down<T>(E, W, l, finelevel, coarselevel, p0, p, u, tmp, b, u_zero);
+}
+
+// Whether the restriction into level lc (visited once, from u = 0) can also
+// run lc's first smoothing sweep: the fused scalar Jacobi sweep from zero,
+// u = omega D^-1 b, is elementwise in the restricted b, so the restriction
+// kernel writes it beside b (restrict_store) and the launch of
+// k_jacobi_from_zero goes. Not where lc's sub-cycle is a recorded program or a
+// dense map, a direct solve, or has hanging nodes (HNDistribute comes between
+// the restriction and the sweep).
+template<class T>
+bool
+fuse_first_sweep(const Emit<T>& E, int lc, int coarselevel, int visits)
+{
+  const Context& c = E.c;
+  const Level& C = c.L[lc];
+  return !E.rec && visits == 1 && !c.jacobi2 && C.B == 1 && fused_smoother(c, C) &&
+         !C.has_hn() &&
+         !(c.coarse_on && (lc == c.mid_level || lc <= c.coarse_root || lc <= c.dense_root)) &&
+         !(lc == 0 && direct_on(c)) &&
+         (lc == coarselevel ? c.params.iterexact : c.params.iterpre) >= 1;
+}
+
+// The rest of mgstep on level l after its pre-smoothing: the residual and its
+// restriction, the coarse visits, the prolonged correction and the
+// post-smoothing.
+template<class T>
+bool
+mgstep_down(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0,
+            char p, T*& u, T*& tmp, const T* b, bool u_zero)
+{
+  Context& c = E.c;
+  const gb_params& P = c.params;
+  const int j = (p0 == 'V') ? 1 : (p0 == 'W') ? 2 : (p0 == 'F') ? 3 : 0;
   // MatrixResidual into tmp (with SubtractMeanAlgebraic), restrict_zero +
   // SetBoundaryVectorZero on l-1
+  bool fused = false;
   if (c.L[l].pf_mask && Emit<T>::pf_comp(c.L[l]) >= 0 && c.L[l].B > 1) {
     // filtered residual: its mean is subtracted as the restriction reads it
     if (u_zero) {
@@ -1007,23 +1062,26 @@ mgstep(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, char& p0
       E.resid(l, u, tmp, b);
     E.pf_sub(l, tmp, false);
     E.restrict_to(l - 1, tmp, W.b[l - 1].p);
-  } else if (u_zero) {
-    E.restrict_to(l - 1, b, W.b[l - 1].p); // u == 0: the residual is b
   } else {
-    E.resid(l, u, tmp, b);
-    E.restrict_to(l - 1, tmp, W.b[l - 1].p);
+    fused = fuse_first_sweep<T>(E, l - 1, coarselevel, j);
+    T* u1 = fused ? W.u[l - 1].p : nullptr;
+    if (u_zero) {
+      E.restrict_to(l - 1, b, W.b[l - 1].p, nullptr, u1); // u == 0: the residual is b
+    } else {
+      E.resid(l, u, tmp, b);
+      E.restrict_to(l - 1, tmp, W.b[l - 1].p, nullptr, u1);
+    }
   }
   if (c.L[l - 1].has_hn()) { // HNDistribute, then SetBoundaryVectorZero again
     E.hn_distribute(l - 1, W.b[l - 1].p);
     E.dirichlet_zero(l - 1, W.b[l - 1].p);
   }
-  int j = (p0 == 'V') ? 1 : (p0 == 'W') ? 2 : (p0 == 'F') ? 3 : 0;
   T* uc = W.u[l - 1].p;
   T* tc = W.v[l - 1].p;
   bool czero = true; // Zero(u) on l-1
   for (int i = 0; i < j; ++i)
     czero = mgstep<T>(E, W, l - 1, finelevel, coarselevel, p0, p, uc, tc,
-                      W.b[l - 1].p, czero);
+                      W.b[l - 1].p, czero, fused && i == 0);
   if (czero) // no sweep ran on l-1: its u is the zero of Zero(u)
     E.fill0(l - 1, uc);
   if ((l == 0) && (p == 'F'))

@@ -96,8 +96,11 @@ struct Emit
   void jacobi(int l, const T* u, T* out, const T* b);
   void resid(int l, const T* u, T* out, const T* b);
   // coarse (level l) = R fine, 0 on the coarse Dirichlet dofs; with smean
-  // (block levels) the filtered component of fine is read minus *smean
-  void restrict_to(int l, const T* fine, T* coarse, const double* smean = nullptr);
+  // (block levels) the filtered component of fine is read minus *smean; with
+  // u1 (scalar levels) the restriction also writes the coarse level's first
+  // Jacobi sweep from 0, u1 = omega D^-1 coarse
+  void restrict_to(int l, const T* fine, T* coarse, const double* smean = nullptr,
+                   T* u1 = nullptr);
   // u = A^-1 b on level 0 (the direct coarse solve)
   void direct(int l, T* u, const T* b);
   void fill0(int l, T* u);

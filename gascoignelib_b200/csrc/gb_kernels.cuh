@@ -387,20 +387,38 @@ transfer_row(const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
   return acc;
 }
 
+// Writes the restricted value of coarse row i and, with u1, the coarse level's
+// first Jacobi sweep from zero on it, u1 = omega (D^-1 b), in the arithmetic of
+// k_jacobi_from_zero<T, T> (the same bits as that kernel's launch after this
+// one).
+template<class T>
+__device__ __forceinline__ void
+restrict_store(int i, T acc, T* __restrict__ coarse, const uint8_t* __restrict__ cdir,
+               const T* __restrict__ dinv, T* __restrict__ u1, double omega)
+{
+  using TA = typename Acc<T, T>::type;
+  const T bi = (cdir && cdir[i]) ? T(0) : acc;
+  coarse[i] = bi;
+  if (u1)
+    u1[i] = static_cast<T>(static_cast<TA>(omega) *
+                           (static_cast<TA>(dinv[i]) * static_cast<TA>(bi)));
+}
+
 // coarse = R fine (MgInterpolatorMatrix::restrict_zero order), then 0 on the
-// coarse Dirichlet dofs.
+// coarse Dirichlet dofs; with u1, also the coarse first sweep (restrict_store).
 template<class T>
 __global__ void
 k_restrict(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
            const T* __restrict__ fine, T* __restrict__ coarse,
-           const uint8_t* __restrict__ cdir)
+           const uint8_t* __restrict__ cdir, const T* __restrict__ dinv,
+           T* __restrict__ u1, double omega)
 {
   GB_PDL_ENTRY();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nc)
     return;
   const T acc = transfer_row<T>(tsp, tent, fine, i);
-  coarse[i] = (cdir && cdir[i]) ? T(0) : acc;
+  restrict_store<T>(i, acc, coarse, cdir, dinv, u1, omega);
 }
 
 // The same restriction with four lanes per coarse row: lane q of the quad
@@ -412,7 +430,8 @@ template<class T>
 __global__ void __launch_bounds__(256)
 k_restrict4(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ tent,
             const T* __restrict__ fine, T* __restrict__ coarse,
-            const uint8_t* __restrict__ cdir)
+            const uint8_t* __restrict__ cdir, const T* __restrict__ dinv,
+            T* __restrict__ u1, double omega)
 {
   GB_PDL_ENTRY();
   const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -455,7 +474,7 @@ k_restrict4(int nc, const int* __restrict__ tsp, const uint32_t* __restrict__ te
         acc = fma(wcode<T>(ek), fk, acc);
     }
   if (ok && q == 0)
-    coarse[i] = (cdir && cdir[i]) ? T(0) : acc;
+    restrict_store<T>(i, acc, coarse, cdir, dinv, u1, omega);
 }
 
 // fine += P coarse (prolongate_add order), optionally masked by the fine
