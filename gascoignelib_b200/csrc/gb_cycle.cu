@@ -1100,27 +1100,58 @@ mgstep_down(Emit<T>& E, MgWork<T>& W, int l, int finelevel, int coarselevel, cha
 }
 
 // One cycle on the finest level into x (T), rhs y (T), from x's content or 0.
+// The buffer that a cycle from x = 0 (precondition_T with x_zero) runs its
+// first finest-level sweep into.
 template<class T>
-void
-precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero)
+static T*
+first_sweep_buffer(Context& c, MgWork<T>& W, T* x, bool x_zero)
 {
-  ensure_work(c);
   const int fl = c.nlevels - 1;
-  T* u = x;
-  T* tmp = W.v[fl].p;
-  // Pick the buffer of the first sweep so that the last write lands in x.
   const gb_params& P = c.params;
   int pingpong = (x_zero ? std::max(P.iterpre - 1, 0) : P.iterpre) + P.iterpost;
   if (fl == 0)
     pingpong = x_zero ? std::max(P.iterexact - 1, 0) : P.iterexact;
   if (!fused_smoother(c, c.L[fl]))
     pingpong = 0; // sweeps in place
-  if (x_zero && (pingpong & 1))
-    std::swap(u, tmp);
+  return x_zero && (pingpong & 1) ? W.v[fl].p : x;
+}
+
+// Where the finest level's first sweep of a cycle from x = 0 can be written by
+// the kernel that forms the cycle's right-hand side (k_load_idx): the buffer,
+// or nullptr where that sweep is not the fused scalar Jacobi sweep from zero.
+template<class T>
+T*
+precondition_first_sweep(Context& c, MgWork<T>& W, T* x)
+{
+  ensure_work(c);
+  const int fl = c.nlevels - 1;
+  Emit<T> E{ c, nullptr };
+  if (fl == 0 || !fuse_first_sweep<T>(E, fl, 0, 1))
+    return nullptr;
+  return first_sweep_buffer<T>(c, W, x, true);
+}
+
+// One cycle into x from x's content or (x_zero) from 0; first_done: from 0,
+// with the first finest-level sweep already in the buffer that
+// precondition_first_sweep named.
+template<class T>
+void
+precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero, bool first_done)
+{
+  ensure_work(c);
+  const int fl = c.nlevels - 1;
+  if (first_done)
+    x_zero = true;
+  T* tmp = W.v[fl].p;
+  // Pick the buffer of the first sweep so that the last write lands in x.
+  T* u = first_sweep_buffer<T>(c, W, x, x_zero);
+  if (u != x)
+    tmp = x;
+  const gb_params& P = c.params;
   char p = P.mgtype;
   char p0 = (p == 'F') ? 'W' : p;
   Emit<T> E{ c, nullptr };
-  if (mgstep<T>(E, W, fl, fl, 0, p0, p, u, tmp, y, x_zero))
+  if (mgstep<T>(E, W, fl, fl, 0, p0, p, u, tmp, y, first_done ? false : x_zero, first_done))
     E.fill0(fl, u);
   if (u != x) {
     GB_CUDA(cudaMemcpyAsync(x, u, c.L[fl].ndof() * sizeof(T),
@@ -1132,7 +1163,8 @@ precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero)
 
 #define GB_CYCLE_INST(T)                                                                   \
   template void smooth<T>(Emit<T>&, int, int, T*&, T*&, const T*, bool&);                  \
-  template void precondition_T<T>(Context&, MgWork<T>&, T*, const T*, bool);
+  template void precondition_T<T>(Context&, MgWork<T>&, T*, const T*, bool, bool);         \
+  template T* precondition_first_sweep<T>(Context&, MgWork<T>&, T*);
 GB_CYCLE_INST(double)
 GB_CYCLE_INST(float)
 #undef GB_CYCLE_INST

@@ -136,6 +136,9 @@ inline float* Emit<float>::vk_out(const Level& L)
 template<class T>
 void smooth(Emit<T>& E, int l, int niter, T*& u, T*& tmp, const T* b, bool& u_zero);
 template<class T>
-void precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero);
+void precondition_T(Context& c, MgWork<T>& W, T* x, const T* y, bool x_zero,
+                    bool first_done = false);
+template<class T>
+T* precondition_first_sweep(Context& c, MgWork<T>& W, T* x);
 
 } // namespace gb

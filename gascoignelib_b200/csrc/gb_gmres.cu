@@ -441,8 +441,12 @@ fg_inner(Context& c, const FBufs<T>& F, cudaGraphConditionalHandle hInner, int u
   const int64_t n = L.ndof();
   GmresDev* G = c.G.p;
   double* V = c.krylov.p;
-  launch(c, k_load_idx<T>, stream_blocks(n), 256, n, F.rhs, V, (const GmresDev*)G);
-  precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true);
+  // the cycle's right-hand side v_j and, where the finest smoother allows,
+  // the cycle's first finest-level sweep from zero in the same pass
+  T* u1 = precondition_first_sweep<T>(c, work<T>(c), F.zfix);
+  launch(c, k_load_idx<T>, stream_blocks(n), 256, n, F.rhs, V, (const GmresDev*)G,
+         dinv_of<T>(L), u1, c.params.omega);
+  precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true, u1 != nullptr);
   spmv<kAx, double, T, double>(c, L, opA(c, L), (const T*)F.zfix, V, nullptr, nullptr, 1.0,
                                (const int*)&G->j, n, F.Z);
   // one block of kCgsThreads per 2 kCgsThreads rows, at most four per SM

@@ -1088,10 +1088,26 @@ k_fg_restart(GmresDev* G, cudaGraphConditionalHandle outer,
 // v_j = w'' / s (s = ||w''||, formed from ||w'|| and the coefficients by the
 // previous step's k_cgs<1>) are applied here and stored back (v_0 was
 // normalised at the restart).
+// With u1, the cycle's first Jacobi sweep from zero on the finest level,
+// u1 = omega D^-1 y, in k_jacobi_from_zero<TO, TO>'s arithmetic (the same bits
+// as that kernel's launch after this one).
+template<class TO>
+__device__ __forceinline__ void
+load_store(int64_t i, TO yi, TO* __restrict__ y, const TO* __restrict__ dinv,
+           TO* __restrict__ u1, double omega)
+{
+  using TA = typename Acc<TO, TO>::type;
+  y[i] = yi;
+  if (u1)
+    u1[i] = static_cast<TO>(static_cast<TA>(omega) *
+                            (static_cast<TA>(dinv[i]) * static_cast<TA>(yi)));
+}
+
 template<class TO, int NV>
 __device__ __forceinline__ void
 load_idx_pass(int64_t n, TO* __restrict__ y, double* __restrict__ V,
-              const volatile double* coef, double s)
+              const volatile double* coef, double s, const TO* __restrict__ dinv,
+              TO* __restrict__ u1, double omega)
 {
   constexpr int kGroup = 8;
   const int j = NV; // the vector being loaded has NV basis vectors before it
@@ -1113,14 +1129,15 @@ load_idx_pass(int64_t n, TO* __restrict__ y, double* __restrict__ V,
     }
     t = s * t;
     v[i] = t;
-    y[i] = static_cast<TO>(t);
+    load_store<TO>(i, static_cast<TO>(t), y, dinv, u1, omega);
   }
 }
 
 template<class TO>
 __global__ void __launch_bounds__(256)
 k_load_idx(int64_t n, TO* __restrict__ y, double* __restrict__ V,
-           const GmresDev* __restrict__ G)
+           const GmresDev* __restrict__ G, const TO* __restrict__ dinv,
+           TO* __restrict__ u1, double omega)
 {
   GB_PDL_ENTRY();
   __shared__ double s_coef[kMaxV];
@@ -1132,14 +1149,14 @@ k_load_idx(int64_t n, TO* __restrict__ y, double* __restrict__ V,
     const double* v = V;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
-      y[i] = static_cast<TO>(v[i]);
+      load_store<TO>(i, static_cast<TO>(v[i]), y, dinv, u1, omega);
     return;
   }
   const double s = G->inv;
   switch (j) {
 #define GB_LOAD_CASE(K)                                                         \
   case K:                                                                      \
-    load_idx_pass<TO, K>(n, y, V, s_coef, s);                                  \
+    load_idx_pass<TO, K>(n, y, V, s_coef, s, dinv, u1, omega);                 \
     break;
     GB_LOAD_CASE(1) GB_LOAD_CASE(2) GB_LOAD_CASE(3) GB_LOAD_CASE(4) GB_LOAD_CASE(5)
     GB_LOAD_CASE(6) GB_LOAD_CASE(7) GB_LOAD_CASE(8) GB_LOAD_CASE(9) GB_LOAD_CASE(10)
