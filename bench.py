@@ -199,6 +199,23 @@ def _rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
 
 
+def max_over_ranks(ms, dist, device):
+    """The whole job's time of a timed region: the largest of the ranks' device
+    times (all-reduce MAX, the same collective on every rank); the local time
+    on one rank."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ndof, steps, world, ms):
+    """DoF/s of the whole job: every replica solves ndof unknowns per step."""
+    return ndof * steps * world / (ms / 1e3)
+
+
 def run_reference_arm(args, world, rank):
     from gascoignelib_b200.problem import seeded_inputs
     if rank != 0:
@@ -903,13 +920,8 @@ def main():
     msleft, infoleft = run_steps(None, args.steps, True)
     torch.cuda.synchronize()
 
-    t32 = sum(ms32)
-    tmax = t32
-    if dist:
-        t = torch.tensor([t32], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tmax = float(t.item())
-    value = ndof * args.steps * world / (tmax / 1e3)
+    tmax = max_over_ranks(sum(ms32), dist, f"cuda:{local}")
+    value = replica_value(ndof, args.steps, world, tmax)
     v64 = ndof * args.steps / (sum(ms64) / 1e3)
     vleft = ndof * args.steps / (sum(msleft) / 1e3)
 
@@ -924,7 +936,8 @@ def main():
         xn = x_host.numpy()
         _, info = ctx.solve_host(bn, method=2, out=xn)
         e2e_ms.append(info["device_ms"])
-    e2e_val = ndof * args.steps * world / (sum(e2e_ms) / 1e3)
+    e2e_val = replica_value(ndof, args.steps, world,
+                            max_over_ranks(sum(e2e_ms), dist, f"cuda:{local}"))
 
     # the solutions of the three solvers, for the accuracy keys (untimed)
     ctx.fgmres(xv, bv, GB_FP32)
