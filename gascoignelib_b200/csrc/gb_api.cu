@@ -29,6 +29,8 @@ gb_ctx_create(gb_ctx** out, int device)
       ctx->ilu_host = atoi(e) != 0;
     if (const char* e = getenv("GB_RB"))
       ctx->rb_on = atoi(e) != 0;
+    if (const char* e = getenv("GB_ROW_ORDER"))
+      ctx->row_order = atoi(e) != 0;
     if (const char* e = getenv("GB_ILU_CTA_ROWS"))
       ctx->ilu_cta_rows = std::max(0, atoi(e));
     if (const char* e = getenv("GB_VANKA_HOST"))
@@ -177,7 +179,7 @@ gb_level_set_matrix(gb_ctx* ctx, int lvl, int64_t n, int B, const int64_t* rowpt
   L.h_col.assign(col, col + nnzb);
   L.h_diag.assign(diag, diag + n);
   L.h_val.assign(val, val + nnzb * B * B);
-  build_sell(L.A, n, rowptr, col, val, ctx->stream, B);
+  build_sell(L.A, n, rowptr, col, val, ctx->stream, B, ctx->row_order);
   build_rows(*ctx, L.A, rowptr);
   L.has_AT = false;
   L.vk_ready = false;

@@ -445,6 +445,10 @@ struct gb_ctx
   bool vanka_host = false;
   bool ilu_host = false; // GB_ILU_HOST=1: block ILU factors formed on the host
   bool rb_on = false;    // GB_RB=1: row-block copies and SpMV on the large FP32 levels
+  // the slots of levels above 1024 rows without column patterns ordered by
+  // each row's smallest column before the windows are sorted by length
+  // (GB_ROW_ORDER=0: not)
+  bool row_order = true;
   // widest substitution level run inside a single-CTA launch
   // (GB_ILU_CTA_ROWS; 0: one launch per level)
   int ilu_cta_rows = gb::kIluCtaDefaultRows;
@@ -683,7 +687,7 @@ constexpr int kRbLanes = 4; // lanes per row (2, 4 and 8 measured; 2 and 4 faste
 void build_patterns(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
                     cudaStream_t st);
 void build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
-                const double* val, cudaStream_t st, int B = 1);
+                const double* val, cudaStream_t st, int B = 1, bool locality = false);
 void rows_refresh(Context& c, const Sell& S, bool columns);
 void build_rows(Context& c, Sell& S, const int64_t* rowptr);
 void host_values(Context& c, Level& L);

@@ -54,16 +54,19 @@ build_patterns(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
 
 void
 build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
-           const double* val, cudaStream_t st, int B)
+           const double* val, cudaStream_t st, int B, bool locality)
 {
   const int B2 = B * B;
   S.B = B;
   S.n = static_cast<int>(n);
   S.nslices = static_cast<int>((n + kSlice - 1) / kSlice);
   S.nnz = rowptr[n];
-  // Slot order: rows sorted by length (descending, stable) inside windows of
-  // kSortWindow rows when that saves more than a tenth of the padded slots
-  // (levels above the single-CTA coarse size only).
+  // the column patterns (per row, independent of the slot order)
+  build_patterns(S, n, rowptr, col, st);
+  // Slot order: on levels without column patterns (locality), rows in the
+  // order of their smallest column; then rows sorted by length (descending,
+  // stable) inside windows of kSortWindow rows when that saves more than a
+  // tenth of the padded slots (levels above the single-CTA coarse size only).
   constexpr int64_t kSortWindow = 256;
   std::vector<int> perm(n);
   for (int64_t r = 0; r < n; ++r)
@@ -79,6 +82,25 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
     return tot;
   };
   S.sorted = false;
+  if (locality && !S.pat && n > 1024) {
+    // slots in the order of each row's smallest column: on a hierarchically
+    // numbered mesh (the reference's refined meshes: no column patterns) the
+    // rows of one neighbourhood share their smallest (coarsest) column, so the
+    // 32 rows of a slice gather nearby x values. Each row keeps its entries
+    // and their order, so every row's result is unchanged. Measured on C4 (the
+    // reference's ball-refined Q2 mesh): FP32 sweep 182 -> 148 us, FP64 SpMV
+    // 203 -> 174 us, mixed solve 170.8 -> 155.8 ms.
+    std::vector<int64_t> key(n);
+    for (int64_t r = 0; r < n; ++r) {
+      int64_t m = r;
+      for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k)
+        m = std::min(m, col[k]);
+      key[r] = m;
+    }
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+    for (int64_t t = 0; t < n && !S.sorted; ++t)
+      S.sorted = perm[t] != t;
+  }
   if (n > 1024) {
     std::vector<int> sp(perm);
     for (int64_t w0 = 0; w0 < n; w0 += kSortWindow)
@@ -154,7 +176,6 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
   GB_CUDA(cudaStreamSynchronize(st));
   S.h_sptr = sptr;
   S.h_perm = perm;
-  build_patterns(S, n, rowptr, col, st);
   S.off16 = false;
   if (!S.pat && S.entries) {
     std::vector<int16_t> h(S.entries, 0);
@@ -333,7 +354,7 @@ ensure_AT(Context& c, Level& L)
       }
   }
   GB_CUDA(cudaStreamSynchronize(c.stream));
-  build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), c.stream, B);
+  build_sell(L.AT, n, tp.data(), tc.data(), tv.data(), c.stream, B, c.row_order);
   build_rows(c, L.AT, tp.data());
   L.has_AT = true;
   if (B == 1 && L.mesh_ncells > 0) { // device-assembled level: keep A^T current on the GPU
