@@ -445,9 +445,9 @@ struct gb_ctx
   bool vanka_host = false;
   bool ilu_host = false; // GB_ILU_HOST=1: block ILU factors formed on the host
   bool rb_on = false;    // GB_RB=1: row-block copies and SpMV on the large FP32 levels
-  // the slots of levels above 1024 rows without column patterns ordered by
-  // each row's smallest column before the windows are sorted by length
-  // (GB_ROW_ORDER=0: not)
+  // the slots of scalar levels above 1024 rows without column patterns
+  // ordered by each row's smallest column before the windows are sorted by
+  // length (GB_ROW_ORDER=0: not)
   bool row_order = true;
   // widest substitution level run inside a single-CTA launch
   // (GB_ILU_CTA_ROWS; 0: one launch per level)

@@ -82,14 +82,16 @@ build_sell(Sell& S, int64_t n, const int64_t* rowptr, const int64_t* col,
     return tot;
   };
   S.sorted = false;
-  if (locality && !S.pat && n > 1024) {
+  if (locality && !S.pat && B == 1 && n > 1024) {
     // slots in the order of each row's smallest column: on a hierarchically
     // numbered mesh (the reference's refined meshes: no column patterns) the
     // rows of one neighbourhood share their smallest (coarsest) column, so the
     // 32 rows of a slice gather nearby x values. Each row keeps its entries
     // and their order, so every row's result is unchanged. Measured on C4 (the
     // reference's ball-refined Q2 mesh): FP32 sweep 182 -> 148 us, FP64 SpMV
-    // 203 -> 174 us, mixed solve 170.8 -> 155.8 ms.
+    // 203 -> 174 us, mixed solve 170.8 -> 155.8 ms. Block levels (B > 1)
+    // keep the mesh's order: on C3 (2D Q1/Q1 Stokes, B = 3) this order made
+    // the FP64 solve slower (16.5 -> 18.0 ms).
     std::vector<int64_t> key(n);
     for (int64_t r = 0; r < n; ++r) {
       int64_t m = r;
