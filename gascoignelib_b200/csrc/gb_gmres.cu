@@ -449,7 +449,7 @@ fg_inner(Context& c, const FBufs<T>& F, cudaGraphConditionalHandle hInner, int u
   precondition_T<T>(c, work<T>(c), F.zfix, F.rhs, true, u1 != nullptr);
   spmv<kAx, double, T, double>(c, L, opA(c, L), (const T*)F.zfix, V, nullptr, nullptr, 1.0,
                                (const int*)&G->j, n, F.Z);
-  // one block of kCgsThreads per 2 kCgsThreads rows, at most four per SM
+  // one block of kCgsThreads per 2 kCgsThreads rows, at most one wave
   const int rg = static_cast<int>(std::max<int64_t>(
     1, std::min<int64_t>((n + 2 * kCgsThreads - 1) / (2 * kCgsThreads), kCgsMaxBlocks)));
   const int m = c.params.gmressize - 1;

@@ -1197,7 +1197,13 @@ k_scale_idx(int64_t n, double* __restrict__ V, const int* __restrict__ jp,
 // block sums the per-block partials in block order: deterministic for a fixed
 // grid.
 constexpr int kCgsThreads = 256;
-constexpr int kCgsMaxBlocks = 4 * 148;
+// at most one wave: the CGS kernels hold 2 blocks per SM (128 registers per
+// thread), and a partial second wave of a 4 x 148 grid made the C2 solves
+// slower (mixed 1.500 against 1.460 ms, FP64 1.646 against 1.593 ms)
+#ifndef GB_CGS_MAX_BLOCKS
+#define GB_CGS_MAX_BLOCKS (2 * 148)
+#endif
+constexpr int kCgsMaxBlocks = GB_CGS_MAX_BLOCKS;
 
 static __device__ void fg_step(GmresDev* G, cudaGraphConditionalHandle inner, int m,
                         int use_cond);
