@@ -499,9 +499,9 @@ int gb_kernel_arch(int* binary_version, int* ptx_version);
  * 4096 * 2048 = 8,388,608; larger n returns GB_EINVAL.
  * The first call on a device looks up that array's device address
  * (cudaGetSymbolAddress, with that device current) and keeps it for the life
- * of the process; that first call should come before any stream capture. The
- * kept address does not survive cudaDeviceReset: a caller that resets a
- * device must not call this function on it again in the same process.
+ * of the process. The kept address does not survive cudaDeviceReset: a caller
+ * that resets a device must not call this function on it again in the same
+ * process.
  * The function makes CUDA runtime calls, so it must not be called from a CUDA
  * host function (cudaLaunchHostFunc, stream callbacks). Calls share the
  * array, and each call clears its ticket before use: two calls that overlap
