@@ -105,3 +105,60 @@ def test_q2_ball_generator_solve_matches_oracle(ctx):
         assert rel_l2(ctx.download(l, x), xo) < 1e-6
     ctx.free(x)
     ctx.free(b)
+
+
+def _context_with(env):
+    from gascoignelib_b200.native import Context
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return Context(0)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+def test_locality_slot_order_leaves_results_unchanged():
+    """The slots of pattern-free scalar levels ordered by each row's smallest
+    column (the default) against the mesh's own order (GB_ROW_ORDER=0): every
+    row keeps its entries and their order, so the SpMV, a smoothing sweep and
+    the reference-semantics and flexible solves give the same bits. The ball
+    mesh's refined levels have no column patterns."""
+    from gascoignelib_b200.problem import structured_q2_ball
+
+    P = structured_q2_ball(2, 3, eps=0.1)
+    l = P.nlevels - 1
+    rng = np.random.default_rng(7)
+    xv = rng.standard_normal(P.levels[l].ndof)
+    out = {}
+    for tag, env in (("mesh", {"GB_ROW_ORDER": "0"}), ("locality", {})):
+        c = _context_with(env)
+        try:
+            c.load_problem(P)
+            c.set_params(iterpre=2, iterpost=2, iterexact=10, omega=0.3, mgomega=1.0,
+                         mgtype="V", gmressize=31, tol=1e-8, globaltol=1e-300, maxiter=100)
+            x, y, h = c.vec(), c.vec(), c.vec()
+            res = []
+            c.upload(l, x, xv)
+            c.vmult(l, y, x, 1.0)
+            res.append(c.download(l, y))
+            c.upload(l, y, P.rhs)
+            c.smooth(l, 2, x, y, h)
+            res.append(c.download(l, x))
+            c.upload(l, x, np.zeros_like(xv))
+            res.append((c.gmres(x, y)["iterations"], c.download(l, x)))
+            for prec in (GB_FP64, GB_FP32):
+                c.fgmres(x, y, prec)
+                res.append(c.download(l, x))
+            out[tag] = res
+        finally:
+            c.close()
+    a, b = out["mesh"], out["locality"]
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(a[1], b[1])
+    assert a[2][0] == b[2][0] and np.array_equal(a[2][1], b[2][1])
+    assert np.array_equal(a[3], b[3])
+    assert np.array_equal(a[4], b[4])
